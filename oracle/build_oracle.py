@@ -1,0 +1,95 @@
+"""Build recipe for the test oracle (test infrastructure only).
+
+Two shared libraries come out of here:
+
+* ``oracle/liboracle.so`` -- the CPU restatement in ``oracle/wbfmm_oracle.c``
+  (our own code; builds anywhere gcc is present);
+* ``oracle/_ref/libwbfmm_ref.so`` -- the UNMODIFIED reference sources from
+  ``/root/reference/src`` plus the GLib/blaswrap shim in ``oracle/shim`` and
+  the call-sequence harness ``oracle/ref_harness.c``.  Built only where the
+  reference tree is present; the built ``.so`` travels with the repository
+  snapshot (``oracle/_ref`` is git-ignored, not snapshot-ignored).
+
+Flags follow the reference's own build (configure.ac, tools/Makefile.am):
+``-O3 -g -mavx -mfma -fopenmp -DWBFMM_USE_AVX -DHAVE_CONFIG_H`` with its shipped
+``config.h``.  The reference's logging module (src/wbfmm-logging.c) is left out:
+nothing on the FMM path calls it.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_ROOT = os.environ.get("WBFMM_REFERENCE_ROOT", "/root/reference")
+REF_OUT = os.path.join(HERE, "_ref")
+BUILD_DIR = os.path.join(HERE, "_build")
+
+REF_FLAGS = [
+    "-O3", "-g", "-mavx", "-mfma", "-fopenmp", "-fPIC",
+    "-DWBFMM_USE_AVX", "-DHAVE_CONFIG_H",
+    '-DWBFMM_COMPILER_FLAGS="-O3 -g -mavx -mfma -fopenmp -DWBFMM_USE_AVX"',
+]
+
+
+def _newer(target: str, sources: list[str]) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(s) > t for s in sources if os.path.exists(s))
+
+
+def _run(cmd: list[str]) -> None:
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError("oracle build failed: " + " ".join(cmd[:4]) + " ...")
+
+
+def build_restatement(force: bool = False) -> str:
+    """Compile the CPU restatement (oracle/wbfmm_oracle.c)."""
+    src = os.path.join(HERE, "wbfmm_oracle.c")
+    out = os.path.join(HERE, "liboracle.so")
+    if force or _newer(out, [src, __file__]):
+        _run(["gcc", "-O2", "-fPIC", "-shared", "-pthread", "-ffp-contract=off",
+              src, "-o", out, "-lm"])
+    return out
+
+
+def build_reference(force: bool = False) -> str | None:
+    """Compile the reference sources + shim + harness; None if absent."""
+    src_dir = os.path.join(REF_ROOT, "src")
+    out = os.path.join(REF_OUT, "libwbfmm_ref.so")
+    if not os.path.isdir(src_dir):
+        return out if os.path.exists(out) else None
+    srcs = sorted(
+        os.path.join(src_dir, f)
+        for f in os.listdir(src_dir)
+        if f.endswith(".c") and f != "wbfmm-logging.c"
+    )
+    extra = [os.path.join(HERE, "shim", "glib_shim.c"),
+             os.path.join(HERE, "ref_harness.c")]
+    deps = srcs + extra + [os.path.join(HERE, "shim", "glib.h"), __file__]
+    if not (force or _newer(out, deps)):
+        return out
+    os.makedirs(REF_OUT, exist_ok=True)
+    os.makedirs(BUILD_DIR, exist_ok=True)
+    objs = []
+    incs = ["-I", os.path.join(HERE, "shim"), "-I", REF_ROOT, "-I", src_dir]
+    for s in srcs + extra:
+        o = os.path.join(BUILD_DIR, os.path.basename(s)[:-2] + ".o")
+        if force or _newer(o, [s]):
+            _run(["gcc", "-c", *REF_FLAGS, *incs, s, "-o", o])
+        objs.append(o)
+    _run(["gcc", "-shared", "-fopenmp", "-o", out, *objs, "-lm", "-lpthread"])
+    return out
+
+
+def main() -> None:
+    print(build_restatement(force="--force" in sys.argv))
+    print(build_reference(force="--force" in sys.argv))
+
+
+if __name__ == "__main__":
+    main()
