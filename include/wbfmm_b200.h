@@ -1,0 +1,145 @@
+/*
+ * C ABI of the B200 FMM engine (libwbfmm_b200.so).
+ *
+ * Plain pointers and sizes only.  Every call returns 0 on success or a
+ * negative status; wbfmm_b200_last_error() describes the last failure of the
+ * calling thread.  All device work of a solver runs on the CUDA stream given
+ * at creation (0 = the library's own stream).
+ *
+ * The solver replays the reference drivers' call sequence
+ * (tools/wbfmm-tree-calc.c.in:270-414, tools/wbfmm-laplace-tree-calc.c.in:
+ * 336-460) on the GPU:
+ *   tree build          wbfmm_tree_add_points + wbfmm_tree_refine x depth
+ *                       (src/boxes.c:118-277)
+ *   operators           wbfmm_shift_operators_new / _coaxial_SR_init /
+ *                       _coaxial_SS_init (src/shift.c:726-861),
+ *                       wbfmm_laplace_coaxial_translate_init (src/laplace.c:727)
+ *   P2M                 wbfmm_tree_leaf_expansions (src/boxes.c:341-490),
+ *                       wbfmm_tree_laplace_leaf_expansions (src/laplace.c:854)
+ *   upward pass         wbfmm_upward_pass, wbfmm_laplace_upward_pass
+ *   downward pass       wbfmm_downward_pass_{ref,avx},
+ *                       wbfmm_laplace_downward_pass_{ref,avx}
+ *   evaluation          wbfmm_tree_box_local_field (src/local.c:264-310),
+ *                       wbfmm_laplace_box_field (src/local-laplace.c:1293)
+ * with coefficients in the reference's Layout L (groups of eight boxes).
+ */
+#ifndef WBFMM_B200_H
+#define WBFMM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WBFMM_B200_LAPLACE 1
+#define WBFMM_B200_HELMHOLTZ 2
+
+#define WBFMM_B200_FP64 0 /* plain form: FP64 everywhere */
+#define WBFMM_B200_FP32 1 /* FP32 bulk, FP64 tables, compensated P2P */
+
+#define WBFMM_B200_POTENTIAL 1
+#define WBFMM_B200_GRADIENT 2
+
+#define WBFMM_B200_MAX_DEPTH 16
+
+/* status codes */
+#define WBFMM_B200_OK 0
+#define WBFMM_B200_E_ARG (-1)       /* invalid argument */
+#define WBFMM_B200_E_DOMAIN (-2)    /* point outside the tree cube */
+#define WBFMM_B200_E_ORDER (-3)     /* expansion order unsupported */
+#define WBFMM_B200_E_STATE (-4)     /* call out of sequence */
+#define WBFMM_B200_E_NOMEM (-5)     /* device allocation failed */
+#define WBFMM_B200_E_ADMISSION (-6) /* over the device-memory budget */
+#define WBFMM_B200_E_NOGPU (-7)     /* no CUDA device */
+
+typedef struct {
+  int problem;        /* WBFMM_B200_LAPLACE or WBFMM_B200_HELMHOLTZ */
+  int depth;          /* tree depth, >= 2 */
+  int order_s[WBFMM_B200_MAX_DEPTH + 1]; /* singular order per level */
+  int order_r[WBFMM_B200_MAX_DEPTH + 1]; /* regular order per level */
+  double k;           /* wavenumber (Helmholtz) */
+  double x0[3];       /* tree cube origin */
+  double D;           /* tree cube width */
+  int precision;      /* WBFMM_B200_FP64 or WBFMM_B200_FP32 */
+  int field;          /* WBFMM_B200_POTENTIAL | WBFMM_B200_GRADIENT */
+  int skip_empty;     /* 1: skip M2L work for boxes with no sources / no
+                         targets below (exact for the fields; the regular
+                         expansions of target-free boxes are then left 0) */
+  int managed;        /* 1: coefficient arrays in CUDA managed memory so the
+                         host can read them in place */
+} wbfmm_b200_config_t;
+
+typedef struct wbfmm_b200_solver wbfmm_b200_solver_t;
+
+/* library */
+const char *wbfmm_b200_last_error(void);
+int wbfmm_b200_device_count(void);
+
+/* solver lifetime */
+int wbfmm_b200_solver_create(wbfmm_b200_solver_t **s,
+                             const wbfmm_b200_config_t *cfg, void *stream);
+int wbfmm_b200_solver_destroy(wbfmm_b200_solver_t *s);
+/* bytes of device memory the solver would hold for n sources and m targets */
+int64_t wbfmm_b200_footprint(const wbfmm_b200_config_t *cfg, int64_t nsrc,
+                             int64_t ntgt);
+
+/* Sources: xs[i*xstr + 0..2]; normals (may be NULL) likewise.  Pointers are
+   host memory unless on_device != 0.  Builds the tree: Morton keys, stable
+   sort, per-level box ranges. */
+int wbfmm_b200_set_sources(wbfmm_b200_solver_t *s, int nsrc, const double *xs,
+                           int xstr, const double *normals, int nstr,
+                           int on_device);
+/* Strengths: Laplace q[i*qstr], Helmholtz (q[i*qstr], q[i*qstr+1]);
+   dipole strengths likewise (need normals).  Either may be NULL. */
+int wbfmm_b200_set_strengths(wbfmm_b200_solver_t *s, const double *q,
+                             int qstr, const double *dipoles, int dstr,
+                             int on_device);
+/* Targets: xt[i*tstr + 0..2] (closed cube). */
+int wbfmm_b200_set_targets(wbfmm_b200_solver_t *s, int ntgt,
+                           const double *xt, int tstr, int on_device);
+
+/* stages */
+int wbfmm_b200_build_operators(wbfmm_b200_solver_t *s);
+int wbfmm_b200_leaf_expansions(wbfmm_b200_solver_t *s);
+int wbfmm_b200_upward_pass(wbfmm_b200_solver_t *s, int level);
+int wbfmm_b200_downward_pass(wbfmm_b200_solver_t *s, int level);
+int wbfmm_b200_evaluate(wbfmm_b200_solver_t *s);
+/* all stages after set_sources/set_strengths/set_targets */
+int wbfmm_b200_run(wbfmm_b200_solver_t *s);
+int wbfmm_b200_synchronize(wbfmm_b200_solver_t *s);
+
+/* Results in ORIGINAL target order.  pot: Laplace [n], Helmholtz [2n];
+   grad: Laplace [3n], Helmholtz [6n] (d/dx re, im, d/dy re, im, d/dz re,
+   im).  Host pointers unless on_device. */
+int wbfmm_b200_get_field(wbfmm_b200_solver_t *s, double *pot, double *grad,
+                         int on_device);
+
+/* tree and coefficient inspection (host copies) */
+int wbfmm_b200_get_tree(wbfmm_b200_solver_t *s, uint32_t *ip,
+                        uint32_t *box_i, uint32_t *box_n, int level);
+/* level coefficient arrays in Layout L as FP64 (FP32 forms are widened):
+   Helmholtz 2*8^l*(p+1)^2 doubles, Laplace 8^l*(p+1)^2 */
+int wbfmm_b200_get_coefficients(wbfmm_b200_solver_t *s, int level,
+                                double *mps, double *mpr);
+/* device pointers of the level arrays (precision of the solver) */
+int wbfmm_b200_coefficient_pointers(wbfmm_b200_solver_t *s, int level,
+                                    void **mps, void **mpr);
+/* per-stage device times of the last run (ms): tree, operators, P2M,
+   upward, downward, evaluation */
+int wbfmm_b200_stage_times(wbfmm_b200_solver_t *s, double *ms6);
+/* number of kernels the solver launched since creation */
+int64_t wbfmm_b200_kernel_launches(wbfmm_b200_solver_t *s);
+
+/* One call: create, build, run, copy out, destroy.  Host buffers. */
+int wbfmm_b200_solve(const wbfmm_b200_config_t *cfg, int nsrc,
+                     const double *xs, const double *q, const double *normals,
+                     const double *dipoles, int ntgt, const double *xt,
+                     double *pot, double *grad);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WBFMM_B200_H */

@@ -1,0 +1,166 @@
+"""Parity of the GPU engine with the reference, through the C ABI.
+
+* plain FP64 form: field and gradient within 1e-10 (relative L2 and relative
+  max) of the reference CPU FMM at the same depth and orders, against the
+  committed golden fixtures and, where the reference library is built, live;
+* tree: `t->ip` and every box {i, n} bit-exact, including the values the
+  reference's refinement leaves in non-leaf levels;
+* coefficients: every level's singular and regular expansions, Layout L,
+  within 1e-10 of the reference;
+* FP32 form: within 1e-6 relative L2 of the plain FP64 form.
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from oracle.oracle_api import HELMHOLTZ, LAPLACE, level_box_offsets
+from wbfmm_b200 import engine, workloads as W
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+TOL_FP64 = 1e-10
+TOL_FP32 = 1e-6
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def rel_max(a, b):
+    return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+
+
+def load_case(path):
+    z = np.load(path)
+    p = W.Problem(os.path.basename(path)[:-4], int(z["problem"]), int(z["depth"]),
+                  list(z["order_s"]), list(z["order_r"]), float(z["k"]), z["xs"],
+                  z["q"] if z["q"].size else None, z["xt"],
+                  normals=z["normals"] if z["normals"].size else None,
+                  dipoles=z["dipoles"] if z["dipoles"].size else None)
+    p.x0, p.D = z["x0"], float(z["D"])
+    return p, z
+
+
+def run(p, precision=engine.FP64, field=engine.POTENTIAL | engine.GRADIENT,
+        keep=False):
+    cfg = engine.SolverConfig.from_problem(p, precision, field)
+    s = engine.Solver(cfg)
+    s.set_sources(p.xs, p.normals)
+    s.set_strengths(p.q, p.dipoles)
+    s.set_targets(p.xt)
+    s.run()
+    pot, grad = s.field()
+    if keep:
+        return s, pot, grad
+    s.close()
+    return pot, grad
+
+
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "*.npz"))),
+                         ids=lambda x: os.path.basename(x)[:-4])
+def test_golden_fp64(gpu_lib, path):
+    p, z = load_case(path)
+    has_grad = z["grad"].size > 0
+    field = engine.POTENTIAL | (engine.GRADIENT if has_grad else 0)
+    s, pot, grad = run(p, field=field, keep=True)
+    try:
+        assert rel_l2(pot, z["pot"]) < TOL_FP64
+        assert rel_max(pot, z["pot"]) < TOL_FP64
+        if has_grad:
+            assert rel_l2(grad, z["grad"]) < TOL_FP64
+            assert rel_max(grad, z["grad"]) < TOL_FP64
+        # tree: bit-exact permutation and box ranges at every level
+        offs = level_box_offsets(p.depth)
+        for lv in range(p.depth + 1):
+            ip, bi, bn = s.tree(lv)
+            ref = z["boxes"][offs[lv]:offs[lv + 1]]
+            assert np.array_equal(ip, z["ip"])
+            assert np.array_equal(bi, ref[:, 0]), f"box .i differs at level {lv}"
+            assert np.array_equal(bn, ref[:, 1]), f"box .n differs at level {lv}"
+    finally:
+        s.close()
+
+
+@pytest.mark.parametrize("name", ["laplace", "helmholtz"])
+def test_coefficients_every_level(gpu_lib, reference, name):
+    if name == "laplace":
+        p = W.laplace_cube(3000, 800, depth=4, order=7, seed=21)
+    else:
+        p = W.helmholtz_cube(3000, k=6.0, depth=4, seed=22)
+        p.xt = p.xt[:800]
+    r = reference.fmm(p.problem, p.depth, p.order_s, p.order_r, p.x0, p.D, p.xs,
+                      p.q, p.xt, k=p.k, want_coeffs=True)
+    s, pot, grad = run(p, keep=True)
+    try:
+        w = 2 if p.problem == HELMHOLTZ else 1
+        os_ = ors = 0
+        for lv in range(1, p.depth + 1):
+            ns = 8 ** lv * (p.order_s[lv] + 1) ** 2 * w
+            nr = 8 ** lv * (p.order_r[lv] + 1) ** 2 * w
+            ms, mr = s.coefficients(lv)
+            if lv >= 2:
+                assert rel_max(ms, r["mps"][os_:os_ + ns]) < TOL_FP64, f"mps level {lv}"
+                assert rel_max(mr, r["mpr"][ors:ors + nr]) < TOL_FP64, f"mpr level {lv}"
+            os_ += ns
+            ors += nr
+        assert rel_l2(pot, r["pot"]) < TOL_FP64
+        assert rel_l2(grad, r["grad"]) < TOL_FP64
+    finally:
+        s.close()
+
+
+def test_laplace_c1_reference_config(gpu_lib, reference):
+    """Laplace, 2e4 sources / 2e4 targets, depth 4, order 12: the
+    reference's own CPU-runnable configuration."""
+    p = W.laplace_cube(20000, 20000, depth=4, order=12, seed=1)
+    r = reference.fmm(p.problem, p.depth, p.order_s, p.order_r, p.x0, p.D, p.xs,
+                      p.q, p.xt, nthreads=os.cpu_count() or 1)
+    pot, grad = run(p)
+    assert rel_l2(pot, r["pot"]) < TOL_FP64
+    assert rel_l2(grad, r["grad"]) < TOL_FP64
+    assert rel_max(pot, r["pot"]) < TOL_FP64
+
+
+def test_helmholtz_per_level_orders(gpu_lib, reference):
+    """Helmholtz with per-level orders from the box width (orders differ
+    between levels, exercising M2M/L2L between different orders)."""
+    p = W.helmholtz_cube(30000, k=8.0, depth=5, seed=2)
+    assert len(set(p.order_s[2:])) > 1
+    p.xt = p.xs[:3000]
+    r = reference.fmm(p.problem, p.depth, p.order_s, p.order_r, p.x0, p.D, p.xs,
+                      p.q, p.xt, k=p.k, nthreads=os.cpu_count() or 1)
+    pot, grad = run(p)
+    assert rel_l2(pot, r["pot"]) < TOL_FP64
+    assert rel_l2(grad, r["grad"]) < TOL_FP64
+
+
+@pytest.mark.parametrize("name", ["laplace_small", "helmholtz_small"])
+def test_fp32_form_vs_fp64(gpu_lib, name):
+    p, z = load_case(os.path.join(GOLDEN, name + ".npz"))
+    pot64, grad64 = run(p, engine.FP64)
+    pot32, grad32 = run(p, engine.FP32)
+    assert rel_l2(pot32, pot64) < TOL_FP32
+    assert rel_l2(grad32, grad64) < TOL_FP32
+
+
+def test_direct_sum_accuracy(gpu_lib):
+    """FMM error against the FP64 direct sum is the truncation error of the
+    expansion order (checked loosely; parity is checked above)."""
+    p, z = load_case(os.path.join(GOLDEN, "laplace_small.npz"))
+    pot, grad = run(p)
+    assert rel_l2(pot, z["direct_pot"]) < 1e-4
+    assert rel_l2(grad, z["direct_grad"]) < 1e-3
+
+
+def test_domain_error(gpu_lib):
+    p = W.laplace_cube(500, 100, depth=2, order=4, seed=3)
+    cfg = engine.SolverConfig.from_problem(p)
+    with engine.Solver(cfg) as s:
+        xs = p.xs.copy()
+        xs[7] = p.x0  # on the cube's corner: not strictly inside
+        with pytest.raises(engine.WbfmmError) as e:
+            s.set_sources(xs)
+        assert e.value.code == -2

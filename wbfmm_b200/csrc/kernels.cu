@@ -1,0 +1,698 @@
+// FMM pass kernels: P2M, M2M, M2L, L2L, L2P and P2P.
+//
+//  P2M  one warp per leaf box; lanes take the box's sources 32 at a time and
+//       every coefficient contribution is reduced across the warp in a fixed
+//       order (deterministic), accumulating in shared memory.
+//  M2M  one CTA per parent; warps take the eight children.
+//  M2L  one CTA per target box (optionally split over several CTAs); warps
+//       take the list-4 sources (src/indexing.c:330-377) and run the
+//       rotate / coaxial / rotate-back sequence in shared memory,
+//       accumulating per warp; the warps' partial sums are added in a
+//       fixed order.
+//  L2L  one CTA per parent; one warp per child.
+//  L2P  one thread per target.
+//  P2P  one warp per leaf box holding targets; lanes take the flattened
+//       sources of the 27 neighbour boxes (src/indexing.c:250-286).
+#include <cuda_runtime.h>
+
+#include "engine.h"
+#include "expand.cuh"
+#include "kernels.h"
+#include "translate.cuh"
+
+namespace wbfmm {
+
+// |d|^2 of the 15 list-4 distances (src/shift.c:709-723), device copy
+__constant__ int c_list_dist2[15] = {4, 5, 6, 8, 9, 10, 11, 12, 13, 14,
+                                     17, 18, 19, 22, 27};
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// box centre exactly as wbfmm_tree_box_centre (src/util.c:290-330)
+__device__ __forceinline__ void box_centre(int64_t b, double x0, double y0,
+                                           double z0, double wb, double* c) {
+  uint32_t i, j, k;
+  demorton((uint64_t)b, &i, &j, &k);
+  c[0] = x0 + wb * i; c[1] = y0 + wb * j; c[2] = z0 + wb * k;
+  c[0] += 0.5 * wb; c[1] += 0.5 * wb; c[2] += 0.5 * wb;
+}
+
+// ------------------------------------------------------------------- P2M
+template <typename T, bool HELM>
+__global__ void k_p2m(P2MParams<T> p) {
+  extern __shared__ unsigned char smraw[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nw = blockDim.x >> 5;
+  const int64_t b = (int64_t)blockIdx.x * nw + warp;
+  if (b >= p.nbox) return;   // whole warp leaves; no block barriers below
+  const int nc = ncoef(p.N);
+  const int w = HELM ? 2 : 1;
+  T* acc = (T*)smraw + (size_t)warp * nc * w;
+  for (int c = lane; c < nc * w; c += 32) acc[c] = T(0);
+  __syncwarp();
+  const uint32_t cnt = p.box_n[b], start = p.box_i[b];
+  if (cnt > 0) {
+    double cd[3];
+    box_centre(b, p.x0, p.y0, p.z0, p.wb, cd);
+    // source position relative to the box centre, formed in FP64
+    const T xc[3] = {T(0), T(0), T(0)};
+    for (uint32_t base = 0; base < cnt; base += 32) {
+      const uint32_t t = base + lane;
+      const bool act = t < cnt;
+      const uint32_t s = start + (act ? t : 0);
+      T xs[3] = {act ? (T)(p.x[s] - cd[0]) : T(0),
+                 act ? (T)(p.y[s] - cd[1]) : T(0),
+                 act ? (T)(p.z[s] - cd[2]) : T(0)};
+      if (HELM) {
+        auto emit = [&](int idx, T re, T im) {
+          re = warp_sum(re); im = warp_sum(im);
+          if (lane == 0) { acc[2 * idx] += re; acc[2 * idx + 1] += im; }
+        };
+        if (p.q) {
+          T qr = act ? p.q[2 * s] : T(0), qi = act ? p.q[2 * s + 1] : T(0);
+          p2m_helmholtz<T>(p.N, p.k, xc, xs, qr, qi, emit);
+        }
+        if (p.dip) {
+          T dr = act ? p.dip[2 * s] : T(0), di = act ? p.dip[2 * s + 1] : T(0);
+          T nrm[3] = {act ? p.nx[s] : T(0), act ? p.ny[s] : T(0),
+                      act ? p.nz[s] : T(1)};
+          p2m_helmholtz_dipole<T>(p.N, p.k, xc, xs, nrm, dr, di, emit);
+        }
+      } else {
+        auto emit = [&](int idx, T v) {
+          v = warp_sum(v);
+          if (lane == 0) acc[idx] += v;
+        };
+        if (p.q) {
+          T qv = act ? p.q[s] : T(0);
+          p2m_laplace<T>(p.N, xc, xs, qv, emit);
+        }
+        if (p.dip) {
+          T dv = act ? p.dip[s] : T(0);
+          T nrm[3] = {act ? p.nx[s] : T(0), act ? p.ny[s] : T(0),
+                      act ? p.nz[s] : T(1)};
+          p2m_laplace_dipole<T>(p.N, xc, xs, nrm, dv, emit);
+        }
+      }
+    }
+  }
+  __syncwarp();
+  for (int c = lane; c < nc; c += 32) {
+    int64_t o = layout_off(b, c, nc);
+    if (HELM) {
+      p.mps[2 * o] = acc[2 * c];
+      p.mps[2 * o + 1] = acc[2 * c + 1];
+    } else {
+      p.mps[o] = acc[c];
+    }
+  }
+}
+
+template <typename T, bool HELM>
+int launch_p2m(const P2MParams<T>& p, cudaStream_t s) {
+  if (p.nbox <= 0) return 0;
+  const int nw = 4;
+  size_t smem = sizeof(T) * (size_t)nw * ncoef(p.N) * (HELM ? 2 : 1);
+  if (smem > 48 * 1024)
+    WBFMM_CUDA(cudaFuncSetAttribute(k_p2m<T, HELM>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem));
+  unsigned grid = (unsigned)((p.nbox + nw - 1) / nw);
+  k_p2m<T, HELM><<<grid, nw * 32, smem, s>>>(p);
+  WBFMM_CUDA(cudaGetLastError());
+  return 0;
+}
+
+// ----------------------------------------------------- translation core
+// vector length (complex entries) for order N
+template <bool HELM>
+__host__ __device__ __forceinline__ int vlen(int N) {
+  return HELM ? (N + 1) * (N + 1) : nhalf(N);
+}
+
+// load a Layout-L box vector into a shared complex vector
+template <typename T, bool HELM>
+__device__ __forceinline__ void load_vec(T* v, const T* arr, int64_t b, int N,
+                                         int nc, int lane) {
+  if (HELM) {
+    for (int c = lane; c < (N + 1) * (N + 1); c += 32) {
+      int64_t o = layout_off(b, c, nc);
+      v[2 * c] = arr[2 * o]; v[2 * c + 1] = arr[2 * o + 1];
+    }
+  } else {
+    for (int c = lane; c < nhalf(N); c += 32) {
+      int n = half_degree(c), m = c - n * (n + 1) / 2;
+      if (m == 0) {
+        v[2 * c] = arr[layout_off(b, n * n, nc)];
+        v[2 * c + 1] = T(0);
+      } else {
+        int id = lidx(n, m);
+        v[2 * c] = arr[layout_off(b, id, nc)];
+        v[2 * c + 1] = arr[layout_off(b, id + 1, nc)];
+      }
+    }
+  }
+}
+
+// out[b] (+)= v  (Layout L), all lanes of the caller cooperate
+template <typename T, bool HELM, bool ACC>
+__device__ __forceinline__ void store_vec(T* arr, int64_t b, int N, int nc,
+                                          const T* v, int tid, int nt) {
+  if (HELM) {
+    for (int c = tid; c < (N + 1) * (N + 1); c += nt) {
+      int64_t o = layout_off(b, c, nc);
+      if (ACC) { arr[2 * o] += v[2 * c]; arr[2 * o + 1] += v[2 * c + 1]; }
+      else { arr[2 * o] = v[2 * c]; arr[2 * o + 1] = v[2 * c + 1]; }
+    }
+  } else {
+    for (int c = tid; c < nhalf(N); c += nt) {
+      int n = half_degree(c), m = c - n * (n + 1) / 2;
+      if (m == 0) {
+        int64_t o = layout_off(b, n * n, nc);
+        if (ACC) arr[o] += v[2 * c]; else arr[o] = v[2 * c];
+      } else {
+        int id = lidx(n, m);
+        int64_t o0 = layout_off(b, id, nc), o1 = layout_off(b, id + 1, nc);
+        if (ACC) { arr[o0] += v[2 * c]; arr[o1] += v[2 * c + 1]; }
+        else { arr[o0] = v[2 * c]; arr[o1] = v[2 * c + 1]; }
+      }
+    }
+  }
+}
+
+// A holds the input vector (order Nin).  Runs rotate -> coaxial -> rotate
+// back for shift operator `op`; result added to (ACC) or written into out.
+// kind: Laplace coaxial kind (0 S|R, 1 S|S, 2 R|R); Helmholtz: CPLX table
+// for M2L (S|R), real for M2M/L2L.
+template <typename T, bool HELM, bool CPLX, bool ACC>
+__device__ void shift_vec(T* A, T* B, T* out, int Nin, int Nout, int op,
+                          const OpTables<T>& t, const T* coax, const T* tp,
+                          int kind, int lane) {
+  const T* H = t.H + (int64_t)t.op_ith[op] * t.hstride;
+  const T* eph = t.ph + (size_t)op * (t.lmax + 1) * 2;
+  const T* ech = t.ch + (size_t)op * (t.lmax + 1) * 2;
+  if (HELM) {
+    phase_full(A, Nin, ech, lane, 32);
+    __syncwarp();
+    hsum_full<T, T, false>(B, A, Nin, H, eph, lane, 32);
+    __syncwarp();
+    coax_full<T, T, CPLX>(A, B, Nout, Nin, coax, lane, 32);
+    __syncwarp();
+    phase_full(A, Nout, eph, lane, 32);
+    __syncwarp();
+    hsum_full<T, T, ACC>(out, A, Nout, H, ech, lane, 32);
+    __syncwarp();
+  } else {
+    phase_half(A, Nin, ech, lane, 32);
+    __syncwarp();
+    hsum_half<T, T, false>(B, A, Nin, H, eph, lane, 32);
+    __syncwarp();
+    coax_half<T, T>(A, B, Nout, Nin,
+                    kind == 0 ? t.lapSR : (kind == 1 ? t.lapSS : t.lapRR),
+                    t.lt, tp, kind, lane, 32);
+    __syncwarp();
+    phase_half(A, Nout, eph, lane, 32);
+    __syncwarp();
+    hsum_half<T, T, ACC>(out, A, Nout, H, ech, lane, 32);
+    __syncwarp();
+  }
+}
+
+// shared memory per warp: three vectors of the larger order
+template <bool HELM>
+static size_t warp_smem_bytes(int Nmax, size_t tsize) {
+  return tsize * 2 * 3 * (size_t)vlen<HELM>(Nmax);
+}
+
+// ------------------------------------------------------------------- M2L
+template <typename T, bool HELM>
+__global__ void k_m2l(XlateParams<T> p, OpTables<T> t) {
+  extern __shared__ unsigned char smraw[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nw = blockDim.x >> 5;
+  const int Ns = p.Nin, Nr = p.Nout, Lm = Ns > Nr ? Ns : Nr;
+  const int V = vlen<HELM>(Lm);
+  T* A = (T*)smraw + (size_t)warp * 6 * V;
+  T* B = A + 2 * V;
+  T* acc = B + 2 * V;
+  T* tpow = (T*)smraw + (size_t)nw * 6 * V;   // Laplace: [15][Ns+Nr+2]
+  const int tpn = Ns + Nr + 2;
+  const int64_t tb = blockIdx.x / p.nsplit;
+  const int split = blockIdx.x % p.nsplit;
+  const int outlen = vlen<HELM>(Nr);
+  for (int c = lane; c < 2 * outlen; c += 32) acc[c] = T(0);
+  if (!HELM) {
+    for (int di = threadIdx.x; di < 15; di += blockDim.x) {
+      T r = p.width * (T)sqrt((double)c_list_dist2[di]);
+      T* tp = tpow + di * tpn;
+      tp[0] = T(1);
+      for (int j = 1; j < tpn; j++) tp[j] = r * tp[j - 1];
+    }
+  }
+  __syncthreads();
+  const bool active = !(p.tmask && !p.tmask[tb]);
+  if (active) {
+    uint32_t i, j, k;
+    demorton((uint64_t)tb, &i, &j, &k);
+    const int nside = 1 << p.level;
+    int i0 = (int)(i - i % 2), j0 = (int)(j - j % 2), k0 = (int)(k - k % 2);
+    int i1 = min(i0 + 3, nside - 1), j1 = min(j0 + 3, nside - 1),
+        k1 = min(k0 + 3, nside - 1);
+    if (i0 > 0) i0 -= 2;
+    if (j0 > 0) j0 -= 2;
+    if (k0 > 0) k0 -= 2;
+    const int ni = i1 - i0 + 1, nj = j1 - j0 + 1, nk = k1 - k0 + 1;
+    const int total = ni * nj * nk;
+    const int ncs = ncoef(Ns);
+    for (int e = split * nw + warp; e < total; e += p.nsplit * nw) {
+      int ii = i0 + e / (nj * nk), jj = j0 + (e / nk) % nj, kk = k0 + e % nk;
+      int dx = ii - (int)i, dy = jj - (int)j, dz = kk - (int)k;
+      if (dx >= -1 && dx <= 1 && dy >= -1 && dy <= 1 && dz >= -1 && dz <= 1)
+        continue;
+      uint64_t s = morton((uint32_t)ii, (uint32_t)jj, (uint32_t)kk);
+      if (p.src_n && p.src_n[s] == 0) continue;
+      const int op = (dx + 3) * 49 + (dy + 3) * 7 + dz + 3;
+      const int di = t.op_dist[op];
+      load_vec<T, HELM>(A, p.cin, (int64_t)s, Ns, ncs, lane);
+      __syncwarp();
+      shift_vec<T, HELM, true, true>(A, B, acc, Ns, Nr, op, t,
+                                     HELM ? p.coax + di * p.coax_stride : nullptr,
+                                     HELM ? nullptr : tpow + di * tpn, 0, lane);
+    }
+  }
+  __syncthreads();
+  // fixed-order sum of the warps' partial results
+  const T* acc0 = (T*)smraw + 4 * V;
+  const int ncr = ncoef(Nr);
+  if (p.nsplit == 1) {
+    if (!active) return;
+    T* red = A;   // reuse warp 0's first vector as the reduction buffer
+    __syncthreads();
+    for (int c = threadIdx.x; c < 2 * outlen; c += blockDim.x) {
+      T v = acc0[c];
+      for (int w = 1; w < nw; w++) v += acc0[(size_t)w * 6 * V + c];
+      ((T*)smraw)[c] = v;
+    }
+    __syncthreads();
+    store_vec<T, HELM, true>(p.cout, tb, Nr, ncr, (T*)smraw, threadIdx.x,
+                             blockDim.x);
+    (void)red;
+  } else {
+    T* part = p.partial + ((size_t)split * p.nbox + tb) * 2 * outlen;
+    for (int c = threadIdx.x; c < 2 * outlen; c += blockDim.x) {
+      T v = acc0[c];
+      for (int w = 1; w < nw; w++) v += acc0[(size_t)w * 6 * V + c];
+      part[c] = v;
+    }
+  }
+}
+
+// adds the split partial sums, in split order, into cout
+template <typename T, bool HELM>
+__global__ void k_m2l_reduce(XlateParams<T> p) {
+  const int64_t tb = blockIdx.x;
+  if (p.tmask && !p.tmask[tb]) return;
+  extern __shared__ unsigned char smraw[];
+  T* v = (T*)smraw;
+  const int Nr = p.Nout, outlen = vlen<HELM>(Nr);
+  for (int c = threadIdx.x; c < 2 * outlen; c += blockDim.x) {
+    T s = T(0);
+    for (int sp = 0; sp < p.nsplit; sp++)
+      s += p.partial[((size_t)sp * p.nbox + tb) * 2 * outlen + c];
+    v[c] = s;
+  }
+  __syncthreads();
+  store_vec<T, HELM, true>(p.cout, tb, Nr, ncoef(Nr), v, threadIdx.x,
+                           blockDim.x);
+}
+
+static int pick_warps(size_t per_warp, size_t extra, int want) {
+  const size_t cap = 200 * 1024;
+  int nw = want;
+  while (nw > 1 && per_warp * nw + extra > cap) nw--;
+  return nw;
+}
+
+template <typename T, bool HELM>
+int launch_m2l(const XlateParams<T>& p, const OpTables<T>& t, cudaStream_t s) {
+  const int Lm = p.Nin > p.Nout ? p.Nin : p.Nout;
+  const size_t per = warp_smem_bytes<HELM>(Lm, sizeof(T));
+  const size_t extra = HELM ? 0 : sizeof(T) * 15 * (p.Nin + p.Nout + 2);
+  const int nw = pick_warps(per, extra, 4);
+  const size_t smem = per * nw + extra;
+  if (smem > 227 * 1024) return set_error(-3, "M2L: expansion order too large for shared memory");
+  WBFMM_CUDA(cudaFuncSetAttribute(k_m2l<T, HELM>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem));
+  unsigned grid = (unsigned)(p.nbox * p.nsplit);
+  k_m2l<T, HELM><<<grid, nw * 32, smem, s>>>(p, t);
+  WBFMM_CUDA(cudaGetLastError());
+  if (p.nsplit > 1) {
+    size_t rs = sizeof(T) * 2 * vlen<HELM>(p.Nout);
+    if (rs > 48 * 1024)
+      WBFMM_CUDA(cudaFuncSetAttribute(k_m2l_reduce<T, HELM>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)rs));
+    k_m2l_reduce<T, HELM><<<(unsigned)p.nbox, 256, rs, s>>>(p);
+    WBFMM_CUDA(cudaGetLastError());
+  }
+  return 0;
+}
+
+// ------------------------------------------------------------------- M2M
+// parents at `level-1` receive the shifted expansions of their children at
+// `level`; p.nbox = number of parents, p.width = child box width
+template <typename T, bool HELM>
+__global__ void k_m2m(XlateParams<T> p, OpTables<T> t) {
+  extern __shared__ unsigned char smraw[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nw = blockDim.x >> 5;
+  const int Nc = p.Nin, Np = p.Nout, Lm = Nc > Np ? Nc : Np;
+  const int V = vlen<HELM>(Lm);
+  T* A = (T*)smraw + (size_t)warp * 6 * V;
+  T* B = A + 2 * V;
+  T* acc = B + 2 * V;
+  T* tp = (T*)smraw + (size_t)nw * 6 * V;
+  const int tpn = Nc + Np + 2;
+  const int64_t P = blockIdx.x;
+  const int outlen = vlen<HELM>(Np);
+  for (int c = lane; c < 2 * outlen; c += 32) acc[c] = T(0);
+  if (!HELM && threadIdx.x == 0) {
+    T r = p.width * (T)t.op_r[kOpM2M];
+    tp[0] = T(1);
+    for (int j = 1; j < tpn; j++) tp[j] = r * tp[j - 1];
+  }
+  __syncthreads();
+  const int ncc = ncoef(Nc);
+  for (int ch = warp; ch < 8; ch += nw) {
+    int64_t c = 8 * P + ch;
+    load_vec<T, HELM>(A, p.cin, c, Nc, ncc, lane);
+    __syncwarp();
+    shift_vec<T, HELM, false, true>(A, B, acc, Nc, Np, kOpM2M + ch, t, p.coax,
+                                    tp, 1, lane);
+  }
+  __syncthreads();
+  const T* acc0 = (T*)smraw + 4 * V;
+  T* red = (T*)smraw;
+  for (int c = threadIdx.x; c < 2 * outlen; c += blockDim.x) {
+    T v = acc0[c];
+    for (int w = 1; w < nw; w++) v += acc0[(size_t)w * 6 * V + c];
+    red[c] = v;   // entries c of warp 0's A are read only by this thread
+  }
+  __syncthreads();
+  store_vec<T, HELM, false>(p.cout, P, Np, ncoef(Np), red, threadIdx.x,
+                            blockDim.x);
+}
+
+template <typename T, bool HELM>
+int launch_m2m(const XlateParams<T>& p, const OpTables<T>& t, cudaStream_t s) {
+  const int Lm = p.Nin > p.Nout ? p.Nin : p.Nout;
+  const size_t per = warp_smem_bytes<HELM>(Lm, sizeof(T));
+  const size_t extra = sizeof(T) * (p.Nin + p.Nout + 2);
+  const int nw = pick_warps(per, extra, 8);
+  const size_t smem = per * nw + extra;
+  if (smem > 227 * 1024) return set_error(-3, "M2M: expansion order too large for shared memory");
+  WBFMM_CUDA(cudaFuncSetAttribute(k_m2m<T, HELM>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem));
+  k_m2m<T, HELM><<<(unsigned)p.nbox, nw * 32, smem, s>>>(p, t);
+  WBFMM_CUDA(cudaGetLastError());
+  return 0;
+}
+
+// ------------------------------------------------------------------- L2L
+// children at `level+1` receive (overwrite) the shifted expansion of their
+// parent at `level`; p.nbox = number of parents, p.width = child width
+template <typename T, bool HELM>
+__global__ void k_l2l(XlateParams<T> p, OpTables<T> t) {
+  extern __shared__ unsigned char smraw[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nw = blockDim.x >> 5;
+  const int Np = p.Nin, Nc = p.Nout, Lm = Nc > Np ? Nc : Np;
+  const int V = vlen<HELM>(Lm);
+  T* A = (T*)smraw + (size_t)warp * 6 * V;
+  T* B = A + 2 * V;
+  T* out = B + 2 * V;
+  T* tp = (T*)smraw + (size_t)nw * 6 * V;
+  const int tpn = Nc + Np + 2;
+  const int64_t P = blockIdx.x;
+  if (!HELM && threadIdx.x == 0) {
+    T r = p.width * (T)t.op_r[kOpL2L];
+    tp[0] = T(1);
+    for (int j = 1; j < tpn; j++) tp[j] = r * tp[j - 1];
+  }
+  __syncthreads();
+  const int ncp = ncoef(Np), ncc = ncoef(Nc);
+  for (int ch = warp; ch < 8; ch += nw) {
+    load_vec<T, HELM>(A, p.cin, P, Np, ncp, lane);
+    __syncwarp();
+    shift_vec<T, HELM, false, false>(A, B, out, Np, Nc, kOpL2L + ch, t, p.coax,
+                                     tp, 2, lane);
+    store_vec<T, HELM, false>(p.cout, 8 * P + ch, Nc, ncc, out, lane, 32);
+    __syncwarp();
+  }
+}
+
+template <typename T, bool HELM>
+int launch_l2l(const XlateParams<T>& p, const OpTables<T>& t, cudaStream_t s) {
+  const int Lm = p.Nin > p.Nout ? p.Nin : p.Nout;
+  const size_t per = warp_smem_bytes<HELM>(Lm, sizeof(T));
+  const size_t extra = sizeof(T) * (p.Nin + p.Nout + 2);
+  const int nw = pick_warps(per, extra, 8);
+  const size_t smem = per * nw + extra;
+  if (smem > 227 * 1024) return set_error(-3, "L2L: expansion order too large for shared memory");
+  WBFMM_CUDA(cudaFuncSetAttribute(k_l2l<T, HELM>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem));
+  k_l2l<T, HELM><<<(unsigned)p.nbox, nw * 32, smem, s>>>(p, t);
+  WBFMM_CUDA(cudaGetLastError());
+  return 0;
+}
+
+// ------------------------------------------------------------------- L2P
+template <typename T, bool HELM>
+__global__ void k_l2p(EvalParams<T> p) {
+  const int jt = blockIdx.x * blockDim.x + threadIdx.x;
+  if (jt >= p.ntgt) return;
+  const int64_t b = p.tbox[jt];
+  double cd[3];
+  box_centre(b, p.x0, p.y0, p.z0, p.wb, cd);
+  // target position relative to the box centre, formed in FP64
+  const T xc[3] = {T(0), T(0), T(0)};
+  const T xf[3] = {(T)(p.tx[jt] - cd[0]), (T)(p.ty[jt] - cd[1]),
+                   (T)(p.tz[jt] - cd[2])};
+  const int nc = ncoef(p.N);
+  const uint32_t o = p.tperm[jt];
+  if (HELM) {
+    auto coef = [&](int idx, T* re, T* im) {
+      int64_t off = layout_off(b, idx, nc);
+      *re = p.mpr[2 * off]; *im = p.mpr[2 * off + 1];
+    };
+    if (p.pot) {
+      T fr = T(0), fi = T(0);
+      l2p_helmholtz<T>(p.N, p.k, xc, xf, coef, &fr, &fi);
+      p.pot[2 * (size_t)o] = fr; p.pot[2 * (size_t)o + 1] = fi;
+    }
+    if (p.grad) {
+      T g[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
+      l2p_helmholtz_grad<T>(p.N, p.k, xc, xf, coef, g);
+      for (int c = 0; c < 6; c++) p.grad[6 * (size_t)o + c] = g[c];
+    }
+  } else {
+    auto coef = [&](int idx) -> T { return p.mpr[layout_off(b, idx, nc)]; };
+    if (p.pot) p.pot[o] = l2p_laplace<T>(p.N, xc, xf, coef);
+    if (p.grad) {
+      T g[3] = {T(0), T(0), T(0)};
+      l2p_laplace_grad<T>(p.N, xc, xf, coef, g);
+      for (int c = 0; c < 3; c++) p.grad[3 * (size_t)o + c] = g[c];
+    }
+  }
+}
+
+template <typename T, bool HELM>
+int launch_l2p(const EvalParams<T>& p, cudaStream_t s) {
+  if (p.ntgt <= 0) return 0;
+  k_l2p<T, HELM><<<(p.ntgt + 127) / 128, 128, 0, s>>>(p);
+  WBFMM_CUDA(cudaGetLastError());
+  return 0;
+}
+
+// ------------------------------------------------------------------- P2P
+// Neumaier two-sum accumulator, used by the FP32 P2P (compensated)
+template <typename T>
+struct Acc {
+  T s = T(0), c = T(0);
+  __device__ __forceinline__ void add(T v, bool comp) {
+    if (!comp) { s += v; return; }
+    T t = s + v;
+    if (fabs(s) >= fabs(v)) c += (s - t) + v; else c += (v - t) + s;
+    s = t;
+  }
+  __device__ __forceinline__ T value() const { return s + c; }
+};
+
+template <typename T, bool HELM>
+__global__ void k_p2p(EvalParams<T> p) {
+  __shared__ uint32_t s_st[8][27], s_pref[8][28];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nw = blockDim.x >> 5;
+  const int64_t b = (int64_t)blockIdx.x * nw + warp;
+  if (b >= p.nbox) return;
+  const uint32_t tc = p.tcount[b];
+  if (tc == 0) return;
+  uint32_t bi, bj, bk;
+  demorton((uint64_t)b, &bi, &bj, &bk);
+  const int nside = 1 << p.level;
+  uint32_t cnt = 0, st = 0;
+  if (lane < 27) {
+    int ii = (int)bi + lane / 9 - 1, jj = (int)bj + (lane / 3) % 3 - 1,
+        kk = (int)bk + lane % 3 - 1;
+    if (ii >= 0 && jj >= 0 && kk >= 0 && ii < nside && jj < nside && kk < nside) {
+      uint64_t nb = morton((uint32_t)ii, (uint32_t)jj, (uint32_t)kk);
+      cnt = p.box_n[nb];
+      st = p.box_i[nb];
+    }
+  }
+  uint32_t incl = cnt;
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+  if (lane < 27) { s_st[warp][lane] = st; s_pref[warp][lane] = incl - cnt; }
+  __syncwarp();
+  const T f4pi = T(0.25 / kPi);
+  const T rc2 = T(kCutoffRadius * kCutoffRadius);
+  const bool comp = p.compensated != 0;
+  const T k = p.k;
+  for (uint32_t tt = 0; tt < tc; tt++) {
+    const uint32_t jt = p.tstart[b] + tt;
+    const double x = p.tx[jt], y = p.ty[jt], z = p.tz[jt];
+    Acc<T> a[8];
+    for (uint32_t f = lane; f < total; f += 32) {
+      int l = 0;
+      while (l < 26 && s_pref[warp][l + 1] <= f) l++;
+      const uint32_t s = s_st[warp][l] + (f - s_pref[warp][l]);
+      // separation formed in FP64, the rest in T
+      const T rx = (T)(x - p.x[s]), ry = (T)(y - p.y[s]), rz = (T)(z - p.z[s]);
+      const T r2 = rx * rx + ry * ry + rz * rz;
+      if (!(r2 > rc2)) continue;
+      const T r = sqrt(r2);
+      if (HELM) {
+        const T kr = k * r;
+        T sn, cs;
+        sincos(kr, &sn, &cs);
+        const T h0r = sn / kr, h0i = -cs / kr;
+        const T h1r = h0r / kr + h0i, h1i = h0i / kr - h0r;
+        T qr = T(0), qi = T(0);
+        if (p.q) { qr = p.q[2 * s]; qi = p.q[2 * s + 1]; }
+        if (p.pot) {
+          T fr = (h0r * qr - h0i * qi) * f4pi, fi = (h0i * qr + h0r * qi) * f4pi;
+          if (p.dip) {
+            T nr = (rx * p.nx[s] + ry * p.ny[s] + rz * p.nz[s]) / r;
+            T dr = p.dip[2 * s] * nr, di = p.dip[2 * s + 1] * nr;
+            fr -= k * (h1r * dr - h1i * di) * f4pi;
+            fi -= k * (h1r * di + h1i * dr) * f4pi;
+          }
+          a[0].add(fr, comp); a[1].add(fi, comp);
+        }
+        if (p.grad) {
+          const T ar = -k * (h1r * qr - h1i * qi) * f4pi / r;
+          const T ai = -k * (h1r * qi + h1i * qr) * f4pi / r;
+          T gr[3] = {ar * rx, ar * ry, ar * rz}, gi[3] = {ai * rx, ai * ry, ai * rz};
+          if (p.dip) {
+            const T nxs = p.nx[s], nys = p.ny[s], nzs = p.nz[s];
+            const T nr = rx * nxs + ry * nys + rz * nzs;
+            const T dpr = h0r - T(2) * h1r / kr, dpi = h0i - T(2) * h1i / kr;
+            const T dr = p.dip[2 * s], di = p.dip[2 * s + 1];
+            const T rv[3] = {rx, ry, rz}, nv[3] = {nxs, nys, nzs};
+            for (int c = 0; c < 3; c++) {
+              T ur = dpr * k * nr * rv[c] / r2 + h1r * (nv[c] / r - nr * rv[c] / (r2 * r));
+              T ui = dpi * k * nr * rv[c] / r2 + h1i * (nv[c] / r - nr * rv[c] / (r2 * r));
+              gr[c] += -k * (ur * dr - ui * di) * f4pi;
+              gi[c] += -k * (ur * di + ui * dr) * f4pi;
+            }
+          }
+          for (int c = 0; c < 3; c++) { a[2 + 2 * c].add(gr[c], comp); a[3 + 2 * c].add(gi[c], comp); }
+        }
+      } else {
+        const T q = p.q ? p.q[s] : T(0);
+        const T g = f4pi / r;
+        if (p.pot) {
+          T v = q;
+          if (p.dip) v += p.dip[s] * (rx * p.nx[s] + ry * p.ny[s] + rz * p.nz[s]) / r2;
+          a[0].add(v * g, comp);
+        }
+        if (p.grad) {
+          const T gq = -q * g / r2;
+          T gv[3] = {gq * rx, gq * ry, gq * rz};
+          if (p.dip) {
+            const T nxs = p.nx[s], nys = p.ny[s], nzs = p.nz[s];
+            const T nr = rx * nxs + ry * nys + rz * nzs;
+            const T ad = p.dip[s] * g / r2;
+            gv[0] += ad * (nxs - T(3) * nr * rx / r2);
+            gv[1] += ad * (nys - T(3) * nr * ry / r2);
+            gv[2] += ad * (nzs - T(3) * nr * rz / r2);
+          }
+          a[1].add(gv[0], comp); a[2].add(gv[1], comp); a[3].add(gv[2], comp);
+        }
+      }
+    }
+    const uint32_t o = p.tperm[jt];
+    if (HELM) {
+      if (p.pot) {
+        T v0 = warp_sum(a[0].value()), v1 = warp_sum(a[1].value());
+        if (lane == 0) { p.pot[2 * (size_t)o] += v0; p.pot[2 * (size_t)o + 1] += v1; }
+      }
+      if (p.grad) {
+        for (int c = 0; c < 6; c++) {
+          T v = warp_sum(a[2 + c].value());
+          if (lane == 0) p.grad[6 * (size_t)o + c] += v;
+        }
+      }
+    } else {
+      if (p.pot) {
+        T v = warp_sum(a[0].value());
+        if (lane == 0) p.pot[o] += v;
+      }
+      if (p.grad) {
+        for (int c = 0; c < 3; c++) {
+          T v = warp_sum(a[1 + c].value());
+          if (lane == 0) p.grad[3 * (size_t)o + c] += v;
+        }
+      }
+    }
+  }
+}
+
+template <typename T, bool HELM>
+int launch_p2p(const EvalParams<T>& p, cudaStream_t s) {
+  if (p.nbox <= 0 || p.ntgt <= 0) return 0;
+  const int nw = 8;
+  k_p2p<T, HELM><<<(unsigned)((p.nbox + nw - 1) / nw), nw * 32, 0, s>>>(p);
+  WBFMM_CUDA(cudaGetLastError());
+  return 0;
+}
+
+// ------------------------------------------------------ instantiations
+#define WBFMM_INST(T, H)                                                      \
+  template int launch_p2m<T, H>(const P2MParams<T>&, cudaStream_t);          \
+  template int launch_m2m<T, H>(const XlateParams<T>&, const OpTables<T>&,   \
+                                cudaStream_t);                               \
+  template int launch_m2l<T, H>(const XlateParams<T>&, const OpTables<T>&,   \
+                                cudaStream_t);                               \
+  template int launch_l2l<T, H>(const XlateParams<T>&, const OpTables<T>&,   \
+                                cudaStream_t);                               \
+  template int launch_l2p<T, H>(const EvalParams<T>&, cudaStream_t);         \
+  template int launch_p2p<T, H>(const EvalParams<T>&, cudaStream_t);
+WBFMM_INST(double, true)
+WBFMM_INST(double, false)
+WBFMM_INST(float, true)
+WBFMM_INST(float, false)
+
+}  // namespace wbfmm

@@ -1,0 +1,99 @@
+// Launch parameters of the FMM pass kernels (kernels.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace wbfmm {
+
+// number of shift operators: 343 list-4 offsets, 8 child->parent (M2M),
+// 8 parent->child (L2L)
+constexpr int kOpM2M = 343;
+constexpr int kOpL2L = 351;
+constexpr int kNumOps = 359;
+
+// Device tables shared by a solve (all T = coefficient precision).
+template <typename T>
+struct OpTables {
+  const T* H = nullptr;          // rotation tables, one per theta
+  int64_t hstride = 0;
+  const int* op_ith = nullptr;   // [kNumOps] theta index
+  const int* op_dist = nullptr;  // [kNumOps] list-4 distance index (0..14)
+  const T* op_r = nullptr;       // [kNumOps] distance in box widths
+  const T* ph = nullptr;         // [kNumOps][lmax+1] (cos, sin)(m ph)
+  const T* ch = nullptr;         // [kNumOps][lmax+1] (cos, sin)(m ch)
+  int lmax = 0;
+  // Laplace dense coaxial tables [n][nd][m], dimension lt+1
+  const T* lapSS = nullptr;
+  const T* lapRR = nullptr;
+  const T* lapSR = nullptr;
+  int lt = 0;
+};
+
+template <typename T>
+struct P2MParams {
+  int64_t nbox;       // boxes at the leaf level
+  int level, N;
+  double x0, y0, z0, wb;
+  T k;
+  const uint32_t* box_i;
+  const uint32_t* box_n;
+  const double* x; const double* y; const double* z;  // sorted sources
+  const T* q;         // Laplace [n]; Helmholtz [2n]; may be null
+  const T* dip;       // dipole strengths (same layout), may be null
+  const T* nx; const T* ny; const T* nz;   // sorted normals (dipoles)
+  T* mps;             // leaf level, Layout L
+};
+
+template <typename T>
+struct EvalParams {
+  int ntgt;
+  int level, N;
+  double x0, y0, z0, wb;
+  T k;
+  const double* tx; const double* ty; const double* tz;  // leaf-box order
+  const uint32_t* tperm;                   // sorted target -> original index
+  const uint32_t* tbox;                    // sorted target -> leaf box
+  const uint32_t* tstart; const uint32_t* tcount;  // per leaf box
+  const uint32_t* box_i; const uint32_t* box_n;    // source leaf ranges
+  const double* x; const double* y; const double* z;  // sorted sources
+  const T* q; const T* dip;
+  const T* nx; const T* ny; const T* nz;
+  const T* mpr;                             // leaf regular expansions
+  T* pot;    // [ntgt] or [2 ntgt] (original order), may be null
+  T* grad;   // [3 ntgt] or [6 ntgt], may be null
+  int64_t nbox;
+  int compensated;    // FP32 P2P: two-sum accumulation
+};
+
+template <typename T>
+struct XlateParams {
+  int level;          // level of the boxes that receive the result
+  int64_t nbox;       // M2L: boxes at `level`; M2M/L2L: parents
+  int Nin, Nout;      // orders of input and output expansions
+  const T* cin;       // input level array (Layout L)
+  T* cout;            // output level array (Layout L)
+  const uint32_t* src_n;   // M2L: source box counts (skip empty), or null
+  const T* coax;           // Helmholtz coaxial table(s) for this level
+  int64_t coax_stride;     // per distance (complex S|R)
+  T width;                 // box width of the translation's distance unit
+  T k;
+  int nsplit;              // M2L: CTAs per target box
+  T* partial;              // M2L split: [nsplit][nbox][2*ncout]
+  const uint8_t* tmask;    // M2L: only targets with tmask[b] != 0, or null
+};
+
+template <typename T, bool HELM>
+int launch_p2m(const P2MParams<T>& p, cudaStream_t s);
+template <typename T, bool HELM>
+int launch_m2m(const XlateParams<T>& p, const OpTables<T>& t, cudaStream_t s);
+template <typename T, bool HELM>
+int launch_m2l(const XlateParams<T>& p, const OpTables<T>& t, cudaStream_t s);
+template <typename T, bool HELM>
+int launch_l2l(const XlateParams<T>& p, const OpTables<T>& t, cudaStream_t s);
+template <typename T, bool HELM>
+int launch_l2p(const EvalParams<T>& p, cudaStream_t s);
+template <typename T, bool HELM>
+int launch_p2p(const EvalParams<T>& p, cudaStream_t s);
+
+}  // namespace wbfmm

@@ -1,0 +1,47 @@
+// Operator tables of the engine (see tables.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <vector>
+
+#include "engine.h"
+
+namespace wbfmm {
+
+struct ShiftAngles {
+  double th = 0, ph = 0, ch = 0, r = 0;  // angles and distance (unit width)
+  int ith = -1;                          // index into ShiftGeometry::thetas
+  int idist = 0;                         // |d|^2 for list-4 offsets
+};
+
+struct ShiftGeometry {
+  ShiftAngles offset[343];          // (dx+3)*49+(dy+3)*7+dz+3, d = src - tgt
+  ShiftAngles child_to_parent[8];   // M2M, unit = child width
+  ShiftAngles parent_to_child[8];   // L2L, unit = child width
+  std::vector<double> thetas;       // distinct rotation angles
+};
+
+void build_shift_geometry(ShiftGeometry* g);
+
+// H tables for every theta: rot_count(N) doubles each at stride hstride
+int generate_rotation_tables(const std::vector<double>& thetas, int N,
+                             double* dH, int64_t hstride, cudaStream_t s);
+// coaxial tables for each kr: nc=2 complex (S|R), nc=1 real (R|R)
+int generate_coaxial_tables(const std::vector<double>& krs, int L, int nc,
+                            double* dout, int64_t ostride, cudaStream_t s);
+// Laplace dense [n][nd][m] tables, n, nd, m <= Lt
+int generate_laplace_tables(int Lt, double* SS, double* RR, double* SR,
+                            cudaStream_t s);
+
+// the 15 list-4 distances |d|^2 (src/shift.c:709-723)
+static const int kListDist2[15] = {4, 5, 6, 8, 9, 10, 11, 12, 13, 14,
+                                   17, 18, 19, 22, 27};
+inline int list_dist_index(int d2) {
+  for (int i = 0; i < 15; i++)
+    if (kListDist2[i] == d2) return i;
+  return -1;
+}
+
+}  // namespace wbfmm

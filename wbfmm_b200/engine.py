@@ -1,0 +1,293 @@
+"""Python host binding of the engine's C ABI (include/wbfmm_b200.h).
+
+The binding loads ``libwbfmm_b200.so`` from this package directory and fails
+loudly if it is missing: there is no CPU fallback.  Arrays are NumPy FP64 on
+the host, or anything exposing a device pointer (``torch`` CUDA tensors,
+``int`` addresses) with ``on_device=True``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libwbfmm_b200.so")
+
+LAPLACE = 1
+HELMHOLTZ = 2
+FP64 = 0
+FP32 = 1
+POTENTIAL = 1
+GRADIENT = 2
+MAX_DEPTH = 16
+
+STATUS = {
+    0: "ok", -1: "invalid argument", -2: "point outside the tree cube",
+    -3: "expansion order unsupported", -4: "call out of sequence",
+    -5: "device allocation failed", -6: "over the device-memory budget",
+    -7: "no CUDA device",
+}
+
+
+class WbfmmError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"wbfmm_b200 error {code} ({STATUS.get(code, 'CUDA')}): {msg}")
+        self.code = code
+
+
+class Config(C.Structure):
+    _fields_ = [
+        ("problem", C.c_int), ("depth", C.c_int),
+        ("order_s", C.c_int * (MAX_DEPTH + 1)),
+        ("order_r", C.c_int * (MAX_DEPTH + 1)),
+        ("k", C.c_double), ("x0", C.c_double * 3), ("D", C.c_double),
+        ("precision", C.c_int), ("field", C.c_int), ("skip_empty", C.c_int),
+        ("managed", C.c_int),
+    ]
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH) -> C.CDLL:
+    """Load libwbfmm_b200.so; raise if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(
+            f"{path} is missing: build it with `python -m wbfmm_b200.build` "
+            "(the library has no CPU fallback)")
+    lib = C.CDLL(path)
+    vp, dp, ip = C.c_void_p, C.POINTER(C.c_double), C.c_int
+    u32p = C.POINTER(C.c_uint32)
+    sigs = {
+        "wbfmm_b200_last_error": (C.c_char_p, []),
+        "wbfmm_b200_device_count": (ip, []),
+        "wbfmm_b200_solver_create": (ip, [C.POINTER(vp), C.POINTER(Config), vp]),
+        "wbfmm_b200_solver_destroy": (ip, [vp]),
+        "wbfmm_b200_footprint": (C.c_int64, [C.POINTER(Config), C.c_int64, C.c_int64]),
+        "wbfmm_b200_set_sources": (ip, [vp, ip, vp, ip, vp, ip, ip]),
+        "wbfmm_b200_set_strengths": (ip, [vp, vp, ip, vp, ip, ip]),
+        "wbfmm_b200_set_targets": (ip, [vp, ip, vp, ip, ip]),
+        "wbfmm_b200_build_operators": (ip, [vp]),
+        "wbfmm_b200_leaf_expansions": (ip, [vp]),
+        "wbfmm_b200_upward_pass": (ip, [vp, ip]),
+        "wbfmm_b200_downward_pass": (ip, [vp, ip]),
+        "wbfmm_b200_evaluate": (ip, [vp]),
+        "wbfmm_b200_run": (ip, [vp]),
+        "wbfmm_b200_synchronize": (ip, [vp]),
+        "wbfmm_b200_get_field": (ip, [vp, vp, vp, ip]),
+        "wbfmm_b200_get_tree": (ip, [vp, u32p, u32p, u32p, ip]),
+        "wbfmm_b200_get_coefficients": (ip, [vp, ip, dp, dp]),
+        "wbfmm_b200_coefficient_pointers": (ip, [vp, ip, C.POINTER(vp), C.POINTER(vp)]),
+        "wbfmm_b200_stage_times": (ip, [vp, dp]),
+        "wbfmm_b200_kernel_launches": (C.c_int64, [vp]),
+        "wbfmm_b200_solve": (ip, [C.POINTER(Config), ip, vp, vp, vp, vp, ip, vp, vp, vp]),
+    }
+    for name, (res, args) in sigs.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        msg = load_library().wbfmm_b200_last_error().decode(errors="replace")
+        raise WbfmmError(rc, msg)
+
+
+def _addr(a):
+    """Address of a host array / device tensor / raw int pointer (or None)."""
+    if a is None:
+        return None
+    if isinstance(a, int):
+        return a
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    if hasattr(a, "data_ptr"):
+        return a.data_ptr()
+    raise TypeError(f"cannot take the address of {type(a)}")
+
+
+def _host(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+
+
+@dataclass
+class SolverConfig:
+    problem: int
+    depth: int
+    order_s: list
+    order_r: list
+    k: float = 0.0
+    x0: tuple = (0.0, 0.0, 0.0)
+    D: float = 1.0
+    precision: int = FP64
+    field: int = POTENTIAL | GRADIENT
+    skip_empty: bool = False
+    managed: bool = False
+
+    def to_c(self) -> Config:
+        c = Config()
+        c.problem = self.problem
+        c.depth = self.depth
+        for lv in range(MAX_DEPTH + 1):
+            c.order_s[lv] = int(self.order_s[lv]) if lv < len(self.order_s) else 0
+            c.order_r[lv] = int(self.order_r[lv]) if lv < len(self.order_r) else 0
+        c.k = float(self.k)
+        for i in range(3):
+            c.x0[i] = float(self.x0[i])
+        c.D = float(self.D)
+        c.precision = self.precision
+        c.field = self.field
+        c.skip_empty = int(bool(self.skip_empty))
+        c.managed = int(bool(self.managed))
+        return c
+
+    @staticmethod
+    def from_problem(p, precision=FP64, field=POTENTIAL | GRADIENT,
+                     skip_empty=False) -> "SolverConfig":
+        return SolverConfig(p.problem, p.depth, list(p.order_s), list(p.order_r),
+                            p.k, tuple(p.x0), p.D, precision, field, skip_empty)
+
+
+class Solver:
+    """One FMM solve on the GPU (see include/wbfmm_b200.h)."""
+
+    def __init__(self, cfg: SolverConfig, stream: int | None = None):
+        self.lib = load_library()
+        self.cfg = cfg
+        self._c = cfg.to_c()
+        h = C.c_void_p()
+        _check(self.lib.wbfmm_b200_solver_create(C.byref(h), C.byref(self._c), stream))
+        self.h = h
+        self.ns = self.nt = 0
+        self._keep = []
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.wbfmm_b200_solver_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_sources(self, xs, normals=None, on_device=False, xstr=3, nstr=3):
+        if not on_device:
+            xs = _host(xs).reshape(-1, 3)
+            normals = _host(normals)
+            n = xs.shape[0]
+        else:
+            n = int(xs.shape[0]) if hasattr(xs, "shape") else None
+        self._keep = [xs, normals]
+        _check(self.lib.wbfmm_b200_set_sources(self.h, n, _addr(xs), xstr,
+                                               _addr(normals), nstr, int(on_device)))
+        self.ns = n
+        return self
+
+    def set_strengths(self, q=None, dipoles=None, on_device=False):
+        w = 2 if self.cfg.problem == HELMHOLTZ else 1
+        if not on_device:
+            q = _host(q); dipoles = _host(dipoles)
+        _check(self.lib.wbfmm_b200_set_strengths(self.h, _addr(q), w, _addr(dipoles),
+                                                 w, int(on_device)))
+        return self
+
+    def set_targets(self, xt, on_device=False, tstr=3):
+        if not on_device:
+            xt = _host(xt).reshape(-1, 3)
+        n = int(xt.shape[0])
+        _check(self.lib.wbfmm_b200_set_targets(self.h, n, _addr(xt), tstr, int(on_device)))
+        self.nt = n
+        return self
+
+    def build_operators(self):
+        _check(self.lib.wbfmm_b200_build_operators(self.h))
+
+    def leaf_expansions(self):
+        _check(self.lib.wbfmm_b200_leaf_expansions(self.h))
+
+    def upward_pass(self, level):
+        _check(self.lib.wbfmm_b200_upward_pass(self.h, level))
+
+    def downward_pass(self, level):
+        _check(self.lib.wbfmm_b200_downward_pass(self.h, level))
+
+    def evaluate(self):
+        _check(self.lib.wbfmm_b200_evaluate(self.h))
+
+    def run(self):
+        _check(self.lib.wbfmm_b200_run(self.h))
+        return self
+
+    def synchronize(self):
+        _check(self.lib.wbfmm_b200_synchronize(self.h))
+
+    def field(self):
+        w = 2 if self.cfg.problem == HELMHOLTZ else 1
+        pot = np.zeros(self.nt * w) if self.cfg.field & POTENTIAL else None
+        grad = np.zeros(self.nt * 3 * w) if self.cfg.field & GRADIENT else None
+        _check(self.lib.wbfmm_b200_get_field(self.h, _addr(pot), _addr(grad), 0))
+        return pot, grad
+
+    def field_to_device(self, pot_ptr=None, grad_ptr=None):
+        _check(self.lib.wbfmm_b200_get_field(self.h, pot_ptr, grad_ptr, 1))
+
+    def tree(self, level):
+        nb = 8 ** level
+        ip = np.zeros(self.ns, dtype=np.uint32)
+        bi = np.zeros(nb, dtype=np.uint32)
+        bn = np.zeros(nb, dtype=np.uint32)
+        u32p = C.POINTER(C.c_uint32)
+        _check(self.lib.wbfmm_b200_get_tree(self.h, ip.ctypes.data_as(u32p),
+                                            bi.ctypes.data_as(u32p),
+                                            bn.ctypes.data_as(u32p), level))
+        return ip, bi, bn
+
+    def coefficients(self, level):
+        w = 2 if self.cfg.problem == HELMHOLTZ else 1
+        nb = 8 ** level
+        ms = np.zeros(nb * (self.cfg.order_s[level] + 1) ** 2 * w)
+        mr = np.zeros(nb * (self.cfg.order_r[level] + 1) ** 2 * w)
+        dp = C.POINTER(C.c_double)
+        _check(self.lib.wbfmm_b200_get_coefficients(self.h, level, ms.ctypes.data_as(dp),
+                                                    mr.ctypes.data_as(dp)))
+        return ms, mr
+
+    def stage_times(self):
+        t = np.zeros(6)
+        _check(self.lib.wbfmm_b200_stage_times(self.h, t.ctypes.data_as(C.POINTER(C.c_double))))
+        return dict(zip(["tree", "operators", "p2m", "upward", "downward", "evaluate"], t))
+
+    def kernel_launches(self) -> int:
+        return int(self.lib.wbfmm_b200_kernel_launches(self.h))
+
+
+def solve(p, precision=FP64, field=POTENTIAL | GRADIENT, skip_empty=False):
+    """Run one FMM solve of a :class:`wbfmm_b200.workloads.Problem`."""
+    cfg = SolverConfig.from_problem(p, precision, field, skip_empty)
+    with Solver(cfg) as s:
+        s.set_sources(p.xs, p.normals)
+        s.set_strengths(p.q, p.dipoles)
+        s.set_targets(p.xt)
+        s.run()
+        return s.field()
+
+
+def device_count() -> int:
+    return int(load_library().wbfmm_b200_device_count())
