@@ -1,0 +1,402 @@
+"""Benchmark: FMM points/s of the B200 engine on the Helmholtz cube workload.
+
+Workload (one step = one full FMM solve): 1,000,000 Helmholtz monopoles
+uniform in [-0.5,0.5]^3, complex N(0,1) strengths, k = 8, octree depth 6,
+per-level order p = ceil(kD + 1.8*6^(2/3)*(kD)^(1/3)) clamped to [6, 30]
+(D = box width), targets = sources (self term excluded), potential and
+gradient.  A step runs the whole solve on the GPU from device-resident
+inputs: Morton keys + radix sort + box ranges, FP64 operator tables, P2M,
+M2M, M2L, L2L, L2P, P2P.
+
+`value` is the FP32 form's points/s (sources + distinct targets per second,
+summed over GPUs); the plain FP64 form is measured in the same run and
+reported under `plain_fp64`.  `e2e` times the same solve through the C ABI
+with pinned host buffers (host->device inputs and device->host field inside
+the timed region).  Accuracy of both forms is measured against the FP64
+direct sum on 10,000 random targets.
+
+`--impl reference` times the reference's own CPU FMM (oracle/_ref, the
+unmodified reference sources) on the host cores, on a bounded sample of the
+workload (see `reference_sample`).
+
+Multi-GPU: one process per GPU (torchrun), independent replicas (weak
+scaling, no collective on the data path); the step time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "FMM points/s + p99 latency: served FP32 vs plain FP64 GPU at rel-L2 err<=1e-6"
+WORKLOAD = "helmholtz_cube_1e6_k8_depth6"
+
+
+# ---------------------------------------------------------------- helpers
+def list4_pairs(depth: int) -> list[int]:
+    """Number of (target, list-4 source) pairs per level of a dense tree."""
+    out = [0] * (depth + 1)
+    for lv in range(2, depth + 1):
+        n = 1 << lv
+        i = np.arange(n)
+        i0 = i - i % 2
+        i1 = np.minimum(i0 + 3, n - 1)
+        lo = np.where(i0 > 0, i0 - 2, i0)
+        span = i1 - lo + 1                              # parent-neighbour extent
+        near = np.minimum(i + 1, n - 1) - np.maximum(i - 1, 0) + 1
+        tot = (span[:, None, None] * span[None, :, None] * span[None, None, :]).sum()
+        nr = (near[:, None, None] * near[None, :, None] * near[None, None, :]).sum()
+        out[lv] = int(tot - nr)
+    return out
+
+
+def helm_flops_per_pair(p: int) -> int:
+    """Algorithmic FLOPs of one Helmholtz rotate/coaxial/rotate-back shift:
+    2*4*R(p) + 8*X(p), R(p) = sum (2n+1)^2, X(p) = coaxial MACs."""
+    R = (p + 1) * (2 * p + 1) * (2 * p + 3) // 3
+    X = (p + 1) ** 2 + p * (p + 1) ** 2 - p * (p + 1) * (p + 2) // 3
+    return 2 * 4 * R + 8 * X
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                self.samples.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for s in self.samples for n, v in zip(names, s[5:9])
+                          if v.strip().lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.samples)}
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return ws, rank, local
+
+
+def dist_max(x: float, ws: int) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ------------------------------------------------------- reference (CPU)
+def reference_sample(scale: int = 2, seed: int = 2):
+    """Bounded sample of the workload for the CPU reference: the same point
+    density, k, box widths and per-level orders, in a sub-cube of 1/scale^3
+    of the volume (125,000 points for scale 2, depth 6 - log2(scale))."""
+    from wbfmm_b200 import workloads as W
+    n = 1_000_000 // scale ** 3
+    depth = 6 - int(round(math.log2(scale)))
+    rng = np.random.default_rng(seed)
+    h = 0.5 / scale
+    xs = rng.uniform(-h, h, size=(n, 3))
+    q = rng.standard_normal(2 * n)
+    p = W.Problem("helmholtz_subcube", W.HELMHOLTZ, depth, [0] * (depth + 1),
+                  [0] * (depth + 1), 8.0, xs, q, xs, targets_are_sources=True)
+    p.x0, p.D = W.fit_box(xs)
+    for lv in range(1, depth + 1):
+        o = W.helmholtz_order(8.0, p.D / 2 ** lv)
+        p.order_s[lv] = p.order_r[lv] = o
+    return p
+
+
+def run_reference_step(p, nthreads):
+    from oracle.oracle_api import Reference
+    R = Reference()
+    t0 = time.perf_counter()
+    R.fmm(p.problem, p.depth, p.order_s, p.order_r, p.x0, p.D, p.xs, p.q, p.xt,
+          k=p.k, pot=True, grad=True, nthreads=nthreads)
+    return time.perf_counter() - t0
+
+
+def reference_arm(args, ws, rank):
+    if rank != 0:
+        return
+    from oracle.oracle_api import have_reference
+    cfgd = {"workload": WORKLOAD, "global_batch": 1_000_000, "seq_len": 0,
+            "parallelism": "cpu"}
+    if not have_reference():
+        print(json.dumps({"impl": "reference", "metric": METRIC,
+                          "unavailable": "oracle/_ref/libwbfmm_ref.so was not built"}))
+        return
+    # the sample shrinks when many steps are asked for, so that the whole
+    # run stays within a few minutes of CPU time
+    p = reference_sample(2 if args.steps + args.warmup <= 8 else 4)
+    nthreads = min(os.cpu_count() or 1, 16)
+    for _ in range(args.warmup):
+        run_reference_step(p, nthreads)
+    times = [run_reference_step(p, nthreads) for _ in range(max(1, args.steps))]
+    t = float(np.mean(times))
+    frac = f"1/{(1_000_000 // p.ns)}"
+    v = p.points / t
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "points/s",
+        "n_gpus": args.gpus, "steps": len(times), "warmup": args.warmup,
+        "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfgd,
+        "cpu_baseline": {"value": v, "unit": "points/s", "cores": nthreads,
+                         "kind": "reference",
+                         "sample": f"{p.ns} points in a {frac}-volume sub-cube, depth {p.depth}, "
+                                   f"orders {p.order_s[1:]}, same density/k/box widths; "
+                                   "reference FMM with M2L on GThreads (others serial)"},
+        "e2e": {"value": v, "unit": "points/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }))
+
+
+# ----------------------------------------------------------- our arm
+def our_arm(args, ws, rank, local):
+    import torch
+
+    from wbfmm_b200 import engine, workloads as W
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream(dev)
+    n = args.points
+    p = W.helmholtz_cube(n, k=8.0, depth=args.depth, seed=2 + rank)
+    field = engine.POTENTIAL | engine.GRADIENT
+    # device-resident inputs
+    xs_d = torch.from_numpy(np.ascontiguousarray(p.xs)).to(dev)
+    q_d = torch.from_numpy(np.ascontiguousarray(p.q)).to(dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def make(precision):
+        cfg = engine.SolverConfig.from_problem(p, precision, field)
+        return engine.Solver(cfg, stream=stream.cuda_stream)
+
+    def step(s):
+        s.set_sources(xs_d, on_device=True)
+        s.set_strengths(q_d, on_device=True)
+        s.set_targets(xs_d, on_device=True)
+        s.invalidate_operators()
+        s.run()
+
+    results = {}
+    for name, prec in (("fp64", engine.FP64), ("fp32", engine.FP32)):
+        s = make(prec)
+        for _ in range(args.warmup):
+            step(s)
+        torch.cuda.synchronize()
+        l0 = s.kernel_launches()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(args.steps)]
+        dist_barrier(ws)
+        torch.cuda.synchronize()
+        with ClockSampler(local) as clk:
+            for i in range(args.steps):
+                flush.zero_()                       # L2 flush between steps
+                ev[i][0].record(stream)
+                step(s)
+                ev[i][1].record(stream)
+            torch.cuda.synchronize()
+        dist_barrier(ws)
+        ms = float(np.sum([a.elapsed_time(b) for a, b in ev])) / args.steps
+        ms = dist_max(ms, ws)
+        launches = (s.kernel_launches() - l0) // args.steps
+        # per-stage split and M2L per level (separate, untimed pass)
+        stages = s.stage_times()
+        m2l_ms = {}
+        for lv in range(2, p.depth + 1):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            flush.zero_()
+            a.record(stream)
+            s.m2l(lv)
+            b.record(stream)
+            torch.cuda.synchronize()
+            m2l_ms[lv] = a.elapsed_time(b)
+        pot, grad = s.field()
+        results[name] = dict(ms=ms, launches=launches, stages=stages, m2l_ms=m2l_ms,
+                             pot=pot, grad=grad, clocks=clk.summary(), solver=s)
+
+    # e2e through the C ABI with pinned host buffers (FP32 form)
+    xs_h = torch.from_numpy(np.ascontiguousarray(p.xs)).pin_memory()
+    q_h = torch.from_numpy(np.ascontiguousarray(p.q)).pin_memory()
+    pot_h = torch.empty(2 * n, dtype=torch.float64).pin_memory()
+    grad_h = torch.empty(6 * n, dtype=torch.float64).pin_memory()
+    s = results["fp32"]["solver"]
+
+    def e2e_step():
+        s.lib.wbfmm_b200_set_sources(s.h, n, xs_h.data_ptr(), 3, None, 3, 0)
+        s.lib.wbfmm_b200_set_strengths(s.h, q_h.data_ptr(), 2, None, 2, 0)
+        s.lib.wbfmm_b200_set_targets(s.h, n, xs_h.data_ptr(), 3, 0)
+        s.invalidate_operators()
+        s.run()
+        rc = s.lib.wbfmm_b200_get_field(s.h, pot_h.data_ptr(), grad_h.data_ptr(), 0)
+        assert rc == 0
+
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    dist_barrier(ws)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        flush.zero_()
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e_s = dist_max((time.perf_counter() - t0) / args.steps, ws)
+    e2e = {"value": ws * p.points / e2e_s, "unit": "points/s",
+           "ms_per_step": e2e_s * 1e3,
+           "h2d_bytes_per_step": int(xs_h.numel() * 8 * 2 + q_h.numel() * 8),
+           "d2h_bytes_per_step": int((pot_h.numel() + grad_h.numel()) * 8)}
+
+    # accuracy vs the FP64 direct sum on 10,000 random targets
+    idx = W.subsample(102, n, 10_000)
+    dpot, dgrad = engine.direct(W.HELMHOLTZ, p.xs, p.q, p.xs[idx], k=p.k)
+    acc = {}
+    for name in ("fp64", "fp32"):
+        pot = results[name]["pot"].reshape(-1, 2)[idx].ravel()
+        grad = results[name]["grad"].reshape(-1, 6)[idx].ravel()
+        acc[name] = {
+            "pot_rel_l2": float(np.linalg.norm(pot - dpot) / np.linalg.norm(dpot)),
+            "grad_rel_l2": float(np.linalg.norm(grad - dgrad) / np.linalg.norm(dgrad)),
+            "pot_rel_max": float(np.max(np.abs(pot - dpot)) / np.max(np.abs(dpot)))}
+    f64, f32 = results["fp64"], results["fp32"]
+    acc["fp32_vs_fp64"] = {
+        "pot_rel_l2": float(np.linalg.norm(f32["pot"] - f64["pot"]) / np.linalg.norm(f64["pot"])),
+        "grad_rel_l2": float(np.linalg.norm(f32["grad"] - f64["grad"]) / np.linalg.norm(f64["grad"]))}
+
+    # roofline of the dominant kernel (M2L, FP32 form): algorithmic FLOPs of
+    # the rotate / coaxial / rotate-back shifts per launch / launch time
+    pairs = list4_pairs(p.depth)
+    lv_dom = max(f32["m2l_ms"], key=lambda lv: f32["m2l_ms"][lv])
+    flops = pairs[lv_dom] * helm_flops_per_pair(p.order_s[lv_dom])
+    achieved = flops / (f32["m2l_ms"][lv_dom] * 1e-3) / 1e12
+    peak_fp32 = 148 * 128 * 2 * 1.965e9 / 1e12
+    roofline = {"bound": "simt", "kernel": f"k_m2l<float,true> level {lv_dom}",
+                "achieved": achieved, "peak": peak_fp32, "unit": "TFLOP/s",
+                "frac": achieved / peak_fp32, "traffic": None,
+                "peak_source": "nominal FP32 SIMT peak (148 SMs x 128 FMA/clk x 1.965 GHz); "
+                               "MEASURED_PEAKS.json holds no SIMT figure",
+                "algorithmic_flops_per_launch": flops,
+                "pairs": pairs[lv_dom], "order": p.order_s[lv_dom]}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        from oracle.oracle_api import have_reference
+        if have_reference():
+            rp = reference_sample()
+            nthreads = min(os.cpu_count() or 1, 16)
+            t = run_reference_step(rp, nthreads)
+            cpu = {"value": rp.points / t, "unit": "points/s", "cores": nthreads,
+                   "kind": "reference",
+                   "sample": f"{rp.ns} points in a 1/8-volume sub-cube of the workload "
+                             f"(depth {rp.depth}, same density, k and box widths), one solve"}
+
+    v32 = ws * p.points / (f32["ms"] * 1e-3)
+    v64 = ws * p.points / (f64["ms"] * 1e-3)
+    line = {
+        "metric": METRIC, "value": v32, "unit": "points/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": f32["ms"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "global_batch": ws * p.points, "seq_len": 0,
+                   "parallelism": f"replicas{ws}", "points_per_gpu": p.points,
+                   "depth": p.depth, "orders": p.order_s[1:], "k": p.k,
+                   "l2": "256 MiB buffer written between timed steps"},
+        "plain_fp64": {"value": v64, "unit": "points/s", "ms_per_step": f64["ms"],
+                       "stages_ms": f64["stages"], "m2l_ms": f64["m2l_ms"]},
+        "fp32_over_fp64": v32 / v64,
+        "stages_ms": f32["stages"], "m2l_ms": f32["m2l_ms"],
+        "accuracy": acc,
+        "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
+        "gpu_launches": int(f32["launches"]),
+        "clocks": f32["clocks"], "clocks_fp64": f64["clocks"],
+    }
+    if rank == 0:
+        print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--points", type=int, default=1_000_000)
+    ap.add_argument("--depth", type=int, default=6)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    ws, rank, local = dist_setup()
+    try:
+        if args.impl == "reference":
+            reference_arm(args, ws, rank)
+        else:
+            our_arm(args, ws, rank, local)
+    finally:
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -105,6 +105,10 @@ int wbfmm_b200_build_operators(wbfmm_b200_solver_t *s);
 int wbfmm_b200_leaf_expansions(wbfmm_b200_solver_t *s);
 int wbfmm_b200_upward_pass(wbfmm_b200_solver_t *s, int level);
 int wbfmm_b200_downward_pass(wbfmm_b200_solver_t *s, int level);
+/* the two halves of a downward-pass level: M2L into level `level`, and L2L
+   from `level` into `level+1` (level < depth) */
+int wbfmm_b200_m2l(wbfmm_b200_solver_t *s, int level);
+int wbfmm_b200_l2l(wbfmm_b200_solver_t *s, int level);
 int wbfmm_b200_evaluate(wbfmm_b200_solver_t *s);
 /* all stages after set_sources/set_strengths/set_targets */
 int wbfmm_b200_run(wbfmm_b200_solver_t *s);
@@ -131,6 +135,20 @@ int wbfmm_b200_coefficient_pointers(wbfmm_b200_solver_t *s, int level,
 int wbfmm_b200_stage_times(wbfmm_b200_solver_t *s, double *ms6);
 /* number of kernels the solver launched since creation */
 int64_t wbfmm_b200_kernel_launches(wbfmm_b200_solver_t *s);
+
+/* Drop cached operator tables so the next stage regenerates them (tables
+   otherwise persist for the solver's lifetime, keyed by its config). */
+int wbfmm_b200_invalidate_operators(wbfmm_b200_solver_t *s);
+
+/* FP64 direct sum with self-exclusion (r <= 1e-6) and compensated
+   accumulation: the GPU counterpart of wbfmm_total_field[_grad]
+   (src/direct.c:35-294) and wbfmm_laplace_field[_grad]
+   (src/direct-laplace.c:200-336).  xs[3ns], xt[3nt]; q / dipoles as in
+   wbfmm_b200_set_strengths with unit stride; pot/grad may be NULL. */
+int wbfmm_b200_direct(int problem, double k, int ns, const double *xs,
+                      const double *q, const double *normals,
+                      const double *dipoles, int nt, const double *xt,
+                      double *pot, double *grad, int on_device);
 
 /* One call: create, build, run, copy out, destroy.  Host buffers. */
 int wbfmm_b200_solve(const wbfmm_b200_config_t *cfg, int nsrc,

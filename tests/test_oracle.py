@@ -1,0 +1,164 @@
+"""Pinning of the CPU restatement oracle (no GPU needed).
+
+The restatement (oracle/wbfmm_oracle.c) is checked bit-exactly against the
+golden fixtures made by the unmodified reference, and -- where the reference
+library is built -- against it live: Morton keys, the stable point sort
+`t->ip`, every box {i, n} (with the values the reference's refinement leaves
+in non-leaf levels), target boxes, neighbour lists and list-4 interaction
+lists with their shift indices (the structural checks of the reference's
+neighbour_test / ilist4_test, tools/wbfmm-tests.c.in:1905-2080).  The FP64
+direct sums match the reference's direct.c / direct-laplace.c.
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from oracle.oracle_api import HELMHOLTZ, LAPLACE, level_box_offsets
+from wbfmm_b200 import workloads as W
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+CASES = sorted(glob.glob(os.path.join(GOLDEN, "*.npz")))
+
+
+@pytest.mark.parametrize("path", CASES, ids=lambda x: os.path.basename(x)[:-4])
+def test_tree_matches_golden(restatement, path):
+    z = np.load(path)
+    ip, boxes = restatement.tree_build(z["x0"], float(z["D"]), int(z["depth"]), z["xs"])
+    assert np.array_equal(ip, z["ip"])
+    assert np.array_equal(boxes, z["boxes"])
+
+
+def test_tree_matches_reference_live(restatement, reference):
+    for seed, n, depth in [(5, 5000, 4), (6, 333, 3), (7, 20000, 5)]:
+        rng = np.random.default_rng(seed)
+        xs = rng.uniform(-0.5, 0.5, (n, 3))
+        # clustered points exercise empty boxes and the refinement quirks
+        xs[: n // 2] = 0.1 * xs[: n // 2] + 0.2
+        x0, D = W.fit_box(xs)
+        q = rng.standard_normal(n)
+        r = reference.fmm(LAPLACE, depth, [0] + [2] * depth, [0] + [2] * depth, x0, D,
+                          xs, q, xs[:10], pot=True, grad=False, want_tree=True)
+        ip, boxes = restatement.tree_build(x0, D, depth, xs)
+        assert np.array_equal(ip, r["ip"])
+        assert np.array_equal(boxes, r["boxes"])
+
+
+def test_point_keys_and_boxes(restatement, reference):
+    rng = np.random.default_rng(9)
+    x0 = np.array([-0.51, -0.52, -0.5])
+    D = 1.03
+    for _ in range(2000):
+        x = x0 + rng.uniform(0, D, 3)
+        assert restatement.point_index_3d(x, x0, D) == reference.point_index_3d(x, x0, D)
+        for lv in (1, 3, 6):
+            assert restatement.point_box(x0, D, lv, x) == reference.point_box(x0, D, lv, x)
+    # box faces, where the floor rule and the truncation rule can differ
+    for lv in (2, 4):
+        wb = D / 2 ** lv
+        for i in range(2 ** lv):
+            x = x0 + np.array([i * wb, 0.5 * D, 0.25 * D])
+            assert restatement.point_box(x0, D, lv, x) == reference.point_box(x0, D, lv, x)
+
+
+@pytest.mark.parametrize("level", [2, 3, 4])
+def test_neighbour_and_list4(restatement, reference, level):
+    nb = 8 ** level
+    rng = np.random.default_rng(level)
+    boxes = np.unique(np.concatenate([np.arange(min(nb, 64)), rng.integers(0, nb, 200)]))
+    for b in boxes:
+        b = int(b)
+        a = restatement.neighbours(level, b)
+        r = reference.neighbours(level, b)
+        assert np.array_equal(a, r)
+        l4 = restatement.interaction_list_4(level, b)
+        r4 = reference.interaction_list_4(level, b)
+        assert np.array_equal(l4, r4)
+        assert len(l4) <= 189
+
+
+def test_list4_structure(restatement):
+    """ilist4_test semantics: every entry non-adjacent, its parent adjacent
+    to ours, shift index = (di+3)*49+(dj+3)*7+dk+3."""
+    from wbfmm_b200.engine import HELMHOLTZ as _  # noqa: F401  (package import)
+
+    def decode(m):
+        c = [0, 0, 0]
+        for b in range(21):
+            for a in range(3):
+                c[a] |= ((m >> (3 * b + a)) & 1) << b
+        return c
+
+    level = 4
+    for b in range(0, 8 ** level, 37):
+        i = decode(b)
+        for s, sh in restatement.interaction_list_4(level, b):
+            j = decode(int(s))
+            d = [j[a] - i[a] for a in range(3)]
+            assert max(abs(x) for x in d) >= 2
+            assert max(abs((j[a] >> 1) - (i[a] >> 1)) for a in range(3)) <= 1
+            assert sh == (d[0] + 3) * 49 + (d[1] + 3) * 7 + d[2] + 3
+
+
+@pytest.mark.parametrize("problem", [LAPLACE, HELMHOLTZ])
+def test_direct_sum_matches_reference(restatement, reference, problem):
+    rng = np.random.default_rng(31)
+    xs = rng.uniform(-0.5, 0.5, (3000, 3))
+    xt = rng.uniform(-0.5, 0.5, (40, 3))
+    q = rng.standard_normal(3000 * (2 if problem == HELMHOLTZ else 1))
+    k = 5.0
+    pot, grad = restatement.direct(problem, xs, q, xt, k=k)
+    rp = reference.direct(problem, xs, q, xt, k=k, grad=False)
+    rg = reference.direct(problem, xs, q, xt, k=k, grad=True)
+    assert np.max(np.abs(pot - rp)) / np.max(np.abs(rp)) < 1e-13
+    assert np.max(np.abs(grad - rg)) / np.max(np.abs(rg)) < 1e-13
+
+
+def test_direct_sum_dipoles_match_reference(restatement, reference):
+    rng = np.random.default_rng(32)
+    xs = rng.uniform(-0.5, 0.5, (2000, 3))
+    nrm = rng.standard_normal((2000, 3))
+    nrm /= np.linalg.norm(nrm, axis=1, keepdims=True)
+    xt = rng.uniform(-0.5, 0.5, (30, 3))
+    q = rng.standard_normal(4000)
+    d = rng.standard_normal(4000)
+    pot, _ = restatement.direct(HELMHOLTZ, xs, q, xt, k=3.0, normals=nrm, dipoles=d,
+                                grad=False)
+    ref = reference.direct(HELMHOLTZ, xs, q, xt, k=3.0, normals=nrm, dipoles=d)
+    assert np.max(np.abs(pot - ref)) / np.max(np.abs(ref)) < 1e-13
+
+
+def test_dipole_gradient_by_finite_differences(restatement):
+    """Dipole gradients have no reference counterpart (the reference aborts,
+    src/local.c:259, src/direct.c:223): pin the oracle's analytic gradient
+    with central differences of the reference-supported potential."""
+    rng = np.random.default_rng(33)
+    xs = rng.uniform(-0.5, 0.5, (50, 3))
+    nrm = rng.standard_normal((50, 3))
+    nrm /= np.linalg.norm(nrm, axis=1, keepdims=True)
+    xt = rng.uniform(-0.5, 0.5, (5, 3))
+    h = 1e-5
+    for problem, w in ((HELMHOLTZ, 2), (LAPLACE, 1)):
+        q = rng.standard_normal(50 * w)
+        d = rng.standard_normal(50 * w)
+        _, g = restatement.direct(problem, xs, q, xt, k=4.0, normals=nrm, dipoles=d)
+        g = g.reshape(5, 3, w)
+        for a in range(3):
+            e = np.zeros(3); e[a] = h
+            pp, _ = restatement.direct(problem, xs, q, xt + e, k=4.0, normals=nrm,
+                                       dipoles=d, grad=False)
+            pm, _ = restatement.direct(problem, xs, q, xt - e, k=4.0, normals=nrm,
+                                       dipoles=d, grad=False)
+            fd = ((pp - pm) / (2 * h)).reshape(5, w)
+            assert np.allclose(g[:, a, :], fd, rtol=1e-5, atol=1e-6 * np.abs(fd).max())
+
+
+def test_golden_direct_sums(restatement):
+    z = np.load(os.path.join(GOLDEN, "helmholtz_small.npz"))
+    pot, grad = restatement.direct(HELMHOLTZ, z["xs"], z["q"], z["xt"][:50], k=float(z["k"]))
+    assert np.allclose(pot, z["direct_pot"][:100], rtol=0, atol=1e-12 * np.abs(pot).max())
+
+
+def test_box_offsets():
+    assert level_box_offsets(2) == [0, 1, 9, 73]

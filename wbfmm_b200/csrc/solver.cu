@@ -122,6 +122,9 @@ struct wbfmm_b200_solver {
   virtual int get_tree(uint32_t*, uint32_t*, uint32_t*, int) = 0;
   virtual int get_coefficients(int, double*, double*) = 0;
   virtual int coefficient_pointers(int, void**, void**) = 0;
+  virtual void invalidate_operators() = 0;
+  virtual int m2l(int level) = 0;
+  virtual int l2l(int level) = 0;
 };
 
 namespace wbfmm {
@@ -508,6 +511,12 @@ struct Solver : public wbfmm_b200_solver {
   }
 
   int downward(int level) override {
+    WBFMM_TRY(m2l(level));
+    if (level == depth) return 0;
+    return l2l(level);
+  }
+
+  int m2l(int level) override {
     if (level < 2 || level > depth) return set_error(WBFMM_B200_E_ARG, "downward pass level must be in [2, depth]");
     WBFMM_TRY(build_operators());
     if (level == 2)
@@ -533,10 +542,13 @@ struct Solver : public wbfmm_b200_solver {
       x.partial = partial.p;
     }
     launches += nsplit > 1 ? 2 : 1;
-    int rc = helm ? launch_m2l<T, true>(x, tables, stream)
-                  : launch_m2l<T, false>(x, tables, stream);
-    if (rc) return rc;
-    if (level == depth) return 0;
+    return helm ? launch_m2l<T, true>(x, tables, stream)
+                : launch_m2l<T, false>(x, tables, stream);
+  }
+
+  int l2l(int level) override {
+    if (level < 2 || level >= depth) return set_error(WBFMM_B200_E_ARG, "L2L level must be in [2, depth-1]");
+    WBFMM_TRY(build_operators());
     XlateParams<T> d = xparams();
     d.level = level + 1;
     d.nbox = (int64_t)1 << (3 * level);
@@ -653,6 +665,8 @@ struct Solver : public wbfmm_b200_solver {
     return 0;
   }
 
+  void invalidate_operators() override { ops_ready = false; }
+
   int coefficient_pointers(int level, void** ms, void** mr) override {
     if (level < 1 || level > depth) return set_error(WBFMM_B200_E_ARG, "bad level");
     if (ms) *ms = mps[level].p;
@@ -746,6 +760,8 @@ int wbfmm_b200_build_operators(wbfmm_b200_solver_t* s) { SOLVER_CALL(s->build_op
 int wbfmm_b200_leaf_expansions(wbfmm_b200_solver_t* s) { SOLVER_CALL(s->leaf_expansions()); }
 int wbfmm_b200_upward_pass(wbfmm_b200_solver_t* s, int level) { SOLVER_CALL(s->upward(level)); }
 int wbfmm_b200_downward_pass(wbfmm_b200_solver_t* s, int level) { SOLVER_CALL(s->downward(level)); }
+int wbfmm_b200_m2l(wbfmm_b200_solver_t* s, int level) { SOLVER_CALL(s->m2l(level)); }
+int wbfmm_b200_l2l(wbfmm_b200_solver_t* s, int level) { SOLVER_CALL(s->l2l(level)); }
 int wbfmm_b200_evaluate(wbfmm_b200_solver_t* s) { SOLVER_CALL(s->evaluate()); }
 int wbfmm_b200_run(wbfmm_b200_solver_t* s) { SOLVER_CALL(s->run()); }
 int wbfmm_b200_synchronize(wbfmm_b200_solver_t* s) {
@@ -768,6 +784,11 @@ int wbfmm_b200_get_coefficients(wbfmm_b200_solver_t* s, int level, double* ms,
 int wbfmm_b200_coefficient_pointers(wbfmm_b200_solver_t* s, int level,
                                     void** ms, void** mr) {
   SOLVER_CALL(s->coefficient_pointers(level, ms, mr));
+}
+int wbfmm_b200_invalidate_operators(wbfmm_b200_solver_t* s) {
+  if (!s) return set_error(WBFMM_B200_E_ARG, "null solver");
+  s->invalidate_operators();
+  return 0;
 }
 int wbfmm_b200_stage_times(wbfmm_b200_solver_t* s, double* ms6) {
   if (!s || !ms6) return set_error(WBFMM_B200_E_ARG, "null argument");

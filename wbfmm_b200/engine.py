@@ -87,6 +87,10 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "wbfmm_b200_stage_times": (ip, [vp, dp]),
         "wbfmm_b200_kernel_launches": (C.c_int64, [vp]),
         "wbfmm_b200_solve": (ip, [C.POINTER(Config), ip, vp, vp, vp, vp, ip, vp, vp, vp]),
+        "wbfmm_b200_invalidate_operators": (ip, [vp]),
+        "wbfmm_b200_m2l": (ip, [vp, ip]),
+        "wbfmm_b200_l2l": (ip, [vp, ip]),
+        "wbfmm_b200_direct": (ip, [ip, C.c_double, ip, vp, vp, vp, vp, ip, vp, vp, vp, ip]),
     }
     for name, (res, args) in sigs.items():
         f = getattr(lib, name)
@@ -228,6 +232,12 @@ class Solver:
     def downward_pass(self, level):
         _check(self.lib.wbfmm_b200_downward_pass(self.h, level))
 
+    def m2l(self, level):
+        _check(self.lib.wbfmm_b200_m2l(self.h, level))
+
+    def l2l(self, level):
+        _check(self.lib.wbfmm_b200_l2l(self.h, level))
+
     def evaluate(self):
         _check(self.lib.wbfmm_b200_evaluate(self.h))
 
@@ -269,6 +279,9 @@ class Solver:
                                                     mr.ctypes.data_as(dp)))
         return ms, mr
 
+    def invalidate_operators(self):
+        _check(self.lib.wbfmm_b200_invalidate_operators(self.h))
+
     def stage_times(self):
         t = np.zeros(6)
         _check(self.lib.wbfmm_b200_stage_times(self.h, t.ctypes.data_as(C.POINTER(C.c_double))))
@@ -287,6 +300,21 @@ def solve(p, precision=FP64, field=POTENTIAL | GRADIENT, skip_empty=False):
         s.set_targets(p.xt)
         s.run()
         return s.field()
+
+
+def direct(problem, xs, q, xt, k=0.0, normals=None, dipoles=None, pot=True,
+           grad=True):
+    """FP64 direct sum on the GPU (self-excluding), host arrays."""
+    lib = load_library()
+    xs = _host(xs).reshape(-1, 3); xt = _host(xt).reshape(-1, 3)
+    q = _host(q); normals = _host(normals); dipoles = _host(dipoles)
+    w = 2 if problem == HELMHOLTZ else 1
+    po = np.zeros(xt.shape[0] * w) if pot else None
+    go = np.zeros(xt.shape[0] * 3 * w) if grad else None
+    _check(lib.wbfmm_b200_direct(problem, float(k), xs.shape[0], _addr(xs), _addr(q),
+                                 _addr(normals), _addr(dipoles), xt.shape[0], _addr(xt),
+                                 _addr(po), _addr(go), 0))
+    return po, go
 
 
 def device_count() -> int:
