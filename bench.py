@@ -221,7 +221,8 @@ def our_arm(args, ws, rank, local):
 
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    stream = torch.cuda.current_stream(dev)
+    stream = torch.cuda.Stream(dev)     # the solvers' stream; events on it
+    torch.cuda.set_stream(stream)
     n = args.points
     p = W.helmholtz_cube(n, k=8.0, depth=args.depth, seed=2 + rank)
     field = engine.POTENTIAL | engine.GRADIENT

@@ -140,6 +140,12 @@ int64_t wbfmm_b200_kernel_launches(wbfmm_b200_solver_t *s);
    otherwise persist for the solver's lifetime, keyed by its config). */
 int wbfmm_b200_invalidate_operators(wbfmm_b200_solver_t *s);
 
+/* M2L kernel selection: 1 (default) = lane-per-pair kernel for the orders it
+   is instantiated for (Helmholtz <= 8, Laplace <= 12, equal singular and
+   regular orders), generic warp kernel otherwise; 0 = always the generic
+   warp kernel. */
+int wbfmm_b200_set_m2l_kernel(wbfmm_b200_solver_t *s, int lanes);
+
 /* FP64 direct sum with self-exclusion (r <= 1e-6) and compensated
    accumulation: the GPU counterpart of wbfmm_total_field[_grad]
    (src/direct.c:35-294) and wbfmm_laplace_field[_grad]

@@ -164,3 +164,25 @@ def test_domain_error(gpu_lib):
         with pytest.raises(engine.WbfmmError) as e:
             s.set_sources(xs)
         assert e.value.code == -2
+
+
+@pytest.mark.parametrize("name,precision", [("laplace", engine.FP64), ("helmholtz", engine.FP64),
+                                            ("laplace", engine.FP32), ("helmholtz", engine.FP32)])
+def test_m2l_lane_kernel_matches_generic(gpu_lib, name, precision):
+    """The lane-per-pair M2L and the generic warp M2L compute the same
+    translations (orders 2..8 cover both kernels' ranges here)."""
+    if name == "laplace":
+        p = W.laplace_cube(20000, 3000, depth=5, order=7, seed=41)
+    else:
+        p = W.helmholtz_cube(20000, k=6.0, depth=5, seed=42)
+        p.xt = p.xt[:3000]
+    outs = []
+    for lanes in (True, False):
+        cfg = engine.SolverConfig.from_problem(p, precision)
+        with engine.Solver(cfg) as s:
+            s.set_m2l_kernel(lanes)
+            s.set_sources(p.xs).set_strengths(p.q).set_targets(p.xt).run()
+            outs.append(s.field())
+    tol = 1e-12 if precision == engine.FP64 else 1e-5
+    for a, b in zip(outs[0], outs[1]):
+        assert rel_l2(a, b) < tol

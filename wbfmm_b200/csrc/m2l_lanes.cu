@@ -1,0 +1,546 @@
+// M2L, lane-per-pair form for expansion orders known at compile time.
+//
+// The list-4 interactions of a level are regrouped by target child type tau
+// (the target's position inside its parent): all targets of one type see
+// the same 189 offsets d = source - target (src/indexing.c:330-377), each
+// with one rotate / coaxial / rotate-back operator.  A CTA takes 128 target
+// parents of one type; its 4 warps x 32 lanes each own one target.  The CTA
+// walks the 189 offsets in a fixed order; for each it stages the offset's
+// operator in shared memory (rotation block H_n^{nu,m}(theta) for n <= P,
+// the phases e^{i m ph}, e^{i m ch}, and the coaxial coefficients), and every
+// lane applies it to its own source vector (shared-memory broadcast of the
+// operator, per-lane vectors).  Degree and order loops are unrolled for the
+// compile-time order P, so each lane's inner work is straight-line FMA code.
+//
+// Sources are read from a transposed copy of the level's singular
+// expansions: per child type, per coefficient, a parent grid padded by one
+// empty parent on every side (so list-4 sources outside the domain read
+// zeros, exactly the reference's clipping), consecutive lanes reading
+// consecutive parents.
+#include <cuda_runtime.h>
+
+#include "engine.h"
+#include "kernels.h"
+#include "m2l_lanes.h"
+#include "translate.cuh"
+
+namespace wbfmm {
+
+template <typename T> struct V2t;
+template <> struct V2t<float> { typedef float2 t; };
+template <> struct V2t<double> { typedef double2 t; };
+
+// per target type: 189 packed offsets (op | sigma << 9 | (dx+1) << 12 |
+// (dy+1) << 14 | (dz+1) << 16), dx.. = parent offset of the source
+__constant__ int c_offsets[8][189];
+static bool g_offsets_ready[64] = {false};
+
+static void build_offset_table(int* tab) {
+  for (int tau = 0; tau < 8; tau++) {
+    int ta[3] = {tau & 1, (tau >> 1) & 1, (tau >> 2) & 1};
+    int j = 0;
+    for (int dx = -2 - ta[0]; dx <= 3 - ta[0]; dx++)
+      for (int dy = -2 - ta[1]; dy <= 3 - ta[1]; dy++)
+        for (int dz = -2 - ta[2]; dz <= 3 - ta[2]; dz++) {
+          if (dx >= -1 && dx <= 1 && dy >= -1 && dy <= 1 && dz >= -1 && dz <= 1)
+            continue;
+          int d[3] = {dx, dy, dz}, sg = 0, Dl[3];
+          for (int a = 0; a < 3; a++) {
+            int s = ta[a] + d[a];
+            sg |= (s & 1) << a;
+            Dl[a] = s >> 1;   // floor division (s in [-2, 4])
+          }
+          int op = (dx + 3) * 49 + (dy + 3) * 7 + dz + 3;
+          tab[tau * 189 + j] = op | (sg << 9) | ((Dl[0] + 1) << 12) |
+                               ((Dl[1] + 1) << 14) | ((Dl[2] + 1) << 16);
+          j++;
+        }
+  }
+}
+
+static int ensure_offsets() {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 64 && g_offsets_ready[dev]) return 0;
+  int tab[8 * 189];
+  build_offset_table(tab);
+  WBFMM_CUDA(cudaMemcpyToSymbol(c_offsets, tab, sizeof(tab)));
+  if (dev < 64) g_offsets_ready[dev] = true;
+  return 0;
+}
+
+// ----------------------------------------------------------- transpose
+// Layout L level array -> lin[tau][c][pp] (complex), pp on the padded
+// parent grid (nx+2)^3; the halo must be zero beforehand
+template <typename T, bool HELM>
+__global__ void k_to_lin(const T* __restrict__ arr, int level, int N,
+                         typename V2t<T>::t* __restrict__ lin) {
+  typedef typename V2t<T>::t T2;
+  const int V = HELM ? (N + 1) * (N + 1) : (N + 1) * (N + 2) / 2;
+  const int nc = (N + 1) * (N + 1);
+  const int nx = 1 << (level - 1), npx = nx + 2;
+  const int64_t npp = (int64_t)npx * npx * npx;
+  const int64_t np = (int64_t)nx * nx * nx;
+  int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= np * V * 8) return;
+  const int tau = (int)(e & 7);
+  const int c = (int)((e >> 3) % V);
+  const int64_t P = (e >> 3) / V;        // parent Morton index
+  uint32_t px, py, pz;
+  demorton((uint64_t)P, &px, &py, &pz);
+  const int64_t pp = (px + 1) + npx * ((int64_t)(py + 1) + npx * (int64_t)(pz + 1));
+  const int64_t b = (P << 3) | tau;
+  T2 v;
+  if (HELM) {
+    int64_t o = layout_off(b, c, nc);
+    v.x = arr[2 * o]; v.y = arr[2 * o + 1];
+  } else {
+    int n = half_degree(c), m = c - n * (n + 1) / 2;
+    if (m == 0) {
+      v.x = arr[layout_off(b, n * n, nc)]; v.y = T(0);
+    } else {
+      int id = lidx(n, m);
+      v.x = arr[layout_off(b, id, nc)]; v.y = arr[layout_off(b, id + 1, nc)];
+    }
+  }
+  lin[((int64_t)tau * V + c) * npp + pp] = v;
+}
+
+// --------------------------------------------------------------- kernel
+// compiler-only memory fence: keeps the unrolled per-degree blocks from
+// being hoisted into one another (bounds register live ranges)
+__device__ __forceinline__ void cfence() { asm volatile("" ::: "memory"); }
+
+template <typename T2, typename T>
+__device__ __forceinline__ T2 cm(T2 a, T er, T ei) {
+  T2 r;
+  r.x = a.x * er - a.y * ei;
+  r.y = a.x * ei + a.y * er;
+  return r;
+}
+
+
+template <int P>
+struct LaneDims {
+  static constexpr int VF = (P + 1) * (P + 1);                 // full vector
+  static constexpr int VH = (P + 1) * (P + 2) / 2;             // half vector
+  static constexpr int NH = (P + 1) * (P + 2) * (4 * P + 3) / 6;  // H, n <= P
+  static constexpr int NC = (P + 1) * (P + 2) * (P + 3) / 6;   // coaxial
+  static constexpr int NL = (P + 1) * (P + 1) * (P + 1);       // Laplace S|R
+};
+
+// shared memory layout, in units of T: [H: NH][eph: 2(P+1)][ech: 2(P+1)]
+// [coax: Helmholtz 2 NC | Laplace NL] then per warp two vector columns; as
+// many warps (<= 4) as fit in 200 KB
+template <typename T, bool HELM, int P>
+struct LaneSmem {
+  static constexpr size_t col_bytes =
+      2 * sizeof(T) * 2 * (size_t)(HELM ? LaneDims<P>::VF : LaneDims<P>::VH) * 32;
+  static constexpr int W = col_bytes * 4 <= 200 * 1024 ? 4
+                         : col_bytes * 2 <= 200 * 1024 ? 2 : 1;
+  static constexpr int CTA = 32 * W;
+  static constexpr int off_eph = LaneDims<P>::NH;
+  static constexpr int off_ech = off_eph + 2 * (P + 1);
+  static constexpr int off_cx = off_ech + 2 * (P + 1);
+  static constexpr int ops = off_cx + (HELM ? 2 * LaneDims<P>::NC : LaneDims<P>::NL);
+  static constexpr int ops_pad = (ops + 3) & ~3;
+  static constexpr int V = HELM ? LaneDims<P>::VF : LaneDims<P>::VH;
+  // two per-lane columns (working vector, accumulator) per warp, T2 each
+  static constexpr size_t bytes = sizeof(T) * (size_t)ops_pad + col_bytes * W;
+};
+
+template <typename T, bool HELM, int P>
+__global__ void __launch_bounds__(LaneSmem<T, HELM, P>::CTA)
+k_m2l_lanes(LanesParams<T> p, OpTables<T> t) {
+  typedef typename V2t<T>::t T2;
+  typedef LaneSmem<T, HELM, P> SM;
+  constexpr int kLanesCTA = SM::CTA;
+  constexpr int V = SM::V;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* ops = (T*)smraw;
+  const T* sH = ops;
+  const T* seph = ops + SM::off_eph;
+  const T* sech = ops + SM::off_ech;
+  const T* scx = ops + SM::off_cx;
+  T2* cols = (T2*)(ops + SM::ops_pad);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  T2* w = cols + (size_t)warp * 2 * V * 32 + lane;   // working vector, stride 32
+  T2* acc = w + (size_t)V * 32;                      // accumulator, stride 32
+
+  const int tau = blockIdx.y;
+  const int split = blockIdx.z;
+  const int nx = 1 << (p.level - 1), npx = nx + 2;
+  const int64_t npp = (int64_t)npx * npx * npx;
+  const int64_t np = (int64_t)nx * nx * nx;
+  const int64_t plin = (int64_t)blockIdx.x * kLanesCTA + threadIdx.x;
+  bool active = plin < np;
+  int64_t pp = 0, pmort = 0;
+  if (active) {
+    int px = (int)(plin % nx), py = (int)((plin / nx) % nx), pz = (int)(plin / ((int64_t)nx * nx));
+    pp = (px + 1) + npx * ((int64_t)(py + 1) + npx * (int64_t)(pz + 1));
+    pmort = (int64_t)morton(px, py, pz);
+    if (p.tmask && !p.tmask[(pmort << 3) | tau]) active = false;
+  }
+#pragma unroll 1
+  for (int c = 0; c < V; c++) { T2 z; z.x = T(0); z.y = T(0); acc[c * 32] = z; }
+
+  const int nH = LaneDims<P>::NH;
+#pragma unroll 1
+  for (int j = split; j < 189; j += p.nsplit) {
+    const int code = c_offsets[tau][j];
+    const int op = code & 511, sg = (code >> 9) & 7;
+    const int ddx = ((code >> 12) & 3) - 1, ddy = ((code >> 14) & 3) - 1,
+              ddz = ((code >> 16) & 3) - 1;
+    __syncthreads();   // previous operator no longer in use
+    {
+      const T* H = t.H + (int64_t)t.op_ith[op] * t.hstride;
+      for (int i = threadIdx.x; i < nH; i += kLanesCTA) ops[i] = H[i];
+      const T* eph = t.ph + (size_t)op * (t.lmax + 1) * 2;
+      const T* ech = t.ch + (size_t)op * (t.lmax + 1) * 2;
+      for (int i = threadIdx.x; i < 2 * (P + 1); i += kLanesCTA) {
+        ops[SM::off_eph + i] = eph[i];
+        ops[SM::off_ech + i] = ech[i];
+      }
+      if (HELM) {
+        const T* cx = p.coax + (int64_t)t.op_dist[op] * p.coax_stride;
+        for (int i = threadIdx.x; i < 2 * LaneDims<P>::NC; i += kLanesCTA)
+          ops[SM::off_cx + i] = cx[i];
+      } else {
+        // S|R(n,nd,m) / t^{n+nd+1}, t = width * |d|
+        const T r = p.width * t.op_r[op];
+        const T rinv = T(1) / r;
+        const int Dm = t.lt + 1;
+        for (int i = threadIdx.x; i < LaneDims<P>::NL; i += kLanesCTA) {
+          int m = i % (P + 1), nd = (i / (P + 1)) % (P + 1), n = i / ((P + 1) * (P + 1));
+          T v = t.lapSR[((int64_t)n * Dm + nd) * Dm + m];
+          T s = rinv;
+          for (int e = 0; e < n + nd; e++) s *= rinv;
+          ops[SM::off_cx + i] = v * s;
+        }
+      }
+    }
+    __syncthreads();
+    if (!active) continue;
+    const T2* src = (const T2*)p.lin_raw + (int64_t)sg * V * npp + pp + ddx +
+                    npx * ((int64_t)ddy + npx * (int64_t)ddz);
+    if (HELM) {
+      // stage A: copy the source into the lane's column with e^{i m ch}
+#pragma unroll
+      for (int n = 0; n <= P; n++) {
+#pragma unroll
+        for (int m = -n; m <= n; m++) {
+          const int am = m < 0 ? -m : m;
+          T2 v = __ldg(src + (int64_t)cidx(n, m) * npp);
+          w[cidx(n, m) * 32] = cm(v, sech[2 * am], m < 0 ? -sech[2 * am + 1] : sech[2 * am + 1]);
+        }
+        cfence();
+      }
+      // stage B: forward rotation per degree, in place, then e^{-i nu ph}
+#pragma unroll
+      for (int n = 0; n <= P; n++) {
+        T2 in[2 * P + 1];
+#pragma unroll
+        for (int m = -n; m <= n; m++) in[m + n] = w[cidx(n, m) * 32];
+        const int hb = rot_idx(-n, 0, n);
+#pragma unroll
+        for (int nu = -n; nu <= n; nu++) {
+          T sr = T(0), si = T(0);
+#pragma unroll
+          for (int m = -n; m <= n; m++) {
+            const T h = m >= 0 ? sH[hb + (nu + n) * (n + 1) + m]
+                               : sH[hb + (-nu + n) * (n + 1) - m];
+            sr += h * in[m + n].x;
+            si += h * in[m + n].y;
+          }
+          const int an = nu < 0 ? -nu : nu;
+          T2 o; o.x = sr; o.y = si;
+          w[cidx(n, nu) * 32] = cm(o, seph[2 * an], nu < 0 ? seph[2 * an + 1] : -seph[2 * an + 1]);
+        }
+        cfence();
+      }
+      // stage C: coaxial (S|R) per order m, in place, then e^{i m ph}
+#pragma unroll
+      for (int m = -P; m <= P; m++) {
+        const int am = m < 0 ? -m : m;
+        T2 tv[P + 1];
+#pragma unroll
+        for (int l = am; l <= P; l++) tv[l] = w[cidx(l, m) * 32];
+#pragma unroll
+        for (int n = am; n <= P; n++) {
+          T sr = T(0), si = T(0);
+#pragma unroll
+          for (int l = am; l <= P; l++) {
+            const int ic = l >= n ? coax_idx(l, am, n) : coax_idx(n, am, l);
+            const T sgn = (l >= n || ((n + l) & 1) == 0) ? T(1) : T(-1);
+            const T cr = sgn * scx[2 * ic], ci = sgn * scx[2 * ic + 1];
+            sr += cr * tv[l].x - ci * tv[l].y;
+            si += ci * tv[l].x + cr * tv[l].y;
+          }
+          T2 o; o.x = sr; o.y = si;
+          w[cidx(n, m) * 32] = cm(o, seph[2 * am], m < 0 ? -seph[2 * am + 1] : seph[2 * am + 1]);
+        }
+        cfence();
+      }
+      // stage D: back rotation, acc[n,nu] += e^{-i nu ch} sum_m H w[n,m]
+#pragma unroll
+      for (int n = 0; n <= P; n++) {
+        T2 in[2 * P + 1];
+#pragma unroll
+        for (int m = -n; m <= n; m++) in[m + n] = w[cidx(n, m) * 32];
+        const int hb = rot_idx(-n, 0, n);
+#pragma unroll
+        for (int nu = -n; nu <= n; nu++) {
+          T sr = T(0), si = T(0);
+#pragma unroll
+          for (int m = -n; m <= n; m++) {
+            const T h = m >= 0 ? sH[hb + (nu + n) * (n + 1) + m]
+                               : sH[hb + (-nu + n) * (n + 1) - m];
+            sr += h * in[m + n].x;
+            si += h * in[m + n].y;
+          }
+          const int an = nu < 0 ? -nu : nu;
+          T2 o; o.x = sr; o.y = si;
+          o = cm(o, sech[2 * an], nu < 0 ? sech[2 * an + 1] : -sech[2 * an + 1]);
+          T2 a = acc[cidx(n, nu) * 32];
+          a.x += o.x; a.y += o.y;
+          acc[cidx(n, nu) * 32] = a;
+        }
+        cfence();
+      }
+    } else {
+      // Laplace, half vectors (m >= 0; negative m are conjugates)
+#pragma unroll
+      for (int n = 0; n <= P; n++) {
+#pragma unroll
+        for (int m = 0; m <= n; m++) {
+          T2 v = __ldg(src + (int64_t)hidx(n, m) * npp);
+          w[hidx(n, m) * 32] = cm(v, sech[2 * m], sech[2 * m + 1]);
+        }
+        cfence();
+      }
+#pragma unroll
+      for (int n = 0; n <= P; n++) {
+        T2 in[P + 1];
+#pragma unroll
+        for (int m = 0; m <= n; m++) in[m] = w[hidx(n, m) * 32];
+        const int hb = rot_idx(-n, 0, n);
+#pragma unroll
+        for (int nu = 0; nu <= n; nu++) {
+          T tr = sH[hb + (nu + n) * (n + 1)] * in[0].x, ti = T(0);
+#pragma unroll
+          for (int m = 1; m <= n; m++) {
+            const T hp = sH[hb + (nu + n) * (n + 1) + m];
+            const T hm = sH[hb + (-nu + n) * (n + 1) + m];
+            tr += (hp + hm) * in[m].x;
+            ti += (hp - hm) * in[m].y;
+          }
+          const T er = seph[2 * nu], ei = seph[2 * nu + 1];
+          T2 o;
+          o.x = er * tr + ei * ti;
+          o.y = nu == 0 ? T(0) : er * ti - ei * tr;
+          w[hidx(n, nu) * 32] = o;
+        }
+        cfence();
+      }
+#pragma unroll
+      for (int m = 0; m <= P; m++) {
+        T2 tv[P + 1];
+#pragma unroll
+        for (int nd = m; nd <= P; nd++) tv[nd] = w[hidx(nd, m) * 32];
+#pragma unroll
+        for (int n = m; n <= P; n++) {
+          T sr = T(0), si = T(0);
+#pragma unroll
+          for (int nd = m; nd <= P; nd++) {
+            const T c = scx[(n * (P + 1) + nd) * (P + 1) + m];
+            sr += c * tv[nd].x;
+            si += c * tv[nd].y;
+          }
+          if (m == 0) si = T(0);
+          T2 o; o.x = sr; o.y = si;
+          w[hidx(n, m) * 32] = cm(o, seph[2 * m], seph[2 * m + 1]);
+        }
+        cfence();
+      }
+#pragma unroll
+      for (int n = 0; n <= P; n++) {
+        T2 in[P + 1];
+#pragma unroll
+        for (int m = 0; m <= n; m++) in[m] = w[hidx(n, m) * 32];
+        const int hb = rot_idx(-n, 0, n);
+#pragma unroll
+        for (int nu = 0; nu <= n; nu++) {
+          T tr = sH[hb + (nu + n) * (n + 1)] * in[0].x, ti = T(0);
+#pragma unroll
+          for (int m = 1; m <= n; m++) {
+            const T hp = sH[hb + (nu + n) * (n + 1) + m];
+            const T hm = sH[hb + (-nu + n) * (n + 1) + m];
+            tr += (hp + hm) * in[m].x;
+            ti += (hp - hm) * in[m].y;
+          }
+          const T er = sech[2 * nu], ei = sech[2 * nu + 1];
+          T2 a = acc[hidx(n, nu) * 32];
+          a.x += er * tr + ei * ti;
+          if (nu != 0) a.y += er * ti - ei * tr;
+          acc[hidx(n, nu) * 32] = a;
+        }
+        cfence();
+      }
+    }
+  }
+  if (!active) return;
+  const int nc = (P + 1) * (P + 1);
+  const int64_t b = (pmort << 3) | tau;
+  if (p.nsplit == 1) {
+    if (HELM) {
+      for (int c = 0; c < V; c++) {
+        T2 a = acc[c * 32];
+        int64_t o = layout_off(b, c, nc);
+        p.cout[2 * o] += a.x;
+        p.cout[2 * o + 1] += a.y;
+      }
+    } else {
+      for (int c = 0; c < V; c++) {
+        T2 a = acc[c * 32];
+        int n = half_degree(c), m = c - n * (n + 1) / 2;
+        if (m == 0) {
+          p.cout[layout_off(b, n * n, nc)] += a.x;
+        } else {
+          int id = lidx(n, m);
+          p.cout[layout_off(b, id, nc)] += a.x;
+          p.cout[layout_off(b, id + 1, nc)] += a.y;
+        }
+      }
+    }
+  } else {
+    T2* part = (T2*)p.partial_raw + ((int64_t)split * 8 + tau) * V * np + plin;
+    for (int c = 0; c < V; c++) part[(int64_t)c * np] = acc[c * 32];
+  }
+}
+
+// sum the split partials (split order) into the Layout L output
+template <typename T, bool HELM>
+__global__ void k_lanes_reduce(LanesParams<T> p, int N) {
+  typedef typename V2t<T>::t T2;
+  const int V = HELM ? (N + 1) * (N + 1) : (N + 1) * (N + 2) / 2;
+  const int nc = (N + 1) * (N + 1);
+  const int nx = 1 << (p.level - 1);
+  const int64_t np = (int64_t)nx * nx * nx;
+  int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= np * 8 * V) return;
+  const int64_t plin = e % np;
+  const int c = (int)((e / np) % V);
+  const int tau = (int)(e / (np * V));
+  int px = (int)(plin % nx), py = (int)((plin / nx) % nx), pz = (int)(plin / ((int64_t)nx * nx));
+  const int64_t b = ((int64_t)morton(px, py, pz) << 3) | tau;
+  if (p.tmask && !p.tmask[b]) return;
+  T sx = T(0), sy = T(0);
+  for (int s = 0; s < p.nsplit; s++) {
+    T2 v = ((const T2*)p.partial_raw)[(((int64_t)s * 8 + tau) * V + c) * np + plin];
+    sx += v.x; sy += v.y;
+  }
+  if (HELM) {
+    int64_t o = layout_off(b, c, nc);
+    p.cout[2 * o] += sx; p.cout[2 * o + 1] += sy;
+  } else {
+    int n = half_degree(c), m = c - n * (n + 1) / 2;
+    if (m == 0) {
+      p.cout[layout_off(b, n * n, nc)] += sx;
+    } else {
+      int id = lidx(n, m);
+      p.cout[layout_off(b, id, nc)] += sx;
+      p.cout[layout_off(b, id + 1, nc)] += sy;
+    }
+  }
+}
+
+// ------------------------------------------------------------- launchers
+template <typename T, bool HELM>
+int lanes_to_lin(const T* arr, int level, int N, void* lin, cudaStream_t s) {
+  typedef typename V2t<T>::t T2;
+  const int V = HELM ? (N + 1) * (N + 1) : (N + 1) * (N + 2) / 2;
+  const int64_t nx = 1 << (level - 1), npx = nx + 2;
+  WBFMM_CUDA(cudaMemsetAsync(lin, 0, sizeof(T2) * 8 * V * npx * npx * npx, s));
+  const int64_t tot = nx * nx * nx * V * 8;
+  k_to_lin<T, HELM><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(arr, level, N, (T2*)lin);
+  WBFMM_CUDA(cudaGetLastError());
+  return 0;
+}
+
+size_t lanes_lin_bytes(int level, int N, bool helm, size_t tsize) {
+  const size_t V = helm ? (N + 1) * (N + 1) : (N + 1) * (N + 2) / 2;
+  const size_t npx = (1u << (level - 1)) + 2;
+  return 2 * tsize * 8 * V * npx * npx * npx;
+}
+
+template <typename T, bool HELM, int P>
+static int launch_lanes_P(const LanesParams<T>& p, const OpTables<T>& t,
+                          cudaStream_t s) {
+  typedef LaneSmem<T, HELM, P> SM;
+  WBFMM_CUDA(cudaFuncSetAttribute(k_m2l_lanes<T, HELM, P>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)SM::bytes));
+  const int64_t np = (int64_t)1 << (3 * (p.level - 1));
+  dim3 grid((unsigned)((np + SM::CTA - 1) / SM::CTA), 8, p.nsplit);
+  k_m2l_lanes<T, HELM, P><<<grid, SM::CTA, SM::bytes, s>>>(p, t);
+  WBFMM_CUDA(cudaGetLastError());
+  if (p.nsplit > 1) {
+    const int64_t tot = np * 8 * SM::V;
+    k_lanes_reduce<T, HELM><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(p, P);
+    WBFMM_CUDA(cudaGetLastError());
+  }
+  return 0;
+}
+
+template <typename T, bool HELM>
+bool lanes_supported(int Ns, int Nr) {
+  if (Ns != Nr) return false;
+  return HELM ? (Ns >= 2 && Ns <= kLanesMaxHelm) : (Ns >= 2 && Ns <= kLanesMaxLap);
+}
+
+template <typename T, bool HELM>
+int launch_m2l_lanes(const LanesParams<T>& p, const OpTables<T>& t,
+                     cudaStream_t s) {
+  {
+    int rc = ensure_offsets();
+    if (rc) return rc;
+  }
+  switch (p.N) {
+#define WBFMM_LANES_CASE(PP) \
+  case PP: return launch_lanes_P<T, HELM, PP>(p, t, s);
+    WBFMM_LANES_CASE(2)
+    WBFMM_LANES_CASE(3)
+    WBFMM_LANES_CASE(4)
+    WBFMM_LANES_CASE(5)
+    WBFMM_LANES_CASE(6)
+    WBFMM_LANES_CASE(7)
+    WBFMM_LANES_CASE(8)
+#undef WBFMM_LANES_CASE
+    default: break;
+  }
+  if (!HELM) {
+    switch (p.N) {
+#define WBFMM_LANES_CASE(PP) \
+  case PP: return launch_lanes_P<T, false, PP>(p, t, s);
+      WBFMM_LANES_CASE(9)
+      WBFMM_LANES_CASE(10)
+      WBFMM_LANES_CASE(11)
+      WBFMM_LANES_CASE(12)
+#undef WBFMM_LANES_CASE
+      default: break;
+    }
+  }
+  return set_error(-3, "M2L lane kernel: order not instantiated");
+}
+
+#define WBFMM_LANES_INST(T, H)                                                   \
+  template int lanes_to_lin<T, H>(const T*, int, int, void*, cudaStream_t);      \
+  template bool lanes_supported<T, H>(int, int);                                 \
+  template int launch_m2l_lanes<T, H>(const LanesParams<T>&, const OpTables<T>&, \
+                                      cudaStream_t);
+WBFMM_LANES_INST(double, true)
+WBFMM_LANES_INST(double, false)
+WBFMM_LANES_INST(float, true)
+WBFMM_LANES_INST(float, false)
+
+}  // namespace wbfmm

@@ -18,6 +18,7 @@
 #include "../../include/wbfmm_b200.h"
 #include "engine.h"
 #include "kernels.h"
+#include "m2l_lanes.h"
 #include "tables.h"
 
 namespace wbfmm {
@@ -124,6 +125,7 @@ struct wbfmm_b200_solver {
   virtual int coefficient_pointers(int, void**, void**) = 0;
   virtual void invalidate_operators() = 0;
   virtual int m2l(int level) = 0;
+  virtual void set_m2l_kernel(int lanes) = 0;
   virtual int l2l(int level) = 0;
 };
 
@@ -174,6 +176,9 @@ struct Solver : public wbfmm_b200_solver {
   DBuf<T> lap[3];
   int lt = 0;
   DBuf<T> partial;
+  DBuf<unsigned char> lin;         // M2L lane kernel: transposed sources
+  DBuf<T> lanes_part;              // and its split partial sums
+  bool use_lanes = true;
   OpTables<T> tables;
   cudaEvent_t ev[8];
   bool events = false;
@@ -531,6 +536,32 @@ struct Solver : public wbfmm_b200_solver {
     x.coax_stride = sr_stride[level];
     x.width = (T)width(level);
     x.tmask = cfg.skip_empty && tmask[level].p ? tmask[level].p : nullptr;
+    if (use_lanes && (helm ? lanes_supported<T, true>(x.Nin, x.Nout)
+                           : lanes_supported<T, false>(x.Nin, x.Nout))) {
+      // lane-per-pair kernel on a transposed copy of the singular expansions
+      WBFMM_TRY(lin.alloc(lanes_lin_bytes(level, x.Nin, helm, sizeof(T))));
+      WBFMM_TRY((helm ? lanes_to_lin<T, true>(x.cin, level, x.Nin, lin.p, stream)
+                      : lanes_to_lin<T, false>(x.cin, level, x.Nin, lin.p, stream)));
+      LanesParams<T> lp;
+      memset(&lp, 0, sizeof(lp));
+      lp.level = level; lp.N = x.Nin;
+      lp.lin_raw = lin.p; lp.cout = x.cout;
+      lp.coax = x.coax; lp.coax_stride = x.coax_stride;
+      lp.width = x.width; lp.tmask = x.tmask;
+      const int64_t np = (int64_t)1 << (3 * (level - 1));
+      const int64_t base = ((np + 127) / 128) * 8;
+      int ns = 1;
+      while (base * ns < 1200 && ns < 32) ns *= 2;
+      lp.nsplit = ns;
+      if (ns > 1) {
+        const int V = helm ? (x.Nin + 1) * (x.Nin + 1) : (x.Nin + 1) * (x.Nin + 2) / 2;
+        WBFMM_TRY(lanes_part.alloc((size_t)ns * 8 * V * np * 2));
+        lp.partial_raw = lanes_part.p;
+      }
+      launches += ns > 1 ? 3 : 2;
+      return helm ? launch_m2l_lanes<T, true>(lp, tables, stream)
+                  : launch_m2l_lanes<T, false>(lp, tables, stream);
+    }
     // split the source lists of coarse levels over several CTAs
     int64_t want = 148 * 8;
     int nsplit = 1;
@@ -666,6 +697,7 @@ struct Solver : public wbfmm_b200_solver {
   }
 
   void invalidate_operators() override { ops_ready = false; }
+  void set_m2l_kernel(int lanes) override { use_lanes = lanes != 0; }
 
   int coefficient_pointers(int level, void** ms, void** mr) override {
     if (level < 1 || level > depth) return set_error(WBFMM_B200_E_ARG, "bad level");
@@ -784,6 +816,11 @@ int wbfmm_b200_get_coefficients(wbfmm_b200_solver_t* s, int level, double* ms,
 int wbfmm_b200_coefficient_pointers(wbfmm_b200_solver_t* s, int level,
                                     void** ms, void** mr) {
   SOLVER_CALL(s->coefficient_pointers(level, ms, mr));
+}
+int wbfmm_b200_set_m2l_kernel(wbfmm_b200_solver_t* s, int lanes) {
+  if (!s) return set_error(WBFMM_B200_E_ARG, "null solver");
+  s->set_m2l_kernel(lanes);
+  return 0;
 }
 int wbfmm_b200_invalidate_operators(wbfmm_b200_solver_t* s) {
   if (!s) return set_error(WBFMM_B200_E_ARG, "null solver");

@@ -89,6 +89,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "wbfmm_b200_solve": (ip, [C.POINTER(Config), ip, vp, vp, vp, vp, ip, vp, vp, vp]),
         "wbfmm_b200_invalidate_operators": (ip, [vp]),
         "wbfmm_b200_m2l": (ip, [vp, ip]),
+        "wbfmm_b200_set_m2l_kernel": (ip, [vp, ip]),
         "wbfmm_b200_l2l": (ip, [vp, ip]),
         "wbfmm_b200_direct": (ip, [ip, C.c_double, ip, vp, vp, vp, vp, ip, vp, vp, vp, ip]),
     }
@@ -231,6 +232,9 @@ class Solver:
 
     def downward_pass(self, level):
         _check(self.lib.wbfmm_b200_downward_pass(self.h, level))
+
+    def set_m2l_kernel(self, lanes: bool):
+        _check(self.lib.wbfmm_b200_set_m2l_kernel(self.h, int(bool(lanes))))
 
     def m2l(self, level):
         _check(self.lib.wbfmm_b200_m2l(self.h, level))
