@@ -140,6 +140,34 @@ int64_t wbfmm_b200_kernel_launches(wbfmm_b200_solver_t *s);
    otherwise persist for the solver's lifetime, keyed by its config). */
 int wbfmm_b200_invalidate_operators(wbfmm_b200_solver_t *s);
 
+/* Fields wbfmm_b200_evaluate computes (subset of the config's field) and
+   whether it adds the near field of the 27 neighbour boxes (the reference's
+   eval_neighbours, src/local.c:264-310). */
+int wbfmm_b200_set_evaluation(wbfmm_b200_solver_t *s, int field,
+                              int neighbours);
+
+/* 1: wbfmm_b200_leaf_expansions adds to the existing leaf coefficients (the
+   reference's zero_expansions = FALSE); 0 (default): overwrites them. */
+int wbfmm_b200_set_p2m_accumulate(wbfmm_b200_solver_t *s, int on);
+
+/* Use caller-supplied coefficient arrays for a level (Layout L, the
+   solver's precision, device-accessible, e.g. from wbfmm_b200_managed_alloc)
+   instead of allocating them; call before wbfmm_b200_set_sources. */
+int wbfmm_b200_adopt_coefficients(wbfmm_b200_solver_t *s, int level,
+                                  void *mps, void *mpr);
+/* zeroed CUDA managed memory (host- and device-accessible) */
+void *wbfmm_b200_managed_alloc(size_t bytes);
+void wbfmm_b200_managed_free(void *p);
+
+/* Tree structure only: the stable Morton permutation ip[n] (t->ip) and the
+   box {i, n} arrays of levels 0..depth concatenated (sum 8^l entries each),
+   exactly as wbfmm_tree_add_points followed by `depth` calls of
+   wbfmm_tree_refine leave them (src/boxes.c:118-277).  Host buffers;
+   pts[i*pstr + 0..2]. */
+int wbfmm_b200_tree_structure(int n, const double *pts, int pstr,
+                              const double *x0, double D, int depth,
+                              uint32_t *ip, uint32_t *box_i, uint32_t *box_n);
+
 /* M2L kernel selection: 1 (default) = lane-per-pair kernel for the orders it
    is instantiated for (Helmholtz <= 8, Laplace <= 12, equal singular and
    regular orders), generic warp kernel otherwise; 0 = always the generic

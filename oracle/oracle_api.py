@@ -137,6 +137,14 @@ class Reference:
         if lib is None:
             raise FileNotFoundError(path)
         self.lib = lib
+        # The reference's dipole P2M touches coefficient index -1 at n = 0
+        # (src/expansions.c:363-371, zero weight): 128 bytes before the first
+        # box of a level.  Arrays below 32 MiB then come from the heap, where
+        # that address is mapped, instead of page-aligned mmap regions.
+        try:
+            C.CDLL(None).mallopt(-3, 32 << 20)     # M_MMAP_THRESHOLD
+        except (AttributeError, OSError):
+            pass
         lib.ref_fmm_run.restype = C.c_int
         lib.ref_fmm_run.argtypes = [C.c_int, C.c_int, _ip, _ip, C.c_double, C.c_int,
                                     C.c_int, _dp, C.c_double, C.c_int, _dp, _dp, _dp,

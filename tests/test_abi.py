@@ -18,7 +18,8 @@ def declared_functions():
             continue
         text = open(os.path.join(INCLUDE, f)).read()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-        text = re.sub(r"#define[^\n]*(\\\n[^\n]*)*", "", text)
+        text = text.replace("\\\n", " ")
+        text = re.sub(r"#define[^\n]*", "", text)
         for m in re.finditer(r"\b(wbfmm_[a-z0-9_]+)\s*\(", text):
             names.add(m.group(1))
     return names

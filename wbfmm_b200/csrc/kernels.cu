@@ -105,10 +105,15 @@ __global__ void k_p2m(P2MParams<T> p) {
   for (int c = lane; c < nc; c += 32) {
     int64_t o = layout_off(b, c, nc);
     if (HELM) {
-      p.mps[2 * o] = acc[2 * c];
-      p.mps[2 * o + 1] = acc[2 * c + 1];
+      if (p.accumulate) {
+        p.mps[2 * o] += acc[2 * c];
+        p.mps[2 * o + 1] += acc[2 * c + 1];
+      } else {
+        p.mps[2 * o] = acc[2 * c];
+        p.mps[2 * o + 1] = acc[2 * c + 1];
+      }
     } else {
-      p.mps[o] = acc[c];
+      if (p.accumulate) p.mps[o] += acc[c]; else p.mps[o] = acc[c];
     }
   }
 }

@@ -43,6 +43,7 @@ struct P2MParams {
   const T* dip;       // dipole strengths (same layout), may be null
   const T* nx; const T* ny; const T* nz;   // sorted normals (dipoles)
   T* mps;             // leaf level, Layout L
+  int accumulate;     // 1: add to the existing coefficients
 };
 
 template <typename T>

@@ -29,12 +29,18 @@ struct DBuf {
   T* p = nullptr;
   size_t n = 0;
   bool managed = false;
+  bool owned = true;        // false: memory supplied by the caller (adopt)
   DBuf() = default;
   DBuf(const DBuf&) = delete;
   DBuf& operator=(const DBuf&) = delete;
   ~DBuf() { release(); }
+  void adopt(T* q, size_t count, bool is_managed) {
+    release();
+    p = q; n = count; managed = is_managed; owned = false;
+  }
   void release() {
-    if (p) cudaFree(p);
+    if (p && owned) cudaFree(p);
+    owned = true;
     p = nullptr; n = 0;
   }
   int alloc(size_t count, bool use_managed = false) {
@@ -126,6 +132,9 @@ struct wbfmm_b200_solver {
   virtual void invalidate_operators() = 0;
   virtual int m2l(int level) = 0;
   virtual void set_m2l_kernel(int lanes) = 0;
+  virtual void set_evaluation(int field, int neighbours) = 0;
+  virtual void set_p2m_accumulate(int on) = 0;
+  virtual int adopt_coefficients(int level, void* ms, void* mr) = 0;
   virtual int l2l(int level) = 0;
 };
 
@@ -179,6 +188,10 @@ struct Solver : public wbfmm_b200_solver {
   DBuf<unsigned char> lin;         // M2L lane kernel: transposed sources
   DBuf<T> lanes_part;              // and its split partial sums
   bool use_lanes = true;
+  bool tree_only = false;          // structure only: no coefficient arrays
+  int eval_field = 3;              // fields evaluate() computes
+  bool eval_neighbours = true;     // evaluate() adds the near field (P2P)
+  bool p2m_accumulate = false;     // leaf expansions add to the arrays
   OpTables<T> tables;
   cudaEvent_t ev[8];
   bool events = false;
@@ -202,11 +215,11 @@ struct Solver : public wbfmm_b200_solver {
     if (cfg.problem != WBFMM_B200_HELMHOLTZ && cfg.problem != WBFMM_B200_LAPLACE)
       return set_error(WBFMM_B200_E_ARG, "problem must be Laplace (1) or Helmholtz (2)");
     depth = cfg.depth;
-    if (depth < 2 || depth > 10)
+    if ((depth < 2 && !tree_only) || depth < 0 || depth > 10)
       return set_error(WBFMM_B200_E_ARG, "depth must be in [2, 10]");
     if (!(cfg.D > 0.0)) return set_error(WBFMM_B200_E_ARG, "tree width must be positive");
     lmax = 0;
-    for (int l = 1; l <= depth; l++) {
+    for (int l = 1; l <= depth && !tree_only; l++) {
       if (cfg.order_s[l] < 1 || cfg.order_r[l] < 1 ||
           cfg.order_s[l] > kMaxOrder || cfg.order_r[l] > kMaxOrder)
         return set_error(WBFMM_B200_E_ORDER, "expansion orders must be in [1, 62]");
@@ -294,8 +307,8 @@ struct Solver : public wbfmm_b200_solver {
       launches += 2;
     }
     WBFMM_CUDA(cudaGetLastError());
-    // coefficient arrays
-    for (int l = 1; l <= depth; l++) {
+    // coefficient arrays (arrays adopted from the caller are kept)
+    for (int l = 1; l <= depth && !tree_only; l++) {
       WBFMM_TRY(mps[l].alloc(level_len(l, cfg.order_s[l]), cfg.managed != 0));
       WBFMM_TRY(mpr[l].alloc(level_len(l, cfg.order_r[l]), cfg.managed != 0));
     }
@@ -488,6 +501,7 @@ struct Solver : public wbfmm_b200_solver {
     p.dip = have_dip ? sdip.p : nullptr;
     p.nx = snx.p; p.ny = sny.p; p.nz = snz.p;
     p.mps = mps[depth].p;
+    p.accumulate = p2m_accumulate ? 1 : 0;
     launches++;
     return helm ? launch_p2m<T, true>(p, stream) : launch_p2m<T, false>(p, stream);
   }
@@ -605,8 +619,8 @@ struct Solver : public wbfmm_b200_solver {
     e.q = have_q ? sq.p : nullptr; e.dip = have_dip ? sdip.p : nullptr;
     e.nx = snx.p; e.ny = sny.p; e.nz = snz.p;
     e.mpr = mpr[depth].p;
-    e.pot = (cfg.field & WBFMM_B200_POTENTIAL) ? pot.p : nullptr;
-    e.grad = (cfg.field & WBFMM_B200_GRADIENT) ? grad.p : nullptr;
+    e.pot = (cfg.field & eval_field & WBFMM_B200_POTENTIAL) ? pot.p : nullptr;
+    e.grad = (cfg.field & eval_field & WBFMM_B200_GRADIENT) ? grad.p : nullptr;
     e.nbox = (int64_t)1 << (3 * depth);
     e.compensated = sizeof(T) == 4 ? 1 : 0;
     return e;
@@ -615,13 +629,13 @@ struct Solver : public wbfmm_b200_solver {
   int evaluate() override {
     if (ntgt <= 0) return set_error(WBFMM_B200_E_STATE, "set_targets first");
     EvalParams<T> e = eparams();
-    launches += 2;
+    launches += eval_neighbours ? 2 : 1;
     if (helm) {
       WBFMM_TRY((launch_l2p<T, true>(e, stream)));
-      return launch_p2p<T, true>(e, stream);
+      return eval_neighbours ? launch_p2p<T, true>(e, stream) : 0;
     }
     WBFMM_TRY((launch_l2p<T, false>(e, stream)));
-    return launch_p2p<T, false>(e, stream);
+    return eval_neighbours ? launch_p2p<T, false>(e, stream) : 0;
   }
 
   int run() override {
@@ -698,6 +712,17 @@ struct Solver : public wbfmm_b200_solver {
 
   void invalidate_operators() override { ops_ready = false; }
   void set_m2l_kernel(int lanes) override { use_lanes = lanes != 0; }
+  void set_p2m_accumulate(int on) override { p2m_accumulate = on != 0; }
+  void set_evaluation(int field, int neighbours) override {
+    eval_field = field;
+    eval_neighbours = neighbours != 0;
+  }
+  int adopt_coefficients(int level, void* ms, void* mr) override {
+    if (level < 1 || level > depth) return set_error(WBFMM_B200_E_ARG, "bad level");
+    if (ms) mps[level].adopt((T*)ms, level_len(level, cfg.order_s[level]), cfg.managed != 0);
+    if (mr) mpr[level].adopt((T*)mr, level_len(level, cfg.order_r[level]), cfg.managed != 0);
+    return 0;
+  }
 
   int coefficient_pointers(int level, void** ms, void** mr) override {
     if (level < 1 || level > depth) return set_error(WBFMM_B200_E_ARG, "bad level");
@@ -816,6 +841,59 @@ int wbfmm_b200_get_coefficients(wbfmm_b200_solver_t* s, int level, double* ms,
 int wbfmm_b200_coefficient_pointers(wbfmm_b200_solver_t* s, int level,
                                     void** ms, void** mr) {
   SOLVER_CALL(s->coefficient_pointers(level, ms, mr));
+}
+int wbfmm_b200_set_p2m_accumulate(wbfmm_b200_solver_t* s, int on) {
+  if (!s) return set_error(WBFMM_B200_E_ARG, "null solver");
+  s->set_p2m_accumulate(on);
+  return 0;
+}
+int wbfmm_b200_set_evaluation(wbfmm_b200_solver_t* s, int field, int neighbours) {
+  if (!s) return set_error(WBFMM_B200_E_ARG, "null solver");
+  s->set_evaluation(field, neighbours);
+  return 0;
+}
+int wbfmm_b200_adopt_coefficients(wbfmm_b200_solver_t* s, int level, void* ms,
+                                  void* mr) {
+  SOLVER_CALL(s->adopt_coefficients(level, ms, mr));
+}
+void* wbfmm_b200_managed_alloc(size_t bytes) {
+  void* p = nullptr;
+  if (cudaMallocManaged(&p, bytes ? bytes : 1) != cudaSuccess) {
+    cudaGetLastError();
+    set_error(WBFMM_B200_E_NOMEM, "managed allocation failed");
+    return nullptr;
+  }
+  memset(p, 0, bytes);
+  return p;
+}
+void wbfmm_b200_managed_free(void* p) {
+  if (p) cudaFree(p);
+}
+int wbfmm_b200_tree_structure(int n, const double* pts, int pstr,
+                              const double* x0, double D, int depth,
+                              uint32_t* ip, uint32_t* box_i, uint32_t* box_n) {
+  if (depth < 0 || depth > 10) return set_error(WBFMM_B200_E_ARG, "depth must be in [0, 10]");
+  if (wbfmm_b200_device_count() < 1)
+    return set_error(WBFMM_B200_E_NOGPU, "no CUDA device is available");
+  wbfmm_b200_config_t c;
+  memset(&c, 0, sizeof(c));
+  c.problem = WBFMM_B200_LAPLACE;
+  c.depth = depth;
+  c.x0[0] = x0[0]; c.x0[1] = x0[1]; c.x0[2] = x0[2];
+  c.D = D;
+  Solver<double> sv;
+  sv.tree_only = true;
+  int rc = sv.init(&c, nullptr);
+  if (!rc) rc = sv.set_sources(n, pts, pstr, nullptr, 3, 0);
+  if (rc) return rc;
+  size_t off = 0;
+  for (int l = 0; l <= depth; l++) {
+    rc = sv.get_tree(l == 0 ? ip : nullptr, box_i ? box_i + off : nullptr,
+                     box_n ? box_n + off : nullptr, l);
+    if (rc) return rc;
+    off += (size_t)1 << (3 * l);
+  }
+  return 0;
 }
 int wbfmm_b200_set_m2l_kernel(wbfmm_b200_solver_t* s, int lanes) {
   if (!s) return set_error(WBFMM_B200_E_ARG, "null solver");
