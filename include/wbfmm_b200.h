@@ -214,6 +214,65 @@ int wbfmm_b200_solve(const wbfmm_b200_config_t *cfg, int nsrc,
                      const double *dipoles, int ntgt, const double *xt,
                      double *pot, double *grad);
 
+/* 1 when the FP32 form keeps this configuration's tables and expansions
+   inside the FP32 range (Helmholtz (S|R) coefficients at the nearest list-4
+   distance and leaf Bessel terms within 1e+-36, Laplace order <= 16);
+   0 when the solve needs the FP64 form. */
+int wbfmm_b200_fp32_range_ok(const wbfmm_b200_config_t *cfg);
+
+/* ------------------------------------------------------------------------
+   Served form (no reference counterpart): continuous batching of
+   independent solves on one GPU.  `nslots` solves run at once, each on its
+   own stream, admitted first come first served while the summed
+   wbfmm_b200_footprint of the solves in flight stays within `hbm_budget`
+   bytes.  Operator tables are shared across solves (per order; Helmholtz
+   coaxial tables per (k * box width, order)).  Inputs and outputs are host
+   arrays that the caller keeps alive until the request completes; fields
+   come back in FP64 in the layouts of wbfmm_b200_get_field.  All calls are
+   thread-safe.
+   ------------------------------------------------------------------------ */
+typedef struct wbfmm_b200_server wbfmm_b200_server_t;
+
+typedef struct {
+  wbfmm_b200_config_t cfg;  /* problem, tree, orders, k, precision, field */
+  int nsrc;
+  const double *xs;         /* [3 nsrc] */
+  const double *q;          /* [w nsrc] or NULL (w = 2 Helmholtz, 1 Laplace) */
+  const double *normals;    /* [3 nsrc] or NULL */
+  const double *dipoles;    /* [w nsrc] or NULL */
+  int ntgt;
+  const double *xt;         /* [3 ntgt]; may be xs (targets = sources) */
+  double *pot;              /* [w ntgt] or NULL */
+  double *grad;             /* [3 w ntgt] or NULL */
+  double arrival;           /* server-clock seconds before which the request
+                               is not started (0: on submission) */
+} wbfmm_b200_request_t;
+
+int wbfmm_b200_server_create(wbfmm_b200_server_t **srv, int nslots,
+                             int64_t hbm_budget);
+/* waits for every request, then releases the server */
+int wbfmm_b200_server_destroy(wbfmm_b200_server_t *srv);
+/* seconds since the server was created (the clock of `arrival`) */
+double wbfmm_b200_server_clock(wbfmm_b200_server_t *srv);
+/* queue a request; WBFMM_B200_E_ADMISSION when its footprint alone exceeds
+   the budget */
+int wbfmm_b200_server_submit(wbfmm_b200_server_t *srv,
+                             const wbfmm_b200_request_t *req, int64_t *ticket);
+/* 1 when the request has completed, 0 when not yet */
+int wbfmm_b200_server_poll(wbfmm_b200_server_t *srv, int64_t ticket);
+/* blocks until the request has completed; returns its status */
+int wbfmm_b200_server_wait(wbfmm_b200_server_t *srv, int64_t ticket);
+/* arrival, start and completion times (server clock) of a completed request */
+int wbfmm_b200_server_times(wbfmm_b200_server_t *srv, int64_t ticket,
+                            double *t3);
+/* drops a completed request's record */
+int wbfmm_b200_server_forget(wbfmm_b200_server_t *srv, int64_t ticket);
+/* blocks until the queue is empty and no solve is running */
+int wbfmm_b200_server_drain(wbfmm_b200_server_t *srv);
+/* completed requests, peak bytes in flight, peak solves in flight, table
+   cache hits, misses and bytes */
+int wbfmm_b200_server_stats(wbfmm_b200_server_t *srv, int64_t *out6);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,373 @@
+// Served form: continuous batching of independent FMM solves on one GPU.
+//
+// A server owns S slots.  Each slot is a host thread with its own CUDA
+// stream and a reusable solver per precision whose buffers come from the
+// device's stream-ordered pool.  Requests wait in an arrival-ordered queue;
+// a slot that falls free takes the oldest request whose arrival time has
+// passed, provided the device-memory footprints of the solves in flight plus
+// its own stay within the budget (first come, first served: a request that
+// does not fit yet holds back the ones behind it).  A slot queues the whole
+// solve -- tree build, passes, evaluation, copy-back -- on its stream with no
+// host wait, then sleeps on a blocking event until the stream drains, so
+// up to S solves run on the device at once and their kernels overlap.
+// Operator tables are shared between slots through a TableCache (rotation
+// and Laplace tables per order, Helmholtz coaxial tables per (k w, order)).
+//
+// Callers keep a request's input and output arrays alive until the request
+// has completed (wbfmm_b200_server_wait / _poll).
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "solver.h"
+
+using namespace wbfmm;
+
+namespace {
+
+double now_s() {
+  using clk = std::chrono::steady_clock;
+  return std::chrono::duration<double>(clk::now().time_since_epoch()).count();
+}
+
+struct Req {
+  int64_t id = 0;
+  wbfmm_b200_request_t r;
+  int64_t footprint = 0;
+  double t_arrival = 0, t_start = 0, t_end = 0;   // server clock
+  int state = 0;                                   // 0 queued, 1 running, 2 done
+  int status = 0;
+  char error[256] = "";
+};
+
+// pinned host staging that only grows
+struct Pinned {
+  double* p = nullptr;
+  size_t n = 0;
+  ~Pinned() { if (p) cudaFreeHost(p); }
+  int reserve(size_t count) {
+    if (count <= n) return 0;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    n = 0;
+    size_t want = count + count / 4;
+    if (cudaMallocHost(&p, sizeof(double) * want) != cudaSuccess) {
+      cudaGetLastError();
+      return set_error(WBFMM_B200_E_NOMEM, "pinned host allocation failed");
+    }
+    n = want;
+    return 0;
+  }
+};
+
+}  // namespace
+
+struct wbfmm_b200_server {
+  struct Slot {
+    std::thread th;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+    Solver<float>* s32 = nullptr;
+    Solver<double>* s64 = nullptr;
+    Pinned in, out;
+  };
+
+  int device = 0;
+  int64_t budget = 0;
+  double epoch = 0;
+  TableCache cache;
+  std::vector<Slot*> slots;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<Req*> queue;                     // ordered by arrival time
+  std::unordered_map<int64_t, Req*> reqs;
+  int64_t next_id = 1, inflight = 0, peak_inflight = 0, completed = 0;
+  int running = 0, peak_running = 0;
+  bool stop = false;
+
+  double clock() const { return now_s() - epoch; }
+
+  ~wbfmm_b200_server() {
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      stop = true;
+    }
+    cv_work.notify_all();
+    for (Slot* s : slots)
+      if (s->th.joinable()) s->th.join();
+    cudaSetDevice(device);
+    for (Slot* s : slots) {
+      delete s->s32;
+      delete s->s64;
+      if (s->done) cudaEventDestroy(s->done);
+      if (s->stream) cudaStreamDestroy(s->stream);
+      delete s;
+    }
+    for (auto& e : reqs) delete e.second;
+  }
+
+  template <typename T>
+  int make_solver(Slot* s, const wbfmm_b200_config_t* c, Solver<T>** out) {
+    if (!*out) {
+      auto* x = new Solver<T>();
+      x->cache = &cache;
+      x->async_checks = true;
+      int rc = x->init(c, (void*)s->stream);
+      if (rc) { delete x; return rc; }
+      *out = x;
+    }
+    return (*out)->reset(c);
+  }
+
+  // one solve on the slot's stream; fields land in the caller's arrays
+  template <typename T>
+  int execute(Slot* s, Solver<T>* sv, const wbfmm_b200_request_t& r) {
+    const int w = r.cfg.problem == WBFMM_B200_HELMHOLTZ ? 2 : 1;
+    const size_t ns = (size_t)r.nsrc, nt = (size_t)r.ntgt;
+    const bool same = r.xt == r.xs && r.ntgt == r.nsrc;
+    size_t need = 3 * ns + (r.q ? w * ns : 0) + (r.normals ? 3 * ns : 0) +
+                  (r.dipoles ? w * ns : 0) + (same ? 0 : 3 * nt);
+    WBFMM_TRY(s->in.reserve(need));
+    double* p = s->in.p;
+    auto stage = [&](const double* src, size_t n) -> const double* {
+      if (!src) return nullptr;
+      memcpy(p, src, sizeof(double) * n);
+      const double* q = p;
+      p += n;
+      return q;
+    };
+    const double* xs = stage(r.xs, 3 * ns);
+    const double* q = stage(r.q, w * ns);
+    const double* nrm = stage(r.normals, 3 * ns);
+    const double* dip = stage(r.dipoles, w * ns);
+    const double* xt = same ? xs : stage(r.xt, 3 * nt);
+    const size_t np = r.pot ? w * nt : 0, ng = r.grad ? 3 * w * nt : 0;
+    WBFMM_TRY(s->out.reserve(np + ng));
+    WBFMM_TRY(sv->set_sources((int)ns, xs, 3, nrm, 3, 0));
+    WBFMM_TRY(sv->set_strengths(q, w, dip, w, 0));
+    WBFMM_TRY(sv->set_targets((int)nt, xt, 3, 0));
+    WBFMM_TRY(sv->run_async());
+    WBFMM_TRY(sv->fetch_async(np ? s->out.p : nullptr, ng ? s->out.p + np : nullptr));
+    WBFMM_CUDA(cudaEventRecord(s->done, s->stream));
+    WBFMM_CUDA(cudaEventSynchronize(s->done));
+    WBFMM_TRY(sv->check_flags());
+    if (np) memcpy(r.pot, s->out.p, sizeof(double) * np);
+    if (ng) memcpy(r.grad, s->out.p + np, sizeof(double) * ng);
+    return 0;
+  }
+
+  int run_one(Slot* s, Req* q) {
+    const wbfmm_b200_request_t& r = q->r;
+    int rc;
+    if (r.cfg.precision == WBFMM_B200_FP32) {
+      rc = make_solver(s, &r.cfg, &s->s32);
+      if (!rc) rc = execute(s, s->s32, r);
+    } else {
+      rc = make_solver(s, &r.cfg, &s->s64);
+      if (!rc) rc = execute(s, s->s64, r);
+    }
+    if (rc) {
+      // drain whatever was queued before the failure
+      cudaStreamSynchronize(s->stream);
+      cudaGetLastError();
+    }
+    if (s->s32) { s->s32->release_cache_refs(); s->s32->release_buffers(); }
+    if (s->s64) { s->s64->release_cache_refs(); s->s64->release_buffers(); }
+    return rc;
+  }
+
+  void slot_main(Slot* s) {
+    cudaSetDevice(device);
+    for (;;) {
+      Req* q = nullptr;
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        for (;;) {
+          if (stop && queue.empty()) return;
+          if (!queue.empty()) {
+            Req* h = queue.front();
+            double t = clock();
+            if (h->t_arrival > t) {
+              cv_work.wait_for(lk, std::chrono::duration<double>(h->t_arrival - t));
+              continue;
+            }
+            if (inflight + h->footprint <= budget || running == 0) {
+              queue.pop_front();
+              q = h;
+              inflight += q->footprint;
+              peak_inflight = std::max(peak_inflight, inflight);
+              running++;
+              peak_running = std::max(peak_running, running);
+              q->state = 1;
+              break;
+            }
+          }
+          cv_work.wait(lk);
+        }
+      }
+      q->t_start = clock();
+      int rc = run_one(s, q);
+      q->t_end = clock();
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        q->status = rc;
+        if (rc) snprintf(q->error, sizeof(q->error), "%s", wbfmm::last_error());
+        q->state = 2;
+        inflight -= q->footprint;
+        running--;
+        completed++;
+      }
+      cv_done.notify_all();
+      cv_work.notify_all();
+    }
+  }
+};
+
+extern "C" {
+
+int wbfmm_b200_server_create(wbfmm_b200_server_t** out, int nslots,
+                             int64_t hbm_budget) {
+  if (!out || nslots < 1 || nslots > 256 || hbm_budget <= 0)
+    return set_error(WBFMM_B200_E_ARG, "server: bad arguments");
+  *out = nullptr;
+  if (wbfmm_b200_device_count() < 1)
+    return set_error(WBFMM_B200_E_NOGPU, "no CUDA device is available");
+  auto* srv = new wbfmm_b200_server();
+  if (cudaGetDevice(&srv->device) != cudaSuccess) {
+    delete srv;
+    return set_error(WBFMM_B200_E_NOGPU, "no current CUDA device");
+  }
+  srv->budget = hbm_budget;
+  srv->epoch = now_s();
+  // keep freed pool memory cached in the process: solves reallocate cheaply
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, srv->device) == cudaSuccess) {
+    uint64_t thr = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
+  for (int i = 0; i < nslots; i++) {
+    auto* s = new wbfmm_b200_server::Slot();
+    srv->slots.push_back(s);
+    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->done, cudaEventBlockingSync | cudaEventDisableTiming) != cudaSuccess) {
+      cudaGetLastError();
+      delete srv;
+      return set_error(WBFMM_B200_E_NOMEM, "server: stream creation failed");
+    }
+  }
+  for (auto* s : srv->slots) s->th = std::thread([srv, s] { srv->slot_main(s); });
+  *out = srv;
+  return 0;
+}
+
+int wbfmm_b200_server_destroy(wbfmm_b200_server_t* srv) {
+  delete srv;
+  return 0;
+}
+
+double wbfmm_b200_server_clock(wbfmm_b200_server_t* srv) {
+  return srv ? srv->clock() : 0.0;
+}
+
+int wbfmm_b200_server_submit(wbfmm_b200_server_t* srv,
+                             const wbfmm_b200_request_t* r, int64_t* ticket) {
+  if (!srv || !r || !ticket) return set_error(WBFMM_B200_E_ARG, "null argument");
+  if (r->nsrc <= 0 || r->ntgt <= 0 || !r->xs || !r->xt || (!r->q && !r->dipoles))
+    return set_error(WBFMM_B200_E_ARG, "request needs sources, strengths and targets");
+  if (r->dipoles && !r->normals)
+    return set_error(WBFMM_B200_E_ARG, "dipole strengths need normals");
+  if (r->cfg.precision != WBFMM_B200_FP32 && r->cfg.precision != WBFMM_B200_FP64)
+    return set_error(WBFMM_B200_E_ARG, "precision must be FP64 (0) or FP32 (1)");
+  auto* q = new Req();
+  q->r = *r;
+  q->footprint = wbfmm_b200_footprint(&r->cfg, r->nsrc, r->ntgt);
+  if (q->footprint > srv->budget) {
+    delete q;
+    return set_error(WBFMM_B200_E_ADMISSION, "request footprint exceeds the server's device-memory budget");
+  }
+  {
+    std::lock_guard<std::mutex> lk(srv->mu);
+    q->id = srv->next_id++;
+    double t = srv->clock();
+    q->t_arrival = r->arrival > t ? r->arrival : t;
+    auto it = srv->queue.end();
+    while (it != srv->queue.begin() && (*(it - 1))->t_arrival > q->t_arrival) --it;
+    srv->queue.insert(it, q);
+    srv->reqs[q->id] = q;
+    *ticket = q->id;
+  }
+  srv->cv_work.notify_all();
+  return 0;
+}
+
+int wbfmm_b200_server_poll(wbfmm_b200_server_t* srv, int64_t ticket) {
+  if (!srv) return set_error(WBFMM_B200_E_ARG, "null server");
+  std::lock_guard<std::mutex> lk(srv->mu);
+  auto it = srv->reqs.find(ticket);
+  if (it == srv->reqs.end()) return set_error(WBFMM_B200_E_ARG, "unknown ticket");
+  return it->second->state == 2 ? 1 : 0;
+}
+
+int wbfmm_b200_server_wait(wbfmm_b200_server_t* srv, int64_t ticket) {
+  if (!srv) return set_error(WBFMM_B200_E_ARG, "null server");
+  std::unique_lock<std::mutex> lk(srv->mu);
+  auto it = srv->reqs.find(ticket);
+  if (it == srv->reqs.end()) return set_error(WBFMM_B200_E_ARG, "unknown ticket");
+  Req* q = it->second;
+  srv->cv_done.wait(lk, [q] { return q->state == 2; });
+  if (q->status) return set_error(q->status, q->error);
+  return 0;
+}
+
+int wbfmm_b200_server_times(wbfmm_b200_server_t* srv, int64_t ticket,
+                            double* t3) {
+  if (!srv || !t3) return set_error(WBFMM_B200_E_ARG, "null argument");
+  std::lock_guard<std::mutex> lk(srv->mu);
+  auto it = srv->reqs.find(ticket);
+  if (it == srv->reqs.end()) return set_error(WBFMM_B200_E_ARG, "unknown ticket");
+  t3[0] = it->second->t_arrival;
+  t3[1] = it->second->t_start;
+  t3[2] = it->second->t_end;
+  return it->second->state == 2 ? 0 : set_error(WBFMM_B200_E_STATE, "request not complete");
+}
+
+int wbfmm_b200_server_forget(wbfmm_b200_server_t* srv, int64_t ticket) {
+  if (!srv) return set_error(WBFMM_B200_E_ARG, "null server");
+  std::lock_guard<std::mutex> lk(srv->mu);
+  auto it = srv->reqs.find(ticket);
+  if (it == srv->reqs.end()) return set_error(WBFMM_B200_E_ARG, "unknown ticket");
+  if (it->second->state != 2) return set_error(WBFMM_B200_E_STATE, "request not complete");
+  delete it->second;
+  srv->reqs.erase(it);
+  return 0;
+}
+
+int wbfmm_b200_server_drain(wbfmm_b200_server_t* srv) {
+  if (!srv) return set_error(WBFMM_B200_E_ARG, "null server");
+  std::unique_lock<std::mutex> lk(srv->mu);
+  srv->cv_done.wait(lk, [srv] { return srv->queue.empty() && srv->running == 0; });
+  return 0;
+}
+
+int wbfmm_b200_server_stats(wbfmm_b200_server_t* srv, int64_t* out6) {
+  if (!srv || !out6) return set_error(WBFMM_B200_E_ARG, "null argument");
+  std::lock_guard<std::mutex> lk(srv->mu);
+  std::lock_guard<std::mutex> lc(srv->cache.mu);
+  out6[0] = srv->completed;
+  out6[1] = srv->peak_inflight;
+  out6[2] = srv->peak_running;
+  out6[3] = srv->cache.hits;
+  out6[4] = srv->cache.misses;
+  out6[5] = (int64_t)srv->cache.coax_bytes;
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,870 @@
+#pragma once
+// The solver: engine orchestration behind the C ABI of include/wbfmm_b200.h.
+//
+// A solver owns, on one CUDA stream: the sorted sources and their Morton
+// keys, the per-level box ranges, the per-level coefficient arrays in the
+// reference's Layout L, the operator tables and the sorted targets.  The
+// FP64 instantiation is the plain form; the FP32 instantiation keeps the
+// same structure with FP32 coefficients, FP64-generated tables converted to
+// FP32, FP64 point separations and compensated P2P accumulation.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <memory>
+#include <vector>
+
+#include "../../include/wbfmm_b200.h"
+#include "engine.h"
+#include "kernels.h"
+#include "m2l_lanes.h"
+#include "table_cache.h"
+#include "tables.h"
+
+namespace wbfmm {
+
+// ------------------------------------------------------------ buffers
+// Device buffer that only grows.  With a stream set, device memory comes
+// from the device's stream-ordered pool (cudaMallocAsync / cudaFreeAsync on
+// that stream): no device-wide synchronisation on reallocation or release.
+template <typename T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  bool managed = false;
+  bool owned = true;        // false: memory supplied by the caller (adopt)
+  cudaStream_t so = nullptr;
+  DBuf() = default;
+  explicit DBuf(cudaStream_t s) : so(s) {}
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  ~DBuf() { release(); }
+  void adopt(T* q, size_t count, bool is_managed) {
+    release();
+    p = q; n = count; managed = is_managed; owned = false;
+  }
+  void release() {
+    if (p && owned) {
+      if (so && !managed) cudaFreeAsync(p, so);
+      else cudaFree(p);
+    }
+    owned = true;
+    p = nullptr; n = 0;
+  }
+  int alloc(size_t count, bool use_managed = false) {
+    if (p && n >= count && managed == use_managed) return 0;
+    release();
+    managed = use_managed;
+    size_t bytes = sizeof(T) * (count ? count : 1);
+    cudaError_t e = use_managed ? cudaMallocManaged(&p, bytes)
+                    : so        ? cudaMallocAsync(&p, bytes, so)
+                                : cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+      p = nullptr;
+      cudaGetLastError();
+      return set_error(WBFMM_B200_E_NOMEM, "device allocation failed");
+    }
+    n = count;
+    return 0;
+  }
+};
+
+#define WBFMM_TRY(call)            \
+  do {                             \
+    int rc_ = (call);              \
+    if (rc_ != 0) return rc_;      \
+  } while (0)
+#define WBFMM_TRY_VOID(call)       \
+  do {                             \
+    if ((call) != 0) return;       \
+  } while (0)
+
+template <typename T>
+__global__ void k_convert(const double* __restrict__ a, T* __restrict__ b,
+                          int64_t n) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) b[i] = (T)a[i];
+}
+template <typename T>
+__global__ void k_widen(const T* __restrict__ a, double* __restrict__ b,
+                        int64_t n) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) b[i] = (double)a[i];
+}
+static __global__ void k_u64_to_u32(const uint64_t* __restrict__ a,
+                             uint32_t* __restrict__ b, int n) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) b[i] = (uint32_t)a[i];
+}
+// box at `level` has targets below it
+static __global__ void k_target_mask(const uint32_t* __restrict__ leaf_count,
+                              int depth, int level, uint8_t* __restrict__ mask) {
+  int64_t nb = (int64_t)1 << (3 * level);
+  int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nb) return;
+  int sh = 3 * (depth - level);
+  int64_t lo = b << sh, hi = (b + 1) << sh;
+  uint8_t any = 0;
+  for (int64_t c = lo; c < hi && !any; c++) any = leaf_count[c] != 0;
+  mask[b] = any;
+}
+
+template <typename T>
+static int convert_to(const double* src, T* dst, int64_t n, cudaStream_t s) {
+  if (n <= 0) return 0;
+  k_convert<T><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(src, dst, n);
+  WBFMM_CUDA(cudaGetLastError());
+  return 0;
+}
+
+}  // namespace wbfmm
+
+// ------------------------------------------------------------- solver
+struct wbfmm_b200_solver {
+  virtual ~wbfmm_b200_solver() {}
+  wbfmm_b200_config_t cfg;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int64_t launches = 0;
+  double stage_ms[6] = {0, 0, 0, 0, 0, 0};
+  virtual int set_sources(int, const double*, int, const double*, int, int) = 0;
+  virtual int set_strengths(const double*, int, const double*, int, int) = 0;
+  virtual int set_targets(int, const double*, int, int) = 0;
+  virtual int build_operators() = 0;
+  virtual int leaf_expansions() = 0;
+  virtual int upward(int level) = 0;
+  virtual int downward(int level) = 0;
+  virtual int evaluate() = 0;
+  virtual int run() = 0;
+  virtual int get_field(double*, double*, int) = 0;
+  virtual int get_tree(uint32_t*, uint32_t*, uint32_t*, int) = 0;
+  virtual int get_coefficients(int, double*, double*) = 0;
+  virtual int coefficient_pointers(int, void**, void**) = 0;
+  virtual void invalidate_operators() = 0;
+  virtual int m2l(int level) = 0;
+  virtual void set_m2l_kernel(int lanes) = 0;
+  virtual void set_evaluation(int field, int neighbours) = 0;
+  virtual void set_p2m_accumulate(int on) = 0;
+  virtual int adopt_coefficients(int level, void* ms, void* mr) = 0;
+  virtual int l2l(int level) = 0;
+};
+
+namespace wbfmm {
+
+template <typename T>
+struct Solver : public wbfmm_b200_solver {
+  bool helm = false;
+  int depth = 0, lmax = 0;
+  // sources
+  int nsrc = 0;
+  DBuf<double> pts_in, nrm_in;
+  int xstr = 3, nstr = 3;
+  DBuf<uint64_t> keys;
+  DBuf<uint32_t> ip;
+  DBuf<double> sx, sy, sz;
+  DBuf<T> snx, sny, snz, sq, sdip;
+  DBuf<double> stage;       // strength staging
+  bool have_q = false, have_dip = false, have_normals = false;
+  RadixScratch rs;
+  DBuf<uint32_t> box_i[kMaxDepth + 1], box_n[kMaxDepth + 1];
+  // coefficients (Layout L)
+  DBuf<T> mps[kMaxDepth + 1], mpr[kMaxDepth + 1];
+  // targets
+  int ntgt = 0;
+  DBuf<double> tpts_in, tx, ty, tz;
+  DBuf<uint64_t> tkeys;
+  DBuf<uint32_t> tperm, tbox, tstart, tcount;
+  DBuf<uint8_t> tmask[kMaxDepth + 1];
+  DBuf<int> flag;
+  // outputs (original order)
+  DBuf<T> pot, grad;
+  DBuf<double> out64;
+  // tables
+  bool ops_ready = false;
+  ShiftGeometry geom;
+  DBuf<double> H64;
+  DBuf<T> H;
+  int64_t hstride = 0;
+  DBuf<int> op_ith, op_dist;
+  DBuf<T> op_r, op_ph, op_ch;
+  DBuf<double> coax64[kMaxDepth + 1];   // Helmholtz: SR (15) for M2L
+  DBuf<T> coaxSR[kMaxDepth + 1];
+  int64_t sr_stride[kMaxDepth + 1] = {0};
+  const T* sr_ptr[kMaxDepth + 1] = {nullptr};   // (S|R) table per level
+  const T* ss_ptr[kMaxDepth + 1] = {nullptr};   // (R|R) table per level
+  DBuf<double> ss64[kMaxDepth + 1];
+  DBuf<T> coaxSS[kMaxDepth + 1];
+  DBuf<double> lap64[3];
+  DBuf<T> lap[3];
+  int lt = 0;
+  DBuf<T> partial;
+  DBuf<unsigned char> lin;         // M2L lane kernel: transposed sources
+  DBuf<T> lanes_part;              // and its split partial sums
+  bool use_lanes = true;
+  bool tree_only = false;          // structure only: no coefficient arrays
+  int eval_field = 3;              // fields evaluate() computes
+  bool eval_neighbours = true;     // evaluate() adds the near field (P2P)
+  bool p2m_accumulate = false;     // leaf expansions add to the arrays
+  OpTables<T> tables;
+  cudaEvent_t ev[8];
+  bool events = false;
+  // served form: shared tables, no host waits inside a solve
+  TableCache* cache = nullptr;
+  std::vector<TableCache::Coax*> held;   // cache entries this solve reads
+  bool async_checks = false;   // domain checks read back after the solve
+  int* hflag = nullptr;        // pinned copy of flag[0..1]
+
+  template <class F>
+  void each_buf(F&& f) {
+    f(pts_in); f(nrm_in); f(keys); f(ip); f(sx); f(sy); f(sz);
+    f(snx); f(sny); f(snz); f(sq); f(sdip); f(stage);
+    for (int l = 0; l <= kMaxDepth; l++) {
+      f(box_i[l]); f(box_n[l]); f(mps[l]); f(mpr[l]); f(tmask[l]);
+      f(coax64[l]); f(coaxSR[l]); f(ss64[l]); f(coaxSS[l]);
+    }
+    f(tpts_in); f(tx); f(ty); f(tz); f(tkeys); f(tperm); f(tbox);
+    f(tstart); f(tcount); f(flag); f(pot); f(grad); f(out64);
+    f(H64); f(H); f(op_ith); f(op_dist); f(op_r); f(op_ph); f(op_ch);
+    for (int i = 0; i < 3; i++) { f(lap64[i]); f(lap[i]); }
+    f(partial); f(lin); f(lanes_part);
+  }
+
+  ~Solver() override {
+    release_cache_refs();
+    each_buf([](auto& b) { b.release(); });
+    if (stream) cudaStreamSynchronize(stream);
+    radix_scratch_free(&rs);
+    if (events)
+      for (int i = 0; i < 8; i++) cudaEventDestroy(ev[i]);
+    if (hflag) cudaFreeHost(hflag);
+    if (own_stream && stream) cudaStreamDestroy(stream);
+  }
+
+  void release_cache_refs() {
+    for (TableCache::Coax* c : held) cache->release(c);
+    held.clear();
+  }
+
+  double width(int level) const { return cfg.D / (double)(1 << level); }
+  int ncoefs(int p) const { return (p + 1) * (p + 1); }
+  size_t level_len(int level, int p) const {
+    return ((size_t)1 << (3 * level)) * ncoefs(p) * (helm ? 2 : 1);
+  }
+
+  // validate and take a configuration (buffers already held are kept)
+  int configure(const wbfmm_b200_config_t* c) {
+    cfg = *c;
+    helm = cfg.problem == WBFMM_B200_HELMHOLTZ;
+    if (cfg.problem != WBFMM_B200_HELMHOLTZ && cfg.problem != WBFMM_B200_LAPLACE)
+      return set_error(WBFMM_B200_E_ARG, "problem must be Laplace (1) or Helmholtz (2)");
+    depth = cfg.depth;
+    if ((depth < 2 && !tree_only) || depth < 0 || depth > 10)
+      return set_error(WBFMM_B200_E_ARG, "depth must be in [2, 10]");
+    if (!(cfg.D > 0.0)) return set_error(WBFMM_B200_E_ARG, "tree width must be positive");
+    lmax = 0;
+    for (int l = 1; l <= depth && !tree_only; l++) {
+      if (cfg.order_s[l] < 1 || cfg.order_r[l] < 1 ||
+          cfg.order_s[l] > kMaxOrder || cfg.order_r[l] > kMaxOrder)
+        return set_error(WBFMM_B200_E_ORDER, "expansion orders must be in [1, 62]");
+      lmax = std::max(lmax, std::max(cfg.order_s[l], cfg.order_r[l]));
+    }
+    if (cfg.field == 0) cfg.field = WBFMM_B200_POTENTIAL;
+    return 0;
+  }
+
+  int init(const wbfmm_b200_config_t* c, void* s) {
+    WBFMM_TRY(configure(c));
+    if (s) {
+      stream = (cudaStream_t)s;
+    } else {
+      WBFMM_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+      own_stream = true;
+    }
+    for (int i = 0; i < 8; i++) WBFMM_CUDA(cudaEventCreate(&ev[i]));
+    events = true;
+    each_buf([&](auto& b) { b.so = stream; });
+    WBFMM_TRY(flag.alloc(2));
+    return 0;
+  }
+
+  // Served form: start a new solve on the same stream and buffers.
+  int reset(const wbfmm_b200_config_t* c) {
+    release_cache_refs();
+    WBFMM_TRY(configure(c));
+    ops_ready = false;
+    nsrc = ntgt = 0;
+    have_q = have_dip = have_normals = false;
+    if (!hflag) WBFMM_CUDA(cudaMallocHost(&hflag, 2 * sizeof(int)));
+    return 0;
+  }
+
+  // Served form: every work buffer back to the stream-ordered pool.
+  void release_buffers() {
+    each_buf([](auto& b) { if (b.owned) b.release(); });
+    WBFMM_TRY_VOID(flag.alloc(2));
+  }
+
+  // flag[0]: first source outside the cube (0x7fffffff: none);
+  // flag[1]: nonzero when a target lies outside the cube
+  static int domain_error(int bad_source, int bad_target) {
+    if (bad_source != 0x7fffffff) {
+      char msg[160];
+      snprintf(msg, sizeof(msg), "source point %d does not lie strictly inside the tree cube", bad_source);
+      return set_error(WBFMM_B200_E_DOMAIN, msg);
+    }
+    if (bad_target) return set_error(WBFMM_B200_E_DOMAIN, "target point outside the tree cube");
+    return 0;
+  }
+
+  // -------------------------------------------------------------- tree
+  int set_sources(int n, const double* xs, int xs_str, const double* normals,
+                  int n_str, int on_device) override {
+    if (n <= 0 || xs == nullptr || xs_str < 3)
+      return set_error(WBFMM_B200_E_ARG, "bad source points");
+    if (normals && n_str < 3) return set_error(WBFMM_B200_E_ARG, "bad normal stride");
+    cudaEventRecord(ev[0], stream);
+    nsrc = n;
+    xstr = xs_str;
+    const double* dpts = xs;
+    if (!on_device) {
+      WBFMM_TRY(pts_in.alloc((size_t)n * xs_str));
+      WBFMM_CUDA(cudaMemcpyAsync(pts_in.p, xs, sizeof(double) * n * xs_str,
+                                 cudaMemcpyHostToDevice, stream));
+      dpts = pts_in.p;
+    }
+    // strict-interior domain check (src/boxes.c:148-153)
+    int big = 0x7fffffff;
+    WBFMM_CUDA(cudaMemcpyAsync(flag.p, &big, sizeof(int), cudaMemcpyHostToDevice, stream));
+    launch_domain_check(dpts, xs_str, n, cfg.x0, cfg.D, flag.p, stream);
+    if (!async_checks) {
+      int bad = 0;
+      WBFMM_CUDA(cudaMemcpyAsync(&bad, flag.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
+      WBFMM_CUDA(cudaStreamSynchronize(stream));
+      WBFMM_TRY(domain_error(bad, 0));
+    }
+    WBFMM_TRY(keys.alloc(n));
+    WBFMM_TRY(ip.alloc(n));
+    launch_point_keys(dpts, xs_str, n, cfg.x0, cfg.D, keys.p, ip.p, stream);
+    WBFMM_TRY(radix_sort_pairs(keys.p, ip.p, n, 60, &rs, stream));
+    launches += 2 + 3 * 8;
+    WBFMM_TRY(sx.alloc(n)); WBFMM_TRY(sy.alloc(n)); WBFMM_TRY(sz.alloc(n));
+    launch_gather_points(dpts, xs_str, ip.p, n, sx.p, sy.p, sz.p, stream);
+    launches++;
+    have_normals = normals != nullptr;
+    if (normals) {
+      const double* dn = normals;
+      nstr = n_str;
+      if (!on_device) {
+        WBFMM_TRY(nrm_in.alloc((size_t)n * n_str));
+        WBFMM_CUDA(cudaMemcpyAsync(nrm_in.p, normals, sizeof(double) * n * n_str,
+                                   cudaMemcpyHostToDevice, stream));
+        dn = nrm_in.p;
+      }
+      DBuf<double> tmp(stream);
+      WBFMM_TRY(tmp.alloc((size_t)3 * n));
+      launch_gather_points(dn, n_str, ip.p, n, tmp.p, tmp.p + n, tmp.p + 2 * n, stream);
+      WBFMM_TRY(snx.alloc(n)); WBFMM_TRY(sny.alloc(n)); WBFMM_TRY(snz.alloc(n));
+      WBFMM_TRY(convert_to<T>(tmp.p, snx.p, n, stream));
+      WBFMM_TRY(convert_to<T>(tmp.p + n, sny.p, n, stream));
+      WBFMM_TRY(convert_to<T>(tmp.p + 2 * n, snz.p, n, stream));
+      launches += 4;
+    }
+    // levels: box {i, n} by repeated refinement (src/boxes.c:208-277)
+    WBFMM_TRY(box_i[0].alloc(1)); WBFMM_TRY(box_n[0].alloc(1));
+    uint32_t root[2] = {0u, (uint32_t)n};
+    WBFMM_CUDA(cudaMemcpyAsync(box_i[0].p, &root[0], 4, cudaMemcpyHostToDevice, stream));
+    WBFMM_CUDA(cudaMemcpyAsync(box_n[0].p, &root[1], 4, cudaMemcpyHostToDevice, stream));
+    for (int l = 1; l <= depth; l++) {
+      size_t nb = (size_t)1 << (3 * l);
+      WBFMM_TRY(box_i[l].alloc(nb)); WBFMM_TRY(box_n[l].alloc(nb));
+      launch_refine_children(keys.p, n, l, box_i[l - 1].p, box_i[l].p, box_n[l].p, stream);
+      launch_refine_parents(l - 1, box_i[l - 1].p, box_n[l - 1].p, stream);
+      launches += 2;
+    }
+    WBFMM_CUDA(cudaGetLastError());
+    // coefficient arrays (arrays adopted from the caller are kept)
+    for (int l = 1; l <= depth && !tree_only; l++) {
+      WBFMM_TRY(mps[l].alloc(level_len(l, cfg.order_s[l]), cfg.managed != 0));
+      WBFMM_TRY(mpr[l].alloc(level_len(l, cfg.order_r[l]), cfg.managed != 0));
+    }
+    cudaEventRecord(ev[1], stream);
+    return 0;
+  }
+
+  int set_strengths(const double* q, int qstr, const double* dip, int dstr,
+                    int on_device) override {
+    if (nsrc <= 0) return set_error(WBFMM_B200_E_STATE, "set_sources first");
+    const int nc = helm ? 2 : 1;
+    if (dip && !have_normals)
+      return set_error(WBFMM_B200_E_ARG, "dipole strengths given but the sources have no normals");
+    if ((q && qstr < nc) || (dip && dstr < nc))
+      return set_error(WBFMM_B200_E_ARG, "strength stride too small");
+    have_q = q != nullptr;
+    have_dip = dip != nullptr;
+    auto upload = [&](const double* a, int str, DBuf<T>& dst) -> int {
+      const double* d = a;
+      if (!on_device) {
+        WBFMM_TRY(stage.alloc((size_t)nsrc * str));
+        WBFMM_CUDA(cudaMemcpyAsync(stage.p, a, sizeof(double) * nsrc * str,
+                                   cudaMemcpyHostToDevice, stream));
+        d = stage.p;
+      }
+      WBFMM_TRY(dst.alloc((size_t)nsrc * nc));
+      if (sizeof(T) == 8)
+        launch_gather_real(d, str, ip.p, nsrc, nc, (double*)dst.p, stream);
+      else
+        launch_gather_real_f32(d, str, ip.p, nsrc, nc, (float*)dst.p, stream);
+      launches++;
+      WBFMM_CUDA(cudaGetLastError());
+      return 0;
+    };
+    if (q) WBFMM_TRY(upload(q, qstr, sq));
+    if (dip) WBFMM_TRY(upload(dip, dstr, sdip));
+    return 0;
+  }
+
+  int set_targets(int n, const double* xt, int tstr, int on_device) override {
+    if (n <= 0 || xt == nullptr || tstr < 3)
+      return set_error(WBFMM_B200_E_ARG, "bad target points");
+    ntgt = n;
+    const double* d = xt;
+    if (!on_device) {
+      WBFMM_TRY(tpts_in.alloc((size_t)n * tstr));
+      WBFMM_CUDA(cudaMemcpyAsync(tpts_in.p, xt, sizeof(double) * n * tstr,
+                                 cudaMemcpyHostToDevice, stream));
+      d = tpts_in.p;
+    }
+    int zero = 0;
+    WBFMM_CUDA(cudaMemcpyAsync(flag.p + 1, &zero, sizeof(int), cudaMemcpyHostToDevice, stream));
+    WBFMM_TRY(tkeys.alloc(n)); WBFMM_TRY(tperm.alloc(n));
+    launch_target_keys(d, tstr, n, cfg.x0, cfg.D, depth, tkeys.p, tperm.p,
+                       flag.p + 1, stream);
+    WBFMM_TRY(radix_sort_pairs(tkeys.p, tperm.p, n, 3 * depth, &rs, stream));
+    WBFMM_TRY(tx.alloc(n)); WBFMM_TRY(ty.alloc(n)); WBFMM_TRY(tz.alloc(n));
+    launch_gather_points(d, tstr, tperm.p, n, tx.p, ty.p, tz.p, stream);
+    WBFMM_TRY(tbox.alloc(n));
+    k_u64_to_u32<<<(n + 255) / 256, 256, 0, stream>>>(tkeys.p, tbox.p, n);
+    size_t nb = (size_t)1 << (3 * depth);
+    WBFMM_TRY(tstart.alloc(nb)); WBFMM_TRY(tcount.alloc(nb));
+    launch_box_ranges(tkeys.p, n, depth, tstart.p, tcount.p, stream);
+    launches += 4 + 3 * ((3 * depth + 7) / 8);
+    if (cfg.skip_empty) {
+      for (int l = 2; l <= depth; l++) {
+        size_t nbl = (size_t)1 << (3 * l);
+        WBFMM_TRY(tmask[l].alloc(nbl));
+        k_target_mask<<<(unsigned)((nbl + 255) / 256), 256, 0, stream>>>(
+            tcount.p, depth, l, tmask[l].p);
+        launches++;
+      }
+    }
+    if (!async_checks) {
+      int bad = 0;
+      WBFMM_CUDA(cudaMemcpyAsync(&bad, flag.p + 1, sizeof(int), cudaMemcpyDeviceToHost, stream));
+      WBFMM_CUDA(cudaStreamSynchronize(stream));
+      WBFMM_TRY(domain_error(0x7fffffff, bad));
+    }
+    const int w = helm ? 2 : 1;
+    if (cfg.field & WBFMM_B200_POTENTIAL) WBFMM_TRY(pot.alloc((size_t)n * w));
+    if (cfg.field & WBFMM_B200_GRADIENT) WBFMM_TRY(grad.alloc((size_t)n * 3 * w));
+    return 0;
+  }
+
+  // ------------------------------------------------------- operators
+  int build_operators() override {
+    if (ops_ready) return 0;
+    cudaEventRecord(ev[2], stream);
+    if (cache) {
+      WBFMM_TRY(shared_operators());
+    } else {
+      WBFMM_TRY(own_operators());
+    }
+    ops_ready = true;
+    cudaEventRecord(ev[3], stream);
+    return 0;
+  }
+
+  // tables from the server's cache (served form)
+  int shared_operators() {
+    WBFMM_TRY(cache->geometry<T>(lmax + 1, stream, &tables));
+    if (!helm) return 0;
+    for (int l = 2; l <= depth; l++) {
+      const int Ll = std::max(cfg.order_s[l], cfg.order_r[l]);
+      const T* p = nullptr;
+      TableCache::Coax* ref = nullptr;
+      WBFMM_TRY(cache->coaxial<T>(0, cfg.k * width(l), Ll, stream, &p, &ref));
+      held.push_back(ref);
+      sr_ptr[l] = p;
+      sr_stride[l] = 2 * ((int64_t)(Ll + 1) * (Ll + 2) * (Ll + 3) / 6 + 1);
+      const int Ls = std::max(std::max(cfg.order_s[l], cfg.order_r[l]),
+                              std::max(cfg.order_s[l - 1], cfg.order_r[l - 1]));
+      WBFMM_TRY(cache->coaxial<T>(1, cfg.k * width(l), Ls, stream, &p, &ref));
+      held.push_back(ref);
+      ss_ptr[l] = p;
+    }
+    return 0;
+  }
+
+  // tables owned by this solver (plain form)
+  int own_operators() {
+    build_shift_geometry(&geom);
+    const int L = lmax + 1;
+    std::vector<int> ith, dist;
+    std::vector<double> r, ph, ch;
+    shift_op_tables(geom, L, ith, dist, r, ph, ch);
+    WBFMM_TRY(op_ith.alloc(kNumOps)); WBFMM_TRY(op_dist.alloc(kNumOps));
+    WBFMM_CUDA(cudaMemcpyAsync(op_ith.p, ith.data(), sizeof(int) * kNumOps, cudaMemcpyHostToDevice, stream));
+    WBFMM_CUDA(cudaMemcpyAsync(op_dist.p, dist.data(), sizeof(int) * kNumOps, cudaMemcpyHostToDevice, stream));
+    {
+      DBuf<double> tmp(stream);
+      size_t nph = ph.size();
+      WBFMM_TRY(tmp.alloc(nph * 2 + kNumOps));
+      WBFMM_CUDA(cudaMemcpyAsync(tmp.p, ph.data(), sizeof(double) * nph, cudaMemcpyHostToDevice, stream));
+      WBFMM_CUDA(cudaMemcpyAsync(tmp.p + nph, ch.data(), sizeof(double) * nph, cudaMemcpyHostToDevice, stream));
+      WBFMM_CUDA(cudaMemcpyAsync(tmp.p + 2 * nph, r.data(), sizeof(double) * kNumOps, cudaMemcpyHostToDevice, stream));
+      WBFMM_TRY(op_ph.alloc(nph)); WBFMM_TRY(op_ch.alloc(nph)); WBFMM_TRY(op_r.alloc(kNumOps));
+      WBFMM_TRY(convert_to<T>(tmp.p, op_ph.p, nph, stream));
+      WBFMM_TRY(convert_to<T>(tmp.p + nph, op_ch.p, nph, stream));
+      WBFMM_TRY(convert_to<T>(tmp.p + 2 * nph, op_r.p, kNumOps, stream));
+    }
+    // rotation tables (FP64 on the GPU)
+    hstride = rot_count(L) + 8;
+    int nth = (int)geom.thetas.size();
+    WBFMM_TRY(H64.alloc((size_t)hstride * nth));
+    WBFMM_TRY(generate_rotation_tables(geom.thetas, L, H64.p, hstride, stream));
+    WBFMM_TRY(H.alloc((size_t)hstride * nth));
+    WBFMM_TRY(convert_to<T>(H64.p, H.p, (int64_t)hstride * nth, stream));
+    launches += 2;
+    if (helm) {
+      for (int l = 2; l <= depth; l++) {
+        // (S|R) for the 15 list-4 distances, order of this level
+        int Ll = std::max(cfg.order_s[l], cfg.order_r[l]);
+        std::vector<double> krs(15);
+        for (int i = 0; i < 15; i++) krs[i] = cfg.k * width(l) * sqrt((double)kListDist2[i]);
+        sr_stride[l] = 2 * ((int64_t)(Ll + 1) * (Ll + 2) * (Ll + 3) / 6 + 1);
+        WBFMM_TRY(coax64[l].alloc((size_t)sr_stride[l] * 15));
+        WBFMM_TRY(generate_coaxial_tables(krs, Ll, 2, coax64[l].p, sr_stride[l], stream));
+        WBFMM_TRY(coaxSR[l].alloc((size_t)sr_stride[l] * 15));
+        WBFMM_TRY(convert_to<T>(coax64[l].p, coaxSR[l].p, sr_stride[l] * 15, stream));
+        sr_ptr[l] = coaxSR[l].p;
+        // (R|R) = (S|S) at k w_l sqrt(3)/2 for M2M l -> l-1 and L2L l-1 -> l
+        int Ls = std::max(std::max(cfg.order_s[l], cfg.order_r[l]),
+                          std::max(cfg.order_s[l - 1], cfg.order_r[l - 1]));
+        std::vector<double> kss(1, cfg.k * width(l) * 0.5 * sqrt(3.0));
+        int64_t n_ss = (int64_t)(Ls + 1) * (Ls + 2) * (Ls + 3) / 6 + 1;
+        WBFMM_TRY(ss64[l].alloc(n_ss));
+        WBFMM_TRY(generate_coaxial_tables(kss, Ls, 1, ss64[l].p, n_ss, stream));
+        WBFMM_TRY(coaxSS[l].alloc(n_ss));
+        WBFMM_TRY(convert_to<T>(ss64[l].p, coaxSS[l].p, n_ss, stream));
+        ss_ptr[l] = coaxSS[l].p;
+        launches += 4;
+      }
+    } else {
+      lt = L;
+      size_t n3 = (size_t)(lt + 1) * (lt + 1) * (lt + 1);
+      for (int i = 0; i < 3; i++) {
+        WBFMM_TRY(lap64[i].alloc(n3));
+        WBFMM_TRY(lap[i].alloc(n3));
+      }
+      WBFMM_TRY(generate_laplace_tables(lt, lap64[0].p, lap64[1].p, lap64[2].p, stream));
+      for (int i = 0; i < 3; i++)
+        WBFMM_TRY(convert_to<T>(lap64[i].p, lap[i].p, (int64_t)n3, stream));
+      launches += 4;
+    }
+    tables.H = H.p; tables.hstride = hstride;
+    tables.op_ith = op_ith.p; tables.op_dist = op_dist.p; tables.op_r = op_r.p;
+    tables.ph = op_ph.p; tables.ch = op_ch.p; tables.lmax = L;
+    if (!helm) {
+      tables.lapSS = lap[0].p; tables.lapRR = lap[1].p; tables.lapSR = lap[2].p;
+      tables.lt = lt;
+    }
+    return 0;
+  }
+
+  // ------------------------------------------------------------- passes
+  int leaf_expansions() override {
+    if (nsrc <= 0) return set_error(WBFMM_B200_E_STATE, "set_sources first");
+    P2MParams<T> p;
+    p.nbox = (int64_t)1 << (3 * depth);
+    p.level = depth; p.N = cfg.order_s[depth];
+    p.x0 = cfg.x0[0]; p.y0 = cfg.x0[1]; p.z0 = cfg.x0[2]; p.wb = width(depth);
+    p.k = (T)cfg.k;
+    p.box_i = box_i[depth].p; p.box_n = box_n[depth].p;
+    p.x = sx.p; p.y = sy.p; p.z = sz.p;
+    p.q = have_q ? sq.p : nullptr;
+    p.dip = have_dip ? sdip.p : nullptr;
+    p.nx = snx.p; p.ny = sny.p; p.nz = snz.p;
+    p.mps = mps[depth].p;
+    p.accumulate = p2m_accumulate ? 1 : 0;
+    launches++;
+    return helm ? launch_p2m<T, true>(p, stream) : launch_p2m<T, false>(p, stream);
+  }
+
+  XlateParams<T> xparams() const {
+    XlateParams<T> x;
+    memset(&x, 0, sizeof(x));
+    x.k = (T)cfg.k;
+    x.nsplit = 1;
+    return x;
+  }
+
+  int upward(int level) override {
+    if (level < 3 || level > depth) return set_error(WBFMM_B200_E_ARG, "upward pass level must be in [3, depth]");
+    WBFMM_TRY(build_operators());
+    XlateParams<T> x = xparams();
+    x.level = level - 1;
+    x.nbox = (int64_t)1 << (3 * (level - 1));
+    x.Nin = cfg.order_s[level]; x.Nout = cfg.order_s[level - 1];
+    x.cin = mps[level].p; x.cout = mps[level - 1].p;
+    x.coax = helm ? ss_ptr[level] : nullptr;
+    x.width = (T)width(level);
+    launches++;
+    return helm ? launch_m2m<T, true>(x, tables, stream)
+                : launch_m2m<T, false>(x, tables, stream);
+  }
+
+  int downward(int level) override {
+    WBFMM_TRY(m2l(level));
+    if (level == depth) return 0;
+    return l2l(level);
+  }
+
+  int m2l(int level) override {
+    if (level < 2 || level > depth) return set_error(WBFMM_B200_E_ARG, "downward pass level must be in [2, depth]");
+    WBFMM_TRY(build_operators());
+    if (level == 2)
+      WBFMM_CUDA(cudaMemsetAsync(mpr[2].p, 0, sizeof(T) * level_len(2, cfg.order_r[2]), stream));
+    XlateParams<T> x = xparams();
+    x.level = level;
+    x.nbox = (int64_t)1 << (3 * level);
+    x.Nin = cfg.order_s[level]; x.Nout = cfg.order_r[level];
+    x.cin = mps[level].p; x.cout = mpr[level].p;
+    x.src_n = box_n[level].p;
+    x.coax = helm ? sr_ptr[level] : nullptr;
+    x.coax_stride = sr_stride[level];
+    x.width = (T)width(level);
+    x.tmask = cfg.skip_empty && tmask[level].p ? tmask[level].p : nullptr;
+    if (use_lanes && (helm ? lanes_supported<T, true>(x.Nin, x.Nout)
+                           : lanes_supported<T, false>(x.Nin, x.Nout))) {
+      // lane-per-pair kernel on a transposed copy of the singular expansions
+      WBFMM_TRY(lin.alloc(lanes_lin_bytes(level, x.Nin, helm, sizeof(T))));
+      WBFMM_TRY((helm ? lanes_to_lin<T, true>(x.cin, level, x.Nin, lin.p, stream)
+                      : lanes_to_lin<T, false>(x.cin, level, x.Nin, lin.p, stream)));
+      LanesParams<T> lp;
+      memset(&lp, 0, sizeof(lp));
+      lp.level = level; lp.N = x.Nin;
+      lp.lin_raw = lin.p; lp.cout = x.cout;
+      lp.coax = x.coax; lp.coax_stride = x.coax_stride;
+      lp.width = x.width; lp.tmask = x.tmask;
+      const int64_t np = (int64_t)1 << (3 * (level - 1));
+      const int64_t base = ((np + 127) / 128) * 8;
+      int ns = 1;
+      while (base * ns < 1200 && ns < 32) ns *= 2;
+      lp.nsplit = ns;
+      if (ns > 1) {
+        const int V = helm ? (x.Nin + 1) * (x.Nin + 1) : (x.Nin + 1) * (x.Nin + 2) / 2;
+        WBFMM_TRY(lanes_part.alloc((size_t)ns * 8 * V * np * 2));
+        lp.partial_raw = lanes_part.p;
+      }
+      launches += ns > 1 ? 3 : 2;
+      return helm ? launch_m2l_lanes<T, true>(lp, tables, stream)
+                  : launch_m2l_lanes<T, false>(lp, tables, stream);
+    }
+    // split the source lists of coarse levels over several CTAs
+    int64_t want = 148 * 8;
+    int nsplit = 1;
+    while (x.nbox * nsplit < want && nsplit < 16) nsplit *= 2;
+    x.nsplit = nsplit;
+    if (nsplit > 1) {
+      int outlen = helm ? (x.Nout + 1) * (x.Nout + 1) : (x.Nout + 1) * (x.Nout + 2) / 2;
+      WBFMM_TRY(partial.alloc((size_t)nsplit * x.nbox * 2 * outlen));
+      x.partial = partial.p;
+    }
+    launches += nsplit > 1 ? 2 : 1;
+    return helm ? launch_m2l<T, true>(x, tables, stream)
+                : launch_m2l<T, false>(x, tables, stream);
+  }
+
+  int l2l(int level) override {
+    if (level < 2 || level >= depth) return set_error(WBFMM_B200_E_ARG, "L2L level must be in [2, depth-1]");
+    WBFMM_TRY(build_operators());
+    XlateParams<T> d = xparams();
+    d.level = level + 1;
+    d.nbox = (int64_t)1 << (3 * level);
+    d.Nin = cfg.order_r[level]; d.Nout = cfg.order_r[level + 1];
+    d.cin = mpr[level].p; d.cout = mpr[level + 1].p;
+    d.coax = helm ? ss_ptr[level + 1] : nullptr;
+    d.width = (T)width(level + 1);
+    launches++;
+    return helm ? launch_l2l<T, true>(d, tables, stream)
+                : launch_l2l<T, false>(d, tables, stream);
+  }
+
+  EvalParams<T> eparams() {
+    EvalParams<T> e;
+    memset(&e, 0, sizeof(e));
+    e.ntgt = ntgt; e.level = depth; e.N = cfg.order_r[depth];
+    e.x0 = cfg.x0[0]; e.y0 = cfg.x0[1]; e.z0 = cfg.x0[2]; e.wb = width(depth);
+    e.k = (T)cfg.k;
+    e.tx = tx.p; e.ty = ty.p; e.tz = tz.p;
+    e.tperm = tperm.p; e.tbox = tbox.p; e.tstart = tstart.p; e.tcount = tcount.p;
+    e.box_i = box_i[depth].p; e.box_n = box_n[depth].p;
+    e.x = sx.p; e.y = sy.p; e.z = sz.p;
+    e.q = have_q ? sq.p : nullptr; e.dip = have_dip ? sdip.p : nullptr;
+    e.nx = snx.p; e.ny = sny.p; e.nz = snz.p;
+    e.mpr = mpr[depth].p;
+    e.pot = (cfg.field & eval_field & WBFMM_B200_POTENTIAL) ? pot.p : nullptr;
+    e.grad = (cfg.field & eval_field & WBFMM_B200_GRADIENT) ? grad.p : nullptr;
+    e.nbox = (int64_t)1 << (3 * depth);
+    e.compensated = sizeof(T) == 4 ? 1 : 0;
+    return e;
+  }
+
+  int evaluate() override {
+    if (ntgt <= 0) return set_error(WBFMM_B200_E_STATE, "set_targets first");
+    EvalParams<T> e = eparams();
+    launches += eval_neighbours ? 2 : 1;
+    if (helm) {
+      WBFMM_TRY((launch_l2p<T, true>(e, stream)));
+      return eval_neighbours ? launch_p2p<T, true>(e, stream) : 0;
+    }
+    WBFMM_TRY((launch_l2p<T, false>(e, stream)));
+    return eval_neighbours ? launch_p2p<T, false>(e, stream) : 0;
+  }
+
+  int run() override {
+    if (nsrc <= 0 || ntgt <= 0) return set_error(WBFMM_B200_E_STATE, "sources and targets must be set");
+    WBFMM_TRY(build_operators());
+    cudaEventRecord(ev[4], stream);
+    WBFMM_TRY(leaf_expansions());
+    cudaEventRecord(ev[5], stream);
+    for (int l = depth; l >= 3; l--) WBFMM_TRY(upward(l));
+    cudaEventRecord(ev[6], stream);
+    for (int l = 2; l <= depth; l++) WBFMM_TRY(downward(l));
+    cudaEventRecord(ev[7], stream);
+    WBFMM_TRY(evaluate());
+    cudaEventRecord(ev[2], stream);
+    WBFMM_CUDA(cudaStreamSynchronize(stream));
+    float t;
+    if (cudaEventElapsedTime(&t, ev[0], ev[1]) == cudaSuccess) stage_ms[0] = t;
+    stage_ms[1] = 0;
+    if (cudaEventElapsedTime(&t, ev[4], ev[5]) == cudaSuccess) stage_ms[2] = t;
+    if (cudaEventElapsedTime(&t, ev[5], ev[6]) == cudaSuccess) stage_ms[3] = t;
+    if (cudaEventElapsedTime(&t, ev[6], ev[7]) == cudaSuccess) stage_ms[4] = t;
+    if (cudaEventElapsedTime(&t, ev[7], ev[2]) == cudaSuccess) stage_ms[5] = t;
+    cudaGetLastError();
+    return 0;
+  }
+
+  // Served form: every pass queued on the stream, no host wait.
+  int run_async() {
+    if (nsrc <= 0 || ntgt <= 0) return set_error(WBFMM_B200_E_STATE, "sources and targets must be set");
+    WBFMM_TRY(build_operators());
+    WBFMM_TRY(leaf_expansions());
+    for (int l = depth; l >= 3; l--) WBFMM_TRY(upward(l));
+    for (int l = 2; l <= depth; l++) WBFMM_TRY(downward(l));
+    return evaluate();
+  }
+
+  // Served form: queue the copies of the fields (FP64, original target
+  // order) into pinned host arrays, and of the domain-check flags.
+  int fetch_async(double* hpot, double* hgrad) {
+    const int w = helm ? 2 : 1;
+    const size_t np = hpot ? (size_t)ntgt * w : 0;
+    const size_t ng = hgrad ? (size_t)ntgt * 3 * w : 0;
+    if (np && !pot.p) return set_error(WBFMM_B200_E_STATE, "potential was not requested");
+    if (ng && !grad.p) return set_error(WBFMM_B200_E_STATE, "gradient was not requested");
+    const double* fp = (const double*)pot.p;
+    const double* fg = (const double*)grad.p;
+    if (sizeof(T) != 8) {
+      WBFMM_TRY(out64.alloc(np + ng));
+      if (np) k_widen<T><<<(unsigned)((np + 255) / 256), 256, 0, stream>>>(pot.p, out64.p, (int64_t)np);
+      if (ng) k_widen<T><<<(unsigned)((ng + 255) / 256), 256, 0, stream>>>(grad.p, out64.p + np, (int64_t)ng);
+      fp = out64.p;
+      fg = out64.p + np;
+      launches += (np ? 1 : 0) + (ng ? 1 : 0);
+    }
+    if (np) WBFMM_CUDA(cudaMemcpyAsync(hpot, fp, sizeof(double) * np, cudaMemcpyDeviceToHost, stream));
+    if (ng) WBFMM_CUDA(cudaMemcpyAsync(hgrad, fg, sizeof(double) * ng, cudaMemcpyDeviceToHost, stream));
+    if (async_checks && hflag)
+      WBFMM_CUDA(cudaMemcpyAsync(hflag, flag.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, stream));
+    return 0;
+  }
+
+  // Served form, after the stream has drained: the deferred domain checks.
+  int check_flags() const {
+    return async_checks && hflag ? domain_error(hflag[0], hflag[1]) : 0;
+  }
+
+  // ------------------------------------------------------------ outputs
+  int fetch(DBuf<T>& src, size_t n, double* dst, int on_device) {
+    const double* from = nullptr;
+    if (sizeof(T) == 8) {
+      from = (const double*)src.p;
+    } else {
+      WBFMM_TRY(out64.alloc(n));
+      k_widen<T><<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(src.p, out64.p, (int64_t)n);
+      from = out64.p;
+    }
+    WBFMM_CUDA(cudaMemcpyAsync(dst, from, sizeof(double) * n,
+                               on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                               stream));
+    WBFMM_CUDA(cudaStreamSynchronize(stream));
+    return 0;
+  }
+
+  int get_field(double* po, double* go, int on_device) override {
+    const int w = helm ? 2 : 1;
+    if (po) {
+      if (!pot.p) return set_error(WBFMM_B200_E_STATE, "potential was not requested");
+      WBFMM_TRY(fetch(pot, (size_t)ntgt * w, po, on_device));
+    }
+    if (go) {
+      if (!grad.p) return set_error(WBFMM_B200_E_STATE, "gradient was not requested");
+      WBFMM_TRY(fetch(grad, (size_t)ntgt * 3 * w, go, on_device));
+    }
+    return 0;
+  }
+
+  int get_tree(uint32_t* ipo, uint32_t* bi, uint32_t* bn, int level) override {
+    if (nsrc <= 0) return set_error(WBFMM_B200_E_STATE, "no tree");
+    if (level < 0 || level > depth) return set_error(WBFMM_B200_E_ARG, "bad level");
+    size_t nb = (size_t)1 << (3 * level);
+    if (ipo) WBFMM_CUDA(cudaMemcpyAsync(ipo, ip.p, sizeof(uint32_t) * nsrc, cudaMemcpyDeviceToHost, stream));
+    if (bi) WBFMM_CUDA(cudaMemcpyAsync(bi, box_i[level].p, sizeof(uint32_t) * nb, cudaMemcpyDeviceToHost, stream));
+    if (bn) WBFMM_CUDA(cudaMemcpyAsync(bn, box_n[level].p, sizeof(uint32_t) * nb, cudaMemcpyDeviceToHost, stream));
+    WBFMM_CUDA(cudaStreamSynchronize(stream));
+    return 0;
+  }
+
+  int get_coefficients(int level, double* ms, double* mr) override {
+    if (level < 1 || level > depth) return set_error(WBFMM_B200_E_ARG, "bad level");
+    if (ms) WBFMM_TRY(fetch(mps[level], level_len(level, cfg.order_s[level]), ms, 0));
+    if (mr) WBFMM_TRY(fetch(mpr[level], level_len(level, cfg.order_r[level]), mr, 0));
+    return 0;
+  }
+
+  void invalidate_operators() override { ops_ready = false; }
+  void set_m2l_kernel(int lanes) override { use_lanes = lanes != 0; }
+  void set_p2m_accumulate(int on) override { p2m_accumulate = on != 0; }
+  void set_evaluation(int field, int neighbours) override {
+    eval_field = field;
+    eval_neighbours = neighbours != 0;
+  }
+  int adopt_coefficients(int level, void* ms, void* mr) override {
+    if (level < 1 || level > depth) return set_error(WBFMM_B200_E_ARG, "bad level");
+    if (ms) mps[level].adopt((T*)ms, level_len(level, cfg.order_s[level]), cfg.managed != 0);
+    if (mr) mpr[level].adopt((T*)mr, level_len(level, cfg.order_r[level]), cfg.managed != 0);
+    return 0;
+  }
+
+  int coefficient_pointers(int level, void** ms, void** mr) override {
+    if (level < 1 || level > depth) return set_error(WBFMM_B200_E_ARG, "bad level");
+    if (ms) *ms = mps[level].p;
+    if (mr) *mr = mpr[level].p;
+    return 0;
+  }
+};
+
+}  // namespace wbfmm

@@ -17,6 +17,7 @@
 
 #include <vector>
 
+#include "../../include/wbfmm_b200.h"
 #include "tables.h"
 
 namespace wbfmm {
@@ -62,13 +63,18 @@ void build_shift_geometry(ShiftGeometry* g) {
 
 // ------------------------------------------------------ rotation tables
 // One block per theta.  scratch holds rot_count(2N+1) doubles per block.
-__global__ void k_rotation_tables(const double* __restrict__ thetas, int N,
+// small per-launch argument lists travel by value in the kernel parameters
+struct Vals64 {
+  double v[64];
+};
+
+__global__ void k_rotation_tables(const Vals64 thetas, int N,
                                   double* __restrict__ H, int64_t hstride,
                                   double* __restrict__ scratch,
                                   int64_t sstride) {
   const int it = blockIdx.x;
   double* h = scratch + (int64_t)it * sstride;
-  const double th = thetas[it], C = cos(th), S = sin(th);
+  const double th = thetas.v[it], C = cos(th), S = sin(th);
   const int NN = 2 * N;
   extern __shared__ double sm[];
   double* Pa = sm;                 // NN + 3 entries each
@@ -127,19 +133,17 @@ __global__ void k_rotation_tables(const double* __restrict__ thetas, int N,
 int generate_rotation_tables(const std::vector<double>& thetas, int N,
                              double* dH, int64_t hstride, cudaStream_t s) {
   int nt = (int)thetas.size();
-  double* dth = nullptr;
+  if (nt > 64) return set_error(WBFMM_B200_E_ARG, "too many rotation angles");
+  Vals64 th;
+  memset(&th, 0, sizeof(th));
+  for (int i = 0; i < nt; i++) th.v[i] = thetas[i];
   double* scratch = nullptr;
   int64_t sstride = rot_count(2 * N + 1) + 16;
-  WBFMM_CUDA(cudaMalloc(&dth, sizeof(double) * nt));
-  WBFMM_CUDA(cudaMalloc(&scratch, sizeof(double) * sstride * nt));
-  WBFMM_CUDA(cudaMemcpyAsync(dth, thetas.data(), sizeof(double) * nt,
-                             cudaMemcpyHostToDevice, s));
+  WBFMM_CUDA(cudaMallocAsync(&scratch, sizeof(double) * sstride * nt, s));
   size_t smem = sizeof(double) * 2 * (2 * N + 3);
-  k_rotation_tables<<<nt, 256, smem, s>>>(dth, N, dH, hstride, scratch, sstride);
+  k_rotation_tables<<<nt, 256, smem, s>>>(th, N, dH, hstride, scratch, sstride);
   WBFMM_CUDA(cudaGetLastError());
-  WBFMM_CUDA(cudaStreamSynchronize(s));
-  cudaFree(dth);
-  cudaFree(scratch);
+  WBFMM_CUDA(cudaFreeAsync(scratch, s));
   return 0;
 }
 
@@ -148,13 +152,13 @@ int generate_rotation_tables(const std::vector<double>& thetas, int N,
 // negative (reverses the sense of the translation).  The table keeps the
 // entries l <= L (coax_idx(L,L,L) < coax_count(L)); scratch holds the
 // recursion's work range l <= 2L+1.
-__global__ void k_coaxial_tables(const double* __restrict__ krs, int L, int nc,
+__global__ void k_coaxial_tables(const Vals64 krs, int L, int nc,
                                  double* __restrict__ out, int64_t ostride,
                                  double* __restrict__ scratch,
                                  int64_t sstride) {
   const int it = blockIdx.x;
   double* cf = scratch + (int64_t)it * sstride;
-  double kr = krs[it];
+  double kr = krs.v[it];
   int sw = 1;
   if (kr < 0) { kr = -kr; sw = -1; }
   const int LL = 2 * L + 2;
@@ -244,19 +248,17 @@ int generate_coaxial_tables(const std::vector<double>& krs, int L, int nc,
                             double* dout, int64_t ostride, cudaStream_t s) {
   int nt = (int)krs.size();
   if (nt == 0) return 0;
-  double* dk = nullptr;
+  if (nt > 64) return set_error(WBFMM_B200_E_ARG, "too many coaxial distances");
+  Vals64 kv;
+  memset(&kv, 0, sizeof(kv));
+  for (int i = 0; i < nt; i++) kv.v[i] = krs[i];
   double* scratch = nullptr;
   int LL = 2 * L + 2;
   int64_t sstride = ((int64_t)coax_idx(LL, LL, LL) + 2) * nc;
-  WBFMM_CUDA(cudaMalloc(&dk, sizeof(double) * nt));
-  WBFMM_CUDA(cudaMalloc(&scratch, sizeof(double) * sstride * nt));
-  WBFMM_CUDA(cudaMemcpyAsync(dk, krs.data(), sizeof(double) * nt,
-                             cudaMemcpyHostToDevice, s));
-  k_coaxial_tables<<<nt, 128, 0, s>>>(dk, L, nc, dout, ostride, scratch, sstride);
+  WBFMM_CUDA(cudaMallocAsync(&scratch, sizeof(double) * sstride * nt, s));
+  k_coaxial_tables<<<nt, 128, 0, s>>>(kv, L, nc, dout, ostride, scratch, sstride);
   WBFMM_CUDA(cudaGetLastError());
-  WBFMM_CUDA(cudaStreamSynchronize(s));
-  cudaFree(dk);
-  cudaFree(scratch);
+  WBFMM_CUDA(cudaFreeAsync(scratch, s));
   return 0;
 }
 

@@ -36,6 +36,12 @@ __global__ void k_point_keys(const double* __restrict__ pts, int64_t pstr,
   uint32_t xi = (uint32_t)(__ddiv_rn(__dsub_rn(p[0], x0), D) * 1048576.0);
   uint32_t yi = (uint32_t)(__ddiv_rn(__dsub_rn(p[1], y0), D) * 1048576.0);
   uint32_t zi = (uint32_t)(__ddiv_rn(__dsub_rn(p[2], z0), D) * 1048576.0);
+  // Points strictly inside the cube give 20-bit coordinates.  Anything else
+  // (rejected by the domain check, which the served form reads back only
+  // after the solve) is clamped so every key stays below 2^60 and every box
+  // index derived from it inside its level's array.
+  const uint32_t top = (1u << 20) - 1;
+  xi = xi < top ? xi : top; yi = yi < top ? yi : top; zi = zi < top ? zi : top;
   keys[i] = morton(xi, yi, zi);
   vals[i] = (uint32_t)i;
 }

@@ -49,6 +49,15 @@ class Config(C.Structure):
     ]
 
 
+class Request(C.Structure):
+    _fields_ = [
+        ("cfg", Config), ("nsrc", C.c_int), ("xs", C.c_void_p),
+        ("q", C.c_void_p), ("normals", C.c_void_p), ("dipoles", C.c_void_p),
+        ("ntgt", C.c_int), ("xt", C.c_void_p), ("pot", C.c_void_p),
+        ("grad", C.c_void_p), ("arrival", C.c_double),
+    ]
+
+
 _lib = None
 
 
@@ -92,6 +101,17 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "wbfmm_b200_set_m2l_kernel": (ip, [vp, ip]),
         "wbfmm_b200_l2l": (ip, [vp, ip]),
         "wbfmm_b200_direct": (ip, [ip, C.c_double, ip, vp, vp, vp, vp, ip, vp, vp, vp, ip]),
+        "wbfmm_b200_fp32_range_ok": (ip, [C.POINTER(Config)]),
+        "wbfmm_b200_server_create": (ip, [C.POINTER(vp), ip, C.c_int64]),
+        "wbfmm_b200_server_destroy": (ip, [vp]),
+        "wbfmm_b200_server_clock": (C.c_double, [vp]),
+        "wbfmm_b200_server_submit": (ip, [vp, C.POINTER(Request), C.POINTER(C.c_int64)]),
+        "wbfmm_b200_server_poll": (ip, [vp, C.c_int64]),
+        "wbfmm_b200_server_wait": (ip, [vp, C.c_int64]),
+        "wbfmm_b200_server_times": (ip, [vp, C.c_int64, dp]),
+        "wbfmm_b200_server_forget": (ip, [vp, C.c_int64]),
+        "wbfmm_b200_server_drain": (ip, [vp]),
+        "wbfmm_b200_server_stats": (ip, [vp, C.POINTER(C.c_int64)]),
     }
     for name, (res, args) in sigs.items():
         f = getattr(lib, name)
@@ -323,3 +343,102 @@ def direct(problem, xs, q, xt, k=0.0, normals=None, dipoles=None, pot=True,
 
 def device_count() -> int:
     return int(load_library().wbfmm_b200_device_count())
+
+
+def fp32_range_ok(cfg: "SolverConfig") -> bool:
+    """Whether the FP32 form keeps this configuration inside the FP32 range."""
+    c = cfg.to_c()
+    return bool(load_library().wbfmm_b200_fp32_range_ok(C.byref(c)))
+
+
+def footprint(cfg: "SolverConfig", ns: int, nt: int) -> int:
+    """Device bytes a solve of this configuration holds (admission estimate)."""
+    c = cfg.to_c()
+    return int(load_library().wbfmm_b200_footprint(C.byref(c), int(ns), int(nt)))
+
+
+class Server:
+    """Served form: continuous batching of independent solves on one GPU
+    (wbfmm_b200_server_* in include/wbfmm_b200.h).
+
+    ``submit`` takes a :class:`wbfmm_b200.workloads.Problem` and a precision
+    and returns a ticket; the host arrays of a request are held here until
+    the request completes, and its fields land in arrays this object owns.
+    """
+
+    def __init__(self, slots: int = 16, hbm_budget: int = 150 * 10**9):
+        self._lib = load_library()
+        self._h = C.c_void_p()
+        _check(self._lib.wbfmm_b200_server_create(C.byref(self._h), int(slots), int(hbm_budget)))
+        self._held = {}
+
+    def close(self):
+        if self._h:
+            self._lib.wbfmm_b200_server_destroy(self._h)
+            self._h = C.c_void_p()
+            self._held.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def clock(self) -> float:
+        return float(self._lib.wbfmm_b200_server_clock(self._h))
+
+    def submit(self, p, precision=FP32, field=POTENTIAL | GRADIENT,
+               arrival: float = 0.0) -> int:
+        cfg = SolverConfig.from_problem(p, precision, field)
+        w = 2 if p.problem == HELMHOLTZ else 1
+        xs = _host(p.xs)
+        xt = xs if p.targets_are_sources else _host(p.xt)
+        q, nrm, dip = _host(p.q), _host(p.normals), _host(p.dipoles)
+        nt = xt.shape[0]
+        pot = np.zeros(nt * w) if field & POTENTIAL else None
+        grad = np.zeros(nt * 3 * w) if field & GRADIENT else None
+        r = Request(cfg.to_c(), xs.shape[0], _addr(xs), _addr(q), _addr(nrm),
+                    _addr(dip), nt, _addr(xt), _addr(pot), _addr(grad),
+                    float(arrival))
+        t = C.c_int64()
+        _check(self._lib.wbfmm_b200_server_submit(self._h, C.byref(r), C.byref(t)))
+        self._held[t.value] = (xs, xt, q, nrm, dip, pot, grad)
+        return t.value
+
+    def done(self, ticket: int) -> bool:
+        rc = self._lib.wbfmm_b200_server_poll(self._h, ticket)
+        if rc < 0:
+            _check(rc)
+        return rc == 1
+
+    def wait(self, ticket: int):
+        """Block until the request completes; return (pot, grad)."""
+        _check(self._lib.wbfmm_b200_server_wait(self._h, ticket))
+        held = self._held[ticket]
+        return held[5], held[6]
+
+    def times(self, ticket: int):
+        """(arrival, start, end) on the server clock, seconds."""
+        t = np.zeros(3)
+        _check(self._lib.wbfmm_b200_server_times(self._h, ticket, t.ctypes.data_as(C.POINTER(C.c_double))))
+        return tuple(float(x) for x in t)
+
+    def forget(self, ticket: int):
+        _check(self._lib.wbfmm_b200_server_forget(self._h, ticket))
+        self._held.pop(ticket, None)
+
+    def drain(self):
+        _check(self._lib.wbfmm_b200_server_drain(self._h))
+
+    def stats(self) -> dict:
+        a = (C.c_int64 * 6)()
+        _check(self._lib.wbfmm_b200_server_stats(self._h, a))
+        keys = ("completed", "peak_bytes_in_flight", "peak_solves_in_flight",
+                "table_cache_hits", "table_cache_misses", "table_cache_bytes")
+        return dict(zip(keys, (int(x) for x in a)))

@@ -151,3 +151,64 @@ def laplace_clusters(n: int = 16_000_000, depth: int = 8, order: int = 10,
 def subsample(rng_seed: int, n_total: int, m: int) -> np.ndarray:
     rng = np.random.default_rng(rng_seed)
     return np.sort(rng.choice(n_total, size=min(m, n_total), replace=False))
+
+
+# ----------------------------------------------------------- serving stream
+# Orders for a 1e-6 relative-L2 field error, from the FP64-vs-direct-sum
+# calibration of this engine (uniform cube and sphere surface, 1e5 points,
+# mean leaf occupancy ~64): Laplace p = 14 gives 6e-8 (potential) and 5e-7
+# (gradient); Helmholtz p_l = max(14, kw + 1.8*6^(2/3)*(kw)^(1/3)) gives at
+# most 1.2e-7 and 5e-7 for k in [1, 30].
+SERVE_LAPLACE_ORDER = 14
+SERVE_HELMHOLTZ_FLOOR = 14
+
+
+def serve_depth(n: int) -> int:
+    """Depth for a mean leaf occupancy of about 64 points (at least 2)."""
+    return int(min(8, max(2, round(math.log(max(n, 1) / 64.0, 8)))))
+
+
+def serve_request(rng: np.random.Generator, n: int, helmholtz: bool, k: float,
+                  sphere: bool, name: str = "request") -> Problem:
+    """One request of the serving stream: targets = sources."""
+    if sphere:
+        v = rng.standard_normal((n, 3))
+        v /= np.linalg.norm(v, axis=1, keepdims=True)
+        xs = 0.45 * v
+    else:
+        xs = rng.uniform(-0.5, 0.5, size=(n, 3))
+    problem = HELMHOLTZ if helmholtz else LAPLACE
+    q = rng.standard_normal(2 * n if helmholtz else n)
+    depth = serve_depth(n)
+    p = Problem(name, problem, depth, [0] * (depth + 1), [0] * (depth + 1),
+                k if helmholtz else 0.0, xs, q, xs, targets_are_sources=True)
+    p = _finish(p)
+    for lv in range(1, depth + 1):
+        if helmholtz:
+            o = helmholtz_order(k, p.D / 2 ** lv, lo=SERVE_HELMHOLTZ_FLOOR, hi=60)
+        else:
+            o = SERVE_LAPLACE_ORDER
+        p.order_s[lv] = p.order_r[lv] = o
+    return p
+
+
+def serving_stream(n_requests: int = 4096, seed: int = 4, n_lo: float = 1e3,
+                   n_hi: float = 3e5):
+    """Yield the requests of the mixed serving stream: N log-uniform in
+    [n_lo, n_hi], half Laplace and half Helmholtz with k ~ U[1, 30], sources
+    in the cube or on the r = 0.45 sphere (fair coin), N(0,1) strengths
+    (complex for Helmholtz), targets = sources."""
+    rng = np.random.default_rng(seed)
+    lo, hi = math.log(n_lo), math.log(n_hi)
+    for i in range(n_requests):
+        n = int(round(math.exp(rng.uniform(lo, hi))))
+        helm = bool(rng.random() < 0.5)
+        k = float(rng.uniform(1.0, 30.0)) if helm else 0.0
+        sphere = bool(rng.random() < 0.5)
+        yield serve_request(rng, n, helm, k, sphere, name=f"request{i}")
+
+
+def poisson_arrivals(n: int, rate: float, seed: int = 104) -> np.ndarray:
+    """Arrival times (s) of a Poisson process of `rate` requests per second."""
+    rng = np.random.default_rng(seed)
+    return np.cumsum(rng.exponential(1.0 / rate, size=n))
