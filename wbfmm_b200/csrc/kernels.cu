@@ -541,136 +541,181 @@ struct Acc {
   __device__ __forceinline__ T value() const { return s + c; }
 };
 
+// One CTA per target leaf box.  The sources of the 27 neighbour boxes (a
+// virtual list, box by box) are staged through shared memory in tiles of
+// kP2PTile.  Each target is swept by a group of G threads (G a power of two,
+// as large as the box's target count leaves room for, at most 32): thread g
+// of the group takes tile entries g, g+G, ..., accumulating in registers in
+// a fixed order (compensated in FP32), and the group's partial sums are
+// added by shuffles at the end.  Pair kernels and the r > 1e-6 cutoff follow
+// src/local.c:32-262 and src/local-laplace.c:400-523, 1091-1227.
+constexpr int kP2PTile = 128;
+
 template <typename T, bool HELM>
-__global__ void k_p2p(EvalParams<T> p) {
-  __shared__ uint32_t s_st[8][27], s_pref[8][28];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int nw = blockDim.x >> 5;
-  const int64_t b = (int64_t)blockIdx.x * nw + warp;
-  if (b >= p.nbox) return;
+struct P2PTile {
+  double x[kP2PTile], y[kP2PTile], z[kP2PTile];
+  T q[kP2PTile * (HELM ? 2 : 1)];
+  T d[kP2PTile * (HELM ? 2 : 1)];
+  T nx[kP2PTile], ny[kP2PTile], nz[kP2PTile];
+};
+
+template <typename T, bool HELM>
+__global__ void __launch_bounds__(kP2PTile)
+k_p2p(EvalParams<T> p) {
+  __shared__ P2PTile<T, HELM> tl;
+  __shared__ uint32_t s_st[27], s_pref[28];
+  const int64_t b = blockIdx.x;
   const uint32_t tc = p.tcount[b];
   if (tc == 0) return;
-  uint32_t bi, bj, bk;
-  demorton((uint64_t)b, &bi, &bj, &bk);
-  const int nside = 1 << p.level;
-  uint32_t cnt = 0, st = 0;
-  if (lane < 27) {
-    int ii = (int)bi + lane / 9 - 1, jj = (int)bj + (lane / 3) % 3 - 1,
-        kk = (int)bk + lane % 3 - 1;
-    if (ii >= 0 && jj >= 0 && kk >= 0 && ii < nside && jj < nside && kk < nside) {
-      uint64_t nb = morton((uint32_t)ii, (uint32_t)jj, (uint32_t)kk);
-      cnt = p.box_n[nb];
-      st = p.box_i[nb];
+  const int tid = threadIdx.x;
+  if (tid < 32) {
+    uint32_t bi, bj, bk;
+    demorton((uint64_t)b, &bi, &bj, &bk);
+    const int nside = 1 << p.level;
+    uint32_t cnt = 0, st = 0;
+    if (tid < 27) {
+      int ii = (int)bi + tid / 9 - 1, jj = (int)bj + (tid / 3) % 3 - 1,
+          kk = (int)bk + tid % 3 - 1;
+      if (ii >= 0 && jj >= 0 && kk >= 0 && ii < nside && jj < nside && kk < nside) {
+        uint64_t nb = morton((uint32_t)ii, (uint32_t)jj, (uint32_t)kk);
+        cnt = p.box_n[nb];
+        st = p.box_i[nb];
+      }
     }
+    uint32_t incl = cnt;
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (tid >= o) incl += v;
+    }
+    if (tid < 27) { s_st[tid] = st; s_pref[tid] = incl - cnt; }
+    if (tid == 26) s_pref[27] = incl;
   }
-  uint32_t incl = cnt;
-  for (int o = 1; o < 32; o <<= 1) {
-    uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
-    if (lane >= o) incl += v;
-  }
-  const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
-  if (lane < 27) { s_st[warp][lane] = st; s_pref[warp][lane] = incl - cnt; }
-  __syncwarp();
+  __syncthreads();
+  const uint32_t total = s_pref[27];
   const T f4pi = T(0.25 / kPi);
   const T rc2 = T(kCutoffRadius * kCutoffRadius);
   const bool comp = p.compensated != 0;
   const T k = p.k;
-  for (uint32_t tt = 0; tt < tc; tt++) {
-    const uint32_t jt = p.tstart[b] + tt;
+  const bool hq = p.q != nullptr, hd = p.dip != nullptr;
+  const bool want_pot = p.pot != nullptr, want_grad = p.grad != nullptr;
+  int G = 32;
+  while (G > 1 && (uint32_t)(kP2PTile / G) < tc) G >>= 1;
+  const int gl = tid & (G - 1), ti = tid / G, tpp = kP2PTile / G;
+  for (uint32_t t0 = 0; t0 < tc; t0 += tpp) {
+    const bool active = t0 + ti < tc;
+    const uint32_t jt = p.tstart[b] + t0 + (active ? ti : 0);
     const double x = p.tx[jt], y = p.ty[jt], z = p.tz[jt];
     Acc<T> a[8];
-    for (uint32_t f = lane; f < total; f += 32) {
-      int l = 0;
-      while (l < 26 && s_pref[warp][l + 1] <= f) l++;
-      const uint32_t s = s_st[warp][l] + (f - s_pref[warp][l]);
-      // separation formed in FP64, the rest in T
-      const T rx = (T)(x - p.x[s]), ry = (T)(y - p.y[s]), rz = (T)(z - p.z[s]);
-      const T r2 = rx * rx + ry * ry + rz * rz;
-      if (!(r2 > rc2)) continue;
-      const T r = sqrt(r2);
-      if (HELM) {
-        const T kr = k * r;
-        T sn, cs;
-        sincos(kr, &sn, &cs);
-        const T h0r = sn / kr, h0i = -cs / kr;
-        const T h1r = h0r / kr + h0i, h1i = h0i / kr - h0r;
-        T qr = T(0), qi = T(0);
-        if (p.q) { qr = p.q[2 * s]; qi = p.q[2 * s + 1]; }
-        if (p.pot) {
-          T fr = (h0r * qr - h0i * qi) * f4pi, fi = (h0i * qr + h0r * qi) * f4pi;
-          if (p.dip) {
-            T nr = (rx * p.nx[s] + ry * p.ny[s] + rz * p.nz[s]) / r;
-            T dr = p.dip[2 * s] * nr, di = p.dip[2 * s + 1] * nr;
-            fr -= k * (h1r * dr - h1i * di) * f4pi;
-            fi -= k * (h1r * di + h1i * dr) * f4pi;
-          }
-          a[0].add(fr, comp); a[1].add(fi, comp);
+    for (uint32_t f0 = 0; f0 < total; f0 += kP2PTile) {
+      const uint32_t f = f0 + tid;
+      __syncthreads();
+      if (f < total) {
+        int l = 0;
+        while (l < 26 && s_pref[l + 1] <= f) l++;
+        const uint32_t s = s_st[l] + (f - s_pref[l]);
+        tl.x[tid] = p.x[s]; tl.y[tid] = p.y[s]; tl.z[tid] = p.z[s];
+        if (HELM) {
+          tl.q[2 * tid] = hq ? p.q[2 * s] : T(0);
+          tl.q[2 * tid + 1] = hq ? p.q[2 * s + 1] : T(0);
+          if (hd) { tl.d[2 * tid] = p.dip[2 * s]; tl.d[2 * tid + 1] = p.dip[2 * s + 1]; }
+        } else {
+          tl.q[tid] = hq ? p.q[s] : T(0);
+          if (hd) tl.d[tid] = p.dip[s];
         }
-        if (p.grad) {
-          const T ar = -k * (h1r * qr - h1i * qi) * f4pi / r;
-          const T ai = -k * (h1r * qi + h1i * qr) * f4pi / r;
-          T gr[3] = {ar * rx, ar * ry, ar * rz}, gi[3] = {ai * rx, ai * ry, ai * rz};
-          if (p.dip) {
-            const T nxs = p.nx[s], nys = p.ny[s], nzs = p.nz[s];
-            const T nr = rx * nxs + ry * nys + rz * nzs;
-            const T dpr = h0r - T(2) * h1r / kr, dpi = h0i - T(2) * h1i / kr;
-            const T dr = p.dip[2 * s], di = p.dip[2 * s + 1];
-            const T rv[3] = {rx, ry, rz}, nv[3] = {nxs, nys, nzs};
-            for (int c = 0; c < 3; c++) {
-              T ur = dpr * k * nr * rv[c] / r2 + h1r * (nv[c] / r - nr * rv[c] / (r2 * r));
-              T ui = dpi * k * nr * rv[c] / r2 + h1i * (nv[c] / r - nr * rv[c] / (r2 * r));
-              gr[c] += -k * (ur * dr - ui * di) * f4pi;
-              gi[c] += -k * (ur * di + ui * dr) * f4pi;
+        if (hd) { tl.nx[tid] = p.nx[s]; tl.ny[tid] = p.ny[s]; tl.nz[tid] = p.nz[s]; }
+      }
+      __syncthreads();
+      if (!active) continue;
+      const int nt = (int)min((uint32_t)kP2PTile, total - f0);
+      for (int j = gl; j < nt; j += G) {
+        // separation formed in FP64, the rest in T
+        const T rx = (T)(x - tl.x[j]), ry = (T)(y - tl.y[j]), rz = (T)(z - tl.z[j]);
+        const T r2 = rx * rx + ry * ry + rz * rz;
+        if (!(r2 > rc2)) continue;
+        const T r = sqrt(r2);
+        const T ir = T(1) / r;
+        if (HELM) {
+          const T kr = k * r, ikr = ir / k;
+          T sn, cs;
+          sincos(kr, &sn, &cs);
+          const T h0r = sn * ikr, h0i = -cs * ikr;
+          const T h1r = h0r * ikr + h0i, h1i = h0i * ikr - h0r;
+          const T qr = tl.q[2 * j], qi = tl.q[2 * j + 1];
+          if (want_pot) {
+            T fr = (h0r * qr - h0i * qi) * f4pi, fi = (h0i * qr + h0r * qi) * f4pi;
+            if (hd) {
+              T nr = (rx * tl.nx[j] + ry * tl.ny[j] + rz * tl.nz[j]) * ir;
+              T dr = tl.d[2 * j] * nr, di = tl.d[2 * j + 1] * nr;
+              fr -= k * (h1r * dr - h1i * di) * f4pi;
+              fi -= k * (h1r * di + h1i * dr) * f4pi;
             }
+            a[0].add(fr, comp); a[1].add(fi, comp);
           }
-          for (int c = 0; c < 3; c++) { a[2 + 2 * c].add(gr[c], comp); a[3 + 2 * c].add(gi[c], comp); }
-        }
-      } else {
-        const T q = p.q ? p.q[s] : T(0);
-        const T g = f4pi / r;
-        if (p.pot) {
-          T v = q;
-          if (p.dip) v += p.dip[s] * (rx * p.nx[s] + ry * p.ny[s] + rz * p.nz[s]) / r2;
-          a[0].add(v * g, comp);
-        }
-        if (p.grad) {
-          const T gq = -q * g / r2;
-          T gv[3] = {gq * rx, gq * ry, gq * rz};
-          if (p.dip) {
-            const T nxs = p.nx[s], nys = p.ny[s], nzs = p.nz[s];
-            const T nr = rx * nxs + ry * nys + rz * nzs;
-            const T ad = p.dip[s] * g / r2;
-            gv[0] += ad * (nxs - T(3) * nr * rx / r2);
-            gv[1] += ad * (nys - T(3) * nr * ry / r2);
-            gv[2] += ad * (nzs - T(3) * nr * rz / r2);
+          if (want_grad) {
+            const T ar = -k * (h1r * qr - h1i * qi) * f4pi * ir;
+            const T ai = -k * (h1r * qi + h1i * qr) * f4pi * ir;
+            T gr[3] = {ar * rx, ar * ry, ar * rz}, gi[3] = {ai * rx, ai * ry, ai * rz};
+            if (hd) {
+              const T nxs = tl.nx[j], nys = tl.ny[j], nzs = tl.nz[j];
+              const T nr = rx * nxs + ry * nys + rz * nzs;
+              const T dpr = h0r - T(2) * h1r * ikr, dpi = h0i - T(2) * h1i * ikr;
+              const T dr = tl.d[2 * j], di = tl.d[2 * j + 1];
+              const T rv[3] = {rx, ry, rz}, nv[3] = {nxs, nys, nzs};
+              const T ir2 = ir * ir;
+              for (int c = 0; c < 3; c++) {
+                T ur = dpr * k * nr * rv[c] * ir2 + h1r * (nv[c] * ir - nr * rv[c] * ir2 * ir);
+                T ui = dpi * k * nr * rv[c] * ir2 + h1i * (nv[c] * ir - nr * rv[c] * ir2 * ir);
+                gr[c] += -k * (ur * dr - ui * di) * f4pi;
+                gi[c] += -k * (ur * di + ui * dr) * f4pi;
+              }
+            }
+            for (int c = 0; c < 3; c++) { a[2 + 2 * c].add(gr[c], comp); a[3 + 2 * c].add(gi[c], comp); }
           }
-          a[1].add(gv[0], comp); a[2].add(gv[1], comp); a[3].add(gv[2], comp);
+        } else {
+          const T q = tl.q[j];
+          const T g = f4pi * ir;
+          const T ir2 = ir * ir;
+          if (want_pot) {
+            T v = q;
+            if (hd) v += tl.d[j] * (rx * tl.nx[j] + ry * tl.ny[j] + rz * tl.nz[j]) * ir2;
+            a[0].add(v * g, comp);
+          }
+          if (want_grad) {
+            const T gq = -q * g * ir2;
+            T gv[3] = {gq * rx, gq * ry, gq * rz};
+            if (hd) {
+              const T nxs = tl.nx[j], nys = tl.ny[j], nzs = tl.nz[j];
+              const T nr = rx * nxs + ry * nys + rz * nzs;
+              const T ad = tl.d[j] * g * ir2;
+              gv[0] += ad * (nxs - T(3) * nr * rx * ir2);
+              gv[1] += ad * (nys - T(3) * nr * ry * ir2);
+              gv[2] += ad * (nzs - T(3) * nr * rz * ir2);
+            }
+            a[1].add(gv[0], comp); a[2].add(gv[1], comp); a[3].add(gv[2], comp);
+          }
         }
       }
     }
+    // sum over the group (lanes of one warp; inactive groups hold zeros)
+    const int na = HELM ? 8 : 4;
+    T v[8];
+    for (int c = 0; c < na; c++) {
+      v[c] = a[c].value();
+      for (int o = 1; o < G; o <<= 1) v[c] += __shfl_xor_sync(0xffffffffu, v[c], o);
+    }
+    if (!active || gl != 0) continue;
     const uint32_t o = p.tperm[jt];
     if (HELM) {
-      if (p.pot) {
-        T v0 = warp_sum(a[0].value()), v1 = warp_sum(a[1].value());
-        if (lane == 0) { p.pot[2 * (size_t)o] += v0; p.pot[2 * (size_t)o + 1] += v1; }
+      if (want_pot) {
+        p.pot[2 * (size_t)o] += v[0];
+        p.pot[2 * (size_t)o + 1] += v[1];
       }
-      if (p.grad) {
-        for (int c = 0; c < 6; c++) {
-          T v = warp_sum(a[2 + c].value());
-          if (lane == 0) p.grad[6 * (size_t)o + c] += v;
-        }
-      }
+      if (want_grad)
+        for (int c = 0; c < 6; c++) p.grad[6 * (size_t)o + c] += v[2 + c];
     } else {
-      if (p.pot) {
-        T v = warp_sum(a[0].value());
-        if (lane == 0) p.pot[o] += v;
-      }
-      if (p.grad) {
-        for (int c = 0; c < 3; c++) {
-          T v = warp_sum(a[1 + c].value());
-          if (lane == 0) p.grad[3 * (size_t)o + c] += v;
-        }
-      }
+      if (want_pot) p.pot[o] += v[0];
+      if (want_grad)
+        for (int c = 0; c < 3; c++) p.grad[3 * (size_t)o + c] += v[1 + c];
     }
   }
 }
@@ -678,8 +723,7 @@ __global__ void k_p2p(EvalParams<T> p) {
 template <typename T, bool HELM>
 int launch_p2p(const EvalParams<T>& p, cudaStream_t s) {
   if (p.nbox <= 0 || p.ntgt <= 0) return 0;
-  const int nw = 8;
-  k_p2p<T, HELM><<<(unsigned)((p.nbox + nw - 1) / nw), nw * 32, 0, s>>>(p);
+  k_p2p<T, HELM><<<(unsigned)p.nbox, kP2PTile, 0, s>>>(p);
   WBFMM_CUDA(cudaGetLastError());
   return 0;
 }
