@@ -15,6 +15,17 @@ with pinned host buffers (host->device inputs and device->host field inside
 the timed region).  Accuracy of both forms is measured against the FP64
 direct sum on 10,000 random targets.
 
+`served` holds the served-versus-plain comparison on the mixed serving
+stream (N log-uniform in [1e3, 3e5], half Laplace / half Helmholtz with
+k ~ U[1, 30], cube or sphere sources, targets = sources, orders for 1e-6):
+batches of SERVE_BATCH requests, host arrays in and out.  The served form
+runs SERVE_SLOTS solves at once, FP32 wherever the FP32 range rule admits
+the request (FP64 otherwise); the plain form is one FP64 solve at a time on
+the same requests.  Both are timed per batch (submission of the first
+request to completion of the last, max over ranks); p50/p99 latency come
+from a Poisson-arrival run at 70% of the served throughput, and the served
+fields of sampled requests are checked against the FP64 direct sum.
+
 `--impl reference` times the reference's own CPU FMM (oracle/_ref, the
 unmodified reference sources) on the host cores, on a bounded sample of the
 workload (see `reference_sample`).
@@ -40,6 +51,9 @@ sys.path.insert(0, ROOT)
 
 METRIC = "FMM points/s + p99 latency: served FP32 vs plain FP64 GPU at rel-L2 err<=1e-6"
 WORKLOAD = "helmholtz_cube_1e6_k8_depth6"
+SERVE_SLOTS = 16
+SERVE_BATCH = 256
+SERVE_LATENCY_REQUESTS = 384
 
 
 # ---------------------------------------------------------------- helpers
@@ -213,6 +227,95 @@ def reference_arm(args, ws, rank):
     }))
 
 
+# ----------------------------------------------------- served stream
+def served_section(args, ws, rank, local):
+    """Served FP32 vs plain FP64 on batches of the mixed serving stream."""
+    from wbfmm_b200 import engine, workloads as W
+
+    nb = max(1, args.steps) + 1                      # one warm-up batch
+    gen = W.serving_stream(SERVE_BATCH * nb + SERVE_LATENCY_REQUESTS, seed=4 + 1000 * rank)
+    batches = [[next(gen) for _ in range(SERVE_BATCH)] for _ in range(nb)]
+    lat_reqs = [next(gen) for _ in range(SERVE_LATENCY_REQUESTS)]
+
+    def served_prec(p):
+        ok = engine.fp32_range_ok(engine.SolverConfig.from_problem(p))
+        return engine.FP32 if ok else engine.FP64
+
+    def plain_prec(p):
+        return engine.FP64
+
+    def run_batch(srv, batch, precf, keep=0):
+        dist_barrier(ws)
+        t0 = srv.clock()
+        tk = [srv.submit(p, precf(p)) for p in batch]
+        srv.drain()
+        span = max(srv.times(t)[2] for t in tk) - t0
+        kept = [tuple(a.copy() for a in srv.wait(t)) for t in tk[:keep]]
+        for t in tk:
+            srv.forget(t)
+        return dist_max(span, ws), kept
+
+    def run_latency(srv, reqs, precf, rate):
+        arr = W.poisson_arrivals(len(reqs), rate, seed=104 + rank)
+        base = srv.clock() + 0.02
+        tk = [srv.submit(p, precf(p), arrival=base + a) for p, a in zip(reqs, arr)]
+        srv.drain()
+        T = np.array([srv.times(t) for t in tk])
+        for t in tk:
+            srv.forget(t)
+        lat = T[:, 2] - T[:, 0]
+        return {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+                "mean_s": float(lat.mean()),
+                "throughput_points_per_s": float(sum(p.points for p in reqs) / (T[:, 2].max() - base))}
+
+    out = {}
+    kept = None
+    for name, slots, precf in (("plain_fp64", 1, plain_prec), ("served", SERVE_SLOTS, served_prec)):
+        with engine.Server(slots=slots) as srv:
+            run_batch(srv, batches[0], precf)                    # warm-up
+            spans = []
+            with ClockSampler(local) as clk:
+                for i, b in enumerate(batches[1:]):
+                    span, k = run_batch(srv, b, precf, keep=8 if (name == "served" and i == 0) else 0)
+                    spans.append(span)
+                    if k:
+                        kept = k
+            pts = sum(p.points for b in batches[1:] for p in b)
+            out[name] = {"points_per_s": ws * pts / sum(spans), "seconds": sum(spans),
+                         "requests": len(batches[1:]) * SERVE_BATCH, "slots": slots,
+                         "clocks": clk.summary(), "stats": srv.stats()}
+    rate_req = 0.7 * out["served"]["points_per_s"] / ws / np.mean(
+        [p.points for b in batches[1:] for p in b])
+    for name, slots, precf in (("served", SERVE_SLOTS, served_prec), ("plain_fp64", 1, plain_prec)):
+        with engine.Server(slots=slots) as srv:
+            out[name]["latency"] = run_latency(srv, lat_reqs, precf, rate_req)
+    # accuracy of served fields against the FP64 direct sum
+    worst, checked = 0.0, []
+    for p, (pot, grad) in zip(batches[1][:8], kept or []):
+        idx = W.subsample(105, p.ns, 1000)
+        dpot, dgrad = engine.direct(p.problem, p.xs, p.q, p.xs[idx], k=p.k)
+        w = 2 if p.problem == W.HELMHOLTZ else 1
+        ep = float(np.linalg.norm(pot.reshape(p.ns, w)[idx].ravel() - dpot) / np.linalg.norm(dpot))
+        eg = float(np.linalg.norm(grad.reshape(p.ns, 3 * w)[idx].ravel() - dgrad) / np.linalg.norm(dgrad))
+        worst = max(worst, ep, eg)
+        checked.append({"n": p.ns, "problem": "helmholtz" if p.problem == W.HELMHOLTZ else "laplace",
+                        "k": p.k, "fp32": served_prec(p) == engine.FP32,
+                        "pot_rel_l2": ep, "grad_rel_l2": eg})
+    fp32_frac = float(np.mean([served_prec(p) == engine.FP32 for b in batches[1:] for p in b]))
+    return {
+        "workload": "serving stream: N log-uniform [1e3, 3e5], 50% Laplace (p=14) / 50% "
+                    "Helmholtz (k~U[1,30], p_l=max(14, kw+1.8*6^(2/3)*(kw)^(1/3))), cube or "
+                    "r=0.45 sphere, targets = sources, depth for ~64 points per leaf",
+        "batch_requests": SERVE_BATCH, "batches": len(batches) - 1,
+        "served_fp32": out["served"], "plain_fp64": out["plain_fp64"],
+        "served_over_plain": out["served"]["points_per_s"] / out["plain_fp64"]["points_per_s"],
+        "fp32_fraction": fp32_frac,
+        "offered_load_requests_per_s": float(rate_req),
+        "accuracy": {"max_rel_l2": worst, "tolerance": 1e-6, "requests": checked},
+        "io": "host arrays in and out (copies inside the timed region)",
+    }
+
+
 # ----------------------------------------------------------- our arm
 def our_arm(args, ws, rank, local):
     import torch
@@ -353,6 +456,8 @@ def our_arm(args, ws, rank, local):
                    "sample": f"{rp.ns} points in a 1/8-volume sub-cube of the workload "
                              f"(depth {rp.depth}, same density, k and box widths), one solve"}
 
+    served = served_section(args, ws, rank, local) if not args.no_served else None
+
     v32 = ws * p.points / (f32["ms"] * 1e-3)
     v64 = ws * p.points / (f64["ms"] * 1e-3)
     line = {
@@ -369,6 +474,7 @@ def our_arm(args, ws, rank, local):
         "fp32_over_fp64": v32 / v64,
         "stages_ms": f32["stages"], "m2l_ms": f32["m2l_ms"],
         "accuracy": acc,
+        "served": served,
         "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
         "gpu_launches": int(f32["launches"]),
         "clocks": f32["clocks"], "clocks_fp64": f64["clocks"],
@@ -386,6 +492,7 @@ def main():
     ap.add_argument("--points", type=int, default=1_000_000)
     ap.add_argument("--depth", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-served", action="store_true")
     args = ap.parse_args()
     ws, rank, local = dist_setup()
     try:

@@ -37,7 +37,7 @@ extern "C" {
 #define WBFMM_B200_HELMHOLTZ 2
 
 #define WBFMM_B200_FP64 0 /* plain form: FP64 everywhere */
-#define WBFMM_B200_FP32 1 /* FP32 bulk, FP64 tables, compensated P2P */
+#define WBFMM_B200_FP32 1 /* FP32 bulk, FP64 tables, FP64 P2P sums */
 
 #define WBFMM_B200_POTENTIAL 1
 #define WBFMM_B200_GRADIENT 2

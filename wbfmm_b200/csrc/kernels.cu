@@ -528,25 +528,13 @@ int launch_l2p(const EvalParams<T>& p, cudaStream_t s) {
 }
 
 // ------------------------------------------------------------------- P2P
-// Neumaier two-sum accumulator, used by the FP32 P2P (compensated)
-template <typename T>
-struct Acc {
-  T s = T(0), c = T(0);
-  __device__ __forceinline__ void add(T v, bool comp) {
-    if (!comp) { s += v; return; }
-    T t = s + v;
-    if (fabs(s) >= fabs(v)) c += (s - t) + v; else c += (v - t) + s;
-    s = t;
-  }
-  __device__ __forceinline__ T value() const { return s + c; }
-};
-
 // One CTA per target leaf box.  The sources of the 27 neighbour boxes (a
 // virtual list, box by box) are staged through shared memory in tiles of
 // kP2PTile.  Each target is swept by a group of G threads (G a power of two,
 // as large as the box's target count leaves room for, at most 32): thread g
-// of the group takes tile entries g, g+G, ..., accumulating in registers in
-// a fixed order (compensated in FP32), and the group's partial sums are
+// of the group takes tile entries g, g+G, ..., accumulating in FP64
+// registers in a fixed order (for the FP32 form too: pair terms in FP32, sums
+// in FP64), and the group's partial sums are
 // added by shuffles at the end.  Pair kernels and the r > 1e-6 cutoff follow
 // src/local.c:32-262 and src/local-laplace.c:400-523, 1091-1227.
 constexpr int kP2PTile = 128;
@@ -594,7 +582,6 @@ k_p2p(EvalParams<T> p) {
   const uint32_t total = s_pref[27];
   const T f4pi = T(0.25 / kPi);
   const T rc2 = T(kCutoffRadius * kCutoffRadius);
-  const bool comp = p.compensated != 0;
   const T k = p.k;
   const bool hq = p.q != nullptr, hd = p.dip != nullptr;
   const bool want_pot = p.pot != nullptr, want_grad = p.grad != nullptr;
@@ -605,7 +592,7 @@ k_p2p(EvalParams<T> p) {
     const bool active = t0 + ti < tc;
     const uint32_t jt = p.tstart[b] + t0 + (active ? ti : 0);
     const double x = p.tx[jt], y = p.ty[jt], z = p.tz[jt];
-    Acc<T> a[8];
+    double a[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     for (uint32_t f0 = 0; f0 < total; f0 += kP2PTile) {
       const uint32_t f = f0 + tid;
       __syncthreads();
@@ -632,8 +619,8 @@ k_p2p(EvalParams<T> p) {
         const T rx = (T)(x - tl.x[j]), ry = (T)(y - tl.y[j]), rz = (T)(z - tl.z[j]);
         const T r2 = rx * rx + ry * ry + rz * rz;
         if (!(r2 > rc2)) continue;
-        const T r = sqrt(r2);
-        const T ir = T(1) / r;
+        const T ir = rsqrt(r2);
+        const T r = r2 * ir;
         if (HELM) {
           const T kr = k * r, ikr = ir / k;
           T sn, cs;
@@ -649,7 +636,7 @@ k_p2p(EvalParams<T> p) {
               fr -= k * (h1r * dr - h1i * di) * f4pi;
               fi -= k * (h1r * di + h1i * dr) * f4pi;
             }
-            a[0].add(fr, comp); a[1].add(fi, comp);
+            a[0] += (double)(fr); a[1] += (double)(fi);
           }
           if (want_grad) {
             const T ar = -k * (h1r * qr - h1i * qi) * f4pi * ir;
@@ -669,7 +656,7 @@ k_p2p(EvalParams<T> p) {
                 gi[c] += -k * (ur * di + ui * dr) * f4pi;
               }
             }
-            for (int c = 0; c < 3; c++) { a[2 + 2 * c].add(gr[c], comp); a[3 + 2 * c].add(gi[c], comp); }
+            for (int c = 0; c < 3; c++) { a[2 + 2 * c] += (double)(gr[c]); a[3 + 2 * c] += (double)(gi[c]); }
           }
         } else {
           const T q = tl.q[j];
@@ -678,7 +665,7 @@ k_p2p(EvalParams<T> p) {
           if (want_pot) {
             T v = q;
             if (hd) v += tl.d[j] * (rx * tl.nx[j] + ry * tl.ny[j] + rz * tl.nz[j]) * ir2;
-            a[0].add(v * g, comp);
+            a[0] += (double)(v * g);
           }
           if (want_grad) {
             const T gq = -q * g * ir2;
@@ -691,31 +678,33 @@ k_p2p(EvalParams<T> p) {
               gv[1] += ad * (nys - T(3) * nr * ry * ir2);
               gv[2] += ad * (nzs - T(3) * nr * rz * ir2);
             }
-            a[1].add(gv[0], comp); a[2].add(gv[1], comp); a[3].add(gv[2], comp);
+            a[1] += (double)(gv[0]); a[2] += (double)(gv[1]); a[3] += (double)(gv[2]);
           }
         }
       }
     }
     // sum over the group (lanes of one warp; inactive groups hold zeros)
     const int na = HELM ? 8 : 4;
-    T v[8];
+    double v[8];
     for (int c = 0; c < na; c++) {
-      v[c] = a[c].value();
+      v[c] = a[c];
       for (int o = 1; o < G; o <<= 1) v[c] += __shfl_xor_sync(0xffffffffu, v[c], o);
     }
     if (!active || gl != 0) continue;
     const uint32_t o = p.tperm[jt];
     if (HELM) {
       if (want_pot) {
-        p.pot[2 * (size_t)o] += v[0];
-        p.pot[2 * (size_t)o + 1] += v[1];
+        p.pot[2 * (size_t)o] = (T)((double)p.pot[2 * (size_t)o] + v[0]);
+        p.pot[2 * (size_t)o + 1] = (T)((double)p.pot[2 * (size_t)o + 1] + v[1]);
       }
       if (want_grad)
-        for (int c = 0; c < 6; c++) p.grad[6 * (size_t)o + c] += v[2 + c];
+        for (int c = 0; c < 6; c++)
+          p.grad[6 * (size_t)o + c] = (T)((double)p.grad[6 * (size_t)o + c] + v[2 + c]);
     } else {
-      if (want_pot) p.pot[o] += v[0];
+      if (want_pot) p.pot[o] = (T)((double)p.pot[o] + v[0]);
       if (want_grad)
-        for (int c = 0; c < 3; c++) p.grad[3 * (size_t)o + c] += v[1 + c];
+        for (int c = 0; c < 3; c++)
+          p.grad[3 * (size_t)o + c] = (T)((double)p.grad[3 * (size_t)o + c] + v[1 + c]);
     }
   }
 }

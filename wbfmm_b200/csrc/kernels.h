@@ -64,7 +64,6 @@ struct EvalParams {
   T* pot;    // [ntgt] or [2 ntgt] (original order), may be null
   T* grad;   // [3 ntgt] or [6 ntgt], may be null
   int64_t nbox;
-  int compensated;    // FP32 P2P: two-sum accumulation
 };
 
 template <typename T>

@@ -2,7 +2,7 @@
 //
 // A server owns S slots.  Each slot is a host thread with its own CUDA
 // stream and a reusable solver per precision whose buffers come from the
-// device's stream-ordered pool.  Requests wait in an arrival-ordered queue;
+// server's stream-ordered pool.  Requests wait in an arrival-ordered queue;
 // a slot that falls free takes the oldest request whose arrival time has
 // passed, provided the device-memory footprints of the solves in flight plus
 // its own stay within the budget (first come, first served: a request that
@@ -82,6 +82,7 @@ struct wbfmm_b200_server {
 
   int device = 0;
   int64_t budget = 0;
+  cudaMemPool_t pool = nullptr;   // the solves' device memory
   double epoch = 0;
   TableCache cache;
   std::vector<Slot*> slots;
@@ -112,6 +113,7 @@ struct wbfmm_b200_server {
       delete s;
     }
     for (auto& e : reqs) delete e.second;
+    if (pool) cudaMemPoolDestroy(pool);
   }
 
   template <typename T>
@@ -122,6 +124,8 @@ struct wbfmm_b200_server {
       x->async_checks = true;
       int rc = x->init(c, (void*)s->stream);
       if (rc) { delete x; return rc; }
+      cudaMemPool_t pl = pool;
+      x->each_buf([pl](auto& b) { b.pool = pl; });
       *out = x;
     }
     return (*out)->reset(c);
@@ -247,12 +251,23 @@ int wbfmm_b200_server_create(wbfmm_b200_server_t** out, int nslots,
   }
   srv->budget = hbm_budget;
   srv->epoch = now_s();
-  // keep freed pool memory cached in the process: solves reallocate cheaply
-  cudaMemPool_t pool;
-  if (cudaDeviceGetDefaultMemPool(&pool, srv->device) == cudaSuccess) {
-    uint64_t thr = UINT64_MAX;
-    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  // A pool of the server's own: freed memory stays cached (solves
+  // reallocate cheaply) and is reused only once its free has completed, so
+  // the pool never makes one slot's stream wait for another's.
+  cudaMemPoolProps props;
+  memset(&props, 0, sizeof(props));
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = srv->device;
+  if (cudaMemPoolCreate(&srv->pool, &props) != cudaSuccess) {
+    cudaGetLastError();
+    delete srv;
+    return set_error(WBFMM_B200_E_NOMEM, "server: memory pool creation failed");
   }
+  uint64_t thr = UINT64_MAX;
+  int off = 0;
+  cudaMemPoolSetAttribute(srv->pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  cudaMemPoolSetAttribute(srv->pool, cudaMemPoolReuseAllowInternalDependencies, &off);
   for (int i = 0; i < nslots; i++) {
     auto* s = new wbfmm_b200_server::Slot();
     srv->slots.push_back(s);

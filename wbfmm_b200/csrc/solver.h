@@ -6,7 +6,7 @@
 // reference's Layout L, the operator tables and the sorted targets.  The
 // FP64 instantiation is the plain form; the FP32 instantiation keeps the
 // same structure with FP32 coefficients, FP64-generated tables converted to
-// FP32, FP64 point separations and compensated P2P accumulation.
+// FP32, FP64 point separations and FP64 accumulation of the P2P sums.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdio.h>
@@ -36,6 +36,7 @@ struct DBuf {
   bool managed = false;
   bool owned = true;        // false: memory supplied by the caller (adopt)
   cudaStream_t so = nullptr;
+  cudaMemPool_t pool = nullptr;   // stream-ordered pool (default: device's)
   DBuf() = default;
   explicit DBuf(cudaStream_t s) : so(s) {}
   DBuf(const DBuf&) = delete;
@@ -59,6 +60,7 @@ struct DBuf {
     managed = use_managed;
     size_t bytes = sizeof(T) * (count ? count : 1);
     cudaError_t e = use_managed ? cudaMallocManaged(&p, bytes)
+                    : (so && pool) ? cudaMallocFromPoolAsync(&p, bytes, pool, so)
                     : so        ? cudaMallocAsync(&p, bytes, so)
                                 : cudaMalloc(&p, bytes);
     if (e != cudaSuccess) {
@@ -717,7 +719,6 @@ struct Solver : public wbfmm_b200_solver {
     e.pot = (cfg.field & eval_field & WBFMM_B200_POTENTIAL) ? pot.p : nullptr;
     e.grad = (cfg.field & eval_field & WBFMM_B200_GRADIENT) ? grad.p : nullptr;
     e.nbox = (int64_t)1 << (3 * depth);
-    e.compensated = sizeof(T) == 4 ? 1 : 0;
     return e;
   }
 
