@@ -249,7 +249,7 @@ def served_section(args, ws, rank, local):
         t0 = srv.clock()
         tk = [srv.submit(p, precf(p)) for p in batch]
         srv.drain()
-        span = max(srv.times(t)[2] for t in tk) - t0
+        span = max(srv.times(t)[3] for t in tk) - t0
         kept = [tuple(a.copy() for a in srv.wait(t)) for t in tk[:keep]]
         for t in tk:
             srv.forget(t)
@@ -263,10 +263,10 @@ def served_section(args, ws, rank, local):
         T = np.array([srv.times(t) for t in tk])
         for t in tk:
             srv.forget(t)
-        lat = T[:, 2] - T[:, 0]
+        lat = T[:, 3] - T[:, 0]
         return {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
                 "mean_s": float(lat.mean()),
-                "throughput_points_per_s": float(sum(p.points for p in reqs) / (T[:, 2].max() - base))}
+                "throughput_points_per_s": float(sum(p.points for p in reqs) / (T[:, 3].max() - base))}
 
     out = {}
     kept = None

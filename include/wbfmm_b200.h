@@ -168,11 +168,13 @@ int wbfmm_b200_tree_structure(int n, const double *pts, int pstr,
                               const double *x0, double D, int depth,
                               uint32_t *ip, uint32_t *box_i, uint32_t *box_n);
 
-/* M2L kernel selection: 1 (default) = lane-per-pair kernel for the orders it
-   is instantiated for (Helmholtz <= 8, Laplace <= 12, equal singular and
-   regular orders), generic warp kernel otherwise; 0 = always the generic
-   warp kernel. */
-int wbfmm_b200_set_m2l_kernel(wbfmm_b200_solver_t *s, int lanes);
+/* M2L kernel selection (all need equal singular and regular orders, else
+   the warp kernel runs): 1 (default) = automatic: lane-per-pair kernel up to
+   order 8 (Helmholtz) / 12 (Laplace), offset-major target tiles above, while
+   their shared memory suffices; 2 = lane-per-pair wherever instantiated
+   (Helmholtz <= 8, Laplace <= 16); 3 = target tiles wherever they fit;
+   0 = always the warp-per-target kernel. */
+int wbfmm_b200_set_m2l_kernel(wbfmm_b200_solver_t *s, int mode);
 
 /* FP64 direct sum with self-exclusion (r <= 1e-6) and compensated
    accumulation: the GPU counterpart of wbfmm_total_field[_grad]
@@ -262,9 +264,11 @@ int wbfmm_b200_server_submit(wbfmm_b200_server_t *srv,
 int wbfmm_b200_server_poll(wbfmm_b200_server_t *srv, int64_t ticket);
 /* blocks until the request has completed; returns its status */
 int wbfmm_b200_server_wait(wbfmm_b200_server_t *srv, int64_t ticket);
-/* arrival, start and completion times (server clock) of a completed request */
+/* server-clock times of a completed request: arrival, start (taken by a
+   slot), queued (all its device work and copies issued on the slot's
+   stream) and completion (fields in the caller's arrays) */
 int wbfmm_b200_server_times(wbfmm_b200_server_t *srv, int64_t ticket,
-                            double *t3);
+                            double *t4);
 /* drops a completed request's record */
 int wbfmm_b200_server_forget(wbfmm_b200_server_t *srv, int64_t ticket);
 /* blocks until the queue is empty and no solve is running */

@@ -187,3 +187,32 @@ def test_m2l_lane_kernel_matches_generic(gpu_lib, name, precision):
     tol = 1e-12 if precision == engine.FP64 else 1e-5
     for a, b in zip(outs[0], outs[1]):
         assert rel_l2(a, b) < tol
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [engine.FP64, engine.FP32])
+@pytest.mark.parametrize("case", ["laplace13", "laplace16", "helmholtz_k6_floor11",
+                                  "helmholtz_k20_floor9"])
+def test_m2l_kernels_agree_at_high_order(gpu_lib, case, precision):
+    """The offset-major tile M2L (mode 3), the lane-per-pair M2L where
+    instantiated (mode 2) and the warp-per-target M2L (mode 0) compute the
+    same translations at the orders of the served stream."""
+    if case.startswith("laplace"):
+        p = W.laplace_cube(30000, 3000, depth=4, order=int(case[7:]), seed=43)
+    else:
+        k = float(case.split("_")[1][1:])
+        lo = int(case.split("floor")[1])
+        p = W.helmholtz_cube(30000, k=k, depth=4, seed=44, lo=lo, hi=40)
+        p.xt = p.xt[:3000]
+        p.targets_are_sources = False
+    outs = {}
+    for mode in (0, 2, 3):
+        cfg = engine.SolverConfig.from_problem(p, precision)
+        with engine.Solver(cfg) as s:
+            s.set_m2l_kernel(mode)
+            s.set_sources(p.xs).set_strengths(p.q).set_targets(p.xt).run()
+            outs[mode] = s.field()
+    tol = 1e-12 if precision == engine.FP64 else 2e-5
+    for mode in (2, 3):
+        for a, b in zip(outs[mode], outs[0]):
+            assert rel_l2(a, b) < tol, (mode, rel_l2(a, b))

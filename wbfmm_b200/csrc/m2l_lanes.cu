@@ -35,29 +35,6 @@ template <> struct V2t<double> { typedef double2 t; };
 __constant__ int c_offsets[8][189];
 static bool g_offsets_ready[64] = {false};
 
-static void build_offset_table(int* tab) {
-  for (int tau = 0; tau < 8; tau++) {
-    int ta[3] = {tau & 1, (tau >> 1) & 1, (tau >> 2) & 1};
-    int j = 0;
-    for (int dx = -2 - ta[0]; dx <= 3 - ta[0]; dx++)
-      for (int dy = -2 - ta[1]; dy <= 3 - ta[1]; dy++)
-        for (int dz = -2 - ta[2]; dz <= 3 - ta[2]; dz++) {
-          if (dx >= -1 && dx <= 1 && dy >= -1 && dy <= 1 && dz >= -1 && dz <= 1)
-            continue;
-          int d[3] = {dx, dy, dz}, sg = 0, Dl[3];
-          for (int a = 0; a < 3; a++) {
-            int s = ta[a] + d[a];
-            sg |= (s & 1) << a;
-            Dl[a] = s >> 1;   // floor division (s in [-2, 4])
-          }
-          int op = (dx + 3) * 49 + (dy + 3) * 7 + dz + 3;
-          tab[tau * 189 + j] = op | (sg << 9) | ((Dl[0] + 1) << 12) |
-                               ((Dl[1] + 1) << 14) | ((Dl[2] + 1) << 16);
-          j++;
-        }
-  }
-}
-
 static int ensure_offsets() {
   int dev = 0;
   cudaGetDevice(&dev);
@@ -456,6 +433,17 @@ __global__ void k_lanes_reduce(LanesParams<T> p, int N) {
 
 // ------------------------------------------------------------- launchers
 template <typename T, bool HELM>
+int launch_lanes_reduce(const LanesParams<T>& p, cudaStream_t s) {
+  const int N = p.N;
+  const int V = HELM ? (N + 1) * (N + 1) : (N + 1) * (N + 2) / 2;
+  const int64_t np = (int64_t)1 << (3 * (p.level - 1));
+  const int64_t tot = np * 8 * V;
+  k_lanes_reduce<T, HELM><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(p, N);
+  WBFMM_CUDA(cudaGetLastError());
+  return 0;
+}
+
+template <typename T, bool HELM>
 int lanes_to_lin(const T* arr, int level, int N, void* lin, cudaStream_t s) {
   typedef typename V2t<T>::t T2;
   const int V = HELM ? (N + 1) * (N + 1) : (N + 1) * (N + 2) / 2;
@@ -484,11 +472,7 @@ static int launch_lanes_P(const LanesParams<T>& p, const OpTables<T>& t,
   dim3 grid((unsigned)((np + SM::CTA - 1) / SM::CTA), 8, p.nsplit);
   k_m2l_lanes<T, HELM, P><<<grid, SM::CTA, SM::bytes, s>>>(p, t);
   WBFMM_CUDA(cudaGetLastError());
-  if (p.nsplit > 1) {
-    const int64_t tot = np * 8 * SM::V;
-    k_lanes_reduce<T, HELM><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(p, P);
-    WBFMM_CUDA(cudaGetLastError());
-  }
+  if (p.nsplit > 1) return launch_lanes_reduce<T, HELM>(p, s);
   return 0;
 }
 
@@ -526,6 +510,10 @@ int launch_m2l_lanes(const LanesParams<T>& p, const OpTables<T>& t,
       WBFMM_LANES_CASE(10)
       WBFMM_LANES_CASE(11)
       WBFMM_LANES_CASE(12)
+      WBFMM_LANES_CASE(13)
+      WBFMM_LANES_CASE(14)
+      WBFMM_LANES_CASE(15)
+      WBFMM_LANES_CASE(16)
 #undef WBFMM_LANES_CASE
       default: break;
     }
@@ -535,6 +523,7 @@ int launch_m2l_lanes(const LanesParams<T>& p, const OpTables<T>& t,
 
 #define WBFMM_LANES_INST(T, H)                                                   \
   template int lanes_to_lin<T, H>(const T*, int, int, void*, cudaStream_t);      \
+  template int launch_lanes_reduce<T, H>(const LanesParams<T>&, cudaStream_t);   \
   template bool lanes_supported<T, H>(int, int);                                 \
   template int launch_m2l_lanes<T, H>(const LanesParams<T>&, const OpTables<T>&, \
                                       cudaStream_t);

@@ -9,7 +9,7 @@
 namespace wbfmm {
 
 constexpr int kLanesMaxHelm = 8;    // orders instantiated for Helmholtz
-constexpr int kLanesMaxLap = 12;    // and for Laplace
+constexpr int kLanesMaxLap = 16;    // and for Laplace
 
 template <typename T>
 struct LanesParams {
@@ -25,8 +25,50 @@ struct LanesParams {
   void* partial_raw;    // [nsplit][8][V][np] complex when nsplit > 1
 };
 
+// The 189 list-4 offsets seen by a target of child type tau, packed as
+// op | sigma << 9 | (dx+1) << 12 | (dy+1) << 14 | (dz+1) << 16 with op the
+// shift code (dx+3)*49+(dy+3)*7+dz+3 of src/indexing.c:330-377, sigma the
+// source's child type and (dx, dy, dz) the source parent's offset from the
+// target's parent (each in [-1, 1]).
+inline void build_offset_table(int* tab) {
+  for (int tau = 0; tau < 8; tau++) {
+    int ta[3] = {tau & 1, (tau >> 1) & 1, (tau >> 2) & 1};
+    int j = 0;
+    for (int dx = -2 - ta[0]; dx <= 3 - ta[0]; dx++)
+      for (int dy = -2 - ta[1]; dy <= 3 - ta[1]; dy++)
+        for (int dz = -2 - ta[2]; dz <= 3 - ta[2]; dz++) {
+          if (dx >= -1 && dx <= 1 && dy >= -1 && dy <= 1 && dz >= -1 && dz <= 1)
+            continue;
+          int d[3] = {dx, dy, dz}, sg = 0, Dl[3];
+          for (int a = 0; a < 3; a++) {
+            int s = ta[a] + d[a];
+            sg |= (s & 1) << a;
+            Dl[a] = s >> 1;   // floor division (s in [-2, 4])
+          }
+          int op = (dx + 3) * 49 + (dy + 3) * 7 + dz + 3;
+          tab[tau * 189 + j] = op | (sg << 9) | ((Dl[0] + 1) << 12) |
+                               ((Dl[1] + 1) << 14) | ((Dl[2] + 1) << 16);
+          j++;
+        }
+  }
+}
+
 template <typename T, bool HELM>
 bool lanes_supported(int Ns, int Nr);
+// sum of the split partial results (split order) into the level array
+template <typename T, bool HELM>
+int launch_lanes_reduce(const LanesParams<T>& p, cudaStream_t s);
+
+// offset-major target tiles (m2l_tiles.cu), any order up to a shared-memory
+// limit
+template <typename T, bool HELM>
+bool tiles_supported(int Ns, int Nr);
+template <typename T, bool HELM>
+int launch_m2l_tiles(const LanesParams<T>& p, const OpTables<T>& t,
+                     cudaStream_t s);
+// targets per CTA of the tile kernel at order N (0: unsupported)
+template <typename T, bool HELM>
+int tiles_per_cta(int N);
 template <typename T, bool HELM>
 int lanes_to_lin(const T* arr, int level, int N, void* lin, cudaStream_t s);
 size_t lanes_lin_bytes(int level, int N, bool helm, size_t tsize);

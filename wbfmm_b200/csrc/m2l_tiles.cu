@@ -1,0 +1,463 @@
+// M2L for any expansion order: offset-major tiles of targets.
+//
+// As in the lane-per-pair kernel, the list-4 interactions of a level are
+// regrouped by target child type tau, so that TC target boxes of one type
+// (the tau-children of TC consecutive parents) see the same 189 offsets,
+// each with one rotate / coaxial / rotate-back operator (src/pass.c:56-105:
+// wbfmm_rotate_H, wbfmm_coaxial_translate_ref, rotate back).  Here a CTA of
+// 256 threads applies each offset's operator to all TC source vectors at
+// once, as three small matrix products staged through shared memory:
+//
+//   A  X[n,m][t]  = e^{i m ch} src_t[n,m]
+//   B  Y[n,nu][t] = e^{-i nu ph} sum_m H_n^{nu,m} X[n,m][t]       (per degree)
+//   C  Z[n,m][t]  = e^{i m ph} sum_l (S|R)_{l,n}^{|m|} Y[l,m][t]   (per order)
+//   D  acc[n,nu][t] += e^{-i nu ch} sum_m H_n^{nu,m} Z[n,m][t]    (per degree)
+//
+// Each thread computes a register tile of 2 output rows x 4 targets, so an
+// operator entry read from shared memory feeds 4 (complex) multiply-adds and
+// a source value 2.  The order is a runtime parameter; TC (32, 16 or 8) is
+// the largest whose three vector blocks fit beside the operator.  Laplace
+// uses half vectors (m >= 0), as the reference's real-packed coefficients.
+#include <cuda_runtime.h>
+
+#include "engine.h"
+#include "kernels.h"
+#include "m2l_lanes.h"
+#include "translate.cuh"
+
+namespace wbfmm {
+
+namespace {
+
+template <typename T> struct C2;
+template <> struct C2<float> { typedef float2 t; };
+template <> struct C2<double> { typedef double2 t; };
+
+__constant__ int c_tile_offsets[8][189];
+bool g_tile_offsets_ready[64] = {false};
+
+int ensure_tile_offsets() {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 64 && g_tile_offsets_ready[dev]) return 0;
+  int tab[8 * 189];
+  build_offset_table(tab);
+  WBFMM_CUDA(cudaMemcpyToSymbol(c_tile_offsets, tab, sizeof(tab)));
+  if (dev < 64) g_tile_offsets_ready[dev] = true;
+  return 0;
+}
+
+constexpr int kTileThreads = 256;
+
+// shared-memory plan of one launch (units: bytes)
+struct TilePlan {
+  int P, V, TC, NH, ncx, nB, nC;
+  size_t ops_bytes, desc_bytes, vec_bytes, total;
+};
+
+template <typename T, bool HELM>
+__host__ __device__ TilePlan tile_plan(int P, int TC) {
+  TilePlan q;
+  q.P = P;
+  q.TC = TC;
+  q.V = HELM ? (P + 1) * (P + 1) : (P + 1) * (P + 2) / 2;
+  q.NH = (P + 1) * (P + 2) * (4 * P + 3) / 6;
+  q.ncx = HELM ? 2 * ((P + 1) * (P + 2) * (P + 3) / 6) : (P + 1) * (P + 1) * (P + 1);
+  q.nB = 0;
+  for (int n = 0; n <= P; n++) q.nB += HELM ? n + 1 : (n + 2) / 2;
+  q.nC = 0;
+  for (int m = HELM ? -P : 0; m <= P; m++) {
+    int am = m < 0 ? -m : m;
+    q.nC += (P + 1 - am + 1) / 2;
+  }
+  size_t ops = sizeof(T) * ((size_t)q.NH + 6 * (P + 1) + q.ncx);
+  q.ops_bytes = (ops + 15) & ~(size_t)15;
+  q.desc_bytes = ((sizeof(int) * (size_t)(q.nB + q.nC + q.V) + 2 * sizeof(int) * TC) + 15) & ~(size_t)15;
+  q.vec_bytes = 3 * sizeof(typename C2<T>::t) * (size_t)q.V * TC;
+  q.total = q.ops_bytes + q.desc_bytes + q.vec_bytes;
+  return q;
+}
+
+constexpr size_t kTileSmemCap = 220 * 1024;
+
+template <typename T, bool HELM>
+int pick_tc(int P) {
+  for (int tc = 32; tc >= 8; tc >>= 1)
+    if (tile_plan<T, HELM>(P, tc).total <= kTileSmemCap) return tc;
+  return 0;
+}
+
+template <typename T2, typename T>
+__device__ __forceinline__ T2 cmul(T2 a, T er, T ei) {
+  T2 r;
+  r.x = a.x * er - a.y * ei;
+  r.y = a.x * ei + a.y * er;
+  return r;
+}
+
+template <typename T, bool HELM>
+__global__ void __launch_bounds__(kTileThreads)
+k_m2l_tiles(LanesParams<T> p, OpTables<T> t, int TC) {
+  typedef typename C2<T>::t T2;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const TilePlan q = tile_plan<T, HELM>(p.N, TC);
+  const int P = q.P, V = q.V, TQ = TC / 4;
+  T* sH = (T*)smraw;
+  T* seph = sH + q.NH;
+  T* sech = seph + 2 * (P + 1);
+  T* spw = sech + 2 * (P + 1);       // Laplace: 1/t^(e+1), e <= 2P+1
+  T* scx = spw + 2 * (P + 1);
+  int* dB = (int*)(smraw + q.ops_bytes);
+  int* dC = dB + q.nB;
+  int* s_nm = dC + q.nC;             // (n, m) of each vector entry
+  int* s_pp = s_nm + V;              // padded-grid index of each target's parent
+  int* s_act = s_pp + TC;
+  T2* X = (T2*)(smraw + q.ops_bytes + q.desc_bytes);
+  T2* Y = X + (size_t)V * TC;
+  T2* A = Y + (size_t)V * TC;
+  const int tid = threadIdx.x;
+
+  const int tau = blockIdx.y, split = blockIdx.z;
+  const int nx = 1 << (p.level - 1), npx = nx + 2;
+  const int64_t npp = (int64_t)npx * npx * npx;
+  const int64_t np = (int64_t)nx * nx * nx;
+  const int64_t base = (int64_t)blockIdx.x * TC;
+
+  // stage descriptors: B/D rows (n, nu0) and C rows (m, n0), 2 rows each
+  if (tid == 0) {
+    int k = 0;
+    for (int n = 0; n <= P; n++)
+      for (int nu = HELM ? -n : 0; nu <= n; nu += 2) dB[k++] = n | ((nu + 64) << 8);
+    k = 0;
+    for (int m = HELM ? -P : 0; m <= P; m++) {
+      int am = m < 0 ? -m : m;
+      for (int n = am; n <= P; n += 2) dC[k++] = n | ((m + 64) << 8);
+    }
+  }
+  for (int c = tid; c < V; c += kTileThreads) {
+    const int n = HELM ? full_degree(c) : half_degree(c);
+    const int m = HELM ? c - n * (n + 1) : c - n * (n + 1) / 2;
+    s_nm[c] = n | ((m + 64) << 8);
+  }
+  for (int i = tid; i < TC; i += kTileThreads) {
+    const int64_t plin = base + i;
+    int act = plin < np;
+    int pp = 0;
+    if (act) {
+      int px = (int)(plin % nx), py = (int)((plin / nx) % nx), pz = (int)(plin / ((int64_t)nx * nx));
+      pp = (px + 1) + npx * ((py + 1) + npx * (pz + 1));
+      if (p.tmask && !p.tmask[((int64_t)morton(px, py, pz) << 3) | tau]) act = 0;
+    }
+    s_pp[i] = pp;
+    s_act[i] = act;
+  }
+  for (int i = tid; i < V * TC; i += kTileThreads) { T2 z; z.x = T(0); z.y = T(0); A[i] = z; }
+  __syncthreads();
+
+#pragma unroll 1
+  for (int j = split; j < 189; j += p.nsplit) {
+    const int code = c_tile_offsets[tau][j];
+    const int op = code & 511, sg = (code >> 9) & 7;
+    const int ddx = ((code >> 12) & 3) - 1, ddy = ((code >> 14) & 3) - 1,
+              ddz = ((code >> 16) & 3) - 1;
+    const int64_t doff = ddx + npx * ((int64_t)ddy + npx * (int64_t)ddz);
+    __syncthreads();   // the previous offset's operator and vectors are free
+    {
+      const T* H = t.H + (int64_t)t.op_ith[op] * t.hstride;
+      for (int i = tid; i < q.NH; i += kTileThreads) sH[i] = H[i];
+      const T* eph = t.ph + (size_t)op * (t.lmax + 1) * 2;
+      const T* ech = t.ch + (size_t)op * (t.lmax + 1) * 2;
+      for (int i = tid; i < 2 * (P + 1); i += kTileThreads) {
+        seph[i] = eph[i];
+        sech[i] = ech[i];
+      }
+      if (HELM) {
+        const T* cx = p.coax + (int64_t)t.op_dist[op] * p.coax_stride;
+        for (int i = tid; i < q.ncx; i += kTileThreads) scx[i] = cx[i];
+      } else {
+        // S|R(n,nd,m) / t^{n+nd+1}, t = width * |d|
+        if (tid == 0) {
+          const T rinv = T(1) / (p.width * t.op_r[op]);
+          T s = rinv;
+          for (int e = 0; e < 2 * (P + 1); e++) { spw[e] = s; s *= rinv; }
+        }
+        __syncthreads();
+        const int Dm = t.lt + 1;
+        for (int i = tid; i < q.ncx; i += kTileThreads) {
+          int m = i % (P + 1), nd = (i / (P + 1)) % (P + 1), n = i / ((P + 1) * (P + 1));
+          scx[i] = t.lapSR[((int64_t)n * Dm + nd) * Dm + m] * spw[n + nd];
+        }
+      }
+    }
+    __syncthreads();   // operator staged
+    // stage A: the TC source vectors, with e^{i m ch}
+    {
+      const T2* src = (const T2*)p.lin_raw + (int64_t)sg * V * npp + doff;
+      for (int i = tid; i < V * TC; i += kTileThreads) {
+        const int c = i / TC, tt = i - c * TC;
+        T2 v;
+        v.x = T(0); v.y = T(0);
+        if (s_act[tt]) {
+          v = src[(int64_t)c * npp + s_pp[tt]];
+          const int m = (s_nm[c] >> 8) - 64, am = m < 0 ? -m : m;
+          v = cmul(v, sech[2 * am], m < 0 ? -sech[2 * am + 1] : sech[2 * am + 1]);
+        }
+        X[i] = v;
+      }
+    }
+    __syncthreads();
+    // stage B: forward rotation per degree, then e^{-i nu ph}
+    for (int w = tid; w < q.nB * TQ; w += kTileThreads) {
+      const int d = dB[w / TQ], t0 = (w % TQ) * 4;
+      const int n = d & 255, nu0 = (d >> 8) - 64;
+      const bool two = nu0 + 1 <= n;
+      const int hb = rot_idx(-n, 0, n);
+      T2 a0[4], a1[4];
+#pragma unroll
+      for (int k = 0; k < 4; k++) { a0[k].x = a0[k].y = a1[k].x = a1[k].y = T(0); }
+      if (HELM) {
+        for (int m = -n; m <= n; m++) {
+          const T2* xr = X + (size_t)cidx(n, m) * TC + t0;
+          const T h0 = m >= 0 ? sH[hb + (nu0 + n) * (n + 1) + m] : sH[hb + (-nu0 + n) * (n + 1) - m];
+          const T h1 = !two ? T(0) : m >= 0 ? sH[hb + (nu0 + 1 + n) * (n + 1) + m]
+                                            : sH[hb + (-nu0 - 1 + n) * (n + 1) - m];
+#pragma unroll
+          for (int k = 0; k < 4; k++) {
+            const T2 x = xr[k];
+            a0[k].x += h0 * x.x; a0[k].y += h0 * x.y;
+            a1[k].x += h1 * x.x; a1[k].y += h1 * x.y;
+          }
+        }
+        for (int r = 0; r < (two ? 2 : 1); r++) {
+          const int nu = nu0 + r, an = nu < 0 ? -nu : nu;
+          const T er = seph[2 * an], ei = nu < 0 ? seph[2 * an + 1] : -seph[2 * an + 1];
+          T2* yr = Y + (size_t)cidx(n, nu) * TC + t0;
+#pragma unroll
+          for (int k = 0; k < 4; k++) yr[k] = cmul(r ? a1[k] : a0[k], er, ei);
+        }
+      } else {
+        // a0/a1 hold (tr, ti) of rows nu0, nu0 + 1
+        for (int m = 0; m <= n; m++) {
+          const T2* xr = X + (size_t)hidx(n, m) * TC + t0;
+          T p0, m0, p1 = T(0), m1 = T(0);
+          p0 = sH[hb + (nu0 + n) * (n + 1) + m];
+          m0 = sH[hb + (-nu0 + n) * (n + 1) + m];
+          if (two) {
+            p1 = sH[hb + (nu0 + 1 + n) * (n + 1) + m];
+            m1 = sH[hb + (-nu0 - 1 + n) * (n + 1) + m];
+          }
+          if (m == 0) { m0 = T(0); m1 = T(0); }
+#pragma unroll
+          for (int k = 0; k < 4; k++) {
+            const T2 x = xr[k];
+            a0[k].x += (p0 + m0) * x.x; a0[k].y += (p0 - m0) * x.y;
+            a1[k].x += (p1 + m1) * x.x; a1[k].y += (p1 - m1) * x.y;
+          }
+        }
+        for (int r = 0; r < (two ? 2 : 1); r++) {
+          const int nu = nu0 + r;
+          const T er = seph[2 * nu], ei = seph[2 * nu + 1];
+          T2* yr = Y + (size_t)hidx(n, nu) * TC + t0;
+#pragma unroll
+          for (int k = 0; k < 4; k++) {
+            const T2 a = r ? a1[k] : a0[k];
+            T2 o;
+            o.x = er * a.x + ei * a.y;
+            o.y = nu == 0 ? T(0) : er * a.y - ei * a.x;
+            yr[k] = o;
+          }
+        }
+      }
+    }
+    __syncthreads();
+    // stage C: coaxial translation per order m, then e^{i m ph}; into X
+    for (int w = tid; w < q.nC * TQ; w += kTileThreads) {
+      const int d = dC[w / TQ], t0 = (w % TQ) * 4;
+      const int n0 = d & 255, m = (d >> 8) - 64, am = m < 0 ? -m : m;
+      const bool two = n0 + 1 <= P;
+      T2 a0[4], a1[4];
+#pragma unroll
+      for (int k = 0; k < 4; k++) { a0[k].x = a0[k].y = a1[k].x = a1[k].y = T(0); }
+      for (int l = am; l <= P; l++) {
+        const T2* yr = Y + (size_t)(HELM ? cidx(l, m) : hidx(l, m)) * TC + t0;
+        if (HELM) {
+          int ic = l >= n0 ? coax_idx(l, am, n0) : coax_idx(n0, am, l);
+          T sg0 = (l >= n0 || ((n0 + l) & 1) == 0) ? T(1) : T(-1);
+          const T c0r = sg0 * scx[2 * ic], c0i = sg0 * scx[2 * ic + 1];
+          T c1r = T(0), c1i = T(0);
+          if (two) {
+            const int n1 = n0 + 1;
+            ic = l >= n1 ? coax_idx(l, am, n1) : coax_idx(n1, am, l);
+            const T sg1 = (l >= n1 || ((n1 + l) & 1) == 0) ? T(1) : T(-1);
+            c1r = sg1 * scx[2 * ic];
+            c1i = sg1 * scx[2 * ic + 1];
+          }
+#pragma unroll
+          for (int k = 0; k < 4; k++) {
+            const T2 y = yr[k];
+            a0[k].x += c0r * y.x - c0i * y.y; a0[k].y += c0i * y.x + c0r * y.y;
+            a1[k].x += c1r * y.x - c1i * y.y; a1[k].y += c1i * y.x + c1r * y.y;
+          }
+        } else {
+          const T c0 = scx[(n0 * (P + 1) + l) * (P + 1) + m];
+          const T c1 = two ? scx[((n0 + 1) * (P + 1) + l) * (P + 1) + m] : T(0);
+#pragma unroll
+          for (int k = 0; k < 4; k++) {
+            const T2 y = yr[k];
+            a0[k].x += c0 * y.x; a0[k].y += c0 * y.y;
+            a1[k].x += c1 * y.x; a1[k].y += c1 * y.y;
+          }
+        }
+      }
+      const T er = seph[2 * am], ei = m < 0 ? -seph[2 * am + 1] : seph[2 * am + 1];
+      for (int r = 0; r < (two ? 2 : 1); r++) {
+        const int n = n0 + r;
+        T2* xr = X + (size_t)(HELM ? cidx(n, m) : hidx(n, m)) * TC + t0;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          T2 a = r ? a1[k] : a0[k];
+          if (!HELM && m == 0) a.y = T(0);
+          xr[k] = cmul(a, er, ei);
+        }
+      }
+    }
+    __syncthreads();
+    // stage D: back rotation per degree, e^{-i nu ch}, accumulate
+    for (int w = tid; w < q.nB * TQ; w += kTileThreads) {
+      const int d = dB[w / TQ], t0 = (w % TQ) * 4;
+      const int n = d & 255, nu0 = (d >> 8) - 64;
+      const bool two = nu0 + 1 <= n;
+      const int hb = rot_idx(-n, 0, n);
+      T2 a0[4], a1[4];
+#pragma unroll
+      for (int k = 0; k < 4; k++) { a0[k].x = a0[k].y = a1[k].x = a1[k].y = T(0); }
+      if (HELM) {
+        for (int m = -n; m <= n; m++) {
+          const T2* xr = X + (size_t)cidx(n, m) * TC + t0;
+          const T h0 = m >= 0 ? sH[hb + (nu0 + n) * (n + 1) + m] : sH[hb + (-nu0 + n) * (n + 1) - m];
+          const T h1 = !two ? T(0) : m >= 0 ? sH[hb + (nu0 + 1 + n) * (n + 1) + m]
+                                            : sH[hb + (-nu0 - 1 + n) * (n + 1) - m];
+#pragma unroll
+          for (int k = 0; k < 4; k++) {
+            const T2 x = xr[k];
+            a0[k].x += h0 * x.x; a0[k].y += h0 * x.y;
+            a1[k].x += h1 * x.x; a1[k].y += h1 * x.y;
+          }
+        }
+        for (int r = 0; r < (two ? 2 : 1); r++) {
+          const int nu = nu0 + r, an = nu < 0 ? -nu : nu;
+          const T er = sech[2 * an], ei = nu < 0 ? sech[2 * an + 1] : -sech[2 * an + 1];
+          T2* ar = A + (size_t)cidx(n, nu) * TC + t0;
+#pragma unroll
+          for (int k = 0; k < 4; k++) {
+            const T2 o = cmul(r ? a1[k] : a0[k], er, ei);
+            ar[k].x += o.x; ar[k].y += o.y;
+          }
+        }
+      } else {
+        for (int m = 0; m <= n; m++) {
+          const T2* xr = X + (size_t)hidx(n, m) * TC + t0;
+          T p0, m0, p1 = T(0), m1 = T(0);
+          p0 = sH[hb + (nu0 + n) * (n + 1) + m];
+          m0 = sH[hb + (-nu0 + n) * (n + 1) + m];
+          if (two) {
+            p1 = sH[hb + (nu0 + 1 + n) * (n + 1) + m];
+            m1 = sH[hb + (-nu0 - 1 + n) * (n + 1) + m];
+          }
+          if (m == 0) { m0 = T(0); m1 = T(0); }
+#pragma unroll
+          for (int k = 0; k < 4; k++) {
+            const T2 x = xr[k];
+            a0[k].x += (p0 + m0) * x.x; a0[k].y += (p0 - m0) * x.y;
+            a1[k].x += (p1 + m1) * x.x; a1[k].y += (p1 - m1) * x.y;
+          }
+        }
+        for (int r = 0; r < (two ? 2 : 1); r++) {
+          const int nu = nu0 + r;
+          const T er = sech[2 * nu], ei = sech[2 * nu + 1];
+          T2* ar = A + (size_t)hidx(n, nu) * TC + t0;
+#pragma unroll
+          for (int k = 0; k < 4; k++) {
+            const T2 a = r ? a1[k] : a0[k];
+            ar[k].x += er * a.x + ei * a.y;
+            if (nu != 0) ar[k].y += er * a.y - ei * a.x;
+          }
+        }
+      }
+    }
+  }
+  __syncthreads();
+  // results: add into the level array, or the split partials
+  const int nc = (P + 1) * (P + 1);
+  for (int i = tid; i < V * TC; i += kTileThreads) {
+    const int c = i / TC, tt = i - c * TC;
+    if (!s_act[tt]) continue;
+    const int64_t plin = base + tt;
+    const T2 a = A[i];
+    if (p.nsplit > 1) {
+      ((T2*)p.partial_raw)[(((int64_t)split * 8 + tau) * V + c) * np + plin] = a;
+      continue;
+    }
+    const int px = (int)(plin % nx), py = (int)((plin / nx) % nx), pz = (int)(plin / ((int64_t)nx * nx));
+    const int64_t b = ((int64_t)morton(px, py, pz) << 3) | tau;
+    if (HELM) {
+      const int64_t o = layout_off(b, c, nc);
+      p.cout[2 * o] += a.x;
+      p.cout[2 * o + 1] += a.y;
+    } else {
+      const int n = s_nm[c] & 255, m = (s_nm[c] >> 8) - 64;
+      if (m == 0) {
+        p.cout[layout_off(b, n * n, nc)] += a.x;
+      } else {
+        const int id = lidx(n, m);
+        p.cout[layout_off(b, id, nc)] += a.x;
+        p.cout[layout_off(b, id + 1, nc)] += a.y;
+      }
+    }
+  }
+}
+
+}  // namespace
+
+template <typename T, bool HELM>
+bool tiles_supported(int Ns, int Nr) {
+  return Ns == Nr && Ns >= 2 && Ns <= 60 && pick_tc<T, HELM>(Ns) > 0;
+}
+
+template <typename T, bool HELM>
+int launch_m2l_tiles(const LanesParams<T>& p, const OpTables<T>& t,
+                     cudaStream_t s) {
+  {
+    int rc = ensure_tile_offsets();
+    if (rc) return rc;
+  }
+  const int TC = pick_tc<T, HELM>(p.N);
+  if (!TC) return set_error(-3, "M2L tiles: expansion order too large for shared memory");
+  const TilePlan q = tile_plan<T, HELM>(p.N, TC);
+  WBFMM_CUDA(cudaFuncSetAttribute(k_m2l_tiles<T, HELM>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)q.total));
+  const int64_t np = (int64_t)1 << (3 * (p.level - 1));
+  dim3 grid((unsigned)((np + TC - 1) / TC), 8, p.nsplit);
+  k_m2l_tiles<T, HELM><<<grid, kTileThreads, q.total, s>>>(p, t, TC);
+  WBFMM_CUDA(cudaGetLastError());
+  if (p.nsplit > 1) return launch_lanes_reduce<T, HELM>(p, s);
+  return 0;
+}
+
+template <typename T, bool HELM>
+int tiles_per_cta(int N) {
+  return pick_tc<T, HELM>(N);
+}
+
+#define WBFMM_TILES_INST(T, H)                                                   \
+  template bool tiles_supported<T, H>(int, int);                                 \
+  template int launch_m2l_tiles<T, H>(const LanesParams<T>&, const OpTables<T>&, \
+                                      cudaStream_t);                             \
+  template int tiles_per_cta<T, H>(int);
+WBFMM_TILES_INST(double, true)
+WBFMM_TILES_INST(double, false)
+WBFMM_TILES_INST(float, true)
+WBFMM_TILES_INST(float, false)
+
+}  // namespace wbfmm

@@ -42,7 +42,7 @@ struct Req {
   int64_t id = 0;
   wbfmm_b200_request_t r;
   int64_t footprint = 0;
-  double t_arrival = 0, t_start = 0, t_end = 0;   // server clock
+  double t_arrival = 0, t_start = 0, t_queued = 0, t_end = 0;   // server clock
   int state = 0;                                   // 0 queued, 1 running, 2 done
   int status = 0;
   char error[256] = "";
@@ -133,7 +133,7 @@ struct wbfmm_b200_server {
 
   // one solve on the slot's stream; fields land in the caller's arrays
   template <typename T>
-  int execute(Slot* s, Solver<T>* sv, const wbfmm_b200_request_t& r) {
+  int execute(Slot* s, Solver<T>* sv, const wbfmm_b200_request_t& r, double* t_queued) {
     const int w = r.cfg.problem == WBFMM_B200_HELMHOLTZ ? 2 : 1;
     const size_t ns = (size_t)r.nsrc, nt = (size_t)r.ntgt;
     const bool same = r.xt == r.xs && r.ntgt == r.nsrc;
@@ -161,6 +161,7 @@ struct wbfmm_b200_server {
     WBFMM_TRY(sv->run_async());
     WBFMM_TRY(sv->fetch_async(np ? s->out.p : nullptr, ng ? s->out.p + np : nullptr));
     WBFMM_CUDA(cudaEventRecord(s->done, s->stream));
+    *t_queued = clock();
     WBFMM_CUDA(cudaEventSynchronize(s->done));
     WBFMM_TRY(sv->check_flags());
     if (np) memcpy(r.pot, s->out.p, sizeof(double) * np);
@@ -173,10 +174,10 @@ struct wbfmm_b200_server {
     int rc;
     if (r.cfg.precision == WBFMM_B200_FP32) {
       rc = make_solver(s, &r.cfg, &s->s32);
-      if (!rc) rc = execute(s, s->s32, r);
+      if (!rc) rc = execute(s, s->s32, r, &q->t_queued);
     } else {
       rc = make_solver(s, &r.cfg, &s->s64);
-      if (!rc) rc = execute(s, s->s64, r);
+      if (!rc) rc = execute(s, s->s64, r, &q->t_queued);
     }
     if (rc) {
       // drain whatever was queued before the failure
@@ -343,14 +344,15 @@ int wbfmm_b200_server_wait(wbfmm_b200_server_t* srv, int64_t ticket) {
 }
 
 int wbfmm_b200_server_times(wbfmm_b200_server_t* srv, int64_t ticket,
-                            double* t3) {
-  if (!srv || !t3) return set_error(WBFMM_B200_E_ARG, "null argument");
+                            double* t4) {
+  if (!srv || !t4) return set_error(WBFMM_B200_E_ARG, "null argument");
   std::lock_guard<std::mutex> lk(srv->mu);
   auto it = srv->reqs.find(ticket);
   if (it == srv->reqs.end()) return set_error(WBFMM_B200_E_ARG, "unknown ticket");
-  t3[0] = it->second->t_arrival;
-  t3[1] = it->second->t_start;
-  t3[2] = it->second->t_end;
+  t4[0] = it->second->t_arrival;
+  t4[1] = it->second->t_start;
+  t4[2] = it->second->t_queued;
+  t4[3] = it->second->t_end;
   return it->second->state == 2 ? 0 : set_error(WBFMM_B200_E_STATE, "request not complete");
 }
 

@@ -199,9 +199,9 @@ int wbfmm_b200_tree_structure(int n, const double* pts, int pstr,
   }
   return 0;
 }
-int wbfmm_b200_set_m2l_kernel(wbfmm_b200_solver_t* s, int lanes) {
+int wbfmm_b200_set_m2l_kernel(wbfmm_b200_solver_t* s, int mode) {
   if (!s) return set_error(WBFMM_B200_E_ARG, "null solver");
-  s->set_m2l_kernel(lanes);
+  s->set_m2l_kernel(mode);
   return 0;
 }
 int wbfmm_b200_invalidate_operators(wbfmm_b200_solver_t* s) {

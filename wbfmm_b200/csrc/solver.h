@@ -204,7 +204,7 @@ struct Solver : public wbfmm_b200_solver {
   DBuf<T> partial;
   DBuf<unsigned char> lin;         // M2L lane kernel: transposed sources
   DBuf<T> lanes_part;              // and its split partial sums
-  bool use_lanes = true;
+  int m2l_mode = 1;                // 0 warp per target, 1 automatic, 2 lanes, 3 tiles
   bool tree_only = false;          // structure only: no coefficient arrays
   int eval_field = 3;              // fields evaluate() computes
   bool eval_neighbours = true;     // evaluate() adds the near field (P2P)
@@ -647,8 +647,49 @@ struct Solver : public wbfmm_b200_solver {
     x.coax_stride = sr_stride[level];
     x.width = (T)width(level);
     x.tmask = cfg.skip_empty && tmask[level].p ? tmask[level].p : nullptr;
-    if (use_lanes && (helm ? lanes_supported<T, true>(x.Nin, x.Nout)
-                           : lanes_supported<T, false>(x.Nin, x.Nout))) {
+    const bool lanes_ok = helm ? lanes_supported<T, true>(x.Nin, x.Nout)
+                               : lanes_supported<T, false>(x.Nin, x.Nout);
+    const bool tiles_ok = helm ? tiles_supported<T, true>(x.Nin, x.Nout)
+                               : tiles_supported<T, false>(x.Nin, x.Nout);
+    // automatic: lanes at the orders where their unrolled code wins, tiles
+    // above, the warp-per-target kernel for what neither covers
+    const int lanes_max = helm ? 8 : 12;
+    bool use_tiles = false, use_lanes = false;
+    if (m2l_mode == 1) {
+      use_lanes = lanes_ok && x.Nin <= lanes_max;
+      use_tiles = !use_lanes && tiles_ok;
+    } else if (m2l_mode == 2) {
+      use_lanes = lanes_ok;
+    } else if (m2l_mode == 3) {
+      use_tiles = tiles_ok;
+    }
+    if (use_tiles) {
+      // offset-major target tiles on the transposed singular expansions
+      WBFMM_TRY(lin.alloc(lanes_lin_bytes(level, x.Nin, helm, sizeof(T))));
+      WBFMM_TRY((helm ? lanes_to_lin<T, true>(x.cin, level, x.Nin, lin.p, stream)
+                      : lanes_to_lin<T, false>(x.cin, level, x.Nin, lin.p, stream)));
+      LanesParams<T> lp;
+      memset(&lp, 0, sizeof(lp));
+      lp.level = level; lp.N = x.Nin;
+      lp.lin_raw = lin.p; lp.cout = x.cout;
+      lp.coax = x.coax; lp.coax_stride = x.coax_stride;
+      lp.width = x.width; lp.tmask = x.tmask;
+      const int64_t np = (int64_t)1 << (3 * (level - 1));
+      const int tc = helm ? tiles_per_cta<T, true>(x.Nin) : tiles_per_cta<T, false>(x.Nin);
+      const int64_t ctas = ((np + tc - 1) / tc) * 8;
+      int ns = 1;
+      while (ctas * ns < 2 * 148 && ns < 32) ns *= 2;
+      lp.nsplit = ns;
+      if (ns > 1) {
+        const int V = helm ? (x.Nin + 1) * (x.Nin + 1) : (x.Nin + 1) * (x.Nin + 2) / 2;
+        WBFMM_TRY(lanes_part.alloc((size_t)ns * 8 * V * np * 2));
+        lp.partial_raw = lanes_part.p;
+      }
+      launches += ns > 1 ? 3 : 2;
+      return helm ? launch_m2l_tiles<T, true>(lp, tables, stream)
+                  : launch_m2l_tiles<T, false>(lp, tables, stream);
+    }
+    if (use_lanes) {
       // lane-per-pair kernel on a transposed copy of the singular expansions
       WBFMM_TRY(lin.alloc(lanes_lin_bytes(level, x.Nin, helm, sizeof(T))));
       WBFMM_TRY((helm ? lanes_to_lin<T, true>(x.cin, level, x.Nin, lin.p, stream)
@@ -847,7 +888,7 @@ struct Solver : public wbfmm_b200_solver {
   }
 
   void invalidate_operators() override { ops_ready = false; }
-  void set_m2l_kernel(int lanes) override { use_lanes = lanes != 0; }
+  void set_m2l_kernel(int mode) override { m2l_mode = mode; }
   void set_p2m_accumulate(int on) override { p2m_accumulate = on != 0; }
   void set_evaluation(int field, int neighbours) override {
     eval_field = field;

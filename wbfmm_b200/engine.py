@@ -253,8 +253,10 @@ class Solver:
     def downward_pass(self, level):
         _check(self.lib.wbfmm_b200_downward_pass(self.h, level))
 
-    def set_m2l_kernel(self, lanes: bool):
-        _check(self.lib.wbfmm_b200_set_m2l_kernel(self.h, int(bool(lanes))))
+    def set_m2l_kernel(self, mode):
+        """0 warp per target, 1 automatic (default), 2 lane per pair, 3 target
+        tiles; True / False select 1 / 0."""
+        _check(self.lib.wbfmm_b200_set_m2l_kernel(self.h, int(mode)))
 
     def m2l(self, level):
         _check(self.lib.wbfmm_b200_m2l(self.h, level))
@@ -424,8 +426,9 @@ class Server:
         return held[5], held[6]
 
     def times(self, ticket: int):
-        """(arrival, start, end) on the server clock, seconds."""
-        t = np.zeros(3)
+        """(arrival, start, queued, end) on the server clock, seconds: queued
+        is when the solve's device work had all been issued."""
+        t = np.zeros(4)
         _check(self._lib.wbfmm_b200_server_times(self._h, ticket, t.ctypes.data_as(C.POINTER(C.c_double))))
         return tuple(float(x) for x in t)
 
