@@ -27,6 +27,9 @@ int set_error(int code, const char* msg);
 const char* last_error();
 
 // ------------------------------------------------------------------ tree
+// *a = va and, when b is non-null, *b = vb (one thread, on stream s)
+void launch_set_words(uint32_t* a, uint32_t va, uint32_t* b, uint32_t vb,
+                      cudaStream_t s);
 // keys[i] = Morton key of point i (src/boxes.c:324-339); vals[i] = i
 void launch_point_keys(const double* pts, int64_t pstr, int n,
                        const double* x0, double D, uint64_t* keys,

@@ -113,6 +113,7 @@ struct wbfmm_b200_server {
       delete s;
     }
     for (auto& e : reqs) delete e.second;
+    cache.clear();
     if (pool) cudaMemPoolDestroy(pool);
   }
 
@@ -265,6 +266,7 @@ int wbfmm_b200_server_create(wbfmm_b200_server_t** out, int nslots,
     delete srv;
     return set_error(WBFMM_B200_E_NOMEM, "server: memory pool creation failed");
   }
+  srv->cache.pool = srv->pool;
   uint64_t thr = UINT64_MAX;
   int off = 0;
   cudaMemPoolSetAttribute(srv->pool, cudaMemPoolAttrReleaseThreshold, &thr);

@@ -337,8 +337,7 @@ struct Solver : public wbfmm_b200_solver {
       dpts = pts_in.p;
     }
     // strict-interior domain check (src/boxes.c:148-153)
-    int big = 0x7fffffff;
-    WBFMM_CUDA(cudaMemcpyAsync(flag.p, &big, sizeof(int), cudaMemcpyHostToDevice, stream));
+    launch_set_words((uint32_t*)flag.p, 0x7fffffffu, nullptr, 0, stream);
     launch_domain_check(dpts, xs_str, n, cfg.x0, cfg.D, flag.p, stream);
     if (!async_checks) {
       int bad = 0;
@@ -350,7 +349,7 @@ struct Solver : public wbfmm_b200_solver {
     WBFMM_TRY(ip.alloc(n));
     launch_point_keys(dpts, xs_str, n, cfg.x0, cfg.D, keys.p, ip.p, stream);
     WBFMM_TRY(radix_sort_pairs(keys.p, ip.p, n, 60, &rs, stream));
-    launches += 2 + 3 * 8;
+    launches += 4 + 3 * 8;
     WBFMM_TRY(sx.alloc(n)); WBFMM_TRY(sy.alloc(n)); WBFMM_TRY(sz.alloc(n));
     launch_gather_points(dpts, xs_str, ip.p, n, sx.p, sy.p, sz.p, stream);
     launches++;
@@ -375,9 +374,7 @@ struct Solver : public wbfmm_b200_solver {
     }
     // levels: box {i, n} by repeated refinement (src/boxes.c:208-277)
     WBFMM_TRY(box_i[0].alloc(1)); WBFMM_TRY(box_n[0].alloc(1));
-    uint32_t root[2] = {0u, (uint32_t)n};
-    WBFMM_CUDA(cudaMemcpyAsync(box_i[0].p, &root[0], 4, cudaMemcpyHostToDevice, stream));
-    WBFMM_CUDA(cudaMemcpyAsync(box_n[0].p, &root[1], 4, cudaMemcpyHostToDevice, stream));
+    launch_set_words(box_i[0].p, 0u, box_n[0].p, (uint32_t)n, stream);
     for (int l = 1; l <= depth; l++) {
       size_t nb = (size_t)1 << (3 * l);
       WBFMM_TRY(box_i[l].alloc(nb)); WBFMM_TRY(box_n[l].alloc(nb));
@@ -438,8 +435,7 @@ struct Solver : public wbfmm_b200_solver {
                                  cudaMemcpyHostToDevice, stream));
       d = tpts_in.p;
     }
-    int zero = 0;
-    WBFMM_CUDA(cudaMemcpyAsync(flag.p + 1, &zero, sizeof(int), cudaMemcpyHostToDevice, stream));
+    WBFMM_CUDA(cudaMemsetAsync(flag.p + 1, 0, sizeof(int), stream));
     WBFMM_TRY(tkeys.alloc(n)); WBFMM_TRY(tperm.alloc(n));
     launch_target_keys(d, tstr, n, cfg.x0, cfg.D, depth, tkeys.p, tperm.p,
                        flag.p + 1, stream);

@@ -90,13 +90,17 @@ struct TableCache {
   using Key = std::tuple<int, uint64_t, int>;
 
   std::mutex mu;
+  cudaMemPool_t pool = nullptr;   // stream-ordered allocations when set
   std::vector<Geo*> geos;
   std::map<Key, Coax*> coax;
   size_t coax_bytes = 0, coax_cap = (size_t)4 << 30;
   uint64_t tick = 0;
   int64_t hits = 0, misses = 0;
 
-  ~TableCache() {
+  ~TableCache() { clear(); }
+
+  // release every table (no solve may be using them)
+  void clear() {
     for (Geo* g : geos) {
       void* ps[] = {g->H64, g->H32, g->op_ith, g->op_dist, g->r64, g->r32,
                     g->ph64, g->ph32, g->ch64, g->ch32, g->lap64[0], g->lap64[1],
@@ -105,19 +109,31 @@ struct TableCache {
       if (g->ready) cudaEventDestroy(g->ready);
       delete g;
     }
-    for (auto& e : coax) drop(e.second);
+    geos.clear();
+    for (auto& e : coax) drop(e.second, nullptr);
+    coax.clear();
+    coax_bytes = 0;
   }
 
-  void drop(Coax* c) {
-    cudaFree(c->d64);
-    cudaFree(c->d32);
+  // frees stream-ordered on s when given (the entry is unreferenced, so no
+  // queued work reads it), else synchronously
+  void drop(Coax* c, cudaStream_t s) {
+    if (s) {
+      cudaFreeAsync(c->d64, s);
+      cudaFreeAsync(c->d32, s);
+    } else {
+      cudaFree(c->d64);
+      cudaFree(c->d32);
+    }
     if (c->ready) cudaEventDestroy(c->ready);
     delete c;
   }
 
   template <typename X>
-  static int dalloc(X** p, size_t n) {
-    if (cudaMalloc(p, sizeof(X) * (n ? n : 1)) != cudaSuccess) {
+  int dalloc(X** p, size_t n, cudaStream_t s) {
+    cudaError_t e = pool ? cudaMallocFromPoolAsync((void**)p, sizeof(X) * (n ? n : 1), pool, s)
+                         : cudaMalloc(p, sizeof(X) * (n ? n : 1));
+    if (e != cudaSuccess) {
       cudaGetLastError();
       *p = nullptr;
       return set_error(WBFMM_B200_E_NOMEM, "table cache allocation failed");
@@ -148,14 +164,14 @@ struct TableCache {
     std::vector<double> r, ph, ch;
     shift_op_tables(geom, L, ith, dist, r, ph, ch);
     const size_t nph = ph.size();
-    WBFMM_CACHE_TRY(dalloc(&g->op_ith, kNumOps));
-    WBFMM_CACHE_TRY(dalloc(&g->op_dist, kNumOps));
-    WBFMM_CACHE_TRY(dalloc(&g->r64, kNumOps));
-    WBFMM_CACHE_TRY(dalloc(&g->r32, kNumOps));
-    WBFMM_CACHE_TRY(dalloc(&g->ph64, nph));
-    WBFMM_CACHE_TRY(dalloc(&g->ph32, nph));
-    WBFMM_CACHE_TRY(dalloc(&g->ch64, nph));
-    WBFMM_CACHE_TRY(dalloc(&g->ch32, nph));
+    WBFMM_CACHE_TRY(dalloc(&g->op_ith, kNumOps, s));
+    WBFMM_CACHE_TRY(dalloc(&g->op_dist, kNumOps, s));
+    WBFMM_CACHE_TRY(dalloc(&g->r64, kNumOps, s));
+    WBFMM_CACHE_TRY(dalloc(&g->r32, kNumOps, s));
+    WBFMM_CACHE_TRY(dalloc(&g->ph64, nph, s));
+    WBFMM_CACHE_TRY(dalloc(&g->ph32, nph, s));
+    WBFMM_CACHE_TRY(dalloc(&g->ch64, nph, s));
+    WBFMM_CACHE_TRY(dalloc(&g->ch32, nph, s));
     WBFMM_CUDA(cudaMemcpyAsync(g->op_ith, ith.data(), sizeof(int) * kNumOps, cudaMemcpyHostToDevice, s));
     WBFMM_CUDA(cudaMemcpyAsync(g->op_dist, dist.data(), sizeof(int) * kNumOps, cudaMemcpyHostToDevice, s));
     WBFMM_CUDA(cudaMemcpyAsync(g->r64, r.data(), sizeof(double) * kNumOps, cudaMemcpyHostToDevice, s));
@@ -167,14 +183,14 @@ struct TableCache {
     g->hstride = rot_count(L) + 8;
     g->nth = (int)geom.thetas.size();
     const size_t nh = (size_t)g->hstride * g->nth;
-    WBFMM_CACHE_TRY(dalloc(&g->H64, nh));
-    WBFMM_CACHE_TRY(dalloc(&g->H32, nh));
+    WBFMM_CACHE_TRY(dalloc(&g->H64, nh, s));
+    WBFMM_CACHE_TRY(dalloc(&g->H32, nh, s));
     WBFMM_CACHE_TRY(generate_rotation_tables(geom.thetas, L, g->H64, g->hstride, s));
     WBFMM_CACHE_TRY(narrow(g->H64, g->H32, (int64_t)nh, s));
     const size_t n3 = (size_t)(L + 1) * (L + 1) * (L + 1);
     for (int i = 0; i < 3; i++) {
-      WBFMM_CACHE_TRY(dalloc(&g->lap64[i], n3));
-      WBFMM_CACHE_TRY(dalloc(&g->lap32[i], n3));
+      WBFMM_CACHE_TRY(dalloc(&g->lap64[i], n3, s));
+      WBFMM_CACHE_TRY(dalloc(&g->lap32[i], n3, s));
     }
     WBFMM_CACHE_TRY(generate_laplace_tables(L, g->lap64[0], g->lap64[1], g->lap64[2], s));
     for (int i = 0; i < 3; i++) WBFMM_CACHE_TRY(narrow(g->lap64[i], g->lap32[i], (int64_t)n3, s));
@@ -246,21 +262,21 @@ struct TableCache {
         nc = 1;
       }
       c->count = per * nc * (int64_t)krs.size();
-      int rc = dalloc(&c->d64, (size_t)c->count);
-      if (!rc) rc = dalloc(&c->d32, (size_t)c->count);
+      int rc = dalloc(&c->d64, (size_t)c->count, s);
+      if (!rc) rc = dalloc(&c->d32, (size_t)c->count, s);
       if (!rc) rc = generate_coaxial_tables(krs, L, nc, c->d64, per * nc, s);
       if (!rc) rc = narrow(c->d64, c->d32, c->count, s);
       cudaError_t e = cudaSuccess;
       if (!rc) e = cudaEventCreateWithFlags(&c->ready, cudaEventDisableTiming);
       if (!rc && e == cudaSuccess) e = cudaEventRecord(c->ready, s);
       if (!rc && e != cudaSuccess) rc = set_cuda_error(e, __FILE__, __LINE__);
-      if (rc) { drop(c); return rc; }
+      if (rc) { drop(c, s); return rc; }
       coax[key] = c;
       coax_bytes += (size_t)c->count * 12;
     }
     c->refs++;
     c->last = ++tick;
-    evict();
+    evict(s);
     *out = sizeof(T) == 4 ? (const T*)c->d32 : (const T*)c->d64;
     *ref = c;
     return 0;
@@ -272,7 +288,7 @@ struct TableCache {
   }
 
   // drop least recently used unreferenced entries above the cap (mu held)
-  void evict() {
+  void evict(cudaStream_t s) {
     while (coax_bytes > coax_cap) {
       auto victim = coax.end();
       for (auto it = coax.begin(); it != coax.end(); ++it)
@@ -281,7 +297,7 @@ struct TableCache {
           victim = it;
       if (victim == coax.end()) return;
       coax_bytes -= (size_t)victim->second->count * 12;
-      drop(victim->second);
+      drop(victim->second, s);
       coax.erase(victim);
     }
   }

@@ -222,8 +222,17 @@ __global__ void k_coaxial_tables(const Vals64 krs, int L, int nc,
     }
     __syncthreads();
   }
-  // G&D (4.79) for m >= 1
-  for (int m = 1; m <= L; m++) {
+}
+
+// G&D (4.79) for each order m >= 1 (independent of the other orders once
+// the (4.84) diagonal is in place), one block per (m, table); then the
+// order-m entries l <= L are copied out.  Block m = 0 only copies.
+__global__ void k_coaxial_orders(int L, int nc, double* __restrict__ out,
+                                 int64_t ostride, double* __restrict__ scratch,
+                                 int64_t sstride) {
+  const int m = blockIdx.x, it = blockIdx.y;
+  double* cf = scratch + (int64_t)it * sstride;
+  if (m >= 1) {
     for (int n = m; n <= L; n++) {
       for (int l = n + 1 + threadIdx.x; l <= 2 * L - n; l += blockDim.x) {
         int i1 = coax_idx(l, m, n - 1), i2 = coax_idx(l, m, n + 1);
@@ -239,9 +248,12 @@ __global__ void k_coaxial_tables(const Vals64 krs, int L, int nc,
       __syncthreads();
     }
   }
-  const int64_t cnt = (int64_t)(L + 1) * (L + 2) * (L + 3) / 6;
-  for (int64_t i = threadIdx.x; i < cnt * nc; i += blockDim.x)
-    out[(int64_t)it * ostride + i] = cf[i];
+  // entries (l, m, n), m <= n <= l <= L
+  for (int l = m; l <= L; l++)
+    for (int n = m + threadIdx.x; n <= l; n += blockDim.x) {
+      const int64_t i = coax_idx(l, m, n);
+      for (int c = 0; c < nc; c++) out[(int64_t)it * ostride + nc * i + c] = cf[nc * i + c];
+    }
 }
 
 int generate_coaxial_tables(const std::vector<double>& krs, int L, int nc,
@@ -257,6 +269,8 @@ int generate_coaxial_tables(const std::vector<double>& krs, int L, int nc,
   int64_t sstride = ((int64_t)coax_idx(LL, LL, LL) + 2) * nc;
   WBFMM_CUDA(cudaMallocAsync(&scratch, sizeof(double) * sstride * nt, s));
   k_coaxial_tables<<<nt, 128, 0, s>>>(kv, L, nc, dout, ostride, scratch, sstride);
+  WBFMM_CUDA(cudaGetLastError());
+  k_coaxial_orders<<<dim3(L + 1, nt), 64, 0, s>>>(L, nc, dout, ostride, scratch, sstride);
   WBFMM_CUDA(cudaGetLastError());
   WBFMM_CUDA(cudaFreeAsync(scratch, s));
   return 0;

@@ -80,6 +80,19 @@ __global__ void k_target_keys(const double* __restrict__ pts, int64_t pstr,
   vals[i] = (uint32_t)i;
 }
 
+// *a = va and, when b is given, *b = vb: device-side initialisation of
+// flags and roots, so that no pageable host->device copy (which may wait for
+// the stream to drain) sits in the middle of a solve
+__global__ void k_set_words(uint32_t* a, uint32_t va, uint32_t* b, uint32_t vb) {
+  *a = va;
+  if (b) *b = vb;
+}
+
+void launch_set_words(uint32_t* a, uint32_t va, uint32_t* b, uint32_t vb,
+                      cudaStream_t s) {
+  k_set_words<<<1, 1, 0, s>>>(a, va, b, vb);
+}
+
 void launch_target_keys(const double* pts, int64_t pstr, int n,
                         const double* x0, double D, int level,
                         uint64_t* keys, uint32_t* vals, int* bad,
