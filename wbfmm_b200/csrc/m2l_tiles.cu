@@ -80,11 +80,21 @@ __host__ __device__ TilePlan tile_plan(int P, int TC) {
 
 constexpr size_t kTileSmemCap = 220 * 1024;
 
+// Targets per CTA: the tile kernel is latency-bound (one offset's stages are
+// separated by barriers), so prefer the TC that keeps the most targets
+// resident per SM (228 KB of shared memory, 1 KB reserved per CTA), and on a
+// tie the smaller TC (more CTAs, more warps to switch between).
 template <typename T, bool HELM>
 int pick_tc(int P) {
-  for (int tc = 32; tc >= 8; tc >>= 1)
-    if (tile_plan<T, HELM>(P, tc).total <= kTileSmemCap) return tc;
-  return 0;
+  int best = 0, best_score = 0;
+  for (int tc = 32; tc >= 8; tc >>= 1) {
+    const size_t bytes = tile_plan<T, HELM>(P, tc).total;
+    if (bytes > kTileSmemCap) continue;
+    const int ctas = (int)((228 * 1024) / (bytes + 1024));
+    const int score = ctas * tc;
+    if (score >= best_score) { best = tc; best_score = score; }
+  }
+  return best;
 }
 
 template <typename T2, typename T>

@@ -649,7 +649,7 @@ struct Solver : public wbfmm_b200_solver {
                                : tiles_supported<T, false>(x.Nin, x.Nout);
     // automatic: lanes at the orders where their unrolled code wins, tiles
     // above, the warp-per-target kernel for what neither covers
-    const int lanes_max = helm ? 8 : 12;
+    const int lanes_max = helm ? 8 : 10;
     bool use_tiles = false, use_lanes = false;
     if (m2l_mode == 1) {
       use_lanes = lanes_ok && x.Nin <= lanes_max;
