@@ -205,6 +205,7 @@ struct Solver : public wbfmm_b200_solver {
   DBuf<unsigned char> lin;         // M2L lane kernel: transposed sources
   DBuf<T> lanes_part;              // and its split partial sums
   int m2l_mode = 1;                // 0 warp per target, 1 automatic, 2 lanes, 3 tiles
+  int64_t lanes_ctas = 1200;       // lane kernel: split offsets below this many CTAs
   bool tree_only = false;          // structure only: no coefficient arrays
   int eval_field = 3;              // fields evaluate() computes
   bool eval_neighbours = true;     // evaluate() adds the near field (P2P)
@@ -699,7 +700,7 @@ struct Solver : public wbfmm_b200_solver {
       const int64_t np = (int64_t)1 << (3 * (level - 1));
       const int64_t base = ((np + 127) / 128) * 8;
       int ns = 1;
-      while (base * ns < 1200 && ns < 32) ns *= 2;
+      while (base * ns < lanes_ctas && ns < 32) ns *= 2;
       lp.nsplit = ns;
       if (ns > 1) {
         const int V = helm ? (x.Nin + 1) * (x.Nin + 1) : (x.Nin + 1) * (x.Nin + 2) / 2;
