@@ -1,6 +1,6 @@
 /*
  * Harness around the UNMODIFIED wbfmm reference sources (built from
- * /root/reference/src by oracle/build_oracle.py into
+ * the reference's src/ directory by oracle/build_oracle.py into
  * oracle/_ref/libwbfmm_ref.so).  It replays the reference drivers' call
  * sequence on in-memory inputs, with no text I/O:
  *

@@ -144,12 +144,14 @@ k_m2l_lanes(LanesParams<T> p, OpTables<T> t) {
   T2* w = cols + (size_t)warp * 2 * V * 32 + lane;   // working vector, stride 32
   T2* acc = w + (size_t)V * 32;                      // accumulator, stride 32
 
-  const int tau = blockIdx.y;
+  // the 8 child types of one parent tile are adjacent in the grid, so the
+  // CTAs that read the same source neighbourhood run together (L2 reuse)
+  const int tau = blockIdx.x & 7;
   const int split = blockIdx.z;
   const int nx = 1 << (p.level - 1), npx = nx + 2;
   const int64_t npp = (int64_t)npx * npx * npx;
   const int64_t np = (int64_t)nx * nx * nx;
-  const int64_t plin = (int64_t)blockIdx.x * kLanesCTA + threadIdx.x;
+  const int64_t plin = (int64_t)(blockIdx.x >> 3) * kLanesCTA + threadIdx.x;
   bool active = plin < np;
   int64_t pp = 0, pmort = 0;
   if (active) {
@@ -469,7 +471,7 @@ static int launch_lanes_P(const LanesParams<T>& p, const OpTables<T>& t,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)SM::bytes));
   const int64_t np = (int64_t)1 << (3 * (p.level - 1));
-  dim3 grid((unsigned)((np + SM::CTA - 1) / SM::CTA), 8, p.nsplit);
+  dim3 grid((unsigned)(8 * ((np + SM::CTA - 1) / SM::CTA)), 1, p.nsplit);
   k_m2l_lanes<T, HELM, P><<<grid, SM::CTA, SM::bytes, s>>>(p, t);
   WBFMM_CUDA(cudaGetLastError());
   if (p.nsplit > 1) return launch_lanes_reduce<T, HELM>(p, s);

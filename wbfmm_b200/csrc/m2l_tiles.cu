@@ -127,11 +127,12 @@ k_m2l_tiles(LanesParams<T> p, OpTables<T> t, int TC) {
   T2* A = Y + (size_t)V * TC;
   const int tid = threadIdx.x;
 
-  const int tau = blockIdx.y, split = blockIdx.z;
+  // child types of one target tile adjacent in the grid: shared sources
+  const int tau = blockIdx.x & 7, split = blockIdx.z;
   const int nx = 1 << (p.level - 1), npx = nx + 2;
   const int64_t npp = (int64_t)npx * npx * npx;
   const int64_t np = (int64_t)nx * nx * nx;
-  const int64_t base = (int64_t)blockIdx.x * TC;
+  const int64_t base = (int64_t)(blockIdx.x >> 3) * TC;
 
   // stage descriptors: B/D rows (n, nu0) and C rows (m, n0), 2 rows each
   if (tid == 0) {
@@ -448,7 +449,7 @@ int launch_m2l_tiles(const LanesParams<T>& p, const OpTables<T>& t,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)q.total));
   const int64_t np = (int64_t)1 << (3 * (p.level - 1));
-  dim3 grid((unsigned)((np + TC - 1) / TC), 8, p.nsplit);
+  dim3 grid((unsigned)(8 * ((np + TC - 1) / TC)), 1, p.nsplit);
   k_m2l_tiles<T, HELM><<<grid, kTileThreads, q.total, s>>>(p, t, TC);
   WBFMM_CUDA(cudaGetLastError());
   if (p.nsplit > 1) return launch_lanes_reduce<T, HELM>(p, s);
