@@ -74,6 +74,28 @@ def list4_pairs(depth: int) -> list[int]:
     return out
 
 
+def list4_pairs_at(xt, x0, D, level: int) -> int:
+    """(target box, list-4 source) pairs of the boxes at `level` that hold
+    one of the points xt (the M2L work of a skip_empty solve)."""
+    n = 1 << level
+    ijk = np.floor((np.asarray(xt) - np.asarray(x0)) / (D / n)).astype(np.int64)
+    ijk = np.unique(np.clip(ijk, 0, n - 1), axis=0)
+    i0 = ijk - ijk % 2
+    i1 = np.minimum(i0 + 3, n - 1)
+    lo = np.where(i0 > 0, i0 - 2, i0)
+    span = i1 - lo + 1
+    near = np.minimum(ijk + 1, n - 1) - np.maximum(ijk - 1, 0) + 1
+    return int((span.prod(axis=1) - near.prod(axis=1)).sum())
+
+
+def lap_flops_per_pair(p: int) -> int:
+    """Algorithmic FLOPs of one Laplace rotate/coaxial/rotate-back shift on
+    half vectors: 2*2*R(p) + 2*X_L(p), X_L(p) = (p+1)^2 + 2 sum_m (p+1-m)^2."""
+    R = (p + 1) * (2 * p + 1) * (2 * p + 3) // 3
+    XL = (p + 1) ** 2 + 2 * sum((p + 1 - m) ** 2 for m in range(1, p + 1))
+    return 2 * 2 * R + 2 * XL
+
+
 def helm_flops_per_pair(p: int) -> int:
     """Algorithmic FLOPs of one Helmholtz rotate/coaxial/rotate-back shift:
     2*4*R(p) + 8*X(p), R(p) = sum (2n+1)^2, X(p) = coaxial MACs."""
@@ -244,10 +266,10 @@ def served_section(args, ws, rank, local):
     def plain_prec(p):
         return engine.FP64
 
-    def run_batch(srv, batch, precf, keep=0):
+    def run_batch(srv, batch, precf, skip, keep=0):
         dist_barrier(ws)
         t0 = srv.clock()
-        tk = [srv.submit(p, precf(p)) for p in batch]
+        tk = [srv.submit(p, precf(p), skip_empty=skip) for p in batch]
         srv.drain()
         span = max(srv.times(t)[3] for t in tk) - t0
         kept = [tuple(a.copy() for a in srv.wait(t)) for t in tk[:keep]]
@@ -255,10 +277,11 @@ def served_section(args, ws, rank, local):
             srv.forget(t)
         return dist_max(span, ws), kept
 
-    def run_latency(srv, reqs, precf, rate):
+    def run_latency(srv, reqs, precf, skip, rate):
         arr = W.poisson_arrivals(len(reqs), rate, seed=104 + rank)
         base = srv.clock() + 0.02
-        tk = [srv.submit(p, precf(p), arrival=base + a) for p, a in zip(reqs, arr)]
+        tk = [srv.submit(p, precf(p), arrival=base + a, skip_empty=skip)
+              for p, a in zip(reqs, arr)]
         srv.drain()
         T = np.array([srv.times(t) for t in tk])
         for t in tk:
@@ -270,25 +293,30 @@ def served_section(args, ws, rank, local):
 
     out = {}
     kept = None
-    for name, slots, precf in (("plain_fp64", 1, plain_prec), ("served", SERVE_SLOTS, served_prec)):
+    # the plain form computes every box's local expansion, as the reference
+    # does; the served form only those of boxes that hold targets
+    arms = (("plain_fp64", 1, plain_prec, False), ("served", SERVE_SLOTS, served_prec, True))
+    for name, slots, precf, skip in arms:
         with engine.Server(slots=slots) as srv:
-            run_batch(srv, batches[0], precf)                    # warm-up
+            run_batch(srv, batches[0], precf, skip)              # warm-up
             spans = []
             with ClockSampler(local) as clk:
                 for i, b in enumerate(batches[1:]):
-                    span, k = run_batch(srv, b, precf, keep=8 if (name == "served" and i == 0) else 0)
+                    span, k = run_batch(srv, b, precf, skip,
+                                        keep=8 if (name == "served" and i == 0) else 0)
                     spans.append(span)
                     if k:
                         kept = k
             pts = sum(p.points for b in batches[1:] for p in b)
             out[name] = {"points_per_s": ws * pts / sum(spans), "seconds": sum(spans),
                          "requests": len(batches[1:]) * SERVE_BATCH, "slots": slots,
+                         "skip_empty": skip,
                          "clocks": clk.summary(), "stats": srv.stats()}
     rate_req = 0.7 * out["served"]["points_per_s"] / ws / np.mean(
         [p.points for b in batches[1:] for p in b])
-    for name, slots, precf in (("served", SERVE_SLOTS, served_prec), ("plain_fp64", 1, plain_prec)):
+    for name, slots, precf, skip in arms[::-1]:
         with engine.Server(slots=slots) as srv:
-            out[name]["latency"] = run_latency(srv, lat_reqs, precf, rate_req)
+            out[name]["latency"] = run_latency(srv, lat_reqs, precf, skip, rate_req)
     # accuracy of served fields against the FP64 direct sum
     worst, checked = 0.0, []
     for p, (pot, grad) in zip(batches[1][:8], kept or []):
@@ -316,6 +344,29 @@ def served_section(args, ws, rank, local):
     }
 
 
+# ------------------------------------------------------------ workloads
+# name -> (builder, accuracy subsample size and seed, skip_empty, label)
+def workload(args, rank):
+    """The problem of --workload: the benchmark's configurations (seeded,
+    synthetic; the reference names no dataset)."""
+    from wbfmm_b200 import workloads as W
+    w = args.workload
+    if w == "cube":
+        p = W.helmholtz_cube(args.points, k=8.0, depth=args.depth, seed=2 + rank)
+        return p, 10_000, 102, False, WORKLOAD
+    if w == "laplace_c1":
+        p = W.laplace_cube(20_000, 20_000, depth=4, order=12, seed=1 + rank)
+        return p, 20_000, 101, False, "laplace_cube_2e4_separate_targets_depth4_p12"
+    if w == "sphere_c3":
+        # per-level order p = kw + 1.8*6^(2/3)*(kw)^(1/3), floor 6, unclamped
+        p = W.helmholtz_sphere(2_000_000, 500_000, k=40.0, depth=7, seed=3 + rank, hi=None)
+        return p, 10_000, 103, True, "helmholtz_sphere_2e6_half_dipoles_5e5_targets_k40_depth7"
+    if w == "clusters_c5":
+        p = W.laplace_clusters(16_000_000, depth=8, order=10, seed=5 + rank)
+        return p, 20_000, 105, True, "laplace_8_gaussian_clusters_1.6e7_depth8_p10"
+    raise SystemExit(f"unknown workload {w}")
+
+
 # ----------------------------------------------------------- our arm
 def our_arm(args, ws, rank, local):
     import torch
@@ -326,22 +377,29 @@ def our_arm(args, ws, rank, local):
     torch.cuda.set_device(dev)
     stream = torch.cuda.Stream(dev)     # the solvers' stream; events on it
     torch.cuda.set_stream(stream)
-    n = args.points
-    p = W.helmholtz_cube(n, k=8.0, depth=args.depth, seed=2 + rank)
+    p, n_acc, acc_seed, skip_empty, label = workload(args, rank)
+    helm = p.problem == W.HELMHOLTZ
+    w = 2 if helm else 1
+    ns, nt = p.ns, p.nt
     field = engine.POTENTIAL | engine.GRADIENT
+
+    def dev_arr(a):
+        return None if a is None else torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+
     # device-resident inputs
-    xs_d = torch.from_numpy(np.ascontiguousarray(p.xs)).to(dev)
-    q_d = torch.from_numpy(np.ascontiguousarray(p.q)).to(dev)
+    xs_d, q_d = dev_arr(p.xs), dev_arr(p.q)
+    nrm_d, dip_d = dev_arr(p.normals), dev_arr(p.dipoles)
+    xt_d = xs_d if p.targets_are_sources else dev_arr(p.xt)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
 
     def make(precision):
-        cfg = engine.SolverConfig.from_problem(p, precision, field)
+        cfg = engine.SolverConfig.from_problem(p, precision, field, skip_empty)
         return engine.Solver(cfg, stream=stream.cuda_stream)
 
     def step(s):
-        s.set_sources(xs_d, on_device=True)
-        s.set_strengths(q_d, on_device=True)
-        s.set_targets(xs_d, on_device=True)
+        s.set_sources(xs_d, nrm_d, on_device=True)
+        s.set_strengths(q_d, dip_d, on_device=True)
+        s.set_targets(xt_d, on_device=True)
         s.invalidate_operators()
         s.run()
 
@@ -381,19 +439,30 @@ def our_arm(args, ws, rank, local):
             m2l_ms[lv] = a.elapsed_time(b)
         pot, grad = s.field()
         results[name] = dict(ms=ms, step_ms=step_ms, launches=launches, stages=stages, m2l_ms=m2l_ms,
-                             pot=pot, grad=grad, clocks=clk.summary(), solver=s)
+                             pot=pot, grad=grad, clocks=clk.summary())
+        if name == "fp64":
+            s.close()                      # room for the FP32 solver's buffers
+            torch.cuda.synchronize()
+        else:
+            results[name]["solver"] = s
 
     # e2e through the C ABI with pinned host buffers (FP32 form)
-    xs_h = torch.from_numpy(np.ascontiguousarray(p.xs)).pin_memory()
-    q_h = torch.from_numpy(np.ascontiguousarray(p.q)).pin_memory()
-    pot_h = torch.empty(2 * n, dtype=torch.float64).pin_memory()
-    grad_h = torch.empty(6 * n, dtype=torch.float64).pin_memory()
+    def pinned(a):
+        return None if a is None else torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+
+    xs_h, q_h, nrm_h, dip_h = pinned(p.xs), pinned(p.q), pinned(p.normals), pinned(p.dipoles)
+    xt_h = xs_h if p.targets_are_sources else pinned(p.xt)
+    pot_h = torch.empty(w * nt, dtype=torch.float64).pin_memory()
+    grad_h = torch.empty(3 * w * nt, dtype=torch.float64).pin_memory()
     s = results["fp32"]["solver"]
 
+    def ptr(t):
+        return None if t is None else t.data_ptr()
+
     def e2e_step():
-        s.lib.wbfmm_b200_set_sources(s.h, n, xs_h.data_ptr(), 3, None, 3, 0)
-        s.lib.wbfmm_b200_set_strengths(s.h, q_h.data_ptr(), 2, None, 2, 0)
-        s.lib.wbfmm_b200_set_targets(s.h, n, xs_h.data_ptr(), 3, 0)
+        s.lib.wbfmm_b200_set_sources(s.h, ns, ptr(xs_h), 3, ptr(nrm_h), 3, 0)
+        s.lib.wbfmm_b200_set_strengths(s.h, ptr(q_h), w, ptr(dip_h), w, 0)
+        s.lib.wbfmm_b200_set_targets(s.h, nt, ptr(xt_h), 3, 0)
         s.invalidate_operators()
         s.run()
         rc = s.lib.wbfmm_b200_get_field(s.h, pot_h.data_ptr(), grad_h.data_ptr(), 0)
@@ -409,18 +478,21 @@ def our_arm(args, ws, rank, local):
         e2e_step()
     torch.cuda.synchronize()
     e2e_s = dist_max((time.perf_counter() - t0) / args.steps, ws)
+    h2d = sum(t.numel() * 8 for t in (xs_h, q_h, nrm_h, dip_h) if t is not None)
+    h2d += xt_h.numel() * 8     # targets are copied even when they are the sources
     e2e = {"value": ws * p.points / e2e_s, "unit": "points/s",
-           "ms_per_step": e2e_s * 1e3,
-           "h2d_bytes_per_step": int(xs_h.numel() * 8 * 2 + q_h.numel() * 8),
+           "ms_per_step": e2e_s * 1e3, "h2d_bytes_per_step": int(h2d),
            "d2h_bytes_per_step": int((pot_h.numel() + grad_h.numel()) * 8)}
+    s.close()
 
-    # accuracy vs the FP64 direct sum on 10,000 random targets
-    idx = W.subsample(102, n, 10_000)
-    dpot, dgrad = engine.direct(W.HELMHOLTZ, p.xs, p.q, p.xs[idx], k=p.k)
-    acc = {}
+    # accuracy vs the FP64 direct sum on a seeded subsample of the targets
+    idx = W.subsample(acc_seed, nt, n_acc)
+    dpot, dgrad = engine.direct(p.problem, p.xs, p.q, p.xt[idx], k=p.k,
+                                normals=p.normals, dipoles=p.dipoles)
+    acc = {"targets_checked": int(len(idx))}
     for name in ("fp64", "fp32"):
-        pot = results[name]["pot"].reshape(-1, 2)[idx].ravel()
-        grad = results[name]["grad"].reshape(-1, 6)[idx].ravel()
+        pot = results[name]["pot"].reshape(-1, w)[idx].ravel()
+        grad = results[name]["grad"].reshape(-1, 3 * w)[idx].ravel()
         acc[name] = {
             "pot_rel_l2": float(np.linalg.norm(pot - dpot) / np.linalg.norm(dpot)),
             "grad_rel_l2": float(np.linalg.norm(grad - dgrad) / np.linalg.norm(dgrad)),
@@ -434,19 +506,24 @@ def our_arm(args, ws, rank, local):
     # the rotate / coaxial / rotate-back shifts per launch / launch time
     pairs = list4_pairs(p.depth)
     lv_dom = max(f32["m2l_ms"], key=lambda lv: f32["m2l_ms"][lv])
-    flops = pairs[lv_dom] * helm_flops_per_pair(p.order_s[lv_dom])
+    if skip_empty:
+        pairs[lv_dom] = list4_pairs_at(p.xt, p.x0, p.D, lv_dom)
+    fpp = helm_flops_per_pair if helm else lap_flops_per_pair
+    flops = pairs[lv_dom] * fpp(p.order_s[lv_dom])
     achieved = flops / (f32["m2l_ms"][lv_dom] * 1e-3) / 1e12
     peak_fp32 = 148 * 128 * 2 * 1.965e9 / 1e12
-    roofline = {"bound": "simt", "kernel": f"k_m2l<float,true> level {lv_dom}",
+    roofline = {"bound": "simt", "kernel": f"M2L level {lv_dom}, order {p.order_s[lv_dom]}, FP32",
                 "achieved": achieved, "peak": peak_fp32, "unit": "TFLOP/s",
                 "frac": achieved / peak_fp32, "traffic": None,
                 "peak_source": "nominal FP32 SIMT peak (148 SMs x 128 FMA/clk x 1.965 GHz); "
                                "MEASURED_PEAKS.json holds no SIMT figure",
                 "algorithmic_flops_per_launch": flops,
-                "pairs": pairs[lv_dom], "order": p.order_s[lv_dom]}
+                "pairs": pairs[lv_dom], "order": p.order_s[lv_dom],
+                "pairs_counted": ("list-4 pairs of the boxes that hold targets"
+                                  if skip_empty else "all list-4 pairs of the dense level")}
 
     cpu = None
-    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline and args.workload == "cube":
         from oracle.oracle_api import have_reference
         if have_reference():
             rp = reference_sample()
@@ -457,7 +534,8 @@ def our_arm(args, ws, rank, local):
                    "sample": f"{rp.ns} points in a 1/8-volume sub-cube of the workload "
                              f"(depth {rp.depth}, same density, k and box widths), one solve"}
 
-    served = served_section(args, ws, rank, local) if not args.no_served else None
+    served = (served_section(args, ws, rank, local)
+              if not args.no_served and args.workload == "cube" else None)
 
     v32 = ws * p.points / (f32["ms"] * 1e-3)
     v64 = ws * p.points / (f64["ms"] * 1e-3)
@@ -466,9 +544,10 @@ def our_arm(args, ws, rank, local):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": f32["ms"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "global_batch": ws * p.points, "seq_len": 0,
+        "config": {"workload": label, "global_batch": ws * p.points, "seq_len": 0,
                    "parallelism": f"replicas{ws}", "points_per_gpu": p.points,
-                   "depth": p.depth, "orders": p.order_s[1:], "k": p.k,
+                   "sources": ns, "targets": nt, "depth": p.depth,
+                   "orders": p.order_s[1:], "k": p.k, "skip_empty": skip_empty,
                    "l2": "256 MiB buffer written between timed steps"},
         "step_ms": f32["step_ms"],
         "plain_fp64": {"value": v64, "unit": "points/s", "ms_per_step": f64["ms"], "step_ms": f64["step_ms"],
@@ -495,6 +574,10 @@ def main():
     ap.add_argument("--depth", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-served", action="store_true")
+    ap.add_argument("--workload", default="cube",
+                    choices=["cube", "laplace_c1", "sphere_c3", "clusters_c5"],
+                    help="cube (default): 1e6 Helmholtz cube + served stream; the others "
+                         "measure the benchmark's further configurations")
     args = ap.parse_args()
     ws, rank, local = dist_setup()
     try:

@@ -218,8 +218,9 @@ int wbfmm_b200_solve(const wbfmm_b200_config_t *cfg, int nsrc,
 
 /* 1 when the FP32 form keeps this configuration's tables and expansions
    inside the FP32 range (Helmholtz (S|R) coefficients at the nearest list-4
-   distance and leaf Bessel terms within 1e+-36, Laplace order <= 16);
-   0 when the solve needs the FP64 form. */
+   distance and leaf Bessel terms within 1e+-36; Laplace order <= 16 with
+   (2w)^-(p+1) and (0.87w)^p within 1e+-30 at every level of box width w,
+   for strengths of order one); 0 when the solve needs the FP64 form. */
 int wbfmm_b200_fp32_range_ok(const wbfmm_b200_config_t *cfg);
 
 /* ------------------------------------------------------------------------

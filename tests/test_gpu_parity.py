@@ -216,3 +216,56 @@ def test_m2l_kernels_agree_at_high_order(gpu_lib, case, precision):
     for mode in (2, 3):
         for a, b in zip(outs[mode], outs[0]):
             assert rel_l2(a, b) < tol, (mode, rel_l2(a, b))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", [0, 2, 3])
+def test_laplace_fp32_deep_levels(gpu_lib, mode):
+    """Laplace FP32 at depth 7, order 10, on clustered points: S|R / t^(n+l+1)
+    at the nearest list-4 distance (t = 2/128, n + l = 20) is beyond the
+    FP32 range, so each M2L kernel must apply it in scaled form.  The FP32
+    field is finite and agrees with the FP64 form and the direct sum."""
+    p = W.laplace_clusters(200_000, depth=7, order=10, seed=45)
+    cfg32 = engine.SolverConfig.from_problem(p, engine.FP32)
+    assert engine.fp32_range_ok(cfg32)
+    outs = {}
+    for prec in (engine.FP64, engine.FP32):
+        cfg = engine.SolverConfig.from_problem(p, prec)
+        with engine.Solver(cfg) as s:
+            s.set_m2l_kernel(mode)
+            s.set_sources(p.xs).set_strengths(p.q).set_targets(p.xt).run()
+            outs[prec] = s.field()
+    for a in outs[engine.FP32]:
+        assert np.all(np.isfinite(a))
+    for a, b in zip(outs[engine.FP32], outs[engine.FP64]):
+        assert rel_l2(a, b) < 1e-5, rel_l2(a, b)
+    idx = W.subsample(46, p.nt, 2000)
+    dpot, dgrad = engine.direct(p.problem, p.xs, p.q, p.xt[idx])
+    pot, grad = outs[engine.FP32]
+    assert rel_l2(pot[idx], dpot) < 1e-4
+    assert rel_l2(grad.reshape(-1, 3)[idx].ravel(), dgrad) < 1e-3
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [engine.FP64, engine.FP32])
+@pytest.mark.parametrize("mode", [0, 2, 3])
+@pytest.mark.parametrize("case", ["helmholtz_spheres", "laplace_clusters"])
+def test_skip_empty_matches_dense(gpu_lib, case, mode, precision):
+    """Sparse geometries: with skip_empty the M2L kernels walk the per-level
+    lists of boxes that hold targets instead of every box; the fields at the
+    targets are those of the dense solve."""
+    if case == "helmholtz_spheres":
+        p = W.helmholtz_sphere(40_000, 10_000, k=12.0, depth=5, seed=47, hi=12)
+    else:
+        p = W.laplace_clusters(60_000, depth=6, order=8, seed=48)
+    outs = {}
+    for skip in (False, True):
+        cfg = engine.SolverConfig.from_problem(p, precision, skip_empty=skip)
+        with engine.Solver(cfg) as s:
+            s.set_m2l_kernel(mode)
+            s.set_sources(p.xs, p.normals).set_strengths(p.q, p.dipoles).set_targets(p.xt).run()
+            outs[skip] = s.field()
+    tol = 1e-13 if precision == engine.FP64 else 1e-6
+    for a, b in zip(outs[True], outs[False]):
+        assert np.all(np.isfinite(a))
+        assert rel_l2(a, b) < tol, rel_l2(a, b)

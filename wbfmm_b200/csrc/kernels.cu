@@ -245,7 +245,7 @@ __global__ void k_m2l(XlateParams<T> p, OpTables<T> t) {
   T* A = (T*)smraw + (size_t)warp * 6 * V;
   T* B = A + 2 * V;
   T* acc = B + 2 * V;
-  T* tpow = (T*)smraw + (size_t)nw * 6 * V;   // Laplace: [15][Ns+Nr+2]
+  T* tpow = (T*)smraw + (size_t)nw * 6 * V;   // Laplace: [15][Ns+Nr+2] of (2^e t)^j
   const int tpn = Ns + Nr + 2;
   const int64_t tb = blockIdx.x / p.nsplit;
   const int split = blockIdx.x % p.nsplit;
@@ -253,7 +253,9 @@ __global__ void k_m2l(XlateParams<T> p, OpTables<T> t) {
   for (int c = lane; c < 2 * outlen; c += 32) acc[c] = T(0);
   if (!HELM) {
     for (int di = threadIdx.x; di < 15; di += blockDim.x) {
-      T r = p.width * (T)sqrt((double)c_list_dist2[di]);
+      // sources enter scaled by 2^(e l) and results leave scaled by
+      // 2^(e (n+1)), so S|R / (2^e t)^(n+l+1) stays in range
+      T r = scale2(p.width * (T)sqrt((double)c_list_dist2[di]), p.lap_e);
       T* tp = tpow + di * tpn;
       tp[0] = T(1);
       for (int j = 1; j < tpn; j++) tp[j] = r * tp[j - 1];
@@ -284,6 +286,13 @@ __global__ void k_m2l(XlateParams<T> p, OpTables<T> t) {
       const int op = (dx + 3) * 49 + (dy + 3) * 7 + dz + 3;
       const int di = t.op_dist[op];
       load_vec<T, HELM>(A, p.cin, (int64_t)s, Ns, ncs, lane);
+      if (!HELM) {
+        for (int c = lane; c < nhalf(Ns); c += 32) {
+          const int n = half_degree(c);
+          A[2 * c] = scale2(A[2 * c], p.lap_e * n);
+          A[2 * c + 1] = scale2(A[2 * c + 1], p.lap_e * n);
+        }
+      }
       __syncwarp();
       shift_vec<T, HELM, true, true>(A, B, acc, Ns, Nr, op, t,
                                      HELM ? p.coax + di * p.coax_stride : nullptr,
@@ -301,6 +310,7 @@ __global__ void k_m2l(XlateParams<T> p, OpTables<T> t) {
     for (int c = threadIdx.x; c < 2 * outlen; c += blockDim.x) {
       T v = acc0[c];
       for (int w = 1; w < nw; w++) v += acc0[(size_t)w * 6 * V + c];
+      if (!HELM) v = scale2(v, p.lap_e * (half_degree(c >> 1) + 1));
       ((T*)smraw)[c] = v;
     }
     __syncthreads();
@@ -312,6 +322,7 @@ __global__ void k_m2l(XlateParams<T> p, OpTables<T> t) {
     for (int c = threadIdx.x; c < 2 * outlen; c += blockDim.x) {
       T v = acc0[c];
       for (int w = 1; w < nw; w++) v += acc0[(size_t)w * 6 * V + c];
+      if (!HELM) v = scale2(v, p.lap_e * (half_degree(c >> 1) + 1));
       part[c] = v;
     }
   }

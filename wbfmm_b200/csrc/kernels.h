@@ -1,6 +1,8 @@
 // Launch parameters of the FMM pass kernels (kernels.cu).
 #pragma once
 
+#include <cmath>
+
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -81,7 +83,16 @@ struct XlateParams {
   int nsplit;              // M2L: CTAs per target box
   T* partial;              // M2L split: [nsplit][nbox][2*ncout]
   const uint8_t* tmask;    // M2L: only targets with tmask[b] != 0, or null
+  int lap_e;               // Laplace M2L scale exponent (lap_scale_exp)
 };
+
+// Laplace M2L scale exponent of a level of box width w: e = -ilogb(w), so
+// 2^e w is in [1, 2).  M2L kernels scale degree l of the singular
+// expansions by 2^(e l) and apply S|R(n,l,m) / (t^(n+1) (2^e t)^l): every
+// factor stays near the size of the expansions themselves, where the plain
+// S|R / t^(n+l+1) (t = |d| w, n + l up to 2p) leaves the FP32 range at
+// deep levels (t = 2/256 at level 8 gives 128^21 ~ 1.8e44 for p = 10).
+inline int lap_scale_exp(double w) { return -std::ilogb(w); }
 
 template <typename T, bool HELM>
 int launch_p2m(const P2MParams<T>& p, cudaStream_t s);

@@ -50,7 +50,7 @@ static int ensure_offsets() {
 // Layout L level array -> lin[tau][c][pp] (complex), pp on the padded
 // parent grid (nx+2)^3; the halo must be zero beforehand
 template <typename T, bool HELM>
-__global__ void k_to_lin(const T* __restrict__ arr, int level, int N,
+__global__ void k_to_lin(const T* __restrict__ arr, int level, int N, int lap_e,
                          typename V2t<T>::t* __restrict__ lin) {
   typedef typename V2t<T>::t T2;
   const int V = HELM ? (N + 1) * (N + 1) : (N + 1) * (N + 2) / 2;
@@ -79,6 +79,8 @@ __global__ void k_to_lin(const T* __restrict__ arr, int level, int N,
       int id = lidx(n, m);
       v.x = arr[layout_off(b, id, nc)]; v.y = arr[layout_off(b, id + 1, nc)];
     }
+    v.x = scale2(v.x, lap_e * n);
+    v.y = scale2(v.y, lap_e * n);
   }
   lin[((int64_t)tau * V + c) * npp + pp] = v;
 }
@@ -151,14 +153,22 @@ k_m2l_lanes(LanesParams<T> p, OpTables<T> t) {
   const int nx = 1 << (p.level - 1), npx = nx + 2;
   const int64_t npp = (int64_t)npx * npx * npx;
   const int64_t np = (int64_t)nx * nx * nx;
-  const int64_t plin = (int64_t)(blockIdx.x >> 3) * kLanesCTA + threadIdx.x;
+  int64_t plin = (int64_t)(blockIdx.x >> 3) * kLanesCTA + threadIdx.x;
   bool active = plin < np;
+  if (p.act) {
+    // sparse targets: this CTA's slots of the child type's list
+    const int na = p.act_n[tau];
+    const int64_t slot0 = (int64_t)(blockIdx.x >> 3) * kLanesCTA;
+    if (slot0 >= na) return;                  // the whole CTA, before any barrier
+    active = plin < na;
+    plin = active ? p.act[(int64_t)tau * np + plin] : 0;
+  }
   int64_t pp = 0, pmort = 0;
   if (active) {
     int px = (int)(plin % nx), py = (int)((plin / nx) % nx), pz = (int)(plin / ((int64_t)nx * nx));
     pp = (px + 1) + npx * ((int64_t)(py + 1) + npx * (int64_t)(pz + 1));
     pmort = (int64_t)morton(px, py, pz);
-    if (p.tmask && !p.tmask[(pmort << 3) | tau]) active = false;
+    if (!p.act && p.tmask && !p.tmask[(pmort << 3) | tau]) active = false;
   }
 #pragma unroll 1
   for (int c = 0; c < V; c++) { T2 z; z.x = T(0); z.y = T(0); acc[c * 32] = z; }
@@ -185,16 +195,18 @@ k_m2l_lanes(LanesParams<T> p, OpTables<T> t) {
         for (int i = threadIdx.x; i < 2 * LaneDims<P>::NC; i += kLanesCTA)
           ops[SM::off_cx + i] = cx[i];
       } else {
-        // S|R(n,nd,m) / t^{n+nd+1}, t = width * |d|
+        // S|R(n,nd,m) / (t^{n+1} (2^e t)^nd), t = width * |d|, on
+        // sources scaled by 2^(e nd)
         const T r = p.width * t.op_r[op];
-        const T rinv = T(1) / r;
+        const T rinv = T(1) / r, qinv = T(1) / scale2(r, p.lap_e);
         const int Dm = t.lt + 1;
         for (int i = threadIdx.x; i < LaneDims<P>::NL; i += kLanesCTA) {
           int m = i % (P + 1), nd = (i / (P + 1)) % (P + 1), n = i / ((P + 1) * (P + 1));
           T v = t.lapSR[((int64_t)n * Dm + nd) * Dm + m];
-          T s = rinv;
-          for (int e = 0; e < n + nd; e++) s *= rinv;
-          ops[SM::off_cx + i] = v * s;
+          T s = rinv, q = T(1);
+          for (int e = 0; e < n; e++) s *= rinv;
+          for (int e = 0; e < nd; e++) q *= qinv;
+          ops[SM::off_cx + i] = (v * q) * s;
         }
       }
     }
@@ -433,6 +445,83 @@ __global__ void k_lanes_reduce(LanesParams<T> p, int N) {
   }
 }
 
+// ------------------------------------------------------- active lists
+constexpr int kActBlock = 256;
+
+__device__ __forceinline__ bool act_flag(const uint8_t* tmask, int nx, int64_t np,
+                                         int64_t plin, int tau) {
+  if (plin >= np) return false;
+  const int px = (int)(plin % nx), py = (int)((plin / nx) % nx),
+            pz = (int)(plin / ((int64_t)nx * nx));
+  return tmask[((int64_t)morton(px, py, pz) << 3) | tau] != 0;
+}
+
+// bcnt[tau][block] = active parents of the block
+__global__ void k_act_count(const uint8_t* __restrict__ tmask, int nx, int64_t np,
+                            int nblk, int* __restrict__ bcnt) {
+  const int tau = blockIdx.y;
+  const int64_t plin = (int64_t)blockIdx.x * kActBlock + threadIdx.x;
+  const int c = __syncthreads_count(act_flag(tmask, nx, np, plin, tau));
+  if (threadIdx.x == 0) bcnt[(int64_t)tau * nblk + blockIdx.x] = c;
+}
+
+// exclusive scan of bcnt[tau][*] in place, one CTA per tau; act_n[tau] = total
+__global__ void k_act_scan(int* __restrict__ bcnt, int nblk, int* __restrict__ act_n) {
+  __shared__ int s[1024];
+  const int tau = blockIdx.x, tid = threadIdx.x;
+  int* b = bcnt + (int64_t)tau * nblk;
+  int carry = 0;
+  for (int base = 0; base < nblk; base += 1024) {
+    const int v = base + tid < nblk ? b[base + tid] : 0;
+    s[tid] = v;
+    __syncthreads();
+    for (int d = 1; d < 1024; d <<= 1) {
+      const int u = tid >= d ? s[tid - d] : 0;
+      __syncthreads();
+      s[tid] += u;
+      __syncthreads();
+    }
+    if (base + tid < nblk) b[base + tid] = carry + s[tid] - v;
+    carry += s[1023];
+    __syncthreads();
+  }
+  if (tid == 0) act_n[tau] = carry;
+}
+
+// act[tau][offset of the block + rank in the block] = plin
+__global__ void k_act_scatter(const uint8_t* __restrict__ tmask, int nx, int64_t np,
+                              int nblk, const int* __restrict__ bcnt, int* __restrict__ act) {
+  __shared__ int wsum[kActBlock / 32];
+  const int tau = blockIdx.y, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t plin = (int64_t)blockIdx.x * kActBlock + threadIdx.x;
+  const bool f = act_flag(tmask, nx, np, plin, tau);
+  const unsigned bal = __ballot_sync(0xffffffffu, f);
+  if (lane == 0) wsum[warp] = __popc(bal);
+  __syncthreads();
+  int off = bcnt[(int64_t)tau * nblk + blockIdx.x];
+  for (int w = 0; w < warp; w++) off += wsum[w];
+  off += __popc(bal & ((1u << lane) - 1u));
+  if (f) act[(int64_t)tau * np + off] = (int)plin;
+}
+
+size_t active_list_scratch(int level) {
+  const int64_t np = (int64_t)1 << (3 * (level - 1));
+  return (size_t)8 * ((np + kActBlock - 1) / kActBlock);
+}
+
+int build_active_lists(const uint8_t* tmask, int level, int* act, int* act_n,
+                       int* scratch, cudaStream_t s) {
+  const int nx = 1 << (level - 1);
+  const int64_t np = (int64_t)nx * nx * nx;
+  const int nblk = (int)((np + kActBlock - 1) / kActBlock);
+  dim3 grid((unsigned)nblk, 8);
+  k_act_count<<<grid, kActBlock, 0, s>>>(tmask, nx, np, nblk, scratch);
+  k_act_scan<<<8, 1024, 0, s>>>(scratch, nblk, act_n);
+  k_act_scatter<<<grid, kActBlock, 0, s>>>(tmask, nx, np, nblk, scratch, act);
+  WBFMM_CUDA(cudaGetLastError());
+  return 0;
+}
+
 // ------------------------------------------------------------- launchers
 template <typename T, bool HELM>
 int launch_lanes_reduce(const LanesParams<T>& p, cudaStream_t s) {
@@ -446,13 +535,14 @@ int launch_lanes_reduce(const LanesParams<T>& p, cudaStream_t s) {
 }
 
 template <typename T, bool HELM>
-int lanes_to_lin(const T* arr, int level, int N, void* lin, cudaStream_t s) {
+int lanes_to_lin(const T* arr, int level, int N, int lap_e, void* lin, cudaStream_t s) {
   typedef typename V2t<T>::t T2;
   const int V = HELM ? (N + 1) * (N + 1) : (N + 1) * (N + 2) / 2;
   const int64_t nx = 1 << (level - 1), npx = nx + 2;
   WBFMM_CUDA(cudaMemsetAsync(lin, 0, sizeof(T2) * 8 * V * npx * npx * npx, s));
   const int64_t tot = nx * nx * nx * V * 8;
-  k_to_lin<T, HELM><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(arr, level, N, (T2*)lin);
+  k_to_lin<T, HELM><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(arr, level, N, lap_e,
+                                                                   (T2*)lin);
   WBFMM_CUDA(cudaGetLastError());
   return 0;
 }
@@ -524,7 +614,7 @@ int launch_m2l_lanes(const LanesParams<T>& p, const OpTables<T>& t,
 }
 
 #define WBFMM_LANES_INST(T, H)                                                   \
-  template int lanes_to_lin<T, H>(const T*, int, int, void*, cudaStream_t);      \
+  template int lanes_to_lin<T, H>(const T*, int, int, int, void*, cudaStream_t); \
   template int launch_lanes_reduce<T, H>(const LanesParams<T>&, cudaStream_t);   \
   template bool lanes_supported<T, H>(int, int);                                 \
   template int launch_m2l_lanes<T, H>(const LanesParams<T>&, const OpTables<T>&, \

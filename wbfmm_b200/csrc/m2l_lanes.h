@@ -22,6 +22,9 @@ struct LanesParams {
   int64_t coax_stride;
   T width;              // box width of the level
   const uint8_t* tmask; // targets to compute, or null for all
+  int lap_e;            // Laplace: degree l of lin_raw is scaled by 2^(lap_e l)
+  const int* act;       // sparse targets: [8][np] parents per child type, or null
+  const int* act_n;     // [8] list lengths (device)
   void* partial_raw;    // [nsplit][8][V][np] complex when nsplit > 1
 };
 
@@ -70,8 +73,16 @@ int launch_m2l_tiles(const LanesParams<T>& p, const OpTables<T>& t,
 template <typename T, bool HELM>
 int tiles_per_cta(int N);
 template <typename T, bool HELM>
-int lanes_to_lin(const T* arr, int level, int N, void* lin, cudaStream_t s);
+int lanes_to_lin(const T* arr, int level, int N, int lap_e, void* lin, cudaStream_t s);
 size_t lanes_lin_bytes(int level, int N, bool helm, size_t tsize);
+
+// Active-target lists of a level for the lane and tile M2L: for each child
+// type tau, the parents (linear index, x fastest) whose child of type tau
+// has tmask set, ascending, in act[tau * np ...], with the lengths in
+// act_n[8].  act holds 8^level ints; scratch active_list_scratch(level) ints.
+size_t active_list_scratch(int level);
+int build_active_lists(const uint8_t* tmask, int level, int* act, int* act_n,
+                       int* scratch, cudaStream_t s);
 template <typename T, bool HELM>
 int launch_m2l_lanes(const LanesParams<T>& p, const OpTables<T>& t,
                      cudaStream_t s);

@@ -115,13 +115,13 @@ k_m2l_tiles(LanesParams<T> p, OpTables<T> t, int TC) {
   T* sH = (T*)smraw;
   T* seph = sH + q.NH;
   T* sech = seph + 2 * (P + 1);
-  T* spw = sech + 2 * (P + 1);       // Laplace: 1/t^(e+1), e <= 2P+1
+  T* spw = sech + 2 * (P + 1);       // Laplace: 1/t^(j+1), then 1/(2^e t)^j, j <= P
   T* scx = spw + 2 * (P + 1);
   int* dB = (int*)(smraw + q.ops_bytes);
   int* dC = dB + q.nB;
   int* s_nm = dC + q.nC;             // (n, m) of each vector entry
   int* s_pp = s_nm + V;              // padded-grid index of each target's parent
-  int* s_act = s_pp + TC;
+  int* s_act = s_pp + TC;            // 1 + parent linear index, 0: no target
   T2* X = (T2*)(smraw + q.ops_bytes + q.desc_bytes);
   T2* Y = X + (size_t)V * TC;
   T2* A = Y + (size_t)V * TC;
@@ -133,6 +133,9 @@ k_m2l_tiles(LanesParams<T> p, OpTables<T> t, int TC) {
   const int64_t npp = (int64_t)npx * npx * npx;
   const int64_t np = (int64_t)nx * nx * nx;
   const int64_t base = (int64_t)(blockIdx.x >> 3) * TC;
+  // sparse targets: this CTA's slots of the child type's list
+  const int64_t nlist = p.act ? (int64_t)p.act_n[tau] : np;
+  if (base >= nlist) return;                  // the whole CTA, before any barrier
 
   // stage descriptors: B/D rows (n, nu0) and C rows (m, n0), 2 rows each
   if (tid == 0) {
@@ -151,16 +154,17 @@ k_m2l_tiles(LanesParams<T> p, OpTables<T> t, int TC) {
     s_nm[c] = n | ((m + 64) << 8);
   }
   for (int i = tid; i < TC; i += kTileThreads) {
-    const int64_t plin = base + i;
-    int act = plin < np;
+    int64_t plin = base + i;
+    int act = plin < nlist;
     int pp = 0;
     if (act) {
+      if (p.act) plin = p.act[(int64_t)tau * np + plin];
       int px = (int)(plin % nx), py = (int)((plin / nx) % nx), pz = (int)(plin / ((int64_t)nx * nx));
       pp = (px + 1) + npx * ((py + 1) + npx * (pz + 1));
-      if (p.tmask && !p.tmask[((int64_t)morton(px, py, pz) << 3) | tau]) act = 0;
+      if (!p.act && p.tmask && !p.tmask[((int64_t)morton(px, py, pz) << 3) | tau]) act = 0;
     }
     s_pp[i] = pp;
-    s_act[i] = act;
+    s_act[i] = act ? (int)plin + 1 : 0;
   }
   for (int i = tid; i < V * TC; i += kTileThreads) { T2 z; z.x = T(0); z.y = T(0); A[i] = z; }
   __syncthreads();
@@ -186,17 +190,22 @@ k_m2l_tiles(LanesParams<T> p, OpTables<T> t, int TC) {
         const T* cx = p.coax + (int64_t)t.op_dist[op] * p.coax_stride;
         for (int i = tid; i < q.ncx; i += kTileThreads) scx[i] = cx[i];
       } else {
-        // S|R(n,nd,m) / t^{n+nd+1}, t = width * |d|
+        // S|R(n,nd,m) / (t^{n+1} (2^e t)^nd), t = width * |d|, on
+        // sources scaled by 2^(e nd)
         if (tid == 0) {
-          const T rinv = T(1) / (p.width * t.op_r[op]);
-          T s = rinv;
-          for (int e = 0; e < 2 * (P + 1); e++) { spw[e] = s; s *= rinv; }
+          const T r = p.width * t.op_r[op];
+          const T rinv = T(1) / r, qinv = T(1) / scale2(r, p.lap_e);
+          T s = rinv, u = T(1);
+          for (int e = 0; e <= P; e++) {
+            spw[e] = s; s *= rinv;
+            spw[P + 1 + e] = u; u *= qinv;
+          }
         }
         __syncthreads();
         const int Dm = t.lt + 1;
         for (int i = tid; i < q.ncx; i += kTileThreads) {
           int m = i % (P + 1), nd = (i / (P + 1)) % (P + 1), n = i / ((P + 1) * (P + 1));
-          scx[i] = t.lapSR[((int64_t)n * Dm + nd) * Dm + m] * spw[n + nd];
+          scx[i] = (t.lapSR[((int64_t)n * Dm + nd) * Dm + m] * spw[P + 1 + nd]) * spw[n];
         }
       }
     }
@@ -403,7 +412,7 @@ k_m2l_tiles(LanesParams<T> p, OpTables<T> t, int TC) {
   for (int i = tid; i < V * TC; i += kTileThreads) {
     const int c = i / TC, tt = i - c * TC;
     if (!s_act[tt]) continue;
-    const int64_t plin = base + tt;
+    const int64_t plin = s_act[tt] - 1;
     const T2 a = A[i];
     if (p.nsplit > 1) {
       ((T2*)p.partial_raw)[(((int64_t)split * 8 + tau) * V + c) * np + plin] = a;

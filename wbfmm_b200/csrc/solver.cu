@@ -3,6 +3,38 @@
 
 using namespace wbfmm;
 
+namespace wbfmm {
+cudaMemPool_t library_pool() {
+  static std::mutex mu;
+  static cudaMemPool_t pools[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> g(mu);
+  if (!pools[dev]) {
+    cudaMemPoolProps props;
+    memset(&props, 0, sizeof(props));
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pl = nullptr;
+    if (cudaMemPoolCreate(&pl, &props) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    uint64_t thr = UINT64_MAX;
+    int off = 0;
+    cudaMemPoolSetAttribute(pl, cudaMemPoolAttrReleaseThreshold, &thr);
+    cudaMemPoolSetAttribute(pl, cudaMemPoolReuseAllowInternalDependencies, &off);
+    pools[dev] = pl;
+  }
+  return pools[dev];
+}
+}  // namespace wbfmm
+
+
 // -------------------------------------------------------------- C ABI
 extern "C" {
 
@@ -58,12 +90,17 @@ int wbfmm_b200_fp32_range_ok(const wbfmm_b200_config_t* c) {
   if (!c) return 0;
   for (int l = 2; l <= c->depth; l++) {
     const int p = std::max(c->order_s[l], c->order_r[l]);
+    const double w = c->D / (double)(1 << l);
     if (c->problem == WBFMM_B200_LAPLACE) {
       // scale-free coaxial tables hold (n+n')! / ... up to n + n' = 2p
       if (p > 16) return 0;
+      // for strengths of order one, local coefficients of degree n scale
+      // like (2w)^-(n+1) and multipole coefficients like (0.87 w)^n: keep
+      // both within 1e+-30, leaving the rest of the range to the sums
+      if (fabs((c->order_r[l] + 1) * log10(2.0 * w)) > 30.0) return 0;
+      if (fabs(c->order_s[l] * log10(0.87 * w)) > 30.0) return 0;
       continue;
     }
-    const double w = c->D / (double)(1 << l);
     const double x = 2.0 * c->k * w;            // nearest list-4 distance
     const int N = 2 * p;
     if (x < N && log10_dfact(2 * N - 1) - (N + 1) * log10(x) > 36.0) return 0;
@@ -93,6 +130,9 @@ int64_t wbfmm_b200_footprint(const wbfmm_b200_config_t* c, int64_t ns,
   // targets, their keys and boxes, fields and their FP64 copies
   b += nt * (24 + 24 + 8 + 4 + 4 + 4 * w * ts + 4 * w * 8);
   b += ((int64_t)1 << (3 * c->depth)) * 8;
+  // skip_empty: target masks (1 byte) and M2L lists (4 bytes) of every
+  // level, sum_l 8^l < 8^depth * 8/7
+  if (c->skip_empty) b += ((int64_t)1 << (3 * c->depth)) * 6;
   // M2L working copies: the transposed, halo-padded sources and split sums
   b += 2 * mps_max;
   return b;

@@ -14,6 +14,7 @@
 
 #include <algorithm>
 #include <memory>
+#include <mutex>
 #include <vector>
 
 #include "../../include/wbfmm_b200.h"
@@ -25,10 +26,18 @@
 
 namespace wbfmm {
 
+// The library's stream-ordered memory pool of the current device (created
+// on first use; release threshold unlimited, no reuse across streams before
+// a free has completed), or null when it cannot be created.  Solvers trim it
+// to kLibPoolKeep unused bytes when they are destroyed.
+cudaMemPool_t library_pool();
+constexpr size_t kLibPoolKeep = (size_t)4 << 30;
+
 // ------------------------------------------------------------ buffers
 // Device buffer that only grows.  With a stream set, device memory comes
-// from the device's stream-ordered pool (cudaMallocAsync / cudaFreeAsync on
-// that stream): no device-wide synchronisation on reallocation or release.
+// from a stream-ordered pool (the library's, a server's, or the device's
+// default; cudaMallocFromPoolAsync / cudaFreeAsync on that stream): no
+// device-wide synchronisation on reallocation or release.
 template <typename T>
 struct DBuf {
   T* p = nullptr;
@@ -168,6 +177,7 @@ struct Solver : public wbfmm_b200_solver {
   DBuf<double> sx, sy, sz;
   DBuf<T> snx, sny, snz, sq, sdip;
   DBuf<double> stage;       // strength staging
+  DBuf<double> nstage;      // normals in tree order before conversion
   bool have_q = false, have_dip = false, have_normals = false;
   RadixScratch rs;
   DBuf<uint32_t> box_i[kMaxDepth + 1], box_n[kMaxDepth + 1];
@@ -179,6 +189,7 @@ struct Solver : public wbfmm_b200_solver {
   DBuf<uint64_t> tkeys;
   DBuf<uint32_t> tperm, tbox, tstart, tcount;
   DBuf<uint8_t> tmask[kMaxDepth + 1];
+  DBuf<int> act[kMaxDepth + 1], act_n[kMaxDepth + 1], act_scr;   // M2L target lists
   DBuf<int> flag;
   // outputs (original order)
   DBuf<T> pot, grad;
@@ -218,26 +229,31 @@ struct Solver : public wbfmm_b200_solver {
   std::vector<TableCache::Coax*> held;   // cache entries this solve reads
   bool async_checks = false;   // domain checks read back after the solve
   int* hflag = nullptr;        // pinned copy of flag[0..1]
+  cudaMemPool_t lib_pool = nullptr;
 
   template <class F>
   void each_buf(F&& f) {
     f(pts_in); f(nrm_in); f(keys); f(ip); f(sx); f(sy); f(sz);
-    f(snx); f(sny); f(snz); f(sq); f(sdip); f(stage);
+    f(snx); f(sny); f(snz); f(sq); f(sdip); f(stage); f(nstage);
     for (int l = 0; l <= kMaxDepth; l++) {
       f(box_i[l]); f(box_n[l]); f(mps[l]); f(mpr[l]); f(tmask[l]);
+      f(act[l]); f(act_n[l]);
       f(coax64[l]); f(coaxSR[l]); f(ss64[l]); f(coaxSS[l]);
     }
     f(tpts_in); f(tx); f(ty); f(tz); f(tkeys); f(tperm); f(tbox);
     f(tstart); f(tcount); f(flag); f(pot); f(grad); f(out64);
     f(H64); f(H); f(op_ith); f(op_dist); f(op_r); f(op_ph); f(op_ch);
     for (int i = 0; i < 3; i++) { f(lap64[i]); f(lap[i]); }
-    f(partial); f(lin); f(lanes_part);
+    f(partial); f(lin); f(lanes_part); f(act_scr);
   }
 
   ~Solver() override {
     release_cache_refs();
+    const bool trim = lib_pool && flag.pool == lib_pool;
     each_buf([](auto& b) { b.release(); });
     if (stream) cudaStreamSynchronize(stream);
+    // what this solver freed stays cached up to kLibPoolKeep bytes
+    if (trim) cudaMemPoolTrimTo(lib_pool, kLibPoolKeep);
     radix_scratch_free(&rs);
     if (events)
       for (int i = 0; i < 8; i++) cudaEventDestroy(ev[i]);
@@ -287,7 +303,10 @@ struct Solver : public wbfmm_b200_solver {
     }
     for (int i = 0; i < 8; i++) WBFMM_CUDA(cudaEventCreate(&ev[i]));
     events = true;
-    each_buf([&](auto& b) { b.so = stream; });
+    // plain solvers allocate from the library's pool of this device, which
+    // keeps freed memory (repeated solves reallocate without mapping)
+    lib_pool = library_pool();
+    each_buf([&](auto& b) { b.so = stream; b.pool = lib_pool; });
     WBFMM_TRY(flag.alloc(2));
     return 0;
   }
@@ -364,13 +383,13 @@ struct Solver : public wbfmm_b200_solver {
                                    cudaMemcpyHostToDevice, stream));
         dn = nrm_in.p;
       }
-      DBuf<double> tmp(stream);
-      WBFMM_TRY(tmp.alloc((size_t)3 * n));
-      launch_gather_points(dn, n_str, ip.p, n, tmp.p, tmp.p + n, tmp.p + 2 * n, stream);
+      WBFMM_TRY(nstage.alloc((size_t)3 * n));
+      double* tmp = nstage.p;
+      launch_gather_points(dn, n_str, ip.p, n, tmp, tmp + n, tmp + 2 * n, stream);
       WBFMM_TRY(snx.alloc(n)); WBFMM_TRY(sny.alloc(n)); WBFMM_TRY(snz.alloc(n));
-      WBFMM_TRY(convert_to<T>(tmp.p, snx.p, n, stream));
-      WBFMM_TRY(convert_to<T>(tmp.p + n, sny.p, n, stream));
-      WBFMM_TRY(convert_to<T>(tmp.p + 2 * n, snz.p, n, stream));
+      WBFMM_TRY(convert_to<T>(tmp, snx.p, n, stream));
+      WBFMM_TRY(convert_to<T>(tmp + n, sny.p, n, stream));
+      WBFMM_TRY(convert_to<T>(tmp + 2 * n, snz.p, n, stream));
       launches += 4;
     }
     // levels: box {i, n} by repeated refinement (src/boxes.c:208-277)
@@ -455,7 +474,12 @@ struct Solver : public wbfmm_b200_solver {
         WBFMM_TRY(tmask[l].alloc(nbl));
         k_target_mask<<<(unsigned)((nbl + 255) / 256), 256, 0, stream>>>(
             tcount.p, depth, l, tmask[l].p);
-        launches++;
+        // the M2L kernels' per-child-type lists of the boxes with targets
+        WBFMM_TRY(act[l].alloc(nbl));
+        WBFMM_TRY(act_n[l].alloc(8));
+        WBFMM_TRY(act_scr.alloc(active_list_scratch(l)));
+        WBFMM_TRY(build_active_lists(tmask[l].p, l, act[l].p, act_n[l].p, act_scr.p, stream));
+        launches += 4;
       }
     }
     if (!async_checks) {
@@ -517,6 +541,7 @@ struct Solver : public wbfmm_b200_solver {
     WBFMM_CUDA(cudaMemcpyAsync(op_dist.p, dist.data(), sizeof(int) * kNumOps, cudaMemcpyHostToDevice, stream));
     {
       DBuf<double> tmp(stream);
+      tmp.pool = flag.pool;
       size_t nph = ph.size();
       WBFMM_TRY(tmp.alloc(nph * 2 + kNumOps));
       WBFMM_CUDA(cudaMemcpyAsync(tmp.p, ph.data(), sizeof(double) * nph, cudaMemcpyHostToDevice, stream));
@@ -644,6 +669,7 @@ struct Solver : public wbfmm_b200_solver {
     x.coax_stride = sr_stride[level];
     x.width = (T)width(level);
     x.tmask = cfg.skip_empty && tmask[level].p ? tmask[level].p : nullptr;
+    x.lap_e = helm ? 0 : lap_scale_exp(width(level));
     const bool lanes_ok = helm ? lanes_supported<T, true>(x.Nin, x.Nout)
                                : lanes_supported<T, false>(x.Nin, x.Nout);
     const bool tiles_ok = helm ? tiles_supported<T, true>(x.Nin, x.Nout)
@@ -663,14 +689,15 @@ struct Solver : public wbfmm_b200_solver {
     if (use_tiles) {
       // offset-major target tiles on the transposed singular expansions
       WBFMM_TRY(lin.alloc(lanes_lin_bytes(level, x.Nin, helm, sizeof(T))));
-      WBFMM_TRY((helm ? lanes_to_lin<T, true>(x.cin, level, x.Nin, lin.p, stream)
-                      : lanes_to_lin<T, false>(x.cin, level, x.Nin, lin.p, stream)));
+      WBFMM_TRY((helm ? lanes_to_lin<T, true>(x.cin, level, x.Nin, 0, lin.p, stream)
+                      : lanes_to_lin<T, false>(x.cin, level, x.Nin, x.lap_e, lin.p, stream)));
       LanesParams<T> lp;
       memset(&lp, 0, sizeof(lp));
       lp.level = level; lp.N = x.Nin;
       lp.lin_raw = lin.p; lp.cout = x.cout;
       lp.coax = x.coax; lp.coax_stride = x.coax_stride;
-      lp.width = x.width; lp.tmask = x.tmask;
+      lp.width = x.width; lp.tmask = x.tmask; lp.lap_e = x.lap_e;
+      if (x.tmask && act[level].p) { lp.act = act[level].p; lp.act_n = act_n[level].p; }
       const int64_t np = (int64_t)1 << (3 * (level - 1));
       const int tc = helm ? tiles_per_cta<T, true>(x.Nin) : tiles_per_cta<T, false>(x.Nin);
       const int64_t ctas = ((np + tc - 1) / tc) * 8;
@@ -689,14 +716,15 @@ struct Solver : public wbfmm_b200_solver {
     if (use_lanes) {
       // lane-per-pair kernel on a transposed copy of the singular expansions
       WBFMM_TRY(lin.alloc(lanes_lin_bytes(level, x.Nin, helm, sizeof(T))));
-      WBFMM_TRY((helm ? lanes_to_lin<T, true>(x.cin, level, x.Nin, lin.p, stream)
-                      : lanes_to_lin<T, false>(x.cin, level, x.Nin, lin.p, stream)));
+      WBFMM_TRY((helm ? lanes_to_lin<T, true>(x.cin, level, x.Nin, 0, lin.p, stream)
+                      : lanes_to_lin<T, false>(x.cin, level, x.Nin, x.lap_e, lin.p, stream)));
       LanesParams<T> lp;
       memset(&lp, 0, sizeof(lp));
       lp.level = level; lp.N = x.Nin;
       lp.lin_raw = lin.p; lp.cout = x.cout;
       lp.coax = x.coax; lp.coax_stride = x.coax_stride;
-      lp.width = x.width; lp.tmask = x.tmask;
+      lp.width = x.width; lp.tmask = x.tmask; lp.lap_e = x.lap_e;
+      if (x.tmask && act[level].p) { lp.act = act[level].p; lp.act_n = act_n[level].p; }
       const int64_t np = (int64_t)1 << (3 * (level - 1));
       const int64_t base = ((np + 127) / 128) * 8;
       int ns = 1;

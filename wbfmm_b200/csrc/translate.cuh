@@ -20,6 +20,10 @@
 namespace wbfmm {
 
 HD int hidx(int n, int m) { return n * (n + 1) / 2 + m; }
+
+// x * 2^e, exact (no overflow of an intermediate power)
+HD float scale2(float x, int e) { return ldexpf(x, e); }
+HD double scale2(double x, int e) { return ldexp(x, e); }
 HD int nhalf(int p) { return (p + 1) * (p + 2) / 2; }
 
 // degree of flattened full index c = n(n+1)+m

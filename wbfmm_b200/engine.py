@@ -396,8 +396,10 @@ class Server:
         return float(self._lib.wbfmm_b200_server_clock(self._h))
 
     def submit(self, p, precision=FP32, field=POTENTIAL | GRADIENT,
-               arrival: float = 0.0) -> int:
-        cfg = SolverConfig.from_problem(p, precision, field)
+               arrival: float = 0.0, skip_empty: bool = False) -> int:
+        """Queue one solve; skip_empty: no local expansions for boxes
+        without targets (the fields at the targets are unchanged)."""
+        cfg = SolverConfig.from_problem(p, precision, field, skip_empty)
         w = 2 if p.problem == HELMHOLTZ else 1
         xs = _host(p.xs)
         xt = xs if p.targets_are_sources else _host(p.xt)
