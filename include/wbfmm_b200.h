@@ -112,6 +112,15 @@ int wbfmm_b200_l2l(wbfmm_b200_solver_t *s, int level);
 int wbfmm_b200_evaluate(wbfmm_b200_solver_t *s);
 /* all stages after set_sources/set_strengths/set_targets */
 int wbfmm_b200_run(wbfmm_b200_solver_t *s);
+/* the same stages queued on the solver's stream, returning at once;
+   wbfmm_b200_wait blocks until they are done (stage times, deferred checks) */
+int wbfmm_b200_run_async(wbfmm_b200_solver_t *s);
+int wbfmm_b200_wait(wbfmm_b200_solver_t *s);
+/* on = 1: set_sources / set_targets queue their checks that the points lie
+   inside the cube instead of waiting for them, and WBFMM_B200_E_DOMAIN is
+   returned by the next wbfmm_b200_run / wbfmm_b200_wait; a solve that
+   fails the check leaves its fields undefined.  Default 0. */
+int wbfmm_b200_set_deferred_checks(wbfmm_b200_solver_t *s, int on);
 int wbfmm_b200_synchronize(wbfmm_b200_solver_t *s);
 
 /* Results in ORIGINAL target order.  pot: Laplace [n], Helmholtz [2n];

@@ -167,6 +167,37 @@ def test_domain_error(gpu_lib):
         assert e.value.code == -2
 
 
+def test_deferred_checks(gpu_lib):
+    """With deferred checks the set calls do not wait: a source or target
+    outside the cube is reported by run / wait, and a valid solve queued with
+    run_async gives the fields of run."""
+    p = W.laplace_cube(3000, 500, depth=3, order=6, seed=3)
+    cfg = engine.SolverConfig.from_problem(p)
+    with engine.Solver(cfg) as s:
+        s.set_sources(p.xs).set_strengths(p.q).set_targets(p.xt).run()
+        ref = s.field()
+    with engine.Solver(cfg) as s:
+        s.set_deferred_checks(True)
+        s.set_sources(p.xs).set_strengths(p.q).set_targets(p.xt).run_async().wait()
+        for a, b in zip(s.field(), ref):
+            assert np.array_equal(a, b)
+        xs = p.xs.copy()
+        xs[7] = p.x0
+        s.set_sources(xs).set_strengths(p.q).set_targets(p.xt)   # no error yet
+        with pytest.raises(engine.WbfmmError) as e:
+            s.run()
+        assert e.value.code == -2
+        xt = p.xt.copy()
+        xt[3] = p.x0 + 2.0 * p.D
+        s.set_sources(p.xs).set_strengths(p.q).set_targets(xt).run_async()
+        with pytest.raises(engine.WbfmmError) as e:
+            s.wait()
+        assert e.value.code == -2
+        s.set_sources(p.xs).set_strengths(p.q).set_targets(p.xt).run()   # recovers
+        for a, b in zip(s.field(), ref):
+            assert np.array_equal(a, b)
+
+
 @pytest.mark.parametrize("name,precision", [("laplace", engine.FP64), ("helmholtz", engine.FP64),
                                             ("laplace", engine.FP32), ("helmholtz", engine.FP32)])
 def test_m2l_lane_kernel_matches_generic(gpu_lib, name, precision):

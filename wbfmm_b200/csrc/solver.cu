@@ -165,6 +165,11 @@ int wbfmm_b200_m2l(wbfmm_b200_solver_t* s, int level) { SOLVER_CALL(s->m2l(level
 int wbfmm_b200_l2l(wbfmm_b200_solver_t* s, int level) { SOLVER_CALL(s->l2l(level)); }
 int wbfmm_b200_evaluate(wbfmm_b200_solver_t* s) { SOLVER_CALL(s->evaluate()); }
 int wbfmm_b200_run(wbfmm_b200_solver_t* s) { SOLVER_CALL(s->run()); }
+int wbfmm_b200_run_async(wbfmm_b200_solver_t* s) { SOLVER_CALL(s->run_queued()); }
+int wbfmm_b200_wait(wbfmm_b200_solver_t* s) { SOLVER_CALL(s->wait()); }
+int wbfmm_b200_set_deferred_checks(wbfmm_b200_solver_t* s, int on) {
+  SOLVER_CALL(s->set_deferred_checks(on));
+}
 int wbfmm_b200_synchronize(wbfmm_b200_solver_t* s) {
   if (!s) return set_error(WBFMM_B200_E_ARG, "null solver");
   WBFMM_CUDA(cudaStreamSynchronize(s->stream));

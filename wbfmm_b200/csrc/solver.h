@@ -149,6 +149,9 @@ struct wbfmm_b200_solver {
   virtual int downward(int level) = 0;
   virtual int evaluate() = 0;
   virtual int run() = 0;
+  virtual int run_queued() = 0;
+  virtual int wait() = 0;
+  virtual int set_deferred_checks(int on) = 0;
   virtual int get_field(double*, double*, int) = 0;
   virtual int get_tree(uint32_t*, uint32_t*, uint32_t*, int) = 0;
   virtual int get_coefficients(int, double*, double*) = 0;
@@ -801,6 +804,13 @@ struct Solver : public wbfmm_b200_solver {
   }
 
   int run() override {
+    WBFMM_TRY(run_queued());
+    return wait();
+  }
+
+  // every pass queued on the stream; with deferred checks, the copy of the
+  // domain-check flags too
+  int run_queued() override {
     if (nsrc <= 0 || ntgt <= 0) return set_error(WBFMM_B200_E_STATE, "sources and targets must be set");
     WBFMM_TRY(build_operators());
     cudaEventRecord(ev[4], stream);
@@ -812,6 +822,13 @@ struct Solver : public wbfmm_b200_solver {
     cudaEventRecord(ev[7], stream);
     WBFMM_TRY(evaluate());
     cudaEventRecord(ev[2], stream);
+    if (async_checks && hflag)
+      WBFMM_CUDA(cudaMemcpyAsync(hflag, flag.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, stream));
+    return 0;
+  }
+
+  // the host waits for the queued solve: stage times, deferred checks
+  int wait() override {
     WBFMM_CUDA(cudaStreamSynchronize(stream));
     float t;
     if (cudaEventElapsedTime(&t, ev[0], ev[1]) == cudaSuccess) stage_ms[0] = t;
@@ -821,6 +838,16 @@ struct Solver : public wbfmm_b200_solver {
     if (cudaEventElapsedTime(&t, ev[6], ev[7]) == cudaSuccess) stage_ms[4] = t;
     if (cudaEventElapsedTime(&t, ev[7], ev[2]) == cudaSuccess) stage_ms[5] = t;
     cudaGetLastError();
+    return check_flags();
+  }
+
+  // set_sources / set_targets queue their domain checks; run / wait report
+  int set_deferred_checks(int on) override {
+    if (on && !hflag) {
+      WBFMM_CUDA(cudaMallocHost(&hflag, 2 * sizeof(int)));
+      hflag[0] = 0x7fffffff; hflag[1] = 0;
+    }
+    async_checks = on != 0;
     return 0;
   }
 

@@ -88,6 +88,9 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "wbfmm_b200_downward_pass": (ip, [vp, ip]),
         "wbfmm_b200_evaluate": (ip, [vp]),
         "wbfmm_b200_run": (ip, [vp]),
+        "wbfmm_b200_run_async": (ip, [vp]),
+        "wbfmm_b200_wait": (ip, [vp]),
+        "wbfmm_b200_set_deferred_checks": (ip, [vp, ip]),
         "wbfmm_b200_synchronize": (ip, [vp]),
         "wbfmm_b200_get_field": (ip, [vp, vp, vp, ip]),
         "wbfmm_b200_get_tree": (ip, [vp, u32p, u32p, u32p, ip]),
@@ -269,6 +272,21 @@ class Solver:
 
     def run(self):
         _check(self.lib.wbfmm_b200_run(self.h))
+        return self
+
+    def run_async(self):
+        """Queue every pass on the solver's stream; wait() blocks."""
+        _check(self.lib.wbfmm_b200_run_async(self.h))
+        return self
+
+    def wait(self):
+        _check(self.lib.wbfmm_b200_wait(self.h))
+        return self
+
+    def set_deferred_checks(self, on=True):
+        """Domain checks of set_sources / set_targets reported by run / wait
+        instead of by the set calls (no host wait inside a solve)."""
+        _check(self.lib.wbfmm_b200_set_deferred_checks(self.h, int(bool(on))))
         return self
 
     def synchronize(self):
