@@ -121,6 +121,12 @@ int wbfmm_b200_wait(wbfmm_b200_solver_t *s);
    returned by the next wbfmm_b200_run / wbfmm_b200_wait; a solve that
    fails the check leaves its fields undefined.  Default 0. */
 int wbfmm_b200_set_deferred_checks(wbfmm_b200_solver_t *s, int on);
+
+/* Self-test of the FP32 near-field sine and cosine: the largest absolute
+   error of the engine's own routine (err2[0]) and of CUDA's sincosf
+   (err2[1]) against FP64 sin/cos at the FP32 arguments i * xmax / n,
+   i = 0..n. */
+int wbfmm_b200_selftest_sincos(double xmax, int n, double *err2);
 int wbfmm_b200_synchronize(wbfmm_b200_solver_t *s);
 
 /* Results in ORIGINAL target order.  pot: Laplace [n], Helmholtz [2n];

@@ -300,3 +300,12 @@ def test_skip_empty_matches_dense(gpu_lib, case, mode, precision):
     for a, b in zip(outs[True], outs[False]):
         assert np.all(np.isfinite(a))
         assert rel_l2(a, b) < tol, rel_l2(a, b)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("xmax", [3.2, 100.0, 1e4])
+def test_near_field_sincos(gpu_lib, xmax):
+    """The FP32 P2P's own sine/cosine (Cody-Waite reduction, Taylor
+    polynomials) is as accurate as CUDA's sincosf at the same arguments."""
+    ours, cuda = engine.selftest_sincos(xmax, 200_000)
+    assert ours <= max(1.5 * cuda, 2.0e-7), (ours, cuda)

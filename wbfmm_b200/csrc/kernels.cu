@@ -540,28 +540,138 @@ int launch_l2p(const EvalParams<T>& p, cudaStream_t s) {
 
 // ------------------------------------------------------------------- P2P
 // One CTA per target leaf box.  The sources of the 27 neighbour boxes (a
-// virtual list, box by box) are staged through shared memory in tiles of
-// kP2PTile.  Each target is swept by a group of G threads (G a power of two,
-// as large as the box's target count leaves room for, at most 32): thread g
-// of the group takes tile entries g, g+G, ..., accumulating in FP64
-// registers in a fixed order (for the FP32 form too: pair terms in FP32, sums
-// in FP64), and the group's partial sums are
-// added by shuffles at the end.  Pair kernels and the r > 1e-6 cutoff follow
+// virtual list, box by box) are staged through shared memory in tiles of NT
+// (the CTA's thread count: 128, or 32 for trees whose leaves hold a few
+// points each, so that more boxes are resident per SM).  Each target is
+// swept by a group of G threads (G a power of two, as large as the box's
+// target count leaves room for, at most 32): thread g of the group takes
+// tile entries g, g+G, ..., accumulating in FP64 registers in a fixed order,
+// and the group's partial sums are added by shuffles at the end.  The FP32
+// form computes pair terms in FP32 from separations that keep FP64 accuracy
+// (coordinates as float pairs hi + lo, the hi parts of neighbouring points
+// subtracting exactly), sums each run of 4 of a thread's terms in FP32 and
+// adds that into the FP64 sums.  Pair kernels and the r > 1e-6 cutoff follow
 // src/local.c:32-262 and src/local-laplace.c:400-523, 1091-1227.
-constexpr int kP2PTile = 128;
+constexpr int kP2PRun = 4;     // FP32 terms summed before each FP64 add
 
-template <typename T, bool HELM>
+template <typename T, bool HELM, int NT>
 struct P2PTile {
-  double x[kP2PTile], y[kP2PTile], z[kP2PTile];
-  T q[kP2PTile * (HELM ? 2 : 1)];
-  T d[kP2PTile * (HELM ? 2 : 1)];
-  T nx[kP2PTile], ny[kP2PTile], nz[kP2PTile];
+  double x[NT], y[NT], z[NT];   // FP32 form: float hi[NT], lo[NT] in each
+  T q[NT * (HELM ? 2 : 1)];
+  T d[NT * (HELM ? 2 : 1)];
+  T nx[NT], ny[NT], nz[NT];
 };
 
-template <typename T, bool HELM>
-__global__ void __launch_bounds__(kP2PTile)
+// sin and cos of x >= 0 in FP32 for the near field: x = n pi/2 + r with
+// |r| <= pi/4 by the two-constant reduction of Cody and Waite (FMA), the
+// Taylor series of sin r to r^9 and of cos r to r^10 (truncation below 2e-9
+// at |r| = pi/4), then the quadrant's swap and signs.  A few ulp for x up to
+// about 1e4; the near field's k r stays far below that.
+__device__ __forceinline__ void sincos_near(float x, float* sp, float* cp) {
+  const float q = rintf(x * 0.636619772367581343f);            // 2/pi
+  float r = fmaf(-q, 1.57079637050628662109375f, x);          // fl(pi/2)
+  r = fmaf(-q, -4.37113900018624283e-8f, r);                  // pi/2 - fl(pi/2)
+  const float r2 = r * r;
+  float ps = fmaf(r2, 2.75573192239858907e-6f, -1.98412698412698413e-4f);
+  ps = fmaf(r2, ps, 8.33333333333333333e-3f);
+  ps = fmaf(r2, ps, -1.66666666666666667e-1f);
+  const float sn = fmaf(r * r2, ps, r);
+  float pc = fmaf(r2, -2.75573192239858907e-7f, 2.48015873015873016e-5f);
+  pc = fmaf(r2, pc, -1.38888888888888889e-3f);
+  pc = fmaf(r2, pc, 4.16666666666666667e-2f);
+  pc = fmaf(r2, pc, -0.5f);
+  const float cn = fmaf(r2, pc, 1.0f);
+  const int n = (int)q;
+  float so = (n & 1) ? cn : sn, co = (n & 1) ? sn : cn;
+  if (n & 2) so = -so;
+  if ((n + 1) & 2) co = -co;
+  *sp = so;
+  *cp = co;
+}
+
+// the terms of one (target, source) pair added to acc[0..] (Helmholtz: pot
+// re, im, then grad x re, x im, y, z; Laplace: pot, grad x, y, z)
+template <typename T, bool HELM, int NT>
+__device__ __forceinline__ void p2p_pair(const P2PTile<T, HELM, NT>& tl, int j, T rx, T ry, T rz,
+                                         T k, T kinv, bool hd, bool want_pot,
+                                         bool want_grad, T* acc) {
+  const T f4pi = T(0.25 / kPi);
+  const T r2 = rx * rx + ry * ry + rz * rz;
+  const T ir = rsqrt(r2);
+  const T r = r2 * ir;
+  if (HELM) {
+    T kr = k * r, ikr, sn, cs;
+    if constexpr (sizeof(T) == 4) {
+      ikr = ir * kinv;
+      sincos_near(kr, &sn, &cs);
+    } else {
+      ikr = ir / k;
+      sincos(kr, &sn, &cs);
+    }
+    const T h0r = sn * ikr, h0i = -cs * ikr;
+    const T h1r = h0r * ikr + h0i, h1i = h0i * ikr - h0r;
+    const T qr = tl.q[2 * j], qi = tl.q[2 * j + 1];
+    if (want_pot) {
+      T fr = (h0r * qr - h0i * qi) * f4pi, fi = (h0i * qr + h0r * qi) * f4pi;
+      if (hd) {
+        T nr = (rx * tl.nx[j] + ry * tl.ny[j] + rz * tl.nz[j]) * ir;
+        T dr = tl.d[2 * j] * nr, di = tl.d[2 * j + 1] * nr;
+        fr -= k * (h1r * dr - h1i * di) * f4pi;
+        fi -= k * (h1r * di + h1i * dr) * f4pi;
+      }
+      acc[0] += fr; acc[1] += fi;
+    }
+    if (want_grad) {
+      const T ar = -k * (h1r * qr - h1i * qi) * f4pi * ir;
+      const T ai = -k * (h1r * qi + h1i * qr) * f4pi * ir;
+      T gr[3] = {ar * rx, ar * ry, ar * rz}, gi[3] = {ai * rx, ai * ry, ai * rz};
+      if (hd) {
+        const T nxs = tl.nx[j], nys = tl.ny[j], nzs = tl.nz[j];
+        const T nr = rx * nxs + ry * nys + rz * nzs;
+        const T dpr = h0r - T(2) * h1r * ikr, dpi = h0i - T(2) * h1i * ikr;
+        const T dr = tl.d[2 * j], di = tl.d[2 * j + 1];
+        const T rv[3] = {rx, ry, rz}, nv[3] = {nxs, nys, nzs};
+        const T ir2 = ir * ir;
+        for (int c = 0; c < 3; c++) {
+          T ur = dpr * k * nr * rv[c] * ir2 + h1r * (nv[c] * ir - nr * rv[c] * ir2 * ir);
+          T ui = dpi * k * nr * rv[c] * ir2 + h1i * (nv[c] * ir - nr * rv[c] * ir2 * ir);
+          gr[c] += -k * (ur * dr - ui * di) * f4pi;
+          gi[c] += -k * (ur * di + ui * dr) * f4pi;
+        }
+      }
+      for (int c = 0; c < 3; c++) { acc[2 + 2 * c] += gr[c]; acc[3 + 2 * c] += gi[c]; }
+    }
+  } else {
+    const T q = tl.q[j];
+    const T g = f4pi * ir;
+    const T ir2 = ir * ir;
+    if (want_pot) {
+      T v = q;
+      if (hd) v += tl.d[j] * (rx * tl.nx[j] + ry * tl.ny[j] + rz * tl.nz[j]) * ir2;
+      acc[0] += v * g;
+    }
+    if (want_grad) {
+      const T gq = -q * g * ir2;
+      T gv[3] = {gq * rx, gq * ry, gq * rz};
+      if (hd) {
+        const T nxs = tl.nx[j], nys = tl.ny[j], nzs = tl.nz[j];
+        const T nr = rx * nxs + ry * nys + rz * nzs;
+        const T ad = tl.d[j] * g * ir2;
+        gv[0] += ad * (nxs - T(3) * nr * rx * ir2);
+        gv[1] += ad * (nys - T(3) * nr * ry * ir2);
+        gv[2] += ad * (nzs - T(3) * nr * rz * ir2);
+      }
+      acc[1] += gv[0]; acc[2] += gv[1]; acc[3] += gv[2];
+    }
+  }
+}
+
+template <typename T, bool HELM, int NT>
+__global__ void __launch_bounds__(NT, NT == 32 ? 20 : 1)
 k_p2p(EvalParams<T> p) {
-  __shared__ P2PTile<T, HELM> tl;
+  constexpr bool F32 = sizeof(T) == 4;
+  constexpr int NA = HELM ? 8 : 4;
+  __shared__ P2PTile<T, HELM, NT> tl;
   __shared__ uint32_t s_st[27], s_pref[28];
   const int64_t b = blockIdx.x;
   const uint32_t tc = p.tcount[b];
@@ -591,27 +701,42 @@ k_p2p(EvalParams<T> p) {
   }
   __syncthreads();
   const uint32_t total = s_pref[27];
-  const T f4pi = T(0.25 / kPi);
   const T rc2 = T(kCutoffRadius * kCutoffRadius);
   const T k = p.k;
+  const T kinv = HELM ? T(1) / k : T(0);
   const bool hq = p.q != nullptr, hd = p.dip != nullptr;
   const bool want_pot = p.pot != nullptr, want_grad = p.grad != nullptr;
+  // FP32 form: source coordinates as float pairs in the FP64 arrays' bytes
+  float* xh = (float*)tl.x; float* xl = xh + NT;
+  float* yh = (float*)tl.y; float* yl = yh + NT;
+  float* zh = (float*)tl.z; float* zl = zh + NT;
   int G = 32;
-  while (G > 1 && (uint32_t)(kP2PTile / G) < tc) G >>= 1;
-  const int gl = tid & (G - 1), ti = tid / G, tpp = kP2PTile / G;
+  while (G > 1 && (uint32_t)(NT / G) < tc) G >>= 1;
+  const int gl = tid & (G - 1), ti = tid / G, tpp = NT / G;
   for (uint32_t t0 = 0; t0 < tc; t0 += tpp) {
     const bool active = t0 + ti < tc;
     const uint32_t jt = p.tstart[b] + t0 + (active ? ti : 0);
     const double x = p.tx[jt], y = p.ty[jt], z = p.tz[jt];
+    const float txh = (float)x, tyh = (float)y, tzh = (float)z;
+    const float txl = (float)(x - (double)txh), tyl = (float)(y - (double)tyh),
+                tzl = (float)(z - (double)tzh);
     double a[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    for (uint32_t f0 = 0; f0 < total; f0 += kP2PTile) {
+    for (uint32_t f0 = 0; f0 < total; f0 += NT) {
       const uint32_t f = f0 + tid;
       __syncthreads();
       if (f < total) {
         int l = 0;
         while (l < 26 && s_pref[l + 1] <= f) l++;
         const uint32_t s = s_st[l] + (f - s_pref[l]);
-        tl.x[tid] = p.x[s]; tl.y[tid] = p.y[s]; tl.z[tid] = p.z[s];
+        const double sx = p.x[s], sy = p.y[s], sz = p.z[s];
+        if constexpr (F32) {
+          const float hx = (float)sx, hy = (float)sy, hz = (float)sz;
+          xh[tid] = hx; xl[tid] = (float)(sx - (double)hx);
+          yh[tid] = hy; yl[tid] = (float)(sy - (double)hy);
+          zh[tid] = hz; zl[tid] = (float)(sz - (double)hz);
+        } else {
+          tl.x[tid] = sx; tl.y[tid] = sy; tl.z[tid] = sz;
+        }
         if (HELM) {
           tl.q[2 * tid] = hq ? p.q[2 * s] : T(0);
           tl.q[2 * tid + 1] = hq ? p.q[2 * s + 1] : T(0);
@@ -624,80 +749,39 @@ k_p2p(EvalParams<T> p) {
       }
       __syncthreads();
       if (!active) continue;
-      const int nt = (int)min((uint32_t)kP2PTile, total - f0);
-      for (int j = gl; j < nt; j += G) {
-        // separation formed in FP64, the rest in T
-        const T rx = (T)(x - tl.x[j]), ry = (T)(y - tl.y[j]), rz = (T)(z - tl.z[j]);
-        const T r2 = rx * rx + ry * ry + rz * rz;
-        if (!(r2 > rc2)) continue;
-        const T ir = rsqrt(r2);
-        const T r = r2 * ir;
-        if (HELM) {
-          const T kr = k * r, ikr = ir / k;
-          T sn, cs;
-          sincos(kr, &sn, &cs);
-          const T h0r = sn * ikr, h0i = -cs * ikr;
-          const T h1r = h0r * ikr + h0i, h1i = h0i * ikr - h0r;
-          const T qr = tl.q[2 * j], qi = tl.q[2 * j + 1];
-          if (want_pot) {
-            T fr = (h0r * qr - h0i * qi) * f4pi, fi = (h0i * qr + h0r * qi) * f4pi;
-            if (hd) {
-              T nr = (rx * tl.nx[j] + ry * tl.ny[j] + rz * tl.nz[j]) * ir;
-              T dr = tl.d[2 * j] * nr, di = tl.d[2 * j + 1] * nr;
-              fr -= k * (h1r * dr - h1i * di) * f4pi;
-              fi -= k * (h1r * di + h1i * dr) * f4pi;
+      const int nt = (int)min((uint32_t)NT, total - f0);
+      if constexpr (F32) {
+        for (int j0 = gl; j0 < nt; j0 += kP2PRun * G) {
+          T acc[NA];
+          for (int c = 0; c < NA; c++) acc[c] = T(0);
+#pragma unroll
+          for (int u = 0; u < kP2PRun; u++) {
+            const int j = j0 + u * G;
+            if (j < nt) {
+              const T rx = (T)((txh - xh[j]) + (txl - xl[j]));
+              const T ry = (T)((tyh - yh[j]) + (tyl - yl[j]));
+              const T rz = (T)((tzh - zh[j]) + (tzl - zl[j]));
+              if (rx * rx + ry * ry + rz * rz > rc2)
+                p2p_pair<T, HELM, NT>(tl, j, rx, ry, rz, k, kinv, hd, want_pot, want_grad, acc);
             }
-            a[0] += (double)(fr); a[1] += (double)(fi);
           }
-          if (want_grad) {
-            const T ar = -k * (h1r * qr - h1i * qi) * f4pi * ir;
-            const T ai = -k * (h1r * qi + h1i * qr) * f4pi * ir;
-            T gr[3] = {ar * rx, ar * ry, ar * rz}, gi[3] = {ai * rx, ai * ry, ai * rz};
-            if (hd) {
-              const T nxs = tl.nx[j], nys = tl.ny[j], nzs = tl.nz[j];
-              const T nr = rx * nxs + ry * nys + rz * nzs;
-              const T dpr = h0r - T(2) * h1r * ikr, dpi = h0i - T(2) * h1i * ikr;
-              const T dr = tl.d[2 * j], di = tl.d[2 * j + 1];
-              const T rv[3] = {rx, ry, rz}, nv[3] = {nxs, nys, nzs};
-              const T ir2 = ir * ir;
-              for (int c = 0; c < 3; c++) {
-                T ur = dpr * k * nr * rv[c] * ir2 + h1r * (nv[c] * ir - nr * rv[c] * ir2 * ir);
-                T ui = dpi * k * nr * rv[c] * ir2 + h1i * (nv[c] * ir - nr * rv[c] * ir2 * ir);
-                gr[c] += -k * (ur * dr - ui * di) * f4pi;
-                gi[c] += -k * (ur * di + ui * dr) * f4pi;
-              }
-            }
-            for (int c = 0; c < 3; c++) { a[2 + 2 * c] += (double)(gr[c]); a[3 + 2 * c] += (double)(gi[c]); }
-          }
-        } else {
-          const T q = tl.q[j];
-          const T g = f4pi * ir;
-          const T ir2 = ir * ir;
-          if (want_pot) {
-            T v = q;
-            if (hd) v += tl.d[j] * (rx * tl.nx[j] + ry * tl.ny[j] + rz * tl.nz[j]) * ir2;
-            a[0] += (double)(v * g);
-          }
-          if (want_grad) {
-            const T gq = -q * g * ir2;
-            T gv[3] = {gq * rx, gq * ry, gq * rz};
-            if (hd) {
-              const T nxs = tl.nx[j], nys = tl.ny[j], nzs = tl.nz[j];
-              const T nr = rx * nxs + ry * nys + rz * nzs;
-              const T ad = tl.d[j] * g * ir2;
-              gv[0] += ad * (nxs - T(3) * nr * rx * ir2);
-              gv[1] += ad * (nys - T(3) * nr * ry * ir2);
-              gv[2] += ad * (nzs - T(3) * nr * rz * ir2);
-            }
-            a[1] += (double)(gv[0]); a[2] += (double)(gv[1]); a[3] += (double)(gv[2]);
-          }
+          for (int c = 0; c < NA; c++) a[c] += (double)acc[c];
+        }
+      } else {
+        for (int j = gl; j < nt; j += G) {
+          // separation formed in FP64, the rest in T
+          const T rx = (T)(x - tl.x[j]), ry = (T)(y - tl.y[j]), rz = (T)(z - tl.z[j]);
+          if (!(rx * rx + ry * ry + rz * rz > rc2)) continue;
+          T acc[NA];
+          for (int c = 0; c < NA; c++) acc[c] = T(0);
+          p2p_pair<T, HELM, NT>(tl, j, rx, ry, rz, k, kinv, hd, want_pot, want_grad, acc);
+          for (int c = 0; c < NA; c++) a[c] += (double)acc[c];
         }
       }
     }
     // sum over the group (lanes of one warp; inactive groups hold zeros)
-    const int na = HELM ? 8 : 4;
     double v[8];
-    for (int c = 0; c < na; c++) {
+    for (int c = 0; c < NA; c++) {
       v[c] = a[c];
       for (int o = 1; o < G; o <<= 1) v[c] += __shfl_xor_sync(0xffffffffu, v[c], o);
     }
@@ -723,8 +807,44 @@ k_p2p(EvalParams<T> p) {
 template <typename T, bool HELM>
 int launch_p2p(const EvalParams<T>& p, cudaStream_t s) {
   if (p.nbox <= 0 || p.ntgt <= 0) return 0;
-  k_p2p<T, HELM><<<(unsigned)p.nbox, kP2PTile, 0, s>>>(p);
+  if (p.ntgt <= 8 * p.nbox)   // a few targets per leaf on average
+    k_p2p<T, HELM, 32><<<(unsigned)p.nbox, 32, 0, s>>>(p);
+  else
+    k_p2p<T, HELM, 128><<<(unsigned)p.nbox, 128, 0, s>>>(p);
   WBFMM_CUDA(cudaGetLastError());
+  return 0;
+}
+
+// largest |sin| and |cos| errors of sincos_near and of sincosf against the
+// FP64 values at the same FP32 arguments x_i = i * xmax / n (one block;
+// err[0] ours, err[1] sincosf)
+__global__ void k_sincos_check(double xmax, int n, double* err) {
+  __shared__ double m[2][256];
+  double e0 = 0, e1 = 0;
+  for (int i = threadIdx.x; i <= n; i += blockDim.x) {
+    const float x = (float)(xmax * i / n);
+    float s, c, s1, c1;
+    sincos_near(x, &s, &c);
+    sincosf(x, &s1, &c1);
+    const double sd = sin((double)x), cd = cos((double)x);
+    e0 = fmax(e0, fmax(fabs(s - sd), fabs(c - cd)));
+    e1 = fmax(e1, fmax(fabs(s1 - sd), fabs(c1 - cd)));
+  }
+  m[0][threadIdx.x] = e0; m[1][threadIdx.x] = e1;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int t = 1; t < blockDim.x; t++) { e0 = fmax(e0, m[0][t]); e1 = fmax(e1, m[1][t]); }
+    err[0] = e0; err[1] = e1;
+  }
+}
+
+int sincos_near_errors(double xmax, int n, double* host_err) {
+  double* d = nullptr;
+  WBFMM_CUDA(cudaMalloc(&d, 2 * sizeof(double)));
+  k_sincos_check<<<1, 256>>>(xmax, n, d);
+  cudaError_t e = cudaMemcpy(host_err, d, 2 * sizeof(double), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  WBFMM_CUDA(e);
   return 0;
 }
 

@@ -106,5 +106,7 @@ template <typename T, bool HELM>
 int launch_l2p(const EvalParams<T>& p, cudaStream_t s);
 template <typename T, bool HELM>
 int launch_p2p(const EvalParams<T>& p, cudaStream_t s);
+// self-test of the FP32 near-field sine/cosine (kernels.cu)
+int sincos_near_errors(double xmax, int n, double* host_err);
 
 }  // namespace wbfmm

@@ -167,6 +167,11 @@ int wbfmm_b200_evaluate(wbfmm_b200_solver_t* s) { SOLVER_CALL(s->evaluate()); }
 int wbfmm_b200_run(wbfmm_b200_solver_t* s) { SOLVER_CALL(s->run()); }
 int wbfmm_b200_run_async(wbfmm_b200_solver_t* s) { SOLVER_CALL(s->run_queued()); }
 int wbfmm_b200_wait(wbfmm_b200_solver_t* s) { SOLVER_CALL(s->wait()); }
+int wbfmm_b200_selftest_sincos(double xmax, int n, double* err2) {
+  if (!err2 || n < 1 || !(xmax > 0)) return set_error(WBFMM_B200_E_ARG, "bad self-test arguments");
+  if (wbfmm_b200_device_count() < 1) return set_error(WBFMM_B200_E_NOGPU, "no CUDA device is available");
+  return sincos_near_errors(xmax, n, err2);
+}
 int wbfmm_b200_set_deferred_checks(wbfmm_b200_solver_t* s, int on) {
   SOLVER_CALL(s->set_deferred_checks(on));
 }

@@ -91,6 +91,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "wbfmm_b200_run_async": (ip, [vp]),
         "wbfmm_b200_wait": (ip, [vp]),
         "wbfmm_b200_set_deferred_checks": (ip, [vp, ip]),
+        "wbfmm_b200_selftest_sincos": (ip, [C.c_double, ip, dp]),
         "wbfmm_b200_synchronize": (ip, [vp]),
         "wbfmm_b200_get_field": (ip, [vp, vp, vp, ip]),
         "wbfmm_b200_get_tree": (ip, [vp, u32p, u32p, u32p, ip]),
@@ -359,6 +360,14 @@ def direct(problem, xs, q, xt, k=0.0, normals=None, dipoles=None, pot=True,
                                  _addr(normals), _addr(dipoles), xt.shape[0], _addr(xt),
                                  _addr(po), _addr(go), 0))
     return po, go
+
+
+def selftest_sincos(xmax: float, n: int):
+    """(engine's FP32 near-field sin/cos, CUDA sincosf): largest absolute
+    errors against FP64 at n+1 FP32 arguments in [0, xmax]."""
+    err = (C.c_double * 2)()
+    _check(load_library().wbfmm_b200_selftest_sincos(float(xmax), int(n), err))
+    return float(err[0]), float(err[1])
 
 
 def device_count() -> int:
