@@ -273,9 +273,10 @@ HD void l2p_helmholtz(int N, T k, const T* xc, const T* xf, Coef&& coef,
 
 // gradient of the regular expansion, G&D (2004) (3.7)
 // (src/gradient.c:193-399); g[0..5] += (dx re, dx im, dy re, dy im, dz re, dz im)
-template <typename T, class Coef>
+// pot (optional): the potential of l2p_helmholtz added in the same sweep
+template <typename T, class Coef, class Rec = RecDirect<T>>
 HD void l2p_helmholtz_grad(int N, T k, const T* xc, const T* xf, Coef&& coef,
-                           T* g) {
+                           T* g, T* pot = nullptr, const Rec& rec = Rec()) {
   T Pm1[kPtMax], Pa[kPtMax], Pb[kPtMax], Cm[kPtMax + 1], Sm[kPtMax + 1];
   T r, th, ph;
   cart2sph(xc, xf, &r, &th, &ph);
@@ -288,25 +289,26 @@ HD void l2p_helmholtz_grad(int N, T k, const T* xc, const T* xf, Coef&& coef,
   Cm[0] = T(1); Sm[0] = T(0); Cm[1] = Cph; Sm[1] = Sph;
   jnm1 = T(0);
   T acc[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
+  T pr = T(0), pi = T(0);
   auto inc = [&](int n, int m, int sgn, T cm1, T sm1, T cmm, T smm, T cp1,
                  T sp1) {
     T tm = k * jnm1, tp = k * jnp1;
     int mm1 = sgn * m - 1; mm1 = mm1 < 0 ? -mm1 : mm1;
     int mp1 = sgn * m + 1; mp1 = mp1 < 0 ? -mp1 : mp1;
     T c[6];
-    T b1 = rec_b<T>(n + 1, -sgn * m - 1) / T(2);
-    T b2 = rec_b<T>(n, sgn * m) / T(2);
+    T b1 = rec.b(n + 1, -sgn * m - 1) / T(2);
+    T b2 = rec.b(n, sgn * m) / T(2);
     T u = b1 * tp * pnp1[mp1] - b2 * tm * Pm1[mp1];
     c[0] = c[4] = cp1 * u;
     c[1] = c[5] = sp1 * u;
-    b1 = rec_b<T>(n + 1, sgn * m - 1) / T(2);
-    b2 = rec_b<T>(n, -sgn * m) / T(2);
+    b1 = rec.b(n + 1, sgn * m - 1) / T(2);
+    b2 = rec.b(n, -sgn * m) / T(2);
     u = b1 * tp * pnp1[mm1] - b2 * tm * Pm1[mm1];
     c[3] = cm1 * u;
     c[2] = -sm1 * u;
     c[0] += c[3]; c[1] -= c[2];
     c[2] += c[5]; c[3] -= c[4];
-    T a1 = rec_a<T>(n - 1, m), a2 = rec_a<T>(n, m);
+    T a1 = rec.a(n - 1, m), a2 = rec.a(n, m);
     u = a1 * tm * Pm1[m] - a2 * tp * pnp1[m];
     c[4] = cmm * u;
     c[5] = smm * u;
@@ -315,6 +317,11 @@ HD void l2p_helmholtz_grad(int N, T k, const T* xc, const T* xf, Coef&& coef,
     acc[0] += c[0] * ar - c[1] * ai; acc[1] += c[0] * ai + c[1] * ar;
     acc[2] += c[2] * ar - c[3] * ai; acc[3] += c[2] * ai + c[3] * ar;
     acc[4] += c[4] * ar - c[5] * ai; acc[5] += c[4] * ai + c[5] * ar;
+    if (pot) {   // j_n P_n^|m| e^(i sgn m ph) C_n^(sgn m)
+      const T w = jn * pn[m];
+      pr += w * (cmm * ar - smm * ai);
+      pi += w * (cmm * ai + smm * ar);
+    }
   };
   inc(0, 0, 1, Cm[1], -Sm[1], Cm[0], Sm[0], Cm[1], Sm[1]);
   jnm1 = jn;
@@ -343,6 +350,7 @@ HD void l2p_helmholtz_grad(int N, T k, const T* xc, const T* xf, Coef&& coef,
     }
   }
   for (int i = 0; i < 6; i++) g[i] += acc[i];
+  if (pot) { pot[0] += pr; pot[1] += pi; }
 }
 
 // ------------------------------------------------------- Laplace L2P
@@ -379,9 +387,11 @@ HD T l2p_laplace(int N, const T* xc, const T* xf, Coef&& coef) {
 }
 
 // gradient of the Laplace regular expansion via the derivatives of the
-// solid harmonics (src/local-laplace.c:525-630, src/wbfmm-derivatives.h)
-template <typename T, class Coef>
-HD void l2p_laplace_grad(int N, const T* xc, const T* xf, Coef&& coef, T* g) {
+// solid harmonics (src/local-laplace.c:525-630, src/wbfmm-derivatives.h);
+// pot (optional): the potential of l2p_laplace added in the same sweep
+template <typename T, class Coef, class LRec = LapRecDirect<T>>
+HD void l2p_laplace_grad(int N, const T* xc, const T* xf, Coef&& coef, T* g,
+                         T* pot = nullptr, const LRec& rec = LRec()) {
   if (N == 0) return;
   T Pa[kPtMax], Pb[kPtMax], Cm[kPtMax + 1], Sm[kPtMax + 1];
   T r, th, ph;
@@ -391,21 +401,21 @@ HD void l2p_laplace_grad(int N, const T* xc, const T* xf, Coef&& coef, T* g) {
   for (int i = 0; i < N + 3 && i < kPtMax; i++) Pa[i] = Pb[i] = T(0);
   legendre_init(C, S, &pm[0], &pn[0], &pn[1]);
   Cm[0] = T(1); Sm[0] = T(0); Cm[1] = cos(ph); Sm[1] = sin(ph);
-  T gx = T(0), gy = T(0), gz = T(0);
-  auto d_m0 = [&](int n, T rnm1, const T* P) {
-    T f = (T)(2 * n + 1) / (T)(2 * n - 1);
-    T a0 = sqrt(f * (T)n * (T)n), a1 = sqrt(f * (T)n * (T)(n - 1));
+  T gx = T(0), gy = T(0), gz = T(0), f = T(0);
+  // degree n >= 2: P holds degree n-1 (gradient), Pn degree n (potential)
+  auto d_m0 = [&](int n, T rnm1, const T* P, const T* Pn) {
+    T am, a0, a1;
+    rec.c(n, 0, &am, &a0, &a1);
     T R0 = rnm1 * P[0] * a0, R1 = rnm1 * P[1] * a1;
     T cr = coef(n * n);
     gx += cr * (-R1 * Cm[1]);
     gy += cr * (-R1 * Sm[1]);
     gz += cr * R0;
+    if (pot) f += cr * rnm1 * r * Pn[0];
   };
-  auto d_m = [&](int n, int m, T rnm1, const T* P) {
-    T f = (T)(2 * n + 1) / (T)(2 * n - 1);
-    T am = sqrt(f * (T)(n + m) * (T)(n + m - 1));
-    T a0 = sqrt(f * (T)(n - m) * (T)(n + m));
-    T ap = sqrt(f * (T)(n - m) * (T)(n - m - 1));
+  auto d_m = [&](int n, int m, T rnm1, const T* P, const T* Pn) {
+    T am, a0, ap;
+    rec.c(n, m, &am, &a0, &ap);
     T Rm = rnm1 * P[m - 1] * am, R0 = rnm1 * P[m] * a0 * T(2);
     T Rp = rnm1 * P[m + 1] * ap;
     T xr = -Rp * Cm[m + 1] + Rm * Cm[m - 1], xi = -Rp * Sm[m + 1] + Rm * Sm[m - 1];
@@ -416,26 +426,28 @@ HD void l2p_laplace_grad(int N, const T* xc, const T* xf, Coef&& coef, T* g) {
     gx += cr * xr + ci * xi;
     gy += cr * yr + ci * yi;
     gz += cr * zr + ci * zi;
+    if (pot) f += T(2) * Pn[m] * rnm1 * r * (cr * Cm[m] + ci * Sm[m]);
   };
   T rnm1 = T(1);
   Cm[2] = Cm[1] * Cm[1] - Sm[1] * Sm[1];
   Sm[2] = Sm[1] * Cm[1] + Cm[1] * Sm[1];
   {  // n = 1, m = 0: only the z derivative is non-zero
-    T f = T(3);
-    T R0 = rnm1 * pm[0] * sqrt(f);
+    T R0 = rnm1 * pm[0] * sqrt(T(3));
     gz += coef(1) * R0;
+    if (pot) f += coef(0) * pm[0] + coef(1) * r * pn[0];
   }
-  d_m(1, 1, rnm1, pm);
+  d_m(1, 1, rnm1, pm, pn);
   for (int n = 2; n <= N; n++) {
     rnm1 *= r;
     legendre_step(pm, pn, n - 1, C, S);
-    T* t = pm; pm = pn; pn = t;       // pm now degree n-1
+    T* t = pm; pm = pn; pn = t;       // pm now degree n-1, pn degree n
     Cm[n + 1] = Cm[n] * Cm[1] - Sm[n] * Sm[1];
     Sm[n + 1] = Sm[n] * Cm[1] + Cm[n] * Sm[1];
-    d_m0(n, rnm1, pm);
-    for (int m = 1; m <= n; m++) d_m(n, m, rnm1, pm);
+    d_m0(n, rnm1, pm, pn);
+    for (int m = 1; m <= n; m++) d_m(n, m, rnm1, pm, pn);
   }
   g[0] += gx; g[1] += gy; g[2] += gz;
+  if (pot) *pot += f;
 }
 
 }  // namespace wbfmm

@@ -98,6 +98,34 @@ HD T rec_b(int n, int m) {
   return m >= 0 ? v : -v;
 }
 
+// the recursion constants rec_a / rec_b as computed on the fly; L2P kernels
+// pass table-backed equivalents
+template <typename T>
+struct RecDirect {
+  HD T a(int n, int m) const { return rec_a<T>(n, m); }
+  HD T b(int n, int m) const { return rec_b<T>(n, m); }
+};
+
+// the constants of the Laplace solid-harmonic derivatives at (n, m >= 0):
+// f = (2n+1)/(2n-1); m = 0: a0 = sqrt(f n n), a1 = sqrt(f n (n-1));
+// m > 0: am = sqrt(f (n+m)(n+m-1)), a0 = sqrt(f (n-m)(n+m)),
+// ap = sqrt(f (n-m)(n-m-1))
+template <typename T>
+struct LapRecDirect {
+  HD void c(int n, int m, T* am, T* a0, T* ap) const {
+    const T f = (T)(2 * n + 1) / (T)(2 * n - 1);
+    if (m == 0) {
+      *am = T(0);
+      *a0 = sqrt(f * (T)n * (T)n);
+      *ap = sqrt(f * (T)n * (T)(n - 1));
+    } else {
+      *am = sqrt(f * (T)(n + m) * (T)(n + m - 1));
+      *a0 = sqrt(f * (T)(n - m) * (T)(n + m));
+      *ap = sqrt(f * (T)(n - m) * (T)(n - m - 1));
+    }
+  }
+};
+
 // ------------------------------------------------------------- geometry
 // r, theta, phi of x relative to x0 (src/util.c:30-49)
 template <typename T>

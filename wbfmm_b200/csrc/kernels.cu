@@ -491,8 +491,61 @@ int launch_l2l(const XlateParams<T>& p, const OpTables<T>& t, cudaStream_t s) {
 }
 
 // ------------------------------------------------------------------- L2P
+// recursion constants of the L2P gradients from shared-memory tables filled
+// once per CTA (rows n = -1..N+1, columns m + M0)
+template <typename T>
+struct RecTab {
+  const T* ta;   // rec_a(n, m): row n + 1, column m
+  const T* tb;   // rec_b(n, m): row n, column m + M0
+  int W, M0;
+  __device__ T a(int n, int m) const { return ta[(n + 1) * W + (m < 0 ? -m : m)]; }
+  __device__ T b(int n, int m) const { return tb[n * W + m + M0]; }
+};
+template <typename T>
+struct LapRecTab {
+  const T* t;    // (am, a0, ap) at ((n (N+1) + m) * 3
+  int N1;
+  __device__ void c(int n, int m, T* am, T* a0, T* ap) const {
+    const T* e = t + (n * N1 + m) * 3;
+    *am = e[0]; *a0 = e[1]; *ap = e[2];
+  }
+};
+
+// shared-memory bytes of the L2P tables at order N (0: computed on the fly)
 template <typename T, bool HELM>
-__global__ void k_l2p(EvalParams<T> p) {
+static size_t l2p_table_bytes(int N) {
+  const size_t b = HELM ? 2 * (size_t)(N + 3) * (2 * N + 3) * sizeof(T)
+                        : 3 * (size_t)(N + 1) * (N + 1) * sizeof(T);
+  return b <= 40 * 1024 ? b : 0;
+}
+
+// one thread per target (sorted by box); potential and gradient in one sweep
+template <typename T, bool HELM>
+__global__ void k_l2p(EvalParams<T> p, int tab) {
+  extern __shared__ __align__(16) unsigned char l2p_sm[];
+  T* st = (T*)l2p_sm;
+  const int N = p.N;
+  const int W = 2 * N + 3, M0 = N + 1;
+  if (tab) {
+    if (HELM) {
+      T* ta = st;
+      T* tb = st + (N + 3) * W;
+      for (int i = threadIdx.x; i < (N + 3) * W; i += blockDim.x) {
+        const int row = i / W, col = i - row * W;
+        ta[i] = rec_a<T>(row - 1, col);
+        tb[i] = rec_b<T>(row, col - M0);
+      }
+    } else {
+      const int N1 = N + 1;
+      for (int i = threadIdx.x; i < N1 * N1; i += blockDim.x) {
+        const int n = i / N1, m = i - n * N1;
+        T* e = st + 3 * i;
+        if (n >= 1 && m <= n) LapRecDirect<T>().c(n, m, &e[0], &e[1], &e[2]);
+        else e[0] = e[1] = e[2] = T(0);
+      }
+    }
+    __syncthreads();
+  }
   const int jt = blockIdx.x * blockDim.x + threadIdx.x;
   if (jt >= p.ntgt) return;
   const int64_t b = p.tbox[jt];
@@ -502,30 +555,44 @@ __global__ void k_l2p(EvalParams<T> p) {
   const T xc[3] = {T(0), T(0), T(0)};
   const T xf[3] = {(T)(p.tx[jt] - cd[0]), (T)(p.ty[jt] - cd[1]),
                    (T)(p.tz[jt] - cd[2])};
-  const int nc = ncoef(p.N);
+  const int nc = ncoef(N);
   const uint32_t o = p.tperm[jt];
   if (HELM) {
     auto coef = [&](int idx, T* re, T* im) {
       int64_t off = layout_off(b, idx, nc);
       *re = p.mpr[2 * off]; *im = p.mpr[2 * off + 1];
     };
-    if (p.pot) {
-      T fr = T(0), fi = T(0);
-      l2p_helmholtz<T>(p.N, p.k, xc, xf, coef, &fr, &fi);
-      p.pot[2 * (size_t)o] = fr; p.pot[2 * (size_t)o + 1] = fi;
-    }
     if (p.grad) {
-      T g[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
-      l2p_helmholtz_grad<T>(p.N, p.k, xc, xf, coef, g);
+      T g[6] = {T(0), T(0), T(0), T(0), T(0), T(0)}, f[2] = {T(0), T(0)};
+      T* fp = p.pot ? f : nullptr;
+      if (tab) {
+        RecTab<T> rt{st, st + (N + 3) * W, W, M0};
+        l2p_helmholtz_grad<T>(N, p.k, xc, xf, coef, g, fp, rt);
+      } else {
+        l2p_helmholtz_grad<T>(N, p.k, xc, xf, coef, g, fp);
+      }
       for (int c = 0; c < 6; c++) p.grad[6 * (size_t)o + c] = g[c];
+      if (p.pot) { p.pot[2 * (size_t)o] = f[0]; p.pot[2 * (size_t)o + 1] = f[1]; }
+    } else if (p.pot) {
+      T fr = T(0), fi = T(0);
+      l2p_helmholtz<T>(N, p.k, xc, xf, coef, &fr, &fi);
+      p.pot[2 * (size_t)o] = fr; p.pot[2 * (size_t)o + 1] = fi;
     }
   } else {
     auto coef = [&](int idx) -> T { return p.mpr[layout_off(b, idx, nc)]; };
-    if (p.pot) p.pot[o] = l2p_laplace<T>(p.N, xc, xf, coef);
     if (p.grad) {
-      T g[3] = {T(0), T(0), T(0)};
-      l2p_laplace_grad<T>(p.N, xc, xf, coef, g);
+      T g[3] = {T(0), T(0), T(0)}, f = T(0);
+      T* fp = p.pot ? &f : nullptr;
+      if (tab) {
+        LapRecTab<T> rt{st, N + 1};
+        l2p_laplace_grad<T>(N, xc, xf, coef, g, fp, rt);
+      } else {
+        l2p_laplace_grad<T>(N, xc, xf, coef, g, fp);
+      }
       for (int c = 0; c < 3; c++) p.grad[3 * (size_t)o + c] = g[c];
+      if (p.pot) p.pot[o] = f;
+    } else if (p.pot) {
+      p.pot[o] = l2p_laplace<T>(N, xc, xf, coef);
     }
   }
 }
@@ -533,7 +600,8 @@ __global__ void k_l2p(EvalParams<T> p) {
 template <typename T, bool HELM>
 int launch_l2p(const EvalParams<T>& p, cudaStream_t s) {
   if (p.ntgt <= 0) return 0;
-  k_l2p<T, HELM><<<(p.ntgt + 127) / 128, 128, 0, s>>>(p);
+  const size_t sm = l2p_table_bytes<T, HELM>(p.N);
+  k_l2p<T, HELM><<<(p.ntgt + 127) / 128, 128, sm, s>>>(p, sm ? 1 : 0);
   WBFMM_CUDA(cudaGetLastError());
   return 0;
 }
