@@ -108,13 +108,58 @@ struct LaneDims {
   static constexpr int NL = (P + 1) * (P + 1) * (P + 1);       // Laplace S|R
 };
 
+
+// whether a lane keeps its working vector in registers (about 100 of them at
+// most); otherwise it is a shared-memory column like the accumulator
+template <typename T, bool HELM, int P>
+struct LaneReg {
+  static constexpr int V = HELM ? LaneDims<P>::VF : LaneDims<P>::VH;
+#ifdef WBFMM_LANES_NO_REGISTER_VECTOR
+  static constexpr bool value = false;
+#else
+  static constexpr bool value = 2 * V * (int)(sizeof(T) / 4) <= 100;
+#endif
+};
+
+// CTAs per SM that the register-resident variant is compiled for (it caps
+// the registers per thread at 65536 / (128 * this)).  Measured on B200, FP32,
+// level-5/6 M2L (ms for caps 3 / 4 / none): Helmholtz p = 6 11.96 / 13.85 /
+// 10.51 (no cap: ILP of the unrolled body beats occupancy), p = 5 0.914 /
+// 0.986 / 0.943; Laplace p = 6 0.863 / 0.756 / 1.048, p = 8 1.694 / 1.837 /
+// 1.781.  WBFMM_LANES_REG_CTAS overrides the table.
+template <typename T, bool HELM, int P>
+struct LaneRegCtas {
+#ifdef WBFMM_LANES_REG_CTAS
+  static constexpr int value = WBFMM_LANES_REG_CTAS;
+#else
+  static constexpr int value = (sizeof(T) == 4 && HELM && P == 6) ? 1
+                             : (sizeof(T) == 4 && !HELM && P == 6) ? 4 : 3;
+#endif
+};
+
+// a lane's working vector: registers, or a shared-memory column of stride 32
+template <typename T2, int V, bool REG>
+struct WVec {
+  T2* p;
+  __device__ explicit WVec(T2* q) : p(q) {}
+  __device__ __forceinline__ T2& operator[](int i) { return p[i * 32]; }
+};
+template <typename T2, int V>
+struct WVec<T2, V, true> {
+  T2 r[V];
+  __device__ explicit WVec(T2*) {}
+  __device__ __forceinline__ T2& operator[](int i) { return r[i]; }
+};
+
 // shared memory layout, in units of T: [H: NH][eph: 2(P+1)][ech: 2(P+1)]
-// [coax: Helmholtz 2 NC | Laplace NL] then per warp two vector columns; as
-// many warps (<= 4) as fit in 200 KB
+// [coax: Helmholtz 2 NC | Laplace NL] then per warp the accumulator column
+// and, unless the working vector is in registers, its column; as many
+// warps (<= 4) as fit in 200 KB
 template <typename T, bool HELM, int P>
 struct LaneSmem {
+  static constexpr int ncols = LaneReg<T, HELM, P>::value ? 1 : 2;
   static constexpr size_t col_bytes =
-      2 * sizeof(T) * 2 * (size_t)(HELM ? LaneDims<P>::VF : LaneDims<P>::VH) * 32;
+      ncols * sizeof(T) * 2 * (size_t)(HELM ? LaneDims<P>::VF : LaneDims<P>::VH) * 32;
   static constexpr int W = col_bytes * 4 <= 200 * 1024 ? 4
                          : col_bytes * 2 <= 200 * 1024 ? 2 : 1;
   static constexpr int CTA = 32 * W;
@@ -124,12 +169,13 @@ struct LaneSmem {
   static constexpr int ops = off_cx + (HELM ? 2 * LaneDims<P>::NC : LaneDims<P>::NL);
   static constexpr int ops_pad = (ops + 3) & ~3;
   static constexpr int V = HELM ? LaneDims<P>::VF : LaneDims<P>::VH;
-  // two per-lane columns (working vector, accumulator) per warp, T2 each
+  // per-lane columns (accumulator, working vector) per warp, T2 each
   static constexpr size_t bytes = sizeof(T) * (size_t)ops_pad + col_bytes * W;
 };
 
 template <typename T, bool HELM, int P>
-__global__ void __launch_bounds__(LaneSmem<T, HELM, P>::CTA)
+__global__ void __launch_bounds__(LaneSmem<T, HELM, P>::CTA,
+                                  LaneReg<T, HELM, P>::value ? LaneRegCtas<T, HELM, P>::value : 1)
 k_m2l_lanes(LanesParams<T> p, OpTables<T> t) {
   typedef typename V2t<T>::t T2;
   typedef LaneSmem<T, HELM, P> SM;
@@ -143,8 +189,9 @@ k_m2l_lanes(LanesParams<T> p, OpTables<T> t) {
   const T* scx = ops + SM::off_cx;
   T2* cols = (T2*)(ops + SM::ops_pad);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  T2* w = cols + (size_t)warp * 2 * V * 32 + lane;   // working vector, stride 32
-  T2* acc = w + (size_t)V * 32;                      // accumulator, stride 32
+  constexpr bool REG = LaneReg<T, HELM, P>::value;
+  T2* acc = cols + (size_t)warp * SM::ncols * V * 32 + lane;   // accumulator, stride 32
+  WVec<T2, V, REG> w(acc + (size_t)V * 32);                      // working vector
 
   // the 8 child types of one parent tile are adjacent in the grid, so the
   // CTAs that read the same source neighbourhood run together (L2 reuse)
@@ -222,7 +269,7 @@ k_m2l_lanes(LanesParams<T> p, OpTables<T> t) {
         for (int m = -n; m <= n; m++) {
           const int am = m < 0 ? -m : m;
           T2 v = __ldg(src + (int64_t)cidx(n, m) * npp);
-          w[cidx(n, m) * 32] = cm(v, sech[2 * am], m < 0 ? -sech[2 * am + 1] : sech[2 * am + 1]);
+          w[cidx(n, m)] = cm(v, sech[2 * am], m < 0 ? -sech[2 * am + 1] : sech[2 * am + 1]);
         }
         cfence();
       }
@@ -231,7 +278,7 @@ k_m2l_lanes(LanesParams<T> p, OpTables<T> t) {
       for (int n = 0; n <= P; n++) {
         T2 in[2 * P + 1];
 #pragma unroll
-        for (int m = -n; m <= n; m++) in[m + n] = w[cidx(n, m) * 32];
+        for (int m = -n; m <= n; m++) in[m + n] = w[cidx(n, m)];
         const int hb = rot_idx(-n, 0, n);
 #pragma unroll
         for (int nu = -n; nu <= n; nu++) {
@@ -245,7 +292,7 @@ k_m2l_lanes(LanesParams<T> p, OpTables<T> t) {
           }
           const int an = nu < 0 ? -nu : nu;
           T2 o; o.x = sr; o.y = si;
-          w[cidx(n, nu) * 32] = cm(o, seph[2 * an], nu < 0 ? seph[2 * an + 1] : -seph[2 * an + 1]);
+          w[cidx(n, nu)] = cm(o, seph[2 * an], nu < 0 ? seph[2 * an + 1] : -seph[2 * an + 1]);
         }
         cfence();
       }
@@ -255,7 +302,7 @@ k_m2l_lanes(LanesParams<T> p, OpTables<T> t) {
         const int am = m < 0 ? -m : m;
         T2 tv[P + 1];
 #pragma unroll
-        for (int l = am; l <= P; l++) tv[l] = w[cidx(l, m) * 32];
+        for (int l = am; l <= P; l++) tv[l] = w[cidx(l, m)];
 #pragma unroll
         for (int n = am; n <= P; n++) {
           T sr = T(0), si = T(0);
@@ -268,7 +315,7 @@ k_m2l_lanes(LanesParams<T> p, OpTables<T> t) {
             si += ci * tv[l].x + cr * tv[l].y;
           }
           T2 o; o.x = sr; o.y = si;
-          w[cidx(n, m) * 32] = cm(o, seph[2 * am], m < 0 ? -seph[2 * am + 1] : seph[2 * am + 1]);
+          w[cidx(n, m)] = cm(o, seph[2 * am], m < 0 ? -seph[2 * am + 1] : seph[2 * am + 1]);
         }
         cfence();
       }
@@ -277,7 +324,7 @@ k_m2l_lanes(LanesParams<T> p, OpTables<T> t) {
       for (int n = 0; n <= P; n++) {
         T2 in[2 * P + 1];
 #pragma unroll
-        for (int m = -n; m <= n; m++) in[m + n] = w[cidx(n, m) * 32];
+        for (int m = -n; m <= n; m++) in[m + n] = w[cidx(n, m)];
         const int hb = rot_idx(-n, 0, n);
 #pragma unroll
         for (int nu = -n; nu <= n; nu++) {
@@ -305,7 +352,7 @@ k_m2l_lanes(LanesParams<T> p, OpTables<T> t) {
 #pragma unroll
         for (int m = 0; m <= n; m++) {
           T2 v = __ldg(src + (int64_t)hidx(n, m) * npp);
-          w[hidx(n, m) * 32] = cm(v, sech[2 * m], sech[2 * m + 1]);
+          w[hidx(n, m)] = cm(v, sech[2 * m], sech[2 * m + 1]);
         }
         cfence();
       }
@@ -313,7 +360,7 @@ k_m2l_lanes(LanesParams<T> p, OpTables<T> t) {
       for (int n = 0; n <= P; n++) {
         T2 in[P + 1];
 #pragma unroll
-        for (int m = 0; m <= n; m++) in[m] = w[hidx(n, m) * 32];
+        for (int m = 0; m <= n; m++) in[m] = w[hidx(n, m)];
         const int hb = rot_idx(-n, 0, n);
 #pragma unroll
         for (int nu = 0; nu <= n; nu++) {
@@ -329,7 +376,7 @@ k_m2l_lanes(LanesParams<T> p, OpTables<T> t) {
           T2 o;
           o.x = er * tr + ei * ti;
           o.y = nu == 0 ? T(0) : er * ti - ei * tr;
-          w[hidx(n, nu) * 32] = o;
+          w[hidx(n, nu)] = o;
         }
         cfence();
       }
@@ -337,7 +384,7 @@ k_m2l_lanes(LanesParams<T> p, OpTables<T> t) {
       for (int m = 0; m <= P; m++) {
         T2 tv[P + 1];
 #pragma unroll
-        for (int nd = m; nd <= P; nd++) tv[nd] = w[hidx(nd, m) * 32];
+        for (int nd = m; nd <= P; nd++) tv[nd] = w[hidx(nd, m)];
 #pragma unroll
         for (int n = m; n <= P; n++) {
           T sr = T(0), si = T(0);
@@ -349,7 +396,7 @@ k_m2l_lanes(LanesParams<T> p, OpTables<T> t) {
           }
           if (m == 0) si = T(0);
           T2 o; o.x = sr; o.y = si;
-          w[hidx(n, m) * 32] = cm(o, seph[2 * m], seph[2 * m + 1]);
+          w[hidx(n, m)] = cm(o, seph[2 * m], seph[2 * m + 1]);
         }
         cfence();
       }
@@ -357,7 +404,7 @@ k_m2l_lanes(LanesParams<T> p, OpTables<T> t) {
       for (int n = 0; n <= P; n++) {
         T2 in[P + 1];
 #pragma unroll
-        for (int m = 0; m <= n; m++) in[m] = w[hidx(n, m) * 32];
+        for (int m = 0; m <= n; m++) in[m] = w[hidx(n, m)];
         const int hb = rot_idx(-n, 0, n);
 #pragma unroll
         for (int nu = 0; nu <= n; nu++) {
