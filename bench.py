@@ -269,7 +269,7 @@ def served_section(args, ws, rank, local):
     def run_batch(srv, batch, precf, skip, keep=0):
         dist_barrier(ws)
         t0 = srv.clock()
-        tk = [srv.submit(p, precf(p), skip_empty=skip) for p in batch]
+        tk = [srv.submit(p, precf(p), skip_empty=skip, leaf_order=skip) for p in batch]
         srv.drain()
         span = max(srv.times(t)[3] for t in tk) - t0
         kept = [tuple(a.copy() for a in srv.wait(t)) for t in tk[:keep]]
@@ -280,7 +280,7 @@ def served_section(args, ws, rank, local):
     def run_latency(srv, reqs, precf, skip, rate):
         arr = W.poisson_arrivals(len(reqs), rate, seed=104 + rank)
         base = srv.clock() + 0.02
-        tk = [srv.submit(p, precf(p), arrival=base + a, skip_empty=skip)
+        tk = [srv.submit(p, precf(p), arrival=base + a, skip_empty=skip, leaf_order=skip)
               for p, a in zip(reqs, arr)]
         srv.drain()
         T = np.array([srv.times(t) for t in tk])
@@ -293,8 +293,9 @@ def served_section(args, ws, rank, local):
 
     out = {}
     kept = None
-    # the plain form computes every box's local expansion, as the reference
-    # does; the served form only those of boxes that hold targets
+    # the plain form computes every box's local expansion and sorts the
+    # points on full keys, as the reference does; the served form forms only
+    # the local expansions of boxes that hold targets and sorts by leaf box
     arms = (("plain_fp64", 1, plain_prec, False), ("served", SERVE_SLOTS, served_prec, True))
     for name, slots, precf, skip in arms:
         with engine.Server(slots=slots) as srv:
@@ -393,7 +394,10 @@ def our_arm(args, ws, rank, local):
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
 
     def make(precision):
-        cfg = engine.SolverConfig.from_problem(p, precision, field, skip_empty)
+        # the FP32 form sorts the sources by leaf box only; the plain FP64
+        # form on full keys, as the reference
+        cfg = engine.SolverConfig.from_problem(p, precision, field, skip_empty,
+                                               leaf_order=precision == engine.FP32)
         s = engine.Solver(cfg, stream=stream.cuda_stream)
         s.set_deferred_checks(True)     # no host wait inside a solve
         return s
@@ -555,6 +559,7 @@ def our_arm(args, ws, rank, local):
                    "parallelism": f"replicas{ws}", "points_per_gpu": p.points,
                    "sources": ns, "targets": nt, "depth": p.depth,
                    "orders": p.order_s[1:], "k": p.k, "skip_empty": skip_empty,
+                   "fp32_leaf_order": True,
                    "l2": "256 MiB buffer written between timed steps"},
         "step_ms": f32["step_ms"],
         "plain_fp64": {"value": v64, "unit": "points/s", "ms_per_step": f64["ms"], "step_ms": f64["step_ms"],

@@ -69,6 +69,11 @@ typedef struct {
                          expansions of target-free boxes are then left 0) */
   int managed;        /* 1: coefficient arrays in CUDA managed memory so the
                          host can read them in place */
+  int leaf_order;     /* 1: sort the sources by leaf box only (the top
+                         3*depth Morton bits, stable): points inside a leaf
+                         keep their input order instead of the reference's
+                         full-key order (t->ip differs inside leaves; boxes
+                         and fields do not); fewer radix passes */
 } wbfmm_b200_config_t;
 
 typedef struct wbfmm_b200_solver wbfmm_b200_solver_t;
@@ -116,6 +121,13 @@ int wbfmm_b200_run(wbfmm_b200_solver_t *s);
    wbfmm_b200_wait blocks until they are done (stage times, deferred checks) */
 int wbfmm_b200_run_async(wbfmm_b200_solver_t *s);
 int wbfmm_b200_wait(wbfmm_b200_solver_t *s);
+/* Repeated solves on an unchanged tree (new strengths each time, as in an
+   iterative solver): queue the passes (P2M to evaluation) as one CUDA graph
+   launch.  The first call after the sources, targets, configuration,
+   operators or options changed runs them as wbfmm_b200_run_async does and
+   captures them; later calls launch the captured graph.  Returns at once;
+   wbfmm_b200_wait blocks. */
+int wbfmm_b200_run_graph(wbfmm_b200_solver_t *s);
 /* on = 1: set_sources / set_targets queue their checks that the points lie
    inside the cube instead of waiting for them, and WBFMM_B200_E_DOMAIN is
    returned by the next wbfmm_b200_run / wbfmm_b200_wait; a solve that

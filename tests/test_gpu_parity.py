@@ -309,3 +309,70 @@ def test_near_field_sincos(gpu_lib, xmax):
     polynomials) is as accurate as CUDA's sincosf at the same arguments."""
     ours, cuda = engine.selftest_sincos(xmax, 200_000)
     assert ours <= max(1.5 * cuda, 2.0e-7), (ours, cuda)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [engine.FP64, engine.FP32])
+@pytest.mark.parametrize("case", ["laplace", "helmholtz"])
+def test_graph_replay(gpu_lib, case, precision):
+    """Repeated solves on one tree with new strengths: the captured graph of
+    the passes gives exactly the fields of a direct run, and a change of the
+    targets makes the next call capture again."""
+    if case == "laplace":
+        p = W.laplace_cube(20000, 3000, depth=4, order=8, seed=51)
+    else:
+        p = W.helmholtz_cube(20000, k=6.0, depth=4, seed=52)
+        p.xt = p.xt[:3000]
+        p.targets_are_sources = False
+    rng = np.random.default_rng(53)
+    qs = [rng.standard_normal(p.q.shape) for _ in range(3)]
+    cfg = engine.SolverConfig.from_problem(p, precision)
+    refs = []
+    with engine.Solver(cfg) as s:
+        s.set_sources(p.xs).set_targets(p.xt)
+        for q in qs:
+            s.set_strengths(q).run()
+            refs.append(s.field())
+    with engine.Solver(cfg) as s:
+        s.set_deferred_checks(True)
+        s.set_sources(p.xs).set_targets(p.xt)
+        s.set_strengths(qs[0]).run_graph().wait()          # runs and captures
+        for q, ref in zip(qs, refs):
+            n1 = s.kernel_launches()
+            s.set_strengths(q).run_graph().wait()          # graph launches
+            per_graph = s.kernel_launches() - n1
+            for a, b in zip(s.field(), ref):
+                assert np.array_equal(a, b)
+        n2 = s.kernel_launches()
+        s.set_strengths(qs[0]).run_async().wait()          # the same passes, launched directly
+        assert per_graph == s.kernel_launches() - n2
+        xt2 = p.xt[::2].copy()
+        s.set_targets(xt2).set_strengths(qs[1]).run_graph().wait()   # captures again
+        with engine.Solver(cfg) as s2:
+            s2.set_sources(p.xs).set_strengths(qs[1]).set_targets(xt2).run()
+            for a, b in zip(s.field(), s2.field()):
+                assert np.array_equal(a, b)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [engine.FP64, engine.FP32])
+def test_leaf_order(gpu_lib, precision):
+    """Sorting the sources by leaf box only gives the same boxes, the same
+    points in every leaf (in input order there) and, up to the order of
+    summation, the same fields."""
+    p = W.helmholtz_cube(30000, k=6.0, depth=4, seed=54)
+    outs, trees = [], []
+    for lo in (False, True):
+        cfg = engine.SolverConfig.from_problem(p, precision, leaf_order=lo)
+        with engine.Solver(cfg) as s:
+            s.set_sources(p.xs).set_strengths(p.q).set_targets(p.xt).run()
+            outs.append(s.field())
+            trees.append(s.tree(p.depth))
+    (ip0, bi0, bn0), (ip1, bi1, bn1) = trees
+    assert np.array_equal(bi0, bi1) and np.array_equal(bn0, bn1)
+    for b in np.nonzero(bn0)[0][:2000]:
+        a, c = ip0[bi0[b]:bi0[b] + bn0[b]], ip1[bi1[b]:bi1[b] + bn1[b]]
+        assert np.array_equal(np.sort(a), c)          # input order inside the leaf
+    tol = 1e-12 if precision == engine.FP64 else 2e-6
+    for a, b in zip(outs[0], outs[1]):
+        assert rel_l2(a, b) < tol

@@ -50,10 +50,10 @@ struct RadixScratch {
   uint32_t* hist = nullptr;
   size_t cap = 0, hist_cap = 0;
 };
-// stable LSD radix sort of (keys, vals) on the low `bits` bits; result in
-// keys/vals (ping-pong through scratch)
+// stable LSD radix sort of (keys, vals) on key bits [lo, lo + bits);
+// result in keys/vals (ping-pong through scratch)
 int radix_sort_pairs(uint64_t* keys, uint32_t* vals, int n, int bits,
-                     RadixScratch* scr, cudaStream_t s);
+                     RadixScratch* scr, cudaStream_t s, int lo = 0);
 void radix_scratch_free(RadixScratch* scr);
 
 // box {i, n} of one level from the sorted keys, reproducing

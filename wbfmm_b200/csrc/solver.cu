@@ -166,6 +166,7 @@ int wbfmm_b200_l2l(wbfmm_b200_solver_t* s, int level) { SOLVER_CALL(s->l2l(level
 int wbfmm_b200_evaluate(wbfmm_b200_solver_t* s) { SOLVER_CALL(s->evaluate()); }
 int wbfmm_b200_run(wbfmm_b200_solver_t* s) { SOLVER_CALL(s->run()); }
 int wbfmm_b200_run_async(wbfmm_b200_solver_t* s) { SOLVER_CALL(s->run_queued()); }
+int wbfmm_b200_run_graph(wbfmm_b200_solver_t* s) { SOLVER_CALL(s->run_graph()); }
 int wbfmm_b200_wait(wbfmm_b200_solver_t* s) { SOLVER_CALL(s->wait()); }
 int wbfmm_b200_selftest_sincos(double xmax, int n, double* err2) {
   if (!err2 || n < 1 || !(xmax > 0)) return set_error(WBFMM_B200_E_ARG, "bad self-test arguments");

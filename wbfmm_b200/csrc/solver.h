@@ -150,6 +150,7 @@ struct wbfmm_b200_solver {
   virtual int evaluate() = 0;
   virtual int run() = 0;
   virtual int run_queued() = 0;
+  virtual int run_graph() = 0;
   virtual int wait() = 0;
   virtual int set_deferred_checks(int on) = 0;
   virtual int get_field(double*, double*, int) = 0;
@@ -233,6 +234,18 @@ struct Solver : public wbfmm_b200_solver {
   bool async_checks = false;   // domain checks read back after the solve
   int* hflag = nullptr;        // pinned copy of flag[0..1]
   cudaMemPool_t lib_pool = nullptr;
+  // graph replay of the passes (run_graph): valid while nothing they depend
+  // on has changed since the capture
+  uint64_t gen = 0;                 // bumped by every change of tree, targets, tables, options
+  struct GraphSig {
+    uint64_t gen; const void* q; const void* dip; bool hq, hd;
+    bool operator==(const GraphSig& o) const {
+      return gen == o.gen && q == o.q && dip == o.dip && hq == o.hq && hd == o.hd;
+    }
+  } gsig{};
+  cudaGraphExec_t gexec = nullptr;
+  int64_t glaunches = 0;            // kernels in the captured graph
+  bool capturing = false;
 
   template <class F>
   void each_buf(F&& f) {
@@ -251,6 +264,7 @@ struct Solver : public wbfmm_b200_solver {
   }
 
   ~Solver() override {
+    if (gexec) cudaGraphExecDestroy(gexec);
     release_cache_refs();
     const bool trim = lib_pool && flag.pool == lib_pool;
     each_buf([](auto& b) { b.release(); });
@@ -277,6 +291,7 @@ struct Solver : public wbfmm_b200_solver {
 
   // validate and take a configuration (buffers already held are kept)
   int configure(const wbfmm_b200_config_t* c) {
+    gen++;
     cfg = *c;
     helm = cfg.problem == WBFMM_B200_HELMHOLTZ;
     if (cfg.problem != WBFMM_B200_HELMHOLTZ && cfg.problem != WBFMM_B200_LAPLACE)
@@ -350,6 +365,7 @@ struct Solver : public wbfmm_b200_solver {
       return set_error(WBFMM_B200_E_ARG, "bad source points");
     if (normals && n_str < 3) return set_error(WBFMM_B200_E_ARG, "bad normal stride");
     cudaEventRecord(ev[0], stream);
+    gen++;
     nsrc = n;
     xstr = xs_str;
     const double* dpts = xs;
@@ -371,8 +387,11 @@ struct Solver : public wbfmm_b200_solver {
     WBFMM_TRY(keys.alloc(n));
     WBFMM_TRY(ip.alloc(n));
     launch_point_keys(dpts, xs_str, n, cfg.x0, cfg.D, keys.p, ip.p, stream);
-    WBFMM_TRY(radix_sort_pairs(keys.p, ip.p, n, 60, &rs, stream));
-    launches += 4 + 3 * 8;
+    // full 60-bit keys (the reference's point order), or with leaf_order
+    // only the bits that select the leaf box
+    const int sort_lo = cfg.leaf_order ? 60 - 3 * depth : 0;
+    WBFMM_TRY(radix_sort_pairs(keys.p, ip.p, n, 60 - sort_lo, &rs, stream, sort_lo));
+    launches += 4 + 3 * ((60 - sort_lo + 7) / 8);
     WBFMM_TRY(sx.alloc(n)); WBFMM_TRY(sy.alloc(n)); WBFMM_TRY(sz.alloc(n));
     launch_gather_points(dpts, xs_str, ip.p, n, sx.p, sy.p, sz.p, stream);
     launches++;
@@ -448,6 +467,7 @@ struct Solver : public wbfmm_b200_solver {
   }
 
   int set_targets(int n, const double* xt, int tstr, int on_device) override {
+    gen++;
     if (n <= 0 || xt == nullptr || tstr < 3)
       return set_error(WBFMM_B200_E_ARG, "bad target points");
     ntgt = n;
@@ -813,17 +833,64 @@ struct Solver : public wbfmm_b200_solver {
   int run_queued() override {
     if (nsrc <= 0 || ntgt <= 0) return set_error(WBFMM_B200_E_STATE, "sources and targets must be set");
     WBFMM_TRY(build_operators());
-    cudaEventRecord(ev[4], stream);
+    return passes();
+  }
+
+  // P2M, upward, downward, evaluation (and the flags' copy with deferred
+  // checks); stage events unless the stream is being captured
+  int passes() {
+    auto mark = [&](int i) { if (!capturing) cudaEventRecord(ev[i], stream); };
+    mark(4);
     WBFMM_TRY(leaf_expansions());
-    cudaEventRecord(ev[5], stream);
+    mark(5);
     for (int l = depth; l >= 3; l--) WBFMM_TRY(upward(l));
-    cudaEventRecord(ev[6], stream);
+    mark(6);
     for (int l = 2; l <= depth; l++) WBFMM_TRY(downward(l));
-    cudaEventRecord(ev[7], stream);
+    mark(7);
     WBFMM_TRY(evaluate());
-    cudaEventRecord(ev[2], stream);
+    mark(2);
     if (async_checks && hflag)
       WBFMM_CUDA(cudaMemcpyAsync(hflag, flag.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, stream));
+    return 0;
+  }
+
+  // The passes as one CUDA graph launch.  The first call after anything
+  // they depend on changed (sources, targets, tables, options, the strength
+  // buffers) runs them as usual, which sizes every work buffer, then
+  // captures the same launches; later calls launch the graph.  Stage times
+  // stay those of the last call that ran the passes directly.
+  int run_graph() override {
+    if (nsrc <= 0 || ntgt <= 0) return set_error(WBFMM_B200_E_STATE, "sources and targets must be set");
+    const GraphSig sig{gen, (const void*)sq.p, (const void*)sdip.p, have_q, have_dip};
+    if (gexec && ops_ready && sig == gsig) {
+      WBFMM_CUDA(cudaGraphLaunch(gexec, stream));
+      launches += glaunches;
+      return 0;
+    }
+    WBFMM_TRY(run_queued());
+    if (gexec) { cudaGraphExecDestroy(gexec); gexec = nullptr; }
+    const int64_t l0 = launches;
+    cudaGraph_t g = nullptr;
+    WBFMM_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    capturing = true;
+    const int rc = passes();
+    capturing = false;
+    const cudaError_t e = cudaStreamEndCapture(stream, &g);
+    glaunches = launches - l0;
+    launches = l0;                      // captured, not launched
+    if (rc || e != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      cudaGetLastError();
+      return rc ? rc : set_cuda_error(e, __FILE__, __LINE__);
+    }
+    const cudaError_t ei = cudaGraphInstantiate(&gexec, g, 0);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess) {
+      gexec = nullptr;
+      cudaGetLastError();
+      return set_cuda_error(ei, __FILE__, __LINE__);
+    }
+    gsig = sig;
     return 0;
   }
 
@@ -939,15 +1006,17 @@ struct Solver : public wbfmm_b200_solver {
     return 0;
   }
 
-  void invalidate_operators() override { ops_ready = false; }
-  void set_m2l_kernel(int mode) override { m2l_mode = mode; }
-  void set_p2m_accumulate(int on) override { p2m_accumulate = on != 0; }
+  void invalidate_operators() override { ops_ready = false; gen++; }
+  void set_m2l_kernel(int mode) override { m2l_mode = mode; gen++; }
+  void set_p2m_accumulate(int on) override { p2m_accumulate = on != 0; gen++; }
   void set_evaluation(int field, int neighbours) override {
+    gen++;
     eval_field = field;
     eval_neighbours = neighbours != 0;
   }
   int adopt_coefficients(int level, void* ms, void* mr) override {
     if (level < 1 || level > depth) return set_error(WBFMM_B200_E_ARG, "bad level");
+    gen++;
     if (ms) mps[level].adopt((T*)ms, level_len(level, cfg.order_s[level]), cfg.managed != 0);
     if (mr) mpr[level].adopt((T*)mr, level_len(level, cfg.order_r[level]), cfg.managed != 0);
     return 0;

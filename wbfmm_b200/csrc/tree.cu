@@ -210,7 +210,7 @@ __global__ void k_radix_scatter(const uint64_t* __restrict__ keys,
 }
 
 int radix_sort_pairs(uint64_t* keys, uint32_t* vals, int n, int bits,
-                     RadixScratch* scr, cudaStream_t s) {
+                     RadixScratch* scr, cudaStream_t s, int lo) {
   if (n <= 1) return 0;
   int ntiles = (n + kSortTile - 1) / kSortTile;
   if (scr->cap < (size_t)n) {
@@ -230,7 +230,7 @@ int radix_sort_pairs(uint64_t* keys, uint32_t* vals, int n, int bits,
   uint64_t *ki = keys, *ko = scr->keys_alt;
   uint32_t *vi = vals, *vo = scr->vals_alt;
   for (int p = 0; p < passes; p++) {
-    int shift = 8 * p;
+    int shift = lo + 8 * p;
     k_radix_hist<<<ntiles, kSortThreads, 0, s>>>(ki, n, shift, ntiles, scr->hist);
     k_scan_exclusive<<<1, 1024, 0, s>>>(scr->hist, 256 * ntiles);
     k_radix_scatter<<<ntiles, kSortThreads, 0, s>>>(ki, vi, n, shift, ntiles,

@@ -45,7 +45,7 @@ class Config(C.Structure):
         ("order_r", C.c_int * (MAX_DEPTH + 1)),
         ("k", C.c_double), ("x0", C.c_double * 3), ("D", C.c_double),
         ("precision", C.c_int), ("field", C.c_int), ("skip_empty", C.c_int),
-        ("managed", C.c_int),
+        ("managed", C.c_int), ("leaf_order", C.c_int),
     ]
 
 
@@ -89,6 +89,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "wbfmm_b200_evaluate": (ip, [vp]),
         "wbfmm_b200_run": (ip, [vp]),
         "wbfmm_b200_run_async": (ip, [vp]),
+        "wbfmm_b200_run_graph": (ip, [vp]),
         "wbfmm_b200_wait": (ip, [vp]),
         "wbfmm_b200_set_deferred_checks": (ip, [vp, ip]),
         "wbfmm_b200_selftest_sincos": (ip, [C.c_double, ip, dp]),
@@ -161,6 +162,7 @@ class SolverConfig:
     field: int = POTENTIAL | GRADIENT
     skip_empty: bool = False
     managed: bool = False
+    leaf_order: bool = False
 
     def to_c(self) -> Config:
         c = Config()
@@ -177,13 +179,15 @@ class SolverConfig:
         c.field = self.field
         c.skip_empty = int(bool(self.skip_empty))
         c.managed = int(bool(self.managed))
+        c.leaf_order = int(bool(self.leaf_order))
         return c
 
     @staticmethod
     def from_problem(p, precision=FP64, field=POTENTIAL | GRADIENT,
-                     skip_empty=False) -> "SolverConfig":
+                     skip_empty=False, leaf_order=False) -> "SolverConfig":
         return SolverConfig(p.problem, p.depth, list(p.order_s), list(p.order_r),
-                            p.k, tuple(p.x0), p.D, precision, field, skip_empty)
+                            p.k, tuple(p.x0), p.D, precision, field, skip_empty,
+                            False, leaf_order)
 
 
 class Solver:
@@ -278,6 +282,12 @@ class Solver:
     def run_async(self):
         """Queue every pass on the solver's stream; wait() blocks."""
         _check(self.lib.wbfmm_b200_run_async(self.h))
+        return self
+
+    def run_graph(self):
+        """The passes as one CUDA graph launch (captured on the first call
+        after a change of tree, targets, tables or options); wait() blocks."""
+        _check(self.lib.wbfmm_b200_run_graph(self.h))
         return self
 
     def wait(self):
@@ -423,10 +433,12 @@ class Server:
         return float(self._lib.wbfmm_b200_server_clock(self._h))
 
     def submit(self, p, precision=FP32, field=POTENTIAL | GRADIENT,
-               arrival: float = 0.0, skip_empty: bool = False) -> int:
+               arrival: float = 0.0, skip_empty: bool = False,
+               leaf_order: bool = False) -> int:
         """Queue one solve; skip_empty: no local expansions for boxes
-        without targets (the fields at the targets are unchanged)."""
-        cfg = SolverConfig.from_problem(p, precision, field, skip_empty)
+        without targets (the fields at the targets are unchanged);
+        leaf_order: sources sorted by leaf box only."""
+        cfg = SolverConfig.from_problem(p, precision, field, skip_empty, leaf_order)
         w = 2 if p.problem == HELMHOLTZ else 1
         xs = _host(p.xs)
         xt = xs if p.targets_are_sources else _host(p.xt)

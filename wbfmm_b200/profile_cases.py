@@ -18,8 +18,8 @@ steady-state launch.  Cases:
                             evaluation (L2P + P2P)
   served_stream             48 requests of the serving stream through a
                             1-slot server, FP32 where the range rule admits
-                            the request, skip_empty (launch lists of a
-                            served mix)
+                            the request, skip_empty and leaf_order (launch
+                            lists of a served mix)
 """
 from __future__ import annotations
 
@@ -68,7 +68,8 @@ def main(case: str) -> None:
         reqs = list(W.serving_stream(48, seed=4))
         with E.Server(slots=1) as srv:
             tickets = [srv.submit(p, E.FP32 if E.fp32_range_ok(E.SolverConfig.from_problem(p))
-                                  else E.FP64, skip_empty=True) for p in reqs]
+                                  else E.FP64, skip_empty=True, leaf_order=True)
+                       for p in reqs]
             srv.drain()
             for t in tickets:
                 srv.wait(t)
