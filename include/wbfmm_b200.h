@@ -213,6 +213,12 @@ int wbfmm_b200_direct(int problem, double k, int ns, const double *xs,
                       const double *dipoles, int nt, const double *xt,
                       double *pot, double *grad, int on_device);
 
+/* Accuracy of a field against a reference, reduced on the GPU in FP64 with
+   a fixed order: out4 = {||f - ref||_2, ||ref||_2, max |f - ref|,
+   max |ref|} over n values (host or device arrays). */
+int wbfmm_b200_error_norms(int64_t n, const double *f, const double *ref,
+                           int on_device, double *out4);
+
 /* Largest point count wbfmm_b200_morton_sort_noalloc accepts. */
 #define WBFMM_B200_NOALLOC_MAX_POINTS (1 << 20)
 

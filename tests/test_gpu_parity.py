@@ -376,3 +376,15 @@ def test_leaf_order(gpu_lib, precision):
     tol = 1e-12 if precision == engine.FP64 else 2e-6
     for a, b in zip(outs[0], outs[1]):
         assert rel_l2(a, b) < tol
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [1, 1000, 3_000_001])
+def test_error_norms(gpu_lib, n):
+    """The GPU accuracy reduction agrees with numpy (relative L2 and max)."""
+    rng = np.random.default_rng(55)
+    ref = rng.standard_normal(n)
+    f = ref + 1e-7 * rng.standard_normal(n)
+    l2, mx = engine.error_norms(f, ref)
+    assert abs(l2 - np.linalg.norm(f - ref) / np.linalg.norm(ref)) <= 1e-12 * l2
+    assert mx == np.max(np.abs(f - ref)) / np.max(np.abs(ref))

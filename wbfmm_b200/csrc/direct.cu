@@ -6,6 +6,8 @@
 // FMM forms are measured against.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "../../include/wbfmm_b200.h"
 #include "engine.h"
 
@@ -186,6 +188,97 @@ extern "C" int wbfmm_b200_direct(int problem, double k, int ns,
     cudaFree(dxs); cudaFree(dq); cudaFree(dn); cudaFree(dd); cudaFree(dxt);
     cudaFree(dp); cudaFree(dg);
   }
+  cudaStreamDestroy(s);
+  return rc;
+}
+
+// ------------------------------------------------------------ error norms
+// The accuracy reduction of a field f against a reference r (FP64): per
+// block sums of (f - r)^2 and r^2 and maxima of |f - r| and |r| in a fixed
+// order, then one block combines the partials in block order, so the
+// result does not depend on scheduling.
+namespace {
+constexpr int kErrThreads = 256;
+constexpr int kErrBlocks = 592;   // 4 per SM
+
+__device__ void err_block_reduce(double v[4], double (*sm)[kErrThreads]) {
+  const int t = threadIdx.x;
+  for (int k = 0; k < 4; k++) sm[k][t] = v[k];
+  __syncthreads();
+  for (int s = kErrThreads / 2; s > 0; s >>= 1) {
+    if (t < s) {
+      sm[0][t] += sm[0][t + s];
+      sm[1][t] += sm[1][t + s];
+      sm[2][t] = fmax(sm[2][t], sm[2][t + s]);
+      sm[3][t] = fmax(sm[3][t], sm[3][t + s]);
+    }
+    __syncthreads();
+  }
+  for (int k = 0; k < 4; k++) v[k] = sm[k][0];
+}
+
+__global__ void k_err_partial(const double* __restrict__ f, const double* __restrict__ r,
+                              int64_t n, double* __restrict__ part) {
+  __shared__ double sm[4][kErrThreads];
+  double v[4] = {0, 0, 0, 0};
+  for (int64_t i = (int64_t)blockIdx.x * kErrThreads + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * kErrThreads) {
+    const double d = f[i] - r[i];
+    v[0] = fma(d, d, v[0]);
+    v[1] = fma(r[i], r[i], v[1]);
+    v[2] = fmax(v[2], fabs(d));
+    v[3] = fmax(v[3], fabs(r[i]));
+  }
+  err_block_reduce(v, sm);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 4; k++) part[4 * blockIdx.x + k] = v[k];
+}
+
+__global__ void k_err_final(const double* __restrict__ part, int nb, double* __restrict__ out) {
+  __shared__ double sm[4][kErrThreads];
+  double v[4] = {0, 0, 0, 0};
+  for (int b = threadIdx.x; b < nb; b += kErrThreads) {
+    v[0] += part[4 * b];
+    v[1] += part[4 * b + 1];
+    v[2] = fmax(v[2], part[4 * b + 2]);
+    v[3] = fmax(v[3], part[4 * b + 3]);
+  }
+  err_block_reduce(v, sm);
+  if (threadIdx.x == 0) {
+    out[0] = sqrt(v[0]); out[1] = sqrt(v[1]); out[2] = v[2]; out[3] = v[3];
+  }
+}
+}  // namespace
+
+extern "C" int wbfmm_b200_error_norms(int64_t n, const double* f, const double* ref,
+                                      int on_device, double* out4) {
+  if (n < 0 || (n > 0 && (!f || !ref)) || !out4)
+    return wbfmm::set_error(WBFMM_B200_E_ARG, "bad error-norm arguments");
+  if (wbfmm_b200_device_count() < 1)
+    return wbfmm::set_error(WBFMM_B200_E_NOGPU, "no CUDA device is available");
+  cudaStream_t s;
+  WBFMM_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  const double *df = f, *dr = ref;
+  double *buf = nullptr, *part = nullptr;
+  const int nb = (int)std::min<int64_t>(kErrBlocks, std::max<int64_t>(1, (n + kErrThreads - 1) / kErrThreads));
+  int rc = 0;
+  cudaError_t e = cudaMallocAsync(&part, sizeof(double) * (4 * nb + 4), s);
+  if (e == cudaSuccess && !on_device && n > 0) {
+    e = cudaMallocAsync(&buf, sizeof(double) * 2 * n, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(buf, f, sizeof(double) * n, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(buf + n, ref, sizeof(double) * n, cudaMemcpyHostToDevice, s);
+    df = buf; dr = buf + n;
+  }
+  if (e == cudaSuccess) {
+    k_err_partial<<<nb, kErrThreads, 0, s>>>(df, dr, n, part);
+    k_err_final<<<1, kErrThreads, 0, s>>>(part, nb, part + 4 * nb);
+    e = cudaMemcpyAsync(out4, part + 4 * nb, 4 * sizeof(double), cudaMemcpyDeviceToHost, s);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) rc = wbfmm::set_cuda_error(e, __FILE__, __LINE__);
+  if (buf) cudaFreeAsync(buf, s);
+  if (part) cudaFreeAsync(part, s);
+  cudaStreamSynchronize(s);
   cudaStreamDestroy(s);
   return rc;
 }

@@ -93,6 +93,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "wbfmm_b200_wait": (ip, [vp]),
         "wbfmm_b200_set_deferred_checks": (ip, [vp, ip]),
         "wbfmm_b200_selftest_sincos": (ip, [C.c_double, ip, dp]),
+        "wbfmm_b200_error_norms": (ip, [C.c_int64, vp, vp, ip, dp]),
         "wbfmm_b200_synchronize": (ip, [vp]),
         "wbfmm_b200_get_field": (ip, [vp, vp, vp, ip]),
         "wbfmm_b200_get_tree": (ip, [vp, u32p, u32p, u32p, ip]),
@@ -370,6 +371,17 @@ def direct(problem, xs, q, xt, k=0.0, normals=None, dipoles=None, pot=True,
                                  _addr(normals), _addr(dipoles), xt.shape[0], _addr(xt),
                                  _addr(po), _addr(go), 0))
     return po, go
+
+
+def error_norms(f, ref):
+    """GPU FP64 reduction: (||f - ref||_2 / ||ref||_2, max|f - ref| / max|ref|)
+    for host arrays of equal size."""
+    f = _host(f).ravel(); ref = _host(ref).ravel()
+    if f.shape != ref.shape:
+        raise ValueError("f and ref differ in size")
+    out = (C.c_double * 4)()
+    _check(load_library().wbfmm_b200_error_norms(f.size, _addr(f), _addr(ref), 0, out))
+    return out[0] / out[1], out[2] / out[3]
 
 
 def selftest_sincos(xmax: float, n: int):
