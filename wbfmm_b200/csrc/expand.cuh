@@ -18,9 +18,9 @@ constexpr int kPtMax = 66;   // per-point scratch: degree <= 64
 // --------------------------------------------------- Helmholtz monopole
 // C_n^m += q j_n(kr) P_n^{|m|}(cos th) e^{-i m ph}
 // (src/expansions.c:30-123; an order-1 expansion keeps only n = 0 there)
-template <typename T, class Emit>
+template <typename T, class Emit, class Leg = LegDirect<T>>
 HD void p2m_helmholtz(int N, T k, const T* xc, const T* xs, T qr, T qi,
-                      Emit&& emit) {
+                      Emit&& emit, const Leg& leg = Leg()) {
   if (N == 0) return;
   T Pa[kPtMax], Pb[kPtMax], Cm[kPtMax], Sm[kPtMax];
   T r, th, ph;
@@ -43,7 +43,7 @@ HD void p2m_helmholtz(int N, T k, const T* xc, const T* xs, T qr, T qi,
   term(1, 1, 1, j, pn);
   term(1, 1, -1, j, pn);
   for (int n = 2; n <= N; n++) {
-    legendre_step(pm, pn, n - 1, C, S);
+    legendre_step(pm, pn, n - 1, C, S, leg);
     T* t = pm; pm = pn; pn = t;
     bessel_j_step(&jm, &j, kr, n - 1);
     Cm[n] = Cm[n - 1] * Cm[1] - Sm[n - 1] * Sm[1];
@@ -60,9 +60,10 @@ HD void p2m_helmholtz(int N, T k, const T* xc, const T* xs, T qr, T qi,
 // Dipole of complex strength d along the unit normal nrm, through the
 // derivative relations G&D (3.2)-(3.7); regular terms of degree n >= N are
 // not propagated, as in the reference (src/expansions.c:346-631).
-template <typename T, class Emit>
+template <typename T, class Emit, class Leg = LegDirect<T>>
 HD void p2m_helmholtz_dipole(int N, T k, const T* xc, const T* xs,
-                             const T* nrm, T dr, T di, Emit&& emit) {
+                             const T* nrm, T dr, T di, Emit&& emit,
+                             const Leg& leg = Leg()) {
   T Pa[kPtMax], Pb[kPtMax], Cm[kPtMax], Sm[kPtMax];
   T fm[2], fp[2], fz[2];
   fm[0] = T(0.5) * k * (dr * nrm[0] + di * nrm[1]);
@@ -103,7 +104,7 @@ HD void p2m_helmholtz_dipole(int N, T k, const T* xc, const T* xs,
   inc(1, 1, 1, j, pn);
   inc(1, 1, -1, j, pn);
   for (int n = 2; n <= N; n++) {
-    legendre_step(pm, pn, n - 1, C, S);
+    legendre_step(pm, pn, n - 1, C, S, leg);
     T* t = pm; pm = pn; pn = t;
     bessel_j_step(&jm, &j, kr, n - 1);
     Cm[n] = Cm[n - 1] * Cm[1] - Sm[n - 1] * Sm[1];
@@ -119,8 +120,9 @@ HD void p2m_helmholtz_dipole(int N, T k, const T* xc, const T* xs,
 // ----------------------------------------------------- Laplace monopole
 // M_n^m += q r^n P_n^m(cos th) e^{-i m ph} / (2n+1), real-packed
 // (src/laplace.c:35-129); emit(index, value) per real slot
-template <typename T, class Emit>
-HD void p2m_laplace(int N, const T* xc, const T* xs, T q, Emit&& emit) {
+template <typename T, class Emit, class Leg = LegDirect<T>>
+HD void p2m_laplace(int N, const T* xc, const T* xs, T q, Emit&& emit,
+                    const Leg& leg = Leg()) {
   if (N == 0) return;
   T Pa[kPtMax], Pb[kPtMax], Cm[kPtMax], Sm[kPtMax];
   T r, th, ph;
@@ -138,7 +140,7 @@ HD void p2m_laplace(int N, const T* xc, const T* xs, T q, Emit&& emit) {
   emit(lidx(1, 1) + 1, -(q * rn * pn[1] * Sm[1] / T(3)));
   for (int n = 2; n <= N; n++) {
     rn *= r;
-    legendre_step(pm, pn, n - 1, C, S);
+    legendre_step(pm, pn, n - 1, C, S, leg);
     T* t = pm; pm = pn; pn = t;
     Cm[n] = Cm[n - 1] * Cm[1] - Sm[n - 1] * Sm[1];
     Sm[n] = Sm[n - 1] * Cm[1] + Cm[n - 1] * Sm[1];
@@ -154,9 +156,9 @@ HD void p2m_laplace(int N, const T* xc, const T* xs, T q, Emit&& emit) {
 
 // ------------------------------------------------------- Laplace dipole
 // Dipole of strength d along the unit normal (src/laplace.c:181-423)
-template <typename T, class Emit>
+template <typename T, class Emit, class Leg = LegDirect<T>>
 HD void p2m_laplace_dipole(int N, const T* xc, const T* xs, const T* nrm,
-                           T d, Emit&& emit) {
+                           T d, Emit&& emit, const Leg& leg = Leg()) {
   if (N == 0) return;
   T Pa[kPtMax], Pb[kPtMax], Cm[kPtMax], Sm[kPtMax];
   T fx = nrm[0] * d, fy = nrm[1] * d, fz = nrm[2] * d;
@@ -215,7 +217,7 @@ HD void p2m_laplace_dipole(int N, const T* xc, const T* xs, const T* nrm,
   if (N == 2) return;
   for (int n = 2; n < N; n++) {
     rn *= r;
-    legendre_step(pm, pn, n - 1, C, S);
+    legendre_step(pm, pn, n - 1, C, S, leg);
     T* t = pm; pm = pn; pn = t;
     Cm[n + 1] = Cm[n] * Cm[1] - Sm[n] * Sm[1];
     Sm[n + 1] = Sm[n] * Cm[1] + Cm[n] * Sm[1];
@@ -228,9 +230,9 @@ HD void p2m_laplace_dipole(int N, const T* xc, const T* xs, const T* nrm,
 // ---------------------------------------------------- Helmholtz L2P
 // f += sum C_n^m j_n(kr) P_n^{|m|} e^{i m ph}   (src/expansions.c:230-344)
 // coef(idx) returns coefficient idx as (re, im)
-template <typename T, class Coef>
+template <typename T, class Coef, class Leg = LegDirect<T>>
 HD void l2p_helmholtz(int N, T k, const T* xc, const T* xf, Coef&& coef,
-                      T* fr, T* fi) {
+                      T* fr, T* fi, const Leg& leg = Leg()) {
   T Pa[kPtMax], Pb[kPtMax], Cm[kPtMax], Sm[kPtMax];
   T r, th, ph;
   cart2sph(xc, xf, &r, &th, &ph);
@@ -260,7 +262,7 @@ HD void l2p_helmholtz(int N, T k, const T* xc, const T* xf, Coef&& coef,
   inc0(1, j, pn);
   inc(1, 1, j, pn);
   for (int n = 2; n <= N; n++) {
-    legendre_step(pm, pn, n - 1, C, S);
+    legendre_step(pm, pn, n - 1, C, S, leg);
     T* t = pm; pm = pn; pn = t;
     bessel_j_step(&jm, &j, kr, n - 1);
     Cm[n] = Cm[n - 1] * Cm[1] - Sm[n - 1] * Sm[1];
@@ -274,9 +276,10 @@ HD void l2p_helmholtz(int N, T k, const T* xc, const T* xf, Coef&& coef,
 // gradient of the regular expansion, G&D (2004) (3.7)
 // (src/gradient.c:193-399); g[0..5] += (dx re, dx im, dy re, dy im, dz re, dz im)
 // pot (optional): the potential of l2p_helmholtz added in the same sweep
-template <typename T, class Coef, class Rec = RecDirect<T>>
+template <typename T, class Coef, class Rec = RecDirect<T>, class Leg = LegDirect<T>>
 HD void l2p_helmholtz_grad(int N, T k, const T* xc, const T* xf, Coef&& coef,
-                           T* g, T* pot = nullptr, const Rec& rec = Rec()) {
+                           T* g, T* pot = nullptr, const Rec& rec = Rec(),
+                           const Leg& leg = Leg()) {
   T Pm1[kPtMax], Pa[kPtMax], Pb[kPtMax], Cm[kPtMax + 1], Sm[kPtMax + 1];
   T r, th, ph;
   cart2sph(xc, xf, &r, &th, &ph);
@@ -328,7 +331,7 @@ HD void l2p_helmholtz_grad(int N, T k, const T* xc, const T* xf, Coef&& coef,
   bessel_j_step(&jn, &jnp1, kr, 1);
   // n = 1
   Pm1[0] = pn[0]; Pm1[1] = pn[1];
-  legendre_step(pn, pnp1, 1, C, S);
+  legendre_step(pn, pnp1, 1, C, S, leg);
   { T* t = pn; pn = pnp1; pnp1 = t; }
   Cm[2] = Cm[1] * Cph - Sm[1] * Sph;
   Sm[2] = Sm[1] * Cph + Cm[1] * Sph;
@@ -337,7 +340,7 @@ HD void l2p_helmholtz_grad(int N, T k, const T* xc, const T* xf, Coef&& coef,
   inc(1, 1, -1, Cm[2], -Sm[2], Cm[1], -Sm[1], Cm[0], -Sm[0]);
   for (int n = 2; n <= N; n++) {
     for (int i = 0; i <= n; i++) Pm1[i] = pn[i];
-    legendre_step(pn, pnp1, n, C, S);
+    legendre_step(pn, pnp1, n, C, S, leg);
     { T* t = pn; pn = pnp1; pnp1 = t; }
     jnm1 = jn;
     bessel_j_step(&jn, &jnp1, kr, n);
@@ -356,8 +359,9 @@ HD void l2p_helmholtz_grad(int N, T k, const T* xc, const T* xf, Coef&& coef,
 // ------------------------------------------------------- Laplace L2P
 // f += L_n^0 r^n P_n^0 + 2 sum_{m>0} r^n P_n^m Re(L_n^m e^{i m ph})
 // (src/local-laplace.c:333-398); coef(idx) returns real slot idx
-template <typename T, class Coef>
-HD T l2p_laplace(int N, const T* xc, const T* xf, Coef&& coef) {
+template <typename T, class Coef, class Leg = LegDirect<T>>
+HD T l2p_laplace(int N, const T* xc, const T* xf, Coef&& coef,
+                 const Leg& leg = Leg()) {
   T Pa[kPtMax], Pb[kPtMax], Cm[kPtMax], Sm[kPtMax];
   T r, th, ph;
   cart2sph(xc, xf, &r, &th, &ph);
@@ -373,7 +377,7 @@ HD T l2p_laplace(int N, const T* xc, const T* xf, Coef&& coef) {
   f += T(2) * pn[1] * rn * (coef(lidx(1, 1)) * Cm[1] - coef(lidx(1, 1) + 1) * Sm[1]);
   for (int n = 2; n <= N; n++) {
     rn *= r;
-    legendre_step(pm, pn, n - 1, C, S);
+    legendre_step(pm, pn, n - 1, C, S, leg);
     T* t = pm; pm = pn; pn = t;
     Cm[n] = Cm[n - 1] * Cm[1] - Sm[n - 1] * Sm[1];
     Sm[n] = Sm[n - 1] * Cm[1] + Cm[n - 1] * Sm[1];
@@ -389,9 +393,10 @@ HD T l2p_laplace(int N, const T* xc, const T* xf, Coef&& coef) {
 // gradient of the Laplace regular expansion via the derivatives of the
 // solid harmonics (src/local-laplace.c:525-630, src/wbfmm-derivatives.h);
 // pot (optional): the potential of l2p_laplace added in the same sweep
-template <typename T, class Coef, class LRec = LapRecDirect<T>>
+template <typename T, class Coef, class LRec = LapRecDirect<T>, class Leg = LegDirect<T>>
 HD void l2p_laplace_grad(int N, const T* xc, const T* xf, Coef&& coef, T* g,
-                         T* pot = nullptr, const LRec& rec = LRec()) {
+                         T* pot = nullptr, const LRec& rec = LRec(),
+                         const Leg& leg = Leg()) {
   if (N == 0) return;
   T Pa[kPtMax], Pb[kPtMax], Cm[kPtMax + 1], Sm[kPtMax + 1];
   T r, th, ph;
@@ -439,7 +444,7 @@ HD void l2p_laplace_grad(int N, const T* xc, const T* xf, Coef&& coef, T* g,
   d_m(1, 1, rnm1, pm, pn);
   for (int n = 2; n <= N; n++) {
     rnm1 *= r;
-    legendre_step(pm, pn, n - 1, C, S);
+    legendre_step(pm, pn, n - 1, C, S, leg);
     T* t = pm; pm = pn; pn = t;       // pm now degree n-1, pn degree n
     Cm[n + 1] = Cm[n] * Cm[1] - Sm[n] * Sm[1];
     Sm[n + 1] = Sm[n] * Cm[1] + Cm[n] * Sm[1];

@@ -147,17 +147,53 @@ HD void legendre_init(T C, T S, T* P0, T* P10, T* P11) {
   *P10 = C * (T)sqrt(3.0) / s4pi;
   *P11 = S * (T)sqrt(1.5) / s4pi;
 }
+// The constants of one step of the normalised Legendre recursion from
+// degree n: d(n) = sqrt((2n+3)/(2n+2)) (new diagonal), c(n) = sqrt(2n+1),
+// a(n, m) = sqrt((n^2 - m^2)/(2n-1)), b(n, m) = 1/sqrt(((n+1)^2 - m^2)/(2n+3)).
+// LegDirect computes them; kernels pass shared-memory tables (LegTab).
+template <typename T>
+struct LegDirect {
+  HD T d(int n) const { return sqrt((T)(2 * n + 3) / (T)(2 * n + 2)); }
+  HD T c(int n) const { return sqrt((T)(2 * n + 1)); }
+  HD T a(int n, int m) const { return sqrt((T)(n * n - m * m) / (T)(2 * n - 1)); }
+  HD T b(int n, int m) const {
+    return T(1) / sqrt((T)((n + 1) * (n + 1) - m * m) / (T)(2 * n + 3));
+  }
+};
+// the same from tables of degrees n <= nmax (rows of nmax + 1 orders)
+template <typename T>
+struct LegTab {
+  const T* t;    // [4][nmax + 1][nmax + 1]: a, b, then c and d in row 0 of planes 2, 3
+  int W;         // nmax + 1
+  HD T d(int n) const { return t[3 * W * W + n]; }
+  HD T c(int n) const { return t[2 * W * W + n]; }
+  HD T a(int n, int m) const { return t[n * W + m]; }
+  HD T b(int n, int m) const { return t[W * W + n * W + m]; }
+};
+// fill a LegTab's storage (4 (nmax+1)^2 values) with threads tid, tid+nt, ...
+template <typename T>
+HD void leg_table_fill(T* t, int nmax, int tid, int nt) {
+  const int W = nmax + 1;
+  const LegDirect<T> L;
+  for (int i = tid; i < W * W; i += nt) {
+    const int n = i / W, m = i - n * W;
+    t[i] = m <= n && n >= 1 ? L.a(n, m) : T(0);
+    t[W * W + i] = m <= n ? L.b(n, m) : T(0);
+    if (i < W) { t[2 * W * W + i] = L.c(i); t[3 * W * W + i] = L.d(i); }
+  }
+}
+
 // Advance: pnm1 holds degree n-1 on entry, pn degree n; on exit pnm1 holds
 // degree n+1 (caller swaps roles).  Entry n+1 of pn is zeroed, as in the
 // reference (src/util.c:58-86).
-template <typename T>
-HD void legendre_step(T* pnm1, T* pn, int n, T C, T S) {
-  pnm1[n + 1] = sqrt((T)(2 * n + 3) / (T)(2 * n + 2)) * S * pn[n];
+template <typename T, class Leg = LegDirect<T>>
+HD void legendre_step(T* pnm1, T* pn, int n, T C, T S, const Leg& L = Leg()) {
+  pnm1[n + 1] = L.d(n) * S * pn[n];
   pn[n + 1] = T(0);
-  T sq = sqrt((T)(2 * n + 1));
+  const T sq = L.c(n);
   for (int m = 0; m <= n; m++) {
-    T v = C * sq * pn[m] - sqrt((T)(n * n - m * m) / (T)(2 * n - 1)) * pnm1[m];
-    pnm1[m] = v / sqrt((T)((n + 1) * (n + 1) - m * m) / (T)(2 * n + 3));
+    const T v = C * sq * pn[m] - L.a(n, m) * pnm1[m];
+    pnm1[m] = v * L.b(n, m);
   }
 }
 

@@ -43,16 +43,31 @@ __device__ __forceinline__ void box_centre(int64_t b, double x0, double y0,
 }
 
 // ------------------------------------------------------------------- P2M
+// shared-memory bytes of the Legendre constants of degrees <= N + 2
+// (LegTab), or 0 where they would take more than 40 KB (then computed)
+template <typename T>
+static size_t leg_table_bytes(int N) {
+  const size_t b = 4 * sizeof(T) * (size_t)(N + 3) * (N + 3);
+  return b <= 40 * 1024 ? b : 0;
+}
+
 template <typename T, bool HELM>
-__global__ void k_p2m(P2MParams<T> p) {
-  extern __shared__ unsigned char smraw[];
+__global__ void k_p2m(P2MParams<T> p, int legt) {
+  extern __shared__ __align__(16) unsigned char smraw[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int nw = blockDim.x >> 5;
+  // Legendre recursion constants of degrees <= N + 2, once per CTA
+  const int LW = p.N + 3;
+  T* lt = (T*)smraw;
+  if (legt) {
+    leg_table_fill(lt, p.N + 2, threadIdx.x, blockDim.x);
+    __syncthreads();
+  }
   const int64_t b = (int64_t)blockIdx.x * nw + warp;
   if (b >= p.nbox) return;   // whole warp leaves; no block barriers below
   const int nc = ncoef(p.N);
   const int w = HELM ? 2 : 1;
-  T* acc = (T*)smraw + (size_t)warp * nc * w;
+  T* acc = (T*)smraw + (legt ? 4 * LW * LW : 0) + (size_t)warp * nc * w;
   for (int c = lane; c < nc * w; c += 32) acc[c] = T(0);
   __syncwarp();
   const uint32_t cnt = p.box_n[b], start = p.box_i[b];
@@ -68,37 +83,41 @@ __global__ void k_p2m(P2MParams<T> p) {
       T xs[3] = {act ? (T)(p.x[s] - cd[0]) : T(0),
                  act ? (T)(p.y[s] - cd[1]) : T(0),
                  act ? (T)(p.z[s] - cd[2]) : T(0)};
-      if (HELM) {
-        auto emit = [&](int idx, T re, T im) {
-          re = warp_sum(re); im = warp_sum(im);
-          if (lane == 0) { acc[2 * idx] += re; acc[2 * idx + 1] += im; }
-        };
-        if (p.q) {
-          T qr = act ? p.q[2 * s] : T(0), qi = act ? p.q[2 * s + 1] : T(0);
-          p2m_helmholtz<T>(p.N, p.k, xc, xs, qr, qi, emit);
+      auto expand = [&](const auto& leg) {
+        if (HELM) {
+          auto emit = [&](int idx, T re, T im) {
+            re = warp_sum(re); im = warp_sum(im);
+            if (lane == 0) { acc[2 * idx] += re; acc[2 * idx + 1] += im; }
+          };
+          if (p.q) {
+            T qr = act ? p.q[2 * s] : T(0), qi = act ? p.q[2 * s + 1] : T(0);
+            p2m_helmholtz<T>(p.N, p.k, xc, xs, qr, qi, emit, leg);
+          }
+          if (p.dip) {
+            T dr = act ? p.dip[2 * s] : T(0), di = act ? p.dip[2 * s + 1] : T(0);
+            T nrm[3] = {act ? p.nx[s] : T(0), act ? p.ny[s] : T(0),
+                        act ? p.nz[s] : T(1)};
+            p2m_helmholtz_dipole<T>(p.N, p.k, xc, xs, nrm, dr, di, emit, leg);
+          }
+        } else {
+          auto emit = [&](int idx, T v) {
+            v = warp_sum(v);
+            if (lane == 0) acc[idx] += v;
+          };
+          if (p.q) {
+            T qv = act ? p.q[s] : T(0);
+            p2m_laplace<T>(p.N, xc, xs, qv, emit, leg);
+          }
+          if (p.dip) {
+            T dv = act ? p.dip[s] : T(0);
+            T nrm[3] = {act ? p.nx[s] : T(0), act ? p.ny[s] : T(0),
+                        act ? p.nz[s] : T(1)};
+            p2m_laplace_dipole<T>(p.N, xc, xs, nrm, dv, emit, leg);
+          }
         }
-        if (p.dip) {
-          T dr = act ? p.dip[2 * s] : T(0), di = act ? p.dip[2 * s + 1] : T(0);
-          T nrm[3] = {act ? p.nx[s] : T(0), act ? p.ny[s] : T(0),
-                      act ? p.nz[s] : T(1)};
-          p2m_helmholtz_dipole<T>(p.N, p.k, xc, xs, nrm, dr, di, emit);
-        }
-      } else {
-        auto emit = [&](int idx, T v) {
-          v = warp_sum(v);
-          if (lane == 0) acc[idx] += v;
-        };
-        if (p.q) {
-          T qv = act ? p.q[s] : T(0);
-          p2m_laplace<T>(p.N, xc, xs, qv, emit);
-        }
-        if (p.dip) {
-          T dv = act ? p.dip[s] : T(0);
-          T nrm[3] = {act ? p.nx[s] : T(0), act ? p.ny[s] : T(0),
-                      act ? p.nz[s] : T(1)};
-          p2m_laplace_dipole<T>(p.N, xc, xs, nrm, dv, emit);
-        }
-      }
+      };
+      if (legt) expand(LegTab<T>{lt, LW});
+      else expand(LegDirect<T>());
     }
   }
   __syncwarp();
@@ -122,13 +141,14 @@ template <typename T, bool HELM>
 int launch_p2m(const P2MParams<T>& p, cudaStream_t s) {
   if (p.nbox <= 0) return 0;
   const int nw = 4;
-  size_t smem = sizeof(T) * (size_t)nw * ncoef(p.N) * (HELM ? 2 : 1);
+  const size_t leg = leg_table_bytes<T>(p.N);
+  size_t smem = leg + sizeof(T) * (size_t)nw * ncoef(p.N) * (HELM ? 2 : 1);
   if (smem > 48 * 1024)
     WBFMM_CUDA(cudaFuncSetAttribute(k_p2m<T, HELM>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)smem));
   unsigned grid = (unsigned)((p.nbox + nw - 1) / nw);
-  k_p2m<T, HELM><<<grid, nw * 32, smem, s>>>(p);
+  k_p2m<T, HELM><<<grid, nw * 32, smem, s>>>(p, leg ? 1 : 0);
   WBFMM_CUDA(cudaGetLastError());
   return 0;
 }
@@ -513,7 +533,7 @@ struct LapRecTab {
 
 // shared-memory bytes of the L2P tables at order N (0: computed on the fly)
 template <typename T, bool HELM>
-static size_t l2p_table_bytes(int N) {
+__host__ __device__ inline size_t l2p_table_bytes(int N) {
   const size_t b = HELM ? 2 * (size_t)(N + 3) * (2 * N + 3) * sizeof(T)
                         : 3 * (size_t)(N + 1) * (N + 1) * sizeof(T);
   return b <= 40 * 1024 ? b : 0;
@@ -521,11 +541,15 @@ static size_t l2p_table_bytes(int N) {
 
 // one thread per target (sorted by box); potential and gradient in one sweep
 template <typename T, bool HELM>
-__global__ void k_l2p(EvalParams<T> p, int tab) {
+__global__ void k_l2p(EvalParams<T> p, int tab, int legt) {
   extern __shared__ __align__(16) unsigned char l2p_sm[];
   T* st = (T*)l2p_sm;
   const int N = p.N;
   const int W = 2 * N + 3, M0 = N + 1;
+  // Legendre constants (degrees <= N + 2) after the recursion tables
+  const int LW = N + 3;
+  T* lt = st + (tab ? l2p_table_bytes<T, HELM>(N) / sizeof(T) : 0);
+  if (legt) leg_table_fill(lt, N + 2, threadIdx.x, blockDim.x);
   if (tab) {
     if (HELM) {
       T* ta = st;
@@ -544,8 +568,8 @@ __global__ void k_l2p(EvalParams<T> p, int tab) {
         else e[0] = e[1] = e[2] = T(0);
       }
     }
-    __syncthreads();
   }
+  if (tab || legt) __syncthreads();
   const int jt = blockIdx.x * blockDim.x + threadIdx.x;
   if (jt >= p.ntgt) return;
   const int64_t b = p.tbox[jt];
@@ -562,38 +586,44 @@ __global__ void k_l2p(EvalParams<T> p, int tab) {
       int64_t off = layout_off(b, idx, nc);
       *re = p.mpr[2 * off]; *im = p.mpr[2 * off + 1];
     };
-    if (p.grad) {
-      T g[6] = {T(0), T(0), T(0), T(0), T(0), T(0)}, f[2] = {T(0), T(0)};
-      T* fp = p.pot ? f : nullptr;
-      if (tab) {
-        RecTab<T> rt{st, st + (N + 3) * W, W, M0};
-        l2p_helmholtz_grad<T>(N, p.k, xc, xf, coef, g, fp, rt);
-      } else {
-        l2p_helmholtz_grad<T>(N, p.k, xc, xf, coef, g, fp);
+    auto eval = [&](const auto& leg) {
+      if (p.grad) {
+        T g[6] = {T(0), T(0), T(0), T(0), T(0), T(0)}, f[2] = {T(0), T(0)};
+        T* fp = p.pot ? f : nullptr;
+        if (tab) {
+          RecTab<T> rt{st, st + (N + 3) * W, W, M0};
+          l2p_helmholtz_grad<T>(N, p.k, xc, xf, coef, g, fp, rt, leg);
+        } else {
+          l2p_helmholtz_grad<T>(N, p.k, xc, xf, coef, g, fp, RecDirect<T>(), leg);
+        }
+        for (int c = 0; c < 6; c++) p.grad[6 * (size_t)o + c] = g[c];
+        if (p.pot) { p.pot[2 * (size_t)o] = f[0]; p.pot[2 * (size_t)o + 1] = f[1]; }
+      } else if (p.pot) {
+        T fr = T(0), fi = T(0);
+        l2p_helmholtz<T>(N, p.k, xc, xf, coef, &fr, &fi, leg);
+        p.pot[2 * (size_t)o] = fr; p.pot[2 * (size_t)o + 1] = fi;
       }
-      for (int c = 0; c < 6; c++) p.grad[6 * (size_t)o + c] = g[c];
-      if (p.pot) { p.pot[2 * (size_t)o] = f[0]; p.pot[2 * (size_t)o + 1] = f[1]; }
-    } else if (p.pot) {
-      T fr = T(0), fi = T(0);
-      l2p_helmholtz<T>(N, p.k, xc, xf, coef, &fr, &fi);
-      p.pot[2 * (size_t)o] = fr; p.pot[2 * (size_t)o + 1] = fi;
-    }
+    };
+    if (legt) eval(LegTab<T>{lt, LW}); else eval(LegDirect<T>());
   } else {
     auto coef = [&](int idx) -> T { return p.mpr[layout_off(b, idx, nc)]; };
-    if (p.grad) {
-      T g[3] = {T(0), T(0), T(0)}, f = T(0);
-      T* fp = p.pot ? &f : nullptr;
-      if (tab) {
-        LapRecTab<T> rt{st, N + 1};
-        l2p_laplace_grad<T>(N, xc, xf, coef, g, fp, rt);
-      } else {
-        l2p_laplace_grad<T>(N, xc, xf, coef, g, fp);
+    auto eval = [&](const auto& leg) {
+      if (p.grad) {
+        T g[3] = {T(0), T(0), T(0)}, f = T(0);
+        T* fp = p.pot ? &f : nullptr;
+        if (tab) {
+          LapRecTab<T> rt{st, N + 1};
+          l2p_laplace_grad<T>(N, xc, xf, coef, g, fp, rt, leg);
+        } else {
+          l2p_laplace_grad<T>(N, xc, xf, coef, g, fp, LapRecDirect<T>(), leg);
+        }
+        for (int c = 0; c < 3; c++) p.grad[3 * (size_t)o + c] = g[c];
+        if (p.pot) p.pot[o] = f;
+      } else if (p.pot) {
+        p.pot[o] = l2p_laplace<T>(N, xc, xf, coef, leg);
       }
-      for (int c = 0; c < 3; c++) p.grad[3 * (size_t)o + c] = g[c];
-      if (p.pot) p.pot[o] = f;
-    } else if (p.pot) {
-      p.pot[o] = l2p_laplace<T>(N, xc, xf, coef);
-    }
+    };
+    if (legt) eval(LegTab<T>{lt, LW}); else eval(LegDirect<T>());
   }
 }
 
@@ -601,7 +631,12 @@ template <typename T, bool HELM>
 int launch_l2p(const EvalParams<T>& p, cudaStream_t s) {
   if (p.ntgt <= 0) return 0;
   const size_t sm = l2p_table_bytes<T, HELM>(p.N);
-  k_l2p<T, HELM><<<(p.ntgt + 127) / 128, 128, sm, s>>>(p, sm ? 1 : 0);
+  const size_t lg = leg_table_bytes<T>(p.N);
+  if (sm + lg > 48 * 1024)
+    WBFMM_CUDA(cudaFuncSetAttribute(k_l2p<T, HELM>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)(sm + lg)));
+  k_l2p<T, HELM><<<(p.ntgt + 127) / 128, 128, sm + lg, s>>>(p, sm ? 1 : 0, lg ? 1 : 0);
   WBFMM_CUDA(cudaGetLastError());
   return 0;
 }
