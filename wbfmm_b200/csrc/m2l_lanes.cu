@@ -99,6 +99,23 @@ __device__ __forceinline__ T2 cm(T2 a, T er, T ei) {
 }
 
 
+// asynchronous global -> shared copies of one element (Ampere-style
+// cp.async, completion by group)
+__device__ __forceinline__ void cp_async_t(float* dst, const float* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src));
+}
+__device__ __forceinline__ void cp_async_t(double* dst, const double* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src));
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::);
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
 template <int P>
 struct LaneDims {
   static constexpr int VF = (P + 1) * (P + 1);                 // full vector
@@ -160,17 +177,23 @@ struct LaneSmem {
   static constexpr int ncols = LaneReg<T, HELM, P>::value ? 1 : 2;
   static constexpr size_t col_bytes =
       ncols * sizeof(T) * 2 * (size_t)(HELM ? LaneDims<P>::VF : LaneDims<P>::VH) * 32;
-  static constexpr int W = col_bytes * 4 <= 200 * 1024 ? 4
-                         : col_bytes * 2 <= 200 * 1024 ? 2 : 1;
-  static constexpr int CTA = 32 * W;
   static constexpr int off_eph = LaneDims<P>::NH;
   static constexpr int off_ech = off_eph + 2 * (P + 1);
   static constexpr int off_cx = off_ech + 2 * (P + 1);
   static constexpr int ops = off_cx + (HELM ? 2 * LaneDims<P>::NC : LaneDims<P>::NL);
-  static constexpr int ops_pad = (ops + 3) & ~3;
+  static constexpr int ops_pad = (ops + 3) & ~3;   // one operator buffer
+  // Laplace stages the next offset's operator while the lanes apply the
+  // current one (two buffers); Helmholtz stages between barriers (one)
+  static constexpr bool DB = !HELM;
+  static constexpr size_t ops_bytes = sizeof(T) * (size_t)((DB ? 2 : 1) * ops_pad);
+  static constexpr size_t cap = 220 * 1024;
+  static constexpr int W = ops_bytes + col_bytes * 4 <= cap ? 4
+                         : ops_bytes + col_bytes * 2 <= cap ? 2 : 1;
+  static constexpr bool fits = ops_bytes + col_bytes * W <= cap;
+  static constexpr int CTA = 32 * W;
   static constexpr int V = HELM ? LaneDims<P>::VF : LaneDims<P>::VH;
   // per-lane columns (accumulator, working vector) per warp, T2 each
-  static constexpr size_t bytes = sizeof(T) * (size_t)ops_pad + col_bytes * W;
+  static constexpr size_t bytes = ops_bytes + col_bytes * W;
 };
 
 template <typename T, bool HELM, int P>
@@ -182,12 +205,8 @@ k_m2l_lanes(LanesParams<T> p, OpTables<T> t) {
   constexpr int kLanesCTA = SM::CTA;
   constexpr int V = SM::V;
   extern __shared__ __align__(16) unsigned char smraw[];
-  T* ops = (T*)smraw;
-  const T* sH = ops;
-  const T* seph = ops + SM::off_eph;
-  const T* sech = ops + SM::off_ech;
-  const T* scx = ops + SM::off_cx;
-  T2* cols = (T2*)(ops + SM::ops_pad);
+  T* opsb = (T*)smraw;                         // operator buffer(s)
+  T2* cols = (T2*)(smraw + SM::ops_bytes);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   constexpr bool REG = LaneReg<T, HELM, P>::value;
   T2* acc = cols + (size_t)warp * SM::ncols * V * 32 + lane;   // accumulator, stride 32
@@ -220,44 +239,59 @@ k_m2l_lanes(LanesParams<T> p, OpTables<T> t) {
 #pragma unroll 1
   for (int c = 0; c < V; c++) { T2 z; z.x = T(0); z.y = T(0); acc[c * 32] = z; }
 
-  const int nH = LaneDims<P>::NH;
+  // Staging of an offset's operator: the rotation block, both phase sets
+  // and the coaxial coefficients (Helmholtz: the level's table of the
+  // offset's distance; Laplace: the level's scaled S|R of the shift code).
+  // Laplace double-buffers it: while the lanes apply offset j's operator
+  // from one buffer, offset j + nsplit's streams into the other (cp.async),
+  // so one barrier per offset both publishes a buffer and retires the other.
+  auto copy = [&](T* d, const T* src) {
+    if constexpr (SM::DB) cp_async_t(d, src); else *d = *src;
+  };
+  auto stage = [&](int j, T* dst) {
+    const int op = c_offsets[tau][j] & 511;
+    const T* H = t.H + (int64_t)t.op_ith[op] * t.hstride;
+    for (int i = threadIdx.x; i < LaneDims<P>::NH; i += kLanesCTA) copy(dst + i, H + i);
+    const T* eph = t.ph + (size_t)op * (t.lmax + 1) * 2;
+    const T* ech = t.ch + (size_t)op * (t.lmax + 1) * 2;
+    for (int i = threadIdx.x; i < 2 * (P + 1); i += kLanesCTA) {
+      copy(dst + SM::off_eph + i, eph + i);
+      copy(dst + SM::off_ech + i, ech + i);
+    }
+    if (HELM) {
+      const T* cx = p.coax + (int64_t)t.op_dist[op] * p.coax_stride;
+      for (int i = threadIdx.x; i < 2 * LaneDims<P>::NC; i += kLanesCTA)
+        copy(dst + SM::off_cx + i, cx + i);
+    } else {
+      const T* cx = (const T*)p.lapsr + (int64_t)op * LaneDims<P>::NL;
+      for (int i = threadIdx.x; i < LaneDims<P>::NL; i += kLanesCTA)
+        copy(dst + SM::off_cx + i, cx + i);
+    }
+    if constexpr (SM::DB) cp_async_commit();
+  };
+  if (SM::DB && split < 189) stage(split, opsb);
+  int buf = 0;
 #pragma unroll 1
   for (int j = split; j < 189; j += p.nsplit) {
     const int code = c_offsets[tau][j];
-    const int op = code & 511, sg = (code >> 9) & 7;
+    const int sg = (code >> 9) & 7;
     const int ddx = ((code >> 12) & 3) - 1, ddy = ((code >> 14) & 3) - 1,
               ddz = ((code >> 16) & 3) - 1;
-    __syncthreads();   // previous operator no longer in use
-    {
-      const T* H = t.H + (int64_t)t.op_ith[op] * t.hstride;
-      for (int i = threadIdx.x; i < nH; i += kLanesCTA) ops[i] = H[i];
-      const T* eph = t.ph + (size_t)op * (t.lmax + 1) * 2;
-      const T* ech = t.ch + (size_t)op * (t.lmax + 1) * 2;
-      for (int i = threadIdx.x; i < 2 * (P + 1); i += kLanesCTA) {
-        ops[SM::off_eph + i] = eph[i];
-        ops[SM::off_ech + i] = ech[i];
-      }
-      if (HELM) {
-        const T* cx = p.coax + (int64_t)t.op_dist[op] * p.coax_stride;
-        for (int i = threadIdx.x; i < 2 * LaneDims<P>::NC; i += kLanesCTA)
-          ops[SM::off_cx + i] = cx[i];
-      } else {
-        // S|R(n,nd,m) / (t^{n+1} (2^e t)^nd), t = width * |d|, on
-        // sources scaled by 2^(e nd)
-        const T r = p.width * t.op_r[op];
-        const T rinv = T(1) / r, qinv = T(1) / scale2(r, p.lap_e);
-        const int Dm = t.lt + 1;
-        for (int i = threadIdx.x; i < LaneDims<P>::NL; i += kLanesCTA) {
-          int m = i % (P + 1), nd = (i / (P + 1)) % (P + 1), n = i / ((P + 1) * (P + 1));
-          T v = t.lapSR[((int64_t)n * Dm + nd) * Dm + m];
-          T s = rinv, q = T(1);
-          for (int e = 0; e < n; e++) s *= rinv;
-          for (int e = 0; e < nd; e++) q *= qinv;
-          ops[SM::off_cx + i] = (v * q) * s;
-        }
-      }
+    if constexpr (SM::DB) {
+      cp_async_wait_all();
+      __syncthreads();   // this offset's operator visible; the other buffer free
+      if (j + p.nsplit < 189) stage(j + p.nsplit, opsb + (buf ^ 1) * SM::ops_pad);
+    } else {
+      __syncthreads();   // previous operator no longer in use
+      stage(j, opsb);
+      __syncthreads();
     }
-    __syncthreads();
+    const T* ops = opsb + buf * SM::ops_pad;
+    if constexpr (SM::DB) buf ^= 1;
+    const T* sH = ops;
+    const T* seph = ops + SM::off_eph;
+    const T* sech = ops + SM::off_ech;
+    const T* scx = ops + SM::off_cx;
     if (!active) continue;
     const T2* src = (const T2*)p.lin_raw + (int64_t)sg * V * npp + pp + ddx +
                     npx * ((int64_t)ddy + npx * (int64_t)ddz);
@@ -492,6 +526,36 @@ __global__ void k_lanes_reduce(LanesParams<T> p, int N) {
   }
 }
 
+// ------------------------------------------------- Laplace operators
+template <typename T>
+__global__ void k_lap_sr_ops(OpTables<T> t, int P, T width, int lap_e, T* out) {
+  const int P1 = P + 1, NL = P1 * P1 * P1;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (int64_t)kNumOps * NL) return;
+  const int op = (int)(i / NL), e = (int)(i % NL);
+  const int m = e % P1, nd = (e / P1) % P1, n = e / (P1 * P1);
+  const T r = width * t.op_r[op];
+  if (!(r > T(0))) { out[i] = T(0); return; }   // shift codes that are not list-4
+  const T rinv = T(1) / r, qinv = T(1) / scale2(r, lap_e);
+  const int Dm = t.lt + 1;
+  const T v = t.lapSR[((int64_t)n * Dm + nd) * Dm + m];
+  T sc = rinv, q = T(1);
+  for (int k = 0; k < n; k++) sc *= rinv;
+  for (int k = 0; k < nd; k++) q *= qinv;
+  out[i] = (v * q) * sc;
+}
+
+template <typename T>
+int build_lap_sr_ops(const OpTables<T>& t, int P, T width, int lap_e, T* out,
+                     cudaStream_t s) {
+  const int64_t tot = (int64_t)kNumOps * (P + 1) * (P + 1) * (P + 1);
+  k_lap_sr_ops<T><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(t, P, width, lap_e, out);
+  WBFMM_CUDA(cudaGetLastError());
+  return 0;
+}
+template int build_lap_sr_ops<float>(const OpTables<float>&, int, float, int, float*, cudaStream_t);
+template int build_lap_sr_ops<double>(const OpTables<double>&, int, double, int, double*, cudaStream_t);
+
 // ------------------------------------------------------- active lists
 constexpr int kActBlock = 256;
 
@@ -618,7 +682,18 @@ static int launch_lanes_P(const LanesParams<T>& p, const OpTables<T>& t,
 template <typename T, bool HELM>
 bool lanes_supported(int Ns, int Nr) {
   if (Ns != Nr) return false;
-  return HELM ? (Ns >= 2 && Ns <= kLanesMaxHelm) : (Ns >= 2 && Ns <= kLanesMaxLap);
+  if (HELM ? (Ns < 2 || Ns > kLanesMaxHelm) : (Ns < 2 || Ns > kLanesMaxLap)) return false;
+  // the instantiation's operator buffers and vector columns fit one CTA
+  switch (Ns) {
+#define WBFMM_LANES_FIT(PP) \
+  case PP: return LaneSmem<T, HELM, PP>::fits;
+    WBFMM_LANES_FIT(2) WBFMM_LANES_FIT(3) WBFMM_LANES_FIT(4) WBFMM_LANES_FIT(5)
+    WBFMM_LANES_FIT(6) WBFMM_LANES_FIT(7) WBFMM_LANES_FIT(8) WBFMM_LANES_FIT(9)
+    WBFMM_LANES_FIT(10) WBFMM_LANES_FIT(11) WBFMM_LANES_FIT(12) WBFMM_LANES_FIT(13)
+    WBFMM_LANES_FIT(14) WBFMM_LANES_FIT(15) WBFMM_LANES_FIT(16)
+#undef WBFMM_LANES_FIT
+    default: return false;
+  }
 }
 
 template <typename T, bool HELM>

@@ -23,6 +23,7 @@ struct LanesParams {
   T width;              // box width of the level
   const uint8_t* tmask; // targets to compute, or null for all
   int lap_e;            // Laplace: degree l of lin_raw is scaled by 2^(lap_e l)
+  const void* lapsr;    // Laplace: [kNumOps][(P+1)^3] scaled S|R per shift (build_lap_sr_ops)
   const int* act;       // sparse targets: [8][np] parents per child type, or null
   const int* act_n;     // [8] list lengths (device)
   void* partial_raw;    // [nsplit][8][V][np] complex when nsplit > 1
@@ -81,6 +82,13 @@ size_t lanes_lin_bytes(int level, int N, bool helm, size_t tsize);
 // has tmask set, ascending, in act[tau * np ...], with the lengths in
 // act_n[8].  act holds 8^level ints; scratch active_list_scratch(level) ints.
 size_t active_list_scratch(int level);
+
+// Laplace M2L operators of one level for the lane kernel, per shift code:
+// out[op][(n (P+1) + nd) (P+1) + m] = S|R(n, nd, m) / (t^(n+1) (2^e t)^nd),
+// t = width |d_op| (the scaled form of lap_scale_exp)
+template <typename T>
+int build_lap_sr_ops(const OpTables<T>& t, int P, T width, int lap_e, T* out,
+                     cudaStream_t s);
 int build_active_lists(const uint8_t* tmask, int level, int* act, int* act_n,
                        int* scratch, cudaStream_t s);
 template <typename T, bool HELM>

@@ -194,6 +194,7 @@ struct Solver : public wbfmm_b200_solver {
   DBuf<uint32_t> tperm, tbox, tstart, tcount;
   DBuf<uint8_t> tmask[kMaxDepth + 1];
   DBuf<int> act[kMaxDepth + 1], act_n[kMaxDepth + 1], act_scr;   // M2L target lists
+  DBuf<T> lapsr;                    // Laplace lane M2L: scaled operators of the level
   DBuf<int> flag;
   // outputs (original order)
   DBuf<T> pot, grad;
@@ -260,7 +261,7 @@ struct Solver : public wbfmm_b200_solver {
     f(tstart); f(tcount); f(flag); f(pot); f(grad); f(out64);
     f(H64); f(H); f(op_ith); f(op_dist); f(op_r); f(op_ph); f(op_ch);
     for (int i = 0; i < 3; i++) { f(lap64[i]); f(lap[i]); }
-    f(partial); f(lin); f(lanes_part); f(act_scr);
+    f(partial); f(lin); f(lanes_part); f(act_scr); f(lapsr);
   }
 
   ~Solver() override {
@@ -748,6 +749,13 @@ struct Solver : public wbfmm_b200_solver {
       lp.coax = x.coax; lp.coax_stride = x.coax_stride;
       lp.width = x.width; lp.tmask = x.tmask; lp.lap_e = x.lap_e;
       if (x.tmask && act[level].p) { lp.act = act[level].p; lp.act_n = act_n[level].p; }
+      if (!helm) {
+        const int P1 = x.Nin + 1;
+        WBFMM_TRY(lapsr.alloc((size_t)kNumOps * P1 * P1 * P1));
+        WBFMM_TRY(build_lap_sr_ops<T>(tables, x.Nin, x.width, x.lap_e, lapsr.p, stream));
+        lp.lapsr = lapsr.p;
+        launches++;
+      }
       const int64_t np = (int64_t)1 << (3 * (level - 1));
       const int64_t base = ((np + 127) / 128) * 8;
       int ns = 1;
