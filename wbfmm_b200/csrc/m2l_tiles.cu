@@ -115,8 +115,7 @@ k_m2l_tiles(LanesParams<T> p, OpTables<T> t, int TC) {
   T* sH = (T*)smraw;
   T* seph = sH + q.NH;
   T* sech = seph + 2 * (P + 1);
-  T* spw = sech + 2 * (P + 1);       // Laplace: 1/t^(j+1), then 1/(2^e t)^j, j <= P
-  T* scx = spw + 2 * (P + 1);
+  T* scx = sech + 4 * (P + 1);       // (2 (P + 1) spare entries between)
   int* dB = (int*)(smraw + q.ops_bytes);
   int* dC = dB + q.nB;
   int* s_nm = dC + q.nC;             // (n, m) of each vector entry
@@ -190,23 +189,10 @@ k_m2l_tiles(LanesParams<T> p, OpTables<T> t, int TC) {
         const T* cx = p.coax + (int64_t)t.op_dist[op] * p.coax_stride;
         for (int i = tid; i < q.ncx; i += kTileThreads) scx[i] = cx[i];
       } else {
-        // S|R(n,nd,m) / (t^{n+1} (2^e t)^nd), t = width * |d|, on
-        // sources scaled by 2^(e nd)
-        if (tid == 0) {
-          const T r = p.width * t.op_r[op];
-          const T rinv = T(1) / r, qinv = T(1) / scale2(r, p.lap_e);
-          T s = rinv, u = T(1);
-          for (int e = 0; e <= P; e++) {
-            spw[e] = s; s *= rinv;
-            spw[P + 1 + e] = u; u *= qinv;
-          }
-        }
-        __syncthreads();
-        const int Dm = t.lt + 1;
-        for (int i = tid; i < q.ncx; i += kTileThreads) {
-          int m = i % (P + 1), nd = (i / (P + 1)) % (P + 1), n = i / ((P + 1) * (P + 1));
-          scx[i] = (t.lapSR[((int64_t)n * Dm + nd) * Dm + m] * spw[P + 1 + nd]) * spw[n];
-        }
+        // the level's S|R(n,nd,m) / (t^{n+1} (2^e t)^nd) of this shift code
+        // (build_lap_sr_ops), on sources scaled by 2^(e nd)
+        const T* cx = (const T*)p.lapsr + (int64_t)op * q.ncx;
+        for (int i = tid; i < q.ncx; i += kTileThreads) scx[i] = cx[i];
       }
     }
     __syncthreads();   // operator staged

@@ -722,6 +722,13 @@ struct Solver : public wbfmm_b200_solver {
       lp.coax = x.coax; lp.coax_stride = x.coax_stride;
       lp.width = x.width; lp.tmask = x.tmask; lp.lap_e = x.lap_e;
       if (x.tmask && act[level].p) { lp.act = act[level].p; lp.act_n = act_n[level].p; }
+      if (!helm) {
+        const int P1 = x.Nin + 1;
+        WBFMM_TRY(lapsr.alloc((size_t)kNumOps * P1 * P1 * P1));
+        WBFMM_TRY(build_lap_sr_ops<T>(tables, x.Nin, x.width, x.lap_e, lapsr.p, stream));
+        lp.lapsr = lapsr.p;
+        launches++;
+      }
       const int64_t np = (int64_t)1 << (3 * (level - 1));
       const int tc = helm ? tiles_per_cta<T, true>(x.Nin) : tiles_per_cta<T, false>(x.Nin);
       const int64_t ctas = ((np + tc - 1) / tc) * 8;
