@@ -134,6 +134,17 @@ int wbfmm_b200_run_graph(wbfmm_b200_solver_t *s);
    fails the check leaves its fields undefined.  Default 0. */
 int wbfmm_b200_set_deferred_checks(wbfmm_b200_solver_t *s, int on);
 
+/* Laplace curl of a vector potential (the reference's WBFMM_FIELD_CURL for
+   three source components, src/local-laplace.c:632-750,
+   src/direct-laplace.c:87-130): curl[3 j + i] = sum over sources of
+   (grad 1/(4 pi r) x q)_i at target j, q = (q3[s qstr], q3[s qstr + 1],
+   q3[s qstr + 2]).  The solver must be Laplace with the gradient field and
+   have its sources and targets set; it runs the three components' solves on
+   its tree (the strengths it holds afterwards are the z components).
+   Blocks until the curl is written. */
+int wbfmm_b200_laplace_curl(wbfmm_b200_solver_t *s, const double *q3, int qstr,
+                            double *curl, int on_device);
+
 /* Self-test of the FP32 near-field sine and cosine: the largest absolute
    error of the engine's own routine (err2[0]) and of CUDA's sincosf
    (err2[1]) against FP64 sin/cos at the FP32 arguments i * xmax / n,

@@ -165,6 +165,10 @@ class Reference:
                                              C.c_int, _dp, C.c_int, _dp]
         lib.ref_direct_laplace.argtypes = [C.c_int, _dp, _dp, _dp, _dp, C.c_int, _dp,
                                            C.c_int, _dp]
+        lib.wbfmm_laplace_field_direct.restype = C.c_int
+        lib.wbfmm_laplace_field_direct.argtypes = [_dp, C.c_int, _dp, C.c_int, C.c_int, _dp,
+                                                   C.c_int, _dp, C.c_int, C.c_int, C.c_uint,
+                                                   _dp, _dp, C.c_int]
 
     def fmm(self, problem, depth, order_s, order_r, x0, D, xs, q, xt, k=0.0,
             normals=None, dipoles=None, pot=True, grad=True, bw=False,
@@ -255,6 +259,27 @@ class Reference:
                                         _ptr(normals), _ptr(dipoles), nt,
                                         _ptr(xt), int(grad), _ptr(f))
         return f
+
+
+    def direct_curl(self, xs, q3, xt):
+        """The reference's direct Laplace curl (WBFMM_FIELD_CURL, nq = 3,
+        src/direct-laplace.c:87-130, 274-340), one target at a time."""
+        xs = _f64(xs).reshape(-1, 3); q3 = _f64(q3).reshape(-1, 3)
+        xt = _f64(xt).reshape(-1, 3)
+        out = np.zeros((xt.shape[0], 3))
+        for j in range(xt.shape[0]):
+            xf = np.ascontiguousarray(xt[j]); f = np.zeros(3)
+            self.lib.wbfmm_laplace_field_direct(_ptr(xs), 3, None, 0, xs.shape[0], _ptr(q3), 3,
+                                                None, 0, 3, 4, _ptr(xf), _ptr(f), 3)
+            out[j] = f
+        return out
+
+
+def curl_from_gradients(g):
+    """curl_i = e_ijk d_j A_k from the gradients g[k] ([nt, 3]) of the three
+    components of a vector potential."""
+    gx, gy, gz = (np.asarray(a).reshape(-1, 3) for a in g)
+    return np.stack([gz[:, 1] - gy[:, 2], gx[:, 2] - gz[:, 0], gy[:, 0] - gx[:, 1]], axis=1)
 
 
 def have_reference() -> bool:

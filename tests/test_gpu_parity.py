@@ -388,3 +388,23 @@ def test_error_norms(gpu_lib, n):
     l2, mx = engine.error_norms(f, ref)
     assert abs(l2 - np.linalg.norm(f - ref) / np.linalg.norm(ref)) <= 1e-12 * l2
     assert mx == np.max(np.abs(f - ref)) / np.max(np.abs(ref))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [engine.FP64, engine.FP32])
+def test_laplace_curl(gpu_lib, precision):
+    """The FMM curl of a vector potential (three source components) against
+    the direct curl built from the oracle's direct gradients, whose
+    convention the CPU suite pins to the reference's direct curl."""
+    from oracle.oracle_api import Restatement, curl_from_gradients
+    p = W.laplace_cube(20000, 2000, depth=4, order=12, seed=62)
+    q3 = np.random.default_rng(63).standard_normal((p.ns, 3))
+    with engine.Solver(engine.SolverConfig.from_problem(p, precision)) as s:
+        s.set_sources(p.xs).set_targets(p.xt)
+        curl = s.laplace_curl(q3)
+    ora = Restatement()
+    g = [ora.direct(LAPLACE, p.xs, q3[:, c].copy(), p.xt, pot=False, grad=True)[1]
+         for c in range(3)]
+    ref = curl_from_gradients(g)
+    tol = 2e-6 if precision == engine.FP64 else 5e-6
+    assert rel_l2(curl.ravel(), ref.ravel()) < tol, rel_l2(curl.ravel(), ref.ravel())

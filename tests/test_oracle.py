@@ -163,3 +163,19 @@ def test_golden_direct_sums(restatement):
 
 def test_box_offsets():
     assert level_box_offsets(2) == [0, 1, 9, 73]
+
+
+def test_curl_convention_matches_reference(restatement, reference):
+    """The Laplace curl as e_ijk d_j A_k of the three components' direct
+    gradients (how the engine forms it) is the reference's direct curl
+    (WBFMM_FIELD_CURL with three source components)."""
+    from oracle.oracle_api import curl_from_gradients
+    rng = np.random.default_rng(61)
+    xs = rng.uniform(-0.5, 0.5, (300, 3))
+    xt = rng.uniform(-0.5, 0.5, (40, 3))
+    q3 = rng.standard_normal((300, 3))
+    g = [restatement.direct(LAPLACE, xs, q3[:, c].copy(), xt, pot=False, grad=True)[1]
+         for c in range(3)]
+    mine = curl_from_gradients(g)
+    ref = reference.direct_curl(xs, q3, xt)
+    assert np.linalg.norm(mine - ref) <= 1e-12 * np.linalg.norm(ref)

@@ -192,6 +192,31 @@ extern "C" int wbfmm_b200_direct(int problem, double k, int ns,
   return rc;
 }
 
+// ------------------------------------------------------------ Laplace curl
+// curl of the vector potential A_k = sum q_k / (4 pi r) from the target
+// gradients g_k of its three components: curl_i = e_ijk d_j A_k
+namespace {
+__global__ void k_curl_combine(const double* __restrict__ g, int nt, double* __restrict__ curl) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= nt) return;
+  const double* gx = g + 3 * (size_t)j;                 // grad A_x
+  const double* gy = g + 3 * ((size_t)nt + j);          // grad A_y
+  const double* gz = g + 3 * (2 * (size_t)nt + j);      // grad A_z
+  curl[3 * (size_t)j] = gz[1] - gy[2];
+  curl[3 * (size_t)j + 1] = gx[2] - gz[0];
+  curl[3 * (size_t)j + 2] = gy[0] - gx[1];
+}
+}  // namespace
+
+namespace wbfmm {
+int launch_curl_combine(const double* g, int nt, double* curl, cudaStream_t s) {
+  if (nt <= 0) return 0;
+  k_curl_combine<<<(nt + 255) / 256, 256, 0, s>>>(g, nt, curl);
+  WBFMM_CUDA(cudaGetLastError());
+  return 0;
+}
+}  // namespace wbfmm
+
 // ------------------------------------------------------------ error norms
 // The accuracy reduction of a field f against a reference r (FP64): per
 // block sums of (f - r)^2 and r^2 and maxima of |f - r| and |r| in a fixed

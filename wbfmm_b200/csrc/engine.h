@@ -56,6 +56,9 @@ int radix_sort_pairs(uint64_t* keys, uint32_t* vals, int n, int bits,
                      RadixScratch* scr, cudaStream_t s, int lo = 0);
 void radix_scratch_free(RadixScratch* scr);
 
+// curl[3 nt] from the gradients g[3][3 nt] of the three potential components
+int launch_curl_combine(const double* g, int nt, double* curl, cudaStream_t s);
+
 // box {i, n} of one level from the sorted keys, reproducing
 // wbfmm_tree_refine (src/boxes.c:208-277); parent_i is read before the
 // parents' .i advance, which launch_refine_parents then applies.

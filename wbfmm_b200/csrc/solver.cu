@@ -168,6 +168,48 @@ int wbfmm_b200_run(wbfmm_b200_solver_t* s) { SOLVER_CALL(s->run()); }
 int wbfmm_b200_run_async(wbfmm_b200_solver_t* s) { SOLVER_CALL(s->run_queued()); }
 int wbfmm_b200_run_graph(wbfmm_b200_solver_t* s) { SOLVER_CALL(s->run_graph()); }
 int wbfmm_b200_wait(wbfmm_b200_solver_t* s) { SOLVER_CALL(s->wait()); }
+int wbfmm_b200_laplace_curl(wbfmm_b200_solver_t* s, const double* q3, int qstr,
+                            double* curl, int on_device) {
+  if (!s || !q3 || !curl || qstr < 3) return set_error(WBFMM_B200_E_ARG, "bad curl arguments");
+  if (s->cfg.problem != WBFMM_B200_LAPLACE)
+    return set_error(WBFMM_B200_E_ARG, "the curl needs a Laplace solver");
+  if (!(s->cfg.field & WBFMM_B200_GRADIENT))
+    return set_error(WBFMM_B200_E_ARG, "the curl needs the gradient field");
+  const int ns = s->sources(), nt = s->targets();
+  if (ns <= 0 || nt <= 0) return set_error(WBFMM_B200_E_STATE, "sources and targets must be set");
+  cudaStream_t st = s->stream;
+  double *g = nullptr, *qd = nullptr, *cd = nullptr;
+  int rc = 0;
+  cudaError_t e = cudaMallocAsync(&g, sizeof(double) * 9 * (size_t)nt, st);
+  // host strengths go to the device whole, so that component c (offset c,
+  // stride qstr) is read inside the array
+  const double* q = q3;
+  if (e == cudaSuccess && !on_device) {
+    e = cudaMallocAsync(&qd, sizeof(double) * (size_t)ns * qstr, st);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(qd, q3, sizeof(double) * (size_t)ns * qstr, cudaMemcpyHostToDevice, st);
+    q = qd;
+  }
+  if (e == cudaSuccess && !on_device) e = cudaMallocAsync(&cd, sizeof(double) * 3 * (size_t)nt, st);
+  if (e != cudaSuccess) rc = set_cuda_error(e, __FILE__, __LINE__);
+  for (int c = 0; c < 3 && !rc; c++) {
+    rc = s->set_strengths(q + c, qstr, nullptr, 0, 1);
+    if (!rc) rc = s->run();
+    if (!rc) rc = s->get_field(nullptr, g + (size_t)c * 3 * nt, 1);
+  }
+  if (!rc) rc = launch_curl_combine(g, nt, on_device ? curl : cd, st);
+  if (!rc && !on_device) {
+    e = cudaMemcpyAsync(curl, cd, sizeof(double) * 3 * (size_t)nt, cudaMemcpyDeviceToHost, st);
+    if (e != cudaSuccess) rc = set_cuda_error(e, __FILE__, __LINE__);
+  }
+  if (g) cudaFreeAsync(g, st);
+  if (qd) cudaFreeAsync(qd, st);
+  if (cd) cudaFreeAsync(cd, st);
+  e = cudaStreamSynchronize(st);
+  if (!rc && e != cudaSuccess) rc = set_cuda_error(e, __FILE__, __LINE__);
+  return rc;
+}
+
 int wbfmm_b200_selftest_sincos(double xmax, int n, double* err2) {
   if (!err2 || n < 1 || !(xmax > 0)) return set_error(WBFMM_B200_E_ARG, "bad self-test arguments");
   if (wbfmm_b200_device_count() < 1) return set_error(WBFMM_B200_E_NOGPU, "no CUDA device is available");

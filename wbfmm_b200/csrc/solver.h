@@ -154,6 +154,8 @@ struct wbfmm_b200_solver {
   virtual int wait() = 0;
   virtual int set_deferred_checks(int on) = 0;
   virtual int get_field(double*, double*, int) = 0;
+  virtual int sources() const = 0;
+  virtual int targets() const = 0;
   virtual int get_tree(uint32_t*, uint32_t*, uint32_t*, int) = 0;
   virtual int get_coefficients(int, double*, double*) = 0;
   virtual int coefficient_pointers(int, void**, void**) = 0;
@@ -1021,6 +1023,8 @@ struct Solver : public wbfmm_b200_solver {
     return 0;
   }
 
+  int sources() const override { return nsrc; }
+  int targets() const override { return ntgt; }
   void invalidate_operators() override { ops_ready = false; gen++; }
   void set_m2l_kernel(int mode) override { m2l_mode = mode; gen++; }
   void set_p2m_accumulate(int on) override { p2m_accumulate = on != 0; gen++; }

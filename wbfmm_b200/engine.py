@@ -94,6 +94,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "wbfmm_b200_set_deferred_checks": (ip, [vp, ip]),
         "wbfmm_b200_selftest_sincos": (ip, [C.c_double, ip, dp]),
         "wbfmm_b200_error_norms": (ip, [C.c_int64, vp, vp, ip, dp]),
+        "wbfmm_b200_laplace_curl": (ip, [vp, vp, ip, vp, ip]),
         "wbfmm_b200_synchronize": (ip, [vp]),
         "wbfmm_b200_get_field": (ip, [vp, vp, vp, ip]),
         "wbfmm_b200_get_tree": (ip, [vp, u32p, u32p, u32p, ip]),
@@ -284,6 +285,14 @@ class Solver:
         """Queue every pass on the solver's stream; wait() blocks."""
         _check(self.lib.wbfmm_b200_run_async(self.h))
         return self
+
+    def laplace_curl(self, q3):
+        """Curl of the vector potential of sources with 3-vector strengths
+        q3 [ns, 3] at the targets: [nt, 3] (Laplace solver, gradient field)."""
+        q3 = _host(q3).reshape(-1, 3)
+        out = np.zeros(self.nt * 3)
+        _check(self.lib.wbfmm_b200_laplace_curl(self.h, _addr(q3), 3, _addr(out), 0))
+        return out.reshape(-1, 3)
 
     def run_graph(self):
         """The passes as one CUDA graph launch (captured on the first call
