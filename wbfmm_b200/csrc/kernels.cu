@@ -15,6 +15,8 @@
 //       sources of the 27 neighbour boxes (src/indexing.c:250-286).
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "engine.h"
 #include "expand.cuh"
 #include "kernels.h"
@@ -694,10 +696,9 @@ __device__ __forceinline__ void sincos_near(float x, float* sp, float* cp) {
 
 // the terms of one (target, source) pair added to acc[0..] (Helmholtz: pot
 // re, im, then grad x re, x im, y, z; Laplace: pot, grad x, y, z)
-template <typename T, bool HELM, int NT>
+template <typename T, bool HELM, int NT, bool want_pot, bool want_grad>
 __device__ __forceinline__ void p2p_pair(const P2PTile<T, HELM, NT>& tl, int j, T rx, T ry, T rz,
-                                         T k, T kinv, bool hd, bool want_pot,
-                                         bool want_grad, T* acc) {
+                                         T k, T kinv, bool hd, T* acc) {
   const T f4pi = T(0.25 / kPi);
   const T r2 = rx * rx + ry * ry + rz * rz;
   const T ir = rsqrt(r2);
@@ -769,7 +770,8 @@ __device__ __forceinline__ void p2p_pair(const P2PTile<T, HELM, NT>& tl, int j, 
   }
 }
 
-template <typename T, bool HELM, int NT>
+// POT / GRAD: the fields computed, fixed at compile time (dipoles at run time)
+template <typename T, bool HELM, int NT, bool POT, bool GRAD>
 __global__ void __launch_bounds__(NT, NT == 32 ? 20 : 1)
 k_p2p(EvalParams<T> p) {
   constexpr bool F32 = sizeof(T) == 4;
@@ -808,11 +810,11 @@ k_p2p(EvalParams<T> p) {
   const T k = p.k;
   const T kinv = HELM ? T(1) / k : T(0);
   const bool hq = p.q != nullptr, hd = p.dip != nullptr;
-  const bool want_pot = p.pot != nullptr, want_grad = p.grad != nullptr;
-  // FP32 form: source coordinates as float pairs in the FP64 arrays' bytes
-  float* xh = (float*)tl.x; float* xl = xh + NT;
-  float* yh = (float*)tl.y; float* yl = yh + NT;
-  float* zh = (float*)tl.z; float* zl = zh + NT;
+  constexpr bool want_pot = POT, want_grad = GRAD;
+  // FP32 form: source coordinates as float pairs (hi, lo) in the FP64 arrays' bytes
+  float2* xp = (float2*)tl.x;
+  float2* yp = (float2*)tl.y;
+  float2* zp = (float2*)tl.z;
   int G = 32;
   while (G > 1 && (uint32_t)(NT / G) < tc) G >>= 1;
   const int gl = tid & (G - 1), ti = tid / G, tpp = NT / G;
@@ -834,9 +836,9 @@ k_p2p(EvalParams<T> p) {
         const double sx = p.x[s], sy = p.y[s], sz = p.z[s];
         if constexpr (F32) {
           const float hx = (float)sx, hy = (float)sy, hz = (float)sz;
-          xh[tid] = hx; xl[tid] = (float)(sx - (double)hx);
-          yh[tid] = hy; yl[tid] = (float)(sy - (double)hy);
-          zh[tid] = hz; zl[tid] = (float)(sz - (double)hz);
+          xp[tid] = make_float2(hx, (float)(sx - (double)hx));
+          yp[tid] = make_float2(hy, (float)(sy - (double)hy));
+          zp[tid] = make_float2(hz, (float)(sz - (double)hz));
         } else {
           tl.x[tid] = sx; tl.y[tid] = sy; tl.z[tid] = sz;
         }
@@ -861,11 +863,12 @@ k_p2p(EvalParams<T> p) {
           for (int u = 0; u < kP2PRun; u++) {
             const int j = j0 + u * G;
             if (j < nt) {
-              const T rx = (T)((txh - xh[j]) + (txl - xl[j]));
-              const T ry = (T)((tyh - yh[j]) + (tyl - yl[j]));
-              const T rz = (T)((tzh - zh[j]) + (tzl - zl[j]));
+              const float2 cx = xp[j], cy = yp[j], cz = zp[j];
+              const T rx = (T)((txh - cx.x) + (txl - cx.y));
+              const T ry = (T)((tyh - cy.x) + (tyl - cy.y));
+              const T rz = (T)((tzh - cz.x) + (tzl - cz.y));
               if (rx * rx + ry * ry + rz * rz > rc2)
-                p2p_pair<T, HELM, NT>(tl, j, rx, ry, rz, k, kinv, hd, want_pot, want_grad, acc);
+                p2p_pair<T, HELM, NT, POT, GRAD>(tl, j, rx, ry, rz, k, kinv, hd, acc);
             }
           }
           for (int c = 0; c < NA; c++) a[c] += (double)acc[c];
@@ -877,7 +880,7 @@ k_p2p(EvalParams<T> p) {
           if (!(rx * rx + ry * ry + rz * rz > rc2)) continue;
           T acc[NA];
           for (int c = 0; c < NA; c++) acc[c] = T(0);
-          p2p_pair<T, HELM, NT>(tl, j, rx, ry, rz, k, kinv, hd, want_pot, want_grad, acc);
+          p2p_pair<T, HELM, NT, POT, GRAD>(tl, j, rx, ry, rz, k, kinv, hd, acc);
           for (int c = 0; c < NA; c++) a[c] += (double)acc[c];
         }
       }
@@ -910,10 +913,16 @@ k_p2p(EvalParams<T> p) {
 template <typename T, bool HELM>
 int launch_p2p(const EvalParams<T>& p, cudaStream_t s) {
   if (p.nbox <= 0 || p.ntgt <= 0) return 0;
-  if (p.ntgt <= 8 * p.nbox)   // a few targets per leaf on average
-    k_p2p<T, HELM, 32><<<(unsigned)p.nbox, 32, 0, s>>>(p);
-  else
-    k_p2p<T, HELM, 128><<<(unsigned)p.nbox, 128, 0, s>>>(p);
+  auto go = [&](auto pot, auto grad) {
+    constexpr bool P = decltype(pot)::value, G = decltype(grad)::value;
+    if (p.ntgt <= 8 * p.nbox)   // a few targets per leaf on average
+      k_p2p<T, HELM, 32, P, G><<<(unsigned)p.nbox, 32, 0, s>>>(p);
+    else
+      k_p2p<T, HELM, 128, P, G><<<(unsigned)p.nbox, 128, 0, s>>>(p);
+  };
+  if (p.pot && p.grad) go(std::true_type(), std::true_type());
+  else if (p.pot) go(std::true_type(), std::false_type());
+  else if (p.grad) go(std::false_type(), std::true_type());
   WBFMM_CUDA(cudaGetLastError());
   return 0;
 }
