@@ -272,7 +272,9 @@ int wbfmm_b200_fp32_range_ok(const wbfmm_b200_config_t *cfg);
    independent solves on one GPU.  `nslots` solves run at once, each on its
    own stream, admitted first come first served while the summed
    wbfmm_b200_footprint of the solves in flight stays within `hbm_budget`
-   bytes.  Operator tables are shared across solves (per order; Helmholtz
+   bytes less the slots' allowance for keeping work buffers between solves
+   (per slot hbm_budget / (4 nslots), at most 4 GB; a slot whose buffers
+   grow past it releases them).  Operator tables are shared across solves (per order; Helmholtz
    coaxial tables per (k * box width, order)).  Inputs and outputs are host
    arrays that the caller keeps alive until the request completes; fields
    come back in FP64 in the layouts of wbfmm_b200_get_field.  All calls are

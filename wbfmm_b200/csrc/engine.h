@@ -7,6 +7,7 @@
 #include <stdint.h>
 #include <stddef.h>
 
+#include <atomic>
 #include <vector>
 
 #include "fmm_math.cuh"
@@ -25,6 +26,34 @@ constexpr int kMaxOrder = 62;       // per-point scratch arrays hold <= 64
 int set_cuda_error(cudaError_t e, const char* file, int line);
 int set_error(int code, const char* msg);
 const char* last_error();
+
+// Raise kernel K's dynamic shared-memory limit on the current device to at
+// least `bytes`, calling the runtime only when a larger size is first needed
+// (cudaFuncSetAttribute takes the driver's locks: issued before every
+// launch it serialised the host threads of concurrent solves).
+template <auto K>
+int ensure_smem(size_t bytes) {
+  static std::atomic<int> done[64];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+    cudaGetLastError();
+    dev = -1;
+  }
+  int cur = dev >= 0 ? done[dev].load(std::memory_order_relaxed) : 0;
+  if (dev >= 0 && (int)bytes <= cur) return 0;
+  WBFMM_CUDA(cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  if (dev >= 0)
+    while (cur < (int)bytes && !done[dev].compare_exchange_weak(cur, (int)bytes)) {
+    }
+  return 0;
+}
+// WBFMM_SMEM(bytes, kernel): ensure_smem, returning its status on failure
+// (the kernel last: its template arguments hold commas)
+#define WBFMM_SMEM(bytes, ...)                                            \
+  do {                                                                    \
+    const int rc_ = wbfmm::ensure_smem<__VA_ARGS__>((size_t)(bytes));     \
+    if (rc_) return rc_;                                                  \
+  } while (0)
 
 // ------------------------------------------------------------------ tree
 // *a = va and, when b is non-null, *b = vb (one thread, on stream s)

@@ -146,9 +146,7 @@ int launch_p2m(const P2MParams<T>& p, cudaStream_t s) {
   const size_t leg = leg_table_bytes<T>(p.N);
   size_t smem = leg + sizeof(T) * (size_t)nw * ncoef(p.N) * (HELM ? 2 : 1);
   if (smem > 48 * 1024)
-    WBFMM_CUDA(cudaFuncSetAttribute(k_p2m<T, HELM>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)smem));
+    WBFMM_SMEM(smem, k_p2m<T, HELM>);
   unsigned grid = (unsigned)((p.nbox + nw - 1) / nw);
   k_p2m<T, HELM><<<grid, nw * 32, smem, s>>>(p, leg ? 1 : 0);
   WBFMM_CUDA(cudaGetLastError());
@@ -384,18 +382,14 @@ int launch_m2l(const XlateParams<T>& p, const OpTables<T>& t, cudaStream_t s) {
   const int nw = pick_warps(per, extra, 4);
   const size_t smem = per * nw + extra;
   if (smem > 227 * 1024) return set_error(-3, "M2L: expansion order too large for shared memory");
-  WBFMM_CUDA(cudaFuncSetAttribute(k_m2l<T, HELM>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)smem));
+  WBFMM_SMEM(smem, k_m2l<T, HELM>);
   unsigned grid = (unsigned)(p.nbox * p.nsplit);
   k_m2l<T, HELM><<<grid, nw * 32, smem, s>>>(p, t);
   WBFMM_CUDA(cudaGetLastError());
   if (p.nsplit > 1) {
     size_t rs = sizeof(T) * 2 * vlen<HELM>(p.Nout);
     if (rs > 48 * 1024)
-      WBFMM_CUDA(cudaFuncSetAttribute(k_m2l_reduce<T, HELM>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)rs));
+      WBFMM_SMEM(rs, k_m2l_reduce<T, HELM>);
     k_m2l_reduce<T, HELM><<<(unsigned)p.nbox, 256, rs, s>>>(p);
     WBFMM_CUDA(cudaGetLastError());
   }
@@ -455,9 +449,7 @@ int launch_m2m(const XlateParams<T>& p, const OpTables<T>& t, cudaStream_t s) {
   const int nw = pick_warps(per, extra, 8);
   const size_t smem = per * nw + extra;
   if (smem > 227 * 1024) return set_error(-3, "M2M: expansion order too large for shared memory");
-  WBFMM_CUDA(cudaFuncSetAttribute(k_m2m<T, HELM>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)smem));
+  WBFMM_SMEM(smem, k_m2m<T, HELM>);
   k_m2m<T, HELM><<<(unsigned)p.nbox, nw * 32, smem, s>>>(p, t);
   WBFMM_CUDA(cudaGetLastError());
   return 0;
@@ -504,9 +496,7 @@ int launch_l2l(const XlateParams<T>& p, const OpTables<T>& t, cudaStream_t s) {
   const int nw = pick_warps(per, extra, 8);
   const size_t smem = per * nw + extra;
   if (smem > 227 * 1024) return set_error(-3, "L2L: expansion order too large for shared memory");
-  WBFMM_CUDA(cudaFuncSetAttribute(k_l2l<T, HELM>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)smem));
+  WBFMM_SMEM(smem, k_l2l<T, HELM>);
   k_l2l<T, HELM><<<(unsigned)p.nbox, nw * 32, smem, s>>>(p, t);
   WBFMM_CUDA(cudaGetLastError());
   return 0;
@@ -635,9 +625,7 @@ int launch_l2p(const EvalParams<T>& p, cudaStream_t s) {
   const size_t sm = l2p_table_bytes<T, HELM>(p.N);
   const size_t lg = leg_table_bytes<T>(p.N);
   if (sm + lg > 48 * 1024)
-    WBFMM_CUDA(cudaFuncSetAttribute(k_l2p<T, HELM>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)(sm + lg)));
+    WBFMM_SMEM((sm + lg), k_l2p<T, HELM>);
   k_l2p<T, HELM><<<(p.ntgt + 127) / 128, 128, sm + lg, s>>>(p, sm ? 1 : 0, lg ? 1 : 0);
   WBFMM_CUDA(cudaGetLastError());
   return 0;

@@ -668,9 +668,7 @@ template <typename T, bool HELM, int P>
 static int launch_lanes_P(const LanesParams<T>& p, const OpTables<T>& t,
                           cudaStream_t s) {
   typedef LaneSmem<T, HELM, P> SM;
-  WBFMM_CUDA(cudaFuncSetAttribute(k_m2l_lanes<T, HELM, P>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)SM::bytes));
+  WBFMM_SMEM(SM::bytes, k_m2l_lanes<T, HELM, P>);
   const int64_t np = (int64_t)1 << (3 * (p.level - 1));
   dim3 grid((unsigned)(8 * ((np + SM::CTA - 1) / SM::CTA)), 1, p.nsplit);
   k_m2l_lanes<T, HELM, P><<<grid, SM::CTA, SM::bytes, s>>>(p, t);

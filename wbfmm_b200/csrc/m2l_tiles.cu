@@ -440,9 +440,7 @@ int launch_m2l_tiles(const LanesParams<T>& p, const OpTables<T>& t,
   const int TC = pick_tc<T, HELM>(p.N);
   if (!TC) return set_error(-3, "M2L tiles: expansion order too large for shared memory");
   const TilePlan q = tile_plan<T, HELM>(p.N, TC);
-  WBFMM_CUDA(cudaFuncSetAttribute(k_m2l_tiles<T, HELM>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)q.total));
+  WBFMM_SMEM(q.total, k_m2l_tiles<T, HELM>);
   const int64_t np = (int64_t)1 << (3 * (p.level - 1));
   dim3 grid((unsigned)(8 * ((np + TC - 1) / TC)), 1, p.nsplit);
   k_m2l_tiles<T, HELM><<<grid, kTileThreads, q.total, s>>>(p, t, TC);

@@ -81,7 +81,8 @@ struct wbfmm_b200_server {
   };
 
   int device = 0;
-  int64_t budget = 0;
+  int64_t budget = 0;       // for the footprints of the solves in flight
+  int64_t keep = 0;         // work buffers a slot may keep between solves
   cudaMemPool_t pool = nullptr;   // the solves' device memory
   double epoch = 0;
   TableCache cache;
@@ -185,8 +186,16 @@ struct wbfmm_b200_server {
       cudaStreamSynchronize(s->stream);
       cudaGetLastError();
     }
-    if (s->s32) { s->s32->release_cache_refs(); s->s32->release_buffers(); }
-    if (s->s64) { s->s64->release_cache_refs(); s->s64->release_buffers(); }
+    // a slot keeps its work buffers for the next solve (no allocation then)
+    // while they stay within its allowance; a failed solve releases them
+    if (s->s32) {
+      s->s32->release_cache_refs();
+      if (rc || (int64_t)s->s32->buffer_bytes() > keep) s->s32->release_buffers();
+    }
+    if (s->s64) {
+      s->s64->release_cache_refs();
+      if (rc || (int64_t)s->s64->buffer_bytes() > keep) s->s64->release_buffers();
+    }
     return rc;
   }
 
@@ -251,7 +260,10 @@ int wbfmm_b200_server_create(wbfmm_b200_server_t** out, int nslots,
     delete srv;
     return set_error(WBFMM_B200_E_NOGPU, "no current CUDA device");
   }
-  srv->budget = hbm_budget;
+  // each slot may keep up to a quarter of its share of the budget (at most
+  // 4 GB) of work buffers between solves; admission counts the rest
+  srv->keep = std::min<int64_t>(hbm_budget / (4 * (int64_t)nslots), (int64_t)4 << 30);
+  srv->budget = hbm_budget - srv->keep * nslots;
   srv->epoch = now_s();
   // A pool of the server's own: freed memory stays cached (solves
   // reallocate cheaply) and is reused only once its free has completed, so

@@ -343,6 +343,13 @@ struct Solver : public wbfmm_b200_solver {
     return 0;
   }
 
+  // device bytes of the work buffers this solver owns
+  size_t buffer_bytes() {
+    size_t b = 0;
+    each_buf([&](auto& x) { if (x.owned && x.p) b += x.n * sizeof(*x.p); });
+    return b;
+  }
+
   // Served form: every work buffer back to the stream-ordered pool.
   void release_buffers() {
     each_buf([](auto& b) { if (b.owned) b.release(); });
