@@ -51,7 +51,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "FMM points/s + p99 latency: served FP32 vs plain FP64 GPU at rel-L2 err<=1e-6"
 WORKLOAD = "helmholtz_cube_1e6_k8_depth6"
-SERVE_SLOTS = 4
+SERVE_SLOTS = 6
 SERVE_BATCH = 256
 SERVE_LATENCY_REQUESTS = 384
 
