@@ -101,7 +101,10 @@ int wbfmm_b200_set_sources(wbfmm_b200_solver_t *s, int nsrc, const double *xs,
 int wbfmm_b200_set_strengths(wbfmm_b200_solver_t *s, const double *q,
                              int qstr, const double *dipoles, int dstr,
                              int on_device);
-/* Targets: xt[i*tstr + 0..2] (closed cube). */
+/* Targets: xt[i*tstr + 0..2] (closed cube).  Passing the array (same
+   pointer, stride and count) given to the last wbfmm_b200_set_sources makes
+   the sources the targets: their ordering is reused, so the array must not
+   have changed in between. */
 int wbfmm_b200_set_targets(wbfmm_b200_solver_t *s, int ntgt,
                            const double *xt, int tstr, int on_device);
 

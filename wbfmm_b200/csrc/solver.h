@@ -109,6 +109,16 @@ static __global__ void k_u64_to_u32(const uint64_t* __restrict__ a,
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) b[i] = (uint32_t)a[i];
 }
+// targets that are the sources: leaf box of each sorted source key
+static __global__ void k_leaf_of_keys(const uint64_t* __restrict__ keys, int shift,
+                                      uint64_t* __restrict__ tkeys,
+                                      uint32_t* __restrict__ tbox, int n) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint64_t b = keys[i] >> shift;
+  tkeys[i] = b;
+  tbox[i] = (uint32_t)b;
+}
 // box at `level` has targets below it
 static __global__ void k_target_mask(const uint32_t* __restrict__ leaf_count,
                               int depth, int level, uint8_t* __restrict__ mask) {
@@ -176,6 +186,8 @@ struct Solver : public wbfmm_b200_solver {
   int depth = 0, lmax = 0;
   // sources
   int nsrc = 0;
+  const double* src_arg = nullptr;  // the set_sources array (for targets = sources)
+  int src_arg_dev = 0;
   DBuf<double> pts_in, nrm_in;
   int xstr = 3, nstr = 3;
   DBuf<uint64_t> keys;
@@ -376,6 +388,7 @@ struct Solver : public wbfmm_b200_solver {
     if (normals && n_str < 3) return set_error(WBFMM_B200_E_ARG, "bad normal stride");
     cudaEventRecord(ev[0], stream);
     gen++;
+    src_arg = nullptr;              // set again only when these sources are in place
     nsrc = n;
     xstr = xs_str;
     const double* dpts = xs;
@@ -440,6 +453,8 @@ struct Solver : public wbfmm_b200_solver {
       WBFMM_TRY(mps[l].alloc(level_len(l, cfg.order_s[l]), cfg.managed != 0));
       WBFMM_TRY(mpr[l].alloc(level_len(l, cfg.order_r[l]), cfg.managed != 0));
     }
+    src_arg = xs;
+    src_arg_dev = on_device;
     cudaEventRecord(ev[1], stream);
     return 0;
   }
@@ -481,26 +496,40 @@ struct Solver : public wbfmm_b200_solver {
     if (n <= 0 || xt == nullptr || tstr < 3)
       return set_error(WBFMM_B200_E_ARG, "bad target points");
     ntgt = n;
-    const double* d = xt;
-    if (!on_device) {
-      WBFMM_TRY(tpts_in.alloc((size_t)n * tstr));
-      WBFMM_CUDA(cudaMemcpyAsync(tpts_in.p, xt, sizeof(double) * n * tstr,
-                                 cudaMemcpyHostToDevice, stream));
-      d = tpts_in.p;
-    }
     WBFMM_CUDA(cudaMemsetAsync(flag.p + 1, 0, sizeof(int), stream));
     WBFMM_TRY(tkeys.alloc(n)); WBFMM_TRY(tperm.alloc(n));
-    launch_target_keys(d, tstr, n, cfg.x0, cfg.D, depth, tkeys.p, tperm.p,
-                       flag.p + 1, stream);
-    WBFMM_TRY(radix_sort_pairs(tkeys.p, tperm.p, n, 3 * depth, &rs, stream));
     WBFMM_TRY(tx.alloc(n)); WBFMM_TRY(ty.alloc(n)); WBFMM_TRY(tz.alloc(n));
-    launch_gather_points(d, tstr, tperm.p, n, tx.p, ty.p, tz.p, stream);
     WBFMM_TRY(tbox.alloc(n));
-    k_u64_to_u32<<<(n + 255) / 256, 256, 0, stream>>>(tkeys.p, tbox.p, n);
+    if (xt == src_arg && on_device == src_arg_dev && tstr == xstr && n == nsrc) {
+      // the sources' array again: the source sort already groups the points
+      // by leaf box (the order inside a leaf changes no target's field), and
+      // the sources passed the domain check
+      WBFMM_CUDA(cudaMemcpyAsync(tperm.p, ip.p, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, stream));
+      WBFMM_CUDA(cudaMemcpyAsync(tx.p, sx.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream));
+      WBFMM_CUDA(cudaMemcpyAsync(ty.p, sy.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream));
+      WBFMM_CUDA(cudaMemcpyAsync(tz.p, sz.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream));
+      k_leaf_of_keys<<<(n + 255) / 256, 256, 0, stream>>>(keys.p, 60 - 3 * depth, tkeys.p,
+                                                         tbox.p, n);
+      launches++;
+    } else {
+      const double* d = xt;
+      if (!on_device) {
+        WBFMM_TRY(tpts_in.alloc((size_t)n * tstr));
+        WBFMM_CUDA(cudaMemcpyAsync(tpts_in.p, xt, sizeof(double) * n * tstr,
+                                   cudaMemcpyHostToDevice, stream));
+        d = tpts_in.p;
+      }
+      launch_target_keys(d, tstr, n, cfg.x0, cfg.D, depth, tkeys.p, tperm.p,
+                         flag.p + 1, stream);
+      WBFMM_TRY(radix_sort_pairs(tkeys.p, tperm.p, n, 3 * depth, &rs, stream));
+      launch_gather_points(d, tstr, tperm.p, n, tx.p, ty.p, tz.p, stream);
+      k_u64_to_u32<<<(n + 255) / 256, 256, 0, stream>>>(tkeys.p, tbox.p, n);
+      launches += 3 + 3 * ((3 * depth + 7) / 8);
+    }
     size_t nb = (size_t)1 << (3 * depth);
     WBFMM_TRY(tstart.alloc(nb)); WBFMM_TRY(tcount.alloc(nb));
     launch_box_ranges(tkeys.p, n, depth, tstart.p, tcount.p, stream);
-    launches += 4 + 3 * ((3 * depth + 7) / 8);
+    launches++;
     if (cfg.skip_empty) {
       for (int l = 2; l <= depth; l++) {
         size_t nbl = (size_t)1 << (3 * l);
