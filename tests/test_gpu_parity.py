@@ -408,3 +408,41 @@ def test_laplace_curl(gpu_lib, precision):
     ref = curl_from_gradients(g)
     tol = 2e-6 if precision == engine.FP64 else 5e-6
     assert rel_l2(curl.ravel(), ref.ravel()) < tol, rel_l2(curl.ravel(), ref.ravel())
+
+
+def _edge_problem(case):
+    rng = np.random.default_rng(71)
+    if case == "coincident":
+        # exact duplicates among the sources; targets on sources (excluded by
+        # the r > 1e-6 cutoff, src/wbfmm.h:36) and on duplicated sources
+        p = W.laplace_cube(3000, 600, depth=3, order=8, seed=72)
+        p.xs[100:200] = p.xs[0:100]
+        p.xt[:60] = p.xs[:60]
+        p.xt[60:90] = p.xs[130:160]
+    elif case == "faces":
+        # points within 1e-9 D of every face of the cube (strictly inside)
+        p = W.helmholtz_cube(4000, k=5.0, depth=3, seed=73)
+        p.xs = p.xs.copy()
+        for a in range(3):
+            p.xs[a * 200:(a * 200 + 100), a] = p.x0[a] + 1e-9 * p.D
+            p.xs[a * 200 + 100:(a + 1) * 200, a] = p.x0[a] + p.D * (1 - 1e-9)
+        p.xt = p.xs
+    elif case == "one_source":
+        p = W.laplace_cube(1, 40, depth=2, order=6, seed=74)
+        p.x0, p.D = np.array([-0.5, -0.5, -0.5]) - 0.01, 1.02
+    else:   # "sparse": 60 points in a depth-5 tree (most boxes empty)
+        p = W.helmholtz_cube(60, k=3.0, depth=5, seed=75)
+    return p
+
+
+@pytest.mark.parametrize("case", ["coincident", "faces", "one_source", "sparse"])
+def test_edge_cases_match_reference(gpu_lib, reference, case):
+    """Coincident points, points at the cube's faces, a single source and a
+    nearly empty tree: fields equal to the reference FMM's (FP64, 1e-10)."""
+    p = _edge_problem(case)
+    r = reference.fmm(p.problem, p.depth, p.order_s, p.order_r, p.x0, p.D, p.xs,
+                      p.q, p.xt, k=p.k, nthreads=os.cpu_count() or 1)
+    pot, grad = run(p)
+    assert np.all(np.isfinite(pot)) and np.all(np.isfinite(grad))
+    assert rel_l2(pot, r["pot"]) < TOL_FP64
+    assert rel_l2(grad, r["grad"]) < TOL_FP64
