@@ -156,6 +156,11 @@ gint wbfmm_tree_coefficient_clear(wbfmm_tree_t *t, guint l);
 gint wbfmm_tree_coefficients_zero(wbfmm_tree_t *t, guint level);
 guint64 wbfmm_point_box(wbfmm_tree_t *t, guint level, gdouble *x);
 guint64 wbfmm_point_index_3d(gdouble *x, gdouble *c, gdouble D);
+/* the tree's points in tree order, "i ip[i] x y z" per line (q, stride
+   unused, as in the reference) */
+gint wbfmm_tree_write_sources(wbfmm_tree_t *t,
+                              gdouble *q, gint stride,
+                              FILE *f);
 guint64 wbfmm_point_locate_box(guint64 x, guint level);
 gint wbfmm_point_from_index(guint64 i, guint32 *x, guint32 *y, guint32 *z);
 guint64 wbfmm_box_index(guint32 i, guint32 j, guint32 k);

@@ -86,9 +86,65 @@ def build_reference(force: bool = False) -> str | None:
     return out
 
 
+REPO = os.path.dirname(HERE)
+DRIVERS = ("wbfmm-tree-calc", "wbfmm-laplace-tree-calc")
+
+
+def _generate_driver(src_in: str, out: str) -> None:
+    """The reference's own generation step for its drivers (tools/make-source:
+    double precision names and formats)."""
+    text = open(src_in).read()
+    for a, b in (("WBFMM_REAL", "gdouble"), ("_FLOAT", ""), ("FLOATFMT", "lg"),
+                 ("FLOATEXP", "1.16e")):
+        text = text.replace(a, b)
+    with open(out, "w") as f:
+        f.write(text)
+
+
+def build_reference_drivers(force: bool = False) -> dict | None:
+    """The reference's command-line drivers (tools/wbfmm-tree-calc.c.in,
+    tools/wbfmm-laplace-tree-calc.c.in: text point files in, fields out),
+    built twice from the same unmodified source: linked with the reference
+    library (``<tool>-reference``) and with this repository's drop-in
+    ``include/wbfmm.h`` + ``libwbfmm_b200.so`` (``<tool>-b200``).  Outputs in
+    ``oracle/_ref``; None where neither the reference tree nor earlier builds
+    are present."""
+    tools_dir = os.path.join(REF_ROOT, "tools")
+    outs = {t: (os.path.join(REF_OUT, t + "-reference"), os.path.join(REF_OUT, t + "-b200"))
+            for t in DRIVERS}
+    if not os.path.isdir(tools_dir):
+        return outs if all(os.path.exists(b) for pair in outs.values() for b in pair) else None
+    ref_lib = build_reference(force)
+    b200_lib = os.path.join(REPO, "wbfmm_b200", "libwbfmm_b200.so")
+    if ref_lib is None or not os.path.exists(b200_lib):
+        return None
+    os.makedirs(BUILD_DIR, exist_ok=True)
+    shim = os.path.join(HERE, "shim", "glib_shim.c")
+    shim_o = os.path.join(BUILD_DIR, "glib_shim_driver.o")
+    if force or _newer(shim_o, [shim]):
+        _run(["gcc", "-O2", "-I", os.path.join(HERE, "shim"), "-c", shim, "-o", shim_o])
+    for t, (ref_bin, b200_bin) in outs.items():
+        src_in = os.path.join(tools_dir, t + ".c.in")
+        gen = os.path.join(BUILD_DIR, t + ".c")
+        if force or _newer(gen, [src_in, __file__]):
+            _generate_driver(src_in, gen)
+        common = ["-O2", "-DHAVE_CONFIG_H", gen]
+        if force or _newer(ref_bin, [gen, ref_lib]):
+            _run(["gcc", *common, "-fopenmp", "-I", os.path.join(HERE, "shim"), "-I", REF_ROOT,
+                  "-I", os.path.join(REF_ROOT, "src"), "-o", ref_bin, "-L", REF_OUT,
+                  "-lwbfmm_ref", "-Wl,-rpath,$ORIGIN", "-lm"])
+        if force or _newer(b200_bin, [gen, b200_lib, shim_o]):
+            _run(["gcc", *common, "-I", os.path.join(REPO, "include"), "-I",
+                  os.path.join(HERE, "shim"), "-I", REF_ROOT, shim_o, "-o", b200_bin,
+                  "-L", os.path.dirname(b200_lib), "-lwbfmm_b200",
+                  "-Wl,-rpath,$ORIGIN/../../wbfmm_b200", "-lm"])
+    return outs
+
+
 def main() -> None:
     print(build_restatement(force="--force" in sys.argv))
     print(build_reference(force="--force" in sys.argv))
+    print(build_reference_drivers(force="--force" in sys.argv))
 
 
 if __name__ == "__main__":

@@ -16,6 +16,7 @@ against the reference and the CPU restatement.
 """
 import ctypes as C
 import os
+import subprocess
 import sys
 
 import numpy as np
@@ -206,3 +207,61 @@ def test_dropin_client_matches_reference(gpu_lib, name):
             for kind in ("mps", "mpr"):
                 a, b = out[f"{kind}{l}"], ref[f"{kind}{l}"]
                 assert np.abs(a - b).max() <= TOL * np.abs(b).max(), (name, kind, l)
+
+
+DRIVER_CASES = [
+    ("wbfmm-tree-calc", ["-b", "-d", "3", "-k", "4", "-R", "8", "-S", "8"]),
+    ("wbfmm-tree-calc", ["-b", "-d", "3", "-k", "4", "-R", "8", "-S", "8", "-g"]),
+    ("wbfmm-tree-calc", ["-b", "-d", "3", "-k", "4", "-t", "1e-6"]),
+    ("wbfmm-laplace-tree-calc", ["-b", "-d", "3", "-R", "8", "-S", "8"]),
+    ("wbfmm-laplace-tree-calc", ["-b", "-d", "3", "-R", "8", "-S", "8", "-g"]),
+    ("wbfmm-laplace-tree-calc", ["-b", "-d", "3", "-R", "8", "-S", "8", "-l"]),
+]
+
+
+def _write_points(path, rows, nq, code):
+    with open(path, "w") as f:
+        f.write(f"{rows.shape[0]} {nq} {code}\n")
+        for r in rows:
+            f.write(" ".join("%.17g" % v for v in r) + "\n")
+
+
+def _read_fields(text):
+    return np.array([[float(v) for v in line.split()] for line in text.strip().splitlines()])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("tool,args", DRIVER_CASES, ids=lambda x: x if isinstance(x, str) else " ".join(x))
+def test_reference_driver_on_dropin(gpu_lib, tmp_path, tool, args):
+    """The reference's own command-line driver (unmodified source, its text
+    point files in and fields out), built once against the reference library
+    and once against this drop-in: the same output to 1e-10."""
+    ref_bin = os.path.join(ROOT, "oracle", "_ref", tool + "-reference")
+    b200_bin = os.path.join(ROOT, "oracle", "_ref", tool + "-b200")
+    if not (os.path.exists(ref_bin) and os.path.exists(b200_bin)):
+        pytest.skip("reference drivers not built (needs the reference sources)")
+    rng = np.random.default_rng(81)
+    n, nf = 3000, 200
+    xs = rng.uniform(-0.5, 0.5, (n, 3))
+    helm = tool == "wbfmm-tree-calc"
+    q = rng.standard_normal((n, 2 if helm else 1))
+    _write_points(tmp_path / "src.txt", np.hstack([xs, q]), q.shape[1], "M")
+    _write_points(tmp_path / "fld.txt", rng.uniform(-0.5, 0.5, (nf, 3)), 0, "F")
+    runs = [subprocess.run([b, "-s", str(tmp_path / "src.txt"), "-f", str(tmp_path / "fld.txt"),
+                            *args], capture_output=True, text=True, timeout=300,
+                           env=dict(os.environ, MALLOC_MMAP_THRESHOLD_=str(32 << 20)))
+            for b in (ref_bin, b200_bin)]
+    if helm and "-g" in args:
+        # the driver passes field stride 2 with the gradient field; the
+        # reference aborts on it (src/local.c:293-296), and so does the drop-in
+        for r in runs:
+            assert r.returncode != 0 and "too small for gradient" in r.stderr
+        return
+    for r in runs:
+        assert r.returncode == 0, r.stderr[-2000:]
+    outs = [_read_fields(r.stdout) for r in runs]
+    a, b = outs
+    assert a.shape == b.shape and a.shape[0] == nf
+    assert np.array_equal(a[:, :3], b[:, :3])
+    fa, fb = a[:, 3:], b[:, 3:]
+    assert np.linalg.norm(fb - fa) <= 1e-10 * np.linalg.norm(fa)

@@ -403,6 +403,19 @@ gint wbfmm_points_origin_width(gdouble *x, gint str, gint n, gdouble *xmin,
 }
 
 /* Gumerov & Duraiswami (2009) truncation rule, as src/util.c:474-503 */
+/* src/util.c:425-450: the points in tree order (q and stride unused) */
+gint wbfmm_tree_write_sources(wbfmm_tree_t *t, gdouble *q, gint stride, FILE *f)
+{
+  guint i;
+  (void)q; (void)stride;
+  for (i = 0; i < t->npoints; i++) {
+    const guint idx = t->ip[i];
+    const gdouble *x = (const gdouble *)(t->points + (gsize)idx * t->pstr);
+    fprintf(f, "%u %u %g %g %g\n", i, idx, x[0], x[1], x[2]);
+  }
+  return 0;
+}
+
 gint wbfmm_truncation_number(wbfmm_tree_t *t, gdouble k, guint level,
                              gdouble tol) {
   const double del = 2.0;
