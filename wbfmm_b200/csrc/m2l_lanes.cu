@@ -125,9 +125,10 @@ struct LaneDims {
   static constexpr int NL = (P + 1) * (P + 1) * (P + 1);       // Laplace S|R
 };
 
-
 // whether a lane keeps its working vector in registers (about 100 of them at
 // most); otherwise it is a shared-memory column like the accumulator
+// (WBFMM_LANES_NO_REGISTER_VECTOR builds every order the second way, to
+// compare the two)
 template <typename T, bool HELM, int P>
 struct LaneReg {
   static constexpr int V = HELM ? LaneDims<P>::VF : LaneDims<P>::VH;
