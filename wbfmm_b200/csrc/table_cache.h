@@ -17,6 +17,7 @@
 
 #include <algorithm>
 #include <map>
+#include <condition_variable>
 #include <mutex>
 #include <tuple>
 #include <vector>
@@ -86,10 +87,12 @@ struct TableCache {
     cudaEvent_t ready = nullptr;
     int refs = 0;
     uint64_t last = 0;
+    int state = 1;               // 0 being built, 1 ready, -1 build failed
   };
   using Key = std::tuple<int, uint64_t, int>;
 
   std::mutex mu;
+  std::condition_variable built;  // a coaxial entry left the "being built" state
   cudaMemPool_t pool = nullptr;   // stream-ordered allocations when set
   std::vector<Geo*> geos;
   std::map<Key, Coax*> coax;
@@ -118,15 +121,19 @@ struct TableCache {
   // frees stream-ordered on s when given (the entry is unreferenced, so no
   // queued work reads it), else synchronously
   void drop(Coax* c, cudaStream_t s) {
+    free_tables(c, s);
+    delete c;
+  }
+  void free_tables(Coax* c, cudaStream_t s) {
     if (s) {
-      cudaFreeAsync(c->d64, s);
-      cudaFreeAsync(c->d32, s);
+      if (c->d64) cudaFreeAsync(c->d64, s);
+      if (c->d32) cudaFreeAsync(c->d32, s);
     } else {
       cudaFree(c->d64);
       cudaFree(c->d32);
     }
     if (c->ready) cudaEventDestroy(c->ready);
-    delete c;
+    c->d64 = nullptr; c->d32 = nullptr; c->ready = nullptr;
   }
 
   template <typename X>
@@ -235,22 +242,45 @@ struct TableCache {
   // Helmholtz coaxial table: kind 0 = (S|R) at the 15 list-4 distances
   // k w sqrt(d2) (complex, stride 2 (coax_count(L) + 1) per distance);
   // kind 1 = (R|R) at k w sqrt(3)/2 (real).  Returns a referenced entry.
+  // The (kind, k w, L) coaxial table, shared: a hit waits (on the stream)
+  // for the table's build; a miss builds it outside the cache's lock, so
+  // solves building different tables (every Helmholtz request of a served
+  // stream has its own k) do not queue behind each other.
   template <typename T>
   int coaxial(int kind, double kw, int L, cudaStream_t s, const T** out,
               Coax** ref) {
     uint64_t bits;
     memcpy(&bits, &kw, sizeof(bits));
     Key key(kind, bits, L);
-    std::lock_guard<std::mutex> lk(mu);
+    std::unique_lock<std::mutex> lk(mu);
     Coax* c = nullptr;
     auto it = coax.find(key);
     if (it != coax.end()) {
       c = it->second;
       hits++;
-      WBFMM_CUDA(cudaStreamWaitEvent(s, c->ready, 0));
+      c->refs++;
+      c->last = ++tick;
+      built.wait(lk, [c] { return c->state != 0; });
+      if (c->state < 0) {
+        if (--c->refs == 0) delete c;
+        return set_error(WBFMM_B200_E_NOMEM, "coaxial table build failed");
+      }
+      cudaEvent_t ev = c->ready;
+      lk.unlock();
+      const cudaError_t e = cudaStreamWaitEvent(s, ev, 0);
+      if (e != cudaSuccess) {
+        lk.lock();
+        c->refs--;
+        return set_cuda_error(e, __FILE__, __LINE__);
+      }
     } else {
       misses++;
       c = new Coax();
+      c->state = 0;
+      c->refs = 1;
+      c->last = ++tick;
+      coax[key] = c;
+      lk.unlock();
       const int64_t per = (int64_t)(L + 1) * (L + 2) * (L + 3) / 6 + 1;
       std::vector<double> krs;
       int nc;
@@ -270,13 +300,20 @@ struct TableCache {
       if (!rc) e = cudaEventCreateWithFlags(&c->ready, cudaEventDisableTiming);
       if (!rc && e == cudaSuccess) e = cudaEventRecord(c->ready, s);
       if (!rc && e != cudaSuccess) rc = set_cuda_error(e, __FILE__, __LINE__);
-      if (rc) { drop(c, s); return rc; }
-      coax[key] = c;
+      lk.lock();
+      if (rc) {
+        coax.erase(key);
+        free_tables(c, s);
+        c->state = -1;
+        built.notify_all();
+        if (--c->refs == 0) delete c;    // else the last waiter deletes it
+        return rc;
+      }
+      c->state = 1;
       coax_bytes += (size_t)c->count * 12;
+      built.notify_all();
+      evict(s);
     }
-    c->refs++;
-    c->last = ++tick;
-    evict(s);
     *out = sizeof(T) == 4 ? (const T*)c->d32 : (const T*)c->d64;
     *ref = c;
     return 0;
