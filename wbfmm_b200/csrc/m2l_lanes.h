@@ -24,6 +24,7 @@ struct LanesParams {
   const uint8_t* tmask; // targets to compute, or null for all
   int lap_e;            // Laplace: degree l of lin_raw is scaled by 2^(lap_e l)
   const void* lapsr;    // Laplace: [kNumOps][(P+1)^3] scaled S|R per shift (build_lap_sr_ops)
+  const void* hcx;      // Helmholtz tiles: the level's coaxial rows (build_helm_coax_rows)
   const int* act;       // sparse targets: [8][np] parents per child type, or null
   const int* act_n;     // [8] list lengths (device)
   void* partial_raw;    // [nsplit][8][V][np] complex when nsplit > 1
@@ -70,9 +71,16 @@ bool tiles_supported(int Ns, int Nr);
 template <typename T, bool HELM>
 int launch_m2l_tiles(const LanesParams<T>& p, const OpTables<T>& t,
                      cudaStream_t s);
-// targets per CTA of the tile kernel at order N (0: unsupported)
+// targets per CTA of the tile kernel at order N (0: unsupported); *dense
+// (if given): whether it reads the level's Helmholtz coaxial rows
 template <typename T, bool HELM>
-int tiles_per_cta(int N);
+int tiles_per_cta(int N, bool* dense = nullptr);
+// the tile kernel's Helmholtz coaxial rows of a level (15 distances, rows
+// of (S|R) pairs with signs folded in) from its (S|R) table, into
+// helm_coax_rows_count(P) values
+template <typename T>
+int build_helm_coax_rows(const T* raw, int64_t raw_stride, int P, T* out, cudaStream_t s);
+size_t helm_coax_rows_count(int P);
 template <typename T, bool HELM>
 int lanes_to_lin(const T* arr, int level, int N, int lap_e, void* lin, cudaStream_t s);
 size_t lanes_lin_bytes(int level, int N, bool helm, size_t tsize);

@@ -209,6 +209,7 @@ struct Solver : public wbfmm_b200_solver {
   DBuf<uint8_t> tmask[kMaxDepth + 1];
   DBuf<int> act[kMaxDepth + 1], act_n[kMaxDepth + 1], act_scr;   // M2L target lists
   DBuf<T> lapsr;                    // Laplace lane M2L: scaled operators of the level
+  DBuf<T> hcx;                      // Helmholtz tile M2L: coaxial rows of the level
   DBuf<int> flag;
   // outputs (original order)
   DBuf<T> pot, grad;
@@ -275,7 +276,7 @@ struct Solver : public wbfmm_b200_solver {
     f(tstart); f(tcount); f(flag); f(pot); f(grad); f(out64);
     f(H64); f(H); f(op_ith); f(op_dist); f(op_r); f(op_ph); f(op_ch);
     for (int i = 0; i < 3; i++) { f(lap64[i]); f(lap[i]); }
-    f(partial); f(lin); f(lanes_part); f(act_scr); f(lapsr);
+    f(partial); f(lin); f(lanes_part); f(act_scr); f(lapsr); f(hcx);
   }
 
   ~Solver() override {
@@ -767,8 +768,15 @@ struct Solver : public wbfmm_b200_solver {
         lp.lapsr = lapsr.p;
         launches++;
       }
+      bool dense = false;
+      const int tc = helm ? tiles_per_cta<T, true>(x.Nin, &dense) : tiles_per_cta<T, false>(x.Nin);
+      if (dense) {
+        WBFMM_TRY(hcx.alloc(helm_coax_rows_count(x.Nin)));
+        WBFMM_TRY(build_helm_coax_rows<T>(x.coax, x.coax_stride, x.Nin, hcx.p, stream));
+        lp.hcx = hcx.p;
+        launches++;
+      }
       const int64_t np = (int64_t)1 << (3 * (level - 1));
-      const int tc = helm ? tiles_per_cta<T, true>(x.Nin) : tiles_per_cta<T, false>(x.Nin);
       const int64_t ctas = ((np + tc - 1) / tc) * 8;
       int ns = 1;
       while (ctas * ns < 2 * 148 && ns < 32) ns *= 2;
