@@ -294,8 +294,9 @@ k_m2l_lanes(LanesParams<T> p, OpTables<T> t) {
     const T* sech = ops + SM::off_ech;
     const T* scx = ops + SM::off_cx;
     if (!active) continue;
-    const T2* src = (const T2*)p.lin_raw + (int64_t)sg * V * npp + pp + ddx +
-                    npx * ((int64_t)ddy + npx * (int64_t)ddz);
+    const int64_t spp = pp + ddx + npx * ((int64_t)ddy + npx * (int64_t)ddz);
+    if (p.smask && !p.smask[(int64_t)sg * npp + spp]) continue;   // no sources there
+    const T2* src = (const T2*)p.lin_raw + (int64_t)sg * V * npp + spp;
     if (HELM) {
       // stage A: copy the source into the lane's column with e^{i m ch}
 #pragma unroll
@@ -655,6 +656,34 @@ int lanes_to_lin(const T* arr, int level, int N, int lap_e, void* lin, cudaStrea
   const int64_t tot = nx * nx * nx * V * 8;
   k_to_lin<T, HELM><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(arr, level, N, lap_e,
                                                                    (T2*)lin);
+  WBFMM_CUDA(cudaGetLastError());
+  return 0;
+}
+
+__global__ void k_source_mask(const uint32_t* __restrict__ src_n, int nx, int64_t npp,
+                              uint8_t* __restrict__ smask) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= 8 * npp) return;
+  const int sg = (int)(e / npp);
+  const int64_t pp = e - sg * npp;
+  const int npx = nx + 2;
+  const int px = (int)(pp % npx) - 1, py = (int)((pp / npx) % npx) - 1,
+            pz = (int)(pp / ((int64_t)npx * npx)) - 1;
+  uint8_t f = 0;
+  if (px >= 0 && px < nx && py >= 0 && py < nx && pz >= 0 && pz < nx)
+    f = src_n[((int64_t)morton(px, py, pz) << 3) | sg] != 0;
+  smask[e] = f;
+}
+
+size_t source_mask_bytes(int level) {
+  const size_t npx = (1u << (level - 1)) + 2;
+  return 8 * npx * npx * npx;
+}
+
+int build_source_mask(const uint32_t* src_n, int level, uint8_t* smask, cudaStream_t s) {
+  const int nx = 1 << (level - 1);
+  const int64_t npp = (int64_t)(nx + 2) * (nx + 2) * (nx + 2);
+  k_source_mask<<<(unsigned)((8 * npp + 255) / 256), 256, 0, s>>>(src_n, nx, npp, smask);
   WBFMM_CUDA(cudaGetLastError());
   return 0;
 }

@@ -27,6 +27,7 @@ struct LanesParams {
   const void* hcx;      // Helmholtz tiles: the level's coaxial rows (build_helm_coax_rows)
   const int* act;       // sparse targets: [8][np] parents per child type, or null
   const int* act_n;     // [8] list lengths (device)
+  const uint8_t* smask; // [8][padded grid]: source box holds sources, or null (all)
   void* partial_raw;    // [nsplit][8][V][np] complex when nsplit > 1
 };
 
@@ -81,6 +82,10 @@ int tiles_per_cta(int N, bool* dense = nullptr);
 template <typename T>
 int build_helm_coax_rows(const T* raw, int64_t raw_stride, int P, T* out, cudaStream_t s);
 size_t helm_coax_rows_count(int P);
+// smask[sg][padded parent] = the level's box of child type sg under that
+// parent holds sources (0 on the padding), from the level's box counts
+int build_source_mask(const uint32_t* src_n, int level, uint8_t* smask, cudaStream_t s);
+size_t source_mask_bytes(int level);
 template <typename T, bool HELM>
 int lanes_to_lin(const T* arr, int level, int N, int lap_e, void* lin, cudaStream_t s);
 size_t lanes_lin_bytes(int level, int N, bool helm, size_t tsize);

@@ -231,7 +231,11 @@ k_m2l_tiles(LanesParams<T> p, OpTables<T> t, int TC, bool dense) {
     const int ddx = ((code >> 12) & 3) - 1, ddy = ((code >> 14) & 3) - 1,
               ddz = ((code >> 16) & 3) - 1;
     const int64_t doff = ddx + npx * ((int64_t)ddy + npx * (int64_t)ddz);
-    __syncthreads();   // the previous offset's operator and vectors are free
+    // the previous offset's operator and vectors are free; an offset whose
+    // sources are all empty boxes adds nothing (the decision is the CTA's)
+    int any = 1;
+    if (p.smask) any = tid < TC && s_act[tid] && p.smask[(int64_t)sg * npp + s_pp[tid] + doff];
+    if (!__syncthreads_or(any)) continue;
     {
       const T* H = t.H + (int64_t)t.op_ith[op] * t.hstride;
       for (int i = tid; i < q.NH; i += kTileThreads) sH[i] = H[i];
@@ -281,11 +285,25 @@ k_m2l_tiles(LanesParams<T> p, OpTables<T> t, int TC, bool dense) {
 #pragma unroll
       for (int k = 0; k < 4; k++) { a0[k].x = a0[k].y = a1[k].x = a1[k].y = T(0); }
       if (HELM) {
-        for (int m = -n; m <= n; m++) {
-          const T2* xr = X + (size_t)cidx(n, m) * TC + t0;
-          const T h0 = m >= 0 ? sH[hb + (nu0 + n) * (n + 1) + m] : sH[hb + (-nu0 + n) * (n + 1) - m];
-          const T h1 = !two ? T(0) : m >= 0 ? sH[hb + (nu0 + 1 + n) * (n + 1) + m]
-                                            : sH[hb + (-nu0 - 1 + n) * (n + 1) - m];
+        // rows nu0 and nu0 + 1 of the half-stored matrix: H(nu, m) for
+        // m >= 0, H(-nu, -m) for m < 0, as two loops (without a second row,
+        // a1 is not stored and reads the first row again)
+        const T* rp0 = sH + hb + (nu0 + n) * (n + 1);
+        const T* rn0 = sH + hb + (-nu0 + n) * (n + 1);
+        const T* rp1 = two ? rp0 + (n + 1) : rp0;
+        const T* rn1 = two ? rn0 - (n + 1) : rn0;
+        const T2* xr = X + (size_t)cidx(n, -n) * TC + t0;
+        for (int m = n; m > 0; m--, xr += TC) {
+          const T h0 = rn0[m], h1 = rn1[m];
+#pragma unroll
+          for (int k = 0; k < 4; k++) {
+            const T2 x = xr[k];
+            a0[k].x += h0 * x.x; a0[k].y += h0 * x.y;
+            a1[k].x += h1 * x.x; a1[k].y += h1 * x.y;
+          }
+        }
+        for (int m = 0; m <= n; m++, xr += TC) {
+          const T h0 = rp0[m], h1 = rp1[m];
 #pragma unroll
           for (int k = 0; k < 4; k++) {
             const T2 x = xr[k];
@@ -404,11 +422,25 @@ k_m2l_tiles(LanesParams<T> p, OpTables<T> t, int TC, bool dense) {
 #pragma unroll
       for (int k = 0; k < 4; k++) { a0[k].x = a0[k].y = a1[k].x = a1[k].y = T(0); }
       if (HELM) {
-        for (int m = -n; m <= n; m++) {
-          const T2* xr = X + (size_t)cidx(n, m) * TC + t0;
-          const T h0 = m >= 0 ? sH[hb + (nu0 + n) * (n + 1) + m] : sH[hb + (-nu0 + n) * (n + 1) - m];
-          const T h1 = !two ? T(0) : m >= 0 ? sH[hb + (nu0 + 1 + n) * (n + 1) + m]
-                                            : sH[hb + (-nu0 - 1 + n) * (n + 1) - m];
+        // rows nu0 and nu0 + 1 of the half-stored matrix: H(nu, m) for
+        // m >= 0, H(-nu, -m) for m < 0, as two loops (without a second row,
+        // a1 is not stored and reads the first row again)
+        const T* rp0 = sH + hb + (nu0 + n) * (n + 1);
+        const T* rn0 = sH + hb + (-nu0 + n) * (n + 1);
+        const T* rp1 = two ? rp0 + (n + 1) : rp0;
+        const T* rn1 = two ? rn0 - (n + 1) : rn0;
+        const T2* xr = X + (size_t)cidx(n, -n) * TC + t0;
+        for (int m = n; m > 0; m--, xr += TC) {
+          const T h0 = rn0[m], h1 = rn1[m];
+#pragma unroll
+          for (int k = 0; k < 4; k++) {
+            const T2 x = xr[k];
+            a0[k].x += h0 * x.x; a0[k].y += h0 * x.y;
+            a1[k].x += h1 * x.x; a1[k].y += h1 * x.y;
+          }
+        }
+        for (int m = 0; m <= n; m++, xr += TC) {
+          const T h0 = rp0[m], h1 = rp1[m];
 #pragma unroll
           for (int k = 0; k < 4; k++) {
             const T2 x = xr[k];

@@ -208,6 +208,7 @@ struct Solver : public wbfmm_b200_solver {
   DBuf<uint32_t> tperm, tbox, tstart, tcount;
   DBuf<uint8_t> tmask[kMaxDepth + 1];
   DBuf<int> act[kMaxDepth + 1], act_n[kMaxDepth + 1], act_scr;   // M2L target lists
+  DBuf<uint8_t> smask;              // M2L skip_empty: source boxes of the level holding sources
   DBuf<T> lapsr;                    // Laplace lane M2L: scaled operators of the level
   DBuf<T> hcx;                      // Helmholtz tile M2L: coaxial rows of the level
   DBuf<int> flag;
@@ -276,7 +277,7 @@ struct Solver : public wbfmm_b200_solver {
     f(tstart); f(tcount); f(flag); f(pot); f(grad); f(out64);
     f(H64); f(H); f(op_ith); f(op_dist); f(op_r); f(op_ph); f(op_ch);
     for (int i = 0; i < 3; i++) { f(lap64[i]); f(lap[i]); }
-    f(partial); f(lin); f(lanes_part); f(act_scr); f(lapsr); f(hcx);
+    f(partial); f(lin); f(lanes_part); f(act_scr); f(lapsr); f(hcx); f(smask);
   }
 
   ~Solver() override {
@@ -761,6 +762,12 @@ struct Solver : public wbfmm_b200_solver {
       lp.coax = x.coax; lp.coax_stride = x.coax_stride;
       lp.width = x.width; lp.tmask = x.tmask; lp.lap_e = x.lap_e;
       if (x.tmask && act[level].p) { lp.act = act[level].p; lp.act_n = act_n[level].p; }
+      if (x.tmask) {
+        WBFMM_TRY(smask.alloc(source_mask_bytes(level)));
+        WBFMM_TRY(build_source_mask(x.src_n, level, smask.p, stream));
+        lp.smask = smask.p;
+        launches++;
+      }
       if (!helm) {
         const int P1 = x.Nin + 1;
         WBFMM_TRY(lapsr.alloc((size_t)kNumOps * P1 * P1 * P1));
@@ -802,6 +809,12 @@ struct Solver : public wbfmm_b200_solver {
       lp.coax = x.coax; lp.coax_stride = x.coax_stride;
       lp.width = x.width; lp.tmask = x.tmask; lp.lap_e = x.lap_e;
       if (x.tmask && act[level].p) { lp.act = act[level].p; lp.act_n = act_n[level].p; }
+      if (x.tmask) {
+        WBFMM_TRY(smask.alloc(source_mask_bytes(level)));
+        WBFMM_TRY(build_source_mask(x.src_n, level, smask.p, stream));
+        lp.smask = smask.p;
+        launches++;
+      }
       if (!helm) {
         const int P1 = x.Nin + 1;
         WBFMM_TRY(lapsr.alloc((size_t)kNumOps * P1 * P1 * P1));
