@@ -50,7 +50,7 @@ static int ensure_offsets() {
 // Layout L level array -> lin[tau][c][pp] (complex), pp on the padded
 // parent grid (nx+2)^3; the halo must be zero beforehand
 template <typename T, bool HELM>
-__global__ void k_to_lin(const T* __restrict__ arr, int level, int N, int lap_e,
+__global__ void k_to_lin(const T* __restrict__ arr, int level, int N, int lap_e, bool boxmajor,
                          typename V2t<T>::t* __restrict__ lin) {
   typedef typename V2t<T>::t T2;
   const int V = HELM ? (N + 1) * (N + 1) : (N + 1) * (N + 2) / 2;
@@ -82,7 +82,8 @@ __global__ void k_to_lin(const T* __restrict__ arr, int level, int N, int lap_e,
     v.x = scale2(v.x, lap_e * n);
     v.y = scale2(v.y, lap_e * n);
   }
-  lin[((int64_t)tau * V + c) * npp + pp] = v;
+  if (boxmajor) lin[((int64_t)tau * npp + pp) * V + c] = v;
+  else lin[((int64_t)tau * V + c) * npp + pp] = v;
 }
 
 // --------------------------------------------------------------- kernel
@@ -296,7 +297,10 @@ k_m2l_lanes(LanesParams<T> p, OpTables<T> t) {
     if (!active) continue;
     const int64_t spp = pp + ddx + npx * ((int64_t)ddy + npx * (int64_t)ddz);
     if (p.smask && !p.smask[(int64_t)sg * npp + spp]) continue;   // no sources there
-    const T2* src = (const T2*)p.lin_raw + (int64_t)sg * V * npp + spp;
+    // a target list's lanes hold boxes that are not neighbours: each reads
+    // its source's coefficients contiguously there (box-major copy)
+    const int64_t cs = p.boxmajor ? 1 : npp;
+    const T2* src = (const T2*)p.lin_raw + (int64_t)sg * V * npp + (p.boxmajor ? spp * V : spp);
     if (HELM) {
       // stage A: copy the source into the lane's column with e^{i m ch}
 #pragma unroll
@@ -304,7 +308,7 @@ k_m2l_lanes(LanesParams<T> p, OpTables<T> t) {
 #pragma unroll
         for (int m = -n; m <= n; m++) {
           const int am = m < 0 ? -m : m;
-          T2 v = __ldg(src + (int64_t)cidx(n, m) * npp);
+          T2 v = __ldg(src + (int64_t)cidx(n, m) * cs);
           w[cidx(n, m)] = cm(v, sech[2 * am], m < 0 ? -sech[2 * am + 1] : sech[2 * am + 1]);
         }
         cfence();
@@ -387,7 +391,7 @@ k_m2l_lanes(LanesParams<T> p, OpTables<T> t) {
       for (int n = 0; n <= P; n++) {
 #pragma unroll
         for (int m = 0; m <= n; m++) {
-          T2 v = __ldg(src + (int64_t)hidx(n, m) * npp);
+          T2 v = __ldg(src + (int64_t)hidx(n, m) * cs);
           w[hidx(n, m)] = cm(v, sech[2 * m], sech[2 * m + 1]);
         }
         cfence();
@@ -648,14 +652,15 @@ int launch_lanes_reduce(const LanesParams<T>& p, cudaStream_t s) {
 }
 
 template <typename T, bool HELM>
-int lanes_to_lin(const T* arr, int level, int N, int lap_e, void* lin, cudaStream_t s) {
+int lanes_to_lin(const T* arr, int level, int N, int lap_e, void* lin, cudaStream_t s,
+                 bool boxmajor) {
   typedef typename V2t<T>::t T2;
   const int V = HELM ? (N + 1) * (N + 1) : (N + 1) * (N + 2) / 2;
   const int64_t nx = 1 << (level - 1), npx = nx + 2;
   WBFMM_CUDA(cudaMemsetAsync(lin, 0, sizeof(T2) * 8 * V * npx * npx * npx, s));
   const int64_t tot = nx * nx * nx * V * 8;
   k_to_lin<T, HELM><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(arr, level, N, lap_e,
-                                                                   (T2*)lin);
+                                                                   boxmajor, (T2*)lin);
   WBFMM_CUDA(cudaGetLastError());
   return 0;
 }
@@ -764,7 +769,7 @@ int launch_m2l_lanes(const LanesParams<T>& p, const OpTables<T>& t,
 }
 
 #define WBFMM_LANES_INST(T, H)                                                   \
-  template int lanes_to_lin<T, H>(const T*, int, int, int, void*, cudaStream_t); \
+  template int lanes_to_lin<T, H>(const T*, int, int, int, void*, cudaStream_t, bool); \
   template int launch_lanes_reduce<T, H>(const LanesParams<T>&, cudaStream_t);   \
   template bool lanes_supported<T, H>(int, int);                                 \
   template int launch_m2l_lanes<T, H>(const LanesParams<T>&, const OpTables<T>&, \

@@ -28,6 +28,7 @@ struct LanesParams {
   const int* act;       // sparse targets: [8][np] parents per child type, or null
   const int* act_n;     // [8] list lengths (device)
   const uint8_t* smask; // [8][padded grid]: source box holds sources, or null (all)
+  int boxmajor;         // lin_raw is [8][padded grid][V] (lanes_to_lin), not [8][V][grid]
   void* partial_raw;    // [nsplit][8][V][np] complex when nsplit > 1
 };
 
@@ -87,7 +88,8 @@ size_t helm_coax_rows_count(int P);
 int build_source_mask(const uint32_t* src_n, int level, uint8_t* smask, cudaStream_t s);
 size_t source_mask_bytes(int level);
 template <typename T, bool HELM>
-int lanes_to_lin(const T* arr, int level, int N, int lap_e, void* lin, cudaStream_t s);
+int lanes_to_lin(const T* arr, int level, int N, int lap_e, void* lin, cudaStream_t s,
+                 bool boxmajor = false);
 size_t lanes_lin_bytes(int level, int N, bool helm, size_t tsize);
 
 // Active-target lists of a level for the lane and tile M2L: for each child

@@ -799,11 +799,15 @@ struct Solver : public wbfmm_b200_solver {
     }
     if (use_lanes) {
       // lane-per-pair kernel on a transposed copy of the singular expansions
+      // (box-major for target lists)
+      const bool boxmajor = x.tmask && act[level].p;
       WBFMM_TRY(lin.alloc(lanes_lin_bytes(level, x.Nin, helm, sizeof(T))));
-      WBFMM_TRY((helm ? lanes_to_lin<T, true>(x.cin, level, x.Nin, 0, lin.p, stream)
-                      : lanes_to_lin<T, false>(x.cin, level, x.Nin, x.lap_e, lin.p, stream)));
+      WBFMM_TRY((helm ? lanes_to_lin<T, true>(x.cin, level, x.Nin, 0, lin.p, stream, boxmajor)
+                      : lanes_to_lin<T, false>(x.cin, level, x.Nin, x.lap_e, lin.p, stream,
+                                               boxmajor)));
       LanesParams<T> lp;
       memset(&lp, 0, sizeof(lp));
+      lp.boxmajor = boxmajor;
       lp.level = level; lp.N = x.Nin;
       lp.lin_raw = lin.p; lp.cout = x.cout;
       lp.coax = x.coax; lp.coax_stride = x.coax_stride;
