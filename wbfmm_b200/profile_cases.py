@@ -14,6 +14,10 @@ steady-state launch.  Cases:
   m2l_lanes_helmholtz_p6    Helmholtz k = 8, 1e6 points, depth 6, the
                             benchmark's orders, FP32: M2L of level 6
                             (lane-per-pair kernel)
+  m2l_lanes_laplace_clusters_p10
+                            Laplace, 2e6 points in 8 Gaussian clusters,
+                            depth 7, order 10, skip_empty, FP32: M2L of
+                            level 7 (lane kernel on target lists)
   p2p_helmholtz             Helmholtz k = 10, 2e5 points, depth 4, FP32:
                             evaluation (L2P + P2P)
   served_stream             48 requests of the serving stream through a
@@ -31,8 +35,8 @@ from . import engine as E
 from . import workloads as W
 
 
-def _solve_then(p, precision, stage):
-    cfg = E.SolverConfig.from_problem(p, precision)
+def _solve_then(p, precision, stage, skip_empty=False):
+    cfg = E.SolverConfig.from_problem(p, precision, skip_empty=skip_empty)
     with E.Solver(cfg) as s:
         s.set_sources(p.xs, p.normals).set_strengths(p.q, p.dipoles).set_targets(p.xt).run()
         stage(s)
@@ -61,6 +65,9 @@ def main(case: str) -> None:
     elif case == "m2l_lanes_helmholtz_p6":
         p = W.helmholtz_cube(1_000_000, k=8.0, depth=6, seed=2)
         _solve_then(p, E.FP32, lambda s: s.m2l(6))
+    elif case == "m2l_lanes_laplace_clusters_p10":
+        p = W.laplace_clusters(2_000_000, depth=7, order=10, seed=5)
+        _solve_then(p, E.FP32, lambda s: s.m2l(7), skip_empty=True)
     elif case == "p2p_helmholtz":
         p = _cube(E.HELMHOLTZ, 200_000, 4, 8, k=10.0)
         _solve_then(p, E.FP32, lambda s: s.evaluate())
