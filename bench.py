@@ -74,18 +74,41 @@ def list4_pairs(depth: int) -> list[int]:
     return out
 
 
-def list4_pairs_at(xt, x0, D, level: int) -> int:
-    """(target box, list-4 source) pairs of the boxes at `level` that hold
-    one of the points xt (the M2L work of a skip_empty solve)."""
+def list4_pairs_at(xt, x0, D, level: int, xs=None) -> int:
+    """(target box, list-4 source box) pairs of the boxes at `level` that hold
+    one of the points xt, counting only source boxes that hold one of the
+    points xs when given (the M2L work of a skip_empty solve, whose kernels
+    skip empty source boxes)."""
     n = 1 << level
-    ijk = np.floor((np.asarray(xt) - np.asarray(x0)) / (D / n)).astype(np.int64)
-    ijk = np.unique(np.clip(ijk, 0, n - 1), axis=0)
+
+    def boxes(pts):
+        ijk = np.floor((np.asarray(pts) - np.asarray(x0)) / (D / n)).astype(np.int64)
+        return np.unique(np.clip(ijk, 0, n - 1), axis=0)
+
+    ijk = boxes(xt)
     i0 = ijk - ijk % 2
     i1 = np.minimum(i0 + 3, n - 1)
     lo = np.where(i0 > 0, i0 - 2, i0)
-    span = i1 - lo + 1
-    near = np.minimum(ijk + 1, n - 1) - np.maximum(ijk - 1, 0) + 1
-    return int((span.prod(axis=1) - near.prod(axis=1)).sum())
+    nlo = np.maximum(ijk - 1, 0)
+    nhi = np.minimum(ijk + 1, n - 1)
+    if xs is None:
+        span = i1 - lo + 1
+        near = nhi - nlo + 1
+        return int((span.prod(axis=1) - near.prod(axis=1)).sum())
+    # occupied source boxes counted over a box range by a summed-volume table
+    occ = np.zeros((n + 1, n + 1, n + 1), dtype=np.int32)
+    sb = boxes(xs)
+    occ[sb[:, 0] + 1, sb[:, 1] + 1, sb[:, 2] + 1] = 1
+    occ = occ.cumsum(0).cumsum(1).cumsum(2)
+
+    def count(a, b):   # boxes in [a, b] per row, inclusive
+        x0_, y0_, z0_ = a[:, 0], a[:, 1], a[:, 2]
+        x1_, y1_, z1_ = b[:, 0] + 1, b[:, 1] + 1, b[:, 2] + 1
+        return (occ[x1_, y1_, z1_] - occ[x0_, y1_, z1_] - occ[x1_, y0_, z1_] - occ[x1_, y1_, z0_]
+                + occ[x0_, y0_, z1_] + occ[x0_, y1_, z0_] + occ[x1_, y0_, z0_]
+                - occ[x0_, y0_, z0_]).astype(np.int64)
+
+    return int((count(lo, i1) - count(nlo, nhi)).sum())
 
 
 def lap_flops_per_pair(p: int) -> int:
@@ -519,7 +542,7 @@ def our_arm(args, ws, rank, local):
     pairs = list4_pairs(p.depth)
     lv_dom = max(f32["m2l_ms"], key=lambda lv: f32["m2l_ms"][lv])
     if skip_empty:
-        pairs[lv_dom] = list4_pairs_at(p.xt, p.x0, p.D, lv_dom)
+        pairs[lv_dom] = list4_pairs_at(p.xt, p.x0, p.D, lv_dom, p.xs)
     fpp = helm_flops_per_pair if helm else lap_flops_per_pair
     flops = pairs[lv_dom] * fpp(p.order_s[lv_dom])
     achieved = flops / (f32["m2l_ms"][lv_dom] * 1e-3) / 1e12
@@ -531,7 +554,8 @@ def our_arm(args, ws, rank, local):
                                "MEASURED_PEAKS.json holds no SIMT figure",
                 "algorithmic_flops_per_launch": flops,
                 "pairs": pairs[lv_dom], "order": p.order_s[lv_dom],
-                "pairs_counted": ("list-4 pairs of the boxes that hold targets"
+                "pairs_counted": ("list-4 pairs of the boxes that hold targets with "
+                                  "source boxes that hold sources"
                                   if skip_empty else "all list-4 pairs of the dense level")}
 
     cpu = None
