@@ -114,7 +114,7 @@ __host__ __device__ TilePlan tile_plan(int P, int TC, bool dense) {
   size_t ops = sizeof(T) * ((size_t)q.cx_off + q.ncx);
   q.ops_bytes = (ops + 15) & ~(size_t)15;
   q.desc_bytes = ((sizeof(int) * (size_t)(q.nB + (q.dense ? 2 : 1) * q.nC + q.V) +
-                   2 * sizeof(int) * TC) + 15) & ~(size_t)15;
+                   3 * sizeof(int) * TC) + 15) & ~(size_t)15;
   q.vec_bytes = 3 * sizeof(typename C2<T>::t) * (size_t)q.V * TC;
   q.total = q.ops_bytes + q.desc_bytes + q.vec_bytes;
   return q;
@@ -163,7 +163,7 @@ k_m2l_tiles(LanesParams<T> p, OpTables<T> t, int TC, bool dense) {
   typedef typename C2<T>::t T2;
   extern __shared__ __align__(16) unsigned char smraw[];
   const TilePlan q = tile_plan<T, HELM>(p.N, TC, dense);
-  const int P = q.P, V = q.V, TQ = TC / 4;
+  const int P = q.P, V = q.V;
   T* sH = (T*)smraw;
   T* seph = sH + q.NH;
   T* sech = seph + 2 * (P + 1);
@@ -173,7 +173,8 @@ k_m2l_tiles(LanesParams<T> p, OpTables<T> t, int TC, bool dense) {
   int* s_nm = dC + q.nC;             // (n, m) of each vector entry
   int* s_pp = s_nm + V;              // padded-grid index of each target's parent
   int* s_act = s_pp + TC;            // 1 + parent linear index, 0: no target
-  int* dCo = s_act + TC;             // Helmholtz: row offset of each C row pair
+  int* s_map = s_act + TC;           // the offset's columns: target of each
+  int* dCo = s_map + TC;             // Helmholtz: row offset of each C row pair
   T2* X = (T2*)(smraw + q.ops_bytes + q.desc_bytes);
   T2* Y = X + (size_t)V * TC;
   T2* A = Y + (size_t)V * TC;
@@ -231,11 +232,28 @@ k_m2l_tiles(LanesParams<T> p, OpTables<T> t, int TC, bool dense) {
     const int ddx = ((code >> 12) & 3) - 1, ddy = ((code >> 14) & 3) - 1,
               ddz = ((code >> 16) & 3) - 1;
     const int64_t doff = ddx + npx * ((int64_t)ddy + npx * (int64_t)ddz);
-    // the previous offset's operator and vectors are free; an offset whose
-    // sources are all empty boxes adds nothing (the decision is the CTA's)
-    int any = 1;
-    if (p.smask) any = tid < TC && s_act[tid] && p.smask[(int64_t)sg * npp + s_pp[tid] + doff];
-    if (!__syncthreads_or(any)) continue;
+    // the previous offset's operator and vectors are free.  Only the targets
+    // whose source box of this offset lies in the grid (and holds sources,
+    // with skip_empty) take a column: the stages run over ceil(cnt / 4)
+    // groups of 4 columns, and an offset with none is skipped (the decision
+    // is the CTA's)
+    int f = 0;
+    if (tid < TC && s_act[tid]) {
+      if (p.smask) {
+        f = p.smask[(int64_t)sg * npp + s_pp[tid] + doff];
+      } else {
+        const int pp = s_pp[tid];
+        const int sx = pp % npx + ddx, sy = (pp / npx) % npx + ddy, sz = pp / (npx * npx) + ddz;
+        f = sx >= 1 && sx <= nx && sy >= 1 && sy <= nx && sz >= 1 && sz <= nx;
+      }
+    }
+    const int cnt = __syncthreads_count(f);
+    if (cnt == 0) continue;
+    if (tid < 32) {
+      const unsigned bal = __ballot_sync(0xffffffffu, f);
+      if (f) s_map[__popc(bal & ((1u << tid) - 1u))] = tid;
+    }
+    const int TQ = (cnt + 3) / 4, TCc = 4 * TQ;
     {
       const T* H = t.H + (int64_t)t.op_ith[op] * t.hstride;
       for (int i = tid; i < q.NH; i += kTileThreads) sH[i] = H[i];
@@ -262,16 +280,16 @@ k_m2l_tiles(LanesParams<T> p, OpTables<T> t, int TC, bool dense) {
     // stage A: the TC source vectors, with e^{i m ch}
     {
       const T2* src = (const T2*)p.lin_raw + (int64_t)sg * V * npp + doff;
-      for (int i = tid; i < V * TC; i += kTileThreads) {
-        const int c = i / TC, tt = i - c * TC;
+      for (int i = tid; i < V * TCc; i += kTileThreads) {
+        const int c = i / TCc, tt = i - c * TCc;
         T2 v;
         v.x = T(0); v.y = T(0);
-        if (s_act[tt]) {
-          v = src[(int64_t)c * npp + s_pp[tt]];
+        if (tt < cnt) {
+          v = src[(int64_t)c * npp + s_pp[s_map[tt]]];
           const int m = (s_nm[c] >> 8) - 64, am = m < 0 ? -m : m;
           v = cmul(v, sech[2 * am], m < 0 ? -sech[2 * am + 1] : sech[2 * am + 1]);
         }
-        X[i] = v;
+        X[(size_t)c * TC + tt] = v;
       }
     }
     __syncthreads();
@@ -451,11 +469,13 @@ k_m2l_tiles(LanesParams<T> p, OpTables<T> t, int TC, bool dense) {
         for (int r = 0; r < (two ? 2 : 1); r++) {
           const int nu = nu0 + r, an = nu < 0 ? -nu : nu;
           const T er = sech[2 * an], ei = nu < 0 ? sech[2 * an + 1] : -sech[2 * an + 1];
-          T2* ar = A + (size_t)cidx(n, nu) * TC + t0;
+          T2* ar = A + (size_t)cidx(n, nu) * TC;
 #pragma unroll
           for (int k = 0; k < 4; k++) {
+            if (t0 + k >= cnt) break;
             const T2 o = cmul(r ? a1[k] : a0[k], er, ei);
-            ar[k].x += o.x; ar[k].y += o.y;
+            T2& a = ar[s_map[t0 + k]];
+            a.x += o.x; a.y += o.y;
           }
         }
       } else {
@@ -479,12 +499,14 @@ k_m2l_tiles(LanesParams<T> p, OpTables<T> t, int TC, bool dense) {
         for (int r = 0; r < (two ? 2 : 1); r++) {
           const int nu = nu0 + r;
           const T er = sech[2 * nu], ei = sech[2 * nu + 1];
-          T2* ar = A + (size_t)hidx(n, nu) * TC + t0;
+          T2* ar = A + (size_t)hidx(n, nu) * TC;
 #pragma unroll
           for (int k = 0; k < 4; k++) {
+            if (t0 + k >= cnt) break;
             const T2 a = r ? a1[k] : a0[k];
-            ar[k].x += er * a.x + ei * a.y;
-            if (nu != 0) ar[k].y += er * a.y - ei * a.x;
+            T2& o = ar[s_map[t0 + k]];
+            o.x += er * a.x + ei * a.y;
+            if (nu != 0) o.y += er * a.y - ei * a.x;
           }
         }
       }
