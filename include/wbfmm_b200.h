@@ -211,8 +211,8 @@ int wbfmm_b200_tree_structure(int n, const double *pts, int pstr,
 
 /* M2L kernel selection (all need equal singular and regular orders, else
    the warp kernel runs): 1 (default) = automatic: lane-per-pair kernel up to
-   order 8 (Helmholtz) / 10 (Laplace) in FP32 and 7 / 9 in FP64,
-   offset-major target tiles above, while their shared memory suffices;
+   order 7 (Helmholtz) / 10 (Laplace FP32) / 9 (Laplace FP64), offset-major
+   target tiles above, while their shared memory suffices;
    2 = lane-per-pair wherever instantiated
    (Helmholtz <= 8, Laplace <= 16); 3 = target tiles wherever they fit;
    0 = always the warp-per-target kernel. */

@@ -739,11 +739,12 @@ struct Solver : public wbfmm_b200_solver {
     const bool tiles_ok = helm ? tiles_supported<T, true>(x.Nin, x.Nout)
                                : tiles_supported<T, false>(x.Nin, x.Nout);
     // automatic: lanes at the orders where their unrolled code wins, tiles
-    // above, the warp-per-target kernel for what neither covers (FP64
-    // Helmholtz p = 8 and Laplace p = 10 run 15-20% faster as tiles, dense
-    // or on target lists; FP32 at those orders, and p = 9 Laplace FP64, as
-    // lanes)
-    const int lanes_max = sizeof(T) == 8 ? (helm ? 7 : 9) : (helm ? 8 : 10);
+    // above, the warp-per-target kernel for what neither covers (Helmholtz
+    // p = 8 runs as fast or faster as tiles in both forms, up to 2x on small
+    // levels, and FP64 Laplace p = 10 15-20% faster, dense or on target
+    // lists; Helmholtz p = 7, FP32 Laplace p = 10 and FP64 Laplace p = 9 run
+    // faster as lanes)
+    const int lanes_max = helm ? 7 : sizeof(T) == 8 ? 9 : 10;
     bool use_tiles = false, use_lanes = false;
     if (m2l_mode == 1) {
       use_lanes = lanes_ok && x.Nin <= lanes_max;
