@@ -48,7 +48,8 @@ struct Req {
   char error[256] = "";
 };
 
-// pinned host staging that only grows
+// pinned host staging that only grows, at least doubling (each regrowth's
+// cudaFreeHost synchronises the device, stalling every slot)
 struct Pinned {
   double* p = nullptr;
   size_t n = 0;
@@ -58,7 +59,7 @@ struct Pinned {
     if (p) cudaFreeHost(p);
     p = nullptr;
     n = 0;
-    size_t want = count + count / 4;
+    size_t want = std::max(count + count / 4, 2 * n);
     if (cudaMallocHost(&p, sizeof(double) * want) != cudaSuccess) {
       cudaGetLastError();
       return set_error(WBFMM_B200_E_NOMEM, "pinned host allocation failed");

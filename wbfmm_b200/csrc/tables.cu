@@ -22,6 +22,18 @@
 
 namespace wbfmm {
 
+cudaMemPool_t library_pool();   // solver.cu
+
+// Scratch of a table build, from the library's pool: its freed blocks stay
+// cached there, so the builds of a serving loop (one per Helmholtz request)
+// map no new device memory.  The device's default pool would return them
+// at the next synchronisation and map them again for the next build.
+static cudaError_t table_scratch(double** p, size_t bytes, cudaStream_t s) {
+  cudaMemPool_t pl = library_pool();
+  return pl ? cudaMallocFromPoolAsync((void**)p, bytes, pl, s)
+            : cudaMallocAsync((void**)p, bytes, s);
+}
+
 // ------------------------------------------------------- host geometry
 static int find_or_add(std::vector<double>& v, double x) {
   for (size_t i = 0; i < v.size(); i++)
@@ -139,7 +151,7 @@ int generate_rotation_tables(const std::vector<double>& thetas, int N,
   for (int i = 0; i < nt; i++) th.v[i] = thetas[i];
   double* scratch = nullptr;
   int64_t sstride = rot_count(2 * N + 1) + 16;
-  WBFMM_CUDA(cudaMallocAsync(&scratch, sizeof(double) * sstride * nt, s));
+  WBFMM_CUDA(table_scratch(&scratch, sizeof(double) * sstride * nt, s));
   size_t smem = sizeof(double) * 2 * (2 * N + 3);
   k_rotation_tables<<<nt, 256, smem, s>>>(th, N, dH, hstride, scratch, sstride);
   WBFMM_CUDA(cudaGetLastError());
@@ -267,7 +279,7 @@ int generate_coaxial_tables(const std::vector<double>& krs, int L, int nc,
   double* scratch = nullptr;
   int LL = 2 * L + 2;
   int64_t sstride = ((int64_t)coax_idx(LL, LL, LL) + 2) * nc;
-  WBFMM_CUDA(cudaMallocAsync(&scratch, sizeof(double) * sstride * nt, s));
+  WBFMM_CUDA(table_scratch(&scratch, sizeof(double) * sstride * nt, s));
   k_coaxial_tables<<<nt, 128, 0, s>>>(kv, L, nc, dout, ostride, scratch, sstride);
   WBFMM_CUDA(cudaGetLastError());
   k_coaxial_orders<<<dim3(L + 1, nt), 64, 0, s>>>(L, nc, dout, ostride, scratch, sstride);

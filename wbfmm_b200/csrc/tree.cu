@@ -209,21 +209,33 @@ __global__ void k_radix_scatter(const uint64_t* __restrict__ keys,
   }
 }
 
+cudaMemPool_t library_pool();   // solver.cu
+
+// Growth of the sort's scratch, stream-ordered from the library's pool: a
+// solver that meets a larger point count (a serving slot, say) does not
+// synchronise the device as cudaFree / cudaMalloc would.
+template <typename X>
+static cudaError_t scratch_regrow(X** p, size_t count, cudaStream_t s) {
+  if (*p) cudaFreeAsync(*p, s);
+  *p = nullptr;
+  cudaMemPool_t pl = library_pool();
+  return pl ? cudaMallocFromPoolAsync((void**)p, sizeof(X) * count, pl, s)
+            : cudaMallocAsync((void**)p, sizeof(X) * count, s);
+}
+
 int radix_sort_pairs(uint64_t* keys, uint32_t* vals, int n, int bits,
                      RadixScratch* scr, cudaStream_t s, int lo) {
   if (n <= 1) return 0;
   int ntiles = (n + kSortTile - 1) / kSortTile;
   if (scr->cap < (size_t)n) {
-    cudaFree(scr->keys_alt); cudaFree(scr->vals_alt);
-    scr->keys_alt = nullptr; scr->vals_alt = nullptr;
-    WBFMM_CUDA(cudaMalloc(&scr->keys_alt, sizeof(uint64_t) * n));
-    WBFMM_CUDA(cudaMalloc(&scr->vals_alt, sizeof(uint32_t) * n));
+    scr->cap = 0;
+    WBFMM_CUDA(scratch_regrow(&scr->keys_alt, (size_t)n, s));
+    WBFMM_CUDA(scratch_regrow(&scr->vals_alt, (size_t)n, s));
     scr->cap = n;
   }
   if (scr->hist_cap < (size_t)ntiles * 256) {
-    cudaFree(scr->hist);
-    scr->hist = nullptr;
-    WBFMM_CUDA(cudaMalloc(&scr->hist, sizeof(uint32_t) * 256 * ntiles));
+    scr->hist_cap = 0;
+    WBFMM_CUDA(scratch_regrow(&scr->hist, (size_t)256 * ntiles, s));
     scr->hist_cap = (size_t)ntiles * 256;
   }
   int passes = (bits + 7) / 8;
