@@ -21,8 +21,9 @@ k ~ U[1, 30], cube or sphere sources, targets = sources, orders for 1e-6):
 batches of SERVE_BATCH requests, host arrays in and out.  The served form
 runs SERVE_SLOTS solves at once, FP32 wherever the FP32 range rule admits
 the request (FP64 otherwise); the plain form is one FP64 solve at a time on
-the same requests.  Both are timed per batch (submission of the first
-request to completion of the last, max over ranks); p50/p99 latency come
+the same requests.  Both run W untimed warm-up batches, then K timed ones,
+each timed from the submission of its first request to the completion of
+its last (max over ranks); p50/p99 latency come
 from a Poisson-arrival run at 70% of the served throughput, and the served
 fields of sampled requests are checked against the FP64 direct sum.
 
@@ -278,8 +279,11 @@ def served_section(args, ws, rank, local):
     """Served FP32 vs plain FP64 on batches of the mixed serving stream."""
     from wbfmm_b200 import engine, workloads as W
 
-    nb = max(1, args.steps) + 1                      # one warm-up batch
-    gen = W.serving_stream(SERVE_BATCH * nb + SERVE_LATENCY_REQUESTS, seed=4 + 1000 * rank)
+    # W warm-up batches (memory pools, pinned staging and table cache reach
+    # their steady state), then K timed ones
+    nw, nb = max(1, args.warmup), max(1, args.steps)
+    gen = W.serving_stream(SERVE_BATCH * (nw + nb) + SERVE_LATENCY_REQUESTS, seed=4 + 1000 * rank)
+    warm = [[next(gen) for _ in range(SERVE_BATCH)] for _ in range(nw)]
     batches = [[next(gen) for _ in range(SERVE_BATCH)] for _ in range(nb)]
     lat_reqs = [next(gen) for _ in range(SERVE_LATENCY_REQUESTS)]
 
@@ -323,28 +327,29 @@ def served_section(args, ws, rank, local):
     arms = (("plain_fp64", 1, plain_prec, False), ("served", SERVE_SLOTS, served_prec, True))
     for name, slots, precf, skip in arms:
         with engine.Server(slots=slots) as srv:
-            run_batch(srv, batches[0], precf, skip)              # warm-up
+            for b in warm:
+                run_batch(srv, b, precf, skip)                  # warm-up
             spans = []
             with ClockSampler(local) as clk:
-                for i, b in enumerate(batches[1:]):
+                for i, b in enumerate(batches):
                     span, k = run_batch(srv, b, precf, skip,
                                         keep=8 if (name == "served" and i == 0) else 0)
                     spans.append(span)
                     if k:
                         kept = k
-            pts = sum(p.points for b in batches[1:] for p in b)
+            pts = sum(p.points for b in batches for p in b)
             out[name] = {"points_per_s": ws * pts / sum(spans), "seconds": sum(spans),
-                         "requests": len(batches[1:]) * SERVE_BATCH, "slots": slots,
+                         "requests": len(batches) * SERVE_BATCH, "slots": slots,
                          "skip_empty": skip,
                          "clocks": clk.summary(), "stats": srv.stats()}
     rate_req = 0.7 * out["served"]["points_per_s"] / ws / np.mean(
-        [p.points for b in batches[1:] for p in b])
+        [p.points for b in batches for p in b])
     for name, slots, precf, skip in arms[::-1]:
         with engine.Server(slots=slots) as srv:
             out[name]["latency"] = run_latency(srv, lat_reqs, precf, skip, rate_req)
     # accuracy of served fields against the FP64 direct sum
     worst, checked = 0.0, []
-    for p, (pot, grad) in zip(batches[1][:8], kept or []):
+    for p, (pot, grad) in zip(batches[0][:8], kept or []):
         idx = W.subsample(105, p.ns, 1000)
         dpot, dgrad = engine.direct(p.problem, p.xs, p.q, p.xs[idx], k=p.k)
         w = 2 if p.problem == W.HELMHOLTZ else 1
@@ -354,12 +359,12 @@ def served_section(args, ws, rank, local):
         checked.append({"n": p.ns, "problem": "helmholtz" if p.problem == W.HELMHOLTZ else "laplace",
                         "k": p.k, "fp32": served_prec(p) == engine.FP32,
                         "pot_rel_l2": ep, "grad_rel_l2": eg})
-    fp32_frac = float(np.mean([served_prec(p) == engine.FP32 for b in batches[1:] for p in b]))
+    fp32_frac = float(np.mean([served_prec(p) == engine.FP32 for b in batches for p in b]))
     return {
         "workload": "serving stream: N log-uniform [1e3, 3e5], 50% Laplace (p=14) / 50% "
                     "Helmholtz (k~U[1,30], p_l=max(14, kw+1.8*6^(2/3)*(kw)^(1/3))), cube or "
                     "r=0.45 sphere, targets = sources, depth for ~64 points per leaf",
-        "batch_requests": SERVE_BATCH, "batches": len(batches) - 1,
+        "batch_requests": SERVE_BATCH, "batches": len(batches), "warmup_batches": len(warm),
         "served_fp32": out["served"], "plain_fp64": out["plain_fp64"],
         "served_over_plain": out["served"]["points_per_s"] / out["plain_fp64"]["points_per_s"],
         "fp32_fraction": fp32_frac,
