@@ -397,6 +397,87 @@ def workload(args, rank):
     raise SystemExit(f"unknown workload {w}")
 
 
+# ------------------------------------------------------ profiling cases
+# Small, fixed workloads for profiling single kernels of the engine
+# (`python bench.py --profile-case <case>`): each builds one solve, runs it
+# once (warm-up: tables, buffers), then launches the stage it is named for
+# once more on its own, so that a profiler filtering on that kernel's name
+# with one or two captured launches sees the steady-state launch.
+PROFILE_CASES = """
+
+  m2l_tiles_laplace_p14     Laplace, 3e5 uniform points, depth 5, order 14,
+                            FP32: M2L of level 5 (offset-major tile kernel)
+  m2l_tiles_helmholtz_p14   Helmholtz k = 10, 1e5 points, depth 4, orders
+                            max(14, kw rule), FP32: M2L of level 4
+  m2l_lanes_helmholtz_p6    Helmholtz k = 8, 1e6 points, depth 6, the
+                            benchmark's orders, FP32: M2L of level 6
+                            (lane-per-pair kernel)
+  m2l_lanes_laplace_clusters_p10
+                            Laplace, 2e6 points in 8 Gaussian clusters,
+                            depth 7, order 10, skip_empty, FP32: M2L of
+                            level 7 (lane kernel on target lists)
+  p2p_helmholtz             Helmholtz k = 10, 2e5 points, depth 4, FP32:
+                            evaluation (L2P + P2P)
+  served_stream             48 requests of the serving stream through a
+                            1-slot server, FP32 where the range rule admits
+                            the request, skip_empty and leaf_order (launch
+                            lists of a served mix)
+"""
+
+
+def _solve_then(p, precision, stage, skip_empty=False):
+    from wbfmm_b200 import engine
+    cfg = engine.SolverConfig.from_problem(p, precision, skip_empty=skip_empty)
+    with engine.Solver(cfg) as s:
+        s.set_sources(p.xs, p.normals).set_strengths(p.q, p.dipoles).set_targets(p.xt).run()
+        stage(s)
+        s.synchronize()
+
+
+def _cube(problem, n, depth, order, k=0.0, seed=1):
+    from wbfmm_b200 import engine, workloads as W
+    rng = np.random.default_rng(seed)
+    p = W.serve_request(rng, n, problem == engine.HELMHOLTZ, k, False)
+    p.depth = depth
+    p.order_s = [0] * (depth + 1)
+    for lv in range(1, depth + 1):
+        p.order_s[lv] = (W.helmholtz_order(k, p.D / 2 ** lv, lo=order, hi=60)
+                         if problem == engine.HELMHOLTZ else order)
+    p.order_r = list(p.order_s)
+    return p
+
+
+def profile_case(case: str) -> None:
+    from wbfmm_b200 import engine, workloads as W
+    if case == "m2l_tiles_laplace_p14":
+        p = _cube(engine.LAPLACE, 300_000, 5, 14)
+        _solve_then(p, engine.FP32, lambda s: s.m2l(5))
+    elif case == "m2l_tiles_helmholtz_p14":
+        p = _cube(engine.HELMHOLTZ, 100_000, 4, 14, k=10.0)
+        _solve_then(p, engine.FP32, lambda s: s.m2l(4))
+    elif case == "m2l_lanes_helmholtz_p6":
+        p = W.helmholtz_cube(1_000_000, k=8.0, depth=6, seed=2)
+        _solve_then(p, engine.FP32, lambda s: s.m2l(6))
+    elif case == "m2l_lanes_laplace_clusters_p10":
+        p = W.laplace_clusters(2_000_000, depth=7, order=10, seed=5)
+        _solve_then(p, engine.FP32, lambda s: s.m2l(7), skip_empty=True)
+    elif case == "p2p_helmholtz":
+        p = _cube(engine.HELMHOLTZ, 200_000, 4, 8, k=10.0)
+        _solve_then(p, engine.FP32, lambda s: s.evaluate())
+    elif case == "served_stream":
+        reqs = list(W.serving_stream(48, seed=4))
+        with engine.Server(slots=1) as srv:
+            tickets = [srv.submit(p, engine.FP32 if engine.fp32_range_ok(engine.SolverConfig.from_problem(p))
+                                  else engine.FP64, skip_empty=True, leaf_order=True)
+                       for p in reqs]
+            srv.drain()
+            for t in tickets:
+                srv.wait(t)
+    else:
+        raise SystemExit(f"unknown profiling case {case!r}; see PROFILE_CASES")
+
+
+
 # ----------------------------------------------------------- our arm
 def our_arm(args, ws, rank, local):
     import torch
@@ -616,11 +697,17 @@ def main():
     ap.add_argument("--depth", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-served", action="store_true")
+    ap.add_argument("--profile-case", default=None,
+                    help="run one small profiling case instead of the benchmark "
+                         "(see PROFILE_CASES)")
     ap.add_argument("--workload", default="cube",
                     choices=["cube", "laplace_c1", "sphere_c3", "clusters_c5"],
                     help="cube (default): 1e6 Helmholtz cube + served stream; the others "
                          "measure the benchmark's further configurations")
     args = ap.parse_args()
+    if args.profile_case:
+        profile_case(args.profile_case)
+        return
     ws, rank, local = dist_setup()
     try:
         if args.impl == "reference":

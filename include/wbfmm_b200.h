@@ -241,19 +241,21 @@ int wbfmm_b200_error_norms(int64_t n, const double *f, const double *ref,
    (the ordering wbfmm_b200_set_sources computes for the tree), with no
    device allocation.  This entry point has no counterpart in the reference.
    It is for callers that cannot allocate device memory where they need the
-   sort: work recorded inside a CUDA stream capture, serving loops that must
-   not take cudaMalloc's device-wide synchronisation, and processes whose
-   device memory belongs to another allocator.  They pass their own buffers:
-   pts[i*pstr + 0..2] (device), keys[n] and ip[n] (device, outputs: sorted
-   keys and the permutation); x0 (3 doubles) is host memory.  The sort's
-   scratch is a fixed array of about 12.6 MB in device memory that every GPU
-   which loads the library holds until the process exits, so n may not
-   exceed WBFMM_B200_NOALLOC_MAX_POINTS (larger n returns WBFMM_B200_E_ARG).
-   The first call on a device looks up that array's device address, so make
-   it before any stream capture.  All calls on a device share the array:
-   calls that overlap on the GPU race with each other.  The call returns after
-   its work on `stream` has finished (it reads back a domain-check flag;
-   points not strictly inside the cube return WBFMM_B200_E_DOMAIN). */
+   sort: serving loops that must not take cudaMalloc's device-wide
+   synchronisation, and processes whose device memory belongs to another
+   allocator.  They pass their own buffers: pts[i*pstr + 0..2] (device),
+   keys[n] and ip[n] (device, outputs: sorted keys and the permutation); x0
+   (3 doubles) is host memory.  The sort's scratch is a fixed array of about
+   12.6 MB in device memory that every GPU which loads the library holds
+   until the process exits, so n may not exceed
+   WBFMM_B200_NOALLOC_MAX_POINTS (larger n returns WBFMM_B200_E_ARG).  The
+   first call on a device looks up that array's device address (make it
+   before any stream capture); the address is kept for the process, so the
+   device must not be reset while the library is in use.  All calls on a
+   device share the array: calls that overlap on the GPU race with each
+   other.  The call returns after its work on `stream` has finished (it
+   reads back a domain-check flag; points not strictly inside the cube
+   return WBFMM_B200_E_DOMAIN). */
 int wbfmm_b200_morton_sort_noalloc(int n, const double *pts, int pstr,
                                    const double *x0, double D, uint64_t *keys,
                                    uint32_t *ip, void *stream);

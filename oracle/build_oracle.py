@@ -22,6 +22,8 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
+# where the reference tree lies in the build container: the one place this
+# repository names it (WBFMM_REFERENCE_ROOT overrides)
 REF_ROOT = os.environ.get("WBFMM_REFERENCE_ROOT", "/root/reference")
 REF_OUT = os.path.join(HERE, "_ref")
 BUILD_DIR = os.path.join(HERE, "_build")

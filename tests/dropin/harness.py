@@ -13,6 +13,7 @@ from __future__ import annotations
 
 import os
 import subprocess
+import sys
 import tempfile
 from dataclasses import dataclass
 
@@ -22,7 +23,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 BUILD = os.path.join(HERE, "_build")
 SRC = os.path.join(HERE, "driver.c")
-REF_ROOT = os.environ.get("WBFMM_REFERENCE_ROOT", "/root/reference")
+sys.path.insert(0, ROOT)
+from oracle.build_oracle import REF_ROOT  # noqa: E402  (the reference tree, if present)
 
 LAPLACE, HELMHOLTZ = 1, 2
 POTENTIAL, GRADIENT = 1, 2

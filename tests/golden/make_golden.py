@@ -1,6 +1,7 @@
 """Generate the golden fixtures in tests/golden/ from the unmodified reference.
 
-Run here (where /root/reference exists):  python tests/golden/make_golden.py
+Run where the reference sources are present (oracle/build_oracle.py's
+REF_ROOT, or WBFMM_REFERENCE_ROOT):  python tests/golden/make_golden.py
 It builds oracle/_ref/libwbfmm_ref.so if needed, runs the reference FMM on
 small seeded inputs through oracle/ref_harness.c, and stores inputs and
 outputs (potential, gradient, t->ip, box {i,n} per level) as .npz files.

@@ -4,14 +4,13 @@
 // cudaMalloc.
 //
 // Some callers of this library cannot allocate device memory at the point
-// where they need the sort: code recorded inside a CUDA stream capture
-// (cudaMalloc is not a capturable operation), latency-critical serving
-// loops that must not take cudaMalloc's implicit device-wide
-// synchronisation, and processes whose device memory is owned by another
-// allocator (a framework's caching allocator that has reserved the GPU).
-// They pass their own input and output buffers; everything else this entry
-// point needs lives in g_noalloc_scratch below, a fixed-size array that
-// every GPU which loads the library holds until the process exits.
+// where they need the sort: latency-critical serving loops that must not
+// take cudaMalloc's implicit device-wide synchronisation, and processes
+// whose device memory is owned by another allocator (a framework's caching
+// allocator that has reserved the GPU).  They pass their own input and
+// output buffers; everything else this entry point needs lives in
+// g_noalloc_scratch below, a fixed-size array that every GPU which loads
+// the library holds until the process exits.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -36,7 +35,9 @@ constexpr size_t kNaBytes = kNaFlagOff + 256;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNaBytes];
 
 // device address of g_noalloc_scratch, looked up once per device with that
-// device current (host code may not use the symbol itself as an address)
+// device current (host code may not use the symbol itself as an address).
+// The address stays valid while the device's primary context lives, so a
+// process must not reset the device (cudaDeviceReset) and then call again.
 static unsigned char* g_na_addr[64] = {nullptr};
 static std::mutex g_na_mutex;
 
@@ -76,9 +77,8 @@ extern "C" int wbfmm_b200_morton_sort_noalloc(int n, const double* pts,
   cudaStream_t s = (cudaStream_t)stream;
   int* flag = (int*)(base + kNaFlagOff);
   // strict-interior domain check (src/boxes.c:148-153): the flag keeps the
-  // last call's value, so it is reset first
-  const int big = 0x7fffffff;
-  WBFMM_CUDA(cudaMemcpyAsync(flag, &big, sizeof(int), cudaMemcpyHostToDevice, s));
+  // last call's value, so a kernel on the caller's stream resets it first
+  launch_set_words((uint32_t*)flag, 0x7fffffffu, nullptr, 0, s);
   launch_domain_check(pts, pstr, n, x0, D, flag, s);
   launch_point_keys(pts, pstr, n, x0, D, keys, ip, s);
   RadixScratch scr;

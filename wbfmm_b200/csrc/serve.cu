@@ -56,10 +56,10 @@ struct Pinned {
   ~Pinned() { if (p) cudaFreeHost(p); }
   int reserve(size_t count) {
     if (count <= n) return 0;
+    const size_t want = std::max(count + count / 4, 2 * n);
     if (p) cudaFreeHost(p);
     p = nullptr;
     n = 0;
-    size_t want = std::max(count + count / 4, 2 * n);
     if (cudaMallocHost(&p, sizeof(double) * want) != cudaSuccess) {
       cudaGetLastError();
       return set_error(WBFMM_B200_E_NOMEM, "pinned host allocation failed");

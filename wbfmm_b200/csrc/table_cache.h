@@ -161,9 +161,37 @@ struct TableCache {
     if (rc_ != 0) return rc_;        \
   } while (0)
 
-  // build the order-only tables for phases up to L (caller holds mu)
+  // release a Geo's tables and event (stream-ordered on s for pool memory)
+  // and the Geo
+  void drop_geo(Geo* g, cudaStream_t s) {
+    void* ps[] = {g->H64, g->H32, g->op_ith, g->op_dist, g->r64, g->r32,
+                  g->ph64, g->ph32, g->ch64, g->ch32, g->lap64[0], g->lap64[1],
+                  g->lap64[2], g->lap32[0], g->lap32[1], g->lap32[2]};
+    for (void* p : ps)
+      if (p) {
+        if (pool) cudaFreeAsync(p, s);
+        else cudaFree(p);
+      }
+    if (g->ready) cudaEventDestroy(g->ready);
+    delete g;
+  }
+
+  // build the order-only tables for phases up to L (caller holds mu); a
+  // failure part way releases what was allocated
   int build_geo(int L, cudaStream_t s, Geo** out) {
     Geo* g = new Geo();
+    const int rc = fill_geo(g, L, s);
+    if (rc) {
+      cudaGetLastError();
+      drop_geo(g, s);
+      return rc;
+    }
+    geos.push_back(g);
+    *out = g;
+    return 0;
+  }
+
+  int fill_geo(Geo* g, int L, cudaStream_t s) {
     g->L = L;
     ShiftGeometry geom;
     build_shift_geometry(&geom);
@@ -203,8 +231,6 @@ struct TableCache {
     for (int i = 0; i < 3; i++) WBFMM_CACHE_TRY(narrow(g->lap64[i], g->lap32[i], (int64_t)n3, s));
     WBFMM_CUDA(cudaEventCreateWithFlags(&g->ready, cudaEventDisableTiming));
     WBFMM_CUDA(cudaEventRecord(g->ready, s));
-    geos.push_back(g);
-    *out = g;
     return 0;
   }
 

@@ -402,7 +402,6 @@ gint wbfmm_points_origin_width(gdouble *x, gint str, gint n, gdouble *xmin,
   return 0;
 }
 
-/* Gumerov & Duraiswami (2009) truncation rule, as src/util.c:474-503 */
 /* src/util.c:425-450: the points in tree order (q and stride unused) */
 gint wbfmm_tree_write_sources(wbfmm_tree_t *t, gdouble *q, gint stride, FILE *f)
 {
@@ -416,6 +415,7 @@ gint wbfmm_tree_write_sources(wbfmm_tree_t *t, gdouble *q, gint stride, FILE *f)
   return 0;
 }
 
+/* Gumerov & Duraiswami (2009) truncation rule, as src/util.c:474-503 */
 gint wbfmm_truncation_number(wbfmm_tree_t *t, gdouble k, guint level,
                              gdouble tol) {
   const double del = 2.0;
