@@ -60,7 +60,7 @@ def run(p, precision=engine.FP64, field=engine.POTENTIAL | engine.GRADIENT,
 
 
 @pytest.mark.parametrize("path", sorted(p for p in glob.glob(os.path.join(GOLDEN, "*.npz"))
-                                        if not os.path.basename(p).startswith("dropin_")),
+                                        if not os.path.basename(p).startswith(("dropin_", "direct_"))),
                          ids=lambda x: os.path.basename(x)[:-4])
 def test_golden_fp64(gpu_lib, path):
     p, z = load_case(path)

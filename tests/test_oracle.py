@@ -20,7 +20,7 @@ from wbfmm_b200 import workloads as W
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 CASES = sorted(p for p in glob.glob(os.path.join(GOLDEN, "*.npz"))
-               if not os.path.basename(p).startswith("dropin_"))
+               if not os.path.basename(p).startswith(("dropin_", "direct_")))
 
 
 @pytest.mark.parametrize("path", CASES, ids=lambda x: os.path.basename(x)[:-4])
@@ -179,3 +179,40 @@ def test_curl_convention_matches_reference(restatement, reference):
     mine = curl_from_gradients(g)
     ref = reference.direct_curl(xs, q3, xt)
     assert np.linalg.norm(mine - ref) <= 1e-12 * np.linalg.norm(ref)
+
+
+DIRECT_CASES = ("helm_mono", "helm_mixed", "lap_mono", "lap_dipole", "lap_mixed")
+
+
+def direct_case(name):
+    """Inputs and the reference's outputs of one case of direct_sums.npz
+    (the reference's own direct sums, make_direct_golden.py)."""
+    z = np.load(os.path.join(GOLDEN, "direct_sums.npz"))
+
+    def g(a):
+        v = z[f"{name}_{a}"]
+        return v if v.size else None
+
+    return {a: g(a) for a in ("xs", "xt", "q", "normals", "dipoles", "pot")} | {
+        "problem": int(z[f"{name}_problem"]), "k": float(z[f"{name}_k"]),
+        "grad": g("grad") if f"{name}_grad" in z.files else None}
+
+
+@pytest.mark.parametrize("name", DIRECT_CASES)
+def test_restatement_direct_matches_reference_fixture(restatement, name):
+    """The restatement's direct sums equal the reference's (src/direct.c,
+    src/direct-laplace.c) to 1e-13.  For Laplace monopoles plus dipoles the
+    reference leaves the 1/(4 pi) off the dipole term
+    (src/direct-laplace.c:261-263), the restatement (like the FMM) does not:
+    there the reference's value is the monopole sum plus 4 pi times the
+    dipole sum."""
+    c = direct_case(name)
+    kw = dict(k=c["k"], normals=c["normals"], dipoles=c["dipoles"])
+    pot, grad = restatement.direct(c["problem"], c["xs"], c["q"], c["xt"], **kw)
+    if name == "lap_mixed":
+        mono, _ = restatement.direct(c["problem"], c["xs"], c["q"], c["xt"], grad=False)
+        dip, _ = restatement.direct(c["problem"], c["xs"], None, c["xt"], grad=False, **kw)
+        pot = mono + 4.0 * np.pi * dip
+    assert np.linalg.norm(pot - c["pot"]) <= 1e-13 * np.linalg.norm(c["pot"])
+    if c["grad"] is not None:
+        assert np.linalg.norm(grad - c["grad"]) <= 1e-13 * np.linalg.norm(c["grad"])

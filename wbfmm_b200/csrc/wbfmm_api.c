@@ -749,28 +749,64 @@ gint wbfmm_target_list_local_field(wbfmm_target_list_t *l, gdouble *src,
 }
 
 /* ---------------------------------------------------- direct sums */
+/* The reference's direct sums, one target point xf per call, evaluated on
+   the GPU by wbfmm_b200_direct one source component at a time.  Semantics
+   kept from src/direct.c and src/direct-laplace.c:
+   * no sources, normals or dipoles: nothing is added;
+   * normals without dipole strengths stop the program;
+   * component j of nq is written at field[j*fstr + c];
+   * Helmholtz monopoles plus dipoles: the terms are summed without the
+     1/(4 pi) and the first 2*nq entries of field are then divided by 4 pi,
+     including what the caller had stored there (src/direct.c:133-134);
+   * Laplace monopoles plus dipoles: the dipole term has no 1/(4 pi)
+     (src/direct-laplace.c:261-263).
+   Where the reference stops instead (dipole-only Helmholtz potential,
+   gradients of dipole fields) this library returns the field of the
+   kernels the FMM uses. */
+static const double kFourPi = 12.566370614359172953850573533118; /* 4 pi */
+
 static gint direct(int problem, double k, gdouble *xs, gint xstride,
                    gdouble *src, gint sstride, gdouble *normals, gint nstr,
                    gdouble *dipoles, gint dstr, gint nq, gint nsrc,
                    gdouble *xf, gdouble *field, gint fstr, int grad,
                    const char *fn) {
-  int w = problem == WBFMM_B200_HELMHOLTZ ? 2 : 1, i, c;
-  double *x = malloc(sizeof(double) * 3 * nsrc);
-  double *q = src ? malloc(sizeof(double) * w * nsrc) : NULL;
-  double *n = normals ? malloc(sizeof(double) * 3 * nsrc) : NULL;
-  double *d = dipoles ? malloc(sizeof(double) * w * nsrc) : NULL;
-  double out[6] = {0, 0, 0, 0, 0, 0};
-  if (nq != 1) die(fn, "only single-component sources (nq = 1) are supported");
+  const int helm = problem == WBFMM_B200_HELMHOLTZ;
+  const int w = helm ? 2 : 1, nout = grad ? 3 * w : w;
+  const int mixed = src != NULL && normals != NULL;
+  /* Helmholtz mixed potential: unnormalised sums, then the division */
+  const int helm_mixed = helm && mixed && !grad;
+  int i, c, j;
+  double *x, *q, *n, *d;
+  if (src == NULL && normals == NULL && dipoles == NULL) return 0;
+  if (normals != NULL && dipoles == NULL)
+    die(fn, "normals specified but no dipole strengths (dipoles == NULL)");
+  if (nq < 1) die(fn, "nq must be positive");
+  if (nq > 1 && fstr < (grad ? 3 * w : w))
+    die(fn, "field stride too small for multi-component sources");
+  x = malloc(sizeof(double) * 3 * nsrc);
+  q = src ? malloc(sizeof(double) * w * nsrc) : NULL;
+  n = normals ? malloc(sizeof(double) * 3 * nsrc) : NULL;
+  d = dipoles ? malloc(sizeof(double) * w * nsrc) : NULL;
   for (i = 0; i < nsrc; i++) {
     for (c = 0; c < 3; c++) x[3 * i + c] = xs[(size_t)i * xstride + c];
-    for (c = 0; c < w && q; c++) q[w * i + c] = src[(size_t)i * sstride + c];
     for (c = 0; c < 3 && n; c++) n[3 * i + c] = normals[(size_t)i * nstr + c];
-    for (c = 0; c < w && d; c++) d[w * i + c] = dipoles[(size_t)i * dstr + c];
   }
-  check(fn, wbfmm_b200_direct(problem, k, nsrc, x, q, n, d, 1, xf,
-                              grad ? NULL : out, grad ? out : NULL, 0));
-  for (c = 0; c < (grad ? 3 * w : w); c++) field[c] += out[c];
-  (void)fstr;
+  for (j = 0; j < nq; j++) {
+    double out[6] = {0, 0, 0, 0, 0, 0};
+    /* the Laplace mixed sum's dipole term carries no 1/(4 pi) */
+    const double dscale = (!helm && mixed) ? kFourPi : 1.0;
+    for (i = 0; i < nsrc; i++)
+      for (c = 0; c < w; c++) {
+        if (q) q[w * i + c] = src[(size_t)i * sstride + w * j + c];
+        if (d) d[w * i + c] = dscale * dipoles[(size_t)i * dstr + w * j + c];
+      }
+    check(fn, wbfmm_b200_direct(problem, k, nsrc, x, q, n, d, 1, xf,
+                                grad ? NULL : out, grad ? out : NULL, 0));
+    for (c = 0; c < nout; c++)
+      field[(size_t)j * fstr + c] += helm_mixed ? kFourPi * out[c] : out[c];
+  }
+  if (helm_mixed)
+    for (c = 0; c < 2 * nq; c++) field[c] /= kFourPi;
   free(x); free(q); free(n); free(d);
   return 0;
 }
