@@ -1,38 +1,50 @@
-"""Benchmark: FMM points/s of the B200 engine on the Helmholtz cube workload.
+"""Benchmark: served FP32 vs plain FP64 FMM on the mixed serving stream.
 
-Workload (one step = one full FMM solve): 1,000,000 Helmholtz monopoles
-uniform in [-0.5,0.5]^3, complex N(0,1) strengths, k = 8, octree depth 6,
-per-level order p = ceil(kD + 1.8*6^(2/3)*(kD)^(1/3)) clamped to [6, 30]
-(D = box width), targets = sources (self term excluded), potential and
-gradient.  A step runs the whole solve on the GPU from device-resident
-inputs: Morton keys + radix sort + box ranges, FP64 operator tables, P2M,
-M2M, M2L, L2L, L2P, P2P.
+Metric: FMM points/s and p99 latency of the served FP32 form against the
+plain FP64 GPU form, at relative-L2 error <= 1e-6 against the FP64 direct sum.
 
-`value` is the FP32 form's points/s (sources + distinct targets per second,
-summed over GPUs); the plain FP64 form is measured in the same run and
-reported under `plain_fp64`.  `e2e` times the same solve through the C ABI
-with pinned host buffers (host->device inputs and device->host field inside
-the timed region).  Accuracy of both forms is measured against the FP64
-direct sum on 10,000 random targets.
+Workload (`--workload stream`, the default): the mixed serving stream --
+requests with N log-uniform in [1e3, 3e5] sources, half Laplace (order 14)
+and half Helmholtz with k ~ U[1, 30] (per-level orders max(14, kw rule)),
+sources uniform in the cube or on the r = 0.45 sphere (fair coin), N(0,1)
+strengths (complex for Helmholtz), targets = sources, depth for about 64
+points per leaf; seeded synthetic requests (the reference names no
+dataset).  One step = one batch of SERVE_BATCH requests.
 
-`served` holds the served-versus-plain comparison on the mixed serving
-stream (N log-uniform in [1e3, 3e5], half Laplace / half Helmholtz with
-k ~ U[1, 30], cube or sphere sources, targets = sources, orders for 1e-6):
-batches of SERVE_BATCH requests, host arrays in and out.  The served form
-runs SERVE_SLOTS solves at once, FP32 wherever the FP32 range rule admits
-the request (FP64 otherwise); the plain form is one FP64 solve at a time on
-the same requests.  Both run W untimed warm-up batches, then K timed ones,
-each timed from the submission of its first request to the completion of
-its last (max over ranks); p50/p99 latency come
-from a Poisson-arrival run at 70% of the served throughput, and the served
-fields of sampled requests are checked against the FP64 direct sum.
+* `value`: the served form (SERVE_SLOTS solves at once, FP32 wherever the
+  FP32 range rule admits a request, FP64 otherwise, boxes without targets
+  skipped) on batches whose inputs and outputs are already in device memory
+  (requests submitted with device arrays); points/s = sources of the batch /
+  the batch's span from the first submission to the last completion (CUDA
+  events, max over ranks).  W untimed batches, then K timed ones.
+* `e2e`: the same served batches through the public API with host arrays:
+  the host->device copies of every request's inputs and the device->host
+  copies of its fields are inside the timed span.
+* `plain_fp64`: the plain form (one FP64 solve at a time, every box, the
+  reference's point order) on the same batches, device-resident and host;
+  `plain_fp64_skip_empty`: the same with boxes without targets skipped, so
+  that the served form's gain from serving and FP32 shows apart from the
+  empty-box savings.  `served_over_plain` is value / plain value.
+* latency: Poisson arrivals at 30/50/70/90% of each arm's own batch
+  throughput (host arrays), p50 / p99 per load; the top-level
+  `served_p50_s` / `served_p99_s` / `plain_p50_s` / `plain_p99_s` are at 70%.
+* accuracy: the served fields of sampled requests against the FP64 GPU
+  direct sum (itself pinned to the reference's direct sums).
+* `roofline`: the tile M2L (the stream's dominant M2L kernel) on a Laplace
+  order-14 level, against the FP32 FMA peak measured live on the GPU
+  (`wbfmm_b200_fp32_fma_peak`); `traffic` from the committed ncu capture of
+  the same launch.
+* `cpu_baseline` and `--impl reference`: the reference's own CPU FMM
+  (oracle/_ref, the unmodified reference sources, M2L on up to 16 threads)
+  run request by request on a bounded sample of the stream.
+* `cube_c2`: the 1e6-point Helmholtz cube (k = 8, depth 6) solved once per
+  step by the FP32 and FP64 forms, and through the C ABI with host buffers.
 
-`--impl reference` times the reference's own CPU FMM (oracle/_ref, the
-unmodified reference sources) on the host cores, on a bounded sample of the
-workload (see `reference_sample`).
+The other `--workload` values (cube, laplace_c1, sphere_c3, clusters_c5)
+measure single solves of those configurations as the headline instead.
 
 Multi-GPU: one process per GPU (torchrun), independent replicas (weak
-scaling, no collective on the data path); the step time is the max over ranks.
+scaling, no collective on the data path); spans are the max over ranks.
 """
 from __future__ import annotations
 
@@ -51,10 +63,18 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "FMM points/s + p99 latency: served FP32 vs plain FP64 GPU at rel-L2 err<=1e-6"
-WORKLOAD = "helmholtz_cube_1e6_k8_depth6"
+STREAM_WORKLOAD = ("serving_stream_N_loguniform_1e3_3e5_half_laplace_p14_half_helmholtz_"
+                   "k1_30_cube_or_sphere_targets_eq_sources")
+CUBE_WORKLOAD = "helmholtz_cube_1e6_k8_depth6"
 SERVE_SLOTS = 6
 SERVE_BATCH = 256
-SERVE_LATENCY_REQUESTS = 384
+SERVE_LATENCY_REQUESTS = 256
+SERVE_LOADS = (0.3, 0.5, 0.7, 0.9)
+# the CPU reference's sample of the stream: the first requests of the first
+# timed batch with at most this many sources, this many of them
+CPU_SAMPLE_MAX_N = 20_000
+CPU_SAMPLE_REQUESTS = 12
+TILE_PROFILE = os.path.join(ROOT, "profiles", "k_m2l_tiles_laplace_3e5_p14_level5.md")
 
 
 # ---------------------------------------------------------------- helpers
@@ -239,139 +259,6 @@ def run_reference_step(p, nthreads):
     return time.perf_counter() - t0
 
 
-def reference_arm(args, ws, rank):
-    if rank != 0:
-        return
-    from oracle.oracle_api import have_reference
-    cfgd = {"workload": WORKLOAD, "global_batch": 1_000_000, "seq_len": 0,
-            "parallelism": "cpu"}
-    if not have_reference():
-        print(json.dumps({"impl": "reference", "metric": METRIC,
-                          "unavailable": "oracle/_ref/libwbfmm_ref.so was not built"}))
-        return
-    # the sample shrinks when many steps are asked for, so that the whole
-    # run stays within a few minutes of CPU time
-    p = reference_sample(2 if args.steps + args.warmup <= 8 else 4)
-    nthreads = min(os.cpu_count() or 1, 16)
-    for _ in range(args.warmup):
-        run_reference_step(p, nthreads)
-    times = [run_reference_step(p, nthreads) for _ in range(max(1, args.steps))]
-    t = float(np.mean(times))
-    frac = f"1/{(1_000_000 // p.ns)}"
-    v = p.points / t
-    print(json.dumps({
-        "impl": "reference", "metric": METRIC, "value": v, "unit": "points/s",
-        "n_gpus": args.gpus, "steps": len(times), "warmup": args.warmup,
-        "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfgd,
-        "cpu_baseline": {"value": v, "unit": "points/s", "cores": nthreads,
-                         "kind": "reference",
-                         "sample": f"{p.ns} points in a {frac}-volume sub-cube, depth {p.depth}, "
-                                   f"orders {p.order_s[1:]}, same density/k/box widths; "
-                                   "reference FMM with M2L on GThreads (others serial)"},
-        "e2e": {"value": v, "unit": "points/s", "h2d_bytes_per_step": 0,
-                "d2h_bytes_per_step": 0},
-    }))
-
-
-# ----------------------------------------------------- served stream
-def served_section(args, ws, rank, local):
-    """Served FP32 vs plain FP64 on batches of the mixed serving stream."""
-    from wbfmm_b200 import engine, workloads as W
-
-    # W warm-up batches (memory pools, pinned staging and table cache reach
-    # their steady state), then K timed ones
-    nw, nb = max(1, args.warmup), max(1, args.steps)
-    gen = W.serving_stream(SERVE_BATCH * (nw + nb) + SERVE_LATENCY_REQUESTS, seed=4 + 1000 * rank)
-    warm = [[next(gen) for _ in range(SERVE_BATCH)] for _ in range(nw)]
-    batches = [[next(gen) for _ in range(SERVE_BATCH)] for _ in range(nb)]
-    lat_reqs = [next(gen) for _ in range(SERVE_LATENCY_REQUESTS)]
-
-    def served_prec(p):
-        ok = engine.fp32_range_ok(engine.SolverConfig.from_problem(p))
-        return engine.FP32 if ok else engine.FP64
-
-    def plain_prec(p):
-        return engine.FP64
-
-    def run_batch(srv, batch, precf, skip, keep=0):
-        dist_barrier(ws)
-        t0 = srv.clock()
-        tk = [srv.submit(p, precf(p), skip_empty=skip, leaf_order=skip) for p in batch]
-        srv.drain()
-        span = max(srv.times(t)[3] for t in tk) - t0
-        kept = [tuple(a.copy() for a in srv.wait(t)) for t in tk[:keep]]
-        for t in tk:
-            srv.forget(t)
-        return dist_max(span, ws), kept
-
-    def run_latency(srv, reqs, precf, skip, rate):
-        arr = W.poisson_arrivals(len(reqs), rate, seed=104 + rank)
-        base = srv.clock() + 0.02
-        tk = [srv.submit(p, precf(p), arrival=base + a, skip_empty=skip, leaf_order=skip)
-              for p, a in zip(reqs, arr)]
-        srv.drain()
-        T = np.array([srv.times(t) for t in tk])
-        for t in tk:
-            srv.forget(t)
-        lat = T[:, 3] - T[:, 0]
-        return {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
-                "mean_s": float(lat.mean()),
-                "throughput_points_per_s": float(sum(p.points for p in reqs) / (T[:, 3].max() - base))}
-
-    out = {}
-    kept = None
-    # the plain form computes every box's local expansion and sorts the
-    # points on full keys, as the reference does; the served form forms only
-    # the local expansions of boxes that hold targets and sorts by leaf box
-    arms = (("plain_fp64", 1, plain_prec, False), ("served", SERVE_SLOTS, served_prec, True))
-    for name, slots, precf, skip in arms:
-        with engine.Server(slots=slots) as srv:
-            for b in warm:
-                run_batch(srv, b, precf, skip)                  # warm-up
-            spans = []
-            with ClockSampler(local) as clk:
-                for i, b in enumerate(batches):
-                    span, k = run_batch(srv, b, precf, skip,
-                                        keep=8 if (name == "served" and i == 0) else 0)
-                    spans.append(span)
-                    if k:
-                        kept = k
-            pts = sum(p.points for b in batches for p in b)
-            out[name] = {"points_per_s": ws * pts / sum(spans), "seconds": sum(spans),
-                         "requests": len(batches) * SERVE_BATCH, "slots": slots,
-                         "skip_empty": skip,
-                         "clocks": clk.summary(), "stats": srv.stats()}
-    rate_req = 0.7 * out["served"]["points_per_s"] / ws / np.mean(
-        [p.points for b in batches for p in b])
-    for name, slots, precf, skip in arms[::-1]:
-        with engine.Server(slots=slots) as srv:
-            out[name]["latency"] = run_latency(srv, lat_reqs, precf, skip, rate_req)
-    # accuracy of served fields against the FP64 direct sum
-    worst, checked = 0.0, []
-    for p, (pot, grad) in zip(batches[0][:8], kept or []):
-        idx = W.subsample(105, p.ns, 1000)
-        dpot, dgrad = engine.direct(p.problem, p.xs, p.q, p.xs[idx], k=p.k)
-        w = 2 if p.problem == W.HELMHOLTZ else 1
-        ep = engine.error_norms(pot.reshape(p.ns, w)[idx].ravel(), dpot)[0]
-        eg = engine.error_norms(grad.reshape(p.ns, 3 * w)[idx].ravel(), dgrad)[0]
-        worst = max(worst, ep, eg)
-        checked.append({"n": p.ns, "problem": "helmholtz" if p.problem == W.HELMHOLTZ else "laplace",
-                        "k": p.k, "fp32": served_prec(p) == engine.FP32,
-                        "pot_rel_l2": ep, "grad_rel_l2": eg})
-    fp32_frac = float(np.mean([served_prec(p) == engine.FP32 for b in batches for p in b]))
-    return {
-        "workload": "serving stream: N log-uniform [1e3, 3e5], 50% Laplace (p=14) / 50% "
-                    "Helmholtz (k~U[1,30], p_l=max(14, kw+1.8*6^(2/3)*(kw)^(1/3))), cube or "
-                    "r=0.45 sphere, targets = sources, depth for ~64 points per leaf",
-        "batch_requests": SERVE_BATCH, "batches": len(batches), "warmup_batches": len(warm),
-        "served_fp32": out["served"], "plain_fp64": out["plain_fp64"],
-        "served_over_plain": out["served"]["points_per_s"] / out["plain_fp64"]["points_per_s"],
-        "fp32_fraction": fp32_frac,
-        "offered_load_requests_per_s": float(rate_req),
-        "accuracy": {"max_rel_l2": worst, "tolerance": 1e-6, "requests": checked},
-        "io": "host arrays in and out (copies inside the timed region)",
-    }
 
 
 # ------------------------------------------------------------ workloads
@@ -383,7 +270,7 @@ def workload(args, rank):
     w = args.workload
     if w == "cube":
         p = W.helmholtz_cube(args.points, k=8.0, depth=args.depth, seed=2 + rank)
-        return p, 10_000, 102, False, WORKLOAD
+        return p, 10_000, 102, False, CUBE_WORKLOAD
     if w == "laplace_c1":
         p = W.laplace_cube(20_000, 20_000, depth=4, order=12, seed=1 + rank)
         return p, 20_000, 101, False, "laplace_cube_2e4_separate_targets_depth4_p12"
@@ -478,17 +365,279 @@ def profile_case(case: str) -> None:
 
 
 
-# ----------------------------------------------------------- our arm
-def our_arm(args, ws, rank, local):
+def stream_requests(args, rank):
+    """The stream's requests for one rank: W warm-up batches, K timed
+    batches, and the latency run's requests (seeded per rank)."""
+    from wbfmm_b200 import workloads as W
+    nw, nb = max(1, args.warmup), max(1, args.steps)
+    gen = W.serving_stream(SERVE_BATCH * (nw + nb) + SERVE_LATENCY_REQUESTS, seed=4 + 1000 * rank)
+    warm = [[next(gen) for _ in range(SERVE_BATCH)] for _ in range(nw)]
+    batches = [[next(gen) for _ in range(SERVE_BATCH)] for _ in range(nb)]
+    lat = [next(gen) for _ in range(SERVE_LATENCY_REQUESTS)]
+    return warm, batches, lat
+
+
+def stream_cpu_sample(rank=0):
+    """The CPU reference's bounded sample of the stream: in stream order, the
+    first CPU_SAMPLE_REQUESTS requests of the first timed batch (the same
+    requests whatever the step counts) with at most CPU_SAMPLE_MAX_N sources.
+    The reference's points/s falls with the request size (deeper trees, more
+    M2L pairs per point), so leaving the larger requests out favours the
+    reference."""
+    from wbfmm_b200 import workloads as W
+    gen = W.serving_stream(SERVE_BATCH * 2, seed=4 + 1000 * rank)
+    reqs = [next(gen) for _ in range(SERVE_BATCH * 2)][SERVE_BATCH:]   # a batch after one warm-up
+    out = [p for p in reqs if p.ns <= CPU_SAMPLE_MAX_N][:CPU_SAMPLE_REQUESTS]
+    return out
+
+
+def stream_config(ws):
+    return {"workload": STREAM_WORKLOAD, "global_batch": ws * SERVE_BATCH, "seq_len": 0,
+            "parallelism": f"replicas{ws}", "requests_per_step_per_gpu": SERVE_BATCH,
+            "l2": "each step's inputs (about 0.5 GB per batch) exceed the 126 MB L2"}
+
+
+def run_reference_requests(reqs, nthreads):
+    """Seconds of the reference's own CPU FMM over the requests, one after
+    another, as its drivers run a solve (tree, operators, passes, potential
+    and gradient evaluation)."""
+    from oracle.oracle_api import Reference
+    R = Reference()
+    t0 = time.perf_counter()
+    for p in reqs:
+        R.fmm(p.problem, p.depth, p.order_s, p.order_r, p.x0, p.D, p.xs, p.q, p.xt,
+              k=p.k, pot=True, grad=True, nthreads=nthreads)
+    return time.perf_counter() - t0
+
+
+def cpu_sample_text(reqs):
+    nh = sum(p.problem == 2 for p in reqs)
+    return (f"{len(reqs)} requests of the stream ({nh} Helmholtz, {len(reqs) - nh} Laplace; "
+            f"{sum(p.ns for p in reqs)} sources; the first {CPU_SAMPLE_REQUESTS} of a batch "
+            f"with N <= {CPU_SAMPLE_MAX_N}), one after another; reference FMM with M2L on "
+            "GThreads (other stages serial), potential and gradient")
+
+
+def reference_arm(args, ws, rank):
+    """The reference's own CPU implementation (oracle/_ref) on the host
+    cores, on this arm's workload, metric and config; rank 0 only."""
+    if rank != 0:
+        return
+    from oracle.oracle_api import have_reference
+    stream = args.workload == "stream"
+    cfgd = stream_config(ws) if stream else {"workload": CUBE_WORKLOAD, "global_batch": ws * 1_000_000,
+                                            "seq_len": 0, "parallelism": f"replicas{ws}"}
+    if not have_reference():
+        print(json.dumps({"impl": "reference", "metric": METRIC,
+                          "unavailable": "oracle/_ref/libwbfmm_ref.so was not built"}))
+        return
+    nthreads = min(os.cpu_count() or 1, 16)
+    if stream:
+        reqs = stream_cpu_sample()
+        points = sum(p.points for p in reqs)
+        sample = cpu_sample_text(reqs)
+
+        def step():
+            return run_reference_requests(reqs, nthreads)
+    else:
+        rp = reference_sample(2)
+        points = rp.points
+        sample = (f"{rp.ns} points in a 1/8-volume sub-cube of the workload, depth {rp.depth}, "
+                  f"orders {rp.order_s[1:]}, same density/k/box widths; reference FMM with M2L "
+                  "on GThreads (others serial)")
+
+        def step():
+            return run_reference_step(rp, nthreads)
+    for _ in range(args.warmup):
+        step()
+    times = [step() for _ in range(max(1, args.steps))]
+    t = float(np.mean(times))
+    v = points / t
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "points/s",
+        "n_gpus": args.gpus, "steps": len(times), "warmup": args.warmup,
+        "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfgd,
+        "cpu_baseline": {"value": v, "unit": "points/s", "cores": nthreads,
+                         "kind": "reference", "sample": sample},
+        "e2e": {"value": v, "unit": "points/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }))
+
+
+# ----------------------------------------------------- served stream
+def request_bytes(p):
+    """(input bytes, output bytes) of a request: sources (+ normals), their
+    strengths (+ dipole strengths), targets when they are not the sources;
+    potential and gradient in FP64."""
+    w = 2 if p.problem == 2 else 1
+    nin = 24 * p.ns + 8 * w * p.ns
+    if p.normals is not None:
+        nin += 24 * p.ns + 8 * w * p.ns
+    if not p.targets_are_sources:
+        nin += 24 * p.nt
+    return nin, 8 * 4 * w * p.nt
+
+
+def served_section(args, ws, rank, local):
+    """Served FP32 vs plain FP64 on batches of the mixed serving stream, with
+    device-resident requests (value) and host arrays (e2e)."""
     import torch
 
     from wbfmm_b200 import engine, workloads as W
 
     dev = torch.device("cuda", local)
-    torch.cuda.set_device(dev)
+    marker = torch.cuda.Stream(dev)          # span events (the slots run their own streams)
+    warm, batches, lat_reqs = stream_requests(args, rank)
+
+    def on_dev(p):
+        w = 2 if p.problem == W.HELMHOLTZ else 1
+
+        def t(a):
+            return None if a is None else torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+
+        return {"xs": t(p.xs), "q": t(p.q), "normals": t(p.normals), "dipoles": t(p.dipoles),
+                "xt": None if p.targets_are_sources else t(p.xt),
+                "pot": torch.empty(w * p.nt, dtype=torch.float64, device=dev),
+                "grad": torch.empty(3 * w * p.nt, dtype=torch.float64, device=dev)}
+
+    # device copies of every batch's inputs (and room for its fields), made
+    # before any timing
+    dev_warm = [[on_dev(p) for p in b] for b in warm]
+    dev_batches = [[on_dev(p) for p in b] for b in batches]
+    torch.cuda.synchronize(dev)
+
+    def served_prec(p):
+        ok = engine.fp32_range_ok(engine.SolverConfig.from_problem(p))
+        return engine.FP32 if ok else engine.FP64
+
+    def plain_prec(p):
+        return engine.FP64
+
+    def run_batch(srv, batch, dbatch, precf, skip, keep=0):
+        dist_barrier(ws)
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = srv.stats()["kernel_launches"]
+        e0.record(marker)
+        tk = [srv.submit(p, precf(p), skip_empty=skip, leaf_order=skip,
+                         device=d if dbatch is not None else None)
+              for p, d in zip(batch, dbatch if dbatch is not None else [None] * len(batch))]
+        srv.drain()
+        e1.record(marker)
+        e1.synchronize()
+        span = e0.elapsed_time(e1) * 1e-3
+        T = np.array([srv.times(t) for t in tk])
+        kept = []
+        for t in tk[:keep]:
+            pot, grad = srv.wait(t)
+            kept.append((pot.cpu().numpy() if hasattr(pot, "cpu") else pot.copy(),
+                         grad.cpu().numpy() if hasattr(grad, "cpu") else grad.copy()))
+        for t in tk:
+            srv.forget(t)
+        return (dist_max(span, ws), kept, srv.stats()["kernel_launches"] - l0,
+                float(np.mean(T[:, 2] - T[:, 1])), float(np.mean(T[:, 3] - T[:, 2])))
+
+    def run_arm(name, slots, precf, skip, device, keep=0):
+        with engine.Server(slots=slots) as srv:
+            for b, d in zip(warm, dev_warm):
+                run_batch(srv, b, d if device else None, precf, skip)
+            spans, launches, issue, wait = [], [], [], []
+            kept = None
+            with ClockSampler(local) as clk:
+                for i, (b, d) in enumerate(zip(batches, dev_batches)):
+                    span, k, nl, ti, tw = run_batch(srv, b, d if device else None, precf, skip,
+                                                    keep=keep if i == 0 else 0)
+                    spans.append(span)
+                    launches.append(nl)
+                    issue.append(ti)
+                    wait.append(tw)
+                    if k:
+                        kept = k
+            pts = sum(p.points for b in batches for p in b)
+            return {"points_per_s": ws * pts / sum(spans), "seconds": sum(spans),
+                    "ms_per_step": 1e3 * float(np.mean(spans)), "step_ms": [1e3 * s for s in spans],
+                    "requests": len(batches) * SERVE_BATCH, "slots": slots, "skip_empty": skip,
+                    "inputs": "device" if device else "host",
+                    "kernel_launches_per_step": int(np.mean(launches)),
+                    "host_issue_ms_per_request": 1e3 * float(np.mean(issue)),
+                    "device_wait_ms_per_request": 1e3 * float(np.mean(wait)),
+                    "clocks": clk.summary(), "stats": srv.stats()}, kept
+
+    out = {}
+    served_dev, _ = run_arm("served", SERVE_SLOTS, served_prec, True, True)
+    served_host, kept = run_arm("served", SERVE_SLOTS, served_prec, True, False, keep=8)
+    plain_dev, _ = run_arm("plain", 1, plain_prec, False, True)
+    plain_host, _ = run_arm("plain", 1, plain_prec, False, False)
+    plain_skip, _ = run_arm("plain_skip", 1, plain_prec, True, True)
+    out["served_fp32"] = {"device": served_dev, "host": served_host}
+    out["plain_fp64"] = {"device": plain_dev, "host": plain_host}
+    out["plain_fp64_skip_empty"] = {"device": plain_skip}
+
+    # latency under Poisson arrivals at fractions of each arm's own
+    # throughput (host arrays, as a caller submits)
+    mean_pts = np.mean([p.points for b in batches for p in b])
+
+    def run_latency(slots, precf, skip, rate, seed):
+        arr = W.poisson_arrivals(len(lat_reqs), rate, seed=seed + rank)
+        with engine.Server(slots=slots) as srv:
+            base = srv.clock() + 0.02
+            tk = [srv.submit(p, precf(p), arrival=base + a, skip_empty=skip, leaf_order=skip)
+                  for p, a in zip(lat_reqs, arr)]
+            srv.drain()
+            T = np.array([srv.times(t) for t in tk])
+        lat = T[:, 3] - T[:, 0]
+        return {"offered_requests_per_s": float(rate),
+                "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+                "mean_s": float(lat.mean()),
+                "achieved_points_per_s": float(sum(p.points for p in lat_reqs) /
+                                               (T[:, 3].max() - base))}
+
+    latency = {}
+    for name, slots, precf, skip, thr in (
+            ("served_fp32", SERVE_SLOTS, served_prec, True, served_host["points_per_s"]),
+            ("plain_fp64", 1, plain_prec, False, plain_host["points_per_s"])):
+        latency[name] = {}
+        for load in SERVE_LOADS:
+            rate = load * thr / ws / mean_pts
+            latency[name][f"{int(load * 100)}%"] = run_latency(slots, precf, skip, rate,
+                                                               104 + int(load * 100))
+    out["latency"] = latency
+
+    # accuracy of served fields against the FP64 direct sum
+    worst, checked = 0.0, []
+    for p, (pot, grad) in zip(batches[0][:8], kept or []):
+        idx = W.subsample(105, p.ns, 1000)
+        dpot, dgrad = engine.direct(p.problem, p.xs, p.q, p.xs[idx], k=p.k)
+        w = 2 if p.problem == W.HELMHOLTZ else 1
+        ep = engine.error_norms(pot.reshape(p.ns, w)[idx].ravel(), dpot)[0]
+        eg = engine.error_norms(grad.reshape(p.ns, 3 * w)[idx].ravel(), dgrad)[0]
+        worst = max(worst, ep, eg)
+        checked.append({"n": p.ns, "problem": "helmholtz" if p.problem == W.HELMHOLTZ else "laplace",
+                        "k": p.k, "fp32": served_prec(p) == engine.FP32,
+                        "pot_rel_l2": ep, "grad_rel_l2": eg})
+    out["accuracy"] = {"max_rel_l2": worst, "tolerance": 1e-6, "requests": checked,
+                       "reference": "FP64 GPU direct sum on 1000 targets per request"}
+    out["fp32_fraction"] = float(np.mean([served_prec(p) == engine.FP32
+                                          for b in batches for p in b]))
+    nin = sum(request_bytes(p)[0] for b in batches for p in b) // len(batches)
+    nout = sum(request_bytes(p)[1] for b in batches for p in b) // len(batches)
+    out["bytes_per_step"] = {"h2d": int(nin), "d2h": int(nout)}
+    return out
+
+
+# ------------------------------------------------- single-solve workloads
+def single_solve_section(args, ws, rank, local, p, n_acc, acc_seed, skip_empty, label, steps):
+    """One workload solved once per step by the FP32 and FP64 forms from
+    device-resident inputs (tree, FP64 tables, passes, evaluation, queued
+    with deferred checks), and by the FP32 form through the C ABI with pinned
+    host buffers (e2e)."""
+    import torch
+
+    from wbfmm_b200 import engine, workloads as W
+
+    dev = torch.device("cuda", local)
     stream = torch.cuda.Stream(dev)     # the solvers' stream; events on it
-    torch.cuda.set_stream(stream)
-    p, n_acc, acc_seed, skip_empty, label = workload(args, rank)
     helm = p.problem == W.HELMHOLTZ
     w = 2 if helm else 1
     ns, nt = p.ns, p.nt
@@ -497,7 +646,6 @@ def our_arm(args, ws, rank, local):
     def dev_arr(a):
         return None if a is None else torch.from_numpy(np.ascontiguousarray(a)).to(dev)
 
-    # device-resident inputs
     xs_d, q_d = dev_arr(p.xs), dev_arr(p.q)
     nrm_d, dip_d = dev_arr(p.normals), dev_arr(p.dipoles)
     xt_d = xs_d if p.targets_are_sources else dev_arr(p.xt)
@@ -513,8 +661,6 @@ def our_arm(args, ws, rank, local):
         return s
 
     def step(s):
-        # one whole solve queued on the stream: tree, operator tables,
-        # passes, evaluation (the domain checks are read by wait())
         s.set_sources(xs_d, nrm_d, on_device=True)
         s.set_strengths(q_d, dip_d, on_device=True)
         s.set_targets(xt_d, on_device=True)
@@ -524,45 +670,45 @@ def our_arm(args, ws, rank, local):
     results = {}
     for name, prec in (("fp64", engine.FP64), ("fp32", engine.FP32)):
         s = make(prec)
-        for _ in range(args.warmup):
+        for _ in range(max(3, args.warmup)):
             step(s)
         s.wait()
-        torch.cuda.synchronize()
+        torch.cuda.synchronize(dev)
         l0 = s.kernel_launches()
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-              for _ in range(args.steps)]
+              for _ in range(steps)]
         dist_barrier(ws)
-        torch.cuda.synchronize()
+        torch.cuda.synchronize(dev)
         with ClockSampler(local) as clk:
-            for i in range(args.steps):
-                flush.zero_()                       # L2 flush between steps
+            for i in range(steps):
+                with torch.cuda.stream(stream):
+                    flush.zero_()                   # L2 flush between steps
                 ev[i][0].record(stream)
                 step(s)
                 ev[i][1].record(stream)
-            torch.cuda.synchronize()
+            torch.cuda.synchronize(dev)
         s.wait()                                    # deferred checks of the last step
         dist_barrier(ws)
         step_ms = [a.elapsed_time(b) for a, b in ev]
-        ms = float(np.sum(step_ms)) / args.steps
-        ms = dist_max(ms, ws)
-        launches = (s.kernel_launches() - l0) // args.steps
-        # per-stage split and M2L per level (separate, untimed pass)
+        ms = dist_max(float(np.mean(step_ms)), ws)
+        launches = (s.kernel_launches() - l0) // steps
         stages = s.stage_times()
         m2l_ms = {}
         for lv in range(2, p.depth + 1):
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            flush.zero_()
+            with torch.cuda.stream(stream):
+                flush.zero_()
             a.record(stream)
             s.m2l(lv)
             b.record(stream)
-            torch.cuda.synchronize()
+            torch.cuda.synchronize(dev)
             m2l_ms[lv] = a.elapsed_time(b)
         pot, grad = s.field()
-        results[name] = dict(ms=ms, step_ms=step_ms, launches=launches, stages=stages, m2l_ms=m2l_ms,
-                             pot=pot, grad=grad, clocks=clk.summary())
+        results[name] = dict(ms=ms, step_ms=step_ms, launches=launches, stages=stages,
+                             m2l_ms=m2l_ms, pot=pot, grad=grad, clocks=clk.summary())
         if name == "fp64":
-            s.close()                      # room for the FP32 solver's buffers
-            torch.cuda.synchronize()
+            s.close()
+            torch.cuda.synchronize(dev)
         else:
             results[name]["solver"] = s
 
@@ -592,13 +738,16 @@ def our_arm(args, ws, rank, local):
     for _ in range(max(1, args.warmup)):
         e2e_step()
     dist_barrier(ws)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        flush.zero_()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
         e2e_step()
-    torch.cuda.synchronize()
-    e2e_s = dist_max((time.perf_counter() - t0) / args.steps, ws)
+    e1.record(stream)
+    e1.synchronize()
+    e2e_s = dist_max(e0.elapsed_time(e1) * 1e-3 / steps, ws)
     h2d = sum(t.numel() * 8 for t in (xs_h, q_h, nrm_h, dip_h) if t is not None)
     h2d += xt_h.numel() * 8     # targets are copied even when they are the sources
     e2e = {"value": ws * p.points / e2e_s, "unit": "points/s",
@@ -610,7 +759,6 @@ def our_arm(args, ws, rank, local):
     idx = W.subsample(acc_seed, nt, n_acc)
     dpot, dgrad = engine.direct(p.problem, p.xs, p.q, p.xt[idx], k=p.k,
                                 normals=p.normals, dipoles=p.dipoles)
-    # relative L2 / max errors by the engine's GPU FP64 reduction
     acc = {"targets_checked": int(len(idx)), "norms": "wbfmm_b200_error_norms"}
     for name in ("fp64", "fp32"):
         pot = results[name]["pot"].reshape(-1, w)[idx].ravel()
@@ -623,65 +771,193 @@ def our_arm(args, ws, rank, local):
         "pot_rel_l2": engine.error_norms(f32["pot"], f64["pot"])[0],
         "grad_rel_l2": engine.error_norms(f32["grad"], f64["grad"])[0]}
 
-    # roofline of the dominant kernel (M2L, FP32 form): algorithmic FLOPs of
-    # the rotate / coaxial / rotate-back shifts per launch / launch time
+    # the dominant kernel of the solve (M2L of its busiest level, FP32)
     pairs = list4_pairs(p.depth)
     lv_dom = max(f32["m2l_ms"], key=lambda lv: f32["m2l_ms"][lv])
     if skip_empty:
         pairs[lv_dom] = list4_pairs_at(p.xt, p.x0, p.D, lv_dom, p.xs)
     fpp = helm_flops_per_pair if helm else lap_flops_per_pair
     flops = pairs[lv_dom] * fpp(p.order_s[lv_dom])
-    achieved = flops / (f32["m2l_ms"][lv_dom] * 1e-3) / 1e12
-    peak_fp32 = 148 * 128 * 2 * 1.965e9 / 1e12
-    roofline = {"bound": "simt", "kernel": f"M2L level {lv_dom}, order {p.order_s[lv_dom]}, FP32",
-                "achieved": achieved, "peak": peak_fp32, "unit": "TFLOP/s",
-                "frac": achieved / peak_fp32, "traffic": None,
-                "peak_source": "nominal FP32 SIMT peak (148 SMs x 128 FMA/clk x 1.965 GHz); "
-                               "MEASURED_PEAKS.json holds no SIMT figure",
-                "algorithmic_flops_per_launch": flops,
-                "pairs": pairs[lv_dom], "order": p.order_s[lv_dom],
-                "pairs_counted": ("list-4 pairs of the boxes that hold targets with "
-                                  "source boxes that hold sources"
-                                  if skip_empty else "all list-4 pairs of the dense level")}
+    m2l = {"kernel": f"M2L level {lv_dom}, order {p.order_s[lv_dom]}, FP32",
+           "ms": f32["m2l_ms"][lv_dom], "algorithmic_flops_per_launch": flops,
+           "achieved_tflops": flops / (f32["m2l_ms"][lv_dom] * 1e-3) / 1e12,
+           "pairs": pairs[lv_dom],
+           "pairs_counted": ("list-4 pairs of the boxes that hold targets with "
+                             "source boxes that hold sources"
+                             if skip_empty else "all list-4 pairs of the dense level")}
+    return {
+        "workload": label, "points": p.points, "sources": ns, "targets": nt, "depth": p.depth,
+        "orders": p.order_s[1:], "k": p.k, "skip_empty": skip_empty,
+        "fp32": {"points_per_s": ws * p.points / (f32["ms"] * 1e-3), "ms_per_step": f32["ms"],
+                 "step_ms": f32["step_ms"], "stages_ms": f32["stages"], "m2l_ms": f32["m2l_ms"],
+                 "launches": int(f32["launches"]), "clocks": f32["clocks"]},
+        "fp64": {"points_per_s": ws * p.points / (f64["ms"] * 1e-3), "ms_per_step": f64["ms"],
+                 "step_ms": f64["step_ms"], "stages_ms": f64["stages"], "m2l_ms": f64["m2l_ms"],
+                 "clocks": f64["clocks"]},
+        "e2e_fp32": e2e, "accuracy": acc, "dominant_m2l": m2l,
+    }
 
+
+# -------------------------------------------------------------- roofline
+def tile_profile_traffic():
+    """DRAM bytes (read + write) of the tile M2L launch in the committed ncu
+    capture of the roofline case, or None."""
+    try:
+        text = open(TILE_PROFILE).read()
+    except OSError:
+        return None
+    tot = 0.0
+    for key in ("dram__bytes_read.sum", "dram__bytes_write.sum"):
+        for line in text.splitlines():
+            if f"`{key}`" in line:
+                val, unit = line.split("|")[2].split()
+                tot += float(val) * {"byte": 1, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9}[unit]
+                break
+        else:
+            return None
+    return tot
+
+
+def tile_roofline(local):
+    """The stream's dominant M2L kernel (the offset-major tile kernel at the
+    stream's Laplace order 14) on a dense level: 3e5 points, depth 5, level
+    5, FP32; algorithmic FLOPs of the rotate / coaxial / rotate-back shifts
+    per launch / CUDA-event launch time (L2 flushed before each), against
+    the FP32 FMA peak measured here."""
+    import torch
+
+    from wbfmm_b200 import engine
+
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(dev)
+    peak = engine.fp32_fma_peak()
+    p = _cube(engine.LAPLACE, 300_000, 5, 14)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    cfg = engine.SolverConfig.from_problem(p, engine.FP32)
+    with engine.Solver(cfg, stream=stream.cuda_stream) as s:
+        s.set_m2l_kernel(3)
+        s.set_sources(p.xs).set_strengths(p.q).set_targets(p.xt).run()
+        times = []
+        for i in range(6):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            a.record(stream)
+            s.m2l(5)
+            b.record(stream)
+            torch.cuda.synchronize(dev)
+            if i:
+                times.append(a.elapsed_time(b))
+    ms = float(np.mean(times))
+    flops = list4_pairs(5)[5] * lap_flops_per_pair(14)
+    achieved = flops / (ms * 1e-3) / 1e12
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    bf16 = peaks.get("bf16_tflops")
+    return {"bound": "simt", "kernel": "k_m2l_tiles<float, Laplace>: M2L of level 5, order 14, "
+                                       "300,000 points, depth 5",
+            "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+            "peak_source": "FP32 FMA throughput measured live (wbfmm_b200_fp32_fma_peak)",
+            "traffic": tile_profile_traffic(),
+            "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of the same launch, "
+                              "profiles/k_m2l_tiles_laplace_3e5_p14_level5.md",
+            "algorithmic_flops_per_launch": flops, "ms_per_launch": ms,
+            "frac_of_bf16_tensor_peak": (achieved / bf16) if bf16 else None}
+
+
+# ----------------------------------------------------------- our arm
+def our_arm(args, ws, rank, local):
+    import torch
+
+    from wbfmm_b200 import workloads as W
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    if args.workload != "stream":
+        p, n_acc, acc_seed, skip_empty, label = workload(args, rank)
+        sec = single_solve_section(args, ws, rank, local, p, n_acc, acc_seed, skip_empty,
+                                   label, args.steps)
+        cpu = None
+        if rank == 0 and ws == 1 and not args.no_cpu_baseline and args.workload == "cube":
+            from oracle.oracle_api import have_reference
+            if have_reference():
+                rp = reference_sample(2)
+                nthreads = min(os.cpu_count() or 1, 16)
+                t = run_reference_step(rp, nthreads)
+                cpu = {"value": rp.points / t, "unit": "points/s", "cores": nthreads,
+                       "kind": "reference",
+                       "sample": f"{rp.ns} points in a 1/8-volume sub-cube of the workload "
+                                 f"(depth {rp.depth}, same density, k and box widths), one solve"}
+        m = sec["dominant_m2l"]
+        from wbfmm_b200 import engine
+        peak = engine.fp32_fma_peak()
+        line = {
+            "metric": METRIC, "value": sec["fp32"]["points_per_s"], "unit": "points/s",
+            "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": sec["fp32"]["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": label, "global_batch": ws * p.points, "seq_len": 0,
+                       "parallelism": f"replicas{ws}", "l2": "256 MiB written between steps"},
+            "single_solve": sec, "e2e": sec["e2e_fp32"],
+            "roofline": {"bound": "simt", "kernel": m["kernel"], "achieved": m["achieved_tflops"],
+                         "peak": peak, "unit": "TFLOP/s", "frac": m["achieved_tflops"] / peak,
+                         "traffic": None,
+                         "peak_source": "FP32 FMA throughput measured live"},
+            "cpu_baseline": cpu, "gpu_launches": sec["fp32"]["launches"],
+            "clocks": sec["fp32"]["clocks"],
+        }
+        if rank == 0:
+            print(json.dumps(line))
+        return
+
+    served = served_section(args, ws, rank, local)
+    sd, sh = served["served_fp32"]["device"], served["served_fp32"]["host"]
+    pd, ph = served["plain_fp64"]["device"], served["plain_fp64"]["host"]
+    pskip = served["plain_fp64_skip_empty"]["device"]
+    lat = served["latency"]
+    cube = None
+    if not args.no_cube:
+        p, n_acc, acc_seed, skip_empty, label = W.helmholtz_cube(1_000_000, k=8.0, depth=6,
+                                                                 seed=2 + rank), 10_000, 102, \
+            False, CUBE_WORKLOAD
+        cube = single_solve_section(args, ws, rank, local, p, n_acc, acc_seed, skip_empty,
+                                    label, min(args.steps, 5))
+        for k in ("fp32", "fp64"):
+            cube[k].pop("step_ms", None)
+    roofline = tile_roofline(local)
     cpu = None
-    if rank == 0 and ws == 1 and not args.no_cpu_baseline and args.workload == "cube":
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         from oracle.oracle_api import have_reference
         if have_reference():
-            rp = reference_sample()
+            reqs = stream_cpu_sample(rank)
             nthreads = min(os.cpu_count() or 1, 16)
-            t = run_reference_step(rp, nthreads)
-            cpu = {"value": rp.points / t, "unit": "points/s", "cores": nthreads,
-                   "kind": "reference",
-                   "sample": f"{rp.ns} points in a 1/8-volume sub-cube of the workload "
-                             f"(depth {rp.depth}, same density, k and box widths), one solve"}
-
-    served = (served_section(args, ws, rank, local)
-              if not args.no_served and args.workload == "cube" else None)
-
-    v32 = ws * p.points / (f32["ms"] * 1e-3)
-    v64 = ws * p.points / (f64["ms"] * 1e-3)
+            t = run_reference_requests(reqs, nthreads)
+            cpu = {"value": sum(p.points for p in reqs) / t, "unit": "points/s",
+                   "cores": nthreads, "kind": "reference", "sample": cpu_sample_text(reqs)}
     line = {
-        "metric": METRIC, "value": v32, "unit": "points/s", "n_gpus": ws,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": f32["ms"],
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32", "data": "synthetic",
-        "config": {"workload": label, "global_batch": ws * p.points, "seq_len": 0,
-                   "parallelism": f"replicas{ws}", "points_per_gpu": p.points,
-                   "sources": ns, "targets": nt, "depth": p.depth,
-                   "orders": p.order_s[1:], "k": p.k, "skip_empty": skip_empty,
-                   "fp32_leaf_order": True,
-                   "l2": "256 MiB buffer written between timed steps"},
-        "step_ms": f32["step_ms"],
-        "plain_fp64": {"value": v64, "unit": "points/s", "ms_per_step": f64["ms"], "step_ms": f64["step_ms"],
-                       "stages_ms": f64["stages"], "m2l_ms": f64["m2l_ms"]},
-        "fp32_over_fp64": v32 / v64,
-        "stages_ms": f32["stages"], "m2l_ms": f32["m2l_ms"],
-        "accuracy": acc,
-        "served": served,
-        "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
-        "gpu_launches": int(f32["launches"]),
-        "clocks": f32["clocks"], "clocks_fp64": f64["clocks"],
+        "metric": METRIC, "value": sd["points_per_s"], "unit": "points/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sd["ms_per_step"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "config": stream_config(ws),
+        "served_over_plain": sd["points_per_s"] / pd["points_per_s"],
+        "served_over_plain_e2e": sh["points_per_s"] / ph["points_per_s"],
+        "served_over_plain_skip_empty": sd["points_per_s"] / pskip["points_per_s"],
+        "served_p50_s": lat["served_fp32"]["70%"]["p50_s"],
+        "served_p99_s": lat["served_fp32"]["70%"]["p99_s"],
+        "plain_p50_s": lat["plain_fp64"]["70%"]["p50_s"],
+        "plain_p99_s": lat["plain_fp64"]["70%"]["p99_s"],
+        "served_max_rel_l2": served["accuracy"]["max_rel_l2"],
+        "plain_fp64_points_per_s": pd["points_per_s"],
+        "fp32_fraction": served["fp32_fraction"],
+        "e2e": {"value": sh["points_per_s"], "unit": "points/s", "ms_per_step": sh["ms_per_step"],
+                "h2d_bytes_per_step": ws * served["bytes_per_step"]["h2d"],
+                "d2h_bytes_per_step": ws * served["bytes_per_step"]["d2h"]},
+        "roofline": roofline, "cpu_baseline": cpu,
+        "gpu_launches": sd["kernel_launches_per_step"], "clocks": sd["clocks"],
+        "served": served, "cube_c2": cube,
     }
     if rank == 0:
         print(json.dumps(line))
@@ -696,14 +972,15 @@ def main():
     ap.add_argument("--points", type=int, default=1_000_000)
     ap.add_argument("--depth", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-served", action="store_true")
+    ap.add_argument("--no-cube", action="store_true",
+                    help="stream workload: leave out the 1e6-point cube single solves")
     ap.add_argument("--profile-case", default=None,
                     help="run one small profiling case instead of the benchmark "
                          "(see PROFILE_CASES)")
-    ap.add_argument("--workload", default="cube",
-                    choices=["cube", "laplace_c1", "sphere_c3", "clusters_c5"],
-                    help="cube (default): 1e6 Helmholtz cube + served stream; the others "
-                         "measure the benchmark's further configurations")
+    ap.add_argument("--workload", default="stream",
+                    choices=["stream", "cube", "laplace_c1", "sphere_c3", "clusters_c5"],
+                    help="stream (default): the served-vs-plain serving stream; the others "
+                         "measure single solves of the benchmark's further configurations")
     args = ap.parse_args()
     if args.profile_case:
         profile_case(args.profile_case)

@@ -155,6 +155,12 @@ int wbfmm_b200_laplace_curl(wbfmm_b200_solver_t *s, const double *q3, int qstr,
 int wbfmm_b200_selftest_sincos(double xmax, int n, double *err2);
 int wbfmm_b200_synchronize(wbfmm_b200_solver_t *s);
 
+/* Measured FP32 FMA throughput of the current GPU (TFLOP/s, 2 flops per
+   FMA; best of three timed launches of a register-only FMA kernel over
+   every SM): the peak that the roofline fractions of the engine's SIMT
+   kernels are quoted against.  Allocates and synchronises. */
+int wbfmm_b200_fp32_fma_peak(double *tflops);
+
 /* Results in ORIGINAL target order.  pot: Laplace [n], Helmholtz [2n];
    grad: Laplace [3n], Helmholtz [6n] (d/dx re, im, d/dy re, im, d/dz re,
    im).  Host pointers unless on_device. */
@@ -282,9 +288,9 @@ int wbfmm_b200_fp32_range_ok(const wbfmm_b200_config_t *cfg);
    (per slot hbm_budget / (4 nslots), at most 4 GB; a slot whose buffers
    grow past it releases them).  Operator tables are shared across solves (per order; Helmholtz
    coaxial tables per (k * box width, order)).  Inputs and outputs are host
-   arrays that the caller keeps alive until the request completes; fields
-   come back in FP64 in the layouts of wbfmm_b200_get_field.  All calls are
-   thread-safe.
+   arrays (or device arrays, with on_device) that the caller keeps alive
+   until the request completes; fields come back in FP64 in the layouts of
+   wbfmm_b200_get_field.  All calls are thread-safe.
    ------------------------------------------------------------------------ */
 typedef struct wbfmm_b200_server wbfmm_b200_server_t;
 
@@ -301,6 +307,9 @@ typedef struct {
   double *grad;             /* [3 w ntgt] or NULL */
   double arrival;           /* server-clock seconds before which the request
                                is not started (0: on submission) */
+  int on_device;            /* 1: xs, q, normals, dipoles, xt, pot and grad
+                               are device pointers (no host staging; the
+                               fields are written there in place) */
 } wbfmm_b200_request_t;
 
 int wbfmm_b200_server_create(wbfmm_b200_server_t **srv, int nslots,
@@ -327,8 +336,8 @@ int wbfmm_b200_server_forget(wbfmm_b200_server_t *srv, int64_t ticket);
 /* blocks until the queue is empty and no solve is running */
 int wbfmm_b200_server_drain(wbfmm_b200_server_t *srv);
 /* completed requests, peak bytes in flight, peak solves in flight, table
-   cache hits, misses and bytes */
-int wbfmm_b200_server_stats(wbfmm_b200_server_t *srv, int64_t *out6);
+   cache hits, misses and bytes, kernels launched by completed solves */
+int wbfmm_b200_server_stats(wbfmm_b200_server_t *srv, int64_t *out7);
 
 #ifdef __cplusplus
 }

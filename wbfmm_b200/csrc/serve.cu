@@ -44,6 +44,7 @@ struct Req {
   int64_t footprint = 0;
   double t_arrival = 0, t_start = 0, t_queued = 0, t_end = 0;   // server clock
   int state = 0;                                   // 0 queued, 1 running, 2 done
+  int64_t launches = 0;                            // kernels its solve launched
   int status = 0;
   char error[256] = "";
 };
@@ -93,6 +94,7 @@ struct wbfmm_b200_server {
   std::deque<Req*> queue;                     // ordered by arrival time
   std::unordered_map<int64_t, Req*> reqs;
   int64_t next_id = 1, inflight = 0, peak_inflight = 0, completed = 0;
+  int64_t launches = 0;                       // kernels of completed solves
   int running = 0, peak_running = 0;
   bool stop = false;
 
@@ -135,11 +137,24 @@ struct wbfmm_b200_server {
   }
 
   // one solve on the slot's stream; fields land in the caller's arrays
+  // (host arrays through the slot's pinned staging, or device arrays)
   template <typename T>
   int execute(Slot* s, Solver<T>* sv, const wbfmm_b200_request_t& r, double* t_queued) {
     const int w = r.cfg.problem == WBFMM_B200_HELMHOLTZ ? 2 : 1;
     const size_t ns = (size_t)r.nsrc, nt = (size_t)r.ntgt;
     const bool same = r.xt == r.xs && r.ntgt == r.nsrc;
+    const size_t np = r.pot ? w * nt : 0, ng = r.grad ? 3 * w * nt : 0;
+    if (r.on_device) {
+      WBFMM_TRY(sv->set_sources((int)ns, r.xs, 3, r.normals, 3, 1));
+      WBFMM_TRY(sv->set_strengths(r.q, w, r.dipoles, w, 1));
+      WBFMM_TRY(sv->set_targets((int)nt, r.xt, 3, 1));
+      WBFMM_TRY(sv->run_async());
+      WBFMM_TRY(sv->fetch_async(r.pot, r.grad, cudaMemcpyDeviceToDevice));
+      WBFMM_CUDA(cudaEventRecord(s->done, s->stream));
+      *t_queued = clock();
+      WBFMM_CUDA(cudaEventSynchronize(s->done));
+      return sv->check_flags();
+    }
     size_t need = 3 * ns + (r.q ? w * ns : 0) + (r.normals ? 3 * ns : 0) +
                   (r.dipoles ? w * ns : 0) + (same ? 0 : 3 * nt);
     WBFMM_TRY(s->in.reserve(need));
@@ -156,13 +171,13 @@ struct wbfmm_b200_server {
     const double* nrm = stage(r.normals, 3 * ns);
     const double* dip = stage(r.dipoles, w * ns);
     const double* xt = same ? xs : stage(r.xt, 3 * nt);
-    const size_t np = r.pot ? w * nt : 0, ng = r.grad ? 3 * w * nt : 0;
     WBFMM_TRY(s->out.reserve(np + ng));
     WBFMM_TRY(sv->set_sources((int)ns, xs, 3, nrm, 3, 0));
     WBFMM_TRY(sv->set_strengths(q, w, dip, w, 0));
     WBFMM_TRY(sv->set_targets((int)nt, xt, 3, 0));
     WBFMM_TRY(sv->run_async());
-    WBFMM_TRY(sv->fetch_async(np ? s->out.p : nullptr, ng ? s->out.p + np : nullptr));
+    WBFMM_TRY(sv->fetch_async(np ? s->out.p : nullptr, ng ? s->out.p + np : nullptr,
+                              cudaMemcpyDeviceToHost));
     WBFMM_CUDA(cudaEventRecord(s->done, s->stream));
     *t_queued = clock();
     WBFMM_CUDA(cudaEventSynchronize(s->done));
@@ -175,6 +190,7 @@ struct wbfmm_b200_server {
   int run_one(Slot* s, Req* q) {
     const wbfmm_b200_request_t& r = q->r;
     int rc;
+    const int64_t l0 = (s->s32 ? s->s32->launches : 0) + (s->s64 ? s->s64->launches : 0);
     if (r.cfg.precision == WBFMM_B200_FP32) {
       rc = make_solver(s, &r.cfg, &s->s32);
       if (!rc) rc = execute(s, s->s32, r, &q->t_queued);
@@ -182,6 +198,7 @@ struct wbfmm_b200_server {
       rc = make_solver(s, &r.cfg, &s->s64);
       if (!rc) rc = execute(s, s->s64, r, &q->t_queued);
     }
+    q->launches = (s->s32 ? s->s32->launches : 0) + (s->s64 ? s->s64->launches : 0) - l0;
     if (rc) {
       // drain whatever was queued before the failure
       cudaStreamSynchronize(s->stream);
@@ -240,6 +257,7 @@ struct wbfmm_b200_server {
         inflight -= q->footprint;
         running--;
         completed++;
+        launches += q->launches;
       }
       cv_done.notify_all();
       cv_work.notify_all();
@@ -391,6 +409,7 @@ int wbfmm_b200_server_drain(wbfmm_b200_server_t* srv) {
 
 int wbfmm_b200_server_stats(wbfmm_b200_server_t* srv, int64_t* out6) {
   if (!srv || !out6) return set_error(WBFMM_B200_E_ARG, "null argument");
+  int64_t* out7 = out6;
   std::lock_guard<std::mutex> lk(srv->mu);
   std::lock_guard<std::mutex> lc(srv->cache.mu);
   out6[0] = srv->completed;
@@ -399,6 +418,7 @@ int wbfmm_b200_server_stats(wbfmm_b200_server_t* srv, int64_t* out6) {
   out6[3] = srv->cache.hits;
   out6[4] = srv->cache.misses;
   out6[5] = (int64_t)srv->cache.coax_bytes;
+  out7[6] = srv->launches;
   return 0;
 }
 

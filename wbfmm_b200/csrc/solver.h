@@ -1011,8 +1011,9 @@ struct Solver : public wbfmm_b200_solver {
   }
 
   // Served form: queue the copies of the fields (FP64, original target
-  // order) into pinned host arrays, and of the domain-check flags.
-  int fetch_async(double* hpot, double* hgrad) {
+  // order) into pinned host arrays (kind cudaMemcpyDeviceToHost) or device
+  // arrays (cudaMemcpyDeviceToDevice), and of the domain-check flags.
+  int fetch_async(double* hpot, double* hgrad, cudaMemcpyKind kind) {
     const int w = helm ? 2 : 1;
     const size_t np = hpot ? (size_t)ntgt * w : 0;
     const size_t ng = hgrad ? (size_t)ntgt * 3 * w : 0;
@@ -1028,8 +1029,8 @@ struct Solver : public wbfmm_b200_solver {
       fg = out64.p + np;
       launches += (np ? 1 : 0) + (ng ? 1 : 0);
     }
-    if (np) WBFMM_CUDA(cudaMemcpyAsync(hpot, fp, sizeof(double) * np, cudaMemcpyDeviceToHost, stream));
-    if (ng) WBFMM_CUDA(cudaMemcpyAsync(hgrad, fg, sizeof(double) * ng, cudaMemcpyDeviceToHost, stream));
+    if (np) WBFMM_CUDA(cudaMemcpyAsync(hpot, fp, sizeof(double) * np, kind, stream));
+    if (ng) WBFMM_CUDA(cudaMemcpyAsync(hgrad, fg, sizeof(double) * ng, kind, stream));
     if (async_checks && hflag)
       WBFMM_CUDA(cudaMemcpyAsync(hflag, flag.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, stream));
     return 0;

@@ -54,7 +54,7 @@ class Request(C.Structure):
         ("cfg", Config), ("nsrc", C.c_int), ("xs", C.c_void_p),
         ("q", C.c_void_p), ("normals", C.c_void_p), ("dipoles", C.c_void_p),
         ("ntgt", C.c_int), ("xt", C.c_void_p), ("pot", C.c_void_p),
-        ("grad", C.c_void_p), ("arrival", C.c_double),
+        ("grad", C.c_void_p), ("arrival", C.c_double), ("on_device", C.c_int),
     ]
 
 
@@ -93,6 +93,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "wbfmm_b200_wait": (ip, [vp]),
         "wbfmm_b200_set_deferred_checks": (ip, [vp, ip]),
         "wbfmm_b200_selftest_sincos": (ip, [C.c_double, ip, dp]),
+        "wbfmm_b200_fp32_fma_peak": (ip, [dp]),
         "wbfmm_b200_error_norms": (ip, [C.c_int64, vp, vp, ip, dp]),
         "wbfmm_b200_laplace_curl": (ip, [vp, vp, ip, vp, ip]),
         "wbfmm_b200_synchronize": (ip, [vp]),
@@ -401,6 +402,13 @@ def selftest_sincos(xmax: float, n: int):
     return float(err[0]), float(err[1])
 
 
+def fp32_fma_peak() -> float:
+    """Measured FP32 FMA throughput of the current GPU, TFLOP/s."""
+    t = C.c_double()
+    _check(load_library().wbfmm_b200_fp32_fma_peak(C.byref(t)))
+    return float(t.value)
+
+
 def device_count() -> int:
     return int(load_library().wbfmm_b200_device_count())
 
@@ -455,12 +463,28 @@ class Server:
 
     def submit(self, p, precision=FP32, field=POTENTIAL | GRADIENT,
                arrival: float = 0.0, skip_empty: bool = False,
-               leaf_order: bool = False) -> int:
+               leaf_order: bool = False, device: dict | None = None) -> int:
         """Queue one solve; skip_empty: no local expansions for boxes
         without targets (the fields at the targets are unchanged);
-        leaf_order: sources sorted by leaf box only."""
+        leaf_order: sources sorted by leaf box only.  With ``device`` (a dict
+        of device arrays -- objects with ``data_ptr()`` -- under the keys
+        xs, q, normals, dipoles, xt, pot, grad, absent or None where unused)
+        the request reads and writes those instead of host arrays; the
+        caller keeps them alive until the request completes."""
         cfg = SolverConfig.from_problem(p, precision, field, skip_empty, leaf_order)
         w = 2 if p.problem == HELMHOLTZ else 1
+        if device is not None:
+            d = {k: device.get(k) for k in ("xs", "q", "normals", "dipoles", "xt", "pot", "grad")}
+            if d["xt"] is None:
+                d["xt"] = d["xs"]
+            r = Request(cfg.to_c(), p.ns, _addr(d["xs"]), _addr(d["q"]), _addr(d["normals"]),
+                        _addr(d["dipoles"]), p.nt, _addr(d["xt"]),
+                        _addr(d["pot"]) if field & POTENTIAL else None,
+                        _addr(d["grad"]) if field & GRADIENT else None, float(arrival), 1)
+            t = C.c_int64()
+            _check(self._lib.wbfmm_b200_server_submit(self._h, C.byref(r), C.byref(t)))
+            self._held[t.value] = (d, None, None, None, None, d["pot"], d["grad"])
+            return t.value
         xs = _host(p.xs)
         xt = xs if p.targets_are_sources else _host(p.xt)
         q, nrm, dip = _host(p.q), _host(p.normals), _host(p.dipoles)
@@ -469,7 +493,7 @@ class Server:
         grad = np.zeros(nt * 3 * w) if field & GRADIENT else None
         r = Request(cfg.to_c(), xs.shape[0], _addr(xs), _addr(q), _addr(nrm),
                     _addr(dip), nt, _addr(xt), _addr(pot), _addr(grad),
-                    float(arrival))
+                    float(arrival), 0)
         t = C.c_int64()
         _check(self._lib.wbfmm_b200_server_submit(self._h, C.byref(r), C.byref(t)))
         self._held[t.value] = (xs, xt, q, nrm, dip, pot, grad)
@@ -502,8 +526,9 @@ class Server:
         _check(self._lib.wbfmm_b200_server_drain(self._h))
 
     def stats(self) -> dict:
-        a = (C.c_int64 * 6)()
+        a = (C.c_int64 * 7)()
         _check(self._lib.wbfmm_b200_server_stats(self._h, a))
         keys = ("completed", "peak_bytes_in_flight", "peak_solves_in_flight",
-                "table_cache_hits", "table_cache_misses", "table_cache_bytes")
+                "table_cache_hits", "table_cache_misses", "table_cache_bytes",
+                "kernel_launches")
         return dict(zip(keys, (int(x) for x in a)))
