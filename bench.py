@@ -581,6 +581,7 @@ def served_section(args, ws, rank, local):
     def run_latency(slots, precf, skip, rate, seed):
         arr = W.poisson_arrivals(len(lat_reqs), rate, seed=seed + rank)
         with engine.Server(slots=slots) as srv:
+            run_batch(srv, warm[0], None, precf, skip)     # steady state: pools, tables
             base = srv.clock() + 0.02
             tk = [srv.submit(p, precf(p), arrival=base + a, skip_empty=skip, leaf_order=skip)
                   for p, a in zip(lat_reqs, arr)]

@@ -286,8 +286,9 @@ int wbfmm_b200_fp32_range_ok(const wbfmm_b200_config_t *cfg);
    wbfmm_b200_footprint of the solves in flight stays within `hbm_budget`
    bytes less the slots' allowance for keeping work buffers between solves
    (per slot hbm_budget / (4 nslots), at most 4 GB; a slot whose buffers
-   grow past it releases them).  Operator tables are shared across solves (per order; Helmholtz
-   coaxial tables per (k * box width, order)).  Inputs and outputs are host
+   grow past it releases them).  The order-only operator tables (rotations,
+   shift phases, Laplace coaxial tables) are shared across solves; Helmholtz
+   coaxial tables (which depend on k) are built per solve.  Inputs and outputs are host
    arrays (or device arrays, with on_device) that the caller keeps alive
    until the request completes; fields come back in FP64 in the layouts of
    wbfmm_b200_get_field.  All calls are thread-safe.
@@ -335,8 +336,9 @@ int wbfmm_b200_server_times(wbfmm_b200_server_t *srv, int64_t ticket,
 int wbfmm_b200_server_forget(wbfmm_b200_server_t *srv, int64_t ticket);
 /* blocks until the queue is empty and no solve is running */
 int wbfmm_b200_server_drain(wbfmm_b200_server_t *srv);
-/* completed requests, peak bytes in flight, peak solves in flight, table
-   cache hits, misses and bytes, kernels launched by completed solves */
+/* completed requests, peak bytes in flight, peak solves in flight, lookups
+   of the shared order-only tables served by an existing set and building a
+   new one, the sets' device bytes, kernels launched by completed solves */
 int wbfmm_b200_server_stats(wbfmm_b200_server_t *srv, int64_t *out7);
 
 #ifdef __cplusplus

@@ -682,16 +682,18 @@ __device__ __forceinline__ void sincos_near(float x, float* sp, float* cp) {
   *cp = co;
 }
 
-// the terms of one (target, source) pair added to acc[0..] (Helmholtz: pot
-// re, im, then grad x re, x im, y, z; Laplace: pot, grad x, y, z)
+// The terms of one (target, source) pair at separation r = (rx, ry, rz)
+// (|r|^2 = r2) added to acc[0..] (Helmholtz: pot re, im, then grad x re,
+// x im, y, z; Laplace: pot, grad x, y, z), without the kernels' constant
+// factors, which the caller applies once per target (p2p_scale): 1/(4 pi)
+// on the potential, -k/(4 pi) (Helmholtz) and 1/(4 pi) (Laplace) on the
+// gradient.
 template <typename T, bool HELM, int NT, bool want_pot, bool want_grad>
 __device__ __forceinline__ void p2p_pair(const P2PTile<T, HELM, NT>& tl, int j, T rx, T ry, T rz,
-                                         T k, T kinv, bool hd, T* acc) {
-  const T f4pi = T(0.25 / kPi);
-  const T r2 = rx * rx + ry * ry + rz * rz;
+                                         T r2, T k, T kinv, bool hd, T* acc) {
   const T ir = rsqrt(r2);
-  const T r = r2 * ir;
   if (HELM) {
+    const T r = r2 * ir;
     T kr = k * r, ikr, sn, cs;
     if constexpr (sizeof(T) == 4) {
       ikr = ir * kinv;
@@ -700,23 +702,26 @@ __device__ __forceinline__ void p2p_pair(const P2PTile<T, HELM, NT>& tl, int j, 
       ikr = ir / k;
       sincos(kr, &sn, &cs);
     }
+    // h0 = e^{ikr} / (i k r), h1 = h0 / (i k r) - ... (the first-order
+    // spherical Hankel function), so that grad h0(kr) = -k h1 r / r
     const T h0r = sn * ikr, h0i = -cs * ikr;
-    const T h1r = h0r * ikr + h0i, h1i = h0i * ikr - h0r;
+    const T h1r = fma(h0r, ikr, h0i), h1i = fma(h0i, ikr, -h0r);
     const T qr = tl.q[2 * j], qi = tl.q[2 * j + 1];
     if (want_pot) {
-      T fr = (h0r * qr - h0i * qi) * f4pi, fi = (h0i * qr + h0r * qi) * f4pi;
+      acc[0] = fma(h0r, qr, fma(-h0i, qi, acc[0]));
+      acc[1] = fma(h0i, qr, fma(h0r, qi, acc[1]));
       if (hd) {
-        T nr = (rx * tl.nx[j] + ry * tl.ny[j] + rz * tl.nz[j]) * ir;
-        T dr = tl.d[2 * j] * nr, di = tl.d[2 * j + 1] * nr;
-        fr -= k * (h1r * dr - h1i * di) * f4pi;
-        fi -= k * (h1r * di + h1i * dr) * f4pi;
+        const T nr = (rx * tl.nx[j] + ry * tl.ny[j] + rz * tl.nz[j]) * ir;
+        const T dr = tl.d[2 * j] * nr, di = tl.d[2 * j + 1] * nr;
+        acc[0] -= k * (h1r * dr - h1i * di);
+        acc[1] -= k * (h1r * di + h1i * dr);
       }
-      acc[0] += fr; acc[1] += fi;
     }
     if (want_grad) {
-      const T ar = -k * (h1r * qr - h1i * qi) * f4pi * ir;
-      const T ai = -k * (h1r * qi + h1i * qr) * f4pi * ir;
-      T gr[3] = {ar * rx, ar * ry, ar * rz}, gi[3] = {ai * rx, ai * ry, ai * rz};
+      const T ar = (h1r * qr - h1i * qi) * ir, ai = (h1r * qi + h1i * qr) * ir;
+      acc[2] = fma(ar, rx, acc[2]); acc[3] = fma(ai, rx, acc[3]);
+      acc[4] = fma(ar, ry, acc[4]); acc[5] = fma(ai, ry, acc[5]);
+      acc[6] = fma(ar, rz, acc[6]); acc[7] = fma(ai, rz, acc[7]);
       if (hd) {
         const T nxs = tl.nx[j], nys = tl.ny[j], nzs = tl.nz[j];
         const T nr = rx * nxs + ry * nys + rz * nzs;
@@ -727,35 +732,40 @@ __device__ __forceinline__ void p2p_pair(const P2PTile<T, HELM, NT>& tl, int j, 
         for (int c = 0; c < 3; c++) {
           T ur = dpr * k * nr * rv[c] * ir2 + h1r * (nv[c] * ir - nr * rv[c] * ir2 * ir);
           T ui = dpi * k * nr * rv[c] * ir2 + h1i * (nv[c] * ir - nr * rv[c] * ir2 * ir);
-          gr[c] += -k * (ur * dr - ui * di) * f4pi;
-          gi[c] += -k * (ur * di + ui * dr) * f4pi;
+          acc[2 + 2 * c] += ur * dr - ui * di;
+          acc[3 + 2 * c] += ur * di + ui * dr;
         }
       }
-      for (int c = 0; c < 3; c++) { acc[2 + 2 * c] += gr[c]; acc[3 + 2 * c] += gi[c]; }
     }
   } else {
     const T q = tl.q[j];
-    const T g = f4pi * ir;
     const T ir2 = ir * ir;
     if (want_pot) {
       T v = q;
       if (hd) v += tl.d[j] * (rx * tl.nx[j] + ry * tl.ny[j] + rz * tl.nz[j]) * ir2;
-      acc[0] += v * g;
+      acc[0] = fma(v, ir, acc[0]);
     }
     if (want_grad) {
-      const T gq = -q * g * ir2;
-      T gv[3] = {gq * rx, gq * ry, gq * rz};
+      const T ir3 = ir * ir2;
+      const T gq = -q * ir3;
+      acc[1] = fma(gq, rx, acc[1]); acc[2] = fma(gq, ry, acc[2]); acc[3] = fma(gq, rz, acc[3]);
       if (hd) {
         const T nxs = tl.nx[j], nys = tl.ny[j], nzs = tl.nz[j];
         const T nr = rx * nxs + ry * nys + rz * nzs;
-        const T ad = tl.d[j] * g * ir2;
-        gv[0] += ad * (nxs - T(3) * nr * rx * ir2);
-        gv[1] += ad * (nys - T(3) * nr * ry * ir2);
-        gv[2] += ad * (nzs - T(3) * nr * rz * ir2);
+        const T ad = tl.d[j] * ir3;
+        acc[1] += ad * (nxs - T(3) * nr * rx * ir2);
+        acc[2] += ad * (nys - T(3) * nr * ry * ir2);
+        acc[3] += ad * (nzs - T(3) * nr * rz * ir2);
       }
-      acc[1] += gv[0]; acc[2] += gv[1]; acc[3] += gv[2];
     }
   }
+}
+
+// the constant factor of accumulator c of p2p_pair (see there)
+template <bool HELM>
+__device__ __forceinline__ double p2p_scale(int c, double k) {
+  const double f4pi = 0.25 / kPi;
+  return HELM ? (c < 2 ? f4pi : -k * f4pi) : f4pi;
 }
 
 // POT / GRAD: the fields computed, fixed at compile time (dipoles at run time)
@@ -855,8 +865,9 @@ k_p2p(EvalParams<T> p) {
               const T rx = (T)((txh - cx.x) + (txl - cx.y));
               const T ry = (T)((tyh - cy.x) + (tyl - cy.y));
               const T rz = (T)((tzh - cz.x) + (tzl - cz.y));
-              if (rx * rx + ry * ry + rz * rz > rc2)
-                p2p_pair<T, HELM, NT, POT, GRAD>(tl, j, rx, ry, rz, k, kinv, hd, acc);
+              const T r2 = rx * rx + ry * ry + rz * rz;
+              if (r2 > rc2)
+                p2p_pair<T, HELM, NT, POT, GRAD>(tl, j, rx, ry, rz, r2, k, kinv, hd, acc);
             }
           }
           for (int c = 0; c < NA; c++) a[c] += (double)acc[c];
@@ -865,10 +876,11 @@ k_p2p(EvalParams<T> p) {
         for (int j = gl; j < nt; j += G) {
           // separation formed in FP64, the rest in T
           const T rx = (T)(x - tl.x[j]), ry = (T)(y - tl.y[j]), rz = (T)(z - tl.z[j]);
-          if (!(rx * rx + ry * ry + rz * rz > rc2)) continue;
+          const T r2 = rx * rx + ry * ry + rz * rz;
+          if (!(r2 > rc2)) continue;
           T acc[NA];
           for (int c = 0; c < NA; c++) acc[c] = T(0);
-          p2p_pair<T, HELM, NT, POT, GRAD>(tl, j, rx, ry, rz, k, kinv, hd, acc);
+          p2p_pair<T, HELM, NT, POT, GRAD>(tl, j, rx, ry, rz, r2, k, kinv, hd, acc);
           for (int c = 0; c < NA; c++) a[c] += (double)acc[c];
         }
       }
@@ -878,6 +890,7 @@ k_p2p(EvalParams<T> p) {
     for (int c = 0; c < NA; c++) {
       v[c] = a[c];
       for (int o = 1; o < G; o <<= 1) v[c] += __shfl_xor_sync(0xffffffffu, v[c], o);
+      v[c] *= p2p_scale<HELM>(c, (double)p.k);
     }
     if (!active || gl != 0) continue;
     const uint32_t o = p.tperm[jt];

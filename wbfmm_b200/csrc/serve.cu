@@ -10,8 +10,9 @@
 // solve -- tree build, passes, evaluation, copy-back -- on its stream with no
 // host wait, then sleeps on a blocking event until the stream drains, so
 // up to S solves run on the device at once and their kernels overlap.
-// Operator tables are shared between slots through a TableCache (rotation
-// and Laplace tables per order, Helmholtz coaxial tables per (k w, order)).
+// The order-only operator tables (rotations, shift phases, Laplace coaxial
+// tables) are shared between slots through a TableCache; each Helmholtz
+// solve builds its own coaxial tables (they depend on its k).
 //
 // Callers keep a request's input and output arrays alive until the request
 // has completed (wbfmm_b200_server_wait / _poll).
@@ -207,11 +208,9 @@ struct wbfmm_b200_server {
     // a slot keeps its work buffers for the next solve (no allocation then)
     // while they stay within its allowance; a failed solve releases them
     if (s->s32) {
-      s->s32->release_cache_refs();
       if (rc || (int64_t)s->s32->buffer_bytes() > keep) s->s32->release_buffers();
     }
     if (s->s64) {
-      s->s64->release_cache_refs();
       if (rc || (int64_t)s->s64->buffer_bytes() > keep) s->s64->release_buffers();
     }
     return rc;
@@ -417,7 +416,7 @@ int wbfmm_b200_server_stats(wbfmm_b200_server_t* srv, int64_t* out6) {
   out6[2] = srv->peak_running;
   out6[3] = srv->cache.hits;
   out6[4] = srv->cache.misses;
-  out6[5] = (int64_t)srv->cache.coax_bytes;
+  out6[5] = (int64_t)srv->cache.bytes;
   out7[6] = srv->launches;
   return 0;
 }

@@ -223,13 +223,12 @@ struct Solver : public wbfmm_b200_solver {
   int64_t hstride = 0;
   DBuf<int> op_ith, op_dist;
   DBuf<T> op_r, op_ph, op_ch;
-  DBuf<double> coax64[kMaxDepth + 1];   // Helmholtz: SR (15) for M2L
-  DBuf<T> coaxSR[kMaxDepth + 1];
+  // Helmholtz coaxial tables of every level, one set (helm_coaxial_set)
+  DBuf<double> coax_set64;
+  DBuf<T> coax_set;
   int64_t sr_stride[kMaxDepth + 1] = {0};
   const T* sr_ptr[kMaxDepth + 1] = {nullptr};   // (S|R) table per level
   const T* ss_ptr[kMaxDepth + 1] = {nullptr};   // (R|R) table per level
-  DBuf<double> ss64[kMaxDepth + 1];
-  DBuf<T> coaxSS[kMaxDepth + 1];
   DBuf<double> lap64[3];
   DBuf<T> lap[3];
   int lt = 0;
@@ -247,7 +246,6 @@ struct Solver : public wbfmm_b200_solver {
   bool events = false;
   // served form: shared tables, no host waits inside a solve
   TableCache* cache = nullptr;
-  std::vector<TableCache::Coax*> held;   // cache entries this solve reads
   bool async_checks = false;   // domain checks read back after the solve
   int* hflag = nullptr;        // pinned copy of flag[0..1]
   cudaMemPool_t lib_pool = nullptr;
@@ -271,8 +269,8 @@ struct Solver : public wbfmm_b200_solver {
     for (int l = 0; l <= kMaxDepth; l++) {
       f(box_i[l]); f(box_n[l]); f(mps[l]); f(mpr[l]); f(tmask[l]);
       f(act[l]); f(act_n[l]);
-      f(coax64[l]); f(coaxSR[l]); f(ss64[l]); f(coaxSS[l]);
     }
+    f(coax_set64); f(coax_set);
     f(tpts_in); f(tx); f(ty); f(tz); f(tkeys); f(tperm); f(tbox);
     f(tstart); f(tcount); f(flag); f(pot); f(grad); f(out64);
     f(H64); f(H); f(op_ith); f(op_dist); f(op_r); f(op_ph); f(op_ch);
@@ -282,7 +280,6 @@ struct Solver : public wbfmm_b200_solver {
 
   ~Solver() override {
     if (gexec) cudaGraphExecDestroy(gexec);
-    release_cache_refs();
     const bool trim = lib_pool && flag.pool == lib_pool;
     each_buf([](auto& b) { b.release(); });
     if (stream) cudaStreamSynchronize(stream);
@@ -293,11 +290,6 @@ struct Solver : public wbfmm_b200_solver {
       for (int i = 0; i < 8; i++) cudaEventDestroy(ev[i]);
     if (hflag) cudaFreeHost(hflag);
     if (own_stream && stream) cudaStreamDestroy(stream);
-  }
-
-  void release_cache_refs() {
-    for (TableCache::Coax* c : held) cache->release(c);
-    held.clear();
   }
 
   double width(int level) const { return cfg.D / (double)(1 << level); }
@@ -348,7 +340,6 @@ struct Solver : public wbfmm_b200_solver {
 
   // Served form: start a new solve on the same stream and buffers.
   int reset(const wbfmm_b200_config_t* c) {
-    release_cache_refs();
     WBFMM_TRY(configure(c));
     ops_ready = false;
     nsrc = ntgt = 0;
@@ -572,24 +563,52 @@ struct Solver : public wbfmm_b200_solver {
     return 0;
   }
 
-  // tables from the server's cache (served form)
+  // tables from the server's cache (served form): the order-only tables are
+  // shared; the Helmholtz coaxial tables depend on k w (every request of a
+  // served stream has its own k) and are built per solve, all levels in one
+  // set, into this solver's buffers
   int shared_operators() {
     WBFMM_TRY(cache->geometry<T>(lmax + 1, stream, &tables));
     if (!helm) return 0;
+    return helm_coaxial_set();
+  }
+
+  // Helmholtz coaxial tables of every level in one launch set: per level
+  // l >= 2, (S|R) at the 15 list-4 distances k w_l sqrt(d2) (order of the
+  // level; M2L), then (R|R) = (S|S) at k w_l sqrt(3)/2 (order of levels l-1
+  // and l; M2M l -> l-1 and L2L l-1 -> l); FP64, and converted for FP32
+  int helm_coaxial_set() {
+    CoaxJob jobs[kMaxCoaxJobs];
+    int nj = 0;
+    int64_t off = 0, sr_off[kMaxDepth + 1] = {0}, ss_off[kMaxDepth + 1] = {0};
     for (int l = 2; l <= depth; l++) {
       const int Ll = std::max(cfg.order_s[l], cfg.order_r[l]);
-      const T* p = nullptr;
-      TableCache::Coax* ref = nullptr;
-      WBFMM_TRY(cache->coaxial<T>(0, cfg.k * width(l), Ll, stream, &p, &ref));
-      held.push_back(ref);
-      sr_ptr[l] = p;
       sr_stride[l] = 2 * ((int64_t)(Ll + 1) * (Ll + 2) * (Ll + 3) / 6 + 1);
+      sr_off[l] = off;
+      for (int i = 0; i < 15; i++) {
+        jobs[nj++] = CoaxJob{cfg.k * width(l) * sqrt((double)kListDist2[i]), Ll, 2, off, 0};
+        off += sr_stride[l];
+      }
       const int Ls = std::max(std::max(cfg.order_s[l], cfg.order_r[l]),
                               std::max(cfg.order_s[l - 1], cfg.order_r[l - 1]));
-      WBFMM_TRY(cache->coaxial<T>(1, cfg.k * width(l), Ls, stream, &p, &ref));
-      held.push_back(ref);
-      ss_ptr[l] = p;
+      ss_off[l] = off;
+      jobs[nj++] = CoaxJob{cfg.k * width(l) * 0.5 * sqrt(3.0), Ls, 1, off, 0};
+      off += (int64_t)(Ls + 1) * (Ls + 2) * (Ls + 3) / 6 + 1;
     }
+    WBFMM_TRY(coax_set64.alloc((size_t)off));
+    WBFMM_TRY(generate_coaxial_set(jobs, nj, coax_set64.p, stream));
+    const T* base = (const T*)coax_set64.p;
+    if (sizeof(T) != 8) {
+      WBFMM_TRY(coax_set.alloc((size_t)off));
+      WBFMM_TRY(convert_to<T>(coax_set64.p, coax_set.p, off, stream));
+      base = coax_set.p;
+      launches++;
+    }
+    for (int l = 2; l <= depth; l++) {
+      sr_ptr[l] = base + sr_off[l];
+      ss_ptr[l] = base + ss_off[l];
+    }
+    launches += 2;
     return 0;
   }
 
@@ -625,29 +644,7 @@ struct Solver : public wbfmm_b200_solver {
     WBFMM_TRY(convert_to<T>(H64.p, H.p, (int64_t)hstride * nth, stream));
     launches += 2;
     if (helm) {
-      for (int l = 2; l <= depth; l++) {
-        // (S|R) for the 15 list-4 distances, order of this level
-        int Ll = std::max(cfg.order_s[l], cfg.order_r[l]);
-        std::vector<double> krs(15);
-        for (int i = 0; i < 15; i++) krs[i] = cfg.k * width(l) * sqrt((double)kListDist2[i]);
-        sr_stride[l] = 2 * ((int64_t)(Ll + 1) * (Ll + 2) * (Ll + 3) / 6 + 1);
-        WBFMM_TRY(coax64[l].alloc((size_t)sr_stride[l] * 15));
-        WBFMM_TRY(generate_coaxial_tables(krs, Ll, 2, coax64[l].p, sr_stride[l], stream));
-        WBFMM_TRY(coaxSR[l].alloc((size_t)sr_stride[l] * 15));
-        WBFMM_TRY(convert_to<T>(coax64[l].p, coaxSR[l].p, sr_stride[l] * 15, stream));
-        sr_ptr[l] = coaxSR[l].p;
-        // (R|R) = (S|S) at k w_l sqrt(3)/2 for M2M l -> l-1 and L2L l-1 -> l
-        int Ls = std::max(std::max(cfg.order_s[l], cfg.order_r[l]),
-                          std::max(cfg.order_s[l - 1], cfg.order_r[l - 1]));
-        std::vector<double> kss(1, cfg.k * width(l) * 0.5 * sqrt(3.0));
-        int64_t n_ss = (int64_t)(Ls + 1) * (Ls + 2) * (Ls + 3) / 6 + 1;
-        WBFMM_TRY(ss64[l].alloc(n_ss));
-        WBFMM_TRY(generate_coaxial_tables(kss, Ls, 1, ss64[l].p, n_ss, stream));
-        WBFMM_TRY(coaxSS[l].alloc(n_ss));
-        WBFMM_TRY(convert_to<T>(ss64[l].p, coaxSS[l].p, n_ss, stream));
-        ss_ptr[l] = coaxSS[l].p;
-        launches += 4;
-      }
+      WBFMM_TRY(helm_coaxial_set());
     } else {
       lt = L;
       size_t n3 = (size_t)(lt + 1) * (lt + 1) * (lt + 1);

@@ -160,17 +160,16 @@ int generate_rotation_tables(const std::vector<double>& thetas, int N,
 }
 
 // --------------------------------------------- Helmholtz coaxial tables
-// One block per table.  nc = 2 (complex S|R) or 1 (real R|R).  kr may be
-// negative (reverses the sense of the translation).  The table keeps the
+// One block per table; a launch builds any set of tables, each with its
+// own kr, order L and kind: nc = 2 (complex S|R) or 1 (real R|R).  kr may
+// be negative (reverses the sense of the translation).  A table keeps the
 // entries l <= L (coax_idx(L,L,L) < coax_count(L)); scratch holds the
 // recursion's work range l <= 2L+1.
-__global__ void k_coaxial_tables(const Vals64 krs, int L, int nc,
-                                 double* __restrict__ out, int64_t ostride,
-                                 double* __restrict__ scratch,
-                                 int64_t sstride) {
+__global__ void k_coaxial_tables(const CoaxJobs jobs, double* __restrict__ scratch) {
   const int it = blockIdx.x;
-  double* cf = scratch + (int64_t)it * sstride;
-  double kr = krs.v[it];
+  const int L = jobs.j[it].L, nc = jobs.j[it].nc;
+  double* cf = scratch + jobs.j[it].scr_off;
+  double kr = jobs.j[it].kr;
   int sw = 1;
   if (kr < 0) { kr = -kr; sw = -1; }
   const int LL = 2 * L + 2;
@@ -238,12 +237,15 @@ __global__ void k_coaxial_tables(const Vals64 krs, int L, int nc,
 
 // G&D (4.79) for each order m >= 1 (independent of the other orders once
 // the (4.84) diagonal is in place), one block per (m, table); then the
-// order-m entries l <= L are copied out.  Block m = 0 only copies.
-__global__ void k_coaxial_orders(int L, int nc, double* __restrict__ out,
-                                 int64_t ostride, double* __restrict__ scratch,
-                                 int64_t sstride) {
+// order-m entries l <= L are copied out to the table's place in `out`.
+// Block m = 0 only copies; blocks with m above the table's order leave.
+__global__ void k_coaxial_orders(const CoaxJobs jobs, double* __restrict__ out,
+                                 double* __restrict__ scratch) {
   const int m = blockIdx.x, it = blockIdx.y;
-  double* cf = scratch + (int64_t)it * sstride;
+  const int L = jobs.j[it].L, nc = jobs.j[it].nc;
+  if (m > L) return;
+  double* cf = scratch + jobs.j[it].scr_off;
+  double* o = out + jobs.j[it].out_off;
   if (m >= 1) {
     for (int n = m; n <= L; n++) {
       for (int l = n + 1 + threadIdx.x; l <= 2 * L - n; l += blockDim.x) {
@@ -264,28 +266,47 @@ __global__ void k_coaxial_orders(int L, int nc, double* __restrict__ out,
   for (int l = m; l <= L; l++)
     for (int n = m + threadIdx.x; n <= l; n += blockDim.x) {
       const int64_t i = coax_idx(l, m, n);
-      for (int c = 0; c < nc; c++) out[(int64_t)it * ostride + nc * i + c] = cf[nc * i + c];
+      for (int c = 0; c < nc; c++) o[nc * i + c] = cf[nc * i + c];
     }
+}
+
+int generate_coaxial_set(const CoaxJob* jobs, int njobs, double* dout, cudaStream_t s) {
+  if (njobs <= 0) return 0;
+  if (njobs > kMaxCoaxJobs) return set_error(WBFMM_B200_E_ARG, "too many coaxial tables in one set");
+  CoaxJobs js;
+  memset(&js, 0, sizeof(js));
+  int Lmax = 0;
+  int64_t scr = 0;
+  for (int i = 0; i < njobs; i++) {
+    js.j[i] = jobs[i];
+    const int LL = 2 * jobs[i].L + 2;
+    js.j[i].scr_off = scr;
+    scr += ((int64_t)coax_idx(LL, LL, LL) + 2) * jobs[i].nc;
+    Lmax = jobs[i].L > Lmax ? jobs[i].L : Lmax;
+  }
+  double* scratch = nullptr;
+  WBFMM_CUDA(table_scratch(&scratch, sizeof(double) * scr, s));
+  k_coaxial_tables<<<njobs, 128, 0, s>>>(js, scratch);
+  WBFMM_CUDA(cudaGetLastError());
+  k_coaxial_orders<<<dim3(Lmax + 1, njobs), 64, 0, s>>>(js, dout, scratch);
+  WBFMM_CUDA(cudaGetLastError());
+  WBFMM_CUDA(cudaFreeAsync(scratch, s));
+  return 0;
 }
 
 int generate_coaxial_tables(const std::vector<double>& krs, int L, int nc,
                             double* dout, int64_t ostride, cudaStream_t s) {
-  int nt = (int)krs.size();
-  if (nt == 0) return 0;
-  if (nt > 64) return set_error(WBFMM_B200_E_ARG, "too many coaxial distances");
-  Vals64 kv;
-  memset(&kv, 0, sizeof(kv));
-  for (int i = 0; i < nt; i++) kv.v[i] = krs[i];
-  double* scratch = nullptr;
-  int LL = 2 * L + 2;
-  int64_t sstride = ((int64_t)coax_idx(LL, LL, LL) + 2) * nc;
-  WBFMM_CUDA(table_scratch(&scratch, sizeof(double) * sstride * nt, s));
-  k_coaxial_tables<<<nt, 128, 0, s>>>(kv, L, nc, dout, ostride, scratch, sstride);
-  WBFMM_CUDA(cudaGetLastError());
-  k_coaxial_orders<<<dim3(L + 1, nt), 64, 0, s>>>(L, nc, dout, ostride, scratch, sstride);
-  WBFMM_CUDA(cudaGetLastError());
-  WBFMM_CUDA(cudaFreeAsync(scratch, s));
-  return 0;
+  const int nt = (int)krs.size();
+  if (nt > kMaxCoaxJobs) return set_error(WBFMM_B200_E_ARG, "too many coaxial distances");
+  std::vector<CoaxJob> jobs(nt);
+  for (int i = 0; i < nt; i++) {
+    jobs[i].kr = krs[i];
+    jobs[i].L = L;
+    jobs[i].nc = nc;
+    jobs[i].out_off = (int64_t)i * ostride;
+    jobs[i].scr_off = 0;
+  }
+  return generate_coaxial_set(jobs.data(), nt, dout, s);
 }
 
 // ----------------------------------------------- Laplace coaxial tables

@@ -31,6 +31,16 @@ int generate_rotation_tables(const std::vector<double>& thetas, int N,
 // coaxial tables for each kr: nc=2 complex (S|R), nc=1 real (R|R)
 int generate_coaxial_tables(const std::vector<double>& krs, int L, int nc,
                             double* dout, int64_t ostride, cudaStream_t s);
+// any set of coaxial tables in one launch pair: table i at dout + out_off
+constexpr int kMaxCoaxJobs = 160;
+struct CoaxJob {
+  double kr;
+  int L, nc;         // order; 2 complex (S|R), 1 real (R|R)
+  int64_t out_off;   // doubles
+  int64_t scr_off;   // the recursion's scratch (set by generate_coaxial_set)
+};
+struct CoaxJobs { CoaxJob j[kMaxCoaxJobs]; };   // kernel argument (5 KB)
+int generate_coaxial_set(const CoaxJob* jobs, int njobs, double* dout, cudaStream_t s);
 // Laplace dense [n][nd][m] tables, n, nd, m <= Lt
 int generate_laplace_tables(int Lt, double* SS, double* RR, double* SR,
                             cudaStream_t s);
