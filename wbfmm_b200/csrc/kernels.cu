@@ -642,10 +642,10 @@ int launch_l2p(const EvalParams<T>& p, cudaStream_t s) {
 // and the group's partial sums are added by shuffles at the end.  The FP32
 // form computes pair terms in FP32 from separations that keep FP64 accuracy
 // (coordinates as float pairs hi + lo, the hi parts of neighbouring points
-// subtracting exactly), sums each run of 4 of a thread's terms in FP32 and
+// subtracting exactly), sums each run of 8 of a thread's terms in FP32 and
 // adds that into the FP64 sums.  Pair kernels and the r > 1e-6 cutoff follow
 // src/local.c:32-262 and src/local-laplace.c:400-523, 1091-1227.
-constexpr int kP2PRun = 4;     // FP32 terms summed before each FP64 add
+constexpr int kP2PRun = 8;     // FP32 terms summed before each FP64 add
 
 template <typename T, bool HELM, int NT>
 struct P2PTile {
