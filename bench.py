@@ -964,6 +964,21 @@ def our_arm(args, ws, rank, local):
         print(json.dumps(line))
 
 
+def free_port() -> int:
+    import socket
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        return so.getsockname()[1]
+
+
+def torchrun_command(argv, n, port):
+    """This script under torchrun with n ranks on this node (rendezvous on
+    127.0.0.1), bounded by `timeout`."""
+    return ["timeout", "-k", "60", "3600", sys.executable, "-m", "torch.distributed.run",
+            "--nnodes=1", f"--nproc-per-node={n}", "--master-addr", "127.0.0.1",
+            "--master-port", str(port), os.path.abspath(__file__)] + list(argv)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -986,6 +1001,10 @@ def main():
     if args.profile_case:
         profile_case(args.profile_case)
         return
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        # not under torchrun: launch one rank per GPU, as the contract's
+        # launcher would
+        sys.exit(subprocess.call(torchrun_command(sys.argv[1:], args.gpus, free_port())))
     ws, rank, local = dist_setup()
     try:
         if args.impl == "reference":
