@@ -278,6 +278,45 @@ def test_laplace_fp32_deep_levels(gpu_lib, mode):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("case", ["cube_k1.5_depth4", "sphere_k2_depth4_skip", "cube_k3_depth5"])
+def test_helmholtz_fp32_scaled_m2l(gpu_lib, case):
+    """Helmholtz at small k w and order 14: the (S|R) coefficients of the
+    finer levels are beyond the FP32 range unscaled, so those levels run the
+    scaled M2L (sources x 2^(e l), table x 2^(-e (n + l)), results x
+    2^(e n)); the FP32 form is admitted by the range rule, finite, within
+    2e-6 of the FP64 form and as close to the direct sum."""
+    kind, kk, dd = case.split("_")[:3]
+    k, depth = float(kk[1:]), int(dd[5:])
+    if kind == "cube":
+        p = W.helmholtz_cube(40_000 if depth == 4 else 120_000, k=k, depth=depth, seed=91,
+                             lo=14, hi=40)
+        p.xt = p.xs[:4000]
+        p.targets_are_sources = False
+        skip = False
+    else:
+        p = W.helmholtz_sphere(40_000, 4000, k=k, depth=depth, seed=92, lo=14, hi=40)
+        skip = True
+    cfg32 = engine.SolverConfig.from_problem(p, engine.FP32, skip_empty=skip)
+    assert engine.fp32_range_ok(cfg32)
+    outs = {}
+    for prec in (engine.FP64, engine.FP32):
+        cfg = engine.SolverConfig.from_problem(p, prec, skip_empty=skip)
+        with engine.Solver(cfg) as s:
+            s.set_sources(p.xs, p.normals).set_strengths(p.q, p.dipoles).set_targets(p.xt).run()
+            outs[prec] = s.field()
+    for a in outs[engine.FP32]:
+        assert np.all(np.isfinite(a))
+    for a, b in zip(outs[engine.FP32], outs[engine.FP64]):
+        assert rel_l2(a, b) < 2e-6, rel_l2(a, b)
+    idx = W.subsample(93, p.nt, 1500)
+    dpot, dgrad = engine.direct(p.problem, p.xs, p.q, p.xt[idx], k=p.k, normals=p.normals,
+                                dipoles=p.dipoles)
+    pot, grad = outs[engine.FP32]
+    assert rel_l2(pot.reshape(-1, 2)[idx].ravel(), dpot) < 1e-5
+    assert rel_l2(grad.reshape(-1, 6)[idx].ravel(), dgrad) < 1e-4
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("precision", [engine.FP64, engine.FP32])
 @pytest.mark.parametrize("mode", [0, 2, 3])
 @pytest.mark.parametrize("case", ["helmholtz_spheres", "laplace_clusters"])

@@ -94,6 +94,26 @@ struct XlateParams {
 // deep levels (t = 2/256 at level 8 gives 128^21 ~ 1.8e44 for p = 10).
 inline int lap_scale_exp(double w) { return -std::ilogb(w); }
 
+// Helmholtz FP32 M2L scale exponent of a level (0: none needed).  With
+// x = 2 k w the nearest list-4 distance, the level's (S|R) coefficients of
+// degrees n, l <= P grow like (2(n+l)-1)!! / x^(n+l+1) (G&D (4.79) seeded
+// by h_l(x)), beyond the FP32 range at small k w and high order.  The M2L
+// then works on sources whose degree l is scaled by 2^(e l), on the table
+// scaled by 2^(-e (n + l)), and scales degree n of its results back by
+// 2^(e n): with 2^-e about the (2P)-th root of x^(2P+1) / (4P-1)!!, the
+// largest scaled coefficient (n = l = P) is of order one and the smallest
+// ((n, l) = (0, 0), h_0(x) ~ 1/x) unchanged; the scaled sources stay below
+// ((sqrt 3 / 4) x 2^e)^l / (2l+1)!! per unit strength.  Exact (powers of
+// two); the stored expansions are not scaled.
+inline int helm_m2l_exp(double k, double w, int P) {
+  const double x = 2.0 * k * w;
+  double lf = 0.0;                       // log10 (4P-1)!!
+  for (int i = 4 * P - 1; i > 1; i -= 2) lf += std::log10((double)i);
+  if (lf - (2 * P + 1) * std::log10(x) <= 30.0) return 0;
+  const double log2s = ((2 * P + 1) * std::log10(x) - lf) / (2.0 * P) / std::log10(2.0);
+  return -(int)std::floor(log2s + 0.5);
+}
+
 template <typename T, bool HELM>
 int launch_p2m(const P2MParams<T>& p, cudaStream_t s);
 template <typename T, bool HELM>

@@ -48,9 +48,10 @@ static int ensure_offsets() {
 
 // ----------------------------------------------------------- transpose
 // Layout L level array -> lin[tau][c][pp] (complex), pp on the padded
-// parent grid (nx+2)^3; the halo must be zero beforehand
+// parent grid (nx+2)^3, degree n scaled by 2^(scale_e n); the halo must be
+// zero beforehand
 template <typename T, bool HELM>
-__global__ void k_to_lin(const T* __restrict__ arr, int level, int N, int lap_e, bool boxmajor,
+__global__ void k_to_lin(const T* __restrict__ arr, int level, int N, int scale_e, bool boxmajor,
                          typename V2t<T>::t* __restrict__ lin) {
   typedef typename V2t<T>::t T2;
   const int V = HELM ? (N + 1) * (N + 1) : (N + 1) * (N + 2) / 2;
@@ -71,6 +72,11 @@ __global__ void k_to_lin(const T* __restrict__ arr, int level, int N, int lap_e,
   if (HELM) {
     int64_t o = layout_off(b, c, nc);
     v.x = arr[2 * o]; v.y = arr[2 * o + 1];
+    if (scale_e) {
+      const int n = full_degree(c);
+      v.x = scale2(v.x, scale_e * n);
+      v.y = scale2(v.y, scale_e * n);
+    }
   } else {
     int n = half_degree(c), m = c - n * (n + 1) / 2;
     if (m == 0) {
@@ -79,8 +85,8 @@ __global__ void k_to_lin(const T* __restrict__ arr, int level, int N, int lap_e,
       int id = lidx(n, m);
       v.x = arr[layout_off(b, id, nc)]; v.y = arr[layout_off(b, id + 1, nc)];
     }
-    v.x = scale2(v.x, lap_e * n);
-    v.y = scale2(v.y, lap_e * n);
+    v.x = scale2(v.x, scale_e * n);
+    v.y = scale2(v.y, scale_e * n);
   }
   if (boxmajor) lin[((int64_t)tau * npp + pp) * V + c] = v;
   else lin[((int64_t)tau * V + c) * npp + pp] = v;
@@ -652,14 +658,14 @@ int launch_lanes_reduce(const LanesParams<T>& p, cudaStream_t s) {
 }
 
 template <typename T, bool HELM>
-int lanes_to_lin(const T* arr, int level, int N, int lap_e, void* lin, cudaStream_t s,
+int lanes_to_lin(const T* arr, int level, int N, int scale_e, void* lin, cudaStream_t s,
                  bool boxmajor) {
   typedef typename V2t<T>::t T2;
   const int V = HELM ? (N + 1) * (N + 1) : (N + 1) * (N + 2) / 2;
   const int64_t nx = 1 << (level - 1), npx = nx + 2;
   WBFMM_CUDA(cudaMemsetAsync(lin, 0, sizeof(T2) * 8 * V * npx * npx * npx, s));
   const int64_t tot = nx * nx * nx * V * 8;
-  k_to_lin<T, HELM><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(arr, level, N, lap_e,
+  k_to_lin<T, HELM><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(arr, level, N, scale_e,
                                                                    boxmajor, (T2*)lin);
   WBFMM_CUDA(cudaGetLastError());
   return 0;

@@ -23,6 +23,9 @@ struct LanesParams {
   T width;              // box width of the level
   const uint8_t* tmask; // targets to compute, or null for all
   int lap_e;            // Laplace: degree l of lin_raw is scaled by 2^(lap_e l)
+  int helm_e;           // Helmholtz tiles (helm_m2l_exp): degree l of lin_raw is
+                        // scaled by 2^(helm_e l), coax by 2^(-helm_e (n + l)),
+                        // and output degree n by 2^(helm_e n)
   const void* lapsr;    // Laplace: [kNumOps][(P+1)^3] scaled S|R per shift (build_lap_sr_ops)
   const void* hcx;      // Helmholtz tiles: the level's coaxial rows (build_helm_coax_rows)
   const int* act;       // sparse targets: [8][np] parents per child type, or null
@@ -87,8 +90,9 @@ size_t helm_coax_rows_count(int P);
 // parent holds sources (0 on the padding), from the level's box counts
 int build_source_mask(const uint32_t* src_n, int level, uint8_t* smask, cudaStream_t s);
 size_t source_mask_bytes(int level);
+// degree l scaled by 2^(scale_e l) (the Laplace or Helmholtz M2L exponent)
 template <typename T, bool HELM>
-int lanes_to_lin(const T* arr, int level, int N, int lap_e, void* lin, cudaStream_t s,
+int lanes_to_lin(const T* arr, int level, int N, int scale_e, void* lin, cudaStream_t s,
                  bool boxmajor = false);
 size_t lanes_lin_bytes(int level, int N, bool helm, size_t tsize);
 

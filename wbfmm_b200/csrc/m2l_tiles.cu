@@ -519,7 +519,12 @@ k_m2l_tiles(LanesParams<T> p, OpTables<T> t, int TC, bool dense) {
     const int c = i / TC, tt = i - c * TC;
     if (!s_act[tt]) continue;
     const int64_t plin = s_act[tt] - 1;
-    const T2 a = A[i];
+    T2 a = A[i];
+    if (HELM && p.helm_e) {
+      const int n = s_nm[c] & 255;
+      a.x = scale2(a.x, p.helm_e * n);
+      a.y = scale2(a.y, p.helm_e * n);
+    }
     if (p.nsplit > 1) {
       ((T2*)p.partial_raw)[(((int64_t)split * 8 + tau) * V + c) * np + plin] = a;
       continue;

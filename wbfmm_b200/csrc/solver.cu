@@ -103,7 +103,16 @@ int wbfmm_b200_fp32_range_ok(const wbfmm_b200_config_t* c) {
     }
     const double x = 2.0 * c->k * w;            // nearest list-4 distance
     const int N = 2 * p;
-    if (x < N && log10_dfact(2 * N - 1) - (N + 1) * log10(x) > 36.0) return 0;
+    // the level's (S|R) table holds degrees n + l up to 2p, about
+    // (2N-1)!! / x^(N+1): beyond the FP32 range the M2L runs in its scaled
+    // form (helm_m2l_exp; tile kernel, equal orders), otherwise the form is
+    // out of range
+    if (x < N && log10_dfact(2 * N - 1) - (N + 1) * log10(x) > 36.0 &&
+        !wbfmm::helm_m2l_scalable(c->order_s[l], c->order_r[l]))
+      return 0;
+    // local coefficients, stored unscaled, reach about (2p-1)!! / x^(p+1)
+    // per unit strength at the nearest list-4 distance
+    if (x < p && log10_dfact(2 * p - 1) - (p + 1) * log10(x) > 34.0) return 0;
     if (l == c->depth) {
       const double xr = 0.5 * c->k * w;         // a typical leaf radius
       if (xr < p && p * log10(xr) - log10_dfact(2 * p + 1) < -36.0) return 0;

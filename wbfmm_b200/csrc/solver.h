@@ -31,6 +31,12 @@ namespace wbfmm {
 // a free has completed), or null when it cannot be created.  Solvers trim it
 // to kLibPoolKeep unused bytes when they are destroyed.
 cudaMemPool_t library_pool();
+
+// whether an FP32 Helmholtz level of these orders can run the scaled M2L
+// (helm_m2l_exp), which only the tile kernel implements
+inline bool helm_m2l_scalable(int order_s, int order_r) {
+  return order_s == order_r && tiles_supported<float, true>(order_s, order_r);
+}
 constexpr size_t kLibPoolKeep = (size_t)4 << 30;
 
 // ------------------------------------------------------------ buffers
@@ -229,6 +235,7 @@ struct Solver : public wbfmm_b200_solver {
   int64_t sr_stride[kMaxDepth + 1] = {0};
   const T* sr_ptr[kMaxDepth + 1] = {nullptr};   // (S|R) table per level
   const T* ss_ptr[kMaxDepth + 1] = {nullptr};   // (R|R) table per level
+  int helm_e[kMaxDepth + 1] = {0};   // FP32 Helmholtz M2L scale exponents (helm_m2l_exp)
   DBuf<double> lap64[3];
   DBuf<T> lap[3];
   int lt = 0;
@@ -603,6 +610,19 @@ struct Solver : public wbfmm_b200_solver {
       WBFMM_TRY(convert_to<T>(coax_set64.p, coax_set.p, off, stream));
       base = coax_set.p;
       launches++;
+      // levels whose (S|R) coefficients leave the FP32 range: the scaled
+      // form of their M2L (helm_m2l_exp), tables written scaled
+      for (int l = 2; l <= depth; l++) {
+        helm_e[l] = helm_m2l_scalable(cfg.order_s[l], cfg.order_r[l])
+                        ? helm_m2l_exp(cfg.k, width(l), cfg.order_s[l]) : 0;
+        if (!helm_e[l]) continue;
+        const int Ll = std::max(cfg.order_s[l], cfg.order_r[l]);
+        WBFMM_TRY(narrow_coax_scaled(coax_set64.p + sr_off[l], (float*)coax_set.p + sr_off[l],
+                                     Ll, sr_stride[l], 15, helm_e[l], stream));
+        launches++;
+      }
+    } else {
+      for (int l = 2; l <= depth; l++) helm_e[l] = 0;
     }
     for (int l = 2; l <= depth; l++) {
       sr_ptr[l] = base + sr_off[l];
@@ -743,7 +763,14 @@ struct Solver : public wbfmm_b200_solver {
     // faster as lanes)
     const int lanes_max = helm ? 7 : sizeof(T) == 8 ? 9 : 10;
     bool use_tiles = false, use_lanes = false;
-    if (m2l_mode == 1) {
+    const int he = helm ? helm_e[level] : 0;
+    if (he) {
+      // the scaled Helmholtz M2L (FP32 tables out of range unscaled) runs
+      // in the tile kernel only
+      if (!tiles_ok)
+        return set_error(WBFMM_B200_E_ORDER, "FP32 Helmholtz M2L out of range at this order; use the FP64 form");
+      use_tiles = true;
+    } else if (m2l_mode == 1) {
       use_lanes = lanes_ok && x.Nin <= lanes_max;
       use_tiles = !use_lanes && tiles_ok;
     } else if (m2l_mode == 2) {
@@ -754,7 +781,7 @@ struct Solver : public wbfmm_b200_solver {
     if (use_tiles) {
       // offset-major target tiles on the transposed singular expansions
       WBFMM_TRY(lin.alloc(lanes_lin_bytes(level, x.Nin, helm, sizeof(T))));
-      WBFMM_TRY((helm ? lanes_to_lin<T, true>(x.cin, level, x.Nin, 0, lin.p, stream)
+      WBFMM_TRY((helm ? lanes_to_lin<T, true>(x.cin, level, x.Nin, he, lin.p, stream)
                       : lanes_to_lin<T, false>(x.cin, level, x.Nin, x.lap_e, lin.p, stream)));
       LanesParams<T> lp;
       memset(&lp, 0, sizeof(lp));
@@ -762,6 +789,7 @@ struct Solver : public wbfmm_b200_solver {
       lp.lin_raw = lin.p; lp.cout = x.cout;
       lp.coax = x.coax; lp.coax_stride = x.coax_stride;
       lp.width = x.width; lp.tmask = x.tmask; lp.lap_e = x.lap_e;
+      lp.helm_e = he;
       if (x.tmask && act[level].p) { lp.act = act[level].p; lp.act_n = act_n[level].p; }
       if (x.tmask) {
         WBFMM_TRY(smask.alloc(source_mask_bytes(level)));

@@ -309,6 +309,40 @@ int generate_coaxial_tables(const std::vector<double>& krs, int L, int nc,
   return generate_coaxial_set(jobs.data(), nt, dout, s);
 }
 
+// FP32 copies of `ntables` complex (S|R) tables of order L (stride
+// `stride` doubles) with entry (l, m, n) scaled by 2^(-e (l + n)): the
+// scaled form of the Helmholtz FP32 M2L (helm_m2l_exp).  Thread per entry.
+__global__ void k_narrow_coax_scaled(const double* __restrict__ src, float* __restrict__ dst,
+                                     int L, int64_t stride, int ntables, int e) {
+  const int64_t ne = coax_idx(L, L, L) + 1;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ne * ntables) return;
+  const int t = (int)(i / ne);
+  const int64_t c = i % ne;
+  // (l, m, n) of entry c = coax_idx(l, m, n) = l(l+1)(l+2)/6 + n(n+1)/2 + m,
+  // m <= n <= l: l is the largest with coax_idx(l, 0, 0) <= c, then n the
+  // largest with n(n+1)/2 <= c - coax_idx(l, 0, 0)
+  int l = 0;
+  while (l < L && coax_idx(l + 1, 0, 0) <= c) l++;
+  const int64_t r = c - coax_idx(l, 0, 0);
+  int n = 0;
+  while (n < l && (int64_t)(n + 1) * (n + 2) / 2 <= r) n++;
+  const double f = ldexp(1.0, -e * (l + n));
+  const double* a = src + (int64_t)t * stride + 2 * c;
+  float* b = dst + (int64_t)t * stride + 2 * c;
+  b[0] = (float)(a[0] * f);
+  b[1] = (float)(a[1] * f);
+}
+
+int narrow_coax_scaled(const double* src, float* dst, int L, int64_t stride, int ntables,
+                       int e, cudaStream_t s) {
+  const int64_t tot = ((int64_t)coax_idx(L, L, L) + 1) * ntables;
+  k_narrow_coax_scaled<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(src, dst, L, stride,
+                                                                      ntables, e);
+  WBFMM_CUDA(cudaGetLastError());
+  return 0;
+}
+
 // ----------------------------------------------- Laplace coaxial tables
 // dense [n][nd][m] arrays for n, nd, m <= Lt (m <= min(n, nd));
 // SS(n,nd,m) n >= nd, RR(n,nd,m) nd >= n, SR(n,nd,m) with (-1)^{n+m}

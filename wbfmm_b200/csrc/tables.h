@@ -41,6 +41,10 @@ struct CoaxJob {
 };
 struct CoaxJobs { CoaxJob j[kMaxCoaxJobs]; };   // kernel argument (5 KB)
 int generate_coaxial_set(const CoaxJob* jobs, int njobs, double* dout, cudaStream_t s);
+// FP32 copies of ntables complex (S|R) tables of order L, entry (l, m, n)
+// scaled by 2^(-e (l + n)) (the Helmholtz FP32 M2L's scaled form)
+int narrow_coax_scaled(const double* src, float* dst, int L, int64_t stride, int ntables,
+                       int e, cudaStream_t s);
 // Laplace dense [n][nd][m] tables, n, nd, m <= Lt
 int generate_laplace_tables(int Lt, double* SS, double* RR, double* SR,
                             cudaStream_t s);

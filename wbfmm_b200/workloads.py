@@ -104,7 +104,7 @@ def helmholtz_cube(n: int = 1_000_000, k: float = 8.0, depth: int = 6,
 
 def helmholtz_sphere(n_src: int = 2_000_000, n_tgt: int = 500_000,
                      k: float = 40.0, depth: int = 7, seed: int = 3,
-                     hi: int | None = None) -> Problem:
+                     hi: int | None = None, lo: int = 6) -> Problem:
     """Helmholtz surface distribution: sources on a sphere r=0.45, first
     half monopoles and second half dipoles along the radial normal; targets
     on a concentric sphere r=0.49."""
@@ -126,7 +126,7 @@ def helmholtz_sphere(n_src: int = 2_000_000, n_tgt: int = 500_000,
                 [0] * (depth + 1), k, xs, q, xt, normals=nrm, dipoles=d)
     p = _finish(p)
     for lv in range(1, depth + 1):
-        o = helmholtz_order(k, p.D / 2 ** lv, lo=6, hi=hi)
+        o = helmholtz_order(k, p.D / 2 ** lv, lo=lo, hi=hi)
         p.order_s[lv] = p.order_r[lv] = o
     return p
 
