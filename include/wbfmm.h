@@ -272,7 +272,101 @@ gint wbfmm_laplace_field_grad(gdouble *xs, gint xstride, gdouble *src,
 gint wbfmm_library_config(wbfmm_library_config_t *c);
 gint wbfmm_library_config_print(wbfmm_library_config_t *c, FILE *f);
 
+/* ------------------------------------------- single precision (*_f) */
+/* The reference's single-precision API (src/wbfmm.h:993-1112, the same
+   sources compiled with WBFMM_REAL = gfloat): trees of FP32 points and
+   coefficients, evaluated by the engine's FP32 form. */
+wbfmm_tree_t *wbfmm_tree_new_f(gfloat *x, gfloat D, guint maxpoints);
+gint wbfmm_tree_add_points_f(wbfmm_tree_t *t, gpointer pts, gsize pstr,
+                             gpointer normals, gsize nstr, guint npts,
+                             gboolean sorted);
+gint wbfmm_tree_sort_points_f(wbfmm_tree_t *t, gpointer pts, gsize psize,
+                              guint npts);
+gint wbfmm_tree_refine_f(wbfmm_tree_t *t);
+gint wbfmm_tree_coefficient_init_f(wbfmm_tree_t *t, guint l, guint nr, guint ns);
+gint wbfmm_tree_laplace_coefficient_init_f(wbfmm_tree_t *t, guint l, guint nr,
+                                           guint ns);
+gint wbfmm_tree_coefficient_clear_f(wbfmm_tree_t *t, guint l);
+guint64 wbfmm_point_box_f(wbfmm_tree_t *t, guint level, gfloat *x);
+guint64 wbfmm_point_index_3d_f(gfloat *x, gfloat *c, gfloat D);
+gint wbfmm_box_location_from_index_f(guint64 i, guint32 level, gfloat *x0,
+                                     gfloat D, gfloat *x, gfloat *wb);
+gint wbfmm_tree_box_centre_f(wbfmm_tree_t *t, guint level, guint64 b,
+                             gfloat *xb, gfloat *wb);
+gint wbfmm_points_origin_width_f(gfloat *x, gint str, gint n, gfloat *xmin,
+                                 gfloat *xmax, gfloat *D, gboolean init_limits);
+gint wbfmm_tree_write_sources_f(wbfmm_tree_t *t, gfloat *q, gint stride,
+                                FILE *f);
+gint wbfmm_truncation_number_f(wbfmm_tree_t *t, gfloat k, guint level,
+                               gfloat tol);
+gint wbfmm_shift_angle_table_init_f(void);
+wbfmm_shift_operators_t *wbfmm_shift_operators_new_f(guint L, gboolean bw,
+                                                     gfloat *work);
+gint wbfmm_shift_operators_coaxial_SR_init_f(wbfmm_shift_operators_t *w,
+                                             gfloat D, guint level, guint L,
+                                             gfloat k, gfloat *work);
+gint wbfmm_shift_operators_coaxial_SS_init_f(wbfmm_shift_operators_t *w,
+                                             gfloat D, guint level, guint L,
+                                             gfloat k, gfloat *work);
+gint wbfmm_laplace_coaxial_translate_init_f(gint N);
+gint wbfmm_tree_leaf_expansions_f(wbfmm_tree_t *t, gfloat k, gfloat *src,
+                                  gint sstr, gfloat *dipoles, gint dstr,
+                                  gboolean zero_expansions, gfloat *work);
+gint wbfmm_tree_laplace_leaf_expansions_f(wbfmm_tree_t *t, gfloat *src,
+                                          gint sstr, gfloat *dipoles,
+                                          gint dstr, gboolean zero_expansions,
+                                          gfloat *work);
+gint wbfmm_upward_pass_f(wbfmm_tree_t *t, wbfmm_shift_operators_t *op,
+                         guint level, gfloat *work);
+gint wbfmm_laplace_upward_pass_f(wbfmm_tree_t *t, wbfmm_shift_operators_t *op,
+                                 guint level, gfloat *work);
+gint wbfmm_downward_pass_ref_f(wbfmm_tree_t *t, wbfmm_shift_operators_t *op,
+                               guint level, gfloat *work, gint nthreads);
+gint wbfmm_laplace_downward_pass_ref_f(wbfmm_tree_t *t,
+                                       wbfmm_shift_operators_t *op,
+                                       guint level, gfloat *work,
+                                       gint nthreads);
+gint wbfmm_tree_box_local_field_f(wbfmm_tree_t *t, guint level, guint b,
+                                  gfloat k, gfloat *x, gfloat *f, gint fstr,
+                                  gfloat *src, gint sstr, gfloat *d, gint dstr,
+                                  gboolean eval_neighbours, guint field,
+                                  gfloat *work);
+gint wbfmm_laplace_box_field_f(wbfmm_tree_t *t, guint level, guint b,
+                               gfloat *src, gint sstr, gfloat *d, gint dstr,
+                               guint field, gboolean eval_neighbours,
+                               gfloat *x, gfloat *f, gint fstr, gfloat *work);
+wbfmm_target_list_t *wbfmm_target_list_new_f(wbfmm_tree_t *t, guint npts);
+gint wbfmm_target_list_add_points_f(wbfmm_target_list_t *l, gpointer pts,
+                                    gsize pstr, guint npts);
+gint wbfmm_target_list_local_coefficients_f(wbfmm_target_list_t *l, gfloat k,
+                                            gfloat *work);
+gint wbfmm_laplace_target_list_local_coefficients_f(wbfmm_target_list_t *l,
+                                                    guint source,
+                                                    gfloat *work);
+gint wbfmm_target_list_local_field_f(wbfmm_target_list_t *l, gfloat *src,
+                                     gint sstr, gfloat *nsrc, gint nstr,
+                                     gfloat *f, gint fstr);
+gint wbfmm_total_field_f(gfloat k, gfloat *xs, gint xstride, gfloat *src,
+                         gint sstride, gfloat *normals, gint nstr,
+                         gfloat *dipoles, gint dstr, gint nq, gint nsrc,
+                         gfloat *xf, gfloat *field, gint fstr);
+gint wbfmm_total_field_grad_f(gfloat k, gfloat *xs, gint xstride, gfloat *src,
+                              gint sstride, gfloat *normals, gint nstr,
+                              gfloat *dipoles, gint dstr, gint nq, gint nsrc,
+                              gfloat *xf, gfloat *field, gint fstr);
+gint wbfmm_laplace_field_f(gfloat *xs, gint xstride, gfloat *src,
+                           gint sstride, gint nq, gfloat *normals, gint nstr,
+                           gfloat *dipoles, gint dstr, gint nsrc, gfloat *xf,
+                           gfloat *field, gint fstr);
+gint wbfmm_laplace_field_grad_f(gfloat *xs, gint xstride, gfloat *src,
+                                gint sstride, gint nq, gfloat *normals,
+                                gint nstr, gfloat *dipoles, gint dstr,
+                                gint nsrc, gfloat *xf, gfloat *field,
+                                gint fstr);
+
 /* dispatch as in the reference (src/wbfmm.h:1138-1194) */
+#define wbfmm_downward_pass_f wbfmm_downward_pass_ref_f
+#define wbfmm_laplace_downward_pass_f wbfmm_laplace_downward_pass_ref_f
 #ifdef WBFMM_USE_AVX
 #define wbfmm_downward_pass wbfmm_downward_pass_avx
 #define wbfmm_laplace_downward_pass wbfmm_laplace_downward_pass_avx

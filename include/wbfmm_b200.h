@@ -74,6 +74,10 @@ typedef struct {
                          keep their input order instead of the reference's
                          full-key order (t->ip differs inside leaves; boxes
                          and fields do not); fewer radix passes */
+  int keys_fp32;      /* 1: Morton keys, domain checks and target boxes in
+                         FP32 arithmetic, as the reference's single-precision
+                         build (its *_f API) computes them; points, origin
+                         and width must then be FP32 values */
 } wbfmm_b200_config_t;
 
 typedef struct wbfmm_b200_solver wbfmm_b200_solver_t;
@@ -214,6 +218,12 @@ void wbfmm_b200_managed_free(void *p);
 int wbfmm_b200_tree_structure(int n, const double *pts, int pstr,
                               const double *x0, double D, int depth,
                               uint32_t *ip, uint32_t *box_i, uint32_t *box_n);
+/* The same for FP32 points (pts[i*pstr + 0..2], stride in floats), with the
+   keys computed as the reference's single-precision build computes them
+   (wbfmm_tree_add_points_f / wbfmm_tree_refine_f). */
+int wbfmm_b200_tree_structure_f(int n, const float *pts, int pstr,
+                                const float *x0, float D, int depth,
+                                uint32_t *ip, uint32_t *box_i, uint32_t *box_n);
 
 /* M2L kernel selection (all need equal singular and regular orders, else
    the warp kernel runs): 1 (default) = automatic: lane-per-pair kernel up to

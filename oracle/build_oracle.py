@@ -59,8 +59,18 @@ def build_restatement(force: bool = False) -> str:
     return out
 
 
+# the sources the reference compiles a second time in single precision
+# (libsub, -DWBFMM_SINGLE_PRECISION: src/Makefile.am), giving its *_f API
+SINGLE_PRECISION = (
+    "expansions.c", "translations.c", "rotations.c", "rotations-laplace.c", "util.c",
+    "boxes.c", "shift.c", "shift-laplace.c", "shiftbw.c", "shiftbw-laplace.c", "pass.c",
+    "pass-laplace.c", "laplace.c", "targets.c", "gradient.c", "gradient-laplace.c",
+    "local.c", "local-laplace.c", "direct.c", "direct-laplace.c")
+
+
 def build_reference(force: bool = False) -> str | None:
-    """Compile the reference sources + shim + harness; None if absent."""
+    """Compile the reference sources + shim + harness; None if absent.  The
+    library holds both precisions, as the reference's own build does."""
     src_dir = os.path.join(REF_ROOT, "src")
     out = os.path.join(REF_OUT, "libwbfmm_ref.so")
     if not os.path.isdir(src_dir):
@@ -84,20 +94,39 @@ def build_reference(force: bool = False) -> str | None:
         if force or _newer(o, [s]):
             _run(["gcc", "-c", *REF_FLAGS, *incs, s, "-o", o])
         objs.append(o)
+    for s in srcs:
+        if os.path.basename(s) not in SINGLE_PRECISION:
+            continue
+        o = os.path.join(BUILD_DIR, os.path.basename(s)[:-2] + "-float.o")
+        if force or _newer(o, [s]):
+            _run(["gcc", "-c", *REF_FLAGS, "-DWBFMM_SINGLE_PRECISION", *incs, s, "-o", o])
+        objs.append(o)
     _run(["gcc", "-shared", "-fopenmp", "-o", out, *objs, "-lm", "-lpthread"])
     return out
 
 
 REPO = os.path.dirname(HERE)
-DRIVERS = ("wbfmm-tree-calc", "wbfmm-laplace-tree-calc")
+# driver name -> (source in tools/, substitutions of the reference's own
+# generation step: tools/make-source for double, tools/make-source-float for
+# single precision)
+_DOUBLE = (("WBFMM_REAL", "gdouble"), ("_FLOAT", ""), ("FLOATFMT", "lg"),
+           ("FLOATEXP", "1.16e"))
+_FLOAT = (("WBFMM_REAL", "gfloat"), ("_FLOAT", "_f"), ("FLOATFMT", "g"),
+          ("FLOATEXP", "1.16e"))
+DRIVER_SOURCES = {
+    "wbfmm-tree-calc": ("wbfmm-tree-calc", _DOUBLE),
+    "wbfmm-laplace-tree-calc": ("wbfmm-laplace-tree-calc", _DOUBLE),
+    "wbfmm-tree-calc-float": ("wbfmm-tree-calc", _FLOAT),
+    "wbfmm-laplace-tree-calc-float": ("wbfmm-laplace-tree-calc", _FLOAT),
+}
+DRIVERS = tuple(DRIVER_SOURCES)
 
 
-def _generate_driver(src_in: str, out: str) -> None:
-    """The reference's own generation step for its drivers (tools/make-source:
-    double precision names and formats)."""
+def _generate_driver(src_in: str, out: str, subs=_DOUBLE) -> None:
+    """The reference's own generation step for its drivers (tools/make-source,
+    tools/make-source-float: names and formats of one precision)."""
     text = open(src_in).read()
-    for a, b in (("WBFMM_REAL", "gdouble"), ("_FLOAT", ""), ("FLOATFMT", "lg"),
-                 ("FLOATEXP", "1.16e")):
+    for a, b in subs:
         text = text.replace(a, b)
     with open(out, "w") as f:
         f.write(text)
@@ -126,10 +155,11 @@ def build_reference_drivers(force: bool = False) -> dict | None:
     if force or _newer(shim_o, [shim]):
         _run(["gcc", "-O2", "-I", os.path.join(HERE, "shim"), "-c", shim, "-o", shim_o])
     for t, (ref_bin, b200_bin) in outs.items():
-        src_in = os.path.join(tools_dir, t + ".c.in")
+        base, subs = DRIVER_SOURCES[t]
+        src_in = os.path.join(tools_dir, base + ".c.in")
         gen = os.path.join(BUILD_DIR, t + ".c")
         if force or _newer(gen, [src_in, __file__]):
-            _generate_driver(src_in, gen)
+            _generate_driver(src_in, gen, subs)
         common = ["-O2", "-DHAVE_CONFIG_H", gen]
         if force or _newer(ref_bin, [gen, ref_lib]):
             _run(["gcc", *common, "-fopenmp", "-I", os.path.join(HERE, "shim"), "-I", REF_ROOT,

@@ -265,3 +265,63 @@ def test_reference_driver_on_dropin(gpu_lib, tmp_path, tool, args):
     assert np.array_equal(a[:, :3], b[:, :3])
     fa, fb = a[:, 3:], b[:, 3:]
     assert np.linalg.norm(fb - fa) <= 1e-10 * np.linalg.norm(fa)
+
+
+FLOAT_DRIVER_CASES = [
+    ("wbfmm-tree-calc-float", ["-b", "-d", "3", "-k", "4", "-R", "8", "-S", "8"]),
+    ("wbfmm-tree-calc-float", ["-b", "-d", "3", "-k", "4", "-t", "1e-6"]),
+    ("wbfmm-laplace-tree-calc-float", ["-b", "-d", "3", "-R", "8", "-S", "8"]),
+    ("wbfmm-laplace-tree-calc-float", ["-b", "-d", "3", "-R", "8", "-S", "8", "-g"]),
+    ("wbfmm-laplace-tree-calc-float", ["-b", "-d", "3", "-R", "8", "-S", "8", "-l"]),
+]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("tool,args", FLOAT_DRIVER_CASES,
+                         ids=lambda x: x if isinstance(x, str) else " ".join(x))
+def test_reference_float_driver_on_dropin(gpu_lib, tmp_path, tool, args):
+    """The reference's single-precision drivers (its own source through its
+    make-source-float step, calling the *_f API) built against the
+    reference's single-precision build and against this drop-in, whose *_f
+    calls run the engine's FP32 form.  The tree order the Helmholtz driver
+    writes (-w: t->ip after the refinements) is identical, since the keys
+    are computed in FP32 arithmetic as the reference's build computes them;
+    the fields agree with the reference's single- and double-precision
+    drivers to the FP32 level (the reference's own FP32 build is 7e-7 from
+    its FP64 build on these cases, and both print 6 digits)."""
+    bins = {k: os.path.join(ROOT, "oracle", "_ref", tool + suffix)
+            for k, suffix in (("ref", "-reference"), ("b200", "-b200"))}
+    bins["ref64"] = os.path.join(ROOT, "oracle", "_ref",
+                                 tool.replace("-float", "") + "-reference")
+    if not all(os.path.exists(b) for b in bins.values()):
+        pytest.skip("reference drivers not built (needs the reference sources)")
+    rng = np.random.default_rng(82)
+    n, nf = 3000, 200
+    f32 = lambda a: a.astype(np.float32).astype(np.float64)   # noqa: E731
+    xs = f32(rng.uniform(-0.5, 0.5, (n, 3)))
+    helm = tool.startswith("wbfmm-tree-calc")
+    q = f32(rng.standard_normal((n, 2 if helm else 1)))
+    # values that are exact FP32 numbers, written in full so that the float
+    # and double drivers read the same points
+    _write_points(tmp_path / "src.txt", np.hstack([xs, q]), q.shape[1], "M")
+    _write_points(tmp_path / "fld.txt", f32(rng.uniform(-0.5, 0.5, (nf, 3))), 0, "F")
+    env = dict(os.environ, MALLOC_MMAP_THRESHOLD_=str(32 << 20))
+
+    def run(b, extra=()):
+        r = subprocess.run([b, "-s", str(tmp_path / "src.txt"), "-f", str(tmp_path / "fld.txt"),
+                            *args, *extra], capture_output=True, text=True, timeout=300, env=env)
+        assert r.returncode == 0, r.stderr[-2000:]
+        return r
+
+    out = {k: _read_fields(run(b).stdout) for k, b in bins.items()}
+    for k in ("ref", "ref64"):
+        assert out[k].shape == out["b200"].shape and out["b200"].shape[0] == nf
+    f = {k: v[:, 3:] for k, v in out.items()}
+    tol = 2e-6
+    assert np.linalg.norm(f["b200"] - f["ref64"]) <= tol * np.linalg.norm(f["ref64"])
+    assert np.linalg.norm(f["b200"] - f["ref"]) <= tol * np.linalg.norm(f["ref"])
+    if helm and "-t" not in args:
+        order = [[line.split()[1] for line in run(bins[k], ["-w"]).stderr.splitlines()
+                  if len(line.split()) == 5 and line.split()[0].isdigit()]
+                 for k in ("ref", "b200")]
+        assert len(order[0]) == n and order[0] == order[1]

@@ -278,42 +278,46 @@ def test_laplace_fp32_deep_levels(gpu_lib, mode):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", ["cube_k1.5_depth4", "sphere_k2_depth4_skip", "cube_k3_depth5"])
+@pytest.mark.parametrize("case", ["cube_k7.8_n200000", "cube_k6.6_n190000", "sphere_k7_n150000"])
 def test_helmholtz_fp32_scaled_m2l(gpu_lib, case):
-    """Helmholtz at small k w and order 14: the (S|R) coefficients of the
-    finer levels are beyond the FP32 range unscaled, so those levels run the
+    """Helmholtz at order 14 with k w just below the unscaled FP32 range of
+    the leaf level's (S|R) table (2 k w in [0.8, 1]): those levels run the
     scaled M2L (sources x 2^(e l), table x 2^(-e (n + l)), results x
-    2^(e n)); the FP32 form is admitted by the range rule, finite, within
-    2e-6 of the FP64 form and as close to the direct sum."""
-    kind, kk, dd = case.split("_")[:3]
-    k, depth = float(kk[1:]), int(dd[5:])
-    if kind == "cube":
-        p = W.helmholtz_cube(40_000 if depth == 4 else 120_000, k=k, depth=depth, seed=91,
-                             lo=14, hi=40)
-        p.xt = p.xs[:4000]
-        p.targets_are_sources = False
-        skip = False
-    else:
-        p = W.helmholtz_sphere(40_000, 4000, k=k, depth=depth, seed=92, lo=14, hi=40)
-        skip = True
+    2^(e n)); the range rule admits the FP32 form, whose fields are finite
+    and within 1.5e-6 of the FP64 form and of the direct sum."""
+    kind, kk, nn = case.split("_")
+    k, n = float(kk[1:]), int(nn[1:])
+    rng = np.random.default_rng(91)
+    p = W.serve_request(rng, n, True, k, kind == "sphere")
+    assert p.depth == 4
+    assert 0.8 <= 2 * k * p.D / 16 < 1.02          # scaled at the leaf level
+    skip = kind == "sphere"
     cfg32 = engine.SolverConfig.from_problem(p, engine.FP32, skip_empty=skip)
     assert engine.fp32_range_ok(cfg32)
     outs = {}
     for prec in (engine.FP64, engine.FP32):
         cfg = engine.SolverConfig.from_problem(p, prec, skip_empty=skip)
         with engine.Solver(cfg) as s:
-            s.set_sources(p.xs, p.normals).set_strengths(p.q, p.dipoles).set_targets(p.xt).run()
+            s.set_sources(p.xs).set_strengths(p.q).set_targets(p.xs).run()
             outs[prec] = s.field()
     for a in outs[engine.FP32]:
         assert np.all(np.isfinite(a))
     for a, b in zip(outs[engine.FP32], outs[engine.FP64]):
-        assert rel_l2(a, b) < 2e-6, rel_l2(a, b)
-    idx = W.subsample(93, p.nt, 1500)
-    dpot, dgrad = engine.direct(p.problem, p.xs, p.q, p.xt[idx], k=p.k, normals=p.normals,
-                                dipoles=p.dipoles)
+        assert rel_l2(a, b) < 1.5e-6, rel_l2(a, b)
+    idx = W.subsample(93, p.ns, 1500)
+    dpot, dgrad = engine.direct(p.problem, p.xs, p.q, p.xs[idx], k=p.k)
     pot, grad = outs[engine.FP32]
-    assert rel_l2(pot.reshape(-1, 2)[idx].ravel(), dpot) < 1e-5
-    assert rel_l2(grad.reshape(-1, 6)[idx].ravel(), dgrad) < 1e-4
+    assert rel_l2(pot.reshape(-1, 2)[idx].ravel(), dpot) < 1.5e-6
+    assert rel_l2(grad.reshape(-1, 6)[idx].ravel(), dgrad) < 1.5e-6
+
+
+def test_helmholtz_fp32_rule_low_kw(gpu_lib):
+    """Below 2 k w = 0.8 at the leaves the FP32 form loses accuracy to
+    cancellation (low-frequency regime); the range rule sends such requests
+    to the FP64 form."""
+    p = W.serve_request(np.random.default_rng(92), 40_000, True, 1.5, False)
+    assert 2 * 1.5 * p.D / 2 ** p.depth < 0.8
+    assert not engine.fp32_range_ok(engine.SolverConfig.from_problem(p, engine.FP32))
 
 
 @pytest.mark.gpu

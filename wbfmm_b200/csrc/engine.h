@@ -59,19 +59,22 @@ int ensure_smem(size_t bytes) {
 // *a = va and, when b is non-null, *b = vb (one thread, on stream s)
 void launch_set_words(uint32_t* a, uint32_t va, uint32_t* b, uint32_t vb,
                       cudaStream_t s);
-// keys[i] = Morton key of point i (src/boxes.c:324-339); vals[i] = i
+// keys[i] = Morton key of point i (src/boxes.c:324-339); vals[i] = i.
+// f32: in FP32 arithmetic, as the single-precision build (the *_f API), on
+// coordinates, origin and width that are FP32 values
 void launch_point_keys(const double* pts, int64_t pstr, int n,
                        const double* x0, double D, uint64_t* keys,
-                       uint32_t* vals, cudaStream_t s);
+                       uint32_t* vals, cudaStream_t s, bool f32 = false);
 // target leaf boxes by floor((x-x0)/wb) (src/boxes.c:585-634); vals[i] = i;
 // points outside the closed cube set *bad (host-visible flag) to 1
 void launch_target_keys(const double* pts, int64_t pstr, int n,
                         const double* x0, double D, int level,
                         uint64_t* keys, uint32_t* vals, int* bad,
-                        cudaStream_t s);
+                        cudaStream_t s, bool f32 = false);
 // strict-interior domain check of sources (src/boxes.c:148-153)
 void launch_domain_check(const double* pts, int64_t pstr, int n,
-                         const double* x0, double D, int* bad, cudaStream_t s);
+                         const double* x0, double D, int* bad, cudaStream_t s,
+                         bool f32 = false);
 
 struct RadixScratch {
   uint64_t* keys_alt = nullptr;

@@ -105,10 +105,14 @@ int wbfmm_b200_fp32_range_ok(const wbfmm_b200_config_t* c) {
     const int N = 2 * p;
     // the level's (S|R) table holds degrees n + l up to 2p, about
     // (2N-1)!! / x^(N+1): beyond the FP32 range the M2L runs in its scaled
-    // form (helm_m2l_exp; tile kernel, equal orders), otherwise the form is
-    // out of range
+    // form (helm_m2l_exp; tile kernel, equal orders), exact in itself, but
+    // admitted only for x >= 0.8: at smaller k w the real parts of the
+    // fields come from the cancellation of much larger imaginary-part terms
+    // (h_n(x) ~ -i y_n(x)), and the FP32 form was measured to lose accuracy
+    // there (relative L2 against FP64 at order 14: below 1e-6 for x >= 0.8,
+    // 2e-6 at x = 0.5, 9e-6 at x = 0.15; unchanged by the scaling)
     if (x < N && log10_dfact(2 * N - 1) - (N + 1) * log10(x) > 36.0 &&
-        !wbfmm::helm_m2l_scalable(c->order_s[l], c->order_r[l]))
+        !(wbfmm::helm_m2l_scalable(c->order_s[l], c->order_r[l]) && x >= 0.8))
       return 0;
     // local coefficients, stored unscaled, reach about (2p-1)!! / x^(p+1)
     // per unit strength at the nearest list-4 distance
@@ -275,9 +279,9 @@ void* wbfmm_b200_managed_alloc(size_t bytes) {
 void wbfmm_b200_managed_free(void* p) {
   if (p) cudaFree(p);
 }
-int wbfmm_b200_tree_structure(int n, const double* pts, int pstr,
-                              const double* x0, double D, int depth,
-                              uint32_t* ip, uint32_t* box_i, uint32_t* box_n) {
+static int tree_structure(int n, const double* pts, int pstr, const double* x0, double D,
+                          int depth, int keys_fp32, uint32_t* ip, uint32_t* box_i,
+                          uint32_t* box_n) {
   if (depth < 0 || depth > 10) return set_error(WBFMM_B200_E_ARG, "depth must be in [0, 10]");
   if (wbfmm_b200_device_count() < 1)
     return set_error(WBFMM_B200_E_NOGPU, "no CUDA device is available");
@@ -287,6 +291,7 @@ int wbfmm_b200_tree_structure(int n, const double* pts, int pstr,
   c.depth = depth;
   c.x0[0] = x0[0]; c.x0[1] = x0[1]; c.x0[2] = x0[2];
   c.D = D;
+  c.keys_fp32 = keys_fp32;
   Solver<double> sv;
   sv.tree_only = true;
   int rc = sv.init(&c, nullptr);
@@ -300,6 +305,22 @@ int wbfmm_b200_tree_structure(int n, const double* pts, int pstr,
     off += (size_t)1 << (3 * l);
   }
   return 0;
+}
+int wbfmm_b200_tree_structure(int n, const double* pts, int pstr,
+                              const double* x0, double D, int depth,
+                              uint32_t* ip, uint32_t* box_i, uint32_t* box_n) {
+  return tree_structure(n, pts, pstr, x0, D, depth, 0, ip, box_i, box_n);
+}
+int wbfmm_b200_tree_structure_f(int n, const float* pts, int pstr,
+                                const float* x0, float D, int depth,
+                                uint32_t* ip, uint32_t* box_i, uint32_t* box_n) {
+  if (n < 0 || (n > 0 && (!pts || pstr < 3)) || !x0)
+    return set_error(WBFMM_B200_E_ARG, "bad points");
+  std::vector<double> p64((size_t)3 * (n > 0 ? n : 1));
+  for (int i = 0; i < n; i++)
+    for (int a = 0; a < 3; a++) p64[3 * (size_t)i + a] = pts[(size_t)i * pstr + a];
+  const double o64[3] = {x0[0], x0[1], x0[2]};
+  return tree_structure(n, p64.data(), 3, o64, (double)D, depth, 1, ip, box_i, box_n);
 }
 int wbfmm_b200_set_m2l_kernel(wbfmm_b200_solver_t* s, int mode) {
   if (!s) return set_error(WBFMM_B200_E_ARG, "null solver");

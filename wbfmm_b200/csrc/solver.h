@@ -400,7 +400,7 @@ struct Solver : public wbfmm_b200_solver {
     }
     // strict-interior domain check (src/boxes.c:148-153)
     launch_set_words((uint32_t*)flag.p, 0x7fffffffu, nullptr, 0, stream);
-    launch_domain_check(dpts, xs_str, n, cfg.x0, cfg.D, flag.p, stream);
+    launch_domain_check(dpts, xs_str, n, cfg.x0, cfg.D, flag.p, stream, cfg.keys_fp32 != 0);
     if (!async_checks) {
       int bad = 0;
       WBFMM_CUDA(cudaMemcpyAsync(&bad, flag.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
@@ -409,7 +409,7 @@ struct Solver : public wbfmm_b200_solver {
     }
     WBFMM_TRY(keys.alloc(n));
     WBFMM_TRY(ip.alloc(n));
-    launch_point_keys(dpts, xs_str, n, cfg.x0, cfg.D, keys.p, ip.p, stream);
+    launch_point_keys(dpts, xs_str, n, cfg.x0, cfg.D, keys.p, ip.p, stream, cfg.keys_fp32 != 0);
     // full 60-bit keys (the reference's point order), or with leaf_order
     // only the bits that select the leaf box
     const int sort_lo = cfg.leaf_order ? 60 - 3 * depth : 0;
@@ -520,7 +520,7 @@ struct Solver : public wbfmm_b200_solver {
         d = tpts_in.p;
       }
       launch_target_keys(d, tstr, n, cfg.x0, cfg.D, depth, tkeys.p, tperm.p,
-                         flag.p + 1, stream);
+                         flag.p + 1, stream, cfg.keys_fp32 != 0);
       WBFMM_TRY(radix_sort_pairs(tkeys.p, tperm.p, n, 3 * depth, &rs, stream));
       launch_gather_points(d, tstr, tperm.p, n, tx.p, ty.p, tz.p, stream);
       k_u64_to_u32<<<(n + 255) / 256, 256, 0, stream>>>(tkeys.p, tbox.p, n);

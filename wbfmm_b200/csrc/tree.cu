@@ -26,16 +26,26 @@ const char* last_error() { return g_err; }
 // ------------------------------------------------------------------- keys
 // (x - c)/D*2^20 truncated per axis: the division comes first and the
 // scaling by 2^20 is exact, so this is bit-identical to the host formula
+// With f32, the single-precision build's arithmetic (src/boxes.c:324-339
+// compiled with WBFMM_REAL = gfloat): coordinates, origin and width are
+// FP32 values (held exactly in the FP64 inputs) and every step rounds to
+// FP32.
+__device__ __forceinline__ uint32_t key_coord(double x, double x0, double D, bool f32) {
+  if (f32)
+    return (uint32_t)__fmul_rn(__fdiv_rn(__fsub_rn((float)x, (float)x0), (float)D), 1048576.0f);
+  return (uint32_t)(__ddiv_rn(__dsub_rn(x, x0), D) * 1048576.0);
+}
+
 __global__ void k_point_keys(const double* __restrict__ pts, int64_t pstr,
                              int n, double x0, double y0, double z0, double D,
                              uint64_t* __restrict__ keys,
-                             uint32_t* __restrict__ vals) {
+                             uint32_t* __restrict__ vals, bool f32) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double* p = pts + (int64_t)i * pstr;
-  uint32_t xi = (uint32_t)(__ddiv_rn(__dsub_rn(p[0], x0), D) * 1048576.0);
-  uint32_t yi = (uint32_t)(__ddiv_rn(__dsub_rn(p[1], y0), D) * 1048576.0);
-  uint32_t zi = (uint32_t)(__ddiv_rn(__dsub_rn(p[2], z0), D) * 1048576.0);
+  uint32_t xi = key_coord(p[0], x0, D, f32);
+  uint32_t yi = key_coord(p[1], y0, D, f32);
+  uint32_t zi = key_coord(p[2], z0, D, f32);
   // Points strictly inside the cube give 20-bit coordinates.  Anything else
   // (rejected by the domain check, which the served form reads back only
   // after the solve) is clamped so every key stays below 2^60 and every box
@@ -48,30 +58,47 @@ __global__ void k_point_keys(const double* __restrict__ pts, int64_t pstr,
 
 void launch_point_keys(const double* pts, int64_t pstr, int n,
                        const double* x0, double D, uint64_t* keys,
-                       uint32_t* vals, cudaStream_t s) {
+                       uint32_t* vals, cudaStream_t s, bool f32) {
   if (n <= 0) return;
   k_point_keys<<<(n + 255) / 256, 256, 0, s>>>(pts, pstr, n, x0[0], x0[1],
-                                               x0[2], D, keys, vals);
+                                               x0[2], D, keys, vals, f32);
+}
+
+// wbfmm_point_box (src/boxes.c:585-634); with f32 in FP32 arithmetic
+__device__ __forceinline__ bool outside_closed(double x, double x0, double D, bool f32) {
+  if (f32) {
+    const float xf = (float)x, x0f = (float)x0;
+    return xf < x0f || xf > __fadd_rn(x0f, (float)D);
+  }
+  return x < x0 || x > x0 + D;
+}
+__device__ __forceinline__ uint32_t box_coord(double x, double x0, double D, int level, bool f32) {
+  if (f32) {
+    const float wb = __fdiv_rn((float)D, (float)(1u << level));
+    return (uint32_t)floorf(__fdiv_rn(__fsub_rn((float)x, (float)x0), wb));
+  }
+  const double wb = __ddiv_rn(D, (double)(1u << level));
+  return (uint32_t)floor(__ddiv_rn(__dsub_rn(x, x0), wb));
 }
 
 __global__ void k_target_keys(const double* __restrict__ pts, int64_t pstr,
                               int n, double x0, double y0, double z0, double D,
                               int level, uint64_t* __restrict__ keys,
-                              uint32_t* __restrict__ vals, int* bad) {
+                              uint32_t* __restrict__ vals, int* bad, bool f32) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double* p = pts + (int64_t)i * pstr;
   double x = p[0], y = p[1], z = p[2];
-  if (x < x0 || x > x0 + D || y < y0 || y > y0 + D || z < z0 || z > z0 + D) {
+  if (outside_closed(x, x0, D, f32) || outside_closed(y, y0, D, f32) ||
+      outside_closed(z, z0, D, f32)) {
     *bad = 1;
     keys[i] = 0;
     vals[i] = (uint32_t)i;
     return;
   }
-  double wb = __ddiv_rn(D, (double)(1u << level));
-  uint32_t a = (uint32_t)floor(__ddiv_rn(__dsub_rn(x, x0), wb));
-  uint32_t b = (uint32_t)floor(__ddiv_rn(__dsub_rn(y, y0), wb));
-  uint32_t c = (uint32_t)floor(__ddiv_rn(__dsub_rn(z, z0), wb));
+  uint32_t a = box_coord(x, x0, D, level, f32);
+  uint32_t b = box_coord(y, y0, D, level, f32);
+  uint32_t c = box_coord(z, z0, D, level, f32);
   // a point on the upper face gives 2^level; the reference then indexes
   // out of its box array, here the index is clamped into the last box
   uint32_t nb = 1u << level;
@@ -96,29 +123,39 @@ void launch_set_words(uint32_t* a, uint32_t va, uint32_t* b, uint32_t vb,
 void launch_target_keys(const double* pts, int64_t pstr, int n,
                         const double* x0, double D, int level,
                         uint64_t* keys, uint32_t* vals, int* bad,
-                        cudaStream_t s) {
+                        cudaStream_t s, bool f32) {
   if (n <= 0) return;
   k_target_keys<<<(n + 255) / 256, 256, 0, s>>>(pts, pstr, n, x0[0], x0[1],
                                                 x0[2], D, level, keys, vals,
-                                                bad);
+                                                bad, f32);
+}
+
+// strict interior (src/boxes.c:148-153); with f32 in FP32 arithmetic
+__device__ __forceinline__ bool outside_open(double x, double x0, double D, bool f32) {
+  if (f32) {
+    const float xf = (float)x, x0f = (float)x0;
+    return xf <= x0f || xf >= __fadd_rn(x0f, (float)D);
+  }
+  return x <= x0 || x >= x0 + D;
 }
 
 __global__ void k_domain_check(const double* __restrict__ pts, int64_t pstr,
                                int n, double x0, double y0, double z0,
-                               double D, int* bad) {
+                               double D, int* bad, bool f32) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double* p = pts + (int64_t)i * pstr;
-  if (p[0] <= x0 || p[0] >= x0 + D || p[1] <= y0 || p[1] >= y0 + D ||
-      p[2] <= z0 || p[2] >= z0 + D)
+  if (outside_open(p[0], x0, D, f32) || outside_open(p[1], y0, D, f32) ||
+      outside_open(p[2], z0, D, f32))
     atomicMin(bad, i);
 }
 
 void launch_domain_check(const double* pts, int64_t pstr, int n,
-                         const double* x0, double D, int* bad, cudaStream_t s) {
+                         const double* x0, double D, int* bad, cudaStream_t s,
+                         bool f32) {
   if (n <= 0) return;
   k_domain_check<<<(n + 255) / 256, 256, 0, s>>>(pts, pstr, n, x0[0], x0[1],
-                                                 x0[2], D, bad);
+                                                 x0[2], D, bad, f32);
 }
 
 // ------------------------------------------------------------ radix sort

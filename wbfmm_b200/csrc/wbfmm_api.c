@@ -34,11 +34,13 @@ typedef struct {
   wbfmm_b200_solver_t *s;
   double k;
   int ready;                     /* solver holds the current points */
-  const double *q, *dip;         /* strengths last uploaded */
+  const void *q, *dip;           /* strengths last uploaded */
   int qstr, dstr;
   const void *targets;           /* target set last uploaded */
   guint ntargets;
   gboolean managed[2][WBFMM_TREE_MAX_DEPTH + 1];
+  int fp32;                      /* a tree of the single-precision API (*_f) */
+  double *pts64, *nrm64;         /* FP64 copies of FP32 points and normals */
 } dtree_t;
 
 #define DT(_t) ((dtree_t *)(_t))
@@ -49,6 +51,30 @@ static void drop_solver(dtree_t *d) {
   d->ready = 0;
   d->q = d->dip = NULL;
   d->targets = NULL;
+}
+
+/* n records of 3 FP32 values at a byte stride, as 3 n doubles (exact) */
+static double *widen3(const char *p, gsize stride, guint n) {
+  double *o = malloc(sizeof(double) * 3 * (n ? n : 1));
+  guint i;
+  int a;
+  if (!o) die("wbfmm", "out of memory");
+  for (i = 0; i < n; i++)
+    for (a = 0; a < 3; a++) o[3 * (size_t)i + a] = ((const float *)(p + (size_t)i * stride))[a];
+  return o;
+}
+
+/* n strengths of w values at a stride of `str` FP32 values, as doubles */
+static double *widen_strengths(const float *q, gint str, guint n, int w) {
+  double *o;
+  guint i;
+  int c;
+  if (!q) return NULL;
+  o = malloc(sizeof(double) * w * (n ? n : 1));
+  if (!o) die("wbfmm", "out of memory");
+  for (i = 0; i < n; i++)
+    for (c = 0; c < w; c++) o[(size_t)i * w + c] = q[(size_t)i * str + c];
+  return o;
 }
 
 static uint64_t spread3(uint64_t v) {
@@ -91,11 +117,18 @@ static void refresh_boxes(wbfmm_tree_t *t) {
   for (l = 0; l <= t->depth; l++) total += (size_t)1 << (3 * l);
   bi = malloc(sizeof(uint32_t) * total);
   bn = malloc(sizeof(uint32_t) * total);
-  check("wbfmm_tree_refine",
-        wbfmm_b200_tree_structure((int)t->npoints, (const double *)t->points,
-                                  (int)(t->pstr / sizeof(double)),
-                                  (const double *)t->x, t->D, (int)t->depth,
-                                  t->ip, bi, bn));
+  if (DT(t)->fp32)
+    check("wbfmm_tree_refine_f",
+          wbfmm_b200_tree_structure_f((int)t->npoints, (const float *)t->points,
+                                      (int)(t->pstr / sizeof(float)),
+                                      (const float *)t->x, (float)t->D, (int)t->depth,
+                                      t->ip, bi, bn));
+  else
+    check("wbfmm_tree_refine",
+          wbfmm_b200_tree_structure((int)t->npoints, (const double *)t->points,
+                                    (int)(t->pstr / sizeof(double)),
+                                    (const double *)t->x, t->D, (int)t->depth,
+                                    t->ip, bi, bn));
   for (l = 0; l <= t->depth; l++) {
     size_t nb = (size_t)1 << (3 * l), b;
     for (b = 0; b < nb; b++) {
@@ -181,19 +214,19 @@ static void coefficient_init(wbfmm_tree_t *t, guint l, guint nr, guint ns,
   d->managed[0][l] = d->managed[1][l] = FALSE;
   if (ns) {
     nc = (size_t)(ns + 1) * (ns + 1);
-    t->mps[l] = wbfmm_b200_managed_alloc(nb * nc * w * sizeof(double));
+    t->mps[l] = wbfmm_b200_managed_alloc(nb * nc * w * t->size);
     if (!t->mps[l]) die("wbfmm_tree_coefficient_init", wbfmm_b200_last_error());
     d->managed[0][l] = TRUE;
     for (b = 0; b < nb; b++)
-      t->boxes[l][b].mps = (double *)t->mps[l] + ((b & ~7) * nc + (b & 7)) * w;
+      t->boxes[l][b].mps = (char *)t->mps[l] + ((b & ~7) * nc + (b & 7)) * w * t->size;
   }
   if (nr) {
     nc = (size_t)(nr + 1) * (nr + 1);
-    t->mpr[l] = wbfmm_b200_managed_alloc(nb * nc * w * sizeof(double));
+    t->mpr[l] = wbfmm_b200_managed_alloc(nb * nc * w * t->size);
     if (!t->mpr[l]) die("wbfmm_tree_coefficient_init", wbfmm_b200_last_error());
     d->managed[1][l] = TRUE;
     for (b = 0; b < nb; b++)
-      t->boxes[l][b].mpr = (double *)t->mpr[l] + ((b & ~7) * nc + (b & 7)) * w;
+      t->boxes[l][b].mpr = (char *)t->mpr[l] + ((b & ~7) * nc + (b & 7)) * w * t->size;
   }
 }
 
@@ -212,22 +245,23 @@ gint wbfmm_tree_laplace_coefficient_init(wbfmm_tree_t *t, guint l, guint nr,
   return 0;
 }
 
-static size_t level_doubles(wbfmm_tree_t *t, guint l, guint p) {
+/* bytes of a level's coefficient array of order p */
+static size_t level_bytes(wbfmm_tree_t *t, guint l, guint p) {
   return ((size_t)1 << (3 * l)) * (size_t)(p + 1) * (p + 1) *
-         (t->problem == WBFMM_PROBLEM_HELMHOLTZ ? 2 : 1);
+         (t->problem == WBFMM_PROBLEM_HELMHOLTZ ? 2 : 1) * t->size;
 }
 
 /* src/boxes.c:636-673 */
 gint wbfmm_tree_coefficient_clear(wbfmm_tree_t *t, guint l) {
-  if (t->mps[l]) memset(t->mps[l], 0, level_doubles(t, l, t->order_s[l]) * sizeof(double));
-  if (t->mpr[l]) memset(t->mpr[l], 0, level_doubles(t, l, t->order_r[l]) * sizeof(double));
+  if (t->mps[l]) memset(t->mps[l], 0, level_bytes(t, l, t->order_s[l]));
+  if (t->mpr[l]) memset(t->mpr[l], 0, level_bytes(t, l, t->order_r[l]));
   return 0;
 }
 
 /* src/tree.c:137-153 */
 gint wbfmm_tree_coefficients_zero(wbfmm_tree_t *t, guint level) {
   if (t->mpr[level])
-    memset(t->mpr[level], 0, level_doubles(t, level, t->order_r[level]) * sizeof(double));
+    memset(t->mpr[level], 0, level_bytes(t, level, t->order_r[level]));
   return 0;
 }
 
@@ -481,41 +515,66 @@ static wbfmm_b200_solver_t *solver_for(wbfmm_tree_t *t, double k,
     c.order_r[l] = (int)t->order_r[l];
   }
   c.k = k;
-  memcpy(c.x0, t->x, sizeof(c.x0));
+  if (d->fp32) {
+    const float *xf = (const float *)t->x;
+    c.x0[0] = xf[0]; c.x0[1] = xf[1]; c.x0[2] = xf[2];
+  } else {
+    memcpy(c.x0, t->x, sizeof(c.x0));
+  }
   c.D = t->D;
-  c.precision = WBFMM_B200_FP64;
+  /* the single-precision API runs the FP32 form, with the tree's keys and
+     boxes computed as the reference's single-precision build does */
+  c.precision = d->fp32 ? WBFMM_B200_FP32 : WBFMM_B200_FP64;
+  c.keys_fp32 = d->fp32;
   c.field = WBFMM_B200_POTENTIAL | WBFMM_B200_GRADIENT;
   c.managed = 1;
   check(fn, wbfmm_b200_solver_create(&d->s, &c, NULL));
   for (l = 1; l <= t->depth; l++)
     check(fn, wbfmm_b200_adopt_coefficients(d->s, (int)l, t->mps[l], t->mpr[l]));
-  check(fn, wbfmm_b200_set_sources(d->s, (int)t->npoints, (const double *)t->points,
-                                   (int)(t->pstr / sizeof(double)),
-                                   (const double *)t->normals,
-                                   (int)(t->nstr / sizeof(double)), 0));
+  if (d->fp32) {
+    free(d->pts64);
+    free(d->nrm64);
+    d->pts64 = widen3(t->points, t->pstr, t->npoints);
+    d->nrm64 = t->normals ? widen3(t->normals, t->nstr, t->npoints) : NULL;
+    check(fn, wbfmm_b200_set_sources(d->s, (int)t->npoints, d->pts64, 3, d->nrm64, 3, 0));
+  } else {
+    check(fn, wbfmm_b200_set_sources(d->s, (int)t->npoints, (const double *)t->points,
+                                     (int)(t->pstr / sizeof(double)),
+                                     (const double *)t->normals,
+                                     (int)(t->nstr / sizeof(double)), 0));
+  }
   d->k = k;
   d->ready = 1;
   return d->s;
 }
 
-static void strengths_for(dtree_t *d, const double *q, int qstr,
-                          const double *dip, int dstr, const char *fn) {
+/* strengths q[i*qstr], dip[i*dstr] (doubles, or floats for an FP32 tree) */
+static void strengths_for(dtree_t *d, const void *q, int qstr,
+                          const void *dip, int dstr, const char *fn) {
   if (d->q == q && d->qstr == qstr && d->dip == dip && d->dstr == dstr && (q || dip))
     return;
   if (dip && !d->t.normals) die(fn, "no normals in tree but dipole strengths specified");
-  check(fn, wbfmm_b200_set_strengths(d->s, q, qstr, dip, dstr, 0));
+  if (d->fp32) {
+    const int w = d->t.problem == WBFMM_PROBLEM_HELMHOLTZ ? 2 : 1;
+    double *q64 = widen_strengths(q, qstr, d->t.npoints, w);
+    double *d64 = widen_strengths(dip, dstr, d->t.npoints, w);
+    check(fn, wbfmm_b200_set_strengths(d->s, q64, w, d64, w, 0));
+    free(q64);
+    free(d64);
+  } else {
+    check(fn, wbfmm_b200_set_strengths(d->s, q, qstr, dip, dstr, 0));
+  }
   d->q = q; d->qstr = qstr; d->dip = dip; d->dstr = dstr;
 }
 
 /* ---------------------------------------------------------- passes */
-static gint leaf(wbfmm_tree_t *t, double k, gdouble *src, gint sstr,
-                 gdouble *dipoles, gint dstr, gboolean zero, const char *fn) {
+static gint leaf(wbfmm_tree_t *t, double k, const void *src, gint sstr,
+                 const void *dipoles, gint dstr, gboolean zero, const char *fn) {
   dtree_t *d = DT(t);
   wbfmm_b200_solver_t *s = solver_for(t, k, fn);
   if (!src && !dipoles) {
     if (zero)
-      memset(t->mps[t->depth], 0,
-             level_doubles(t, t->depth, t->order_s[t->depth]) * sizeof(double));
+      memset(t->mps[t->depth], 0, level_bytes(t, t->depth, t->order_s[t->depth]));
     return 0;
   }
   d->q = d->dip = NULL;       /* strengths may have changed in place */
@@ -604,7 +663,7 @@ gint wbfmm_laplace_downward_pass_avx(wbfmm_tree_t *t,
    both are asked for) */
 static void evaluate_targets(dtree_t *d, const void *key, guint n,
                              const double *x, int xstr, guint field,
-                             gboolean neighbours, double *f, gint fstr,
+                             gboolean neighbours, void *fv, gint fstr,
                              const char *fn) {
   int w = d->t.problem == WBFMM_PROBLEM_HELMHOLTZ ? 2 : 1;
   int want = (field & WBFMM_FIELD_POTENTIAL ? WBFMM_B200_POTENTIAL : 0) |
@@ -613,6 +672,7 @@ static void evaluate_targets(dtree_t *d, const void *key, guint n,
   guint i;
   int c, off;
   if (d->targets != key || d->ntargets != n || !key) {
+    if (!x) die(fn, "targets are not in place");
     check(fn, wbfmm_b200_set_targets(d->s, (int)n, x, xstr, 0));
     d->targets = key;
     d->ntargets = n;
@@ -622,16 +682,26 @@ static void evaluate_targets(dtree_t *d, const void *key, guint n,
   if (want & WBFMM_B200_POTENTIAL) pot = malloc(sizeof(double) * n * w);
   if (want & WBFMM_B200_GRADIENT) grad = malloc(sizeof(double) * n * 3 * w);
   check(fn, wbfmm_b200_get_field(d->s, pot, grad, 0));
-  for (i = 0; i < n; i++) {
-    off = 0;
-    if (pot) {
-      for (c = 0; c < w; c++) f[(size_t)i * fstr + c] += pot[(size_t)i * w + c];
-      off = w;
-    }
-    if (grad)
-      for (c = 0; c < 3 * w; c++)
-        f[(size_t)i * fstr + off + c] += grad[(size_t)i * 3 * w + c];
-  }
+  /* fields added into the caller's doubles, or floats for an FP32 tree */
+#define WBFMM_ADD_FIELDS(_T)                                                  \
+  do {                                                                        \
+    _T *f = (_T *)fv;                                                         \
+    for (i = 0; i < n; i++) {                                                 \
+      off = 0;                                                                \
+      if (pot) {                                                              \
+        for (c = 0; c < w; c++) f[(size_t)i * fstr + c] += (_T)pot[(size_t)i * w + c]; \
+        off = w;                                                              \
+      }                                                                       \
+      if (grad)                                                               \
+        for (c = 0; c < 3 * w; c++)                                           \
+          f[(size_t)i * fstr + off + c] += (_T)grad[(size_t)i * 3 * w + c];   \
+    }                                                                         \
+  } while (0)
+  if (d->fp32)
+    WBFMM_ADD_FIELDS(float);
+  else
+    WBFMM_ADD_FIELDS(double);
+#undef WBFMM_ADD_FIELDS
   free(pot);
   free(grad);
 }
@@ -712,8 +782,14 @@ gint wbfmm_target_list_coefficients_init(wbfmm_target_list_t *l, guint field) {
 static gint list_prepare(wbfmm_target_list_t *l, double k, const char *fn) {
   dtree_t *d = DT(l->t);
   solver_for(l->t, k, fn);
-  check(fn, wbfmm_b200_set_targets(d->s, (int)l->npoints, (const double *)l->points,
-                                   (int)(l->pstr / sizeof(double)), 0));
+  if (d->fp32) {
+    double *x64 = widen3(l->points, l->pstr, l->npoints);
+    check(fn, wbfmm_b200_set_targets(d->s, (int)l->npoints, x64, 3, 0));
+    free(x64);
+  } else {
+    check(fn, wbfmm_b200_set_targets(d->s, (int)l->npoints, (const double *)l->points,
+                                     (int)(l->pstr / sizeof(double)), 0));
+  }
   d->targets = l;
   d->ntargets = l->npoints;
   return 0;
@@ -733,19 +809,319 @@ gint wbfmm_laplace_target_list_local_coefficients(wbfmm_target_list_t *l,
 }
 
 /* src/targets.c:424-603 */
+static gint list_field(wbfmm_target_list_t *l, const void *src, gint sstr,
+                       const void *nsrc, gint nstr, void *f, gint fstr, const char *fn) {
+  dtree_t *d = DT(l->t);
+  if (!l->field) die(fn, "field not set (wbfmm_target_list_coefficients_init)");
+  if (l->field & (WBFMM_FIELD_CURL | WBFMM_FIELD_CURL_GRADIENT))
+    die(fn, "curl fields are not supported");
+  if (!d->s || !d->ready) list_prepare(l, d->k, fn);
+  if (src || nsrc) strengths_for(d, src, sstr, nsrc, nstr, fn);
+  if (d->targets != l || d->ntargets != l->npoints) list_prepare(l, d->k, fn);
+  /* the targets are in place (list_prepare), so no points are passed */
+  evaluate_targets(d, l, l->npoints, NULL, 3, l->field, (src || nsrc), f, fstr, fn);
+  return 0;
+}
+
 gint wbfmm_target_list_local_field(wbfmm_target_list_t *l, gdouble *src,
                                    gint sstr, gdouble *nsrc, gint nstr,
                                    gdouble *f, gint fstr) {
-  dtree_t *d = DT(l->t);
-  if (!l->field) die(__func__, "field not set (wbfmm_target_list_coefficients_init)");
-  if (l->field & (WBFMM_FIELD_CURL | WBFMM_FIELD_CURL_GRADIENT))
-    die(__func__, "curl fields are not supported");
-  if (!d->s || !d->ready) list_prepare(l, d->k, __func__);
-  if (src || nsrc) strengths_for(d, src, sstr, nsrc, nstr, __func__);
-  evaluate_targets(d, l, l->npoints, (const double *)l->points,
-                   (int)(l->pstr / sizeof(double)), l->field, (src || nsrc), f,
-                   fstr, __func__);
+  return list_field(l, src, sstr, nsrc, nstr, f, fstr, __func__);
+}
+
+/* ------------------------------------------ single precision (*_f) */
+/* The reference's single-precision API: the same sources compiled with
+   WBFMM_REAL = gfloat (its libsub, src/Makefile.am), trees holding FP32
+   points, origin and coefficients.  Here an FP32 tree runs the engine's
+   FP32 form; its Morton keys, domain checks and target boxes are computed
+   in FP32 arithmetic as the reference's build computes them, so t->ip and
+   every box {i, n} are those of the reference's *_f calls.  Operator
+   tables are generated in FP64 on the GPU and rounded, near-field sums
+   are accumulated in FP64. */
+
+/* src/boxes.c:58-91 */
+wbfmm_tree_t *wbfmm_tree_new_f(gfloat *x, gfloat D, guint maxpoints) {
+  dtree_t *d = calloc(1, sizeof(dtree_t));
+  wbfmm_tree_t *t;
+  float *xt;
+  if (!d) die(__func__, "out of memory");
+  d->fp32 = 1;
+  t = &d->t;
+  t->maxpoints = maxpoints;
+  t->ip = malloc(sizeof(guint) * (maxpoints ? maxpoints : 1));
+  t->boxes[0] = calloc(1, sizeof(wbfmm_box_t));
+  t->size = sizeof(gfloat);
+  xt = (float *)t->x;
+  xt[0] = x[0]; xt[1] = x[1]; xt[2] = x[2];
+  t->D = D;
+  return t;
+}
+
+static void need_fp32(wbfmm_tree_t *t, const char *fn) {
+  if (t->size != sizeof(gfloat))
+    die(fn, "mixed precision not implemented (tree is not single precision)");
+}
+
+/* src/boxes.c:118-166 */
+gint wbfmm_tree_add_points_f(wbfmm_tree_t *t, gpointer pts, gsize pstr,
+                             gpointer normals, gsize nstr, guint npts,
+                             gboolean sorted) {
+  need_fp32(t, __func__);
+  if (npts > t->maxpoints) die(__func__, "too many points for tree");
+  if (pstr % sizeof(float) || (normals && nstr % sizeof(float)))
+    die(__func__, "point and normal strides must be multiples of sizeof(float)");
+  t->npoints = npts;
+  t->points = (char *)pts;
+  t->pstr = pstr;
+  t->normals = (char *)normals;
+  t->nstr = nstr;
+  t->sorted = sorted;
+  drop_solver(DT(t));
+  refresh_boxes(t);
+  t->boxes[0][0].i = 0;
+  t->boxes[0][0].n = npts;
   return 0;
+}
+
+/* src/boxes.c:190-206 */
+gint wbfmm_tree_sort_points_f(wbfmm_tree_t *t, gpointer pts, gsize psize, guint npts) {
+  uint32_t *ip = malloc(sizeof(uint32_t) * (npts ? npts : 1));
+  char *tmp = malloc(psize * (npts ? npts : 1));
+  guint i;
+  need_fp32(t, __func__);
+  if (psize % sizeof(float)) die(__func__, "record size must be a multiple of sizeof(float)");
+  check(__func__, wbfmm_b200_tree_structure_f((int)npts, (const float *)pts,
+                                              (int)(psize / sizeof(float)),
+                                              (const float *)t->x, (float)t->D, 0, ip,
+                                              NULL, NULL));
+  for (i = 0; i < npts; i++)
+    memcpy(tmp + (size_t)i * psize, (char *)pts + (size_t)ip[i] * psize, psize);
+  memcpy(pts, tmp, psize * npts);
+  free(tmp);
+  free(ip);
+  return 0;
+}
+
+/* src/boxes.c:208-277 */
+gint wbfmm_tree_refine_f(wbfmm_tree_t *t) {
+  need_fp32(t, __func__);
+  return wbfmm_tree_refine(t);
+}
+
+gint wbfmm_tree_coefficient_init_f(wbfmm_tree_t *t, guint l, guint nr, guint ns) {
+  need_fp32(t, __func__);
+  return wbfmm_tree_coefficient_init(t, l, nr, ns);
+}
+gint wbfmm_tree_laplace_coefficient_init_f(wbfmm_tree_t *t, guint l, guint nr, guint ns) {
+  need_fp32(t, __func__);
+  return wbfmm_tree_laplace_coefficient_init(t, l, nr, ns);
+}
+gint wbfmm_tree_coefficient_clear_f(wbfmm_tree_t *t, guint l) {
+  return wbfmm_tree_coefficient_clear(t, l);
+}
+
+/* src/boxes.c:585-634 in FP32 arithmetic */
+guint64 wbfmm_point_box_f(wbfmm_tree_t *t, guint level, gfloat *x) {
+  const float *x0 = (const float *)t->x;
+  const float D = (float)t->D, wb = D / (float)(1u << level);
+  if (x[0] < x0[0] || x[0] > x0[0] + D || x[1] < x0[1] || x[1] > x0[1] + D ||
+      x[2] < x0[2] || x[2] > x0[2] + D)
+    die(__func__, "point not in octree");
+  return wbfmm_box_index((guint32)floorf((x[0] - x0[0]) / wb),
+                         (guint32)floorf((x[1] - x0[1]) / wb),
+                         (guint32)floorf((x[2] - x0[2]) / wb));
+}
+
+/* src/boxes.c:324-339 in FP32 arithmetic */
+guint64 wbfmm_point_index_3d_f(gfloat *x, gfloat *c, gfloat D) {
+  return wbfmm_box_index((guint32)((x[0] - c[0]) / D * (float)WBFMM_INDEX_SHIFT),
+                         (guint32)((x[1] - c[1]) / D * (float)WBFMM_INDEX_SHIFT),
+                         (guint32)((x[2] - c[2]) / D * (float)WBFMM_INDEX_SHIFT));
+}
+
+/* src/util.c:290-330 */
+gint wbfmm_box_location_from_index_f(guint64 idx, guint32 level, gfloat *x0,
+                                     gfloat D, gfloat *x, gfloat *wb) {
+  guint32 i, j, k;
+  if (!(idx < ((guint64)1 << (3 * level)))) die(__func__, "box is not at this level");
+  *wb = D / (float)(1u << level);
+  wbfmm_box_location(idx, &i, &j, &k);
+  x[0] = x0[0] + (*wb) * i;
+  x[1] = x0[1] + (*wb) * j;
+  x[2] = x0[2] + (*wb) * k;
+  return 0;
+}
+gint wbfmm_tree_box_centre_f(wbfmm_tree_t *t, guint level, guint64 b, gfloat *xb,
+                             gfloat *wb) {
+  wbfmm_box_location_from_index_f(b, level, (gfloat *)t->x, (gfloat)t->D, xb, wb);
+  xb[0] += 0.5f * (*wb); xb[1] += 0.5f * (*wb); xb[2] += 0.5f * (*wb);
+  return 0;
+}
+
+/* src/util.c:375-405 */
+gint wbfmm_points_origin_width_f(gfloat *x, gint str, gint n, gfloat *xmin,
+                                 gfloat *xmax, gfloat *D, gboolean init_limits) {
+  gint i, a;
+  if (init_limits)
+    for (a = 0; a < 3; a++) { xmin[a] = 3.4028234663852886e38f; xmax[a] = -3.4028234663852886e38f; }
+  for (i = 0; i < n; i++)
+    for (a = 0; a < 3; a++) {
+      if (x[str * i + a] < xmin[a]) xmin[a] = x[str * i + a];
+      if (x[str * i + a] > xmax[a]) xmax[a] = x[str * i + a];
+    }
+  *D = xmax[0] - xmin[0];
+  if (xmax[1] - xmin[1] > *D) *D = xmax[1] - xmin[1];
+  if (xmax[2] - xmin[2] > *D) *D = xmax[2] - xmin[2];
+  return 0;
+}
+
+/* src/util.c:425-450 */
+gint wbfmm_tree_write_sources_f(wbfmm_tree_t *t, gfloat *q, gint stride, FILE *f) {
+  guint i;
+  (void)q; (void)stride;
+  for (i = 0; i < t->npoints; i++) {
+    const guint idx = t->ip[i];
+    const gfloat *x = (const gfloat *)(t->points + (gsize)idx * t->pstr);
+    fprintf(f, "%u %u %g %g %g\n", i, idx, x[0], x[1], x[2]);
+  }
+  return 0;
+}
+
+gint wbfmm_truncation_number_f(wbfmm_tree_t *t, gfloat k, guint level, gfloat tol) {
+  return wbfmm_truncation_number(t, k, level, tol);
+}
+
+/* operators: recorded orders, as the double-precision calls */
+gint wbfmm_shift_angle_table_init_f(void) { return 0; }
+wbfmm_shift_operators_t *wbfmm_shift_operators_new_f(guint L, gboolean bw, gfloat *work) {
+  wbfmm_shift_operators_t *op = wbfmm_shift_operators_new(L, bw, NULL);
+  (void)work;
+  op->size = sizeof(gfloat);
+  return op;
+}
+gint wbfmm_shift_operators_coaxial_SR_init_f(wbfmm_shift_operators_t *w, gfloat D,
+                                             guint level, guint L, gfloat k, gfloat *work) {
+  (void)work;
+  return wbfmm_shift_operators_coaxial_SR_init(w, D, level, L, k, NULL);
+}
+gint wbfmm_shift_operators_coaxial_SS_init_f(wbfmm_shift_operators_t *w, gfloat D,
+                                             guint level, guint L, gfloat k, gfloat *work) {
+  (void)work;
+  return wbfmm_shift_operators_coaxial_SS_init(w, D, level, L, k, NULL);
+}
+gint wbfmm_laplace_coaxial_translate_init_f(gint N) { return wbfmm_laplace_coaxial_translate_init(N); }
+
+/* passes */
+gint wbfmm_tree_leaf_expansions_f(wbfmm_tree_t *t, gfloat k, gfloat *src, gint sstr,
+                                  gfloat *dipoles, gint dstr, gboolean zero_expansions,
+                                  gfloat *work) {
+  (void)work;
+  need_fp32(t, __func__);
+  if (t->problem != WBFMM_PROBLEM_HELMHOLTZ) die(__func__, "tree problem is not Helmholtz");
+  return leaf(t, k, src, sstr, dipoles, dstr, zero_expansions, __func__);
+}
+gint wbfmm_tree_laplace_leaf_expansions_f(wbfmm_tree_t *t, gfloat *src, gint sstr,
+                                          gfloat *dipoles, gint dstr,
+                                          gboolean zero_expansions, gfloat *work) {
+  (void)work;
+  need_fp32(t, __func__);
+  if (t->problem != WBFMM_PROBLEM_LAPLACE) die(__func__, "tree problem is not Laplace");
+  return leaf(t, 0.0, src, sstr, dipoles, dstr, zero_expansions, __func__);
+}
+gint wbfmm_upward_pass_f(wbfmm_tree_t *t, wbfmm_shift_operators_t *op, guint level,
+                         gfloat *work) {
+  (void)op; (void)work;
+  return upward(t, level, __func__);
+}
+gint wbfmm_laplace_upward_pass_f(wbfmm_tree_t *t, wbfmm_shift_operators_t *op,
+                                 guint level, gfloat *work) {
+  (void)op; (void)work;
+  return upward(t, level, __func__);
+}
+gint wbfmm_downward_pass_ref_f(wbfmm_tree_t *t, wbfmm_shift_operators_t *op,
+                               guint level, gfloat *work, gint nthreads) {
+  (void)op; (void)work; (void)nthreads;
+  return downward(t, level, __func__);
+}
+gint wbfmm_laplace_downward_pass_ref_f(wbfmm_tree_t *t, wbfmm_shift_operators_t *op,
+                                       guint level, gfloat *work, gint nthreads) {
+  (void)op; (void)work; (void)nthreads;
+  return downward(t, level, __func__);
+}
+
+/* evaluation (src/local.c:264-310, src/local-laplace.c:1293-1336) */
+gint wbfmm_tree_box_local_field_f(wbfmm_tree_t *t, guint level, guint b, gfloat k,
+                                  gfloat *x, gfloat *f, gint fstr, gfloat *src,
+                                  gint sstr, gfloat *d, gint dstr,
+                                  gboolean eval_neighbours, guint field, gfloat *work) {
+  dtree_t *dt = DT(t);
+  double x64[3] = {x[0], x[1], x[2]};
+  (void)b; (void)work;
+  need_fp32(t, __func__);
+  if (t->problem != WBFMM_PROBLEM_HELMHOLTZ) die(__func__, "tree problem is not Helmholtz");
+  if (level != t->depth) die(__func__, "evaluation is supported at the leaf level");
+  if (field == WBFMM_FIELD_POTENTIAL && fstr < 2) die(__func__, "field stride too small");
+  if (field == WBFMM_FIELD_GRADIENT && fstr < 6) die(__func__, "field stride too small for gradient");
+  if (field != WBFMM_FIELD_POTENTIAL && field != WBFMM_FIELD_GRADIENT)
+    die(__func__, "unrecognized field identifier");
+  solver_for(t, k, __func__);
+  if (eval_neighbours && (src || d)) strengths_for(dt, src, sstr, d, dstr, __func__);
+  evaluate_targets(dt, NULL, 1, x64, 3, field, eval_neighbours && (src || d), f, fstr,
+                   __func__);
+  return 0;
+}
+gint wbfmm_laplace_box_field_f(wbfmm_tree_t *t, guint level, guint b, gfloat *src,
+                               gint sstr, gfloat *d, gint dstr, guint field,
+                               gboolean eval_neighbours, gfloat *x, gfloat *f, gint fstr,
+                               gfloat *work) {
+  dtree_t *dt = DT(t);
+  double x64[3] = {x[0], x[1], x[2]};
+  (void)b; (void)work; (void)fstr;
+  need_fp32(t, __func__);
+  if (t->problem != WBFMM_PROBLEM_LAPLACE) die(__func__, "tree problem is not Laplace");
+  if (level != t->depth) die(__func__, "evaluation is supported at the leaf level");
+  if (field & (WBFMM_FIELD_CURL | WBFMM_FIELD_CURL_GRADIENT))
+    die(__func__, "curl fields are not supported");
+  if (field & WBFMM_FIELD_GRADIENT) field = WBFMM_FIELD_GRADIENT;
+  solver_for(t, 0.0, __func__);
+  if (eval_neighbours && (src || d)) strengths_for(dt, src, sstr, d, dstr, __func__);
+  evaluate_targets(dt, NULL, 1, x64, 3, field, eval_neighbours && (src || d), f, 0,
+                   __func__);
+  return 0;
+}
+
+/* target lists (src/targets.c) */
+wbfmm_target_list_t *wbfmm_target_list_new_f(wbfmm_tree_t *t, guint npts) {
+  wbfmm_target_list_t *l = wbfmm_target_list_new(t, npts);
+  l->size = sizeof(gfloat);
+  return l;
+}
+gint wbfmm_target_list_add_points_f(wbfmm_target_list_t *l, gpointer pts, gsize pstr,
+                                    guint npts) {
+  guint i;
+  if (npts > l->maxpoints) die(__func__, "too many points for target list");
+  if (pstr % sizeof(float)) die(__func__, "point stride must be a multiple of sizeof(float)");
+  l->points = (char *)pts;
+  l->pstr = pstr;
+  l->npoints = npts;
+  for (i = 0; i < npts; i++)
+    l->boxes[i] = (guint32)wbfmm_point_box_f(l->t, l->t->depth,
+                                             (gfloat *)(l->points + (size_t)i * pstr));
+  return 0;
+}
+gint wbfmm_target_list_local_coefficients_f(wbfmm_target_list_t *l, gfloat k, gfloat *work) {
+  (void)work;
+  return list_prepare(l, k, __func__);
+}
+gint wbfmm_laplace_target_list_local_coefficients_f(wbfmm_target_list_t *l, guint source,
+                                                    gfloat *work) {
+  (void)work;
+  l->source = source;
+  return list_prepare(l, 0.0, __func__);
+}
+gint wbfmm_target_list_local_field_f(wbfmm_target_list_t *l, gfloat *src, gint sstr,
+                                     gfloat *nsrc, gint nstr, gfloat *f, gint fstr) {
+  return list_field(l, src, sstr, nsrc, nstr, f, fstr, __func__);
 }
 
 /* ---------------------------------------------------- direct sums */
@@ -843,6 +1219,71 @@ gint wbfmm_laplace_field_grad(gdouble *xs, gint xstride, gdouble *src,
                               gint fstr) {
   return direct(WBFMM_B200_LAPLACE, 0.0, xs, xstride, src, sstride, normals,
                 nstr, dipoles, dstr, nq, nsrc, xf, field, fstr, 1, __func__);
+}
+
+/* The single-precision direct sums: the same semantics on FP32 arrays
+   (widened exactly, summed on the GPU in FP64, rounded once into the
+   caller's FP32 field). */
+static double *widen_n(const float *a, size_t n) {
+  double *o;
+  size_t i;
+  if (!a) return NULL;
+  o = malloc(sizeof(double) * (n ? n : 1));
+  if (!o) die("wbfmm", "out of memory");
+  for (i = 0; i < n; i++) o[i] = a[i];
+  return o;
+}
+
+static gint direct_f(int problem, float k, gfloat *xs, gint xstride, gfloat *src,
+                     gint sstride, gfloat *normals, gint nstr, gfloat *dipoles,
+                     gint dstr, gint nq, gint nsrc, gfloat *xf, gfloat *field,
+                     gint fstr, int grad, const char *fn) {
+  const int w = problem == WBFMM_B200_HELMHOLTZ ? 2 : 1;
+  const size_t n = (size_t)(nsrc > 0 ? nsrc : 0);
+  size_t nf = (size_t)(nq > 0 ? nq - 1 : 0) * (size_t)(fstr > 0 ? fstr : 0) + (grad ? 3 * w : w), i;
+  /* the records' extent: (n - 1) strides plus the values of the last one */
+#define WBFMM_EXTENT(_str, _cnt) (n ? (n - 1) * (size_t)(_str) + (size_t)(_cnt) : 0)
+  double *x64 = widen_n(xs, WBFMM_EXTENT(xstride, 3));
+  double *q64 = widen_n(src, WBFMM_EXTENT(sstride, w * nq));
+  double *n64 = widen_n(normals, WBFMM_EXTENT(nstr, 3));
+  double *d64 = widen_n(dipoles, WBFMM_EXTENT(dstr, w * nq));
+#undef WBFMM_EXTENT
+  double xf64[3] = {xf[0], xf[1], xf[2]};
+  double *f64;
+  if (nf < (size_t)(2 * nq)) nf = (size_t)(2 * nq);
+  f64 = widen_n(field, nf);
+  direct(problem, k, x64, xstride, q64, sstride, n64, nstr, d64, dstr, nq, nsrc, xf64,
+         f64, fstr, grad, fn);
+  for (i = 0; i < nf; i++) field[i] = (float)f64[i];
+  free(x64); free(q64); free(n64); free(d64); free(f64);
+  return 0;
+}
+
+gint wbfmm_total_field_f(gfloat k, gfloat *xs, gint xstride, gfloat *src, gint sstride,
+                         gfloat *normals, gint nstr, gfloat *dipoles, gint dstr, gint nq,
+                         gint nsrc, gfloat *xf, gfloat *field, gint fstr) {
+  return direct_f(WBFMM_B200_HELMHOLTZ, k, xs, xstride, src, sstride, normals, nstr,
+                  dipoles, dstr, nq, nsrc, xf, field, fstr, 0, __func__);
+}
+gint wbfmm_total_field_grad_f(gfloat k, gfloat *xs, gint xstride, gfloat *src,
+                              gint sstride, gfloat *normals, gint nstr, gfloat *dipoles,
+                              gint dstr, gint nq, gint nsrc, gfloat *xf, gfloat *field,
+                              gint fstr) {
+  return direct_f(WBFMM_B200_HELMHOLTZ, k, xs, xstride, src, sstride, normals, nstr,
+                  dipoles, dstr, nq, nsrc, xf, field, fstr, 1, __func__);
+}
+gint wbfmm_laplace_field_f(gfloat *xs, gint xstride, gfloat *src, gint sstride, gint nq,
+                           gfloat *normals, gint nstr, gfloat *dipoles, gint dstr,
+                           gint nsrc, gfloat *xf, gfloat *field, gint fstr) {
+  return direct_f(WBFMM_B200_LAPLACE, 0.0f, xs, xstride, src, sstride, normals, nstr,
+                  dipoles, dstr, nq, nsrc, xf, field, fstr, 0, __func__);
+}
+gint wbfmm_laplace_field_grad_f(gfloat *xs, gint xstride, gfloat *src, gint sstride,
+                                gint nq, gfloat *normals, gint nstr, gfloat *dipoles,
+                                gint dstr, gint nsrc, gfloat *xf, gfloat *field,
+                                gint fstr) {
+  return direct_f(WBFMM_B200_LAPLACE, 0.0f, xs, xstride, src, sstride, normals, nstr,
+                  dipoles, dstr, nq, nsrc, xf, field, fstr, 1, __func__);
 }
 
 /* ---------------------------------------------------------- config */

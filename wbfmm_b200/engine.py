@@ -45,7 +45,7 @@ class Config(C.Structure):
         ("order_r", C.c_int * (MAX_DEPTH + 1)),
         ("k", C.c_double), ("x0", C.c_double * 3), ("D", C.c_double),
         ("precision", C.c_int), ("field", C.c_int), ("skip_empty", C.c_int),
-        ("managed", C.c_int), ("leaf_order", C.c_int),
+        ("managed", C.c_int), ("leaf_order", C.c_int), ("keys_fp32", C.c_int),
     ]
 
 
