@@ -231,7 +231,10 @@ int wbfmm_b200_tree_structure_f(int n, const float *pts, int pstr,
    target tiles above, while their shared memory suffices;
    2 = lane-per-pair wherever instantiated
    (Helmholtz <= 8, Laplace <= 16); 3 = target tiles wherever they fit;
-   0 = always the warp-per-target kernel. */
+   0 = always the warp-per-target kernel; 4 = Laplace FP32 on the tensor
+   cores (dense per-shift operators, tcgen05 kind::tf32 with 3xTF32
+   splitting, FP32 accumulation in tensor memory) for equal orders with
+   (p+1)^2 <= 256, the automatic choice elsewhere. */
 int wbfmm_b200_set_m2l_kernel(wbfmm_b200_solver_t *s, int mode);
 
 /* FP64 direct sum with self-exclusion (r <= 1e-6) and compensated

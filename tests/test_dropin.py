@@ -318,8 +318,15 @@ def test_reference_float_driver_on_dropin(gpu_lib, tmp_path, tool, args):
         assert out[k].shape == out["b200"].shape and out["b200"].shape[0] == nf
     f = {k: v[:, 3:] for k, v in out.items()}
     tol = 2e-6
+    assert np.all(np.isfinite(f["b200"]))
     assert np.linalg.norm(f["b200"] - f["ref64"]) <= tol * np.linalg.norm(f["ref64"])
-    assert np.linalg.norm(f["b200"] - f["ref"]) <= tol * np.linalg.norm(f["ref"])
+    # the reference's own FP32 build overflows at the high coarse-level
+    # orders of the truncation rule (-t): NaN fields, which the drop-in's
+    # FP32 form (tables generated in FP64) does not share
+    if np.all(np.isfinite(f["ref"])):
+        assert np.linalg.norm(f["b200"] - f["ref"]) <= tol * np.linalg.norm(f["ref"])
+    else:
+        assert "-t" in args
     if helm and "-t" not in args:
         order = [[line.split()[1] for line in run(bins[k], ["-w"]).stderr.splitlines()
                   if len(line.split()) == 5 and line.split()[0].isdigit()]

@@ -250,6 +250,45 @@ def test_m2l_kernels_agree_at_high_order(gpu_lib, case, precision):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("order", [8, 10, 12, 14, 15])
+def test_laplace_m2l_tensor_cores(gpu_lib, order):
+    """The Laplace FP32 M2L on the tensor cores (mode 4: dense shift
+    operators, tcgen05 3xTF32 products accumulated in FP32) against the
+    offset-major tile kernel (mode 3) and the FP64 form: every level of a
+    depth-4 tree (split sums on the small levels, one pass on level 4)."""
+    p = W.laplace_cube(30000, 3000, depth=4, order=order, seed=47)
+    outs = {}
+    for prec, mode in ((engine.FP64, 1), (engine.FP32, 3), (engine.FP32, 4)):
+        cfg = engine.SolverConfig.from_problem(p, prec)
+        with engine.Solver(cfg) as s:
+            s.set_m2l_kernel(mode)
+            s.set_sources(p.xs).set_strengths(p.q).set_targets(p.xt).run()
+            outs[(prec, mode)] = s.field()
+    tc, tiles, f64 = outs[(engine.FP32, 4)], outs[(engine.FP32, 3)], outs[(engine.FP64, 1)]
+    for a, b, c in zip(tc, tiles, f64):
+        assert np.all(np.isfinite(a))
+        assert rel_l2(a, c) < 2e-6, rel_l2(a, c)
+        assert rel_l2(a, b) < 2e-6, rel_l2(a, b)
+
+
+@pytest.mark.gpu
+def test_laplace_m2l_tensor_cores_target_lists(gpu_lib):
+    """The tensor-core M2L on the per-child-type target lists and source
+    masks of skip_empty (clustered points, order 10, depth 6)."""
+    p = W.laplace_clusters(60_000, depth=6, order=10, seed=48)
+    outs = {}
+    for skip, mode in ((False, 3), (True, 4)):
+        cfg = engine.SolverConfig.from_problem(p, engine.FP32, skip_empty=skip)
+        with engine.Solver(cfg) as s:
+            s.set_m2l_kernel(mode)
+            s.set_sources(p.xs).set_strengths(p.q).set_targets(p.xt).run()
+            outs[mode] = s.field()
+    for a, b in zip(outs[4], outs[3]):
+        assert np.all(np.isfinite(a))
+        assert rel_l2(a, b) < 2e-6, rel_l2(a, b)
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("mode", [0, 2, 3])
 def test_laplace_fp32_deep_levels(gpu_lib, mode):
     """Laplace FP32 at depth 7, order 10, on clustered points: S|R / t^(n+l+1)

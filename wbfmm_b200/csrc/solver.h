@@ -21,6 +21,7 @@
 #include "engine.h"
 #include "kernels.h"
 #include "m2l_lanes.h"
+#include "m2l_tc.h"
 #include "table_cache.h"
 #include "tables.h"
 
@@ -236,6 +237,8 @@ struct Solver : public wbfmm_b200_solver {
   const T* sr_ptr[kMaxDepth + 1] = {nullptr};   // (S|R) table per level
   const T* ss_ptr[kMaxDepth + 1] = {nullptr};   // (R|R) table per level
   int helm_e[kMaxDepth + 1] = {0};   // FP32 Helmholtz M2L scale exponents (helm_m2l_exp)
+  bool tc_used = false;             // the tensor-core M2L ran since the sources were set
+  DBuf<float> tc_part;              // its split partial sums
   DBuf<double> lap64[3];
   DBuf<T> lap[3];
   int lt = 0;
@@ -254,7 +257,7 @@ struct Solver : public wbfmm_b200_solver {
   // served form: shared tables, no host waits inside a solve
   TableCache* cache = nullptr;
   bool async_checks = false;   // domain checks read back after the solve
-  int* hflag = nullptr;        // pinned copy of flag[0..1]
+  int* hflag = nullptr;        // pinned copy of flag[0..2]
   cudaMemPool_t lib_pool = nullptr;
   // graph replay of the passes (run_graph): valid while nothing they depend
   // on has changed since the capture
@@ -282,7 +285,7 @@ struct Solver : public wbfmm_b200_solver {
     f(tstart); f(tcount); f(flag); f(pot); f(grad); f(out64);
     f(H64); f(H); f(op_ith); f(op_dist); f(op_r); f(op_ph); f(op_ch);
     for (int i = 0; i < 3; i++) { f(lap64[i]); f(lap[i]); }
-    f(partial); f(lin); f(lanes_part); f(act_scr); f(lapsr); f(hcx); f(smask);
+    f(partial); f(lin); f(lanes_part); f(act_scr); f(lapsr); f(hcx); f(smask); f(tc_part);
   }
 
   ~Solver() override {
@@ -341,7 +344,7 @@ struct Solver : public wbfmm_b200_solver {
     // keeps freed memory (repeated solves reallocate without mapping)
     lib_pool = library_pool();
     each_buf([&](auto& b) { b.so = stream; b.pool = lib_pool; });
-    WBFMM_TRY(flag.alloc(2));
+    WBFMM_TRY(flag.alloc(3));
     return 0;
   }
 
@@ -351,7 +354,7 @@ struct Solver : public wbfmm_b200_solver {
     ops_ready = false;
     nsrc = ntgt = 0;
     have_q = have_dip = have_normals = false;
-    if (!hflag) WBFMM_CUDA(cudaMallocHost(&hflag, 2 * sizeof(int)));
+    if (!hflag) WBFMM_CUDA(cudaMallocHost(&hflag, 3 * sizeof(int)));
     return 0;
   }
 
@@ -365,11 +368,12 @@ struct Solver : public wbfmm_b200_solver {
   // Served form: every work buffer back to the stream-ordered pool.
   void release_buffers() {
     each_buf([](auto& b) { if (b.owned) b.release(); });
-    WBFMM_TRY_VOID(flag.alloc(2));
+    WBFMM_TRY_VOID(flag.alloc(3));
   }
 
   // flag[0]: first source outside the cube (0x7fffffff: none);
-  // flag[1]: nonzero when a target lies outside the cube
+  // flag[1]: nonzero when a target lies outside the cube;
+  // flag[2]: nonzero when a bounded wait of the tensor-core M2L ran out
   static int domain_error(int bad_source, int bad_target) {
     if (bad_source != 0x7fffffff) {
       char msg[160];
@@ -399,7 +403,7 @@ struct Solver : public wbfmm_b200_solver {
       dpts = pts_in.p;
     }
     // strict-interior domain check (src/boxes.c:148-153)
-    launch_set_words((uint32_t*)flag.p, 0x7fffffffu, nullptr, 0, stream);
+    launch_set_words((uint32_t*)flag.p, 0x7fffffffu, (uint32_t*)flag.p + 2, 0, stream);
     launch_domain_check(dpts, xs_str, n, cfg.x0, cfg.D, flag.p, stream, cfg.keys_fp32 != 0);
     if (!async_checks) {
       int bad = 0;
@@ -764,6 +768,9 @@ struct Solver : public wbfmm_b200_solver {
     const int lanes_max = helm ? 7 : sizeof(T) == 8 ? 9 : 10;
     bool use_tiles = false, use_lanes = false;
     const int he = helm ? helm_e[level] : 0;
+    // tensor cores: Laplace, FP32, equal orders up to (p+1)^2 = 256, mode 4
+    if (!helm && sizeof(T) == 4 && m2l_mode == 4 && tc_lap_supported(x.Nin, x.Nout))
+      return m2l_tc(level, x);
     if (he) {
       // the scaled Helmholtz M2L (FP32 tables out of range unscaled) runs
       // in the tile kernel only
@@ -884,6 +891,46 @@ struct Solver : public wbfmm_b200_solver {
                 : launch_m2l<T, false>(x, tables, stream);
   }
 
+  // The Laplace M2L of a level on the tensor cores (m2l_tc.cu).
+  int m2l_tc(int level, const XlateParams<T>& x) {
+    LapTcParams lp;
+    memset(&lp, 0, sizeof(lp));
+    lp.level = level;
+    lp.P = x.Nin;
+    WBFMM_TRY(tc_lap_ops(lp.P, stream, &lp));
+    // w^-n in, w^-(n+1) out, per degree (finite in FP32 within the range rule)
+    const double w = width(level);
+    for (int n = 0; n <= lp.P; n++) {
+      lp.sc.in[n] = (float)pow(w, -(double)n);
+      lp.sc.out[n] = (float)pow(w, -(double)(n + 1));
+      if (!std::isfinite(lp.sc.out[n]) || !std::isfinite(lp.sc.in[n]))
+        return set_error(WBFMM_B200_E_ORDER, "tensor-core M2L: level scaling out of the FP32 range");
+    }
+    lp.cout = (float*)x.cout;
+    lp.tmask = x.tmask;
+    if (x.tmask && act[level].p) { lp.act = act[level].p; lp.act_n = act_n[level].p; }
+    if (x.tmask) {
+      WBFMM_TRY(smask.alloc(source_mask_bytes(level)));
+      WBFMM_TRY(build_source_mask(x.src_n, level, smask.p, stream));
+      lp.smask = smask.p;
+      launches++;
+    }
+    lp.err = flag.p + 2;
+    const int64_t np = (int64_t)1 << (3 * (level - 1));
+    const int64_t ctas = ((np + 127) / 128) * 8;
+    int ns = 1;
+    while (ctas * ns < 148 && ns < 16) ns *= 2;
+    lp.nsplit = ns;
+    if (ns > 1) {
+      WBFMM_TRY(tc_part.alloc((size_t)ns * 8 * (lp.P + 1) * (lp.P + 1) * np));
+      lp.partial = tc_part.p;
+    }
+    WBFMM_TRY(lin.alloc(tc_lin_bytes(level, lp.P)));
+    tc_used = true;
+    launches += ns > 1 ? 3 : 2;
+    return launch_m2l_tc(lp, (const float*)x.cin, lin.p, stream);
+  }
+
   int l2l(int level) override {
     if (level < 2 || level >= depth) return set_error(WBFMM_B200_E_ARG, "L2L level must be in [2, depth-1]");
     WBFMM_TRY(build_operators());
@@ -957,7 +1004,7 @@ struct Solver : public wbfmm_b200_solver {
     WBFMM_TRY(evaluate());
     mark(2);
     if (async_checks && hflag)
-      WBFMM_CUDA(cudaMemcpyAsync(hflag, flag.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, stream));
+      WBFMM_CUDA(cudaMemcpyAsync(hflag, flag.p, 3 * sizeof(int), cudaMemcpyDeviceToHost, stream));
     return 0;
   }
 
@@ -1012,14 +1059,19 @@ struct Solver : public wbfmm_b200_solver {
     if (cudaEventElapsedTime(&t, ev[6], ev[7]) == cudaSuccess) stage_ms[4] = t;
     if (cudaEventElapsedTime(&t, ev[7], ev[2]) == cudaSuccess) stage_ms[5] = t;
     cudaGetLastError();
+    if (tc_used && !async_checks) {
+      int err = 0;
+      WBFMM_CUDA(cudaMemcpy(&err, flag.p + 2, sizeof(int), cudaMemcpyDeviceToHost));
+      if (err) return set_error(WBFMM_B200_E_STATE, "tensor-core M2L: a wait ran out");
+    }
     return check_flags();
   }
 
   // set_sources / set_targets queue their domain checks; run / wait report
   int set_deferred_checks(int on) override {
     if (on && !hflag) {
-      WBFMM_CUDA(cudaMallocHost(&hflag, 2 * sizeof(int)));
-      hflag[0] = 0x7fffffff; hflag[1] = 0;
+      WBFMM_CUDA(cudaMallocHost(&hflag, 3 * sizeof(int)));
+      hflag[0] = 0x7fffffff; hflag[1] = 0; hflag[2] = 0;
     }
     async_checks = on != 0;
     return 0;
@@ -1057,13 +1109,16 @@ struct Solver : public wbfmm_b200_solver {
     if (np) WBFMM_CUDA(cudaMemcpyAsync(hpot, fp, sizeof(double) * np, kind, stream));
     if (ng) WBFMM_CUDA(cudaMemcpyAsync(hgrad, fg, sizeof(double) * ng, kind, stream));
     if (async_checks && hflag)
-      WBFMM_CUDA(cudaMemcpyAsync(hflag, flag.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, stream));
+      WBFMM_CUDA(cudaMemcpyAsync(hflag, flag.p, 3 * sizeof(int), cudaMemcpyDeviceToHost, stream));
     return 0;
   }
 
-  // Served form, after the stream has drained: the deferred domain checks.
+  // Served form, after the stream has drained: the deferred domain checks
+  // and the tensor-core M2L's bounded waits.
   int check_flags() const {
-    return async_checks && hflag ? domain_error(hflag[0], hflag[1]) : 0;
+    if (!(async_checks && hflag)) return 0;
+    if (hflag[2]) return set_error(WBFMM_B200_E_STATE, "tensor-core M2L: a wait ran out");
+    return domain_error(hflag[0], hflag[1]);
   }
 
   // ------------------------------------------------------------ outputs
