@@ -18,7 +18,8 @@
 // warp-cooperative shift applied to unit vectors), split into TF32 hi + lo
 // parts and stored in the tensor core's shared-memory layout.  The product
 // runs as tcgen05.mma kind::tf32 with the FP32 accumulator in tensor memory:
-// 3xTF32 (A_hi B_hi + A_hi B_lo + A_lo B_hi) keeps FP32 accuracy.  One CTA
+// 3xTF32 (A_hi B_hi + A_hi B_lo + A_lo B_hi, both parts rounded to TF32)
+// keeps FP32 accuracy.  One CTA
 // takes up to 128 target boxes of one child type; its 128 threads stage the
 // shifted source vectors (split into hi / lo) while the tensor core works
 // on the previous stage, the operator tiles arrive by bulk copy, and one
@@ -180,8 +181,10 @@ __global__ void k_lap_tc_ops(OpTables<double> t, int P, int KS, int MT, float* _
   for (int row = lane; row < C; row += 32) {
     const int n = (int)sqrt((double)row + 0.5), q = row - n * n, m = (q + 1) / 2;
     const double v = O[2 * hidx(n, m) + ((q > 0 && (q & 1) == 0) ? 1 : 0)];
+    // both parts rounded to TF32 (the tensor core would truncate the low
+    // bits of an FP32 operand, a bias of up to 2^-21 relative)
     const float hi = __uint_as_float(to_tf32((float)v));
-    const float lo = (float)(v - (double)hi);
+    const float lo = __uint_as_float(to_tf32((float)(v - (double)hi)));
     const int s = j >> 3, kk = j & 7, mt = row / kTcRows, rr = row % kTcRows;
     float* tile = base + ((int64_t)s * MT + mt) * 2 * (kTileBytes / 4);
     tile[tile_off(rr, kk) / 4] = hi;
@@ -327,7 +330,7 @@ k_m2l_tc(LapTcParams p) {
         float hi[8], lo[8];
         for (int c = 0; c < 8; c++) {
           hi[c] = __uint_as_float(to_tf32(v[c]));
-          lo[c] = v[c] - hi[c];
+          lo[c] = __uint_as_float(to_tf32(v[c] - hi[c]));
         }
         unsigned char* bt = sm.b[buf] + s * 2 * kTileBytes;
         *(float4*)(bt + tile_off(tid, 0)) = make_float4(hi[0], hi[1], hi[2], hi[3]);
