@@ -49,8 +49,8 @@ namespace {
 constexpr int kTcRows = 128;                 // MMA M (rows of one tile)
 constexpr int kTcN = 128;                    // MMA N (target boxes per CTA)
 constexpr int kTcThreads = 128;
-constexpr int kTcStageK = 4;                 // k-steps (8 K each) per stage
-constexpr int kTcStages = 2;
+constexpr int kTcStageK = 2;                 // k-steps (8 K each) per stage
+constexpr int kTcStages = 4;
 constexpr int kTileBytes = kTcRows * 8 * 4;  // one 128 x 8 TF32 tile: 4 KB
 
 // byte offset of element (row r, k) in a 128 x 8 K-major tile without
@@ -193,9 +193,10 @@ __global__ void k_lap_tc_ops(OpTables<double> t, int P, int KS, int MT, float* _
 }
 
 // ------------------------------------------------------ source vectors
-// lin[sg][pp][k] = w^-n M_k of the level's box of child type sg under padded
-// parent pp (k real-packed, degree n), zero for k >= C and on the halo
-__global__ void k_to_lin_tc(const float* __restrict__ mps, int level, int P, int KP,
+// lin[sg][pp][s][16]: for each 8-K chunk s of the box's scaled vector
+// (w^-n M_k, k real-packed of degree n, zero for k >= C) its TF32 hi parts
+// (8) then lo parts (8); zero on the halo
+__global__ void k_to_lin_tc(const float* __restrict__ mps, int level, int P, int KS,
                             const LapTcScales sc, float* __restrict__ lin) {
   const int C = (P + 1) * (P + 1);
   const int nx = 1 << (level - 1), npx = nx + 2;
@@ -210,26 +211,41 @@ __global__ void k_to_lin_tc(const float* __restrict__ mps, int level, int P, int
   const int64_t pp = (px + 1) + npx * ((int64_t)(py + 1) + npx * (int64_t)(pz + 1));
   const int64_t b = (Pm << 3) | tau;
   const int n = (int)sqrtf((float)k + 0.5f);
-  lin[((int64_t)tau * (npx * (int64_t)npx * npx) + pp) * KP + k] =
-      mps[layout_off(b, k, C)] * sc.in[n];
+  const float v = mps[layout_off(b, k, C)] * sc.in[n];
+  const float hi = __uint_as_float(to_tf32(v));
+  const float lo = __uint_as_float(to_tf32(v - hi));
+  float* row = lin + ((int64_t)tau * (npx * (int64_t)npx * npx) + pp) * KS * 16 + (k >> 3) * 16;
+  row[k & 7] = hi;
+  row[8 + (k & 7)] = lo;
 }
 
 // ----------------------------------------------------------- the GEMM
 struct TcSmem {
   // per stage: operator tiles (kTcStageK x MT x {hi, lo} x 4 KB) and the
-  // shifted sources (kTcStageK x {hi, lo} x 4 KB); fixed at MT = 2
+  // shifted sources (kTcStageK x {hi, lo} x 4 KB); sized for MT = 2
   unsigned char a[kTcStages][kTcStageK * 2 * 2 * kTileBytes];
   unsigned char b[kTcStages][kTcStageK * 2 * kTileBytes];
   uint64_t full[kTcStages];     // operator bulk copies landed
   uint64_t mma[kTcStages];      // the MMAs reading the stage finished
+  int ns[kTcStages];            // k-steps in the stage
   uint32_t tmem;
   int pp[kTcN];                 // padded parent index of each target (or -1)
   int plin[kTcN];               // parent linear index of each target
-  int any;
 };
 
 constexpr int kWaitLimit = 1 << 22;
 
+__device__ __forceinline__ void cp16(void* dst, const void* src, bool valid) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src),
+               "r"(valid ? 16 : 0)
+               : "memory");
+}
+
+// Accumulators in tensor memory (512 columns): per M tile, the hi*hi
+// products (columns mt*128) and, apart, the hi*lo + lo*hi corrections
+// (columns 256 + mt*128): the tensor core adds into its FP32 accumulator
+// without rounding to nearest, and the corrections (2^-11 of the main
+// terms) lose fewer bits summed on their own.  The epilogue adds the two.
 __global__ void __launch_bounds__(kTcThreads, 1)
 k_m2l_tc(LapTcParams p) {
   extern __shared__ __align__(16) unsigned char tc_smem[];
@@ -267,7 +283,7 @@ k_m2l_tc(LapTcParams p) {
     asm volatile("fence.mbarrier_init.release.cluster;");
   }
   if (tid < 32) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 256;"
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;"
                  ::"r"(smem_u32(&sm.tmem)));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
@@ -277,11 +293,40 @@ k_m2l_tc(LapTcParams p) {
   const uint32_t tmem = sm.tmem;
   const uint32_t idesc = tf32_idesc(kTcRows, kTcN);
   const int64_t op_floats = (int64_t)KS * MT * 2 * (kTileBytes / 4);
+  const int64_t row_floats = (int64_t)KS * 16;
   int ok = 1;                  // all waits completed
-  int g = 0;                   // stages issued by this CTA
-  bool started = false;        // the accumulators hold a product
-  int copy_pending = 0;        // thread 0: the last operator copy is unwaited
-  int mma_pending = 0;         // thread 0: the last commit is unwaited
+  int gl = 0, gm = 0;          // stages loaded / stages whose MMAs were issued
+  bool started = false;        // thread 0: the accumulators hold a product
+  int copy_pending = 0, mma_pending = 0;   // thread 0: unwaited operator copy / commit
+
+  // thread 0: the MMAs of stage gm (its operator tiles and sources landed)
+  auto issue = [&]() {
+    const int buf = gm % kTcStages;
+    const uint32_t use = (uint32_t)(gm / kTcStages);
+    if (tid == 0 && ok) {
+      if (!mbar_wait(&sm.full[buf], use & 1, kWaitLimit)) {
+        ok = 0;
+      } else {
+        copy_pending = 0;
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        for (int s = 0; s < sm.ns[buf]; s++) {
+          const uint32_t bb = smem_u32(sm.b[buf] + s * 2 * kTileBytes);
+          for (int mt = 0; mt < MT; mt++) {
+            const uint32_t aa = smem_u32(sm.a[buf] + (s * MT + mt) * 2 * kTileBytes);
+            const uint32_t dm = tmem + (uint32_t)(mt * kTcN);
+            const uint32_t dc = tmem + (uint32_t)(2 * kTcN + mt * kTcN);
+            mma_tf32(dm, mat_desc(aa), mat_desc(bb), idesc, started ? 1u : 0u);
+            mma_tf32(dc, mat_desc(aa), mat_desc(bb + kTileBytes), idesc, started ? 1u : 0u);
+            mma_tf32(dc, mat_desc(aa + kTileBytes), mat_desc(bb), idesc, 1u);
+          }
+          started = true;
+        }
+        mma_commit(&sm.mma[buf]);
+        mma_pending = 1;
+      }
+    }
+    gm++;
+  };
 
   for (int j = split; j < 189 && ok; j += p.nsplit) {
     const int code = p.offsets[tau * 189 + j];
@@ -298,90 +343,70 @@ k_m2l_tc(LapTcParams p) {
                 sz = (int)(pp / ((int64_t)npx * npx)) + ddz;
       bool in = sx >= 1 && sx <= nx && sy >= 1 && sy <= nx && sz >= 1 && sz <= nx;
       if (in && p.smask) in = p.smask[(int64_t)sg * npp + pp + doff] != 0;
-      if (in) src = ((int64_t)sg * npp + pp + doff) * p.KP;
+      if (in) src = ((int64_t)sg * npp + pp + doff) * row_floats;
     }
     if (!__syncthreads_or(src >= 0)) continue;
     const float* A = p.ops + (int64_t)p.slot[op] * op_floats;
     for (int s0 = 0; s0 < KS && ok; s0 += kTcStageK) {
       const int ns = KS - s0 < kTcStageK ? KS - s0 : kTcStageK;
-      const int buf = g % kTcStages;
-      const uint32_t use = (uint32_t)(g / kTcStages);
+      const int buf = gl % kTcStages;
+      const uint32_t use = (uint32_t)(gl / kTcStages);
       // the buffer's previous MMAs must be done before it is overwritten
-      if (g >= kTcStages && !mbar_wait(&sm.mma[buf], (use - 1) & 1, kWaitLimit)) ok = 0;
+      if (gl >= kTcStages && !mbar_wait(&sm.mma[buf], (use - 1) & 1, kWaitLimit)) ok = 0;
       ok = __syncthreads_and(ok);
       if (!ok) break;
-      const uint32_t abytes = (uint32_t)(ns * MT * 2 * kTileBytes);
       if (tid == 0) {
+        const uint32_t abytes = (uint32_t)(ns * MT * 2 * kTileBytes);
+        sm.ns[buf] = ns;
         mbar_expect_tx(&sm.full[buf], abytes);
         bulk_g2s(sm.a[buf], A + (int64_t)s0 * MT * 2 * (kTileBytes / 4), abytes, &sm.full[buf]);
         copy_pending = 1;
       }
-      // this target's source vector, k = 8 s0 .. 8 (s0 + ns), split hi / lo
+      // this target's source chunks, hi and lo, straight into the tiles
+      const float* q = p.lin + (src >= 0 ? src : 0) + (int64_t)s0 * 16;
       for (int s = 0; s < ns; s++) {
-        float v[8];
-        if (src >= 0) {
-          const float4* q = (const float4*)(p.lin + src + 8 * (s0 + s));
-          const float4 x0 = q[0], x1 = q[1];
-          v[0] = x0.x; v[1] = x0.y; v[2] = x0.z; v[3] = x0.w;
-          v[4] = x1.x; v[5] = x1.y; v[6] = x1.z; v[7] = x1.w;
-        } else {
-          for (int c = 0; c < 8; c++) v[c] = 0.f;
-        }
-        float hi[8], lo[8];
-        for (int c = 0; c < 8; c++) {
-          hi[c] = __uint_as_float(to_tf32(v[c]));
-          lo[c] = __uint_as_float(to_tf32(v[c] - hi[c]));
-        }
         unsigned char* bt = sm.b[buf] + s * 2 * kTileBytes;
-        *(float4*)(bt + tile_off(tid, 0)) = make_float4(hi[0], hi[1], hi[2], hi[3]);
-        *(float4*)(bt + tile_off(tid, 4)) = make_float4(hi[4], hi[5], hi[6], hi[7]);
-        *(float4*)(bt + kTileBytes + tile_off(tid, 0)) = make_float4(lo[0], lo[1], lo[2], lo[3]);
-        *(float4*)(bt + kTileBytes + tile_off(tid, 4)) = make_float4(lo[4], lo[5], lo[6], lo[7]);
+        cp16(bt + tile_off(tid, 0), q + s * 16, src >= 0);
+        cp16(bt + tile_off(tid, 4), q + s * 16 + 4, src >= 0);
+        cp16(bt + kTileBytes + tile_off(tid, 0), q + s * 16 + 8, src >= 0);
+        cp16(bt + kTileBytes + tile_off(tid, 4), q + s * 16 + 12, src >= 0);
       }
-      asm volatile("fence.proxy.async.shared::cta;");
-      __syncthreads();
-      if (tid == 0) {
-        if (!mbar_wait(&sm.full[buf], use & 1, kWaitLimit)) {
-          ok = 0;
-        } else {
-          copy_pending = 0;
-          asm volatile("tcgen05.fence::after_thread_sync;");
-          for (int s = 0; s < ns; s++) {
-            const uint32_t bb = smem_u32(sm.b[buf] + s * 2 * kTileBytes);
-            for (int mt = 0; mt < MT; mt++) {
-              const uint32_t aa = smem_u32(sm.a[buf] + (s * MT + mt) * 2 * kTileBytes);
-              const uint32_t d = tmem + (uint32_t)(mt * kTcN);
-              // 3xTF32: hi*hi + hi*lo + lo*hi
-              mma_tf32(d, mat_desc(aa), mat_desc(bb), idesc, started ? 1u : 0u);
-              mma_tf32(d, mat_desc(aa), mat_desc(bb + kTileBytes), idesc, 1u);
-              mma_tf32(d, mat_desc(aa + kTileBytes), mat_desc(bb), idesc, 1u);
-            }
-            started = true;
-          }
-          mma_commit(&sm.mma[buf]);
-          mma_pending = 1;
-        }
+      asm volatile("cp.async.commit_group;");
+      gl++;
+      if (gl - gm == kTcStages) {
+        // the ring is full: the oldest stage's copies are done once at most
+        // kTcStages - 1 groups are pending
+        asm volatile("cp.async.wait_group %0;" ::"n"(kTcStages - 1));
+        asm volatile("fence.proxy.async.shared::cta;");
+        __syncthreads();
+        issue();
+        ok = __syncthreads_and(ok);
       }
-      ok = __syncthreads_and(ok);
-      g++;
     }
   }
-  // the last stage's MMAs (every earlier one was waited for before its
-  // buffer was reused, and MMAs complete in order)
-  if (ok && g > 0) {
-    const int last = (g - 1) % kTcStages;
-    if (!mbar_wait(&sm.mma[last], ((g - 1) / kTcStages) & 1, kWaitLimit)) ok = 0;
+  // the stages still in the ring
+  asm volatile("cp.async.wait_all;");
+  asm volatile("fence.proxy.async.shared::cta;");
+  __syncthreads();
+  while (gm < gl && ok) {
+    issue();
+    ok = __syncthreads_and(ok);
+  }
+  // the last stage's MMAs (MMAs complete in order)
+  if (ok && gl > 0) {
+    const int last = (gl - 1) % kTcStages;
+    if (!mbar_wait(&sm.mma[last], ((gl - 1) / kTcStages) & 1, kWaitLimit)) ok = 0;
   }
   ok = __syncthreads_and(ok);
   asm volatile("tcgen05.fence::after_thread_sync;");
-  bool started_all = __syncthreads_or(started ? 1 : 0);
+  const bool started_all = __syncthreads_or(started ? 1 : 0);
   if (!ok) {
     if (tid == 0) {
       atomicExch(p.err, 1);
       // let what this CTA started finish (bounded) before its memory goes
-      if (g > 0) {
-        const int last = (g - 1) % kTcStages;
-        const uint32_t u = (uint32_t)((g - 1) / kTcStages) & 1;
+      if (gl > 0) {
+        const int last = (gl - 1) % kTcStages;
+        const uint32_t u = (uint32_t)((gl - 1) / kTcStages) & 1;
         if (copy_pending) mbar_wait(&sm.full[last], u, kWaitLimit);
         if (mma_pending) mbar_wait(&sm.mma[last], u, kWaitLimit);
       }
@@ -401,19 +426,23 @@ k_m2l_tc(LapTcParams p) {
       const int n = (int)sqrtf((float)row + 0.5f);
       const float sc = row < C ? p.sc.out[n] : 0.f;
       for (int c0 = 0; c0 < kTcN; c0 += 8) {
-        uint32_t r[8];
+        uint32_t r[8], q[8];
         const uint32_t addr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(mt * kTcN + c0);
         asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
                      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
                        "=r"(r[6]), "=r"(r[7])
                      : "r"(addr));
+        asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                     : "=r"(q[0]), "=r"(q[1]), "=r"(q[2]), "=r"(q[3]), "=r"(q[4]), "=r"(q[5]),
+                       "=r"(q[6]), "=r"(q[7])
+                     : "r"(addr + (uint32_t)(2 * kTcN)));
         asm volatile("tcgen05.wait::ld.sync.aligned;");
         if (row >= C) continue;
         for (int c = 0; c < 8; c++) {
           const int t = c0 + c;
           const int pl = sm.plin[t];
           if (pl < 0) continue;
-          const float v = __uint_as_float(r[c]) * sc;
+          const float v = (__uint_as_float(r[c]) + __uint_as_float(q[c])) * sc;
           if (p.nsplit > 1) {
             p.partial[(((int64_t)split * 8 + tau) * C + row) * np + pl] = v;
           } else {
@@ -428,7 +457,7 @@ k_m2l_tc(LapTcParams p) {
   asm volatile("tcgen05.fence::before_thread_sync;");
   __syncthreads();
   if (tid < 32)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 256;" ::"r"(tmem));
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem));
 }
 
 // sum of the split partial results (split order) into the level array
@@ -471,8 +500,8 @@ bool tc_lap_supported(int Ns, int Nr) {
 
 size_t tc_lin_bytes(int level, int P) {
   const int64_t npx = (1 << (level - 1)) + 2;
-  const int KP = ((P + 1) * (P + 1) + 7) / 8 * 8;
-  return sizeof(float) * 8 * (size_t)(npx * npx * npx) * KP;
+  const int KS = ((P + 1) * (P + 1) + 7) / 8;
+  return sizeof(float) * 8 * (size_t)(npx * npx * npx) * KS * 16;
 }
 
 // the order's operators, built on first use (FP64 tables, unit width)
@@ -539,7 +568,7 @@ int launch_m2l_tc(LapTcParams p, const float* mps, void* lin, cudaStream_t s) {
   const int64_t np = (int64_t)nx * nx * nx;
   WBFMM_CUDA(cudaMemsetAsync(lin, 0, tc_lin_bytes(p.level, p.P), s));
   const int64_t tot = np * 8 * C;
-  k_to_lin_tc<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(mps, p.level, p.P, p.KP, p.sc,
+  k_to_lin_tc<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(mps, p.level, p.P, p.KS, p.sc,
                                                             (float*)lin);
   WBFMM_CUDA(cudaGetLastError());
   p.lin = (const float*)lin;

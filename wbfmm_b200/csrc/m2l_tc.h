@@ -22,7 +22,7 @@ struct LapTcParams {
   const float* ops;          // dense operators, TF32 hi / lo tiles per shift slot
   const int* slot;           // shift code -> operator slot (-1: near field)
   const int* offsets;        // [8][189] packed list-4 offsets (build_offset_table)
-  const float* lin;          // [8][padded grid][KP] scaled source vectors
+  const float* lin;          // [8][padded grid][KS][16] scaled sources, TF32 hi / lo per 8-K chunk
   float* cout;               // regular expansions of the level (Layout L), added to
   float* partial;            // [nsplit][8][C][np] when nsplit > 1
   const int* act;            // sparse targets: [8][np] parents per child type, or null
