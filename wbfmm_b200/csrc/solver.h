@@ -918,8 +918,12 @@ struct Solver : public wbfmm_b200_solver {
     lp.err = flag.p + 2;
     const int64_t np = (int64_t)1 << (3 * (level - 1));
     const int64_t ctas = ((np + 127) / 128) * 8;
-    int ns = 1;
-    while (ctas * ns < 148 && ns < 16) ns *= 2;
+    // the tensor core's FP32 accumulation does not round to nearest: its
+    // error grows with the number of products summed into one accumulator,
+    // so each CTA takes at most 12 of the 189 offsets (and enough CTAs to
+    // fill the GPU); the splits' partial sums are added in FP32
+    int ns = 16;
+    while (ctas * ns < 148 && ns < 64) ns *= 2;
     lp.nsplit = ns;
     if (ns > 1) {
       WBFMM_TRY(tc_part.alloc((size_t)ns * 8 * (lp.P + 1) * (lp.P + 1) * np));
