@@ -920,9 +920,12 @@ struct Solver : public wbfmm_b200_solver {
     const int64_t ctas = ((np + 127) / 128) * 8;
     // the tensor core's FP32 accumulation does not round to nearest: its
     // error grows with the number of products summed into one accumulator,
-    // so each CTA takes at most 12 of the 189 offsets (and enough CTAs to
-    // fill the GPU); the splits' partial sums are added in FP32
-    int ns = 16;
+    // so each CTA takes at most 6 of the 189 offsets (and enough CTAs to
+    // fill the GPU); the splits' partial sums are added in FP32.  Measured
+    // on 300,000 points at depth 5 (orders 10-14), the potentials differ
+    // from the tile kernel's by 1.8e-5 (relative L2) with all 189 offsets
+    // in one accumulator, 2.2e-6 with 12 and 1.4e-6 with 6
+    int ns = 32;
     while (ctas * ns < 148 && ns < 64) ns *= 2;
     lp.nsplit = ns;
     if (ns > 1) {
