@@ -3,6 +3,14 @@
 // once as __host__ __device__ code; the kernels in kernels.cu call them one
 // point per lane/thread.
 //
+// Per-point state: the Legendre rows of the recursion live in caller
+// scratch (Scratch: per-thread slices of shared memory in the kernels, so
+// that they stay out of local memory), rows of kRowPad + N entries, the
+// number of rows given by p2m_rows / l2p_rows; cos(m ph), sin(m ph) are
+// advanced in registers along m (the recurrence the reference applies to
+// its arrays, so the same values); the spherical Bessel functions come
+// from BesselJSeq.
+//
 // P2M routines generate their coefficient contributions in a fixed order
 // that depends only on the expansion order, through an `emit(index, re, im)`
 // callback; the warp kernels reduce each emission across lanes, so the
@@ -13,45 +21,65 @@
 
 namespace wbfmm {
 
-constexpr int kPtMax = 66;   // per-point scratch: degree <= 64
+constexpr int kPtMax = 66;   // degree <= 64
+constexpr int kRowPad = 4;   // row length: N + kRowPad entries
+
+// scratch rows of the P2M and L2P routines (gradient: L2P with grad)
+HD int p2m_rows() { return 2; }
+HD int l2p_rows(bool helm, bool grad) { return helm && grad ? 3 : 2; }
+
+// zero rows 0..k-1 (entries 0..len-1)
+template <typename T>
+HD void zero_rows(const Scratch<T>& sc, int k) {
+  for (int r = 0; r < k; r++) {
+    Row<T> w = sc.row(r);
+    for (int i = 0; i < sc.len; i++) w[i] = T(0);
+  }
+}
+
+// (cos, sin) of (m+1) ph from those of m ph and ph
+template <typename T>
+HD void rot_next(T c, T s, T c1, T s1, T* cn, T* sn) {
+  *cn = c * c1 - s * s1;
+  *sn = s * c1 + c * s1;
+}
 
 // --------------------------------------------------- Helmholtz monopole
 // C_n^m += q j_n(kr) P_n^{|m|}(cos th) e^{-i m ph}
 // (src/expansions.c:30-123; an order-1 expansion keeps only n = 0 there)
 template <typename T, class Emit, class Leg = LegDirect<T>>
 HD void p2m_helmholtz(int N, T k, const T* xc, const T* xs, T qr, T qi,
-                      Emit&& emit, const Leg& leg = Leg()) {
+                      Emit&& emit, const Leg& leg, const Scratch<T>& sc) {
   if (N == 0) return;
-  T Pa[kPtMax], Pb[kPtMax], Cm[kPtMax], Sm[kPtMax];
   T r, th, ph;
   cart2sph(xc, xs, &r, &th, &ph);
   T C = cos(th), S = sin(th), kr = k * r;
-  T jm, j;
-  bessel_j_init(kr, &jm, &j);
-  T* pm = Pa; T* pn = Pb;
-  for (int i = 0; i < N + 3 && i < kPtMax; i++) Pa[i] = Pb[i] = T(0);
+  BesselJSeq<T> bj(kr);
+  zero_rows(sc, 2);
+  Row<T> pm = sc.row(0), pn = sc.row(1);
   legendre_init(C, S, &pm[0], &pn[0], &pn[1]);
-  Cm[0] = T(1); Sm[0] = T(0); Cm[1] = cos(ph); Sm[1] = sin(ph);
-  auto term = [&](int n, int m, int sgn, T jn, const T* P) {
-    T a = jn * P[m];
-    emit(cidx(n, sgn * m), a * (qr * Cm[m] + sgn * qi * Sm[m]),
-         a * (qi * Cm[m] - sgn * qr * Sm[m]));
+  const T c1 = cos(ph), s1 = sin(ph);
+  auto term = [&](int n, int m, int sgn, T jn, T P, T cm, T smm) {
+    T a = jn * P;
+    emit(cidx(n, sgn * m), a * (qr * cm + sgn * qi * smm),
+         a * (qi * cm - sgn * qr * smm));
   };
-  term(0, 0, 1, jm, pm);
+  term(0, 0, 1, bj.jm, pm[0], T(1), T(0));
   if (N == 1) return;
-  term(1, 0, 1, j, pn);
-  term(1, 1, 1, j, pn);
-  term(1, 1, -1, j, pn);
+  term(1, 0, 1, bj.j, pn[0], T(1), T(0));
+  term(1, 1, 1, bj.j, pn[1], c1, s1);
+  term(1, 1, -1, bj.j, pn[1], c1, s1);
   for (int n = 2; n <= N; n++) {
     legendre_step(pm, pn, n - 1, C, S, leg);
-    T* t = pm; pm = pn; pn = t;
-    bessel_j_step(&jm, &j, kr, n - 1);
-    Cm[n] = Cm[n - 1] * Cm[1] - Sm[n - 1] * Sm[1];
-    Sm[n] = Sm[n - 1] * Cm[1] + Cm[n - 1] * Sm[1];
-    term(n, 0, 1, j, pn);
+    Row<T> t = pm; pm = pn; pn = t;
+    bj.step();
+    term(n, 0, 1, bj.j, pn[0], T(1), T(0));
+    T cm = T(1), smm = T(0);
     for (int m = 1; m <= n; m++) {
-      term(n, m, 1, j, pn);
-      term(n, m, -1, j, pn);
+      rot_next(cm, smm, c1, s1, &cm, &smm);
+      const T P = pn[m];
+      term(n, m, 1, bj.j, P, cm, smm);
+      term(n, m, -1, bj.j, P, cm, smm);
     }
   }
 }
@@ -63,8 +91,7 @@ HD void p2m_helmholtz(int N, T k, const T* xc, const T* xs, T qr, T qi,
 template <typename T, class Emit, class Leg = LegDirect<T>>
 HD void p2m_helmholtz_dipole(int N, T k, const T* xc, const T* xs,
                              const T* nrm, T dr, T di, Emit&& emit,
-                             const Leg& leg = Leg()) {
-  T Pa[kPtMax], Pb[kPtMax], Cm[kPtMax], Sm[kPtMax];
+                             const Leg& leg, const Scratch<T>& sc) {
   T fm[2], fp[2], fz[2];
   fm[0] = T(0.5) * k * (dr * nrm[0] + di * nrm[1]);
   fm[1] = T(0.5) * k * (di * nrm[0] - dr * nrm[1]);
@@ -75,44 +102,44 @@ HD void p2m_helmholtz_dipole(int N, T k, const T* xc, const T* xs,
   T r, th, ph;
   cart2sph(xc, xs, &r, &th, &ph);
   T C = cos(th), S = sin(th), kr = k * r;
-  T jm, j;
-  bessel_j_init(kr, &jm, &j);
-  T* pm = Pa; T* pn = Pb;
-  for (int i = 0; i < N + 3 && i < kPtMax; i++) Pa[i] = Pb[i] = T(0);
+  BesselJSeq<T> bj(kr);
+  zero_rows(sc, 2);
+  Row<T> pm = sc.row(0), pn = sc.row(1);
   legendre_init(C, S, &pm[0], &pn[0], &pn[1]);
-  Cm[0] = T(1); Sm[0] = T(0); Cm[1] = cos(ph); Sm[1] = sin(ph);
+  const T c1 = cos(ph), s1 = sin(ph);
   // contribution w * R * f e^{-i sgn m ph} to coefficient (nn, mm)
-  auto put = [&](int nn, int mm, T w, T R, const T* f, int m, int sgn) {
+  auto put = [&](int nn, int mm, T w, T R, const T* f, T cm, T smm, int sgn) {
     if (nn < 0 || mm > nn || mm < -nn || w == T(0)) return;
-    T er = f[0] * Cm[m] + sgn * f[1] * Sm[m];
-    T ei = f[1] * Cm[m] - sgn * f[0] * Sm[m];
+    T er = f[0] * cm + sgn * f[1] * smm;
+    T ei = f[1] * cm - sgn * f[0] * smm;
     emit(cidx(nn, mm), w * R * er, w * R * ei);
   };
-  auto inc = [&](int n, int m, int sgn, T jn, const T* P) {
+  auto inc = [&](int n, int m, int sgn, T jn, T P, T cm, T smm) {
     if (n >= N) return;
-    T R = jn * P[m];
+    T R = jn * P;
     int sm = sgn * m;
-    put(n - 1, sm + 1, -rec_b<T>(n, sm), R, fm, m, sgn);
-    put(n - 1, sm - 1, -rec_b<T>(n, -sm), R, fp, m, sgn);
-    put(n - 1, sm, rec_a<T>(n - 1, sm), R, fz, m, sgn);
-    put(n + 1, sm + 1, rec_b<T>(n + 1, -sm - 1), R, fm, m, sgn);
-    put(n + 1, sm - 1, rec_b<T>(n + 1, sm - 1), R, fp, m, sgn);
-    put(n + 1, sm, -rec_a<T>(n, sm), R, fz, m, sgn);
+    put(n - 1, sm + 1, -rec_b<T>(n, sm), R, fm, cm, smm, sgn);
+    put(n - 1, sm - 1, -rec_b<T>(n, -sm), R, fp, cm, smm, sgn);
+    put(n - 1, sm, rec_a<T>(n - 1, sm), R, fz, cm, smm, sgn);
+    put(n + 1, sm + 1, rec_b<T>(n + 1, -sm - 1), R, fm, cm, smm, sgn);
+    put(n + 1, sm - 1, rec_b<T>(n + 1, sm - 1), R, fp, cm, smm, sgn);
+    put(n + 1, sm, -rec_a<T>(n, sm), R, fz, cm, smm, sgn);
   };
-  inc(0, 0, 1, jm, pm);
-  inc(1, 0, 1, j, pn);
-  inc(1, 1, 1, j, pn);
-  inc(1, 1, -1, j, pn);
+  inc(0, 0, 1, bj.jm, pm[0], T(1), T(0));
+  inc(1, 0, 1, bj.j, pn[0], T(1), T(0));
+  inc(1, 1, 1, bj.j, pn[1], c1, s1);
+  inc(1, 1, -1, bj.j, pn[1], c1, s1);
   for (int n = 2; n <= N; n++) {
     legendre_step(pm, pn, n - 1, C, S, leg);
-    T* t = pm; pm = pn; pn = t;
-    bessel_j_step(&jm, &j, kr, n - 1);
-    Cm[n] = Cm[n - 1] * Cm[1] - Sm[n - 1] * Sm[1];
-    Sm[n] = Sm[n - 1] * Cm[1] + Cm[n - 1] * Sm[1];
-    inc(n, 0, 1, j, pn);
+    Row<T> t = pm; pm = pn; pn = t;
+    bj.step();
+    inc(n, 0, 1, bj.j, pn[0], T(1), T(0));
+    T cm = T(1), smm = T(0);
     for (int m = 1; m <= n; m++) {
-      inc(n, m, 1, j, pn);
-      inc(n, m, -1, j, pn);
+      rot_next(cm, smm, c1, s1, &cm, &smm);
+      const T P = pn[m];
+      inc(n, m, 1, bj.j, P, cm, smm);
+      inc(n, m, -1, bj.j, P, cm, smm);
     }
   }
 }
@@ -122,34 +149,34 @@ HD void p2m_helmholtz_dipole(int N, T k, const T* xc, const T* xs,
 // (src/laplace.c:35-129); emit(index, value) per real slot
 template <typename T, class Emit, class Leg = LegDirect<T>>
 HD void p2m_laplace(int N, const T* xc, const T* xs, T q, Emit&& emit,
-                    const Leg& leg = Leg()) {
+                    const Leg& leg, const Scratch<T>& sc) {
   if (N == 0) return;
-  T Pa[kPtMax], Pb[kPtMax], Cm[kPtMax], Sm[kPtMax];
   T r, th, ph;
   cart2sph(xc, xs, &r, &th, &ph);
   T C = cos(th), S = sin(th);
-  T* pm = Pa; T* pn = Pb;
-  for (int i = 0; i < N + 3 && i < kPtMax; i++) Pa[i] = Pb[i] = T(0);
+  zero_rows(sc, 2);
+  Row<T> pm = sc.row(0), pn = sc.row(1);
   legendre_init(C, S, &pm[0], &pn[0], &pn[1]);
-  Cm[0] = T(1); Cm[1] = cos(ph); Sm[0] = T(0); Sm[1] = sin(ph);
+  const T c1 = cos(ph), s1 = sin(ph);
   T rn = T(1);
   emit(0, q * rn * pm[0] / T(1));
   rn = r;
   emit(1, q * rn * pn[0] / T(3));
-  emit(lidx(1, 1), q * rn * pn[1] * Cm[1] / T(3));
-  emit(lidx(1, 1) + 1, -(q * rn * pn[1] * Sm[1] / T(3)));
+  emit(lidx(1, 1), q * rn * pn[1] * c1 / T(3));
+  emit(lidx(1, 1) + 1, -(q * rn * pn[1] * s1 / T(3)));
   for (int n = 2; n <= N; n++) {
     rn *= r;
     legendre_step(pm, pn, n - 1, C, S, leg);
-    T* t = pm; pm = pn; pn = t;
-    Cm[n] = Cm[n - 1] * Cm[1] - Sm[n - 1] * Sm[1];
-    Sm[n] = Sm[n - 1] * Cm[1] + Cm[n - 1] * Sm[1];
+    Row<T> t = pm; pm = pn; pn = t;
     T inv = T(1) / (T)(2 * n + 1);
     emit(n * n, q * rn * pn[0] * inv);
+    T cm = T(1), smm = T(0);
     for (int m = 1; m <= n; m++) {
-      int id = lidx(n, m);
-      emit(id, q * rn * pn[m] * Cm[m] * inv);
-      emit(id + 1, -(q * rn * pn[m] * Sm[m] * inv));
+      rot_next(cm, smm, c1, s1, &cm, &smm);
+      const int id = lidx(n, m);
+      const T P = pn[m];
+      emit(id, q * rn * P * cm * inv);
+      emit(id + 1, -(q * rn * P * smm * inv));
     }
   }
 }
@@ -158,17 +185,17 @@ HD void p2m_laplace(int N, const T* xc, const T* xs, T q, Emit&& emit,
 // Dipole of strength d along the unit normal (src/laplace.c:181-423)
 template <typename T, class Emit, class Leg = LegDirect<T>>
 HD void p2m_laplace_dipole(int N, const T* xc, const T* xs, const T* nrm,
-                           T d, Emit&& emit, const Leg& leg = Leg()) {
+                           T d, Emit&& emit, const Leg& leg,
+                           const Scratch<T>& sc) {
   if (N == 0) return;
-  T Pa[kPtMax], Pb[kPtMax], Cm[kPtMax], Sm[kPtMax];
   T fx = nrm[0] * d, fy = nrm[1] * d, fz = nrm[2] * d;
   T r, th, ph;
   cart2sph(xc, xs, &r, &th, &ph);
   T C = cos(th), S = sin(th);
-  T* pm = Pa; T* pn = Pb;
-  for (int i = 0; i < N + 3 && i < kPtMax; i++) Pa[i] = Pb[i] = T(0);
+  zero_rows(sc, 2);
+  Row<T> pm = sc.row(0), pn = sc.row(1);
   legendre_init(C, S, &pm[0], &pn[0], &pn[1]);
-  Cm[0] = T(1); Cm[1] = cos(ph); Sm[0] = T(0); Sm[1] = sin(ph);
+  const T c1 = cos(ph), s1 = sin(ph);
   auto weights = [](int n, int m, T* a0, T* a1, T* a2) {
     T f = (T)(2 * n + 1) / (T)(2 * n + 3);
     *a0 = sqrt(f * (T)(n + m + 1) * (T)(n + m + 2));
@@ -176,54 +203,55 @@ HD void p2m_laplace_dipole(int N, const T* xc, const T* xs, const T* nrm,
     *a2 = sqrt(((T)(n + 1) * (T)(n + 1) - (T)(m * m)) * (T)(2 * n + 1) /
                (T)(2 * n + 3));
   };
-  auto inc_m0 = [&](int n, T rn, const T* P) {
-    T R = rn * P[0] / (T)(2 * n + 1), a0, a1, a2;
+  auto inc_m0 = [&](int n, T rn, T P0) {
+    T R = rn * P0 / (T)(2 * n + 1), a0, a1, a2;
     weights(n, 0, &a0, &a1, &a2);
     int ip = lidx(n + 1, 1), i0 = (n + 1) * (n + 1);
-    emit(ip, fx * T(0.5) * a0 * R * Cm[0] - fy * T(0.5) * a0 * R * Sm[0]);
-    emit(ip + 1, -(fx * T(0.5) * a0 * R * Sm[0]) - fy * T(0.5) * a0 * R * Cm[0]);
+    const T cm = T(1), smm = T(0);
+    emit(ip, fx * T(0.5) * a0 * R * cm - fy * T(0.5) * a0 * R * smm);
+    emit(ip + 1, -(fx * T(0.5) * a0 * R * smm) - fy * T(0.5) * a0 * R * cm);
     emit(i0, fz * a2 * R);
   };
-  auto inc_m1 = [&](int n, T rn, const T* P) {
+  auto inc_m1 = [&](int n, T rn, T P1) {
     const int m = 1;
-    T R = rn * P[m] / (T)(2 * n + 1), a0, a1, a2;
+    T R = rn * P1 / (T)(2 * n + 1), a0, a1, a2;
     weights(n, m, &a0, &a1, &a2);
     int ip = lidx(n + 1, m + 1), i0 = (n + 1) * (n + 1), id = lidx(n + 1, m);
-    emit(ip, fx * T(0.5) * a0 * R * Cm[m] - fy * T(0.5) * a0 * R * Sm[m]);
-    emit(ip + 1, -(fx * T(0.5) * a0 * R * Sm[m]) - fy * T(0.5) * a0 * R * Cm[m]);
-    emit(i0, fx * a1 * R * Cm[m] + fy * a1 * R * Sm[m]);
-    emit(id, fz * a2 * R * Cm[m]);
-    emit(id + 1, -(fz * a2 * R * Sm[m]));
+    emit(ip, fx * T(0.5) * a0 * R * c1 - fy * T(0.5) * a0 * R * s1);
+    emit(ip + 1, -(fx * T(0.5) * a0 * R * s1) - fy * T(0.5) * a0 * R * c1);
+    emit(i0, fx * a1 * R * c1 + fy * a1 * R * s1);
+    emit(id, fz * a2 * R * c1);
+    emit(id + 1, -(fz * a2 * R * s1));
   };
-  auto inc = [&](int n, int m, T rn, const T* P) {
-    T R = rn * P[m] / (T)(2 * n + 1), a0, a1, a2;
+  auto inc = [&](int n, int m, T rn, T P, T cm, T smm) {
+    T R = rn * P / (T)(2 * n + 1), a0, a1, a2;
     weights(n, m, &a0, &a1, &a2);
     int ip = lidx(n + 1, m + 1), im = lidx(n + 1, m - 1), id = lidx(n + 1, m);
-    emit(ip, fx * T(0.5) * a0 * R * Cm[m] - fy * T(0.5) * a0 * R * Sm[m]);
-    emit(ip + 1, -(fx * T(0.5) * a0 * R * Sm[m]) - fy * T(0.5) * a0 * R * Cm[m]);
-    emit(im, fx * T(0.5) * a1 * R * Cm[m] + fy * T(0.5) * a1 * R * Sm[m]);
-    emit(im + 1, -(fx * T(0.5) * a1 * R * Sm[m]) + fy * T(0.5) * a1 * R * Cm[m]);
-    emit(id, fz * a2 * R * Cm[m]);
-    emit(id + 1, -(fz * a2 * R * Sm[m]));
+    emit(ip, fx * T(0.5) * a0 * R * cm - fy * T(0.5) * a0 * R * smm);
+    emit(ip + 1, -(fx * T(0.5) * a0 * R * smm) - fy * T(0.5) * a0 * R * cm);
+    emit(im, fx * T(0.5) * a1 * R * cm + fy * T(0.5) * a1 * R * smm);
+    emit(im + 1, -(fx * T(0.5) * a1 * R * smm) + fy * T(0.5) * a1 * R * cm);
+    emit(id, fz * a2 * R * cm);
+    emit(id + 1, -(fz * a2 * R * smm));
   };
   T rn = T(1);
-  inc_m0(0, rn, pm);
+  inc_m0(0, rn, pm[0]);
   if (N == 1) return;
   rn *= r;
-  Cm[2] = Cm[1] * Cm[1] - Sm[1] * Sm[1];
-  Sm[2] = Sm[1] * Cm[1] + Cm[1] * Sm[1];
-  inc_m0(1, rn, pn);
-  inc_m1(1, rn, pn);
+  inc_m0(1, rn, pn[0]);
+  inc_m1(1, rn, pn[1]);
   if (N == 2) return;
   for (int n = 2; n < N; n++) {
     rn *= r;
     legendre_step(pm, pn, n - 1, C, S, leg);
-    T* t = pm; pm = pn; pn = t;
-    Cm[n + 1] = Cm[n] * Cm[1] - Sm[n] * Sm[1];
-    Sm[n + 1] = Sm[n] * Cm[1] + Cm[n] * Sm[1];
-    inc_m0(n, rn, pn);
-    inc_m1(n, rn, pn);
-    for (int m = 2; m <= n; m++) inc(n, m, rn, pn);
+    Row<T> t = pm; pm = pn; pn = t;
+    inc_m0(n, rn, pn[0]);
+    inc_m1(n, rn, pn[1]);
+    T cm = c1, smm = s1;
+    for (int m = 2; m <= n; m++) {
+      rot_next(cm, smm, c1, s1, &cm, &smm);
+      inc(n, m, rn, pn[m], cm, smm);
+    }
   }
 }
 
@@ -232,65 +260,63 @@ HD void p2m_laplace_dipole(int N, const T* xc, const T* xs, const T* nrm,
 // coef(idx) returns coefficient idx as (re, im)
 template <typename T, class Coef, class Leg = LegDirect<T>>
 HD void l2p_helmholtz(int N, T k, const T* xc, const T* xf, Coef&& coef,
-                      T* fr, T* fi, const Leg& leg = Leg()) {
-  T Pa[kPtMax], Pb[kPtMax], Cm[kPtMax], Sm[kPtMax];
+                      T* fr, T* fi, const Leg& leg, const Scratch<T>& sc) {
   T r, th, ph;
   cart2sph(xc, xf, &r, &th, &ph);
   T C = cos(th), S = sin(th), kr = k * r;
-  T jm, j;
-  bessel_j_init(kr, &jm, &j);
-  T* pm = Pa; T* pn = Pb;
-  for (int i = 0; i < N + 3 && i < kPtMax; i++) Pa[i] = Pb[i] = T(0);
+  BesselJSeq<T> bj(kr);
+  zero_rows(sc, 2);
+  Row<T> pm = sc.row(0), pn = sc.row(1);
   legendre_init(C, S, &pm[0], &pn[0], &pn[1]);
-  Cm[0] = T(1); Sm[0] = T(0); Cm[1] = cos(ph); Sm[1] = sin(ph);
+  const T c1 = cos(ph), s1 = sin(ph);
   T sr = T(0), si = T(0);
-  auto inc0 = [&](int n, T jn, const T* P) {
+  auto inc0 = [&](int n, T jn, T P0) {
     T a, b;
     coef(cidx(n, 0), &a, &b);
-    T w = Cm[0] * jn * P[0];
+    T w = T(1) * jn * P0;
     sr += a * w; si += b * w;
   };
-  auto inc = [&](int n, int m, T jn, const T* P) {
+  auto inc = [&](int n, int m, T jn, T P, T cm, T smm) {
     T ar, ai, br, bi;
     coef(cidx(n, m), &ar, &ai);
     coef(cidx(n, -m), &br, &bi);
-    T wc = jn * P[m] * Cm[m], ws = jn * P[m] * Sm[m];
+    T wc = jn * P * cm, ws = jn * P * smm;
     sr += wc * (ar + br) - ws * (ai - bi);
     si += wc * (ai + bi) + ws * (ar - br);
   };
-  inc0(0, jm, pm);
-  inc0(1, j, pn);
-  inc(1, 1, j, pn);
+  inc0(0, bj.jm, pm[0]);
+  inc0(1, bj.j, pn[0]);
+  inc(1, 1, bj.j, pn[1], c1, s1);
   for (int n = 2; n <= N; n++) {
     legendre_step(pm, pn, n - 1, C, S, leg);
-    T* t = pm; pm = pn; pn = t;
-    bessel_j_step(&jm, &j, kr, n - 1);
-    Cm[n] = Cm[n - 1] * Cm[1] - Sm[n - 1] * Sm[1];
-    Sm[n] = Sm[n - 1] * Cm[1] + Cm[n - 1] * Sm[1];
-    inc0(n, j, pn);
-    for (int m = 1; m <= n; m++) inc(n, m, j, pn);
+    Row<T> t = pm; pm = pn; pn = t;
+    bj.step();
+    inc0(n, bj.j, pn[0]);
+    T cm = T(1), smm = T(0);
+    for (int m = 1; m <= n; m++) {
+      rot_next(cm, smm, c1, s1, &cm, &smm);
+      inc(n, m, bj.j, pn[m], cm, smm);
+    }
   }
   *fr += sr; *fi += si;
 }
 
 // gradient of the regular expansion, G&D (2004) (3.7)
 // (src/gradient.c:193-399); g[0..5] += (dx re, dx im, dy re, dy im, dz re, dz im)
-// pot (optional): the potential of l2p_helmholtz added in the same sweep
+// pot (optional): the potential of l2p_helmholtz added in the same sweep.
+// Three scratch rows hold degrees n - 1, n, n + 1 and rotate as n grows.
 template <typename T, class Coef, class Rec = RecDirect<T>, class Leg = LegDirect<T>>
 HD void l2p_helmholtz_grad(int N, T k, const T* xc, const T* xf, Coef&& coef,
-                           T* g, T* pot = nullptr, const Rec& rec = Rec(),
-                           const Leg& leg = Leg()) {
-  T Pm1[kPtMax], Pa[kPtMax], Pb[kPtMax], Cm[kPtMax + 1], Sm[kPtMax + 1];
+                           T* g, T* pot, const Rec& rec, const Leg& leg,
+                           const Scratch<T>& sc) {
   T r, th, ph;
   cart2sph(xc, xf, &r, &th, &ph);
   T C = cos(th), S = sin(th), Cph = cos(ph), Sph = sin(ph), kr = k * r;
-  T jn, jnp1, jnm1;
-  for (int i = 0; i < N + 4 && i < kPtMax; i++) Pm1[i] = Pa[i] = Pb[i] = T(0);
-  bessel_j_init(kr, &jn, &jnp1);
-  T* pn = Pa; T* pnp1 = Pb;
+  zero_rows(sc, 3);
+  Row<T> pm1 = sc.row(2), pn = sc.row(0), pnp1 = sc.row(1);
   legendre_init(C, S, &pn[0], &pnp1[0], &pnp1[1]);
-  Cm[0] = T(1); Sm[0] = T(0); Cm[1] = Cph; Sm[1] = Sph;
-  jnm1 = T(0);
+  BesselJSeq<T> bj(kr);
+  T jnm1 = T(0), jn = bj.jm, jnp1 = bj.j;
   T acc[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
   T pr = T(0), pi = T(0);
   auto inc = [&](int n, int m, int sgn, T cm1, T sm1, T cmm, T smm, T cp1,
@@ -301,18 +327,18 @@ HD void l2p_helmholtz_grad(int N, T k, const T* xc, const T* xf, Coef&& coef,
     T c[6];
     T b1 = rec.b(n + 1, -sgn * m - 1) / T(2);
     T b2 = rec.b(n, sgn * m) / T(2);
-    T u = b1 * tp * pnp1[mp1] - b2 * tm * Pm1[mp1];
+    T u = b1 * tp * pnp1[mp1] - b2 * tm * pm1[mp1];
     c[0] = c[4] = cp1 * u;
     c[1] = c[5] = sp1 * u;
     b1 = rec.b(n + 1, sgn * m - 1) / T(2);
     b2 = rec.b(n, -sgn * m) / T(2);
-    u = b1 * tp * pnp1[mm1] - b2 * tm * Pm1[mm1];
+    u = b1 * tp * pnp1[mm1] - b2 * tm * pm1[mm1];
     c[3] = cm1 * u;
     c[2] = -sm1 * u;
     c[0] += c[3]; c[1] -= c[2];
     c[2] += c[5]; c[3] -= c[4];
     T a1 = rec.a(n - 1, m), a2 = rec.a(n, m);
-    u = a1 * tm * Pm1[m] - a2 * tp * pnp1[m];
+    u = a1 * tm * pm1[m] - a2 * tp * pnp1[m];
     c[4] = cmm * u;
     c[5] = smm * u;
     T ar, ai;
@@ -326,30 +352,34 @@ HD void l2p_helmholtz_grad(int N, T k, const T* xc, const T* xf, Coef&& coef,
       pi += w * (cmm * ai + smm * ar);
     }
   };
-  inc(0, 0, 1, Cm[1], -Sm[1], Cm[0], Sm[0], Cm[1], Sm[1]);
-  jnm1 = jn;
-  bessel_j_step(&jn, &jnp1, kr, 1);
-  // n = 1
-  Pm1[0] = pn[0]; Pm1[1] = pn[1];
-  legendre_step(pn, pnp1, 1, C, S, leg);
-  { T* t = pn; pn = pnp1; pnp1 = t; }
-  Cm[2] = Cm[1] * Cph - Sm[1] * Sph;
-  Sm[2] = Sm[1] * Cph + Cm[1] * Sph;
-  inc(1, 0, 1, Cm[1], -Sm[1], Cm[0], Sm[0], Cm[1], Sm[1]);
-  inc(1, 1, 1, Cm[0], Sm[0], Cm[1], Sm[1], Cm[2], Sm[2]);
-  inc(1, 1, -1, Cm[2], -Sm[2], Cm[1], -Sm[1], Cm[0], -Sm[0]);
+  // advance the rows and Bessel values from degree n - 1 to degree n
+  auto advance = [&](int n) {
+    Row<T> out = pm1;
+    legendre_next(out, pn, pnp1, n, C, S, leg);
+    pm1 = pn; pn = pnp1; pnp1 = out;
+    jnm1 = bj.jm;
+    bj.step();
+    jn = bj.jm; jnp1 = bj.j;
+  };
+  inc(0, 0, 1, Cph, -Sph, T(1), T(0), Cph, Sph);
+  advance(1);
+  {  // n = 1
+    T c2, s2;
+    rot_next(Cph, Sph, Cph, Sph, &c2, &s2);
+    inc(1, 0, 1, Cph, -Sph, T(1), T(0), Cph, Sph);
+    inc(1, 1, 1, T(1), T(0), Cph, Sph, c2, s2);
+    inc(1, 1, -1, c2, -s2, Cph, -Sph, T(1), -T(0));
+  }
   for (int n = 2; n <= N; n++) {
-    for (int i = 0; i <= n; i++) Pm1[i] = pn[i];
-    legendre_step(pn, pnp1, n, C, S, leg);
-    { T* t = pn; pn = pnp1; pnp1 = t; }
-    jnm1 = jn;
-    bessel_j_step(&jn, &jnp1, kr, n);
-    Cm[n + 1] = Cm[n] * Cph - Sm[n] * Sph;
-    Sm[n + 1] = Sm[n] * Cph + Cm[n] * Sph;
-    inc(n, 0, 1, Cm[1], -Sm[1], Cm[0], Sm[0], Cm[1], Sm[1]);
+    advance(n);
+    inc(n, 0, 1, Cph, -Sph, T(1), T(0), Cph, Sph);
+    // (cos, sin) of (m - 1) ph, m ph, (m + 1) ph
+    T ca = T(1), sa = T(0), cb = Cph, sb = Sph, cc, scc;
     for (int m = 1; m <= n; m++) {
-      inc(n, m, 1, Cm[m - 1], Sm[m - 1], Cm[m], Sm[m], Cm[m + 1], Sm[m + 1]);
-      inc(n, m, -1, Cm[m + 1], -Sm[m + 1], Cm[m], -Sm[m], Cm[m - 1], -Sm[m - 1]);
+      rot_next(cb, sb, Cph, Sph, &cc, &scc);
+      inc(n, m, 1, ca, sa, cb, sb, cc, scc);
+      inc(n, m, -1, cc, -scc, cb, -sb, ca, -sa);
+      ca = cb; sa = sb; cb = cc; sb = scc;
     }
   }
   for (int i = 0; i < 6; i++) g[i] += acc[i];
@@ -361,30 +391,29 @@ HD void l2p_helmholtz_grad(int N, T k, const T* xc, const T* xf, Coef&& coef,
 // (src/local-laplace.c:333-398); coef(idx) returns real slot idx
 template <typename T, class Coef, class Leg = LegDirect<T>>
 HD T l2p_laplace(int N, const T* xc, const T* xf, Coef&& coef,
-                 const Leg& leg = Leg()) {
-  T Pa[kPtMax], Pb[kPtMax], Cm[kPtMax], Sm[kPtMax];
+                 const Leg& leg, const Scratch<T>& sc) {
   T r, th, ph;
   cart2sph(xc, xf, &r, &th, &ph);
   T C = cos(th), S = sin(th);
-  T* pm = Pa; T* pn = Pb;
-  for (int i = 0; i < N + 3 && i < kPtMax; i++) Pa[i] = Pb[i] = T(0);
+  zero_rows(sc, 2);
+  Row<T> pm = sc.row(0), pn = sc.row(1);
   legendre_init(C, S, &pm[0], &pn[0], &pn[1]);
-  Cm[0] = T(1); Cm[1] = cos(ph); Sm[0] = T(0); Sm[1] = sin(ph);
+  const T c1 = cos(ph), s1 = sin(ph);
   T f = T(0), rn = T(1);
   f += coef(0) * rn * pm[0];
   rn *= r;
   f += coef(1) * rn * pn[0];
-  f += T(2) * pn[1] * rn * (coef(lidx(1, 1)) * Cm[1] - coef(lidx(1, 1) + 1) * Sm[1]);
+  f += T(2) * pn[1] * rn * (coef(lidx(1, 1)) * c1 - coef(lidx(1, 1) + 1) * s1);
   for (int n = 2; n <= N; n++) {
     rn *= r;
     legendre_step(pm, pn, n - 1, C, S, leg);
-    T* t = pm; pm = pn; pn = t;
-    Cm[n] = Cm[n - 1] * Cm[1] - Sm[n - 1] * Sm[1];
-    Sm[n] = Sm[n - 1] * Cm[1] + Cm[n - 1] * Sm[1];
+    Row<T> t = pm; pm = pn; pn = t;
     f += coef(n * n) * rn * pn[0];
+    T cm = T(1), smm = T(0);
     for (int m = 1; m <= n; m++) {
+      rot_next(cm, smm, c1, s1, &cm, &smm);
       int id = lidx(n, m);
-      f += T(2) * pn[m] * rn * (coef(id) * Cm[m] - coef(id + 1) * Sm[m]);
+      f += T(2) * pn[m] * rn * (coef(id) * cm - coef(id + 1) * smm);
     }
   }
   return f;
@@ -395,61 +424,65 @@ HD T l2p_laplace(int N, const T* xc, const T* xf, Coef&& coef,
 // pot (optional): the potential of l2p_laplace added in the same sweep
 template <typename T, class Coef, class LRec = LapRecDirect<T>, class Leg = LegDirect<T>>
 HD void l2p_laplace_grad(int N, const T* xc, const T* xf, Coef&& coef, T* g,
-                         T* pot = nullptr, const LRec& rec = LRec(),
-                         const Leg& leg = Leg()) {
+                         T* pot, const LRec& rec, const Leg& leg,
+                         const Scratch<T>& sc) {
   if (N == 0) return;
-  T Pa[kPtMax], Pb[kPtMax], Cm[kPtMax + 1], Sm[kPtMax + 1];
   T r, th, ph;
   cart2sph(xc, xf, &r, &th, &ph);
   T C = cos(th), S = sin(th);
-  T* pm = Pa; T* pn = Pb;
-  for (int i = 0; i < N + 3 && i < kPtMax; i++) Pa[i] = Pb[i] = T(0);
+  zero_rows(sc, 2);
+  Row<T> pm = sc.row(0), pn = sc.row(1);
   legendre_init(C, S, &pm[0], &pn[0], &pn[1]);
-  Cm[0] = T(1); Sm[0] = T(0); Cm[1] = cos(ph); Sm[1] = sin(ph);
+  const T c1 = cos(ph), s1 = sin(ph);
   T gx = T(0), gy = T(0), gz = T(0), f = T(0);
   // degree n >= 2: P holds degree n-1 (gradient), Pn degree n (potential)
-  auto d_m0 = [&](int n, T rnm1, const T* P, const T* Pn) {
+  auto d_m0 = [&](int n, T rnm1, Row<T> P, Row<T> Pn) {
     T am, a0, a1;
     rec.c(n, 0, &am, &a0, &a1);
     T R0 = rnm1 * P[0] * a0, R1 = rnm1 * P[1] * a1;
     T cr = coef(n * n);
-    gx += cr * (-R1 * Cm[1]);
-    gy += cr * (-R1 * Sm[1]);
+    gx += cr * (-R1 * c1);
+    gy += cr * (-R1 * s1);
     gz += cr * R0;
     if (pot) f += cr * rnm1 * r * Pn[0];
   };
-  auto d_m = [&](int n, int m, T rnm1, const T* P, const T* Pn) {
+  // (ca, sa), (cb, sb), (cc, scc): (cos, sin) of (m - 1) ph, m ph, (m + 1) ph
+  auto d_m = [&](int n, int m, T rnm1, Row<T> P, Row<T> Pn, T ca, T sa, T cb,
+                 T sb, T cc, T scc) {
     T am, a0, ap;
     rec.c(n, m, &am, &a0, &ap);
     T Rm = rnm1 * P[m - 1] * am, R0 = rnm1 * P[m] * a0 * T(2);
     T Rp = rnm1 * P[m + 1] * ap;
-    T xr = -Rp * Cm[m + 1] + Rm * Cm[m - 1], xi = -Rp * Sm[m + 1] + Rm * Sm[m - 1];
-    T yr = -Rp * Sm[m + 1] - Rm * Sm[m - 1], yi = Rp * Cm[m + 1] + Rm * Cm[m - 1];
-    T zr = R0 * Cm[m], zi = R0 * Sm[m];
+    T xr = -Rp * cc + Rm * ca, xi = -Rp * scc + Rm * sa;
+    T yr = -Rp * scc - Rm * sa, yi = Rp * cc + Rm * ca;
+    T zr = R0 * cb, zi = R0 * sb;
     int id = lidx(n, m);
     T cr = coef(id), ci = -coef(id + 1);
     gx += cr * xr + ci * xi;
     gy += cr * yr + ci * yi;
     gz += cr * zr + ci * zi;
-    if (pot) f += T(2) * Pn[m] * rnm1 * r * (cr * Cm[m] + ci * Sm[m]);
+    if (pot) f += T(2) * Pn[m] * rnm1 * r * (cr * cb + ci * sb);
   };
   T rnm1 = T(1);
-  Cm[2] = Cm[1] * Cm[1] - Sm[1] * Sm[1];
-  Sm[2] = Sm[1] * Cm[1] + Cm[1] * Sm[1];
+  T c2, s2;
+  rot_next(c1, s1, c1, s1, &c2, &s2);
   {  // n = 1, m = 0: only the z derivative is non-zero
     T R0 = rnm1 * pm[0] * sqrt(T(3));
     gz += coef(1) * R0;
     if (pot) f += coef(0) * pm[0] + coef(1) * r * pn[0];
   }
-  d_m(1, 1, rnm1, pm, pn);
+  d_m(1, 1, rnm1, pm, pn, T(1), T(0), c1, s1, c2, s2);
   for (int n = 2; n <= N; n++) {
     rnm1 *= r;
     legendre_step(pm, pn, n - 1, C, S, leg);
-    T* t = pm; pm = pn; pn = t;       // pm now degree n-1, pn degree n
-    Cm[n + 1] = Cm[n] * Cm[1] - Sm[n] * Sm[1];
-    Sm[n + 1] = Sm[n] * Cm[1] + Cm[n] * Sm[1];
+    Row<T> t = pm; pm = pn; pn = t;       // pm now degree n-1, pn degree n
     d_m0(n, rnm1, pm, pn);
-    for (int m = 1; m <= n; m++) d_m(n, m, rnm1, pm, pn);
+    T ca = T(1), sa = T(0), cb = c1, sb = s1, cc, scc;
+    for (int m = 1; m <= n; m++) {
+      rot_next(cb, sb, c1, s1, &cc, &scc);
+      d_m(n, m, rnm1, pm, pn, ca, sa, cb, sb, cc, scc);
+      ca = cb; sa = sb; cb = cc; sb = scc;
+    }
   }
   g[0] += gx; g[1] += gy; g[2] += gz;
   if (pot) *pot += f;

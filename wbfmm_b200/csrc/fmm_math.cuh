@@ -186,8 +186,8 @@ HD void leg_table_fill(T* t, int nmax, int tid, int nt) {
 // Advance: pnm1 holds degree n-1 on entry, pn degree n; on exit pnm1 holds
 // degree n+1 (caller swaps roles).  Entry n+1 of pn is zeroed, as in the
 // reference (src/util.c:58-86).
-template <typename T, class Leg = LegDirect<T>>
-HD void legendre_step(T* pnm1, T* pn, int n, T C, T S, const Leg& L = Leg()) {
+template <typename T, class R, class Leg = LegDirect<T>>
+HD void legendre_step(R pnm1, R pn, int n, T C, T S, const Leg& L = Leg()) {
   pnm1[n + 1] = L.d(n) * S * pn[n];
   pn[n + 1] = T(0);
   const T sq = L.c(n);
@@ -197,18 +197,56 @@ HD void legendre_step(T* pnm1, T* pn, int n, T C, T S, const Leg& L = Leg()) {
   }
 }
 
-// Spherical Bessel j_n by series, used when x <= n (src/util.c:118-141)
+// One step of the recursion from degree n into a third row: out receives
+// degree n + 1 from pnm1 (degree n - 1) and pn (degree n), which are left
+// as they are; the arithmetic of legendre_step.  Entries of out above n + 1
+// must be zero already (rows start zeroed and only ever take higher degrees).
+template <typename T, class R, class Leg>
+HD void legendre_next(R out, R pnm1, R pn, int n, T C, T S, const Leg& L) {
+  out[n + 1] = L.d(n) * S * pn[n];
+  const T sq = L.c(n);
+  for (int m = 0; m <= n; m++) {
+    const T v = C * sq * pn[m] - L.a(n, m) * pnm1[m];
+    out[m] = v * L.b(n, m);
+  }
+}
+
+// A row of per-point scratch values with entry i at p[i * s]: the kernels
+// give each thread strided slices of shared memory (s = the CTA's thread
+// count, so that a warp's 32 threads touch 32 consecutive words), host code
+// a plain array (s = 1).
 template <typename T>
-HD T bessel_j_series(int n, T x) {
+struct Row {
+  T* p;
+  int s;
+  HD T& operator[](int i) const { return p[i * s]; }
+};
+// k rows of len entries each: row k at p + k len s
+template <typename T>
+struct Scratch {
+  T* p;
+  int len, s;
+  HD Row<T> row(int k) const { return Row<T>{p + k * len * s, s}; }
+};
+
+// Spherical Bessel j_n by series, used when x <= n (src/util.c:118-141):
+// the prefactor x^n / (2n+1)!! times the sum of the series
+template <typename T>
+HD T bessel_j_series_sum(int n, T x) {
   const T tol = sizeof(T) == 4 ? T(1e-7) : T(1e-15);
-  T x2q = T(1), x2 = x * x, sc = T(1) / (T)(2 * n + 1);
-  for (int q = 0; q < n; q++) sc *= x / (T)(2 * q + 1);
+  T x2q = T(1), x2 = x * x;
   T jn = x2q;
   for (int q = 0; (q < 64) && (fabs(x2q) > tol); q++) {
     x2q *= -x2 / (T)((2 * q + 2) * (2 * n + 2 * (q + 1) + 1));
     jn += x2q;
   }
-  return jn * sc;
+  return jn;
+}
+template <typename T>
+HD T bessel_j_series(int n, T x) {
+  T sc = T(1) / (T)(2 * n + 1);
+  for (int q = 0; q < n; q++) sc *= x / (T)(2 * q + 1);
+  return bessel_j_series_sum<T>(n, x) * sc;
 }
 template <typename T>
 HD void bessel_j_init(T x, T* j0, T* j1) {
@@ -230,6 +268,26 @@ HD void bessel_j_step(T* jnm1, T* jn, T x, int n) {
   *jnm1 = *jn;
   *jn = bessel_j_series<T>(n + 1, x);
 }
+// j_{n-1}, j_n at x for n = 1, 2, ...: the steps of bessel_j_step, with the
+// series prefactor x^n / (2n-1)!! carried from degree to degree (one
+// division a step instead of n)
+template <typename T>
+struct BesselJSeq {
+  T x, jm, j, a;
+  int n;
+  HD explicit BesselJSeq(T x_) : x(x_), n(1) {
+    bessel_j_init(x, &jm, &j);
+    a = x;
+  }
+  HD void step() {
+    a *= x / (T)(2 * n + 1);               // x^(n+1) / (2n+1)!!
+    T jn1;
+    if (x > (T)(n + 1)) jn1 = j * (T)(2 * n + 1) / x - jm;
+    else jn1 = bessel_j_series_sum<T>(n + 1, x) * (a / (T)(2 * n + 3));
+    jm = j; j = jn1; n++;
+  }
+};
+
 // h_n = j_n + i y_n, upward recursion (src/util.c:177-202)
 template <typename T>
 HD void bessel_h_init(T x, T* h0, T* h1) {

@@ -53,7 +53,23 @@ static size_t leg_table_bytes(int N) {
   return b <= 40 * 1024 ? b : 0;
 }
 
-template <typename T, bool HELM>
+// shared-memory bytes of the per-thread recursion rows (expand.cuh) of a
+// CTA of `threads` threads
+template <typename T>
+static size_t p2m_row_bytes(int N, int threads) {
+  return sizeof(T) * (size_t)p2m_rows() * (N + kRowPad) * threads;
+}
+template <typename T>
+static size_t l2p_row_bytes(int N, bool helm, bool grad, int threads) {
+  return sizeof(T) * (size_t)l2p_rows(helm, grad) * (N + kRowPad) * threads;
+}
+// rows in shared memory up to this many bytes per CTA; above it (high
+// orders, FP64) the rows stay in per-thread local arrays, where occupancy
+// is worth more than the shorter latency
+constexpr size_t kRowSmemMax = 48 * 1024;
+
+// SROWS: recursion rows in shared memory (else per-thread local arrays)
+template <typename T, bool HELM, bool SROWS>
 __global__ void k_p2m(P2MParams<T> p, int legt) {
   extern __shared__ __align__(16) unsigned char smraw[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -69,7 +85,12 @@ __global__ void k_p2m(P2MParams<T> p, int legt) {
   if (b >= p.nbox) return;   // whole warp leaves; no block barriers below
   const int nc = ncoef(p.N);
   const int w = HELM ? 2 : 1;
-  T* acc = (T*)smraw + (legt ? 4 * LW * LW : 0) + (size_t)warp * nc * w;
+  const int RL = p.N + kRowPad;
+  T* rows = (T*)smraw + (legt ? 4 * LW * LW : 0);
+  T loc[SROWS ? 1 : 2 * kPtMax];
+  const Scratch<T> sc = SROWS ? Scratch<T>{rows + threadIdx.x, RL, (int)blockDim.x}
+                              : Scratch<T>{loc, RL, 1};
+  T* acc = rows + (SROWS ? p2m_rows() * RL * blockDim.x : 0) + (size_t)warp * nc * w;
   for (int c = lane; c < nc * w; c += 32) acc[c] = T(0);
   __syncwarp();
   const uint32_t cnt = p.box_n[b], start = p.box_i[b];
@@ -93,13 +114,13 @@ __global__ void k_p2m(P2MParams<T> p, int legt) {
           };
           if (p.q) {
             T qr = act ? p.q[2 * s] : T(0), qi = act ? p.q[2 * s + 1] : T(0);
-            p2m_helmholtz<T>(p.N, p.k, xc, xs, qr, qi, emit, leg);
+            p2m_helmholtz<T>(p.N, p.k, xc, xs, qr, qi, emit, leg, sc);
           }
           if (p.dip) {
             T dr = act ? p.dip[2 * s] : T(0), di = act ? p.dip[2 * s + 1] : T(0);
             T nrm[3] = {act ? p.nx[s] : T(0), act ? p.ny[s] : T(0),
                         act ? p.nz[s] : T(1)};
-            p2m_helmholtz_dipole<T>(p.N, p.k, xc, xs, nrm, dr, di, emit, leg);
+            p2m_helmholtz_dipole<T>(p.N, p.k, xc, xs, nrm, dr, di, emit, leg, sc);
           }
         } else {
           auto emit = [&](int idx, T v) {
@@ -108,13 +129,13 @@ __global__ void k_p2m(P2MParams<T> p, int legt) {
           };
           if (p.q) {
             T qv = act ? p.q[s] : T(0);
-            p2m_laplace<T>(p.N, xc, xs, qv, emit, leg);
+            p2m_laplace<T>(p.N, xc, xs, qv, emit, leg, sc);
           }
           if (p.dip) {
             T dv = act ? p.dip[s] : T(0);
             T nrm[3] = {act ? p.nx[s] : T(0), act ? p.ny[s] : T(0),
                         act ? p.nz[s] : T(1)};
-            p2m_laplace_dipole<T>(p.N, xc, xs, nrm, dv, emit, leg);
+            p2m_laplace_dipole<T>(p.N, xc, xs, nrm, dv, emit, leg, sc);
           }
         }
       };
@@ -144,11 +165,17 @@ int launch_p2m(const P2MParams<T>& p, cudaStream_t s) {
   if (p.nbox <= 0) return 0;
   const int nw = 4;
   const size_t leg = leg_table_bytes<T>(p.N);
-  size_t smem = leg + sizeof(T) * (size_t)nw * ncoef(p.N) * (HELM ? 2 : 1);
-  if (smem > 48 * 1024)
-    WBFMM_SMEM(smem, k_p2m<T, HELM>);
+  const size_t rows = p2m_row_bytes<T>(p.N, nw * 32);
+  const bool srows = rows <= kRowSmemMax;
+  size_t smem = leg + (srows ? rows : 0) + sizeof(T) * (size_t)nw * ncoef(p.N) * (HELM ? 2 : 1);
   unsigned grid = (unsigned)((p.nbox + nw - 1) / nw);
-  k_p2m<T, HELM><<<grid, nw * 32, smem, s>>>(p, leg ? 1 : 0);
+  if (srows) {
+    if (smem > 48 * 1024) WBFMM_SMEM(smem, k_p2m<T, HELM, true>);
+    k_p2m<T, HELM, true><<<grid, nw * 32, smem, s>>>(p, leg ? 1 : 0);
+  } else {
+    if (smem > 48 * 1024) WBFMM_SMEM(smem, k_p2m<T, HELM, false>);
+    k_p2m<T, HELM, false><<<grid, nw * 32, smem, s>>>(p, leg ? 1 : 0);
+  }
   WBFMM_CUDA(cudaGetLastError());
   return 0;
 }
@@ -532,7 +559,9 @@ __host__ __device__ inline size_t l2p_table_bytes(int N) {
 }
 
 // one thread per target (sorted by box); potential and gradient in one sweep
-template <typename T, bool HELM>
+// SROWS: recursion rows in shared memory, after the tables (else
+// per-thread local arrays)
+template <typename T, bool HELM, bool SROWS>
 __global__ void k_l2p(EvalParams<T> p, int tab, int legt) {
   extern __shared__ __align__(16) unsigned char l2p_sm[];
   T* st = (T*)l2p_sm;
@@ -541,6 +570,10 @@ __global__ void k_l2p(EvalParams<T> p, int tab, int legt) {
   // Legendre constants (degrees <= N + 2) after the recursion tables
   const int LW = N + 3;
   T* lt = st + (tab ? l2p_table_bytes<T, HELM>(N) / sizeof(T) : 0);
+  T* rows = lt + (legt ? 4 * LW * LW : 0);
+  T loc[SROWS ? 1 : 3 * kPtMax];
+  const Scratch<T> sc = SROWS ? Scratch<T>{rows + threadIdx.x, N + kRowPad, (int)blockDim.x}
+                              : Scratch<T>{loc, N + kRowPad, 1};
   if (legt) leg_table_fill(lt, N + 2, threadIdx.x, blockDim.x);
   if (tab) {
     if (HELM) {
@@ -584,15 +617,15 @@ __global__ void k_l2p(EvalParams<T> p, int tab, int legt) {
         T* fp = p.pot ? f : nullptr;
         if (tab) {
           RecTab<T> rt{st, st + (N + 3) * W, W, M0};
-          l2p_helmholtz_grad<T>(N, p.k, xc, xf, coef, g, fp, rt, leg);
+          l2p_helmholtz_grad<T>(N, p.k, xc, xf, coef, g, fp, rt, leg, sc);
         } else {
-          l2p_helmholtz_grad<T>(N, p.k, xc, xf, coef, g, fp, RecDirect<T>(), leg);
+          l2p_helmholtz_grad<T>(N, p.k, xc, xf, coef, g, fp, RecDirect<T>(), leg, sc);
         }
         for (int c = 0; c < 6; c++) p.grad[6 * (size_t)o + c] = g[c];
         if (p.pot) { p.pot[2 * (size_t)o] = f[0]; p.pot[2 * (size_t)o + 1] = f[1]; }
       } else if (p.pot) {
         T fr = T(0), fi = T(0);
-        l2p_helmholtz<T>(N, p.k, xc, xf, coef, &fr, &fi, leg);
+        l2p_helmholtz<T>(N, p.k, xc, xf, coef, &fr, &fi, leg, sc);
         p.pot[2 * (size_t)o] = fr; p.pot[2 * (size_t)o + 1] = fi;
       }
     };
@@ -605,14 +638,14 @@ __global__ void k_l2p(EvalParams<T> p, int tab, int legt) {
         T* fp = p.pot ? &f : nullptr;
         if (tab) {
           LapRecTab<T> rt{st, N + 1};
-          l2p_laplace_grad<T>(N, xc, xf, coef, g, fp, rt, leg);
+          l2p_laplace_grad<T>(N, xc, xf, coef, g, fp, rt, leg, sc);
         } else {
-          l2p_laplace_grad<T>(N, xc, xf, coef, g, fp, LapRecDirect<T>(), leg);
+          l2p_laplace_grad<T>(N, xc, xf, coef, g, fp, LapRecDirect<T>(), leg, sc);
         }
         for (int c = 0; c < 3; c++) p.grad[3 * (size_t)o + c] = g[c];
         if (p.pot) p.pot[o] = f;
       } else if (p.pot) {
-        p.pot[o] = l2p_laplace<T>(N, xc, xf, coef, leg);
+        p.pot[o] = l2p_laplace<T>(N, xc, xf, coef, leg, sc);
       }
     };
     if (legt) eval(LegTab<T>{lt, LW}); else eval(LegDirect<T>());
@@ -624,9 +657,17 @@ int launch_l2p(const EvalParams<T>& p, cudaStream_t s) {
   if (p.ntgt <= 0) return 0;
   const size_t sm = l2p_table_bytes<T, HELM>(p.N);
   const size_t lg = leg_table_bytes<T>(p.N);
-  if (sm + lg > 48 * 1024)
-    WBFMM_SMEM((sm + lg), k_l2p<T, HELM>);
-  k_l2p<T, HELM><<<(p.ntgt + 127) / 128, 128, sm + lg, s>>>(p, sm ? 1 : 0, lg ? 1 : 0);
+  const size_t rows = l2p_row_bytes<T>(p.N, HELM, p.grad != nullptr, 128);
+  const unsigned grid = (unsigned)((p.ntgt + 127) / 128);
+  if (rows <= kRowSmemMax) {
+    if (sm + lg + rows > 48 * 1024)
+      WBFMM_SMEM((sm + lg + rows), k_l2p<T, HELM, true>);
+    k_l2p<T, HELM, true><<<grid, 128, sm + lg + rows, s>>>(p, sm ? 1 : 0, lg ? 1 : 0);
+  } else {
+    if (sm + lg > 48 * 1024)
+      WBFMM_SMEM((sm + lg), k_l2p<T, HELM, false>);
+    k_l2p<T, HELM, false><<<grid, 128, sm + lg, s>>>(p, sm ? 1 : 0, lg ? 1 : 0);
+  }
   WBFMM_CUDA(cudaGetLastError());
   return 0;
 }
