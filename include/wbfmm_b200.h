@@ -152,6 +152,25 @@ int wbfmm_b200_set_deferred_checks(wbfmm_b200_solver_t *s, int on);
 int wbfmm_b200_laplace_curl(wbfmm_b200_solver_t *s, const double *q3, int qstr,
                             double *curl, int on_device);
 
+/* Second derivatives of the Laplace potential at the solver's targets,
+   after a run (or the downward passes): hess[9 j + 3 a + b] = d_a d_b phi
+   at target j (original order), from the leaf regular expansions (the
+   coefficients of d/dx, d/dy, d/dz of each leaf expansion, evaluated with
+   the gradient L2P) and, with neighbours != 0, the monopoles of the 27
+   neighbour boxes (dipole sources: WBFMM_B200_E_ARG).  The second
+   derivatives behind the reference's curl gradient
+   (src/local-laplace.c:752-1010, :147-197).  Blocks until written. */
+int wbfmm_b200_laplace_hessian(wbfmm_b200_solver_t *s, double *hess,
+                               int neighbours, int on_device);
+
+/* The curl of a vector potential and its gradient (the reference's
+   WBFMM_FIELD_CURL | WBFMM_FIELD_GRADIENT for three source components,
+   src/local-laplace.c:1229-1291): out[12 j + i] = curl_i, then
+   out[12 j + 3 + 3 a + i] = d_a curl_i at target j; q3 as for
+   wbfmm_b200_laplace_curl.  Blocks until written. */
+int wbfmm_b200_laplace_curl_gradient(wbfmm_b200_solver_t *s, const double *q3,
+                                     int qstr, double *out, int on_device);
+
 /* Self-test of the FP32 near-field sine and cosine: the largest absolute
    error of the engine's own routine (err2[0]) and of CUDA's sincosf
    (err2[1]) against FP64 sin/cos at the FP32 arguments i * xmax / n,

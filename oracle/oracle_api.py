@@ -275,6 +275,22 @@ class Reference:
         return out
 
 
+    def direct_curl_gradient(self, xs, q3, xt):
+        """The reference's direct Laplace curl and curl gradient
+        (WBFMM_FIELD_CURL | WBFMM_FIELD_GRADIENT, nq = 3,
+        src/direct-laplace.c:132-198, 274-340): [nt, 12], the curl then
+        d/dx, d/dy, d/dz of its three components, one target at a time."""
+        xs = _f64(xs).reshape(-1, 3); q3 = _f64(q3).reshape(-1, 3)
+        xt = _f64(xt).reshape(-1, 3)
+        out = np.zeros((xt.shape[0], 12))
+        for j in range(xt.shape[0]):
+            xf = np.ascontiguousarray(xt[j]); f = np.zeros(12)
+            self.lib.wbfmm_laplace_field_direct(_ptr(xs), 3, None, 0, xs.shape[0], _ptr(q3), 3,
+                                                None, 0, 3, 4 | 2, _ptr(xf), _ptr(f), 12)
+            out[j] = f
+        return out
+
+
 def curl_from_gradients(g):
     """curl_i = e_ijk d_j A_k from the gradients g[k] ([nt, 3]) of the three
     components of a vector potential."""

@@ -492,6 +492,62 @@ def test_laplace_curl(gpu_lib, precision):
     assert rel_l2(curl.ravel(), ref.ravel()) < tol, rel_l2(curl.ravel(), ref.ravel())
 
 
+def _direct_hessian(xs, q, xt, chunk=256):
+    """d_a d_b of sum q / (4 pi r) at xt (self terms r <= 1e-6 excluded)."""
+    out = np.zeros((xt.shape[0], 3, 3))
+    for i in range(0, xt.shape[0], chunk):
+        d = xt[i:i + chunk, None, :] - xs[None, :, :]
+        r2 = np.einsum("tsk,tsk->ts", d, d)
+        ok = r2 > 1e-12
+        r2 = np.where(ok, r2, 1.0)
+        r = np.sqrt(r2)
+        w3 = np.where(ok, q[None, :] / (4 * np.pi * r2 * r), 0.0)
+        w5 = 3.0 * w3 / r2
+        out[i:i + chunk] = (np.einsum("ts,tsa,tsb->tab", w5, d, d)
+                            - np.einsum("ts->t", w3)[:, None, None] * np.eye(3))
+    return out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [engine.FP64, engine.FP32])
+def test_laplace_hessian(gpu_lib, precision):
+    """Second derivatives of the Laplace potential (derived local
+    expansions through the gradient L2P, plus the near-field monopoles)
+    against a direct sum; symmetric as computed."""
+    p = W.laplace_cube(20000, 1500, depth=4, order=12, seed=64)
+    with engine.Solver(engine.SolverConfig.from_problem(p, precision)) as s:
+        s.set_sources(p.xs).set_strengths(p.q).set_targets(p.xt).run()
+        h = s.hessian()
+        hfar = s.hessian(neighbours=False)
+    ref = _direct_hessian(p.xs, p.q, p.xt)
+    tol = 2e-5 if precision == engine.FP64 else 5e-5
+    assert rel_l2(h.ravel(), ref.ravel()) < tol, rel_l2(h.ravel(), ref.ravel())
+    assert np.abs(h - h.transpose(0, 2, 1)).max() <= 1e-6 * np.abs(h).max()
+    # the far field alone is harmonic: the trace of its Hessian vanishes
+    tr = np.trace(hfar, axis1=1, axis2=2)
+    assert np.abs(tr).max() <= 1e-6 * np.abs(hfar).max()
+
+
+@pytest.mark.gpu
+def test_laplace_curl_gradient(gpu_lib):
+    """The curl of a vector potential and its gradient (three source
+    components) against the reference's own direct curl gradient
+    (WBFMM_FIELD_CURL | WBFMM_FIELD_GRADIENT)."""
+    from oracle.oracle_api import Reference, have_reference
+    if not have_reference():
+        pytest.skip("reference library not built")
+    p = W.laplace_cube(20000, 600, depth=4, order=12, seed=65)
+    q3 = np.random.default_rng(66).standard_normal((p.ns, 3))
+    with engine.Solver(engine.SolverConfig.from_problem(p, engine.FP64)) as s:
+        s.set_sources(p.xs).set_targets(p.xt)
+        cg = s.laplace_curl_gradient(q3)
+        curl = s.laplace_curl(q3)
+    ref = Reference().direct_curl_gradient(p.xs, q3, p.xt)
+    assert np.allclose(cg[:, :3], curl, rtol=0, atol=1e-12 * np.abs(curl).max())
+    assert rel_l2(cg[:, :3].ravel(), ref[:, :3].ravel()) < 2e-6
+    assert rel_l2(cg[:, 3:].ravel(), ref[:, 3:].ravel()) < 2e-5, rel_l2(cg[:, 3:].ravel(), ref[:, 3:].ravel())
+
+
 def _edge_problem(case):
     rng = np.random.default_rng(71)
     if case == "coincident":

@@ -181,6 +181,69 @@ def test_curl_convention_matches_reference(restatement, reference):
     assert np.linalg.norm(mine - ref) <= 1e-12 * np.linalg.norm(ref)
 
 
+def test_curl_gradient_convention_matches_reference(reference):
+    """The reference's direct curl gradient (WBFMM_FIELD_CURL |
+    WBFMM_FIELD_GRADIENT): the curl, then d/dx, d/dy, d/dz of its three
+    components, formed here from the second derivatives of 1/(4 pi r) as the
+    engine combines them (curl_i = e_ijk d_j A_k; entry 3 + 3 a + i is
+    d_a curl_i)."""
+    rng = np.random.default_rng(67)
+    xs = rng.uniform(-0.5, 0.5, (200, 3))
+    xt = rng.uniform(-0.5, 0.5, (30, 3))
+    q3 = rng.standard_normal((200, 3))
+    d = xt[:, None, :] - xs[None, :, :]
+    r = np.linalg.norm(d, axis=2)
+    g = -d / (4 * np.pi * r[..., None] ** 3)                       # d_j (1/4 pi r)
+    H = (3 * d[..., :, None] * d[..., None, :] / r[..., None, None] ** 2
+         - np.eye(3)) / (4 * np.pi * r[..., None, None] ** 3)     # d_a d_j (1/4 pi r)
+    G = np.einsum("tsj,sc->tcj", g, q3)                            # d_j A_c
+    HH = np.einsum("tsaj,sc->tcaj", H, q3)                         # d_a d_j A_c
+    curl = np.stack([G[:, 2, 1] - G[:, 1, 2], G[:, 0, 2] - G[:, 2, 0],
+                     G[:, 1, 0] - G[:, 0, 1]], axis=1)
+    dcurl = np.stack([HH[:, 2, :, 1] - HH[:, 1, :, 2], HH[:, 0, :, 2] - HH[:, 2, :, 0],
+                      HH[:, 1, :, 0] - HH[:, 0, :, 1]], axis=2)    # [t, a, i]
+    mine = np.hstack([curl, dcurl.reshape(-1, 9)])
+    ref = reference.direct_curl_gradient(xs, q3, xt)
+    assert np.linalg.norm(mine - ref) <= 1e-12 * np.linalg.norm(ref)
+
+
+def test_reference_local_curl_gradient_is_inexact(reference):
+    """The reference's evaluation of the curl gradient from a local
+    expansion (wbfmm_laplace_expansion_local_eval, WBFMM_FIELD_CURL |
+    WBFMM_FIELD_GRADIENT, src/local-laplace.c:752-1010) is not the derivative
+    of its curl evaluation (WBFMM_FIELD_CURL, :632-750): central differences
+    of the curl differ from it by far more than their own error on random
+    order-10 coefficients.  The engine evaluates the exact derivative
+    (derived expansions through the gradient L2P), so curl-gradient parity is
+    measured against the reference's direct sums."""
+    import ctypes as C
+    f = reference.lib.wbfmm_laplace_expansion_local_eval
+    f.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_uint, C.c_void_p,
+                  C.c_void_p, C.c_int, C.c_void_p]
+    ptr = lambda a: a.ctypes.data_as(C.c_void_p)
+    N, nq = 10, 3
+    rng = np.random.default_rng(5)
+    cf = rng.standard_normal((N + 1) ** 2 * nq)
+    x0, work = np.zeros(3), np.zeros(100000)
+
+    def ev(field, x, nout):
+        out, xf = np.zeros(nout), np.array(x, dtype=float)
+        f(ptr(x0), ptr(cf), nq, N, nq, field, ptr(xf), ptr(out), 1, ptr(work))
+        return out
+    worst = 0.0
+    for _ in range(5):
+        x = rng.uniform(-0.3, 0.3, 3)
+        cg = ev(4 | 2, x, 12)
+        assert np.array_equal(cg[:3], ev(4, x, 3))
+        for a in range(3):
+            e = 1e-5
+            xp, xm = x.copy(), x.copy()
+            xp[a] += e; xm[a] -= e
+            fd = (ev(4, xp, 3) - ev(4, xm, 3)) / (2 * e)
+            worst = max(worst, np.abs(fd - cg[3 + 3 * a:6 + 3 * a]).max() / np.abs(cg[3:]).max())
+    assert worst > 1e-5, worst
+
+
 DIRECT_CASES = ("helm_mono", "helm_mixed", "lap_mono", "lap_dipole", "lap_mixed")
 
 

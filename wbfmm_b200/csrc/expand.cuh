@@ -426,7 +426,10 @@ template <typename T, class Coef, class LRec = LapRecDirect<T>, class Leg = LegD
 HD void l2p_laplace_grad(int N, const T* xc, const T* xf, Coef&& coef, T* g,
                          T* pot, const LRec& rec, const Leg& leg,
                          const Scratch<T>& sc) {
-  if (N == 0) return;
+  if (N == 0) {   // a constant: no gradient
+    if (pot) *pot += coef(0) * (T(1) / (T)sqrt(4.0 * kPi));
+    return;
+  }
   T r, th, ph;
   cart2sph(xc, xf, &r, &th, &ph);
   T C = cos(th), S = sin(th);

@@ -126,6 +126,21 @@ template <typename T, bool HELM>
 int launch_l2p(const EvalParams<T>& p, cudaStream_t s);
 template <typename T, bool HELM>
 int launch_p2p(const EvalParams<T>& p, cudaStream_t s);
+// Laplace second derivatives (hessian.cu): the coefficients of d/dx, d/dy,
+// d/dz (degree N - 1) of each box's regular expansion L (degree N >= 1);
+// hess[9 t + 3 a + b] = g[a][3 t + b] (g null: zeros); the near-field
+// second derivatives of the monopoles of the 27 neighbour boxes added into
+// hess; out[12 t] = curl and its gradient from the components' gradients
+// g[3][3 nt] and Hessians h[3][9 nt]
+template <typename T>
+int launch_laplace_deriv(const T* L, int N, int64_t nbox, T* Dx, T* Dy, T* Dz,
+                         cudaStream_t s);
+template <typename T>
+int launch_hess_gather(const T* g, int nt, double* hess, cudaStream_t s);
+template <typename T>
+int launch_p2p_hessian(const EvalParams<T>& p, double* hess, cudaStream_t s);
+int launch_curl_gradient_combine(const double* g, const double* h, int nt, double* out,
+                                 cudaStream_t s);
 // self-test of the FP32 near-field sine/cosine (kernels.cu)
 int sincos_near_errors(double xmax, int n, double* host_err);
 

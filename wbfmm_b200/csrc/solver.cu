@@ -181,6 +181,71 @@ int wbfmm_b200_run(wbfmm_b200_solver_t* s) { SOLVER_CALL(s->run()); }
 int wbfmm_b200_run_async(wbfmm_b200_solver_t* s) { SOLVER_CALL(s->run_queued()); }
 int wbfmm_b200_run_graph(wbfmm_b200_solver_t* s) { SOLVER_CALL(s->run_graph()); }
 int wbfmm_b200_wait(wbfmm_b200_solver_t* s) { SOLVER_CALL(s->wait()); }
+int wbfmm_b200_laplace_hessian(wbfmm_b200_solver_t* s, double* hess, int neighbours,
+                               int on_device) {
+  if (!s || !hess) return set_error(WBFMM_B200_E_ARG, "bad Hessian arguments");
+  const int nt = s->targets();
+  if (nt <= 0) return set_error(WBFMM_B200_E_STATE, "set_targets first");
+  cudaStream_t st = s->stream;
+  double* hd = hess;
+  int rc = 0;
+  cudaError_t e = cudaSuccess;
+  if (!on_device) e = cudaMallocAsync(&hd, sizeof(double) * 9 * (size_t)nt, st);
+  if (e != cudaSuccess) return set_cuda_error(e, __FILE__, __LINE__);
+  rc = s->hessian(hd, neighbours);
+  if (!rc && !on_device) {
+    e = cudaMemcpyAsync(hess, hd, sizeof(double) * 9 * (size_t)nt, cudaMemcpyDeviceToHost, st);
+    if (e != cudaSuccess) rc = set_cuda_error(e, __FILE__, __LINE__);
+  }
+  if (!on_device) cudaFreeAsync(hd, st);
+  e = cudaStreamSynchronize(st);
+  if (!rc && e != cudaSuccess) rc = set_cuda_error(e, __FILE__, __LINE__);
+  return rc;
+}
+
+int wbfmm_b200_laplace_curl_gradient(wbfmm_b200_solver_t* s, const double* q3, int qstr,
+                                     double* out, int on_device) {
+  if (!s || !q3 || !out || qstr < 3) return set_error(WBFMM_B200_E_ARG, "bad curl arguments");
+  if (s->cfg.problem != WBFMM_B200_LAPLACE)
+    return set_error(WBFMM_B200_E_ARG, "the curl needs a Laplace solver");
+  if (!(s->cfg.field & WBFMM_B200_GRADIENT))
+    return set_error(WBFMM_B200_E_ARG, "the curl needs the gradient field");
+  const int ns = s->sources(), nt = s->targets();
+  if (ns <= 0 || nt <= 0) return set_error(WBFMM_B200_E_STATE, "sources and targets must be set");
+  cudaStream_t st = s->stream;
+  double *g = nullptr, *h = nullptr, *qd = nullptr, *od = nullptr;
+  int rc = 0;
+  cudaError_t e = cudaMallocAsync(&g, sizeof(double) * 9 * (size_t)nt, st);
+  if (e == cudaSuccess) e = cudaMallocAsync(&h, sizeof(double) * 27 * (size_t)nt, st);
+  const double* q = q3;
+  if (e == cudaSuccess && !on_device) {
+    e = cudaMallocAsync(&qd, sizeof(double) * (size_t)ns * qstr, st);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(qd, q3, sizeof(double) * (size_t)ns * qstr, cudaMemcpyHostToDevice, st);
+    q = qd;
+  }
+  if (e == cudaSuccess && !on_device) e = cudaMallocAsync(&od, sizeof(double) * 12 * (size_t)nt, st);
+  if (e != cudaSuccess) rc = set_cuda_error(e, __FILE__, __LINE__);
+  for (int c = 0; c < 3 && !rc; c++) {
+    rc = s->set_strengths(q + c, qstr, nullptr, 0, 1);
+    if (!rc) rc = s->run();
+    if (!rc) rc = s->get_field(nullptr, g + (size_t)c * 3 * nt, 1);
+    if (!rc) rc = s->hessian(h + (size_t)c * 9 * nt, 1);
+  }
+  if (!rc) rc = launch_curl_gradient_combine(g, h, nt, on_device ? out : od, st);
+  if (!rc && !on_device) {
+    e = cudaMemcpyAsync(out, od, sizeof(double) * 12 * (size_t)nt, cudaMemcpyDeviceToHost, st);
+    if (e != cudaSuccess) rc = set_cuda_error(e, __FILE__, __LINE__);
+  }
+  if (g) cudaFreeAsync(g, st);
+  if (h) cudaFreeAsync(h, st);
+  if (qd) cudaFreeAsync(qd, st);
+  if (od) cudaFreeAsync(od, st);
+  e = cudaStreamSynchronize(st);
+  if (!rc && e != cudaSuccess) rc = set_cuda_error(e, __FILE__, __LINE__);
+  return rc;
+}
+
 int wbfmm_b200_laplace_curl(wbfmm_b200_solver_t* s, const double* q3, int qstr,
                             double* curl, int on_device) {
   if (!s || !q3 || !curl || qstr < 3) return set_error(WBFMM_B200_E_ARG, "bad curl arguments");

@@ -171,6 +171,7 @@ struct wbfmm_b200_solver {
   virtual int wait() = 0;
   virtual int set_deferred_checks(int on) = 0;
   virtual int get_field(double*, double*, int) = 0;
+  virtual int hessian(double* hess, int neighbours) = 0;
   virtual int sources() const = 0;
   virtual int targets() const = 0;
   virtual int get_tree(uint32_t*, uint32_t*, uint32_t*, int) = 0;
@@ -221,6 +222,7 @@ struct Solver : public wbfmm_b200_solver {
   DBuf<int> flag;
   // outputs (original order)
   DBuf<T> pot, grad;
+  DBuf<T> hess_d, hess_g;           // Hessian: derived expansions, gradients
   DBuf<double> out64;
   // tables
   bool ops_ready = false;
@@ -282,7 +284,7 @@ struct Solver : public wbfmm_b200_solver {
     }
     f(coax_set64); f(coax_set);
     f(tpts_in); f(tx); f(ty); f(tz); f(tkeys); f(tperm); f(tbox);
-    f(tstart); f(tcount); f(flag); f(pot); f(grad); f(out64);
+    f(tstart); f(tcount); f(flag); f(pot); f(grad); f(out64); f(hess_d); f(hess_g);
     f(H64); f(H); f(op_ith); f(op_dist); f(op_r); f(op_ph); f(op_ch);
     for (int i = 0; i < 3; i++) { f(lap64[i]); f(lap[i]); }
     f(partial); f(lin); f(lanes_part); f(act_scr); f(lapsr); f(hcx); f(smask); f(tc_part);
@@ -1142,6 +1144,44 @@ struct Solver : public wbfmm_b200_solver {
                                on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
                                stream));
     WBFMM_CUDA(cudaStreamSynchronize(stream));
+    return 0;
+  }
+
+  // Laplace: second derivatives of the potential at the targets into the
+  // device array hess[9 ntgt] (original order, d_a d_b at 3 a + b), from
+  // the leaf regular expansions (after the downward pass) and, with
+  // neighbours, the monopoles of the 27 neighbour boxes
+  int hessian(double* hess, int neighbours) override {
+    if (helm) return set_error(WBFMM_B200_E_ARG, "the Hessian is for Laplace solvers");
+    if (nsrc <= 0 || ntgt <= 0) return set_error(WBFMM_B200_E_STATE, "sources and targets must be set");
+    if (neighbours && have_dip)
+      return set_error(WBFMM_B200_E_ARG, "the near-field Hessian takes monopole sources only");
+    const int N = cfg.order_r[depth];
+    const int64_t nb = (int64_t)1 << (3 * depth);
+    if (N >= 1) {
+      const size_t len = level_len(depth, N - 1);
+      WBFMM_TRY(hess_d.alloc(3 * len));
+      WBFMM_TRY(hess_g.alloc(9 * (size_t)ntgt));
+      WBFMM_TRY(launch_laplace_deriv<T>(mpr[depth].p, N, nb, hess_d.p, hess_d.p + len,
+                                        hess_d.p + 2 * len, stream));
+      for (int a = 0; a < 3; a++) {
+        EvalParams<T> e = eparams();
+        e.N = N - 1;
+        e.mpr = hess_d.p + a * len;
+        e.pot = nullptr;
+        e.grad = hess_g.p + (size_t)a * 3 * ntgt;
+        WBFMM_TRY((launch_l2p<T, false>(e, stream)));
+      }
+      WBFMM_TRY(launch_hess_gather<T>(hess_g.p, ntgt, hess, stream));
+      launches += 5;
+    } else {
+      WBFMM_TRY(launch_hess_gather<T>(nullptr, ntgt, hess, stream));
+      launches++;
+    }
+    if (neighbours && have_q) {
+      WBFMM_TRY(launch_p2p_hessian<T>(eparams(), hess, stream));
+      launches++;
+    }
     return 0;
   }
 

@@ -28,6 +28,8 @@ static void check(const char *fn, int rc) {
   if (rc != 0) die(fn, wbfmm_b200_last_error());
 }
 
+#define DT_MAX_NQ 16             /* source components of one tree */
+
 /* the tree as callers see it, followed by the engine state behind it */
 typedef struct {
   wbfmm_tree_t t;
@@ -41,13 +43,28 @@ typedef struct {
   gboolean managed[2][WBFMM_TREE_MAX_DEPTH + 1];
   int fp32;                      /* a tree of the single-precision API (*_f) */
   double *pts64, *nrm64;         /* FP64 copies of FP32 points and normals */
+  /* Laplace sources of nq > 1 components: one engine solver per component
+     (s for component 0, sc[c] for the others), each on its own coefficient
+     arrays cms/cmr (engine layout), copied into the tree's interleaved
+     arrays (src/laplace.c:795-852) after every pass */
+  int nq;
+  wbfmm_b200_solver_t *sc[DT_MAX_NQ];
+  void *cms[DT_MAX_NQ][WBFMM_TREE_MAX_DEPTH + 1], *cmr[DT_MAX_NQ][WBFMM_TREE_MAX_DEPTH + 1];
 } dtree_t;
 
 #define DT(_t) ((dtree_t *)(_t))
 
+static int ncomp(const dtree_t *d) { return d->nq > 1 ? d->nq : 1; }
+static wbfmm_b200_solver_t *comp_solver(dtree_t *d, int c) { return c ? d->sc[c] : d->s; }
+
 static void drop_solver(dtree_t *d) {
+  int c;
   if (d->s) wbfmm_b200_solver_destroy(d->s);
   d->s = NULL;
+  for (c = 1; c < DT_MAX_NQ; c++) {
+    if (d->sc[c]) wbfmm_b200_solver_destroy(d->sc[c]);
+    d->sc[c] = NULL;
+  }
   d->ready = 0;
   d->q = d->dip = NULL;
   d->targets = NULL;
@@ -198,35 +215,78 @@ gint wbfmm_tree_refine(wbfmm_tree_t *t) {
   return 0;
 }
 
+static void *managed_or_die(size_t bytes) {
+  void *p = wbfmm_b200_managed_alloc(bytes);
+  if (!p) die("wbfmm_tree_coefficient_init", wbfmm_b200_last_error());
+  return p;
+}
+
+static void free_components(dtree_t *d, guint l) {
+  int c;
+  for (c = 0; c < DT_MAX_NQ; c++) {
+    if (d->cms[c][l]) wbfmm_b200_managed_free(d->cms[c][l]);
+    if (d->cmr[c][l]) wbfmm_b200_managed_free(d->cmr[c][l]);
+    d->cms[c][l] = d->cmr[c][l] = NULL;
+  }
+}
+
+/* box b's coefficients start at ((b & ~7) nc + (b & 7)) nq, coefficient c
+   of component q at +8 nq c + q (w values each) */
 static void coefficient_init(wbfmm_tree_t *t, guint l, guint nr, guint ns,
                              int w) {
   dtree_t *d = DT(t);
   size_t nb = (size_t)1 << (3 * l), b, nc;
-  gint nq = wbfmm_tree_source_size(t);
-  if (nq != 1) die("wbfmm_tree_coefficient_init", "only single-component sources (nq = 1) are supported");
+  gint nq = wbfmm_tree_source_size(t), c;
+  if (nq < 1) die("wbfmm_tree_coefficient_init", "tree has invalid number of components in source terms");
+  if (nq > 1 && w != 1) die("wbfmm_tree_coefficient_init", "multi-component sources (nq > 1) are supported for Laplace trees");
+  if (nq > DT_MAX_NQ) die("wbfmm_tree_coefficient_init", "too many source components (at most 16)");
   if (l > t->depth) die("wbfmm_tree_coefficient_init", "level deeper than the tree");
   drop_solver(d);
+  d->nq = nq;
   t->order_s[l] = ns;
   t->order_r[l] = nr;
   if (d->managed[0][l]) wbfmm_b200_managed_free(t->mps[l]);
   if (d->managed[1][l]) wbfmm_b200_managed_free(t->mpr[l]);
+  free_components(d, l);
   t->mps[l] = t->mpr[l] = NULL;
   d->managed[0][l] = d->managed[1][l] = FALSE;
   if (ns) {
     nc = (size_t)(ns + 1) * (ns + 1);
-    t->mps[l] = wbfmm_b200_managed_alloc(nb * nc * w * t->size);
-    if (!t->mps[l]) die("wbfmm_tree_coefficient_init", wbfmm_b200_last_error());
+    t->mps[l] = managed_or_die(nb * nc * w * nq * t->size);
     d->managed[0][l] = TRUE;
     for (b = 0; b < nb; b++)
-      t->boxes[l][b].mps = (char *)t->mps[l] + ((b & ~7) * nc + (b & 7)) * w * t->size;
+      t->boxes[l][b].mps = (char *)t->mps[l] + ((b & ~7) * nc + (b & 7)) * nq * w * t->size;
+    if (nq > 1)
+      for (c = 0; c < nq; c++) d->cms[c][l] = managed_or_die(nb * nc * t->size);
   }
   if (nr) {
     nc = (size_t)(nr + 1) * (nr + 1);
-    t->mpr[l] = wbfmm_b200_managed_alloc(nb * nc * w * t->size);
-    if (!t->mpr[l]) die("wbfmm_tree_coefficient_init", wbfmm_b200_last_error());
+    t->mpr[l] = managed_or_die(nb * nc * w * nq * t->size);
     d->managed[1][l] = TRUE;
     for (b = 0; b < nb; b++)
-      t->boxes[l][b].mpr = (char *)t->mpr[l] + ((b & ~7) * nc + (b & 7)) * w * t->size;
+      t->boxes[l][b].mpr = (char *)t->mpr[l] + ((b & ~7) * nc + (b & 7)) * nq * w * t->size;
+    if (nq > 1)
+      for (c = 0; c < nq; c++) d->cmr[c][l] = managed_or_die(nb * nc * t->size);
+  }
+}
+
+/* nq > 1: the components' level-l arrays into the tree's interleaved one */
+static void interleave(wbfmm_tree_t *t, guint l, int singular) {
+  dtree_t *d = DT(t);
+  const int nq = d->nq;
+  const guint p = singular ? t->order_s[l] : t->order_r[l];
+  const size_t nb = (size_t)1 << (3 * l), nc = (size_t)(p + 1) * (p + 1), es = t->size;
+  char *dst = (char *)(singular ? t->mps[l] : t->mpr[l]);
+  size_t g, i, j;
+  int q;
+  if (nq <= 1 || !dst) return;
+  for (q = 0; q < nq; q++) {
+    const char *src = (const char *)(singular ? d->cms[q][l] : d->cmr[q][l]);
+    for (g = 0; g < nb / 8 + (nb < 8); g++)
+      for (i = 0; i < nc; i++)
+        for (j = 0; j < 8 && g * 8 + j < nb; j++)
+          memcpy(dst + ((g * 8 * nc + i * 8 + j) * nq + q) * es,
+                 src + ((g * nc + i) * 8 + j) * es, es);
   }
 }
 
@@ -246,22 +306,34 @@ gint wbfmm_tree_laplace_coefficient_init(wbfmm_tree_t *t, guint l, guint nr,
 }
 
 /* bytes of a level's coefficient array of order p */
+/* bytes of one component's level array of order p */
 static size_t level_bytes(wbfmm_tree_t *t, guint l, guint p) {
   return ((size_t)1 << (3 * l)) * (size_t)(p + 1) * (p + 1) *
          (t->problem == WBFMM_PROBLEM_HELMHOLTZ ? 2 : 1) * t->size;
 }
 
+/* zero the singular (or regular) expansions of level l, every component */
+static void zero_level(wbfmm_tree_t *t, guint l, int singular) {
+  dtree_t *d = DT(t);
+  const guint p = singular ? t->order_s[l] : t->order_r[l];
+  void *a = singular ? t->mps[l] : t->mpr[l];
+  int c;
+  if (!a) return;
+  memset(a, 0, level_bytes(t, l, p) * ncomp(d));
+  if (d->nq > 1)
+    for (c = 0; c < d->nq; c++) memset(singular ? d->cms[c][l] : d->cmr[c][l], 0, level_bytes(t, l, p));
+}
+
 /* src/boxes.c:636-673 */
 gint wbfmm_tree_coefficient_clear(wbfmm_tree_t *t, guint l) {
-  if (t->mps[l]) memset(t->mps[l], 0, level_bytes(t, l, t->order_s[l]));
-  if (t->mpr[l]) memset(t->mpr[l], 0, level_bytes(t, l, t->order_r[l]));
+  zero_level(t, l, 1);
+  zero_level(t, l, 0);
   return 0;
 }
 
 /* src/tree.c:137-153 */
 gint wbfmm_tree_coefficients_zero(wbfmm_tree_t *t, guint level) {
-  if (t->mpr[level])
-    memset(t->mpr[level], 0, level_bytes(t, level, t->order_r[level]));
+  zero_level(t, level, 0);
   return 0;
 }
 
@@ -501,6 +573,7 @@ static wbfmm_b200_solver_t *solver_for(wbfmm_tree_t *t, double k,
   dtree_t *d = DT(t);
   wbfmm_b200_config_t c;
   guint l;
+  int q;
   if (d->s && d->ready && (t->problem == WBFMM_PROBLEM_LAPLACE || d->k == k))
     return d->s;
   drop_solver(d);
@@ -528,41 +601,52 @@ static wbfmm_b200_solver_t *solver_for(wbfmm_tree_t *t, double k,
   c.keys_fp32 = d->fp32;
   c.field = WBFMM_B200_POTENTIAL | WBFMM_B200_GRADIENT;
   c.managed = 1;
-  check(fn, wbfmm_b200_solver_create(&d->s, &c, NULL));
-  for (l = 1; l <= t->depth; l++)
-    check(fn, wbfmm_b200_adopt_coefficients(d->s, (int)l, t->mps[l], t->mpr[l]));
   if (d->fp32) {
     free(d->pts64);
     free(d->nrm64);
     d->pts64 = widen3(t->points, t->pstr, t->npoints);
     d->nrm64 = t->normals ? widen3(t->normals, t->nstr, t->npoints) : NULL;
-    check(fn, wbfmm_b200_set_sources(d->s, (int)t->npoints, d->pts64, 3, d->nrm64, 3, 0));
-  } else {
-    check(fn, wbfmm_b200_set_sources(d->s, (int)t->npoints, (const double *)t->points,
-                                     (int)(t->pstr / sizeof(double)),
-                                     (const double *)t->normals,
-                                     (int)(t->nstr / sizeof(double)), 0));
+  }
+  for (q = 0; q < ncomp(d); q++) {
+    wbfmm_b200_solver_t **sp = q ? &d->sc[q] : &d->s;
+    check(fn, wbfmm_b200_solver_create(sp, &c, NULL));
+    for (l = 1; l <= t->depth; l++)
+      check(fn, wbfmm_b200_adopt_coefficients(*sp, (int)l, d->nq > 1 ? d->cms[q][l] : t->mps[l],
+                                              d->nq > 1 ? d->cmr[q][l] : t->mpr[l]));
+    if (d->fp32)
+      check(fn, wbfmm_b200_set_sources(*sp, (int)t->npoints, d->pts64, 3, d->nrm64, 3, 0));
+    else
+      check(fn, wbfmm_b200_set_sources(*sp, (int)t->npoints, (const double *)t->points,
+                                       (int)(t->pstr / sizeof(double)),
+                                       (const double *)t->normals,
+                                       (int)(t->nstr / sizeof(double)), 0));
   }
   d->k = k;
   d->ready = 1;
   return d->s;
 }
 
-/* strengths q[i*qstr], dip[i*dstr] (doubles, or floats for an FP32 tree) */
+/* strengths q[i*qstr], dip[i*dstr] (doubles, or floats for an FP32 tree);
+   component c of a multi-component tree at q[i*qstr + c], dip[i*dstr + c] */
 static void strengths_for(dtree_t *d, const void *q, int qstr,
                           const void *dip, int dstr, const char *fn) {
+  int c;
   if (d->q == q && d->qstr == qstr && d->dip == dip && d->dstr == dstr && (q || dip))
     return;
   if (dip && !d->t.normals) die(fn, "no normals in tree but dipole strengths specified");
-  if (d->fp32) {
-    const int w = d->t.problem == WBFMM_PROBLEM_HELMHOLTZ ? 2 : 1;
-    double *q64 = widen_strengths(q, qstr, d->t.npoints, w);
-    double *d64 = widen_strengths(dip, dstr, d->t.npoints, w);
-    check(fn, wbfmm_b200_set_strengths(d->s, q64, w, d64, w, 0));
-    free(q64);
-    free(d64);
-  } else {
-    check(fn, wbfmm_b200_set_strengths(d->s, q, qstr, dip, dstr, 0));
+  for (c = 0; c < ncomp(d); c++) {
+    wbfmm_b200_solver_t *s = comp_solver(d, c);
+    if (d->fp32) {
+      const int w = d->t.problem == WBFMM_PROBLEM_HELMHOLTZ ? 2 : 1;
+      double *q64 = widen_strengths(q ? (const float *)q + c : NULL, qstr, d->t.npoints, w);
+      double *d64 = widen_strengths(dip ? (const float *)dip + c : NULL, dstr, d->t.npoints, w);
+      check(fn, wbfmm_b200_set_strengths(s, q64, w, d64, w, 0));
+      free(q64);
+      free(d64);
+    } else {
+      check(fn, wbfmm_b200_set_strengths(s, q ? (const double *)q + c : NULL, qstr,
+                                         dip ? (const double *)dip + c : NULL, dstr, 0));
+    }
   }
   d->q = q; d->qstr = qstr; d->dip = dip; d->dstr = dstr;
 }
@@ -571,17 +655,21 @@ static void strengths_for(dtree_t *d, const void *q, int qstr,
 static gint leaf(wbfmm_tree_t *t, double k, const void *src, gint sstr,
                  const void *dipoles, gint dstr, gboolean zero, const char *fn) {
   dtree_t *d = DT(t);
-  wbfmm_b200_solver_t *s = solver_for(t, k, fn);
+  int c;
+  solver_for(t, k, fn);
   if (!src && !dipoles) {
-    if (zero)
-      memset(t->mps[t->depth], 0, level_bytes(t, t->depth, t->order_s[t->depth]));
+    if (zero) zero_level(t, t->depth, 1);
     return 0;
   }
   d->q = d->dip = NULL;       /* strengths may have changed in place */
   strengths_for(d, src, sstr, dipoles, dstr, fn);
-  check(fn, wbfmm_b200_set_p2m_accumulate(s, zero ? 0 : 1));
-  check(fn, wbfmm_b200_leaf_expansions(s));
-  check(fn, wbfmm_b200_synchronize(s));
+  for (c = 0; c < ncomp(d); c++) {
+    wbfmm_b200_solver_t *s = comp_solver(d, c);
+    check(fn, wbfmm_b200_set_p2m_accumulate(s, zero ? 0 : 1));
+    check(fn, wbfmm_b200_leaf_expansions(s));
+    check(fn, wbfmm_b200_synchronize(s));
+  }
+  interleave(t, t->depth, 1);
   return 0;
 }
 
@@ -606,17 +694,26 @@ gint wbfmm_tree_laplace_leaf_expansions(wbfmm_tree_t *t, gdouble *src,
 
 static gint upward(wbfmm_tree_t *t, guint level, const char *fn) {
   dtree_t *d = DT(t);
+  int c;
   if (!d->s || !d->ready) die(fn, "leaf expansions must be computed first");
-  check(fn, wbfmm_b200_upward_pass(d->s, (int)level));
-  check(fn, wbfmm_b200_synchronize(d->s));
+  for (c = 0; c < ncomp(d); c++) {
+    check(fn, wbfmm_b200_upward_pass(comp_solver(d, c), (int)level));
+    check(fn, wbfmm_b200_synchronize(comp_solver(d, c)));
+  }
+  if (level >= 1) interleave(t, level - 1, 1);
   return 0;
 }
 
 static gint downward(wbfmm_tree_t *t, guint level, const char *fn) {
   dtree_t *d = DT(t);
+  int c;
   if (!d->s || !d->ready) die(fn, "leaf expansions must be computed first");
-  check(fn, wbfmm_b200_downward_pass(d->s, (int)level));
-  check(fn, wbfmm_b200_synchronize(d->s));
+  for (c = 0; c < ncomp(d); c++) {
+    check(fn, wbfmm_b200_downward_pass(comp_solver(d, c), (int)level));
+    check(fn, wbfmm_b200_synchronize(comp_solver(d, c)));
+  }
+  interleave(t, level, 0);
+  if (level < t->depth) interleave(t, level + 1, 0);   /* its L2L part */
   return 0;
 }
 
@@ -706,6 +803,72 @@ static void evaluate_targets(dtree_t *d, const void *key, guint n,
   free(grad);
 }
 
+/* Laplace field at one point x for a multi-component tree, or a curl
+   field (src/local-laplace.c:1293-1336): added into fv (doubles, or floats
+   for an FP32 tree).  Potential: component c at fv[c fstr]; gradient:
+   fv[c fstr + 0..2] (fstr >= 3 when nq > 1); curl (nq >= 3, the first
+   three components): fv[0..2]; curl and gradient: fv[0..11], the curl then
+   d/dx, d/dy, d/dz of its components (fstr ignored, as the reference) */
+static void laplace_field_point(dtree_t *d, const double *x, guint field,
+                                gboolean nb, void *fv, gint fstr, const char *fn) {
+  const int nq = ncomp(d);
+  double out[DT_MAX_NQ * 3], g[3][3], h[3][9];
+  int c, j, n = 0, stride = 1;
+  memset(out, 0, sizeof(out));
+  if (field & WBFMM_FIELD_CURL) {
+    const int cg = (field & WBFMM_FIELD_GRADIENT) != 0;
+    if (nq < 3) die(fn, "not enough source components for curl calculation");
+    for (c = 0; c < 3; c++) {
+      wbfmm_b200_solver_t *s = comp_solver(d, c);
+      check(fn, wbfmm_b200_set_targets(s, 1, x, 3, 0));
+      check(fn, wbfmm_b200_set_evaluation(s, WBFMM_B200_GRADIENT, nb));
+      check(fn, wbfmm_b200_evaluate(s));
+      check(fn, wbfmm_b200_get_field(s, NULL, g[c], 0));
+      if (cg) check(fn, wbfmm_b200_laplace_hessian(s, h[c], nb, 0));
+    }
+    out[0] = g[2][1] - g[1][2];
+    out[1] = g[0][2] - g[2][0];
+    out[2] = g[1][0] - g[0][1];
+    n = 3;
+    if (cg) {
+      for (j = 0; j < 3; j++) {
+        out[3 + 3 * j + 0] = h[2][3 * j + 1] - h[1][3 * j + 2];
+        out[3 + 3 * j + 1] = h[0][3 * j + 2] - h[2][3 * j + 0];
+        out[3 + 3 * j + 2] = h[1][3 * j + 0] - h[0][3 * j + 1];
+      }
+      n = 12;
+    }
+  } else {
+    const int grad = (field & WBFMM_FIELD_GRADIENT) != 0;
+    if (grad && nq > 1 && fstr < 3) die(fn, "field data stride must be greater than two");
+    for (c = 0; c < nq; c++) {
+      wbfmm_b200_solver_t *s = comp_solver(d, c);
+      check(fn, wbfmm_b200_set_targets(s, 1, x, 3, 0));
+      check(fn, wbfmm_b200_set_evaluation(s, grad ? WBFMM_B200_GRADIENT : WBFMM_B200_POTENTIAL, nb));
+      check(fn, wbfmm_b200_evaluate(s));
+      check(fn, wbfmm_b200_get_field(s, grad ? NULL : out + 3 * c, grad ? out + 3 * c : NULL, 0));
+    }
+    /* out[3 c + j] -> f[c fstr + j] */
+    stride = fstr;
+    n = -(grad ? 3 : 1);
+  }
+  d->targets = NULL;   /* the solvers' targets are this point now */
+#define WBFMM_ADD_POINT(_T)                                                   \
+  do {                                                                        \
+    _T *f = (_T *)fv;                                                         \
+    if (n > 0)                                                                \
+      for (j = 0; j < n; j++) f[j] += (_T)out[j];                             \
+    else                                                                      \
+      for (c = 0; c < nq; c++)                                                \
+        for (j = 0; j < -n; j++) f[(size_t)c * stride + j] += (_T)out[3 * c + j]; \
+  } while (0)
+  if (d->fp32)
+    WBFMM_ADD_POINT(float);
+  else
+    WBFMM_ADD_POINT(double);
+#undef WBFMM_ADD_POINT
+}
+
 /* src/local.c:264-310 */
 gint wbfmm_tree_box_local_field(wbfmm_tree_t *t, guint level, guint b,
                                 gdouble k, gdouble *x, gdouble *f, gint fstr,
@@ -737,12 +900,14 @@ gint wbfmm_laplace_box_field(wbfmm_tree_t *t, guint level, guint b,
   (void)b; (void)work;
   if (t->problem != WBFMM_PROBLEM_LAPLACE) die(__func__, "tree problem is not Laplace");
   if (level != t->depth) die(__func__, "evaluation is supported at the leaf level");
-  if (field & (WBFMM_FIELD_CURL | WBFMM_FIELD_CURL_GRADIENT))
-    die(__func__, "curl fields are not supported");
-  if (field & WBFMM_FIELD_GRADIENT) field = WBFMM_FIELD_GRADIENT;
-  (void)fstr;
+  if (field < 1 || field > 7) die(__func__, "unrecognized field type");
   solver_for(t, 0.0, __func__);
   if (eval_neighbours && (src || d)) strengths_for(dt, src, sstr, d, dstr, __func__);
+  if ((field & WBFMM_FIELD_CURL) || dt->nq > 1) {
+    laplace_field_point(dt, x, field, eval_neighbours && (src || d), f, fstr, __func__);
+    return 0;
+  }
+  if (field & WBFMM_FIELD_GRADIENT) field = WBFMM_FIELD_GRADIENT;
   evaluate_targets(dt, NULL, 1, x, 3, field, eval_neighbours && (src || d), f,
                    0, __func__);
   return 0;
@@ -814,7 +979,8 @@ static gint list_field(wbfmm_target_list_t *l, const void *src, gint sstr,
   dtree_t *d = DT(l->t);
   if (!l->field) die(fn, "field not set (wbfmm_target_list_coefficients_init)");
   if (l->field & (WBFMM_FIELD_CURL | WBFMM_FIELD_CURL_GRADIENT))
-    die(fn, "curl fields are not supported");
+    die(fn, "curl fields are not supported with target lists");
+  if (d->nq > 1) die(fn, "multi-component sources are not supported with target lists");
   if (!d->s || !d->ready) list_prepare(l, d->k, fn);
   if (src || nsrc) strengths_for(d, src, sstr, nsrc, nstr, fn);
   if (d->targets != l || d->ntargets != l->npoints) list_prepare(l, d->k, fn);
@@ -1076,15 +1242,18 @@ gint wbfmm_laplace_box_field_f(wbfmm_tree_t *t, guint level, guint b, gfloat *sr
                                gfloat *work) {
   dtree_t *dt = DT(t);
   double x64[3] = {x[0], x[1], x[2]};
-  (void)b; (void)work; (void)fstr;
+  (void)b; (void)work;
   need_fp32(t, __func__);
   if (t->problem != WBFMM_PROBLEM_LAPLACE) die(__func__, "tree problem is not Laplace");
   if (level != t->depth) die(__func__, "evaluation is supported at the leaf level");
-  if (field & (WBFMM_FIELD_CURL | WBFMM_FIELD_CURL_GRADIENT))
-    die(__func__, "curl fields are not supported");
-  if (field & WBFMM_FIELD_GRADIENT) field = WBFMM_FIELD_GRADIENT;
+  if (field < 1 || field > 7) die(__func__, "unrecognized field type");
   solver_for(t, 0.0, __func__);
   if (eval_neighbours && (src || d)) strengths_for(dt, src, sstr, d, dstr, __func__);
+  if ((field & WBFMM_FIELD_CURL) || dt->nq > 1) {
+    laplace_field_point(dt, x64, field, eval_neighbours && (src || d), f, fstr, __func__);
+    return 0;
+  }
+  if (field & WBFMM_FIELD_GRADIENT) field = WBFMM_FIELD_GRADIENT;
   evaluate_targets(dt, NULL, 1, x64, 3, field, eval_neighbours && (src || d), f, 0,
                    __func__);
   return 0;

@@ -96,6 +96,8 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "wbfmm_b200_fp32_fma_peak": (ip, [dp]),
         "wbfmm_b200_error_norms": (ip, [C.c_int64, vp, vp, ip, dp]),
         "wbfmm_b200_laplace_curl": (ip, [vp, vp, ip, vp, ip]),
+        "wbfmm_b200_laplace_curl_gradient": (ip, [vp, vp, ip, vp, ip]),
+        "wbfmm_b200_laplace_hessian": (ip, [vp, vp, ip, ip]),
         "wbfmm_b200_synchronize": (ip, [vp]),
         "wbfmm_b200_get_field": (ip, [vp, vp, vp, ip]),
         "wbfmm_b200_get_tree": (ip, [vp, u32p, u32p, u32p, ip]),
@@ -294,6 +296,22 @@ class Solver:
         out = np.zeros(self.nt * 3)
         _check(self.lib.wbfmm_b200_laplace_curl(self.h, _addr(q3), 3, _addr(out), 0))
         return out.reshape(-1, 3)
+
+    def laplace_curl_gradient(self, q3):
+        """Curl of the vector potential of sources with 3-vector strengths
+        q3 [ns, 3] and its gradient at the targets: [nt, 12] (curl, then
+        d/dx, d/dy, d/dz of the curl; Laplace solver, gradient field)."""
+        q3 = _host(q3).reshape(-1, 3)
+        out = np.zeros(self.nt * 12)
+        _check(self.lib.wbfmm_b200_laplace_curl_gradient(self.h, _addr(q3), 3, _addr(out), 0))
+        return out.reshape(-1, 12)
+
+    def hessian(self, neighbours=True):
+        """Second derivatives of the potential at the targets after run():
+        [nt, 3, 3] (Laplace solver)."""
+        out = np.zeros(self.nt * 9)
+        _check(self.lib.wbfmm_b200_laplace_hessian(self.h, _addr(out), int(bool(neighbours)), 0))
+        return out.reshape(-1, 3, 3)
 
     def run_graph(self):
         """The passes as one CUDA graph launch (captured on the first call
