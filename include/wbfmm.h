@@ -364,15 +364,149 @@ gint wbfmm_laplace_field_grad_f(gfloat *xs, gint xstride, gfloat *src,
                                 gint nsrc, gfloat *xf, gfloat *field,
                                 gint fstr);
 
+/* ------------------------------------- single-expansion primitives
+   (src/wbfmm.h:247-263, :266-320, :347-361, :402-420, :525-643).  The
+   array primitives run on the GPU (one CTA per call; the caller's host
+   arrays are copied in and out before the call returns); the scalar
+   helpers run on the host.  Coefficient c of component j: Helmholtz at
+   cfft[2 (c cstr + j)] (complex), Laplace at cfft[c cstr + j]
+   (real-packed); rotation and coaxial translation leave Co = sc Co + T(Ci);
+   expansions and fields are added to what the caller holds.  The FP32
+   twins compute in FP64 and round. */
+gint wbfmm_cartesian_to_spherical(gdouble *x0, gdouble *x, gdouble *r,
+                                  gdouble *th, gdouble *ph);
+gint wbfmm_legendre_init(gdouble C, gdouble S, gdouble *P0, gdouble *P10,
+                         gdouble *P11);
+gint wbfmm_legendre_recursion_array(gdouble **Pnm1, gdouble **Pn, gint n,
+                                    gdouble C, gdouble S);
+gint wbfmm_bessel_j_init(gdouble x, gdouble *j0, gdouble *j1);
+gint wbfmm_bessel_j_recursion(gdouble *jnm1, gdouble *jn, gdouble x, gint n);
+gint wbfmm_bessel_h_init(gdouble x, gdouble *h0, gdouble *h1);
+gint wbfmm_bessel_h_recursion(gdouble *hnm1, gdouble *hn, gdouble x, gint n);
+gint wbfmm_coefficients_H_rotation(gdouble *H, gint N, gdouble th,
+                                   gdouble *work);
+gint wbfmm_coefficients_RR_coaxial(gdouble *cfftRR, gint L, gdouble kr,
+                                   gdouble *work);
+gint wbfmm_coefficients_SR_coaxial(gdouble *cfftSR, gint L, gdouble kr,
+                                   gdouble *work);
+gint wbfmm_rotate_H_ref(gdouble *Co, gint cstro, gdouble *Ci, gint cstri,
+                        gint N, gint nq, gdouble *H, gdouble ph, gdouble ch,
+                        gdouble sc);
+gint wbfmm_rotate_H_avx(gdouble *Co, gint cstro, gdouble *Ci, gint cstri,
+                        gint N, gint nq, gdouble *H, gdouble ph, gdouble ch,
+                        gdouble sc);
+gint wbfmm_coaxial_translate_ref(gdouble *Co, gint cstro, gint No,
+                                 gdouble *Ci, gint cstri, gint Ni, gint nq,
+                                 gdouble *cfft, gint L, gboolean complex,
+                                 gdouble sc);
+gint wbfmm_expansion_h_cfft(gdouble k, gint N, gdouble *x0, gdouble *xs,
+                            gdouble *q, gint nq, gdouble *cfft, gint cstr,
+                            gdouble *work);
+gint wbfmm_expansion_j_evaluate(gdouble k, gdouble *x0, gdouble *cfft,
+                                gint cstr, gint N, gint nq, gdouble *xf,
+                                gdouble *field, gint fstr, gdouble *work);
+gint wbfmm_expansion_h_evaluate(gdouble k, gdouble *x0, gdouble *cfft,
+                                gint cstr, gint N, gint nq, gdouble *xf,
+                                gdouble *field, gint fstr, gdouble *work);
+gint wbfmm_laplace_expansion_cfft(gint N, gdouble *x0, gdouble *xs,
+                                  gdouble *q, gint nq, gdouble *cfft,
+                                  gint cstr, gdouble *work);
+gint wbfmm_laplace_expansion_evaluate(gdouble *x0, gdouble *cfft, gint cstr,
+                                      gint N, gint nq, gdouble *xf,
+                                      gdouble *field, gdouble *work);
+/* potential and gradient fields (curl fields: wbfmm_laplace_box_field) */
+gint wbfmm_laplace_expansion_local_eval(gdouble *x0, gdouble *cfft,
+                                        gint cstr, gint N, gint nq,
+                                        guint field, gdouble *xf,
+                                        gdouble *f, gint fstr, gdouble *work);
+gint wbfmm_laplace_rotate_H_ref(gdouble *Co, gint cstro, gdouble *Ci,
+                                gint cstri, gint N, gint nq, gdouble *H,
+                                gdouble ph, gdouble ch, gdouble sc);
+gint wbfmm_laplace_rotate_H_avx(gdouble *Co, gint cstro, gdouble *Ci,
+                                gint cstri, gint N, gint nq, gdouble *H,
+                                gdouble ph, gdouble ch, gdouble sc);
+gint wbfmm_laplace_coaxial_translate_SS(gdouble *Co, gint cstro, gint No,
+                                        gdouble *Ci, gint cstri, gint Ni,
+                                        gint nq, gdouble t, gdouble sc);
+gint wbfmm_laplace_coaxial_translate_RR(gdouble *Co, gint cstro, gint No,
+                                        gdouble *Ci, gint cstri, gint Ni,
+                                        gint nq, gdouble t, gdouble sc);
+gint wbfmm_laplace_coaxial_translate_SR(gdouble *Co, gint cstro, gint No,
+                                        gdouble *Ci, gint cstri, gint Ni,
+                                        gint nq, gdouble t, gdouble sc);
+
+gint wbfmm_cartesian_to_spherical_f(gfloat *x0, gfloat *x, gfloat *r,
+                                    gfloat *th, gfloat *ph);
+gint wbfmm_legendre_init_f(gfloat C, gfloat S, gfloat *P0, gfloat *P10,
+                           gfloat *P11);
+gint wbfmm_legendre_recursion_array_f(gfloat **Pnm1, gfloat **Pn, gint n,
+                                      gfloat C, gfloat S);
+gint wbfmm_bessel_j_init_f(gfloat x, gfloat *j0, gfloat *j1);
+gint wbfmm_bessel_j_recursion_f(gfloat *jnm1, gfloat *jn, gfloat x, gint n);
+gint wbfmm_bessel_h_init_f(gfloat x, gfloat *h0, gfloat *h1);
+gint wbfmm_bessel_h_recursion_f(gfloat *hnm1, gfloat *hn, gfloat x, gint n);
+gint wbfmm_coefficients_H_rotation_f(gfloat *H, gint N, gfloat th,
+                                     gfloat *work);
+gint wbfmm_coefficients_RR_coaxial_f(gfloat *cfftRR, gint L, gfloat kr,
+                                     gfloat *work);
+gint wbfmm_coefficients_SR_coaxial_f(gfloat *cfftSR, gint L, gfloat kr,
+                                     gfloat *work);
+gint wbfmm_rotate_H_ref_f(gfloat *Co, gint cstro, gfloat *Ci, gint cstri,
+                          gint N, gint nq, gfloat *H, gfloat ph, gfloat ch,
+                          gfloat sc);
+gint wbfmm_coaxial_translate_ref_f(gfloat *Co, gint cstro, gint No,
+                                   gfloat *Ci, gint cstri, gint Ni, gint nq,
+                                   gfloat *cfft, gint L, gboolean complex,
+                                   gfloat sc);
+gint wbfmm_expansion_h_cfft_f(gfloat k, gint N, gfloat *x0, gfloat *xs,
+                              gfloat *q, gint nq, gfloat *cfft, gint cstr,
+                              gfloat *work);
+gint wbfmm_expansion_j_evaluate_f(gfloat k, gfloat *x0, gfloat *cfft,
+                                  gint cstr, gint N, gint nq, gfloat *xf,
+                                  gfloat *field, gint fstr, gfloat *work);
+gint wbfmm_expansion_h_evaluate_f(gfloat k, gfloat *x0, gfloat *cfft,
+                                  gint cstr, gint N, gint nq, gfloat *xf,
+                                  gfloat *field, gint fstr, gfloat *work);
+gint wbfmm_laplace_expansion_cfft_f(gint N, gfloat *x0, gfloat *xs,
+                                    gfloat *q, gint nq, gfloat *cfft,
+                                    gint cstr, gfloat *work);
+gint wbfmm_laplace_expansion_evaluate_f(gfloat *x0, gfloat *cfft, gint cstr,
+                                        gint N, gint nq, gfloat *xf,
+                                        gfloat *field, gfloat *work);
+gint wbfmm_laplace_expansion_local_eval_f(gfloat *x0, gfloat *cfft,
+                                          gint cstr, gint N, gint nq,
+                                          guint field, gfloat *xf, gfloat *f,
+                                          gint fstr, gfloat *work);
+gint wbfmm_laplace_rotate_H_ref_f(gfloat *Co, gint cstro, gfloat *Ci,
+                                  gint cstri, gint N, gint nq, gfloat *H,
+                                  gfloat ph, gfloat ch, gfloat sc);
+gint wbfmm_laplace_coaxial_translate_SS_f(gfloat *Co, gint cstro, gint No,
+                                          gfloat *Ci, gint cstri, gint Ni,
+                                          gint nq, gfloat t, gfloat sc);
+gint wbfmm_laplace_coaxial_translate_RR_f(gfloat *Co, gint cstro, gint No,
+                                          gfloat *Ci, gint cstri, gint Ni,
+                                          gint nq, gfloat t, gfloat sc);
+gint wbfmm_laplace_coaxial_translate_SR_f(gfloat *Co, gint cstro, gint No,
+                                          gfloat *Ci, gint cstri, gint Ni,
+                                          gint nq, gfloat t, gfloat sc);
+
 /* dispatch as in the reference (src/wbfmm.h:1138-1194) */
 #define wbfmm_downward_pass_f wbfmm_downward_pass_ref_f
 #define wbfmm_laplace_downward_pass_f wbfmm_laplace_downward_pass_ref_f
+#define wbfmm_rotate_H_f wbfmm_rotate_H_ref_f
+#define wbfmm_laplace_rotate_H_f wbfmm_laplace_rotate_H_ref_f
+#define wbfmm_coaxial_translate wbfmm_coaxial_translate_ref
+#define wbfmm_coaxial_translate_f wbfmm_coaxial_translate_ref_f
 #ifdef WBFMM_USE_AVX
 #define wbfmm_downward_pass wbfmm_downward_pass_avx
 #define wbfmm_laplace_downward_pass wbfmm_laplace_downward_pass_avx
+#define wbfmm_rotate_H wbfmm_rotate_H_avx
+#define wbfmm_laplace_rotate_H wbfmm_laplace_rotate_H_avx
 #else
 #define wbfmm_downward_pass wbfmm_downward_pass_ref
 #define wbfmm_laplace_downward_pass wbfmm_laplace_downward_pass_ref
+#define wbfmm_rotate_H wbfmm_rotate_H_ref
+#define wbfmm_laplace_rotate_H wbfmm_laplace_rotate_H_ref
 #endif
 
 #ifdef __cplusplus
