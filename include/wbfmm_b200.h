@@ -152,6 +152,19 @@ int wbfmm_b200_set_deferred_checks(wbfmm_b200_solver_t *s, int on);
 int wbfmm_b200_laplace_curl(wbfmm_b200_solver_t *s, const double *q3, int qstr,
                             double *curl, int on_device);
 
+/* Precomputed target bases (the reference's target-list strategy,
+   src/targets.c:168-603, potential only): for the solver's current sources
+   and targets, the basis of each target's leaf regular expansion and the
+   near-field weights of the sources of its 27 neighbour boxes, stored on the
+   device until the sources or targets change.  wbfmm_b200_evaluate_bases
+   then writes the potential at the targets (read with
+   wbfmm_b200_get_field) from the leaf regular expansions of the last
+   downward pass and, with neighbours != 0, the current strengths: a product
+   with stored bases and weights instead of the L2P and P2P's special
+   functions, for repeated solves at fixed targets. */
+int wbfmm_b200_target_bases(wbfmm_b200_solver_t *s);
+int wbfmm_b200_evaluate_bases(wbfmm_b200_solver_t *s, int neighbours);
+
 /* Second derivatives of the Laplace potential at the solver's targets,
    after a run (or the downward passes): hess[9 j + 3 a + b] = d_a d_b phi
    at target j (original order), from the leaf regular expansions (the

@@ -548,6 +548,46 @@ def test_laplace_curl_gradient(gpu_lib):
     assert rel_l2(cg[:, 3:].ravel(), ref[:, 3:].ravel()) < 2e-5, rel_l2(cg[:, 3:].ravel(), ref[:, 3:].ravel())
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [engine.FP64, engine.FP32])
+@pytest.mark.parametrize("case", ["laplace", "helmholtz", "helmholtz_dipoles"])
+def test_target_bases(gpu_lib, case, precision):
+    """Potential at fixed targets from the precomputed bases and near-field
+    weights (the reference's target-list strategy) against the L2P + P2P
+    evaluation, for the first strengths and for new ones after a repeated
+    solve; the far field alone without the near-field weights."""
+    if case == "laplace":
+        p = W.laplace_cube(20000, 3000, depth=4, order=10, seed=91)
+    elif case == "helmholtz":
+        p = W.helmholtz_cube(20000, k=6.0, depth=4, seed=92)
+    else:
+        p = W.helmholtz_sphere(20000, 3000, k=10.0, depth=4, seed=93)
+    rng = np.random.default_rng(94)
+    tol = 1e-12 if precision == engine.FP64 else 1e-6
+    with engine.Solver(engine.SolverConfig.from_problem(p, precision)) as s:
+        s.set_sources(p.xs, normals=p.normals)
+        s.set_strengths(p.q, dipoles=p.dipoles).set_targets(p.xt).run()
+        ref = s.field()[0]
+        s.target_bases().evaluate_bases()
+        got = s.field()[0]
+        assert rel_l2(got, ref) < tol, rel_l2(got, ref)
+        q2 = rng.standard_normal(p.q.shape)
+        s.set_strengths(q2, dipoles=p.dipoles).run()
+        ref2 = s.field()[0]
+        s.evaluate_bases()
+        assert rel_l2(s.field()[0], ref2) < tol, rel_l2(s.field()[0], ref2)
+        s.evaluate_bases(neighbours=False)
+        far = s.field()[0]
+    with engine.Solver(engine.SolverConfig.from_problem(p, precision)) as s:
+        s.set_sources(p.xs, normals=p.normals)
+        s.set_strengths(q2, dipoles=p.dipoles).set_targets(p.xt).run()
+        s.set_evaluation(engine.POTENTIAL, neighbours=False)
+        s.evaluate()
+        s.synchronize()
+        far_ref = s.field()[0]
+    assert rel_l2(far, far_ref) < tol, rel_l2(far, far_ref)
+
+
 def _edge_problem(case):
     rng = np.random.default_rng(71)
     if case == "coincident":

@@ -141,6 +141,17 @@ template <typename T>
 int launch_p2p_hessian(const EvalParams<T>& p, double* hess, cudaStream_t s);
 int launch_curl_gradient_combine(const double* g, const double* h, int nt, double* out,
                                  cudaStream_t s);
+// precomputed target bases (target_bases.cu): pair offsets of the targets'
+// near fields; the CSR sources, monopole and (wd non-null) dipole weights
+// and the coefficient-major regular-expansion bases; the potential from them
+template <typename T>
+int tl_offsets(const EvalParams<T>& p, int64_t* off, int64_t* npairs, cudaStream_t s);
+template <typename T, bool HELM>
+int tl_fill(const EvalParams<T>& p, const int64_t* off, uint32_t* src, T* wq, T* wd, T* basis,
+            cudaStream_t s);
+template <typename T, bool HELM>
+int tl_apply(const EvalParams<T>& p, const T* basis, const int64_t* off, const uint32_t* src,
+             const T* wq, const T* wd, cudaStream_t s);
 // self-test of the FP32 near-field sine/cosine (kernels.cu)
 int sincos_near_errors(double xmax, int n, double* host_err);
 

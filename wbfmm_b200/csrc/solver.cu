@@ -181,6 +181,11 @@ int wbfmm_b200_run(wbfmm_b200_solver_t* s) { SOLVER_CALL(s->run()); }
 int wbfmm_b200_run_async(wbfmm_b200_solver_t* s) { SOLVER_CALL(s->run_queued()); }
 int wbfmm_b200_run_graph(wbfmm_b200_solver_t* s) { SOLVER_CALL(s->run_graph()); }
 int wbfmm_b200_wait(wbfmm_b200_solver_t* s) { SOLVER_CALL(s->wait()); }
+int wbfmm_b200_target_bases(wbfmm_b200_solver_t* s) { SOLVER_CALL(s->target_bases()); }
+int wbfmm_b200_evaluate_bases(wbfmm_b200_solver_t* s, int neighbours) {
+  SOLVER_CALL(s->evaluate_bases(neighbours));
+}
+
 int wbfmm_b200_laplace_hessian(wbfmm_b200_solver_t* s, double* hess, int neighbours,
                                int on_device) {
   if (!s || !hess) return set_error(WBFMM_B200_E_ARG, "bad Hessian arguments");

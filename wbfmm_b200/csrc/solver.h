@@ -172,6 +172,8 @@ struct wbfmm_b200_solver {
   virtual int set_deferred_checks(int on) = 0;
   virtual int get_field(double*, double*, int) = 0;
   virtual int hessian(double* hess, int neighbours) = 0;
+  virtual int target_bases() = 0;
+  virtual int evaluate_bases(int neighbours) = 0;
   virtual int sources() const = 0;
   virtual int targets() const = 0;
   virtual int get_tree(uint32_t*, uint32_t*, uint32_t*, int) = 0;
@@ -223,6 +225,13 @@ struct Solver : public wbfmm_b200_solver {
   // outputs (original order)
   DBuf<T> pot, grad;
   DBuf<T> hess_d, hess_g;           // Hessian: derived expansions, gradients
+  // precomputed target bases (potential): CSR near-field weights, bases
+  DBuf<int64_t> tl_off;
+  DBuf<uint32_t> tl_src;
+  DBuf<T> tl_wq, tl_wd, tl_basis;
+  uint64_t geo = 0;                 // bumped by set_sources / set_targets
+  uint64_t tl_geo = ~0ull;          // geo of the bases held
+  bool tl_dip = false;
   DBuf<double> out64;
   // tables
   bool ops_ready = false;
@@ -285,6 +294,7 @@ struct Solver : public wbfmm_b200_solver {
     f(coax_set64); f(coax_set);
     f(tpts_in); f(tx); f(ty); f(tz); f(tkeys); f(tperm); f(tbox);
     f(tstart); f(tcount); f(flag); f(pot); f(grad); f(out64); f(hess_d); f(hess_g);
+    f(tl_off); f(tl_src); f(tl_wq); f(tl_wd); f(tl_basis);
     f(H64); f(H); f(op_ith); f(op_dist); f(op_r); f(op_ph); f(op_ch);
     for (int i = 0; i < 3; i++) { f(lap64[i]); f(lap[i]); }
     f(partial); f(lin); f(lanes_part); f(act_scr); f(lapsr); f(hcx); f(smask); f(tc_part);
@@ -394,6 +404,7 @@ struct Solver : public wbfmm_b200_solver {
     if (normals && n_str < 3) return set_error(WBFMM_B200_E_ARG, "bad normal stride");
     cudaEventRecord(ev[0], stream);
     gen++;
+    geo++;
     src_arg = nullptr;              // set again only when these sources are in place
     nsrc = n;
     xstr = xs_str;
@@ -499,6 +510,7 @@ struct Solver : public wbfmm_b200_solver {
 
   int set_targets(int n, const double* xt, int tstr, int on_device) override {
     gen++;
+    geo++;
     if (n <= 0 || xt == nullptr || tstr < 3)
       return set_error(WBFMM_B200_E_ARG, "bad target points");
     ntgt = n;
@@ -1182,6 +1194,46 @@ struct Solver : public wbfmm_b200_solver {
       WBFMM_TRY(launch_p2p_hessian<T>(eparams(), hess, stream));
       launches++;
     }
+    return 0;
+  }
+
+  // precomputed target bases for repeated potential evaluations at these
+  // targets (target_bases.cu): held until the sources or targets change
+  int target_bases() override {
+    if (nsrc <= 0 || ntgt <= 0) return set_error(WBFMM_B200_E_STATE, "sources and targets must be set");
+    const EvalParams<T> e = eparams();
+    int64_t np = 0;
+    WBFMM_TRY(tl_off.alloc((size_t)ntgt + 1));
+    WBFMM_TRY(tl_offsets<T>(e, tl_off.p, &np, stream));
+    const int w = helm ? 2 : 1;
+    tl_dip = have_normals;
+    WBFMM_TRY(tl_src.alloc((size_t)np + 1));
+    WBFMM_TRY(tl_wq.alloc(((size_t)np + 1) * w));
+    if (tl_dip) WBFMM_TRY(tl_wd.alloc(((size_t)np + 1) * w));
+    WBFMM_TRY(tl_basis.alloc((size_t)ncoefs(cfg.order_r[depth]) * ntgt * w));
+    T* wd = tl_dip ? tl_wd.p : nullptr;
+    WBFMM_TRY((helm ? tl_fill<T, true>(e, tl_off.p, tl_src.p, tl_wq.p, wd, tl_basis.p, stream)
+                    : tl_fill<T, false>(e, tl_off.p, tl_src.p, tl_wq.p, wd, tl_basis.p, stream)));
+    launches += 3;
+    tl_geo = geo;
+    return 0;
+  }
+
+  // the potential at the targets from the bases, the leaf regular
+  // expansions (after the downward pass) and, with neighbours, the current
+  // strengths
+  int evaluate_bases(int neighbours) override {
+    if (tl_geo != geo)
+      return set_error(WBFMM_B200_E_STATE, "target bases must be computed for these sources and targets");
+    if (!(cfg.field & WBFMM_B200_POTENTIAL))
+      return set_error(WBFMM_B200_E_ARG, "the bases give the potential field");
+    EvalParams<T> e = eparams();
+    e.pot = pot.p;
+    if (!neighbours) e.q = e.dip = nullptr;
+    const T* wd = tl_dip ? tl_wd.p : nullptr;
+    WBFMM_TRY((helm ? tl_apply<T, true>(e, tl_basis.p, tl_off.p, tl_src.p, tl_wq.p, wd, stream)
+                    : tl_apply<T, false>(e, tl_basis.p, tl_off.p, tl_src.p, tl_wq.p, wd, stream)));
+    launches += 2;
     return 0;
   }
 

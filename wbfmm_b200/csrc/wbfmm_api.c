@@ -957,6 +957,10 @@ static gint list_prepare(wbfmm_target_list_t *l, double k, const char *fn) {
   }
   d->targets = l;
   d->ntargets = l->npoints;
+  /* the potential (the reference's only target-list field) from
+     precomputed bases, as its local_coefficients prepares them */
+  if (l->field == WBFMM_FIELD_POTENTIAL && d->nq <= 1)
+    check(fn, wbfmm_b200_target_bases(d->s));
   return 0;
 }
 
@@ -984,6 +988,21 @@ static gint list_field(wbfmm_target_list_t *l, const void *src, gint sstr,
   if (!d->s || !d->ready) list_prepare(l, d->k, fn);
   if (src || nsrc) strengths_for(d, src, sstr, nsrc, nstr, fn);
   if (d->targets != l || d->ntargets != l->npoints) list_prepare(l, d->k, fn);
+  if (l->field == WBFMM_FIELD_POTENTIAL) {
+    const int w = l->t->problem == WBFMM_PROBLEM_HELMHOLTZ ? 2 : 1;
+    double *pot = malloc(sizeof(double) * w * (l->npoints ? l->npoints : 1));
+    guint i;
+    int c;
+    check(fn, wbfmm_b200_evaluate_bases(d->s, (src || nsrc) ? 1 : 0));
+    check(fn, wbfmm_b200_get_field(d->s, pot, NULL, 0));
+    for (i = 0; i < l->npoints; i++)
+      for (c = 0; c < w; c++) {
+        if (d->fp32) ((float *)f)[(size_t)i * fstr + c] += (float)pot[(size_t)i * w + c];
+        else ((double *)f)[(size_t)i * fstr + c] += pot[(size_t)i * w + c];
+      }
+    free(pot);
+    return 0;
+  }
   /* the targets are in place (list_prepare), so no points are passed */
   evaluate_targets(d, l, l->npoints, NULL, 3, l->field, (src || nsrc), f, fstr, fn);
   return 0;

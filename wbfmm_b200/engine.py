@@ -98,6 +98,9 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "wbfmm_b200_laplace_curl": (ip, [vp, vp, ip, vp, ip]),
         "wbfmm_b200_laplace_curl_gradient": (ip, [vp, vp, ip, vp, ip]),
         "wbfmm_b200_laplace_hessian": (ip, [vp, vp, ip, ip]),
+        "wbfmm_b200_target_bases": (ip, [vp]),
+        "wbfmm_b200_set_evaluation": (ip, [vp, ip, ip]),
+        "wbfmm_b200_evaluate_bases": (ip, [vp, ip]),
         "wbfmm_b200_synchronize": (ip, [vp]),
         "wbfmm_b200_get_field": (ip, [vp, vp, vp, ip]),
         "wbfmm_b200_get_tree": (ip, [vp, u32p, u32p, u32p, ip]),
@@ -312,6 +315,25 @@ class Solver:
         out = np.zeros(self.nt * 9)
         _check(self.lib.wbfmm_b200_laplace_hessian(self.h, _addr(out), int(bool(neighbours)), 0))
         return out.reshape(-1, 3, 3)
+
+    def set_evaluation(self, field, neighbours=True):
+        """Fields written by evaluate() (a subset of the configured ones) and
+        whether the near field (P2P) is added."""
+        _check(self.lib.wbfmm_b200_set_evaluation(self.h, int(field), int(bool(neighbours))))
+        return self
+
+    def target_bases(self):
+        """Precompute the targets' expansion bases and near-field weights
+        (potential; kept until the sources or targets change)."""
+        _check(self.lib.wbfmm_b200_target_bases(self.h))
+        return self
+
+    def evaluate_bases(self, neighbours=True):
+        """The potential at the targets from the precomputed bases, the leaf
+        expansions of the last downward pass and the current strengths
+        (read it with field())."""
+        _check(self.lib.wbfmm_b200_evaluate_bases(self.h, int(bool(neighbours))))
+        return self
 
     def run_graph(self):
         """The passes as one CUDA graph launch (captured on the first call
