@@ -303,8 +303,12 @@ PROFILE_CASES = """
                             Laplace, 2e6 points in 8 Gaussian clusters,
                             depth 7, order 10, skip_empty, FP32: M2L of
                             level 7 (lane kernel on target lists)
+  m2l_tc_laplace_p14        as m2l_tiles_laplace_p14 on the tensor cores
+                            (M2L mode 4: tcgen05 3xTF32)
   p2p_helmholtz             Helmholtz k = 10, 2e5 points, depth 4, FP32:
                             evaluation (L2P + P2P)
+  target_bases_helmholtz    Helmholtz k = 10, 2e5 points, depth 4, FP64:
+                            potential from precomputed target bases
   served_stream             48 requests of the serving stream through a
                             1-slot server, FP32 where the range rule admits
                             the request, skip_empty and leaf_order (launch
@@ -339,6 +343,16 @@ def profile_case(case: str) -> None:
     if case == "m2l_tiles_laplace_p14":
         p = _cube(engine.LAPLACE, 300_000, 5, 14)
         _solve_then(p, engine.FP32, lambda s: s.m2l(5))
+    elif case == "m2l_tc_laplace_p14":
+        p = _cube(engine.LAPLACE, 300_000, 5, 14)
+
+        def tc(s):
+            s.set_m2l_kernel(4)
+            s.m2l(5)
+        _solve_then(p, engine.FP32, tc)
+    elif case == "target_bases_helmholtz":
+        p = _cube(engine.HELMHOLTZ, 200_000, 4, 8, k=10.0)
+        _solve_then(p, engine.FP64, lambda s: s.target_bases().evaluate_bases())
     elif case == "m2l_tiles_helmholtz_p14":
         p = _cube(engine.HELMHOLTZ, 100_000, 4, 14, k=10.0)
         _solve_then(p, engine.FP32, lambda s: s.m2l(4))
