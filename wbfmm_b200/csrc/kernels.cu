@@ -729,10 +729,13 @@ __device__ __forceinline__ void sincos_near(float x, float* sp, float* cp) {
 // factors, which the caller applies once per target (p2p_scale): 1/(4 pi)
 // on the potential, -k/(4 pi) (Helmholtz) and 1/(4 pi) (Laplace) on the
 // gradient.
-template <typename T, bool HELM, int NT, bool want_pot, bool want_grad>
+// MASKED: a pair within the cutoff (r2 <= rc2) takes 1/r = 0, which makes
+// each of its terms an exact zero, instead of being branched around (the
+// pairs of a run then interleave without divergence)
+template <typename T, bool HELM, int NT, bool want_pot, bool want_grad, bool MASKED = false>
 __device__ __forceinline__ void p2p_pair(const P2PTile<T, HELM, NT>& tl, int j, T rx, T ry, T rz,
-                                         T r2, T k, T kinv, bool hd, T* acc) {
-  const T ir = rsqrt(r2);
+                                         T r2, T k, T kinv, bool hd, T* acc, T rc2 = T(0)) {
+  const T ir = MASKED ? (r2 > rc2 ? rsqrt(r2) : T(0)) : rsqrt(r2);
   if (HELM) {
     const T r = r2 * ir;
     T kr = k * r, ikr, sn, cs;
@@ -809,9 +812,14 @@ __device__ __forceinline__ double p2p_scale(int c, double k) {
   return HELM ? (c < 2 ? f4pi : -k * f4pi) : f4pi;
 }
 
-// POT / GRAD: the fields computed, fixed at compile time (dipoles at run time)
+// POT / GRAD: the fields computed, fixed at compile time (dipoles at run time).
+// 128-thread CTAs are held to 4 (Helmholtz) / 5 (Laplace) resident per SM:
+// with the masked runs the compiler's own choice took 149 registers; the
+// caps measured best (FP32 Helmholtz pot+grad evaluation of 2e5 points:
+// 1.152 ms before the masking, 1.130 ms masked, 1.046 ms with 4 CTAs, 1.093
+// with 5; Laplace 0.615 / 0.564 / 0.566 / 0.544 ms)
 template <typename T, bool HELM, int NT, bool POT, bool GRAD>
-__global__ void __launch_bounds__(NT, NT == 32 ? 20 : 1)
+__global__ void __launch_bounds__(NT, NT == 32 ? 20 : (HELM ? 4 : 5))
 k_p2p(EvalParams<T> p) {
   constexpr bool F32 = sizeof(T) == 4;
   constexpr int NA = HELM ? 8 : 4;
@@ -895,21 +903,26 @@ k_p2p(EvalParams<T> p) {
       if (!active) continue;
       const int nt = (int)min((uint32_t)NT, total - f0);
       if constexpr (F32) {
+        // runs of kP2PRun pairs: a full run without bounds checks, the
+        // tile's last run with them; the cutoff by masking (p2p_pair)
+        auto pair_at = [&](int j, T* acc) {
+          const float2 cx = xp[j], cy = yp[j], cz = zp[j];
+          const T rx = (T)((txh - cx.x) + (txl - cx.y));
+          const T ry = (T)((tyh - cy.x) + (tyl - cy.y));
+          const T rz = (T)((tzh - cz.x) + (tzl - cz.y));
+          const T r2 = rx * rx + ry * ry + rz * rz;
+          p2p_pair<T, HELM, NT, POT, GRAD, true>(tl, j, rx, ry, rz, r2, k, kinv, hd, acc, rc2);
+        };
         for (int j0 = gl; j0 < nt; j0 += kP2PRun * G) {
           T acc[NA];
           for (int c = 0; c < NA; c++) acc[c] = T(0);
+          if (j0 + (kP2PRun - 1) * G < nt) {
 #pragma unroll
-          for (int u = 0; u < kP2PRun; u++) {
-            const int j = j0 + u * G;
-            if (j < nt) {
-              const float2 cx = xp[j], cy = yp[j], cz = zp[j];
-              const T rx = (T)((txh - cx.x) + (txl - cx.y));
-              const T ry = (T)((tyh - cy.x) + (tyl - cy.y));
-              const T rz = (T)((tzh - cz.x) + (tzl - cz.y));
-              const T r2 = rx * rx + ry * ry + rz * rz;
-              if (r2 > rc2)
-                p2p_pair<T, HELM, NT, POT, GRAD>(tl, j, rx, ry, rz, r2, k, kinv, hd, acc);
-            }
+            for (int u = 0; u < kP2PRun; u++) pair_at(j0 + u * G, acc);
+          } else {
+#pragma unroll
+            for (int u = 0; u < kP2PRun; u++)
+              if (j0 + u * G < nt) pair_at(j0 + u * G, acc);
           }
           for (int c = 0; c < NA; c++) a[c] += (double)acc[c];
         }
