@@ -12,8 +12,8 @@ points per leaf; seeded synthetic requests (the reference names no
 dataset).  One step = one batch of SERVE_BATCH requests.
 
 * `value`: the served form (SERVE_SLOTS solves at once, FP32 wherever the
-  FP32 range rule admits a request, FP64 otherwise, boxes without targets
-  skipped) on batches whose inputs and outputs are already in device memory
+  FP32 range rule admits a request, FP64 expansions with an FP32 near field
+  otherwise, boxes without targets skipped) on batches whose inputs and outputs are already in device memory
   (requests submitted with device arrays); points/s = sources of the batch /
   the batch's span from the first submission to the last completion (CUDA
   events, max over ranks).  W untimed batches, then K timed ones.
@@ -524,6 +524,12 @@ def served_section(args, ws, rank, local):
     def served_prec(p):
         ok = engine.fp32_range_ok(engine.SolverConfig.from_problem(p))
         return engine.FP32 if ok else engine.FP64
+    # the served form runs the requests that stay in FP64 with their near
+    # field in FP32 (FP64 expansions and L2P; near_fp32)
+    served_prec.near32 = True
+
+    def near32(precf, p):
+        return bool(getattr(precf, "near32", False)) and precf(p) == engine.FP64
 
     def plain_prec(p):
         return engine.FP64
@@ -535,7 +541,7 @@ def served_section(args, ws, rank, local):
         l0 = srv.stats()["kernel_launches"]
         e0.record(marker)
         tk = [srv.submit(p, precf(p), skip_empty=skip, leaf_order=skip,
-                         device=d if dbatch is not None else None)
+                         device=d if dbatch is not None else None, near_fp32=near32(precf, p))
               for p, d in zip(batch, dbatch if dbatch is not None else [None] * len(batch))]
         srv.drain()
         e1.record(marker)
@@ -597,7 +603,8 @@ def served_section(args, ws, rank, local):
         with engine.Server(slots=slots) as srv:
             run_batch(srv, warm[0], None, precf, skip)     # steady state: pools, tables
             base = srv.clock() + 0.02
-            tk = [srv.submit(p, precf(p), arrival=base + a, skip_empty=skip, leaf_order=skip)
+            tk = [srv.submit(p, precf(p), arrival=base + a, skip_empty=skip, leaf_order=skip,
+                             near_fp32=near32(precf, p))
                   for p, a in zip(lat_reqs, arr)]
             srv.drain()
             T = np.array([srv.times(t) for t in tk])

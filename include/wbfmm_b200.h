@@ -78,6 +78,10 @@ typedef struct {
                          FP32 arithmetic, as the reference's single-precision
                          build (its *_f API) computes them; points, origin
                          and width must then be FP32 values */
+  int near_fp32;      /* FP64 solvers, 1: the near field (P2P) in the FP32
+                         form's kernel (FP32 pair terms from FP64 positions,
+                         one FP64 add per run of 8 terms), the expansions and
+                         the L2P in FP64 */
 } wbfmm_b200_config_t;
 
 typedef struct wbfmm_b200_solver wbfmm_b200_solver_t;

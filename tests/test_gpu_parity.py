@@ -588,6 +588,32 @@ def test_target_bases(gpu_lib, case, precision):
     assert rel_l2(far, far_ref) < tol, rel_l2(far, far_ref)
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["laplace", "helmholtz_dipoles"])
+def test_fp64_with_fp32_near_field(gpu_lib, case):
+    """An FP64 solve with its near field in the FP32 form's kernel
+    (near_fp32) against the FP64 solve and the direct sum."""
+    if case == "laplace":
+        p = W.laplace_cube(20000, 2000, depth=4, order=12, seed=95)
+    else:
+        p = W.helmholtz_sphere(20000, 2000, k=8.0, depth=4, seed=96)
+    outs = {}
+    for near in (False, True):
+        cfg = engine.SolverConfig.from_problem(p, engine.FP64, near_fp32=near)
+        with engine.Solver(cfg) as s:
+            s.set_sources(p.xs, normals=p.normals)
+            s.set_strengths(p.q, dipoles=p.dipoles).set_targets(p.xt).run()
+            outs[near] = s.field()
+    for a, b in zip(outs[True], outs[False]):
+        assert rel_l2(a, b) < 2e-7, rel_l2(a, b)
+    idx = W.subsample(97, p.nt, 500)
+    dpot, dgrad = engine.direct(p.problem, p.xs, p.q, p.xt[idx], k=p.k, normals=p.normals,
+                                dipoles=p.dipoles)
+    w = 2 if p.problem == engine.HELMHOLTZ else 1
+    pot = outs[True][0].reshape(p.nt, w)[idx].ravel()
+    assert rel_l2(pot, dpot) < 1e-5
+
+
 def _edge_problem(case):
     rng = np.random.default_rng(71)
     if case == "coincident":

@@ -982,6 +982,28 @@ int launch_p2p(const EvalParams<T>& p, cudaStream_t s) {
   return 0;
 }
 
+// dst[i] = (float)src[i]; dst[i] += src[i] (FP64 solvers' FP32 near field)
+__global__ void k_narrow(const double* __restrict__ src, float* __restrict__ dst, int64_t n) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = (float)src[i];
+}
+__global__ void k_add_widened(double* __restrict__ dst, const float* __restrict__ src, int64_t n) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dst[i] += (double)src[i];
+}
+int launch_narrow(const double* src, float* dst, int64_t n, cudaStream_t s) {
+  if (n <= 0) return 0;
+  k_narrow<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(src, dst, n);
+  WBFMM_CUDA(cudaGetLastError());
+  return 0;
+}
+int launch_add_widened(double* dst, const float* src, int64_t n, cudaStream_t s) {
+  if (n <= 0) return 0;
+  k_add_widened<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(dst, src, n);
+  WBFMM_CUDA(cudaGetLastError());
+  return 0;
+}
+
 // largest |sin| and |cos| errors of sincos_near and of sincosf against the
 // FP64 values at the same FP32 arguments x_i = i * xmax / n (one block;
 // err[0] ours, err[1] sincosf)

@@ -152,6 +152,9 @@ int tl_fill(const EvalParams<T>& p, const int64_t* off, uint32_t* src, T* wq, T*
 template <typename T, bool HELM>
 int tl_apply(const EvalParams<T>& p, const T* basis, const int64_t* off, const uint32_t* src,
              const T* wq, const T* wd, cudaStream_t s);
+// FP32 copies of FP64 arrays, and FP32 results added into FP64 ones
+int launch_narrow(const double* src, float* dst, int64_t n, cudaStream_t s);
+int launch_add_widened(double* dst, const float* src, int64_t n, cudaStream_t s);
 // self-test of the FP32 near-field sine/cosine (kernels.cu)
 int sincos_near_errors(double xmax, int n, double* host_err);
 

@@ -225,6 +225,8 @@ struct Solver : public wbfmm_b200_solver {
   // outputs (original order)
   DBuf<T> pot, grad;
   DBuf<T> hess_d, hess_g;           // Hessian: derived expansions, gradients
+  // near_fp32 (FP64 solvers): FP32 strengths, normals and near-field sums
+  DBuf<float> n32_q, n32_dip, n32_nx, n32_ny, n32_nz, n32_pot, n32_grad;
   // precomputed target bases (potential): CSR near-field weights, bases
   DBuf<int64_t> tl_off;
   DBuf<uint32_t> tl_src;
@@ -295,6 +297,7 @@ struct Solver : public wbfmm_b200_solver {
     f(tpts_in); f(tx); f(ty); f(tz); f(tkeys); f(tperm); f(tbox);
     f(tstart); f(tcount); f(flag); f(pot); f(grad); f(out64); f(hess_d); f(hess_g);
     f(tl_off); f(tl_src); f(tl_wq); f(tl_wd); f(tl_basis);
+    f(n32_q); f(n32_dip); f(n32_nx); f(n32_ny); f(n32_nz); f(n32_pot); f(n32_grad);
     f(H64); f(H); f(op_ith); f(op_dist); f(op_r); f(op_ph); f(op_ch);
     for (int i = 0; i < 3; i++) { f(lap64[i]); f(lap[i]); }
     f(partial); f(lin); f(lanes_part); f(act_scr); f(lapsr); f(hcx); f(smask); f(tc_part);
@@ -990,12 +993,59 @@ struct Solver : public wbfmm_b200_solver {
     if (ntgt <= 0) return set_error(WBFMM_B200_E_STATE, "set_targets first");
     EvalParams<T> e = eparams();
     launches += eval_neighbours ? 2 : 1;
-    if (helm) {
-      WBFMM_TRY((launch_l2p<T, true>(e, stream)));
-      return eval_neighbours ? launch_p2p<T, true>(e, stream) : 0;
+    if (helm) WBFMM_TRY((launch_l2p<T, true>(e, stream)));
+    else WBFMM_TRY((launch_l2p<T, false>(e, stream)));
+    if (!eval_neighbours) return 0;
+    if constexpr (sizeof(T) == 8)
+      if (cfg.near_fp32) return p2p_fp32(e);
+    return helm ? launch_p2p<T, true>(e, stream) : launch_p2p<T, false>(e, stream);
+  }
+
+  // FP64 solver, near_fp32: the near field in the FP32 form's P2P kernel on
+  // FP32 copies of the strengths and normals (positions stay FP64), its
+  // results added to the FP64 fields
+  int p2p_fp32(const EvalParams<T>& e) {
+    EvalParams<float> f;
+    memset(&f, 0, sizeof(f));
+    f.ntgt = e.ntgt; f.level = e.level; f.N = e.N;
+    f.x0 = e.x0; f.y0 = e.y0; f.z0 = e.z0; f.wb = e.wb;
+    f.k = (float)e.k;
+    f.tx = e.tx; f.ty = e.ty; f.tz = e.tz;
+    f.tperm = e.tperm; f.tbox = e.tbox; f.tstart = e.tstart; f.tcount = e.tcount;
+    f.box_i = e.box_i; f.box_n = e.box_n;
+    f.x = e.x; f.y = e.y; f.z = e.z;
+    f.nbox = e.nbox;
+    const int w = helm ? 2 : 1;
+    const int64_t ns = nsrc, nt = ntgt;
+    auto narrow = [&](const T* src, DBuf<float>& dst, int64_t n, const float** out) -> int {
+      if (!src) { *out = nullptr; return 0; }
+      WBFMM_TRY(dst.alloc((size_t)n));
+      WBFMM_TRY(launch_narrow((const double*)src, dst.p, n, stream));
+      *out = dst.p;
+      return 0;
+    };
+    WBFMM_TRY(narrow(e.q, n32_q, ns * w, &f.q));
+    WBFMM_TRY(narrow(e.dip, n32_dip, ns * w, &f.dip));
+    if (e.dip) {
+      WBFMM_TRY(narrow(e.nx, n32_nx, ns, &f.nx));
+      WBFMM_TRY(narrow(e.ny, n32_ny, ns, &f.ny));
+      WBFMM_TRY(narrow(e.nz, n32_nz, ns, &f.nz));
     }
-    WBFMM_TRY((launch_l2p<T, false>(e, stream)));
-    return eval_neighbours ? launch_p2p<T, false>(e, stream) : 0;
+    if (e.pot) {
+      WBFMM_TRY(n32_pot.alloc((size_t)(nt * w)));
+      WBFMM_CUDA(cudaMemsetAsync(n32_pot.p, 0, sizeof(float) * nt * w, stream));
+      f.pot = n32_pot.p;
+    }
+    if (e.grad) {
+      WBFMM_TRY(n32_grad.alloc((size_t)(nt * 3 * w)));
+      WBFMM_CUDA(cudaMemsetAsync(n32_grad.p, 0, sizeof(float) * nt * 3 * w, stream));
+      f.grad = n32_grad.p;
+    }
+    WBFMM_TRY((helm ? launch_p2p<float, true>(f, stream) : launch_p2p<float, false>(f, stream)));
+    if (e.pot) WBFMM_TRY(launch_add_widened((double*)e.pot, n32_pot.p, nt * w, stream));
+    if (e.grad) WBFMM_TRY(launch_add_widened((double*)e.grad, n32_grad.p, nt * 3 * w, stream));
+    launches += 2 + (e.q ? 1 : 0) + (e.dip ? 4 : 0) + (e.pot ? 1 : 0) + (e.grad ? 1 : 0);
+    return 0;
   }
 
   int run() override {

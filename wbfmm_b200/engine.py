@@ -46,6 +46,7 @@ class Config(C.Structure):
         ("k", C.c_double), ("x0", C.c_double * 3), ("D", C.c_double),
         ("precision", C.c_int), ("field", C.c_int), ("skip_empty", C.c_int),
         ("managed", C.c_int), ("leaf_order", C.c_int), ("keys_fp32", C.c_int),
+        ("near_fp32", C.c_int),
     ]
 
 
@@ -171,6 +172,7 @@ class SolverConfig:
     skip_empty: bool = False
     managed: bool = False
     leaf_order: bool = False
+    near_fp32: bool = False
 
     def to_c(self) -> Config:
         c = Config()
@@ -188,14 +190,15 @@ class SolverConfig:
         c.skip_empty = int(bool(self.skip_empty))
         c.managed = int(bool(self.managed))
         c.leaf_order = int(bool(self.leaf_order))
+        c.near_fp32 = int(bool(self.near_fp32))
         return c
 
     @staticmethod
     def from_problem(p, precision=FP64, field=POTENTIAL | GRADIENT,
-                     skip_empty=False, leaf_order=False) -> "SolverConfig":
+                     skip_empty=False, leaf_order=False, near_fp32=False) -> "SolverConfig":
         return SolverConfig(p.problem, p.depth, list(p.order_s), list(p.order_r),
                             p.k, tuple(p.x0), p.D, precision, field, skip_empty,
-                            False, leaf_order)
+                            False, leaf_order, near_fp32)
 
 
 class Solver:
@@ -503,15 +506,17 @@ class Server:
 
     def submit(self, p, precision=FP32, field=POTENTIAL | GRADIENT,
                arrival: float = 0.0, skip_empty: bool = False,
-               leaf_order: bool = False, device: dict | None = None) -> int:
+               leaf_order: bool = False, device: dict | None = None,
+               near_fp32: bool = False) -> int:
         """Queue one solve; skip_empty: no local expansions for boxes
         without targets (the fields at the targets are unchanged);
-        leaf_order: sources sorted by leaf box only.  With ``device`` (a dict
+        leaf_order: sources sorted by leaf box only; near_fp32: an FP64
+        solve with its near field in FP32.  With ``device`` (a dict
         of device arrays -- objects with ``data_ptr()`` -- under the keys
         xs, q, normals, dipoles, xt, pot, grad, absent or None where unused)
         the request reads and writes those instead of host arrays; the
         caller keeps them alive until the request completes."""
-        cfg = SolverConfig.from_problem(p, precision, field, skip_empty, leaf_order)
+        cfg = SolverConfig.from_problem(p, precision, field, skip_empty, leaf_order, near_fp32)
         w = 2 if p.problem == HELMHOLTZ else 1
         if device is not None:
             d = {k: device.get(k) for k in ("xs", "q", "normals", "dipoles", "xt", "pot", "grad")}
