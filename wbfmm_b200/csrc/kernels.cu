@@ -67,6 +67,12 @@ static size_t l2p_row_bytes(int N, bool helm, bool grad, int threads) {
 // orders, FP64) the rows stay in per-thread local arrays, where occupancy
 // is worth more than the shorter latency
 constexpr size_t kRowSmemMax = 48 * 1024;
+constexpr int kL2PBoxes = 4;     // leaf boxes whose expansions an L2P CTA stages
+#define WBFMM_TRY_K(call)          \
+  do {                             \
+    const int rc_ = (call);        \
+    if (rc_) return rc_;           \
+  } while (0)
 
 // SROWS: recursion rows in shared memory (else per-thread local arrays)
 template <typename T, bool HELM, bool SROWS>
@@ -561,9 +567,14 @@ __host__ __device__ inline size_t l2p_table_bytes(int N) {
 // one thread per target (sorted by box); potential and gradient in one sweep
 // SROWS: recursion rows in shared memory, after the tables (else
 // per-thread local arrays)
-template <typename T, bool HELM, bool SROWS>
+// stage: the CTA's leaf expansions copied to shared memory when its targets
+// fall in at most kL2PBoxes leaf boxes (targets are sorted by box)
+template <typename T, bool HELM, bool SROWS, bool STAGE>
 __global__ void k_l2p(EvalParams<T> p, int tab, int legt) {
+  const int stage = STAGE ? 1 : 0;
   extern __shared__ __align__(16) unsigned char l2p_sm[];
+  __shared__ unsigned s_bal[32];
+  __shared__ int64_t s_box[kL2PBoxes];
   T* st = (T*)l2p_sm;
   const int N = p.N;
   const int W = 2 * N + 3, M0 = N + 1;
@@ -571,6 +582,7 @@ __global__ void k_l2p(EvalParams<T> p, int tab, int legt) {
   const int LW = N + 3;
   T* lt = st + (tab ? l2p_table_bytes<T, HELM>(N) / sizeof(T) : 0);
   T* rows = lt + (legt ? 4 * LW * LW : 0);
+  T* cst = rows + (SROWS ? (size_t)l2p_rows(HELM, p.grad != nullptr) * (N + kRowPad) * blockDim.x : 0);
   T loc[SROWS ? 1 : 3 * kPtMax];
   const Scratch<T> sc = SROWS ? Scratch<T>{rows + threadIdx.x, N + kRowPad, (int)blockDim.x}
                               : Scratch<T>{loc, N + kRowPad, 1};
@@ -594,8 +606,33 @@ __global__ void k_l2p(EvalParams<T> p, int tab, int legt) {
       }
     }
   }
-  if (tab || legt) __syncthreads();
   const int jt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nc = ncoef(N), wc = HELM ? 2 : 1;
+  int slot = -1;
+  if (stage) {
+    const int j0 = blockIdx.x * blockDim.x;
+    const bool in = jt < p.ntgt;
+    const bool first = in && (jt == j0 || p.tbox[jt] != p.tbox[jt - 1]);
+    const int nb = __syncthreads_count(first);
+    if (nb <= kL2PBoxes) {
+      const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+      const unsigned bal = __ballot_sync(0xffffffffu, first);
+      if (lane == 0) s_bal[warp] = bal;
+      __syncthreads();
+      int before = __popc(bal & ((1u << lane) - 1u));
+      for (int w = 0; w < warp; w++) before += __popc(s_bal[w]);
+      slot = before + (first ? 1 : 0) - 1;
+      if (first) s_box[slot] = p.tbox[jt];
+      __syncthreads();
+      for (int i = threadIdx.x; i < nb * nc; i += blockDim.x) {
+        const int k = i / nc, c = i - k * nc;
+        const int64_t o = layout_off(s_box[k], c, nc);
+        for (int u = 0; u < wc; u++) cst[(size_t)i * wc + u] = p.mpr[wc * o + u];
+      }
+      if (!in) slot = -1;
+    }
+  }
+  if (tab || legt || stage) __syncthreads();
   if (jt >= p.ntgt) return;
   const int64_t b = p.tbox[jt];
   double cd[3];
@@ -604,10 +641,12 @@ __global__ void k_l2p(EvalParams<T> p, int tab, int legt) {
   const T xc[3] = {T(0), T(0), T(0)};
   const T xf[3] = {(T)(p.tx[jt] - cd[0]), (T)(p.ty[jt] - cd[1]),
                    (T)(p.tz[jt] - cd[2])};
-  const int nc = ncoef(N);
   const uint32_t o = p.tperm[jt];
+  // the staged copy, or (a CTA whose targets span more boxes) null
+  const T* mine = STAGE && slot >= 0 ? cst + (size_t)slot * nc * wc : nullptr;
   if (HELM) {
     auto coef = [&](int idx, T* re, T* im) {
+      if (STAGE && mine) { *re = mine[2 * idx]; *im = mine[2 * idx + 1]; return; }
       int64_t off = layout_off(b, idx, nc);
       *re = p.mpr[2 * off]; *im = p.mpr[2 * off + 1];
     };
@@ -631,7 +670,9 @@ __global__ void k_l2p(EvalParams<T> p, int tab, int legt) {
     };
     if (legt) eval(LegTab<T>{lt, LW}); else eval(LegDirect<T>());
   } else {
-    auto coef = [&](int idx) -> T { return p.mpr[layout_off(b, idx, nc)]; };
+    auto coef = [&](int idx) -> T {
+      return STAGE && mine ? mine[idx] : p.mpr[layout_off(b, idx, nc)];
+    };
     auto eval = [&](const auto& leg) {
       if (p.grad) {
         T g[3] = {T(0), T(0), T(0)}, f = T(0);
@@ -659,14 +700,20 @@ int launch_l2p(const EvalParams<T>& p, cudaStream_t s) {
   const size_t lg = leg_table_bytes<T>(p.N);
   const size_t rows = l2p_row_bytes<T>(p.N, HELM, p.grad != nullptr, 128);
   const unsigned grid = (unsigned)((p.ntgt + 127) / 128);
+  // staged leaf expansions: up to kL2PBoxes per CTA within 32 KB
+  const size_t cb = (size_t)kL2PBoxes * ncoef(p.N) * (HELM ? 2 : 1) * sizeof(T);
+  const int stage = cb <= 32 * 1024 ? 1 : 0;
+  auto go = [&](auto srows, auto stg) -> int {
+    constexpr bool SR = decltype(srows)::value, ST = decltype(stg)::value;
+    const size_t bytes = sm + lg + (SR ? rows : 0) + (ST ? cb : 0);
+    if (bytes > 48 * 1024) WBFMM_SMEM(bytes, k_l2p<T, HELM, SR, ST>);
+    k_l2p<T, HELM, SR, ST><<<grid, 128, bytes, s>>>(p, sm ? 1 : 0, lg ? 1 : 0);
+    return 0;
+  };
   if (rows <= kRowSmemMax) {
-    if (sm + lg + rows > 48 * 1024)
-      WBFMM_SMEM((sm + lg + rows), k_l2p<T, HELM, true>);
-    k_l2p<T, HELM, true><<<grid, 128, sm + lg + rows, s>>>(p, sm ? 1 : 0, lg ? 1 : 0);
+    WBFMM_TRY_K(stage ? go(std::true_type(), std::true_type()) : go(std::true_type(), std::false_type()));
   } else {
-    if (sm + lg > 48 * 1024)
-      WBFMM_SMEM((sm + lg), k_l2p<T, HELM, false>);
-    k_l2p<T, HELM, false><<<grid, 128, sm + lg, s>>>(p, sm ? 1 : 0, lg ? 1 : 0);
+    WBFMM_TRY_K(stage ? go(std::false_type(), std::true_type()) : go(std::false_type(), std::false_type()));
   }
   WBFMM_CUDA(cudaGetLastError());
   return 0;
