@@ -30,7 +30,11 @@ dataset).  One step = one batch of SERVE_BATCH requests.
   `served_p50_s` / `served_p99_s` / `plain_p50_s` / `plain_p99_s` are at 70%.
 * accuracy: the served fields of sampled requests against the FP64 GPU
   direct sum (itself pinned to the reference's direct sums).
-* `roofline`: the tile M2L (the stream's dominant M2L kernel) on a Laplace
+* `roofline`: the FP32 near field (the stream's dominant kernel, k_p2p,
+  41% of its device time) on a 2e5-point Helmholtz cube: algorithmic FLOPs
+  of the exact pair count / event time, against the FP32 FMA peak measured
+  live, DRAM traffic from its committed ncu capture.  `roofline_m2l`: the
+  tile M2L (the stream's dominant M2L kernel) on a Laplace
   order-14 level, against the FP32 FMA peak measured live on the GPU
   (`wbfmm_b200_fp32_fma_peak`); `traffic` from the committed ncu capture of
   the same launch.
@@ -821,11 +825,14 @@ def single_solve_section(args, ws, rank, local, p, n_acc, acc_seed, skip_empty, 
 
 
 # -------------------------------------------------------------- roofline
-def tile_profile_traffic():
-    """DRAM bytes (read + write) of the tile M2L launch in the committed ncu
-    capture of the roofline case, or None."""
+P2P_PROFILE = os.path.join(ROOT, "profiles", "k_p2p_helmholtz_2e5.md")
+
+
+def tile_profile_traffic(path=None):
+    """DRAM bytes (read + write) of the launch in a committed ncu capture
+    (default: the tile M2L roofline case), or None."""
     try:
-        text = open(TILE_PROFILE).read()
+        text = open(path or TILE_PROFILE).read()
     except OSError:
         return None
     tot = 0.0
@@ -890,6 +897,79 @@ def tile_roofline(local):
             "frac_of_bf16_tensor_peak": (achieved / bf16) if bf16 else None}
 
 
+def p2p_pairs(s, depth):
+    """(target, source) pairs of the near field with targets = sources:
+    every point against the points of its leaf's 27 neighbours, less the
+    self pairs (the r > 1e-6 cutoff)."""
+    from wbfmm_b200 import engine
+    _, bi, bn = s.tree(depth)
+    n = 1 << depth
+    idx = np.arange(8 ** depth, dtype=np.uint64)
+    def gather(v):
+        r = np.zeros(idx.shape, dtype=np.int64)
+        for b in range(depth):
+            r |= ((v >> np.uint64(3 * b)) & np.uint64(1)).astype(np.int64) << b
+        return r
+    i, j, k = gather(idx), gather(idx >> np.uint64(1)), gather(idx >> np.uint64(2))
+    grid = np.zeros((n, n, n), dtype=np.int64)
+    grid[i, j, k] = bn.astype(np.int64)
+    pad = np.pad(grid, 1)
+    nsum = sum(pad[1 + a:1 + a + n, 1 + b:1 + b + n, 1 + c:1 + c + n]
+               for a in (-1, 0, 1) for b in (-1, 0, 1) for c in (-1, 0, 1))
+    return int((grid * nsum).sum() - bn.astype(np.int64).sum())
+
+
+def p2p_roofline(local):
+    """The served stream's dominant kernel (the FP32 near field, Helmholtz
+    potential and gradient, 44 flops per pair with each MUFU operation counted
+    once): 2e5 points, depth 4, k = 10; its time is the evaluation's minus the
+    L2P's (CUDA events, L2 flushed before each), against the FP32 FMA peak
+    measured here."""
+    import torch
+
+    from wbfmm_b200 import engine
+
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(dev)
+    peak = engine.fp32_fma_peak()
+    p = _cube(engine.HELMHOLTZ, 200_000, 4, 8, k=10.0)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    cfg = engine.SolverConfig.from_problem(p, engine.FP32)
+
+    def timed(s):
+        times = []
+        for i in range(6):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            a.record(stream)
+            s.evaluate()
+            b.record(stream)
+            torch.cuda.synchronize(dev)
+            if i:
+                times.append(a.elapsed_time(b))
+        return float(np.mean(times))
+    with engine.Solver(cfg, stream=stream.cuda_stream) as s:
+        s.set_sources(p.xs).set_strengths(p.q).set_targets(p.xt).run()
+        pairs = p2p_pairs(s, 4)
+        both = timed(s)
+        s.set_evaluation(engine.POTENTIAL | engine.GRADIENT, neighbours=False)
+        l2p = timed(s)
+    ms = both - l2p
+    flops = pairs * 44
+    achieved = flops / (ms * 1e-3) / 1e12
+    return {"bound": "simt", "kernel": "k_p2p<float, Helmholtz> potential + gradient: near field "
+                                       "of 200,000 points, depth 4 (41% of the served stream's "
+                                       "device time)",
+            "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+            "peak_source": "FP32 FMA throughput measured live (wbfmm_b200_fp32_fma_peak)",
+            "traffic": tile_profile_traffic(P2P_PROFILE),
+            "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of the same launch, "
+                              "profiles/k_p2p_helmholtz_2e5.md",
+            "pairs_per_launch": pairs, "algorithmic_flops_per_launch": flops,
+            "ms_per_launch": ms, "gpairs_per_s": pairs / (ms * 1e-3) / 1e9}
+
+
 # ----------------------------------------------------------- our arm
 def our_arm(args, ws, rank, local):
     import torch
@@ -949,7 +1029,8 @@ def our_arm(args, ws, rank, local):
                                     label, min(args.steps, 5))
         for k in ("fp32", "fp64"):
             cube[k].pop("step_ms", None)
-    roofline = tile_roofline(local)
+    roofline = p2p_roofline(local)
+    roofline_m2l = tile_roofline(local)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         from oracle.oracle_api import have_reference
@@ -977,7 +1058,7 @@ def our_arm(args, ws, rank, local):
         "e2e": {"value": sh["points_per_s"], "unit": "points/s", "ms_per_step": sh["ms_per_step"],
                 "h2d_bytes_per_step": ws * served["bytes_per_step"]["h2d"],
                 "d2h_bytes_per_step": ws * served["bytes_per_step"]["d2h"]},
-        "roofline": roofline, "cpu_baseline": cpu,
+        "roofline": roofline, "roofline_m2l": roofline_m2l, "cpu_baseline": cpu,
         "gpu_launches": sd["kernel_launches_per_step"], "clocks": sd["clocks"],
         "served": served, "cube_c2": cube,
     }
