@@ -563,7 +563,10 @@ def served_section(args, ws, rank, local):
                 float(np.mean(T[:, 2] - T[:, 1])), float(np.mean(T[:, 3] - T[:, 2])))
 
     def run_arm(name, slots, precf, skip, device, keep=0):
-        with engine.Server(slots=slots) as srv:
+        # a batch is submitted at once: the served form's slots take its
+        # largest requests first (largest-first order); one slot runs the
+        # batch's solves one after another whatever the order
+        with engine.Server(slots=slots, largest_first=slots > 1) as srv:
             for b, d in zip(warm, dev_warm):
                 run_batch(srv, b, d if device else None, precf, skip)
             spans, launches, issue, wait = [], [], [], []
@@ -582,6 +585,7 @@ def served_section(args, ws, rank, local):
             return {"points_per_s": ws * pts / sum(spans), "seconds": sum(spans),
                     "ms_per_step": 1e3 * float(np.mean(spans)), "step_ms": [1e3 * s for s in spans],
                     "requests": len(batches) * SERVE_BATCH, "slots": slots, "skip_empty": skip,
+                    "order": "largest first" if slots > 1 else "arrival",
                     "inputs": "device" if device else "host",
                     "kernel_launches_per_step": int(np.mean(launches)),
                     "host_issue_ms_per_request": 1e3 * float(np.mean(issue)),
@@ -836,11 +840,15 @@ def tile_profile_traffic(path=None):
     except OSError:
         return None
     tot = 0.0
+    scale = {"byte": 1, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9}
     for key in ("dram__bytes_read.sum", "dram__bytes_write.sum"):
         for line in text.splitlines():
             if f"`{key}`" in line:
-                val, unit = line.split("|")[2].split()
-                tot += float(val) * {"byte": 1, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9}[unit]
+                try:
+                    val, unit = line.split("|")[2].split()
+                    tot += float(val) * scale[unit]
+                except (ValueError, KeyError, IndexError):
+                    return None
                 break
         else:
             return None

@@ -373,6 +373,11 @@ double wbfmm_b200_server_clock(wbfmm_b200_server_t *srv);
 int wbfmm_b200_server_submit(wbfmm_b200_server_t *srv,
                              const wbfmm_b200_request_t *req, int64_t *ticket);
 /* 1 when the request has completed, 0 when not yet */
+/* Order in which free slots take the requests that have arrived: 0 (the
+   default) first come first served; 1 the largest device-memory footprint
+   first (for batches submitted together: the big solves start first and the
+   small ones fill the end, which shortens the batch's span). */
+int wbfmm_b200_server_set_order(wbfmm_b200_server_t *srv, int largest_first);
 int wbfmm_b200_server_poll(wbfmm_b200_server_t *srv, int64_t ticket);
 /* blocks until the request has completed; returns its status */
 int wbfmm_b200_server_wait(wbfmm_b200_server_t *srv, int64_t ticket);

@@ -153,3 +153,30 @@ def test_failed_request_is_isolated(gpu_lib):
         for t in tickets:
             pot, grad = s.wait(t)
             assert np.all(np.isfinite(pot)) and np.all(np.isfinite(grad))
+
+
+@pytest.mark.gpu
+def test_largest_first_order(gpu_lib):
+    """With the largest-first order, a free slot takes the arrived request of
+    the largest footprint: on one slot, the requests queued behind the first
+    start in decreasing size, and every field is the one the arrival order
+    gives."""
+    rng = np.random.default_rng(31)
+    sizes = [3000, 9000, 5000, 20000, 12000, 7000]
+    reqs = [W.serve_request(rng, n, False, 0.0, False) for n in sizes]
+    for p in reqs:        # one tree shape, so that the footprint follows n
+        p.depth = 3
+        p.order_s = p.order_r = [0, 10, 10, 10]
+    out = {}
+    for lf in (False, True):
+        with E.Server(slots=1, largest_first=lf) as s:
+            tickets = [s.submit(p, E.FP64) for p in reqs]
+            s.drain()
+            starts = [s.times(t)[1] for t in tickets]
+            out[lf] = [[a.copy() for a in s.wait(t)] for t in tickets]
+        if lf:
+            queued = sorted(range(len(reqs)), key=lambda i: starts[i])[1:]
+            assert queued == sorted(queued, key=lambda i: -sizes[i]), (queued, starts)
+    for a, b in zip(out[False], out[True]):
+        for x, y in zip(a, b):
+            assert rel(y, x) <= 1e-12

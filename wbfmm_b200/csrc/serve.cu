@@ -6,7 +6,10 @@
 // a slot that falls free takes the oldest request whose arrival time has
 // passed, provided the device-memory footprints of the solves in flight plus
 // its own stay within the budget (first come, first served: a request that
-// does not fit yet holds back the ones behind it).  A slot queues the whole
+// does not fit yet holds back the ones behind it), or, with the
+// largest-first order, the largest of the requests that have arrived (a
+// batch submitted at once then runs its big solves first and its small ones
+// fill the tail).  A slot queues the whole
 // solve -- tree build, passes, evaluation, copy-back -- on its stream with no
 // host wait, then sleeps on a blocking event until the stream drains, so
 // up to S solves run on the device at once and their kernels overlap.
@@ -84,6 +87,7 @@ struct wbfmm_b200_server {
   };
 
   int device = 0;
+  int largest_first = 0;    // among arrived requests, the largest footprint first
   int64_t budget = 0;       // for the footprints of the solves in flight
   int64_t keep = 0;         // work buffers a slot may keep between solves
   cudaMemPool_t pool = nullptr;   // the solves' device memory
@@ -225,14 +229,18 @@ struct wbfmm_b200_server {
         for (;;) {
           if (stop && queue.empty()) return;
           if (!queue.empty()) {
-            Req* h = queue.front();
+            auto hi = queue.begin();
             double t = clock();
-            if (h->t_arrival > t) {
-              cv_work.wait_for(lk, std::chrono::duration<double>(h->t_arrival - t));
+            if ((*hi)->t_arrival > t) {
+              cv_work.wait_for(lk, std::chrono::duration<double>((*hi)->t_arrival - t));
               continue;
             }
+            if (largest_first)   // the largest of the requests that have arrived
+              for (auto it = queue.begin(); it != queue.end() && (*it)->t_arrival <= t; ++it)
+                if ((*it)->footprint > (*hi)->footprint) hi = it;
+            Req* h = *hi;
             if (inflight + h->footprint <= budget || running == 0) {
-              queue.pop_front();
+              queue.erase(hi);
               q = h;
               inflight += q->footprint;
               peak_inflight = std::max(peak_inflight, inflight);
@@ -353,6 +361,13 @@ int wbfmm_b200_server_submit(wbfmm_b200_server_t* srv,
     *ticket = q->id;
   }
   srv->cv_work.notify_all();
+  return 0;
+}
+
+int wbfmm_b200_server_set_order(wbfmm_b200_server_t* srv, int largest_first) {
+  if (!srv) return set_error(WBFMM_B200_E_ARG, "null server");
+  std::lock_guard<std::mutex> lk(srv->mu);
+  srv->largest_first = largest_first != 0;
   return 0;
 }
 

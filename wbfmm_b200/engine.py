@@ -121,6 +121,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "wbfmm_b200_server_clock": (C.c_double, [vp]),
         "wbfmm_b200_server_submit": (ip, [vp, C.POINTER(Request), C.POINTER(C.c_int64)]),
         "wbfmm_b200_server_poll": (ip, [vp, C.c_int64]),
+        "wbfmm_b200_server_set_order": (ip, [vp, ip]),
         "wbfmm_b200_server_wait": (ip, [vp, C.c_int64]),
         "wbfmm_b200_server_times": (ip, [vp, C.c_int64, dp]),
         "wbfmm_b200_server_forget": (ip, [vp, C.c_int64]),
@@ -477,10 +478,13 @@ class Server:
     the request completes, and its fields land in arrays this object owns.
     """
 
-    def __init__(self, slots: int = 16, hbm_budget: int = 150 * 10**9):
+    def __init__(self, slots: int = 16, hbm_budget: int = 150 * 10**9,
+                 largest_first: bool = False):
         self._lib = load_library()
         self._h = C.c_void_p()
         _check(self._lib.wbfmm_b200_server_create(C.byref(self._h), int(slots), int(hbm_budget)))
+        if largest_first:
+            _check(self._lib.wbfmm_b200_server_set_order(self._h, 1))
         self._held = {}
 
     def close(self):
