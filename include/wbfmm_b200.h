@@ -82,6 +82,17 @@ typedef struct {
                          form's kernel (FP32 pair terms from FP64 positions,
                          one FP64 add per run of 8 terms), the expansions and
                          the L2P in FP64 */
+  int sparse;         /* 1: sparse level storage: a level's coefficient arrays
+                         hold only the groups of eight sibling boxes whose
+                         parent holds sources or targets (implies skip_empty;
+                         not with managed; arrays sized after the targets are
+                         set, with one host wait).  The M2L runs the tile
+                         kernel (equal orders in [2, 60] per level); the
+                         Hessian, target bases, coefficient pointers and
+                         adopted arrays need dense storage, and
+                         wbfmm_b200_get_coefficients returns the dense
+                         Layout L arrays (zeros outside the stored groups).
+                         Not for served requests. */
 } wbfmm_b200_config_t;
 
 typedef struct wbfmm_b200_solver wbfmm_b200_solver_t;
@@ -217,6 +228,14 @@ int wbfmm_b200_get_coefficients(wbfmm_b200_solver_t *s, int level,
 /* device pointers of the level arrays (precision of the solver) */
 int wbfmm_b200_coefficient_pointers(wbfmm_b200_solver_t *s, int level,
                                     void **mps, void **mpr);
+/* Storage of the coefficient arrays: for level in [1, depth], the groups of
+   eight boxes stored (dense: 8^(level-1); sparse: those whose parent holds
+   sources or targets) and the device bytes of the level's two arrays;
+   level 0 gives the totals over every level.  Replaces reading the
+   reference's per-level allocation (src/boxes.c:518-583), which is always
+   dense. */
+int wbfmm_b200_coefficient_storage(wbfmm_b200_solver_t *s, int level,
+                                   int64_t *groups, int64_t *bytes);
 /* per-stage device times of the last run (ms): tree, operators, P2M,
    upward, downward, evaluation */
 int wbfmm_b200_stage_times(wbfmm_b200_solver_t *s, double *ms6);

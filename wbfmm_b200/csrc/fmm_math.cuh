@@ -55,6 +55,19 @@ HD int64_t layout_off(int64_t b, int c, int nc) {
   return ((b >> 3) * (int64_t)nc + c) * 8 + (b & 7);
 }
 
+// Sparse level storage keeps only the groups of eight boxes whose parent
+// holds sources or targets, each group still in Layout L, at consecutive
+// slots in Morton order; gmap[group] is the group's slot, kNoGroup for a
+// group not stored.  The compact index of box b is 8 slot + (b & 7) (-1
+// when its group is not stored; dense storage, gmap null: b), and
+// layout_off of the compact index addresses its coefficients.
+constexpr uint32_t kNoGroup = 0xffffffffu;
+HD int64_t compact_box(const uint32_t* gmap, int64_t b) {
+  if (!gmap) return b;
+  const uint32_t g = gmap[b >> 3];
+  return g == kNoGroup ? -1 : (((int64_t)g << 3) | (b & 7));
+}
+
 // Morton interleave, x in bit 0 (src/boxes.c:279-322)
 HD uint64_t spread3(uint64_t v) {
   v &= 0x1fffffull;

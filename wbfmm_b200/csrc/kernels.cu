@@ -87,8 +87,10 @@ __global__ void k_p2m(P2MParams<T> p, int legt) {
     leg_table_fill(lt, p.N + 2, threadIdx.x, blockDim.x);
     __syncthreads();
   }
-  const int64_t b = (int64_t)blockIdx.x * nw + warp;
-  if (b >= p.nbox) return;   // whole warp leaves; no block barriers below
+  // the box's storage index, and (sparse storage) its Morton index
+  const int64_t cb = (int64_t)blockIdx.x * nw + warp;
+  if (cb >= p.nbox) return;   // whole warp leaves; no block barriers below
+  const int64_t b = p.glist ? (((int64_t)p.glist[cb >> 3] << 3) | (cb & 7)) : cb;
   const int nc = ncoef(p.N);
   const int w = HELM ? 2 : 1;
   const int RL = p.N + kRowPad;
@@ -151,7 +153,7 @@ __global__ void k_p2m(P2MParams<T> p, int legt) {
   }
   __syncwarp();
   for (int c = lane; c < nc; c += 32) {
-    int64_t o = layout_off(b, c, nc);
+    int64_t o = layout_off(cb, c, nc);
     if (HELM) {
       if (p.accumulate) {
         p.mps[2 * o] += acc[2 * c];
@@ -444,7 +446,10 @@ __global__ void k_m2m(XlateParams<T> p, OpTables<T> t) {
   T* acc = B + 2 * V;
   T* tp = (T*)smraw + (size_t)nw * 6 * V;
   const int tpn = Nc + Np + 2;
+  // the children's group (dense: the parent box); the parent's storage index
   const int64_t P = blockIdx.x;
+  const int64_t Pout = p.glist ? compact_box(p.gmap, (int64_t)p.glist[P]) : P;
+  if (Pout < 0) return;   // (a stored group's parent is stored) whole CTA, before any barrier
   const int outlen = vlen<HELM>(Np);
   for (int c = lane; c < 2 * outlen; c += 32) acc[c] = T(0);
   if (!HELM && threadIdx.x == 0) {
@@ -470,7 +475,7 @@ __global__ void k_m2m(XlateParams<T> p, OpTables<T> t) {
     red[c] = v;   // entries c of warp 0's A are read only by this thread
   }
   __syncthreads();
-  store_vec<T, HELM, false>(p.cout, P, Np, ncoef(Np), red, threadIdx.x,
+  store_vec<T, HELM, false>(p.cout, Pout, Np, ncoef(Np), red, threadIdx.x,
                             blockDim.x);
 }
 
@@ -503,7 +508,10 @@ __global__ void k_l2l(XlateParams<T> p, OpTables<T> t) {
   T* out = B + 2 * V;
   T* tp = (T*)smraw + (size_t)nw * 6 * V;
   const int tpn = Nc + Np + 2;
+  // the children's group (dense: the parent box); the parent's storage index
   const int64_t P = blockIdx.x;
+  const int64_t Pin = p.glist ? compact_box(p.gmap, (int64_t)p.glist[P]) : P;
+  if (Pin < 0) return;    // (a stored group's parent is stored) whole CTA, before any barrier
   if (!HELM && threadIdx.x == 0) {
     T r = p.width * (T)t.op_r[kOpL2L];
     tp[0] = T(1);
@@ -512,7 +520,7 @@ __global__ void k_l2l(XlateParams<T> p, OpTables<T> t) {
   __syncthreads();
   const int ncp = ncoef(Np), ncc = ncoef(Nc);
   for (int ch = warp; ch < 8; ch += nw) {
-    load_vec<T, HELM>(A, p.cin, P, Np, ncp, lane);
+    load_vec<T, HELM>(A, p.cin, Pin, Np, ncp, lane);
     __syncwarp();
     shift_vec<T, HELM, false, false>(A, B, out, Np, Nc, kOpL2L + ch, t, p.coax,
                                      tp, 2, lane);
@@ -622,10 +630,14 @@ __global__ void k_l2p(EvalParams<T> p, int tab, int legt) {
       int before = __popc(bal & ((1u << lane) - 1u));
       for (int w = 0; w < warp; w++) before += __popc(s_bal[w]);
       slot = before + (first ? 1 : 0) - 1;
-      if (first) s_box[slot] = p.tbox[jt];
+      if (first) s_box[slot] = compact_box(p.gmap, (int64_t)p.tbox[jt]);
       __syncthreads();
       for (int i = threadIdx.x; i < nb * nc; i += blockDim.x) {
         const int k = i / nc, c = i - k * nc;
+        if (s_box[k] < 0) {   // (targets lie in stored groups)
+          for (int u = 0; u < wc; u++) cst[(size_t)i * wc + u] = T(0);
+          continue;
+        }
         const int64_t o = layout_off(s_box[k], c, nc);
         for (int u = 0; u < wc; u++) cst[(size_t)i * wc + u] = p.mpr[wc * o + u];
       }
@@ -635,6 +647,8 @@ __global__ void k_l2p(EvalParams<T> p, int tab, int legt) {
   if (tab || legt || stage) __syncthreads();
   if (jt >= p.ntgt) return;
   const int64_t b = p.tbox[jt];
+  const int64_t cb = compact_box(p.gmap, b);   // storage index
+  if (cb < 0) return;   // (targets lie in stored groups) no barriers below
   double cd[3];
   box_centre(b, p.x0, p.y0, p.z0, p.wb, cd);
   // target position relative to the box centre, formed in FP64
@@ -647,7 +661,7 @@ __global__ void k_l2p(EvalParams<T> p, int tab, int legt) {
   if (HELM) {
     auto coef = [&](int idx, T* re, T* im) {
       if (STAGE && mine) { *re = mine[2 * idx]; *im = mine[2 * idx + 1]; return; }
-      int64_t off = layout_off(b, idx, nc);
+      int64_t off = layout_off(cb, idx, nc);
       *re = p.mpr[2 * off]; *im = p.mpr[2 * off + 1];
     };
     auto eval = [&](const auto& leg) {
@@ -671,7 +685,7 @@ __global__ void k_l2p(EvalParams<T> p, int tab, int legt) {
     if (legt) eval(LegTab<T>{lt, LW}); else eval(LegDirect<T>());
   } else {
     auto coef = [&](int idx) -> T {
-      return STAGE && mine ? mine[idx] : p.mpr[layout_off(b, idx, nc)];
+      return STAGE && mine ? mine[idx] : p.mpr[layout_off(cb, idx, nc)];
     };
     auto eval = [&](const auto& leg) {
       if (p.grad) {

@@ -46,6 +46,9 @@ struct P2MParams {
   const T* nx; const T* ny; const T* nz;   // sorted normals (dipoles)
   T* mps;             // leaf level, Layout L
   int accumulate;     // 1: add to the existing coefficients
+  // sparse storage: slot -> group (parent box) of the leaf level; boxes are
+  // then the compact indices 8 slot + child (nbox = 8 x slots), or null
+  const uint32_t* glist = nullptr;
 };
 
 template <typename T>
@@ -66,6 +69,7 @@ struct EvalParams {
   T* pot;    // [ntgt] or [2 ntgt] (original order), may be null
   T* grad;   // [3 ntgt] or [6 ntgt], may be null
   int64_t nbox;
+  const uint32_t* gmap = nullptr;   // sparse storage: leaf group -> slot, or null
 };
 
 template <typename T>
@@ -84,6 +88,11 @@ struct XlateParams {
   T* partial;              // M2L split: [nsplit][nbox][2*ncout]
   const uint8_t* tmask;    // M2L: only targets with tmask[b] != 0, or null
   int lap_e;               // Laplace M2L scale exponent (lap_scale_exp)
+  // sparse storage (M2M, L2L): one CTA per slot of the child level
+  // (nbox = its slots), glist its slot -> group (the parent box), gmap the
+  // parent level's group -> slot; both null for dense storage
+  const uint32_t* glist;
+  const uint32_t* gmap;
 };
 
 // Laplace M2L scale exponent of a level of box width w: e = -ilogb(w), so
@@ -157,5 +166,18 @@ int launch_narrow(const double* src, float* dst, int64_t n, cudaStream_t s);
 int launch_add_widened(double* dst, const float* src, int64_t n, cudaStream_t s);
 // self-test of the FP32 near-field sine/cosine (kernels.cu)
 int sincos_near_errors(double xmax, int n, double* host_err);
+// sparse level storage (sparse.cu): the group map of a level from the n
+// boxes of the level above (stored: box_n != 0 or tmask set; tmask may be
+// null): gmap[g] = slot or kNoGroup, *count = stored groups (device);
+// scratch of sparse_scan_scratch(n) bytes; then the slot -> group list, and
+// a compact array expanded to the dense Layout L array (zeros elsewhere)
+size_t sparse_scan_scratch(int64_t n);
+int sparse_group_map(const uint32_t* box_n, const uint8_t* tmask, int64_t n, uint32_t* flag,
+                     uint32_t* gmap, uint32_t* count, void* scratch, size_t scratch_bytes,
+                     cudaStream_t s);
+int sparse_group_list(const uint32_t* gmap, int64_t n, uint32_t* glist, cudaStream_t s);
+template <typename T>
+int sparse_expand(const T* compact, const uint32_t* glist, int64_t groups, int64_t glen,
+                  T* dense, int64_t dense_len, cudaStream_t s);
 
 }  // namespace wbfmm

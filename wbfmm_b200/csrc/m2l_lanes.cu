@@ -92,6 +92,63 @@ __global__ void k_to_lin(const T* __restrict__ arr, int level, int N, int scale_
   else lin[((int64_t)tau * V + c) * npp + pp] = v;
 }
 
+// sparse storage: compact level array -> lin[tau][c][slot], slot in
+// [0, groups] (slot `groups` zero), degree n scaled by 2^(scale_e n)
+template <typename T, bool HELM>
+__global__ void k_to_lin_groups(const T* __restrict__ arr, int64_t groups, int N, int scale_e,
+                                typename V2t<T>::t* __restrict__ lin) {
+  typedef typename V2t<T>::t T2;
+  const int V = HELM ? (N + 1) * (N + 1) : (N + 1) * (N + 2) / 2;
+  const int nc = (N + 1) * (N + 1);
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (groups + 1) * V * 8) return;
+  const int tau = (int)(e & 7);
+  const int c = (int)((e >> 3) % V);
+  const int64_t slot = (e >> 3) / V;
+  T2 v;
+  v.x = T(0); v.y = T(0);
+  if (slot < groups) {
+    const int64_t b = (slot << 3) | tau;
+    int n;
+    if (HELM) {
+      const int64_t o = layout_off(b, c, nc);
+      v.x = arr[2 * o]; v.y = arr[2 * o + 1];
+      n = full_degree(c);
+    } else {
+      n = half_degree(c);
+      const int m = c - n * (n + 1) / 2;
+      if (m == 0) {
+        v.x = arr[layout_off(b, n * n, nc)];
+      } else {
+        const int id = lidx(n, m);
+        v.x = arr[layout_off(b, id, nc)]; v.y = arr[layout_off(b, id + 1, nc)];
+      }
+    }
+    if (scale_e) {
+      v.x = scale2(v.x, scale_e * n);
+      v.y = scale2(v.y, scale_e * n);
+    }
+  }
+  lin[((int64_t)tau * V + c) * (groups + 1) + slot] = v;
+}
+
+// pmap[pp]: slot of the padded-grid parent pp, `groups` on the padding and
+// where the parent's group is not stored
+__global__ void k_parent_slot_map(const uint32_t* __restrict__ gmap, int nx, int64_t npp,
+                                  uint32_t groups, uint32_t* __restrict__ pmap) {
+  const int64_t pp = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (pp >= npp) return;
+  const int npx = nx + 2;
+  const int px = (int)(pp % npx) - 1, py = (int)((pp / npx) % npx) - 1,
+            pz = (int)(pp / ((int64_t)npx * npx)) - 1;
+  uint32_t v = groups;
+  if (px >= 0 && px < nx && py >= 0 && py < nx && pz >= 0 && pz < nx) {
+    const uint32_t g = gmap[morton(px, py, pz)];
+    if (g != kNoGroup) v = g;
+  }
+  pmap[pp] = v;
+}
+
 // --------------------------------------------------------------- kernel
 // compiler-only memory fence: keeps the unrolled per-degree blocks from
 // being hoisted into one another (bounds register live ranges)
@@ -516,8 +573,11 @@ __global__ void k_lanes_reduce(LanesParams<T> p, int N) {
   const int c = (int)((e / np) % V);
   const int tau = (int)(e / (np * V));
   int px = (int)(plin % nx), py = (int)((plin / nx) % nx), pz = (int)(plin / ((int64_t)nx * nx));
-  const int64_t b = ((int64_t)morton(px, py, pz) << 3) | tau;
-  if (p.tmask && !p.tmask[b]) return;
+  const int64_t pm = (int64_t)morton(px, py, pz);
+  if (p.tmask && !p.tmask[(pm << 3) | tau]) return;
+  const int64_t g0 = compact_box(p.gmap, pm << 3);
+  if (g0 < 0) return;
+  const int64_t b = g0 | tau;   // storage index
   T sx = T(0), sy = T(0);
   for (int s = 0; s < p.nsplit; s++) {
     T2 v = ((const T2*)p.partial_raw)[(((int64_t)s * 8 + tau) * V + c) * np + plin];
@@ -671,6 +731,32 @@ int lanes_to_lin(const T* arr, int level, int N, int scale_e, void* lin, cudaStr
   return 0;
 }
 
+template <typename T, bool HELM>
+int lanes_to_lin_groups(const T* arr, int64_t groups, int N, int scale_e, void* lin,
+                        cudaStream_t s) {
+  typedef typename V2t<T>::t T2;
+  const int V = HELM ? (N + 1) * (N + 1) : (N + 1) * (N + 2) / 2;
+  const int64_t tot = (groups + 1) * V * 8;
+  k_to_lin_groups<T, HELM><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(arr, groups, N, scale_e,
+                                                                         (T2*)lin);
+  WBFMM_CUDA(cudaGetLastError());
+  return 0;
+}
+
+size_t lanes_lin_groups_bytes(int64_t groups, int N, bool helm, size_t tsize) {
+  const size_t V = helm ? (N + 1) * (N + 1) : (N + 1) * (N + 2) / 2;
+  return 2 * tsize * 8 * V * (size_t)(groups + 1);
+}
+
+int build_parent_slot_map(const uint32_t* gmap, int level, uint32_t groups, uint32_t* pmap,
+                          cudaStream_t s) {
+  const int nx = 1 << (level - 1);
+  const int64_t npp = (int64_t)(nx + 2) * (nx + 2) * (nx + 2);
+  k_parent_slot_map<<<(unsigned)((npp + 255) / 256), 256, 0, s>>>(gmap, nx, npp, groups, pmap);
+  WBFMM_CUDA(cudaGetLastError());
+  return 0;
+}
+
 __global__ void k_source_mask(const uint32_t* __restrict__ src_n, int nx, int64_t npp,
                               uint8_t* __restrict__ smask) {
   const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -776,6 +862,7 @@ int launch_m2l_lanes(const LanesParams<T>& p, const OpTables<T>& t,
 
 #define WBFMM_LANES_INST(T, H)                                                   \
   template int lanes_to_lin<T, H>(const T*, int, int, int, void*, cudaStream_t, bool); \
+  template int lanes_to_lin_groups<T, H>(const T*, int64_t, int, int, void*, cudaStream_t); \
   template int launch_lanes_reduce<T, H>(const LanesParams<T>&, cudaStream_t);   \
   template bool lanes_supported<T, H>(int, int);                                 \
   template int launch_m2l_lanes<T, H>(const LanesParams<T>&, const OpTables<T>&, \

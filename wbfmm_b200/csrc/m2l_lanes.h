@@ -33,6 +33,13 @@ struct LanesParams {
   const uint8_t* smask; // [8][padded grid]: source box holds sources, or null (all)
   int boxmajor;         // lin_raw is [8][padded grid][V] (lanes_to_lin), not [8][V][grid]
   void* partial_raw;    // [nsplit][8][V][np] complex when nsplit > 1
+  // sparse storage (tile kernel): lin_raw is [8][V][lin_stride] over the
+  // source slots (lanes_to_lin_groups), pmap maps the padded parent grid to
+  // a slot (lin_stride - 1, a zero column, where no group is stored), gmap
+  // the target groups to their slots; null for dense storage
+  const uint32_t* pmap;
+  const uint32_t* gmap;
+  int64_t lin_stride;
 };
 
 // The 189 list-4 offsets seen by a target of child type tau, packed as
@@ -77,9 +84,10 @@ template <typename T, bool HELM>
 int launch_m2l_tiles(const LanesParams<T>& p, const OpTables<T>& t,
                      cudaStream_t s);
 // targets per CTA of the tile kernel at order N (0: unsupported); *dense
-// (if given): whether it reads the level's Helmholtz coaxial rows
+// (if given): whether it reads the level's Helmholtz coaxial rows; sparse:
+// the launch on sparse level storage (LanesParams::pmap set)
 template <typename T, bool HELM>
-int tiles_per_cta(int N, bool* dense = nullptr);
+int tiles_per_cta(int N, bool* dense = nullptr, bool sparse = false);
 // the tile kernel's Helmholtz coaxial rows of a level (15 distances, rows
 // of (S|R) pairs with signs folded in) from its (S|R) table, into
 // helm_coax_rows_count(P) values
@@ -95,6 +103,18 @@ template <typename T, bool HELM>
 int lanes_to_lin(const T* arr, int level, int N, int scale_e, void* lin, cudaStream_t s,
                  bool boxmajor = false);
 size_t lanes_lin_bytes(int level, int N, bool helm, size_t tsize);
+// sparse storage: a level's compact array (groups slots, Layout L per
+// group) -> lin[tau][c][slot] over groups + 1 slots (the last zero), degree
+// n scaled by 2^(scale_e n); bytes: lanes_lin_groups_bytes
+template <typename T, bool HELM>
+int lanes_to_lin_groups(const T* arr, int64_t groups, int N, int scale_e, void* lin,
+                        cudaStream_t s);
+size_t lanes_lin_groups_bytes(int64_t groups, int N, bool helm, size_t tsize);
+// pmap[pp] = slot of the parent at padded-grid position pp (gmap of the
+// level), or `groups` (the zero column) on the padding and for parents
+// whose group is not stored; source_mask_bytes(level) / 8 entries
+int build_parent_slot_map(const uint32_t* gmap, int level, uint32_t groups, uint32_t* pmap,
+                          cudaStream_t s);
 
 // Active-target lists of a level for the lane and tile M2L: for each child
 // type tau, the parents (linear index, x fastest) whose child of type tau

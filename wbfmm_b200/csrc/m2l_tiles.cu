@@ -89,15 +89,17 @@ constexpr int kTileThreads = 256;
 struct TilePlan {
   int P, V, TC, NH, ncx, nB, nC, cx_off;
   bool dense;  // Helmholtz: stage C reads the level's coaxial rows (k_helm_coax_rows)
+  bool sparse; // sparse level storage: each target's source column (s_src)
   size_t ops_bytes, desc_bytes, vec_bytes, total;
 };
 
 template <typename T, bool HELM>
-__host__ __device__ TilePlan tile_plan(int P, int TC, bool dense) {
+__host__ __device__ TilePlan tile_plan(int P, int TC, bool dense, bool sparse) {
   TilePlan q;
   q.P = P;
   q.TC = TC;
   q.dense = HELM && dense;
+  q.sparse = sparse;
   q.V = HELM ? (P + 1) * (P + 1) : (P + 1) * (P + 2) / 2;
   q.NH = (P + 1) * (P + 2) * (4 * P + 3) / 6;
   q.ncx = !HELM ? (P + 1) * (P + 1) * (P + 1)
@@ -114,7 +116,7 @@ __host__ __device__ TilePlan tile_plan(int P, int TC, bool dense) {
   size_t ops = sizeof(T) * ((size_t)q.cx_off + q.ncx);
   q.ops_bytes = (ops + 15) & ~(size_t)15;
   q.desc_bytes = ((sizeof(int) * (size_t)(q.nB + (q.dense ? 2 : 1) * q.nC + q.V) +
-                   3 * sizeof(int) * TC) + 15) & ~(size_t)15;
+                   (sparse ? 4 : 3) * sizeof(int) * TC) + 15) & ~(size_t)15;
   q.vec_bytes = 3 * sizeof(typename C2<T>::t) * (size_t)q.V * TC;
   q.total = q.ops_bytes + q.desc_bytes + q.vec_bytes;
   return q;
@@ -132,12 +134,12 @@ constexpr size_t kTileSmemCap = 220 * 1024;
 struct TileChoice { int tc; bool dense; };
 
 template <typename T, bool HELM>
-TileChoice pick_tc(int P) {
+TileChoice pick_tc(int P, bool sparse) {
   TileChoice best = {0, false};
   int best_score = 0;
   for (int dense = 0; dense <= (HELM ? 1 : 0); dense++)
     for (int tc = 32; tc >= 8; tc >>= 1) {
-      const size_t bytes = tile_plan<T, HELM>(P, tc, dense).total;
+      const size_t bytes = tile_plan<T, HELM>(P, tc, dense, sparse).total;
       if (bytes > kTileSmemCap) continue;
       const int ctas = (int)((228 * 1024) / (bytes + 1024));
       const int score = ctas * tc;
@@ -162,7 +164,7 @@ __global__ void __launch_bounds__(kTileThreads)
 k_m2l_tiles(LanesParams<T> p, OpTables<T> t, int TC, bool dense) {
   typedef typename C2<T>::t T2;
   extern __shared__ __align__(16) unsigned char smraw[];
-  const TilePlan q = tile_plan<T, HELM>(p.N, TC, dense);
+  const TilePlan q = tile_plan<T, HELM>(p.N, TC, dense, p.pmap != nullptr);
   const int P = q.P, V = q.V;
   T* sH = (T*)smraw;
   T* seph = sH + q.NH;
@@ -174,7 +176,8 @@ k_m2l_tiles(LanesParams<T> p, OpTables<T> t, int TC, bool dense) {
   int* s_pp = s_nm + V;              // padded-grid index of each target's parent
   int* s_act = s_pp + TC;            // 1 + parent linear index, 0: no target
   int* s_map = s_act + TC;           // the offset's columns: target of each
-  int* dCo = s_map + TC;             // Helmholtz: row offset of each C row pair
+  int* s_src = s_map + TC;           // sparse: each target's source column in lin
+  int* dCo = s_src + (q.sparse ? TC : 0);   // Helmholtz: row offset of each C row pair
   T2* X = (T2*)(smraw + q.ops_bytes + q.desc_bytes);
   T2* Y = X + (size_t)V * TC;
   T2* A = Y + (size_t)V * TC;
@@ -185,6 +188,7 @@ k_m2l_tiles(LanesParams<T> p, OpTables<T> t, int TC, bool dense) {
   const int nx = 1 << (p.level - 1), npx = nx + 2;
   const int64_t npp = (int64_t)npx * npx * npx;
   const int64_t np = (int64_t)nx * nx * nx;
+  const int64_t lstride = p.pmap ? p.lin_stride : npp;   // lin columns per (tau, c)
   const int64_t base = (int64_t)(blockIdx.x >> 3) * TC;
   // sparse targets: this CTA's slots of the child type's list
   const int64_t nlist = p.act ? (int64_t)p.act_n[tau] : np;
@@ -238,6 +242,11 @@ k_m2l_tiles(LanesParams<T> p, OpTables<T> t, int TC, bool dense) {
     // groups of 4 columns, and an offset with none is skipped (the decision
     // is the CTA's)
     int f = 0;
+    if (q.sparse && tid < TC) {
+      // an active target's s_pp + doff stays on the padded grid (doff moves
+      // one parent at most); a slot without a target is never read
+      s_src[tid] = s_act[tid] ? (int)p.pmap[s_pp[tid] + doff] : 0;
+    }
     if (tid < TC && s_act[tid]) {
       if (p.smask) {
         f = p.smask[(int64_t)sg * npp + s_pp[tid] + doff];
@@ -279,13 +288,14 @@ k_m2l_tiles(LanesParams<T> p, OpTables<T> t, int TC, bool dense) {
     __syncthreads();   // operator staged
     // stage A: the TC source vectors, with e^{i m ch}
     {
-      const T2* src = (const T2*)p.lin_raw + (int64_t)sg * V * npp + doff;
+      const T2* src = (const T2*)p.lin_raw + (int64_t)sg * V * lstride + (q.sparse ? 0 : doff);
+      const int* col = q.sparse ? s_src : s_pp;
       for (int i = tid; i < V * TCc; i += kTileThreads) {
         const int c = i / TCc, tt = i - c * TCc;
         T2 v;
         v.x = T(0); v.y = T(0);
         if (tt < cnt) {
-          v = src[(int64_t)c * npp + s_pp[s_map[tt]]];
+          v = src[(int64_t)c * lstride + col[s_map[tt]]];
           const int m = (s_nm[c] >> 8) - 64, am = m < 0 ? -m : m;
           v = cmul(v, sech[2 * am], m < 0 ? -sech[2 * am + 1] : sech[2 * am + 1]);
         }
@@ -530,7 +540,9 @@ k_m2l_tiles(LanesParams<T> p, OpTables<T> t, int TC, bool dense) {
       continue;
     }
     const int px = (int)(plin % nx), py = (int)((plin / nx) % nx), pz = (int)(plin / ((int64_t)nx * nx));
-    const int64_t b = ((int64_t)morton(px, py, pz) << 3) | tau;
+    const int64_t g0 = compact_box(p.gmap, (int64_t)morton(px, py, pz) << 3);
+    if (g0 < 0) continue;   // (targets lie in stored groups)
+    const int64_t b = g0 | tau;
     if (HELM) {
       const int64_t o = layout_off(b, c, nc);
       p.cout[2 * o] += a.x;
@@ -552,7 +564,7 @@ k_m2l_tiles(LanesParams<T> p, OpTables<T> t, int TC, bool dense) {
 
 template <typename T, bool HELM>
 bool tiles_supported(int Ns, int Nr) {
-  return Ns == Nr && Ns >= 2 && Ns <= 60 && pick_tc<T, HELM>(Ns).tc > 0;
+  return Ns == Nr && Ns >= 2 && Ns <= 60 && pick_tc<T, HELM>(Ns, false).tc > 0;
 }
 
 template <typename T, bool HELM>
@@ -562,11 +574,12 @@ int launch_m2l_tiles(const LanesParams<T>& p, const OpTables<T>& t,
     int rc = ensure_tile_offsets();
     if (rc) return rc;
   }
-  const TileChoice c = pick_tc<T, HELM>(p.N);
+  const bool sparse = p.pmap != nullptr;
+  const TileChoice c = pick_tc<T, HELM>(p.N, sparse);
   const int TC = c.tc;
   if (!TC) return set_error(-3, "M2L tiles: expansion order too large for shared memory");
   if (c.dense && !p.hcx) return set_error(-3, "M2L tiles: coaxial rows of the level missing");
-  const TilePlan q = tile_plan<T, HELM>(p.N, TC, c.dense);
+  const TilePlan q = tile_plan<T, HELM>(p.N, TC, c.dense, sparse);
   WBFMM_SMEM(q.total, k_m2l_tiles<T, HELM>);
   const int64_t np = (int64_t)1 << (3 * (p.level - 1));
   dim3 grid((unsigned)(8 * ((np + TC - 1) / TC)), 1, p.nsplit);
@@ -587,8 +600,8 @@ template int build_helm_coax_rows<double>(const double*, int64_t, int, double*, 
 size_t helm_coax_rows_count(int P) { return (size_t)15 * 4 * coax_rows(P); }
 
 template <typename T, bool HELM>
-int tiles_per_cta(int N, bool* dense) {
-  const TileChoice c = pick_tc<T, HELM>(N);
+int tiles_per_cta(int N, bool* dense, bool sparse) {
+  const TileChoice c = pick_tc<T, HELM>(N, sparse);
   if (dense) *dense = c.dense;
   return c.tc;
 }
@@ -597,7 +610,7 @@ int tiles_per_cta(int N, bool* dense) {
   template bool tiles_supported<T, H>(int, int);                                 \
   template int launch_m2l_tiles<T, H>(const LanesParams<T>&, const OpTables<T>&, \
                                       cudaStream_t);                             \
-  template int tiles_per_cta<T, H>(int, bool*);
+  template int tiles_per_cta<T, H>(int, bool*, bool);
 WBFMM_TILES_INST(double, true)
 WBFMM_TILES_INST(double, false)
 WBFMM_TILES_INST(float, true)

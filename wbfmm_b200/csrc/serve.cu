@@ -342,6 +342,8 @@ int wbfmm_b200_server_submit(wbfmm_b200_server_t* srv,
     return set_error(WBFMM_B200_E_ARG, "dipole strengths need normals");
   if (r->cfg.precision != WBFMM_B200_FP32 && r->cfg.precision != WBFMM_B200_FP64)
     return set_error(WBFMM_B200_E_ARG, "precision must be FP64 (0) or FP32 (1)");
+  if (r->cfg.sparse)
+    return set_error(WBFMM_B200_E_ARG, "served requests use dense level storage (sparse storage sizes its arrays with a host wait)");
   auto* q = new Req();
   q->r = *r;
   q->footprint = wbfmm_b200_footprint(&r->cfg, r->nsrc, r->ntgt);

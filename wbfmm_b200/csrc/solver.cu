@@ -322,6 +322,10 @@ int wbfmm_b200_coefficient_pointers(wbfmm_b200_solver_t* s, int level,
                                     void** ms, void** mr) {
   SOLVER_CALL(s->coefficient_pointers(level, ms, mr));
 }
+int wbfmm_b200_coefficient_storage(wbfmm_b200_solver_t* s, int level, int64_t* groups,
+                                   int64_t* bytes) {
+  SOLVER_CALL(s->coefficient_storage(level, groups, bytes));
+}
 int wbfmm_b200_set_p2m_accumulate(wbfmm_b200_solver_t* s, int on) {
   if (!s) return set_error(WBFMM_B200_E_ARG, "null solver");
   s->set_p2m_accumulate(on);

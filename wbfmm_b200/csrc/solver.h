@@ -139,6 +139,16 @@ static __global__ void k_target_mask(const uint32_t* __restrict__ leaf_count,
   mask[b] = any;
 }
 
+// parent[b] = any of child[8 b .. 8 b + 7] (a target mask one level up)
+static __global__ void k_mask_up(const uint8_t* __restrict__ child, int64_t n,
+                                 uint8_t* __restrict__ parent) {
+  const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  uint8_t any = 0;
+  for (int c = 0; c < 8; c++) any |= child[8 * b + c];
+  parent[b] = any ? 1 : 0;
+}
+
 template <typename T>
 static int convert_to(const double* src, T* dst, int64_t n, cudaStream_t s) {
   if (n <= 0) return 0;
@@ -186,6 +196,7 @@ struct wbfmm_b200_solver {
   virtual void set_p2m_accumulate(int on) = 0;
   virtual int adopt_coefficients(int level, void* ms, void* mr) = 0;
   virtual int l2l(int level) = 0;
+  virtual int coefficient_storage(int level, int64_t* groups, int64_t* bytes) = 0;
 };
 
 namespace wbfmm {
@@ -209,8 +220,16 @@ struct Solver : public wbfmm_b200_solver {
   bool have_q = false, have_dip = false, have_normals = false;
   RadixScratch rs;
   DBuf<uint32_t> box_i[kMaxDepth + 1], box_n[kMaxDepth + 1];
-  // coefficients (Layout L)
+  // coefficients (Layout L; with sparse storage, per stored group)
   DBuf<T> mps[kMaxDepth + 1], mpr[kMaxDepth + 1];
+  // sparse level storage (sparse.cu): per level the group -> slot map, the
+  // slot -> group list and the count of stored groups, for the sources and
+  // targets of geometry sparse_geo
+  DBuf<uint32_t> gmap[kMaxDepth + 1], glist[kMaxDepth + 1], gflag, gcount, pmap;
+  DBuf<unsigned char> gscratch;
+  int64_t ngroups[kMaxDepth + 1] = {0};
+  uint64_t sparse_geo = ~0ull;
+  DBuf<T> dense_tmp;                // a sparse level expanded for get_coefficients
   // targets
   int ntgt = 0;
   DBuf<double> tpts_in, tx, ty, tz;
@@ -291,8 +310,9 @@ struct Solver : public wbfmm_b200_solver {
     f(snx); f(sny); f(snz); f(sq); f(sdip); f(stage); f(nstage);
     for (int l = 0; l <= kMaxDepth; l++) {
       f(box_i[l]); f(box_n[l]); f(mps[l]); f(mpr[l]); f(tmask[l]);
-      f(act[l]); f(act_n[l]);
+      f(act[l]); f(act_n[l]); f(gmap[l]); f(glist[l]);
     }
+    f(gflag); f(gcount); f(pmap); f(gscratch); f(dense_tmp);
     f(coax_set64); f(coax_set);
     f(tpts_in); f(tx); f(ty); f(tz); f(tkeys); f(tperm); f(tbox);
     f(tstart); f(tcount); f(flag); f(pot); f(grad); f(out64); f(hess_d); f(hess_g);
@@ -322,6 +342,11 @@ struct Solver : public wbfmm_b200_solver {
   size_t level_len(int level, int p) const {
     return ((size_t)1 << (3 * level)) * ncoefs(p) * (helm ? 2 : 1);
   }
+  // values of the coefficient array of a level at order p as stored
+  size_t coef_len(int level, int p) const {
+    if (!cfg.sparse) return level_len(level, p);
+    return (size_t)ngroups[level] * 8 * ncoefs(p) * (helm ? 2 : 1);
+  }
 
   // validate and take a configuration (buffers already held are kept)
   int configure(const wbfmm_b200_config_t* c) {
@@ -342,6 +367,12 @@ struct Solver : public wbfmm_b200_solver {
       lmax = std::max(lmax, std::max(cfg.order_s[l], cfg.order_r[l]));
     }
     if (cfg.field == 0) cfg.field = WBFMM_B200_POTENTIAL;
+    if (cfg.sparse) {
+      // coefficients of the boxes that hold sources or targets (and their
+      // siblings) only: the M2L skips the rest, as skip_empty does
+      if (cfg.managed) return set_error(WBFMM_B200_E_ARG, "sparse level storage does not take managed arrays");
+      cfg.skip_empty = 1;
+    }
     return 0;
   }
 
@@ -468,8 +499,9 @@ struct Solver : public wbfmm_b200_solver {
       launches += 2;
     }
     WBFMM_CUDA(cudaGetLastError());
-    // coefficient arrays (arrays adopted from the caller are kept)
-    for (int l = 1; l <= depth && !tree_only; l++) {
+    // coefficient arrays (arrays adopted from the caller are kept; sparse
+    // storage allocates once the targets are known, prepare_sparse)
+    for (int l = 1; l <= depth && !tree_only && !cfg.sparse; l++) {
       WBFMM_TRY(mps[l].alloc(level_len(l, cfg.order_s[l]), cfg.managed != 0));
       WBFMM_TRY(mpr[l].alloc(level_len(l, cfg.order_r[l]), cfg.managed != 0));
     }
@@ -708,9 +740,59 @@ struct Solver : public wbfmm_b200_solver {
     return 0;
   }
 
+  // Sparse level storage: the group maps of every level from the boxes
+  // holding sources (box counts) or targets (target masks), then the
+  // compact coefficient arrays.  Once per geometry; one host wait (the
+  // group counts size the arrays).
+  int prepare_sparse() {
+    if (!cfg.sparse || tree_only || sparse_geo == geo) return 0;
+    if (nsrc <= 0 || ntgt <= 0)
+      return set_error(WBFMM_B200_E_STATE, "sparse level storage: set the sources and the targets first");
+    // target masks of levels 1 and 0 from level 2's (set_targets builds the
+    // levels >= 2 with skip_empty, which sparse storage implies)
+    if (!tmask[2].p) return set_error(WBFMM_B200_E_STATE, "sparse level storage: no target masks");
+    for (int l = 1; l >= 0; l--) {
+      const int64_t nbl = (int64_t)1 << (3 * l);
+      WBFMM_TRY(tmask[l].alloc((size_t)nbl));
+      k_mask_up<<<1, 64, 0, stream>>>(tmask[l + 1].p, nbl, tmask[l].p);
+      launches++;
+    }
+    WBFMM_TRY(gcount.alloc(kMaxDepth + 1));
+    const int64_t nmax = (int64_t)1 << (3 * (depth - 1));
+    WBFMM_TRY(gflag.alloc((size_t)nmax));
+    const size_t scr = sparse_scan_scratch(nmax);
+    WBFMM_TRY(gscratch.alloc(scr));
+    for (int l = 1; l <= depth; l++) {
+      const int64_t n = (int64_t)1 << (3 * (l - 1));    // groups: boxes of level l - 1
+      WBFMM_TRY(gmap[l].alloc((size_t)n));
+      WBFMM_TRY(sparse_group_map(box_n[l - 1].p, tmask[l - 1].p, n, gflag.p, gmap[l].p,
+                                 gcount.p + l, gscratch.p, scr, stream));
+      launches += 3;
+    }
+    uint32_t cnt[kMaxDepth + 1] = {0};
+    WBFMM_CUDA(cudaMemcpyAsync(cnt + 1, gcount.p + 1, sizeof(uint32_t) * depth,
+                               cudaMemcpyDeviceToHost, stream));
+    WBFMM_CUDA(cudaStreamSynchronize(stream));
+    const int w = helm ? 2 : 1;
+    for (int l = 1; l <= depth; l++) {
+      const int64_t n = (int64_t)1 << (3 * (l - 1));
+      ngroups[l] = cnt[l];
+      if (ngroups[l] <= 0 || ngroups[l] > n)
+        return set_error(WBFMM_B200_E_STATE, "sparse level storage: bad group count");
+      WBFMM_TRY(glist[l].alloc((size_t)ngroups[l]));
+      WBFMM_TRY(sparse_group_list(gmap[l].p, n, glist[l].p, stream));
+      WBFMM_TRY(mps[l].alloc((size_t)ngroups[l] * 8 * ncoefs(cfg.order_s[l]) * w));
+      WBFMM_TRY(mpr[l].alloc((size_t)ngroups[l] * 8 * ncoefs(cfg.order_r[l]) * w));
+      launches++;
+    }
+    sparse_geo = geo;
+    return 0;
+  }
+
   // ------------------------------------------------------------- passes
   int leaf_expansions() override {
     if (nsrc <= 0) return set_error(WBFMM_B200_E_STATE, "set_sources first");
+    WBFMM_TRY(prepare_sparse());
     P2MParams<T> p;
     p.nbox = (int64_t)1 << (3 * depth);
     p.level = depth; p.N = cfg.order_s[depth];
@@ -723,6 +805,10 @@ struct Solver : public wbfmm_b200_solver {
     p.nx = snx.p; p.ny = sny.p; p.nz = snz.p;
     p.mps = mps[depth].p;
     p.accumulate = p2m_accumulate ? 1 : 0;
+    if (cfg.sparse) {
+      p.nbox = 8 * ngroups[depth];
+      p.glist = glist[depth].p;
+    }
     launches++;
     return helm ? launch_p2m<T, true>(p, stream) : launch_p2m<T, false>(p, stream);
   }
@@ -738,6 +824,7 @@ struct Solver : public wbfmm_b200_solver {
   int upward(int level) override {
     if (level < 3 || level > depth) return set_error(WBFMM_B200_E_ARG, "upward pass level must be in [3, depth]");
     WBFMM_TRY(build_operators());
+    WBFMM_TRY(prepare_sparse());
     XlateParams<T> x = xparams();
     x.level = level - 1;
     x.nbox = (int64_t)1 << (3 * (level - 1));
@@ -745,6 +832,14 @@ struct Solver : public wbfmm_b200_solver {
     x.cin = mps[level].p; x.cout = mps[level - 1].p;
     x.coax = helm ? ss_ptr[level] : nullptr;
     x.width = (T)width(level);
+    if (cfg.sparse) {
+      // one CTA per stored group of the children; the parents' other
+      // siblings (no sources or targets) hold zeros
+      WBFMM_CUDA(cudaMemsetAsync(x.cout, 0, sizeof(T) * coef_len(level - 1, x.Nout), stream));
+      x.nbox = ngroups[level];
+      x.glist = glist[level].p;
+      x.gmap = gmap[level - 1].p;
+    }
     launches++;
     return helm ? launch_m2m<T, true>(x, tables, stream)
                 : launch_m2m<T, false>(x, tables, stream);
@@ -759,8 +854,9 @@ struct Solver : public wbfmm_b200_solver {
   int m2l(int level) override {
     if (level < 2 || level > depth) return set_error(WBFMM_B200_E_ARG, "downward pass level must be in [2, depth]");
     WBFMM_TRY(build_operators());
+    WBFMM_TRY(prepare_sparse());
     if (level == 2)
-      WBFMM_CUDA(cudaMemsetAsync(mpr[2].p, 0, sizeof(T) * level_len(2, cfg.order_r[2]), stream));
+      WBFMM_CUDA(cudaMemsetAsync(mpr[2].p, 0, sizeof(T) * coef_len(2, cfg.order_r[2]), stream));
     XlateParams<T> x = xparams();
     x.level = level;
     x.nbox = (int64_t)1 << (3 * level);
@@ -785,6 +881,7 @@ struct Solver : public wbfmm_b200_solver {
     const int lanes_max = helm ? 7 : sizeof(T) == 8 ? 9 : 10;
     bool use_tiles = false, use_lanes = false;
     const int he = helm ? helm_e[level] : 0;
+    if (cfg.sparse) return m2l_sparse(level, x, he, tiles_ok);
     // tensor cores: Laplace, FP32, equal orders up to (p+1)^2 = 256, mode 4
     if (!helm && sizeof(T) == 4 && m2l_mode == 4 && tc_lap_supported(x.Nin, x.Nout))
       return m2l_tc(level, x);
@@ -908,6 +1005,63 @@ struct Solver : public wbfmm_b200_solver {
                 : launch_m2l<T, false>(x, tables, stream);
   }
 
+  // The M2L of a level with sparse storage: the tile kernel on the
+  // compact transposed sources (one column per stored source group and a
+  // zero column), source parents found through the padded-grid slot map,
+  // targets from the level's active lists written at their slots
+  int m2l_sparse(int level, const XlateParams<T>& x, int he, bool tiles_ok) {
+    bool dense = false;
+    const int tc = helm ? tiles_per_cta<T, true>(x.Nin, &dense, true)
+                        : tiles_per_cta<T, false>(x.Nin, nullptr, true);
+    if (!tiles_ok || tc == 0)
+      return set_error(WBFMM_B200_E_ORDER, "sparse level storage: the M2L needs equal orders in [2, 60] at each level");
+    const int64_t G = ngroups[level];
+    WBFMM_TRY(lin.alloc(lanes_lin_groups_bytes(G, x.Nin, helm, sizeof(T))));
+    const int se = helm ? he : x.lap_e;
+    WBFMM_TRY((helm ? lanes_to_lin_groups<T, true>(x.cin, G, x.Nin, se, lin.p, stream)
+                    : lanes_to_lin_groups<T, false>(x.cin, G, x.Nin, se, lin.p, stream)));
+    WBFMM_TRY(pmap.alloc(source_mask_bytes(level) / 8));
+    WBFMM_TRY(build_parent_slot_map(gmap[level].p, level, (uint32_t)G, pmap.p, stream));
+    LanesParams<T> lp;
+    memset(&lp, 0, sizeof(lp));
+    lp.level = level; lp.N = x.Nin;
+    lp.lin_raw = lin.p; lp.cout = x.cout;
+    lp.coax = x.coax; lp.coax_stride = x.coax_stride;
+    lp.width = x.width; lp.tmask = x.tmask; lp.lap_e = x.lap_e;
+    lp.helm_e = he;
+    lp.act = act[level].p; lp.act_n = act_n[level].p;
+    lp.pmap = pmap.p; lp.gmap = gmap[level].p; lp.lin_stride = G + 1;
+    WBFMM_TRY(smask.alloc(source_mask_bytes(level)));
+    WBFMM_TRY(build_source_mask(x.src_n, level, smask.p, stream));
+    lp.smask = smask.p;
+    if (!helm) {
+      const int P1 = x.Nin + 1;
+      WBFMM_TRY(lapsr.alloc((size_t)kNumOps * P1 * P1 * P1));
+      WBFMM_TRY(build_lap_sr_ops<T>(tables, x.Nin, x.width, x.lap_e, lapsr.p, stream));
+      lp.lapsr = lapsr.p;
+      launches++;
+    }
+    if (dense) {
+      WBFMM_TRY(hcx.alloc(helm_coax_rows_count(x.Nin)));
+      WBFMM_TRY(build_helm_coax_rows<T>(x.coax, x.coax_stride, x.Nin, hcx.p, stream));
+      lp.hcx = hcx.p;
+      launches++;
+    }
+    const int64_t np = (int64_t)1 << (3 * (level - 1));
+    const int64_t ctas = ((np + tc - 1) / tc) * 8;
+    int ns = 1;
+    while (ctas * ns < 2 * 148 && ns < 32) ns *= 2;
+    lp.nsplit = ns;
+    if (ns > 1) {
+      const int V = helm ? (x.Nin + 1) * (x.Nin + 1) : (x.Nin + 1) * (x.Nin + 2) / 2;
+      WBFMM_TRY(lanes_part.alloc((size_t)ns * 8 * V * np * 2));
+      lp.partial_raw = lanes_part.p;
+    }
+    launches += 3 + (ns > 1 ? 2 : 1);
+    return helm ? launch_m2l_tiles<T, true>(lp, tables, stream)
+                : launch_m2l_tiles<T, false>(lp, tables, stream);
+  }
+
   // The Laplace M2L of a level on the tensor cores (m2l_tc.cu).
   int m2l_tc(int level, const XlateParams<T>& x) {
     LapTcParams lp;
@@ -958,6 +1112,7 @@ struct Solver : public wbfmm_b200_solver {
   int l2l(int level) override {
     if (level < 2 || level >= depth) return set_error(WBFMM_B200_E_ARG, "L2L level must be in [2, depth-1]");
     WBFMM_TRY(build_operators());
+    WBFMM_TRY(prepare_sparse());
     XlateParams<T> d = xparams();
     d.level = level + 1;
     d.nbox = (int64_t)1 << (3 * level);
@@ -965,6 +1120,13 @@ struct Solver : public wbfmm_b200_solver {
     d.cin = mpr[level].p; d.cout = mpr[level + 1].p;
     d.coax = helm ? ss_ptr[level + 1] : nullptr;
     d.width = (T)width(level + 1);
+    if (cfg.sparse) {
+      // one CTA per stored group of the children (every box of a stored
+      // group is written)
+      d.nbox = ngroups[level + 1];
+      d.glist = glist[level + 1].p;
+      d.gmap = gmap[level].p;
+    }
     launches++;
     return helm ? launch_l2l<T, true>(d, tables, stream)
                 : launch_l2l<T, false>(d, tables, stream);
@@ -986,11 +1148,13 @@ struct Solver : public wbfmm_b200_solver {
     e.pot = (cfg.field & eval_field & WBFMM_B200_POTENTIAL) ? pot.p : nullptr;
     e.grad = (cfg.field & eval_field & WBFMM_B200_GRADIENT) ? grad.p : nullptr;
     e.nbox = (int64_t)1 << (3 * depth);
+    e.gmap = cfg.sparse ? gmap[depth].p : nullptr;
     return e;
   }
 
   int evaluate() override {
     if (ntgt <= 0) return set_error(WBFMM_B200_E_STATE, "set_targets first");
+    WBFMM_TRY(prepare_sparse());
     EvalParams<T> e = eparams();
     launches += eval_neighbours ? 2 : 1;
     if (helm) WBFMM_TRY((launch_l2p<T, true>(e, stream)));
@@ -1215,6 +1379,7 @@ struct Solver : public wbfmm_b200_solver {
   // neighbours, the monopoles of the 27 neighbour boxes
   int hessian(double* hess, int neighbours) override {
     if (helm) return set_error(WBFMM_B200_E_ARG, "the Hessian is for Laplace solvers");
+    if (cfg.sparse) return set_error(WBFMM_B200_E_ARG, "the Hessian needs dense level storage");
     if (nsrc <= 0 || ntgt <= 0) return set_error(WBFMM_B200_E_STATE, "sources and targets must be set");
     if (neighbours && have_dip)
       return set_error(WBFMM_B200_E_ARG, "the near-field Hessian takes monopole sources only");
@@ -1251,6 +1416,7 @@ struct Solver : public wbfmm_b200_solver {
   // targets (target_bases.cu): held until the sources or targets change
   int target_bases() override {
     if (nsrc <= 0 || ntgt <= 0) return set_error(WBFMM_B200_E_STATE, "sources and targets must be set");
+    if (cfg.sparse) return set_error(WBFMM_B200_E_ARG, "target bases need dense level storage");
     const EvalParams<T> e = eparams();
     int64_t np = 0;
     WBFMM_TRY(tl_off.alloc((size_t)ntgt + 1));
@@ -1313,6 +1479,22 @@ struct Solver : public wbfmm_b200_solver {
 
   int get_coefficients(int level, double* ms, double* mr) override {
     if (level < 1 || level > depth) return set_error(WBFMM_B200_E_ARG, "bad level");
+    if (cfg.sparse) {
+      // the dense Layout L arrays, zero outside the stored groups
+      WBFMM_TRY(prepare_sparse());
+      const int w = helm ? 2 : 1;
+      auto one = [&](DBuf<T>& a, int p, double* out) -> int {
+        const size_t dl = level_len(level, p);
+        WBFMM_TRY(dense_tmp.alloc(dl));
+        WBFMM_TRY(sparse_expand<T>(a.p, glist[level].p, ngroups[level],
+                                   (int64_t)8 * ncoefs(p) * w, dense_tmp.p, (int64_t)dl, stream));
+        launches++;
+        return fetch(dense_tmp, dl, out, 0);
+      };
+      if (ms) WBFMM_TRY(one(mps[level], cfg.order_s[level], ms));
+      if (mr) WBFMM_TRY(one(mpr[level], cfg.order_r[level], mr));
+      return 0;
+    }
     if (ms) WBFMM_TRY(fetch(mps[level], level_len(level, cfg.order_s[level]), ms, 0));
     if (mr) WBFMM_TRY(fetch(mpr[level], level_len(level, cfg.order_r[level]), mr, 0));
     return 0;
@@ -1330,6 +1512,7 @@ struct Solver : public wbfmm_b200_solver {
   }
   int adopt_coefficients(int level, void* ms, void* mr) override {
     if (level < 1 || level > depth) return set_error(WBFMM_B200_E_ARG, "bad level");
+    if (cfg.sparse) return set_error(WBFMM_B200_E_ARG, "adopted arrays need dense level storage");
     gen++;
     if (ms) mps[level].adopt((T*)ms, level_len(level, cfg.order_s[level]), cfg.managed != 0);
     if (mr) mpr[level].adopt((T*)mr, level_len(level, cfg.order_r[level]), cfg.managed != 0);
@@ -1338,8 +1521,25 @@ struct Solver : public wbfmm_b200_solver {
 
   int coefficient_pointers(int level, void** ms, void** mr) override {
     if (level < 1 || level > depth) return set_error(WBFMM_B200_E_ARG, "bad level");
+    if (cfg.sparse) return set_error(WBFMM_B200_E_ARG, "Layout L pointers need dense level storage");
     if (ms) *ms = mps[level].p;
     if (mr) *mr = mpr[level].p;
+    return 0;
+  }
+
+  // stored groups of eight boxes of a level (dense: 8^(level-1)) and the
+  // bytes of its two coefficient arrays; level 0: totals over levels 1..depth
+  int coefficient_storage(int level, int64_t* groups, int64_t* bytes) override {
+    if (level < 0 || level > depth) return set_error(WBFMM_B200_E_ARG, "bad level");
+    if (tree_only) return set_error(WBFMM_B200_E_STATE, "no coefficient arrays");
+    if (cfg.sparse) WBFMM_TRY(prepare_sparse());
+    int64_t g = 0, by = 0;
+    for (int l = level ? level : 1; l <= (level ? level : depth); l++) {
+      g += cfg.sparse ? ngroups[l] : (int64_t)1 << (3 * (l - 1));
+      by += (int64_t)sizeof(T) * (int64_t)(coef_len(l, cfg.order_s[l]) + coef_len(l, cfg.order_r[l]));
+    }
+    if (groups) *groups = g;
+    if (bytes) *bytes = by;
     return 0;
   }
 };

@@ -46,7 +46,7 @@ class Config(C.Structure):
         ("k", C.c_double), ("x0", C.c_double * 3), ("D", C.c_double),
         ("precision", C.c_int), ("field", C.c_int), ("skip_empty", C.c_int),
         ("managed", C.c_int), ("leaf_order", C.c_int), ("keys_fp32", C.c_int),
-        ("near_fp32", C.c_int),
+        ("near_fp32", C.c_int), ("sparse", C.c_int),
     ]
 
 
@@ -107,6 +107,8 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "wbfmm_b200_get_tree": (ip, [vp, u32p, u32p, u32p, ip]),
         "wbfmm_b200_get_coefficients": (ip, [vp, ip, dp, dp]),
         "wbfmm_b200_coefficient_pointers": (ip, [vp, ip, C.POINTER(vp), C.POINTER(vp)]),
+        "wbfmm_b200_coefficient_storage": (ip, [vp, ip, C.POINTER(C.c_int64),
+                                                C.POINTER(C.c_int64)]),
         "wbfmm_b200_stage_times": (ip, [vp, dp]),
         "wbfmm_b200_kernel_launches": (C.c_int64, [vp]),
         "wbfmm_b200_solve": (ip, [C.POINTER(Config), ip, vp, vp, vp, vp, ip, vp, vp, vp]),
@@ -174,6 +176,7 @@ class SolverConfig:
     managed: bool = False
     leaf_order: bool = False
     near_fp32: bool = False
+    sparse: bool = False
 
     def to_c(self) -> Config:
         c = Config()
@@ -192,14 +195,16 @@ class SolverConfig:
         c.managed = int(bool(self.managed))
         c.leaf_order = int(bool(self.leaf_order))
         c.near_fp32 = int(bool(self.near_fp32))
+        c.sparse = int(bool(self.sparse))
         return c
 
     @staticmethod
     def from_problem(p, precision=FP64, field=POTENTIAL | GRADIENT,
-                     skip_empty=False, leaf_order=False, near_fp32=False) -> "SolverConfig":
+                     skip_empty=False, leaf_order=False, near_fp32=False,
+                     sparse=False) -> "SolverConfig":
         return SolverConfig(p.problem, p.depth, list(p.order_s), list(p.order_r),
                             p.k, tuple(p.x0), p.D, precision, field, skip_empty,
-                            False, leaf_order, near_fp32)
+                            False, leaf_order, near_fp32, sparse)
 
 
 class Solver:
@@ -389,6 +394,13 @@ class Solver:
                                                     mr.ctypes.data_as(dp)))
         return ms, mr
 
+    def coefficient_storage(self, level=0):
+        """(stored groups of eight boxes, device bytes of the coefficient
+        arrays) of a level, or totals over all levels for level 0."""
+        g, b = C.c_int64(), C.c_int64()
+        _check(self.lib.wbfmm_b200_coefficient_storage(self.h, level, C.byref(g), C.byref(b)))
+        return g.value, b.value
+
     def invalidate_operators(self):
         _check(self.lib.wbfmm_b200_invalidate_operators(self.h))
 
@@ -401,9 +413,10 @@ class Solver:
         return int(self.lib.wbfmm_b200_kernel_launches(self.h))
 
 
-def solve(p, precision=FP64, field=POTENTIAL | GRADIENT, skip_empty=False):
-    """Run one FMM solve of a :class:`wbfmm_b200.workloads.Problem`."""
-    cfg = SolverConfig.from_problem(p, precision, field, skip_empty)
+def solve(p, precision=FP64, field=POTENTIAL | GRADIENT, skip_empty=False, sparse=False):
+    """Run one FMM solve of a :class:`wbfmm_b200.workloads.Problem`
+    (sparse: sparse level storage)."""
+    cfg = SolverConfig.from_problem(p, precision, field, skip_empty, sparse=sparse)
     with Solver(cfg) as s:
         s.set_sources(p.xs, p.normals)
         s.set_strengths(p.q, p.dipoles)
