@@ -273,7 +273,7 @@ def workload(args, rank):
     from wbfmm_b200 import workloads as W
     w = args.workload
     if w == "cube":
-        p = W.helmholtz_cube(args.points, k=8.0, depth=args.depth, seed=2 + rank)
+        p = W.helmholtz_cube(args.points, k=8.0, depth=args.depth or 6, seed=2 + rank)
         return p, 10_000, 102, False, CUBE_WORKLOAD
     if w == "laplace_c1":
         p = W.laplace_cube(20_000, 20_000, depth=4, order=12, seed=1 + rank)
@@ -283,8 +283,9 @@ def workload(args, rank):
         p = W.helmholtz_sphere(2_000_000, 500_000, k=40.0, depth=7, seed=3 + rank, hi=None)
         return p, 10_000, 103, True, "helmholtz_sphere_2e6_half_dipoles_5e5_targets_k40_depth7"
     if w == "clusters_c5":
-        p = W.laplace_clusters(16_000_000, depth=8, order=10, seed=5 + rank)
-        return p, 20_000, 105, True, "laplace_8_gaussian_clusters_1.6e7_depth8_p10"
+        d = args.depth or 8
+        p = W.laplace_clusters(16_000_000, depth=d, order=10, seed=5 + rank)
+        return p, 20_000, 105, True, f"laplace_8_gaussian_clusters_1.6e7_depth{d}_p10"
     raise SystemExit(f"unknown workload {w}")
 
 
@@ -681,11 +682,14 @@ def single_solve_section(args, ws, rank, local, p, n_acc, acc_seed, skip_empty, 
     xt_d = xs_d if p.targets_are_sources else dev_arr(p.xt)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
 
+    sparse = bool(getattr(args, "sparse", False))
+
     def make(precision):
         # the FP32 form sorts the sources by leaf box only; the plain FP64
         # form on full keys, as the reference
         cfg = engine.SolverConfig.from_problem(p, precision, field, skip_empty,
-                                               leaf_order=precision == engine.FP32)
+                                               leaf_order=precision == engine.FP32,
+                                               sparse=sparse)
         s = engine.Solver(cfg, stream=stream.cuda_stream)
         s.set_deferred_checks(True)     # no host wait inside a solve
         return s
@@ -735,7 +739,8 @@ def single_solve_section(args, ws, rank, local, p, n_acc, acc_seed, skip_empty, 
             m2l_ms[lv] = a.elapsed_time(b)
         pot, grad = s.field()
         results[name] = dict(ms=ms, step_ms=step_ms, launches=launches, stages=stages,
-                             m2l_ms=m2l_ms, pot=pot, grad=grad, clocks=clk.summary())
+                             m2l_ms=m2l_ms, pot=pot, grad=grad, clocks=clk.summary(),
+                             coef_bytes=s.coefficient_storage(0)[1])
         if name == "fp64":
             s.close()
             torch.cuda.synchronize(dev)
@@ -818,12 +823,14 @@ def single_solve_section(args, ws, rank, local, p, n_acc, acc_seed, skip_empty, 
     return {
         "workload": label, "points": p.points, "sources": ns, "targets": nt, "depth": p.depth,
         "orders": p.order_s[1:], "k": p.k, "skip_empty": skip_empty,
+        "storage": "sparse" if sparse else "dense",
         "fp32": {"points_per_s": ws * p.points / (f32["ms"] * 1e-3), "ms_per_step": f32["ms"],
                  "step_ms": f32["step_ms"], "stages_ms": f32["stages"], "m2l_ms": f32["m2l_ms"],
-                 "launches": int(f32["launches"]), "clocks": f32["clocks"]},
+                 "launches": int(f32["launches"]), "clocks": f32["clocks"],
+                 "coefficient_bytes": int(f32["coef_bytes"])},
         "fp64": {"points_per_s": ws * p.points / (f64["ms"] * 1e-3), "ms_per_step": f64["ms"],
                  "step_ms": f64["step_ms"], "stages_ms": f64["stages"], "m2l_ms": f64["m2l_ms"],
-                 "clocks": f64["clocks"]},
+                 "clocks": f64["clocks"], "coefficient_bytes": int(f64["coef_bytes"])},
         "e2e_fp32": e2e, "accuracy": acc, "dominant_m2l": m2l,
     }
 
@@ -1096,7 +1103,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--points", type=int, default=1_000_000)
-    ap.add_argument("--depth", type=int, default=6)
+    ap.add_argument("--depth", type=int, default=None,
+                    help="tree depth of the cube (default 6) and clusters_c5 (default 8) workloads")
+    ap.add_argument("--sparse", action="store_true",
+                    help="single-solve workloads: sparse level storage (coefficients of the "
+                         "groups of boxes whose parent holds points only)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-cube", action="store_true",
                     help="stream workload: leave out the 1e6-point cube single solves")

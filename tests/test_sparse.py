@@ -3,8 +3,9 @@ arrays hold only the groups of eight sibling boxes whose parent holds
 sources or targets (the reference always stores all 8^l boxes,
 src/boxes.c:518-583).
 
-* the fields equal the dense solve's with the same M2L kernel (the tile
-  kernel) and skip_empty, which sparse storage implies: FP64 and FP32,
+* the fields equal the dense solve's with the same M2L kernels (the tile
+  kernel, or the automatic choice of the lane kernel at low orders) and
+  skip_empty, which sparse storage implies: FP64 and FP32,
   Laplace and Helmholtz (dipoles, the scaled FP32 Helmholtz M2L), targets
   equal to the sources and targets in boxes that hold no sources;
 * the coefficients of levels 2..depth, expanded to Layout L, equal the
@@ -55,10 +56,10 @@ def case_problem(case):
     raise ValueError(case)
 
 
-def solve(p, precision, sparse, keep=False):
+def solve(p, precision, sparse, keep=False, mode=3):
     cfg = engine.SolverConfig.from_problem(p, precision, skip_empty=True, sparse=sparse)
     s = engine.Solver(cfg)
-    s.set_m2l_kernel(3)          # the tile kernel, which sparse storage runs
+    s.set_m2l_kernel(mode)       # 3: the tile kernel; 1: lanes at low orders, tiles above
     s.set_sources(p.xs, p.normals).set_strengths(p.q, p.dipoles).set_targets(p.xt).run()
     out = s.field()
     if keep:
@@ -67,13 +68,14 @@ def solve(p, precision, sparse, keep=False):
     return out
 
 
+@pytest.mark.parametrize("mode", [1, 3])
 @pytest.mark.parametrize("precision", [engine.FP64, engine.FP32])
 @pytest.mark.parametrize("case", ["laplace_clusters", "helmholtz_sphere", "helmholtz_low_kw",
                                   "separate_targets"])
-def test_sparse_fields_match_dense(gpu_lib, case, precision):
+def test_sparse_fields_match_dense(gpu_lib, case, precision, mode):
     p = case_problem(case)
-    dense = solve(p, precision, False)
-    sparse = solve(p, precision, True)
+    dense = solve(p, precision, False, mode=mode)
+    sparse = solve(p, precision, True, mode=mode)
     # the same kernels in the same order on the same values: equal up to
     # rounding (in practice bit for bit)
     tol = 1e-13 if precision == engine.FP64 else 1e-6

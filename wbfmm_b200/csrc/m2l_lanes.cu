@@ -92,11 +92,12 @@ __global__ void k_to_lin(const T* __restrict__ arr, int level, int N, int scale_
   else lin[((int64_t)tau * V + c) * npp + pp] = v;
 }
 
-// sparse storage: compact level array -> lin[tau][c][slot], slot in
-// [0, groups] (slot `groups` zero), degree n scaled by 2^(scale_e n)
+// sparse storage: compact level array -> lin[tau][c][slot] (box-major:
+// lin[tau][slot][c]), slot in [0, groups] (slot `groups` zero), degree n
+// scaled by 2^(scale_e n)
 template <typename T, bool HELM>
 __global__ void k_to_lin_groups(const T* __restrict__ arr, int64_t groups, int N, int scale_e,
-                                typename V2t<T>::t* __restrict__ lin) {
+                                bool boxmajor, typename V2t<T>::t* __restrict__ lin) {
   typedef typename V2t<T>::t T2;
   const int V = HELM ? (N + 1) * (N + 1) : (N + 1) * (N + 2) / 2;
   const int nc = (N + 1) * (N + 1);
@@ -129,7 +130,8 @@ __global__ void k_to_lin_groups(const T* __restrict__ arr, int64_t groups, int N
       v.y = scale2(v.y, scale_e * n);
     }
   }
-  lin[((int64_t)tau * V + c) * (groups + 1) + slot] = v;
+  if (boxmajor) lin[((int64_t)tau * (groups + 1) + slot) * V + c] = v;
+  else lin[((int64_t)tau * V + c) * (groups + 1) + slot] = v;
 }
 
 // pmap[pp]: slot of the padded-grid parent pp, `groups` on the padding and
@@ -361,9 +363,12 @@ k_m2l_lanes(LanesParams<T> p, OpTables<T> t) {
     const int64_t spp = pp + ddx + npx * ((int64_t)ddy + npx * (int64_t)ddz);
     if (p.smask && !p.smask[(int64_t)sg * npp + spp]) continue;   // no sources there
     // a target list's lanes hold boxes that are not neighbours: each reads
-    // its source's coefficients contiguously there (box-major copy)
-    const int64_t cs = p.boxmajor ? 1 : npp;
-    const T2* src = (const T2*)p.lin_raw + (int64_t)sg * V * npp + (p.boxmajor ? spp * V : spp);
+    // its source's coefficients contiguously there (box-major copy); sparse
+    // storage: the source parent's slot column (the zero column where none)
+    const int64_t lstride = p.pmap ? p.lin_stride : npp;
+    const int64_t col = p.pmap ? (int64_t)p.pmap[spp] : spp;
+    const int64_t cs = p.boxmajor ? 1 : lstride;
+    const T2* src = (const T2*)p.lin_raw + (int64_t)sg * V * lstride + (p.boxmajor ? col * V : col);
     if (HELM) {
       // stage A: copy the source into the lane's column with e^{i m ch}
 #pragma unroll
@@ -531,7 +536,9 @@ k_m2l_lanes(LanesParams<T> p, OpTables<T> t) {
   }
   if (!active) return;
   const int nc = (P + 1) * (P + 1);
-  const int64_t b = (pmort << 3) | tau;
+  const int64_t g0 = compact_box(p.gmap, pmort << 3);   // storage index of the group
+  if (g0 < 0) return;   // (targets lie in stored groups)
+  const int64_t b = g0 | tau;
   if (p.nsplit == 1) {
     if (HELM) {
       for (int c = 0; c < V; c++) {
@@ -733,12 +740,12 @@ int lanes_to_lin(const T* arr, int level, int N, int scale_e, void* lin, cudaStr
 
 template <typename T, bool HELM>
 int lanes_to_lin_groups(const T* arr, int64_t groups, int N, int scale_e, void* lin,
-                        cudaStream_t s) {
+                        cudaStream_t s, bool boxmajor) {
   typedef typename V2t<T>::t T2;
   const int V = HELM ? (N + 1) * (N + 1) : (N + 1) * (N + 2) / 2;
   const int64_t tot = (groups + 1) * V * 8;
   k_to_lin_groups<T, HELM><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(arr, groups, N, scale_e,
-                                                                         (T2*)lin);
+                                                                         boxmajor, (T2*)lin);
   WBFMM_CUDA(cudaGetLastError());
   return 0;
 }
@@ -862,7 +869,7 @@ int launch_m2l_lanes(const LanesParams<T>& p, const OpTables<T>& t,
 
 #define WBFMM_LANES_INST(T, H)                                                   \
   template int lanes_to_lin<T, H>(const T*, int, int, int, void*, cudaStream_t, bool); \
-  template int lanes_to_lin_groups<T, H>(const T*, int64_t, int, int, void*, cudaStream_t); \
+  template int lanes_to_lin_groups<T, H>(const T*, int64_t, int, int, void*, cudaStream_t, bool); \
   template int launch_lanes_reduce<T, H>(const LanesParams<T>&, cudaStream_t);   \
   template bool lanes_supported<T, H>(int, int);                                 \
   template int launch_m2l_lanes<T, H>(const LanesParams<T>&, const OpTables<T>&, \

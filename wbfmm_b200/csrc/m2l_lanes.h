@@ -33,10 +33,11 @@ struct LanesParams {
   const uint8_t* smask; // [8][padded grid]: source box holds sources, or null (all)
   int boxmajor;         // lin_raw is [8][padded grid][V] (lanes_to_lin), not [8][V][grid]
   void* partial_raw;    // [nsplit][8][V][np] complex when nsplit > 1
-  // sparse storage (tile kernel): lin_raw is [8][V][lin_stride] over the
-  // source slots (lanes_to_lin_groups), pmap maps the padded parent grid to
-  // a slot (lin_stride - 1, a zero column, where no group is stored), gmap
-  // the target groups to their slots; null for dense storage
+  // sparse storage: lin_raw is [8][V][lin_stride] (box-major:
+  // [8][lin_stride][V]) over the source slots (lanes_to_lin_groups), pmap
+  // maps the padded parent grid to a slot (lin_stride - 1, a zero column,
+  // where no group is stored), gmap the target groups to their slots; null
+  // for dense storage
   const uint32_t* pmap;
   const uint32_t* gmap;
   int64_t lin_stride;
@@ -104,11 +105,12 @@ int lanes_to_lin(const T* arr, int level, int N, int scale_e, void* lin, cudaStr
                  bool boxmajor = false);
 size_t lanes_lin_bytes(int level, int N, bool helm, size_t tsize);
 // sparse storage: a level's compact array (groups slots, Layout L per
-// group) -> lin[tau][c][slot] over groups + 1 slots (the last zero), degree
-// n scaled by 2^(scale_e n); bytes: lanes_lin_groups_bytes
+// group) -> lin[tau][c][slot] (boxmajor: lin[tau][slot][c]) over groups + 1
+// slots (the last zero), degree n scaled by 2^(scale_e n); bytes:
+// lanes_lin_groups_bytes
 template <typename T, bool HELM>
 int lanes_to_lin_groups(const T* arr, int64_t groups, int N, int scale_e, void* lin,
-                        cudaStream_t s);
+                        cudaStream_t s, bool boxmajor = false);
 size_t lanes_lin_groups_bytes(int64_t groups, int N, bool helm, size_t tsize);
 // pmap[pp] = slot of the parent at padded-grid position pp (gmap of the
 // level), or `groups` (the zero column) on the padding and for parents

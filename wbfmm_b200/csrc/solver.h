@@ -881,7 +881,7 @@ struct Solver : public wbfmm_b200_solver {
     const int lanes_max = helm ? 7 : sizeof(T) == 8 ? 9 : 10;
     bool use_tiles = false, use_lanes = false;
     const int he = helm ? helm_e[level] : 0;
-    if (cfg.sparse) return m2l_sparse(level, x, he, tiles_ok);
+    if (cfg.sparse) return m2l_sparse(level, x, he, tiles_ok, lanes_ok, lanes_max);
     // tensor cores: Laplace, FP32, equal orders up to (p+1)^2 = 256, mode 4
     if (!helm && sizeof(T) == 4 && m2l_mode == 4 && tc_lap_supported(x.Nin, x.Nout))
       return m2l_tc(level, x);
@@ -1005,21 +1005,26 @@ struct Solver : public wbfmm_b200_solver {
                 : launch_m2l<T, false>(x, tables, stream);
   }
 
-  // The M2L of a level with sparse storage: the tile kernel on the
-  // compact transposed sources (one column per stored source group and a
-  // zero column), source parents found through the padded-grid slot map,
-  // targets from the level's active lists written at their slots
-  int m2l_sparse(int level, const XlateParams<T>& x, int he, bool tiles_ok) {
+  // The M2L of a level with sparse storage: the lane or tile kernel (the
+  // automatic choice, or the one set with set_m2l_kernel 2 / 3) on compact
+  // transposed sources, one column per stored source group and a zero
+  // column, source parents found through the padded-grid slot map, targets
+  // from the level's active lists written at their slots
+  int m2l_sparse(int level, const XlateParams<T>& x, int he, bool tiles_ok, bool lanes_ok,
+                 int lanes_max) {
     bool dense = false;
-    const int tc = helm ? tiles_per_cta<T, true>(x.Nin, &dense, true)
-                        : tiles_per_cta<T, false>(x.Nin, nullptr, true);
-    if (!tiles_ok || tc == 0)
+    const int tc = !tiles_ok ? 0
+                   : helm ? tiles_per_cta<T, true>(x.Nin, &dense, true)
+                          : tiles_per_cta<T, false>(x.Nin, nullptr, true);
+    bool use_lanes = !he && lanes_ok && (m2l_mode == 2 || (m2l_mode != 3 && x.Nin <= lanes_max));
+    if (!use_lanes && tc == 0) use_lanes = !he && lanes_ok;
+    if (!use_lanes && tc == 0)
       return set_error(WBFMM_B200_E_ORDER, "sparse level storage: the M2L needs equal orders in [2, 60] at each level");
     const int64_t G = ngroups[level];
-    WBFMM_TRY(lin.alloc(lanes_lin_groups_bytes(G, x.Nin, helm, sizeof(T))));
     const int se = helm ? he : x.lap_e;
-    WBFMM_TRY((helm ? lanes_to_lin_groups<T, true>(x.cin, G, x.Nin, se, lin.p, stream)
-                    : lanes_to_lin_groups<T, false>(x.cin, G, x.Nin, se, lin.p, stream)));
+    WBFMM_TRY(lin.alloc(lanes_lin_groups_bytes(G, x.Nin, helm, sizeof(T))));
+    WBFMM_TRY((helm ? lanes_to_lin_groups<T, true>(x.cin, G, x.Nin, se, lin.p, stream, use_lanes)
+                    : lanes_to_lin_groups<T, false>(x.cin, G, x.Nin, se, lin.p, stream, use_lanes)));
     WBFMM_TRY(pmap.alloc(source_mask_bytes(level) / 8));
     WBFMM_TRY(build_parent_slot_map(gmap[level].p, level, (uint32_t)G, pmap.p, stream));
     LanesParams<T> lp;
@@ -1031,6 +1036,7 @@ struct Solver : public wbfmm_b200_solver {
     lp.helm_e = he;
     lp.act = act[level].p; lp.act_n = act_n[level].p;
     lp.pmap = pmap.p; lp.gmap = gmap[level].p; lp.lin_stride = G + 1;
+    lp.boxmajor = use_lanes ? 1 : 0;
     WBFMM_TRY(smask.alloc(source_mask_bytes(level)));
     WBFMM_TRY(build_source_mask(x.src_n, level, smask.p, stream));
     lp.smask = smask.p;
@@ -1041,16 +1047,21 @@ struct Solver : public wbfmm_b200_solver {
       lp.lapsr = lapsr.p;
       launches++;
     }
-    if (dense) {
+    if (!use_lanes && dense) {
       WBFMM_TRY(hcx.alloc(helm_coax_rows_count(x.Nin)));
       WBFMM_TRY(build_helm_coax_rows<T>(x.coax, x.coax_stride, x.Nin, hcx.p, stream));
       lp.hcx = hcx.p;
       launches++;
     }
     const int64_t np = (int64_t)1 << (3 * (level - 1));
-    const int64_t ctas = ((np + tc - 1) / tc) * 8;
     int ns = 1;
-    while (ctas * ns < 2 * 148 && ns < 32) ns *= 2;
+    if (use_lanes) {
+      const int64_t base = ((np + 127) / 128) * 8;
+      while (base * ns < lanes_ctas && ns < 32) ns *= 2;
+    } else {
+      const int64_t ctas = ((np + tc - 1) / tc) * 8;
+      while (ctas * ns < 2 * 148 && ns < 32) ns *= 2;
+    }
     lp.nsplit = ns;
     if (ns > 1) {
       const int V = helm ? (x.Nin + 1) * (x.Nin + 1) : (x.Nin + 1) * (x.Nin + 2) / 2;
@@ -1058,6 +1069,9 @@ struct Solver : public wbfmm_b200_solver {
       lp.partial_raw = lanes_part.p;
     }
     launches += 3 + (ns > 1 ? 2 : 1);
+    if (use_lanes)
+      return helm ? launch_m2l_lanes<T, true>(lp, tables, stream)
+                  : launch_m2l_lanes<T, false>(lp, tables, stream);
     return helm ? launch_m2l_tiles<T, true>(lp, tables, stream)
                 : launch_m2l_tiles<T, false>(lp, tables, stream);
   }
