@@ -105,7 +105,8 @@ int wbfmm_b200_device_count(void);
 int wbfmm_b200_solver_create(wbfmm_b200_solver_t **s,
                              const wbfmm_b200_config_t *cfg, void *stream);
 int wbfmm_b200_solver_destroy(wbfmm_b200_solver_t *s);
-/* bytes of device memory the solver would hold for n sources and m targets */
+/* bytes of device memory the solver would hold for n sources and m targets
+   (dense level storage; an upper bound for sparse storage) */
 int64_t wbfmm_b200_footprint(const wbfmm_b200_config_t *cfg, int64_t nsrc,
                              int64_t ntgt);
 
@@ -350,7 +351,8 @@ int wbfmm_b200_fp32_range_ok(const wbfmm_b200_config_t *cfg);
 /* ------------------------------------------------------------------------
    Served form (no reference counterpart): continuous batching of
    independent solves on one GPU.  `nslots` solves run at once, each on its
-   own stream, admitted first come first served while the summed
+   own stream, admitted first come first served (or largest first,
+   wbfmm_b200_server_set_order) while the summed
    wbfmm_b200_footprint of the solves in flight stays within `hbm_budget`
    bytes less the slots' allowance for keeping work buffers between solves
    (per slot hbm_budget / (4 nslots), at most 4 GB; a slot whose buffers
@@ -391,12 +393,12 @@ double wbfmm_b200_server_clock(wbfmm_b200_server_t *srv);
    the budget */
 int wbfmm_b200_server_submit(wbfmm_b200_server_t *srv,
                              const wbfmm_b200_request_t *req, int64_t *ticket);
-/* 1 when the request has completed, 0 when not yet */
 /* Order in which free slots take the requests that have arrived: 0 (the
    default) first come first served; 1 the largest device-memory footprint
    first (for batches submitted together: the big solves start first and the
    small ones fill the end, which shortens the batch's span). */
 int wbfmm_b200_server_set_order(wbfmm_b200_server_t *srv, int largest_first);
+/* 1 when the request has completed, 0 when not yet */
 int wbfmm_b200_server_poll(wbfmm_b200_server_t *srv, int64_t ticket);
 /* blocks until the request has completed; returns its status */
 int wbfmm_b200_server_wait(wbfmm_b200_server_t *srv, int64_t ticket);
