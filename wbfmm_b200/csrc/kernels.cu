@@ -737,11 +737,12 @@ int launch_l2p(const EvalParams<T>& p, cudaStream_t s) {
 // One CTA per target leaf box.  The sources of the 27 neighbour boxes (a
 // virtual list, box by box) are staged through shared memory in tiles of NT
 // (the CTA's thread count: 128, or 32 for trees whose leaves hold a few
-// points each, so that more boxes are resident per SM).  Each target is
-// swept by a group of G threads (G a power of two, as large as the box's
-// target count leaves room for, at most 32): thread g of the group takes
-// tile entries g, g+G, ..., accumulating in FP64 registers in a fixed order,
-// and the group's partial sums are added by shuffles at the end.  The FP32
+// points each, so that more boxes are resident per SM).  The box's targets
+// are taken NT at a time, the m of a pass spread over all NT threads (NT/m
+// or NT/m + 1 consecutive threads per target, so that no thread idles
+// whatever m is): thread gl of a target's g takes tile entries gl, gl + g,
+// ..., accumulating in FP64 registers in a fixed order, and the target's
+// first thread adds its threads' sums in thread order.  The FP32
 // form computes pair terms in FP32 from separations that keep FP64 accuracy
 // (coordinates as float pairs hi + lo, the hi parts of neighbouring points
 // subtracting exactly), sums each run of 8 of a thread's terms in FP32 and
@@ -886,6 +887,7 @@ k_p2p(EvalParams<T> p) {
   constexpr int NA = HELM ? 8 : 4;
   __shared__ P2PTile<T, HELM, NT> tl;
   __shared__ uint32_t s_st[27], s_pref[28];
+  __shared__ double s_red[NA][NT];     // each lane's sums, for its target's group
   const int64_t b = blockIdx.x;
   const uint32_t tc = p.tcount[b];
   if (tc == 0) return;
@@ -914,6 +916,7 @@ k_p2p(EvalParams<T> p) {
   }
   __syncthreads();
   const uint32_t total = s_pref[27];
+  if (total == 0) return;   // no sources near: the whole CTA, before any other barrier
   const T rc2 = T(kCutoffRadius * kCutoffRadius);
   const T k = p.k;
   const T kinv = HELM ? T(1) / k : T(0);
@@ -923,12 +926,18 @@ k_p2p(EvalParams<T> p) {
   float2* xp = (float2*)tl.x;
   float2* yp = (float2*)tl.y;
   float2* zp = (float2*)tl.z;
-  int G = 32;
-  while (G > 1 && (uint32_t)(NT / G) < tc) G >>= 1;
-  const int gl = tid & (G - 1), ti = tid / G, tpp = NT / G;
-  for (uint32_t t0 = 0; t0 < tc; t0 += tpp) {
-    const bool active = t0 + ti < tc;
-    const uint32_t jt = p.tstart[b] + t0 + (active ? ti : 0);
+  // Each pass takes m = min(NT, targets left) targets and spreads them over
+  // all NT lanes: NT / m lanes per target, one more for the first
+  // NT mod m targets, the lanes of a target consecutive; lane gl of a
+  // target's g lanes takes tile entries gl, gl + g, ... (every lane busy
+  // whatever the box's target count)
+  for (uint32_t t0 = 0; t0 < tc; t0 += NT) {
+    const int m = (int)min((uint32_t)NT, tc - t0);
+    const int glo = NT / m, extra = NT - glo * m, split = extra * (glo + 1);
+    const int ti = tid < split ? tid / (glo + 1) : extra + (tid - split) / glo;
+    const int g = tid < split ? glo + 1 : glo;
+    const int gl = tid < split ? tid % (glo + 1) : (tid - split) % glo;
+    const uint32_t jt = p.tstart[b] + t0 + ti;
     const double x = p.tx[jt], y = p.ty[jt], z = p.tz[jt];
     const float txh = (float)x, tyh = (float)y, tzh = (float)z;
     const float txl = (float)(x - (double)txh), tyl = (float)(y - (double)tyh),
@@ -961,7 +970,6 @@ k_p2p(EvalParams<T> p) {
         if (hd) { tl.nx[tid] = p.nx[s]; tl.ny[tid] = p.ny[s]; tl.nz[tid] = p.nz[s]; }
       }
       __syncthreads();
-      if (!active) continue;
       const int nt = (int)min((uint32_t)NT, total - f0);
       if constexpr (F32) {
         // runs of kP2PRun pairs: a full run without bounds checks, the
@@ -974,21 +982,21 @@ k_p2p(EvalParams<T> p) {
           const T r2 = rx * rx + ry * ry + rz * rz;
           p2p_pair<T, HELM, NT, POT, GRAD, true>(tl, j, rx, ry, rz, r2, k, kinv, hd, acc, rc2);
         };
-        for (int j0 = gl; j0 < nt; j0 += kP2PRun * G) {
+        for (int j0 = gl; j0 < nt; j0 += kP2PRun * g) {
           T acc[NA];
           for (int c = 0; c < NA; c++) acc[c] = T(0);
-          if (j0 + (kP2PRun - 1) * G < nt) {
+          if (j0 + (kP2PRun - 1) * g < nt) {
 #pragma unroll
-            for (int u = 0; u < kP2PRun; u++) pair_at(j0 + u * G, acc);
+            for (int u = 0; u < kP2PRun; u++) pair_at(j0 + u * g, acc);
           } else {
 #pragma unroll
             for (int u = 0; u < kP2PRun; u++)
-              if (j0 + u * G < nt) pair_at(j0 + u * G, acc);
+              if (j0 + u * g < nt) pair_at(j0 + u * g, acc);
           }
           for (int c = 0; c < NA; c++) a[c] += (double)acc[c];
         }
       } else {
-        for (int j = gl; j < nt; j += G) {
+        for (int j = gl; j < nt; j += g) {
           // separation formed in FP64, the rest in T
           const T rx = (T)(x - tl.x[j]), ry = (T)(y - tl.y[j]), rz = (T)(z - tl.z[j]);
           const T r2 = rx * rx + ry * ry + rz * rz;
@@ -1000,14 +1008,17 @@ k_p2p(EvalParams<T> p) {
         }
       }
     }
-    // sum over the group (lanes of one warp; inactive groups hold zeros)
+    // the sums of a target's lanes, in lane order, by its first lane (the
+    // next pass writes s_red only after its first tile barrier)
+    for (int c = 0; c < NA; c++) s_red[c][tid] = a[c];
+    __syncthreads();
+    if (gl != 0) continue;
     double v[8];
     for (int c = 0; c < NA; c++) {
-      v[c] = a[c];
-      for (int o = 1; o < G; o <<= 1) v[c] += __shfl_xor_sync(0xffffffffu, v[c], o);
-      v[c] *= p2p_scale<HELM>(c, (double)p.k);
+      double sum = s_red[c][tid];
+      for (int i = 1; i < g; i++) sum += s_red[c][tid + i];
+      v[c] = sum * p2p_scale<HELM>(c, (double)p.k);
     }
-    if (!active || gl != 0) continue;
     const uint32_t o = p.tperm[jt];
     if (HELM) {
       if (want_pot) {
