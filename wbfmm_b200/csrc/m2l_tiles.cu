@@ -18,6 +18,10 @@
 // a source value 2.  The order is a runtime parameter; TC (32, 16 or 8) is
 // the largest whose three vector blocks fit beside the operator.  Laplace
 // uses half vectors (m >= 0), as the reference's real-packed coefficients.
+// Per offset: the column map (double-buffered, so that it is built while
+// the previous offset's stage D still reads its own) and one barrier; the
+// operator staging and stage A in one phase (A reads its phases from the
+// table, not the staged copy), then B, C and D, four barriers in all.
 #include <cuda_runtime.h>
 
 #include "engine.h"
@@ -116,7 +120,7 @@ __host__ __device__ TilePlan tile_plan(int P, int TC, bool dense, bool sparse) {
   size_t ops = sizeof(T) * ((size_t)q.cx_off + q.ncx);
   q.ops_bytes = (ops + 15) & ~(size_t)15;
   q.desc_bytes = ((sizeof(int) * (size_t)(q.nB + (q.dense ? 2 : 1) * q.nC + q.V) +
-                   (sparse ? 4 : 3) * sizeof(int) * TC) + 15) & ~(size_t)15;
+                   (sparse ? 5 : 4) * sizeof(int) * TC) + 15) & ~(size_t)15;
   q.vec_bytes = 3 * sizeof(typename C2<T>::t) * (size_t)q.V * TC;
   q.total = q.ops_bytes + q.desc_bytes + q.vec_bytes;
   return q;
@@ -151,6 +155,19 @@ TileChoice pick_tc(int P, bool sparse) {
   return best;
 }
 
+// the 4 consecutive columns of a thread's register tile (16-byte aligned:
+// row offsets are multiples of TC and t0 of 4): two 16-byte loads for FP32
+__device__ __forceinline__ void load_cols(const float2* p, float2 (&o)[4]) {
+  const float4 a = reinterpret_cast<const float4*>(p)[0];
+  const float4 b = reinterpret_cast<const float4*>(p)[1];
+  o[0] = make_float2(a.x, a.y); o[1] = make_float2(a.z, a.w);
+  o[2] = make_float2(b.x, b.y); o[3] = make_float2(b.z, b.w);
+}
+__device__ __forceinline__ void load_cols(const double2* p, double2 (&o)[4]) {
+#pragma unroll
+  for (int k = 0; k < 4; k++) o[k] = p[k];
+}
+
 template <typename T2, typename T>
 __device__ __forceinline__ T2 cmul(T2 a, T er, T ei) {
   T2 r;
@@ -159,8 +176,10 @@ __device__ __forceinline__ T2 cmul(T2 a, T er, T ei) {
   return r;
 }
 
+// resident CTAs the register budget is sized for: the shared-memory limit
+// of the serving orders (FP32 Laplace 3 per SM at p = 14, the others 2)
 template <typename T, bool HELM>
-__global__ void __launch_bounds__(kTileThreads)
+__global__ void __launch_bounds__(kTileThreads, (HELM || sizeof(T) == 8) ? 2 : 3)
 k_m2l_tiles(LanesParams<T> p, OpTables<T> t, int TC, bool dense) {
   typedef typename C2<T>::t T2;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -175,8 +194,8 @@ k_m2l_tiles(LanesParams<T> p, OpTables<T> t, int TC, bool dense) {
   int* s_nm = dC + q.nC;             // (n, m) of each vector entry
   int* s_pp = s_nm + V;              // padded-grid index of each target's parent
   int* s_act = s_pp + TC;            // 1 + parent linear index, 0: no target
-  int* s_map = s_act + TC;           // the offset's columns: target of each
-  int* s_src = s_map + TC;           // sparse: each target's source column in lin
+  int* s_map = s_act + TC;           // the offset's columns: target of each (two buffers)
+  int* s_src = s_map + 2 * TC;       // sparse: each target's source column in lin
   int* dCo = s_src + (q.sparse ? TC : 0);   // Helmholtz: row offset of each C row pair
   T2* X = (T2*)(smraw + q.ops_bytes + q.desc_bytes);
   T2* Y = X + (size_t)V * TC;
@@ -256,13 +275,19 @@ k_m2l_tiles(LanesParams<T> p, OpTables<T> t, int TC, bool dense) {
         f = sx >= 1 && sx <= nx && sy >= 1 && sy <= nx && sz >= 1 && sz <= nx;
       }
     }
-    const int cnt = __syncthreads_count(f);
-    if (cnt == 0) continue;
+    // the columns (targets in warp 0: TC <= 32), into the buffer that the
+    // offset before last read in its stage D (finished before the last
+    // barrier); stage D of the previous offset reads the other one
+    int* smap = s_map + ((j - split) / p.nsplit & 1) * TC;
     if (tid < 32) {
       const unsigned bal = __ballot_sync(0xffffffffu, f);
-      if (f) s_map[__popc(bal & ((1u << tid) - 1u))] = tid;
+      if (f) smap[__popc(bal & ((1u << tid) - 1u))] = tid;
     }
+    const int cnt = __syncthreads_count(f);
+    if (cnt == 0) continue;
     const int TQ = (cnt + 3) / 4, TCc = 4 * TQ;
+    // the operator into shared memory and (same phase, one barrier) stage A:
+    // the TC source vectors with e^{i m ch}, the phases read from the table
     {
       const T* H = t.H + (int64_t)t.op_ith[op] * t.hstride;
       for (int i = tid; i < q.NH; i += kTileThreads) sH[i] = H[i];
@@ -285,9 +310,8 @@ k_m2l_tiles(LanesParams<T> p, OpTables<T> t, int TC, bool dense) {
         for (int i = tid; i < q.ncx; i += kTileThreads) scx[i] = cx[i];
       }
     }
-    __syncthreads();   // operator staged
-    // stage A: the TC source vectors, with e^{i m ch}
     {
+      const T* ech = t.ch + (size_t)op * (t.lmax + 1) * 2;
       const T2* src = (const T2*)p.lin_raw + (int64_t)sg * V * lstride + (q.sparse ? 0 : doff);
       const int* col = q.sparse ? s_src : s_pp;
       for (int i = tid; i < V * TCc; i += kTileThreads) {
@@ -295,9 +319,10 @@ k_m2l_tiles(LanesParams<T> p, OpTables<T> t, int TC, bool dense) {
         T2 v;
         v.x = T(0); v.y = T(0);
         if (tt < cnt) {
-          v = src[(int64_t)c * lstride + col[s_map[tt]]];
+          v = src[(int64_t)c * lstride + col[smap[tt]]];
           const int m = (s_nm[c] >> 8) - 64, am = m < 0 ? -m : m;
-          v = cmul(v, sech[2 * am], m < 0 ? -sech[2 * am + 1] : sech[2 * am + 1]);
+          const T er = __ldg(ech + 2 * am), ei = __ldg(ech + 2 * am + 1);
+          v = cmul(v, er, m < 0 ? -ei : ei);
         }
         X[(size_t)c * TC + tt] = v;
       }
@@ -323,18 +348,22 @@ k_m2l_tiles(LanesParams<T> p, OpTables<T> t, int TC, bool dense) {
         const T2* xr = X + (size_t)cidx(n, -n) * TC + t0;
         for (int m = n; m > 0; m--, xr += TC) {
           const T h0 = rn0[m], h1 = rn1[m];
+          T2 xv[4];
+          load_cols(xr, xv);
 #pragma unroll
           for (int k = 0; k < 4; k++) {
-            const T2 x = xr[k];
+            const T2 x = xv[k];
             a0[k].x += h0 * x.x; a0[k].y += h0 * x.y;
             a1[k].x += h1 * x.x; a1[k].y += h1 * x.y;
           }
         }
         for (int m = 0; m <= n; m++, xr += TC) {
           const T h0 = rp0[m], h1 = rp1[m];
+          T2 xv[4];
+          load_cols(xr, xv);
 #pragma unroll
           for (int k = 0; k < 4; k++) {
-            const T2 x = xr[k];
+            const T2 x = xv[k];
             a0[k].x += h0 * x.x; a0[k].y += h0 * x.y;
             a1[k].x += h1 * x.x; a1[k].y += h1 * x.y;
           }
@@ -358,9 +387,11 @@ k_m2l_tiles(LanesParams<T> p, OpTables<T> t, int TC, bool dense) {
             m1 = sH[hb + (-nu0 - 1 + n) * (n + 1) + m];
           }
           if (m == 0) { m0 = T(0); m1 = T(0); }
+          T2 xv[4];
+          load_cols(xr, xv);
 #pragma unroll
           for (int k = 0; k < 4; k++) {
-            const T2 x = xr[k];
+            const T2 x = xv[k];
             a0[k].x += (p0 + m0) * x.x; a0[k].y += (p0 - m0) * x.y;
             a1[k].x += (p1 + m1) * x.x; a1[k].y += (p1 - m1) * x.y;
           }
@@ -410,18 +441,22 @@ k_m2l_tiles(LanesParams<T> p, OpTables<T> t, int TC, bool dense) {
               c1i = sg1 * scx[2 * ic + 1];
             }
           }
+          T2 yv[4];
+          load_cols(yr, yv);
 #pragma unroll
           for (int k = 0; k < 4; k++) {
-            const T2 y = yr[k];
+            const T2 y = yv[k];
             a0[k].x += c0r * y.x - c0i * y.y; a0[k].y += c0i * y.x + c0r * y.y;
             a1[k].x += c1r * y.x - c1i * y.y; a1[k].y += c1i * y.x + c1r * y.y;
           }
         } else {
           const T c0 = scx[(n0 * (P + 1) + l) * (P + 1) + m];
           const T c1 = two ? scx[((n0 + 1) * (P + 1) + l) * (P + 1) + m] : T(0);
+          T2 yv[4];
+          load_cols(yr, yv);
 #pragma unroll
           for (int k = 0; k < 4; k++) {
-            const T2 y = yr[k];
+            const T2 y = yv[k];
             a0[k].x += c0 * y.x; a0[k].y += c0 * y.y;
             a1[k].x += c1 * y.x; a1[k].y += c1 * y.y;
           }
@@ -460,18 +495,22 @@ k_m2l_tiles(LanesParams<T> p, OpTables<T> t, int TC, bool dense) {
         const T2* xr = X + (size_t)cidx(n, -n) * TC + t0;
         for (int m = n; m > 0; m--, xr += TC) {
           const T h0 = rn0[m], h1 = rn1[m];
+          T2 xv[4];
+          load_cols(xr, xv);
 #pragma unroll
           for (int k = 0; k < 4; k++) {
-            const T2 x = xr[k];
+            const T2 x = xv[k];
             a0[k].x += h0 * x.x; a0[k].y += h0 * x.y;
             a1[k].x += h1 * x.x; a1[k].y += h1 * x.y;
           }
         }
         for (int m = 0; m <= n; m++, xr += TC) {
           const T h0 = rp0[m], h1 = rp1[m];
+          T2 xv[4];
+          load_cols(xr, xv);
 #pragma unroll
           for (int k = 0; k < 4; k++) {
-            const T2 x = xr[k];
+            const T2 x = xv[k];
             a0[k].x += h0 * x.x; a0[k].y += h0 * x.y;
             a1[k].x += h1 * x.x; a1[k].y += h1 * x.y;
           }
@@ -484,7 +523,7 @@ k_m2l_tiles(LanesParams<T> p, OpTables<T> t, int TC, bool dense) {
           for (int k = 0; k < 4; k++) {
             if (t0 + k >= cnt) break;
             const T2 o = cmul(r ? a1[k] : a0[k], er, ei);
-            T2& a = ar[s_map[t0 + k]];
+            T2& a = ar[smap[t0 + k]];
             a.x += o.x; a.y += o.y;
           }
         }
@@ -499,9 +538,11 @@ k_m2l_tiles(LanesParams<T> p, OpTables<T> t, int TC, bool dense) {
             m1 = sH[hb + (-nu0 - 1 + n) * (n + 1) + m];
           }
           if (m == 0) { m0 = T(0); m1 = T(0); }
+          T2 xv[4];
+          load_cols(xr, xv);
 #pragma unroll
           for (int k = 0; k < 4; k++) {
-            const T2 x = xr[k];
+            const T2 x = xv[k];
             a0[k].x += (p0 + m0) * x.x; a0[k].y += (p0 - m0) * x.y;
             a1[k].x += (p1 + m1) * x.x; a1[k].y += (p1 - m1) * x.y;
           }
@@ -514,7 +555,7 @@ k_m2l_tiles(LanesParams<T> p, OpTables<T> t, int TC, bool dense) {
           for (int k = 0; k < 4; k++) {
             if (t0 + k >= cnt) break;
             const T2 a = r ? a1[k] : a0[k];
-            T2& o = ar[s_map[t0 + k]];
+            T2& o = ar[smap[t0 + k]];
             o.x += er * a.x + ei * a.y;
             if (nu != 0) o.y += er * a.y - ei * a.x;
           }
