@@ -880,7 +880,10 @@ __device__ __forceinline__ double p2p_scale(int c, double k) {
 // caps measured best (FP32 Helmholtz pot+grad evaluation of 2e5 points:
 // 1.152 ms before the masking, 1.130 ms masked, 1.046 ms with 4 CTAs, 1.093
 // with 5; Laplace 0.615 / 0.564 / 0.566 / 0.544 ms)
-template <typename T, bool HELM, int NT, bool POT, bool GRAD>
+// DIP: dipole sources (p.dip set), fixed at compile time so that the
+// monopole kernels carry no dipole code (a smaller loop body: fewer
+// instruction-fetch stalls)
+template <typename T, bool HELM, int NT, bool POT, bool GRAD, bool DIP>
 __global__ void __launch_bounds__(NT, NT == 32 ? 20 : (HELM ? 4 : 5))
 k_p2p(EvalParams<T> p) {
   constexpr bool F32 = sizeof(T) == 4;
@@ -920,8 +923,8 @@ k_p2p(EvalParams<T> p) {
   const T rc2 = T(kCutoffRadius * kCutoffRadius);
   const T k = p.k;
   const T kinv = HELM ? T(1) / k : T(0);
-  const bool hq = p.q != nullptr, hd = p.dip != nullptr;
-  constexpr bool want_pot = POT, want_grad = GRAD;
+  const bool hq = p.q != nullptr;
+  constexpr bool hd = DIP, want_pot = POT, want_grad = GRAD;
   // FP32 form: source coordinates as float pairs (hi, lo) in the FP64 arrays' bytes
   float2* xp = (float2*)tl.x;
   float2* yp = (float2*)tl.y;
@@ -1040,16 +1043,21 @@ k_p2p(EvalParams<T> p) {
 template <typename T, bool HELM>
 int launch_p2p(const EvalParams<T>& p, cudaStream_t s) {
   if (p.nbox <= 0 || p.ntgt <= 0) return 0;
-  auto go = [&](auto pot, auto grad) {
+  auto go = [&](auto pot, auto grad, auto dip) {
     constexpr bool P = decltype(pot)::value, G = decltype(grad)::value;
+    constexpr bool D = decltype(dip)::value;
     if (p.ntgt <= 8 * p.nbox)   // a few targets per leaf on average
-      k_p2p<T, HELM, 32, P, G><<<(unsigned)p.nbox, 32, 0, s>>>(p);
+      k_p2p<T, HELM, 32, P, G, D><<<(unsigned)p.nbox, 32, 0, s>>>(p);
     else
-      k_p2p<T, HELM, 128, P, G><<<(unsigned)p.nbox, 128, 0, s>>>(p);
+      k_p2p<T, HELM, 128, P, G, D><<<(unsigned)p.nbox, 128, 0, s>>>(p);
   };
-  if (p.pot && p.grad) go(std::true_type(), std::true_type());
-  else if (p.pot) go(std::true_type(), std::false_type());
-  else if (p.grad) go(std::false_type(), std::true_type());
+  auto fields = [&](auto dip) {
+    if (p.pot && p.grad) go(std::true_type(), std::true_type(), dip);
+    else if (p.pot) go(std::true_type(), std::false_type(), dip);
+    else if (p.grad) go(std::false_type(), std::true_type(), dip);
+  };
+  if (p.dip) fields(std::true_type());
+  else fields(std::false_type());
   WBFMM_CUDA(cudaGetLastError());
   return 0;
 }
