@@ -794,10 +794,21 @@ __device__ __forceinline__ void sincos_near(float x, float* sp, float* cp) {
 // MASKED: a pair within the cutoff (r2 <= rc2) takes 1/r = 0, which makes
 // each of its terms an exact zero, instead of being branched around (the
 // pairs of a run then interleave without divergence)
+// 1/sqrt(x) of a pair: in FP32 the MUFU approximation alone
+// (rsqrt.approx.ftz: no subnormal handling, which a squared distance above
+// the cutoff, at least 1e-12, never needs; for such normal arguments it is
+// the approximation rsqrtf returns)
+__device__ __forceinline__ float pair_rsqrt(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ double pair_rsqrt(double x) { return rsqrt(x); }
+
 template <typename T, bool HELM, int NT, bool want_pot, bool want_grad, bool MASKED = false>
 __device__ __forceinline__ void p2p_pair(const P2PTile<T, HELM, NT>& tl, int j, T rx, T ry, T rz,
                                          T r2, T k, T kinv, bool hd, T* acc, T rc2 = T(0)) {
-  const T ir = MASKED ? (r2 > rc2 ? rsqrt(r2) : T(0)) : rsqrt(r2);
+  const T ir = MASKED ? (r2 > rc2 ? pair_rsqrt(r2) : T(0)) : pair_rsqrt(r2);
   if (HELM) {
     const T r = r2 * ir;
     T kr = k * r, ikr, sn, cs;
