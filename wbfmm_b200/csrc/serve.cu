@@ -58,17 +58,24 @@ struct Req {
 struct Pinned {
   double* p = nullptr;
   size_t n = 0;
-  ~Pinned() { if (p) cudaFreeHost(p); }
+  // outgrown buffers, freed with the server: cudaFreeHost synchronises the
+  // device, which would stall every slot's work; growth is geometric, so
+  // they hold less than the current buffer
+  std::vector<double*> retired;
+  ~Pinned() {
+    if (p) cudaFreeHost(p);
+    for (double* r : retired) cudaFreeHost(r);
+  }
   int reserve(size_t count) {
     if (count <= n) return 0;
     const size_t want = std::max(count + count / 4, 2 * n);
-    if (p) cudaFreeHost(p);
-    p = nullptr;
-    n = 0;
-    if (cudaMallocHost(&p, sizeof(double) * want) != cudaSuccess) {
+    double* q = nullptr;
+    if (cudaMallocHost(&q, sizeof(double) * want) != cudaSuccess) {
       cudaGetLastError();
       return set_error(WBFMM_B200_E_NOMEM, "pinned host allocation failed");
     }
+    if (p) retired.push_back(p);   // idle: each solve ends with the slot's event wait
+    p = q;
     n = want;
     return 0;
   }
