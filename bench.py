@@ -30,14 +30,15 @@ dataset).  One step = one batch of SERVE_BATCH requests.
   `served_p50_s` / `served_p99_s` / `plain_p50_s` / `plain_p99_s` are at 70%.
 * accuracy: the served fields of sampled requests against the FP64 GPU
   direct sum (itself pinned to the reference's direct sums).
-* `roofline`: the FP32 near field (the stream's dominant kernel, k_p2p,
-  41% of its device time) on a 2e5-point Helmholtz cube: algorithmic FLOPs
-  of the exact pair count / event time, against the FP32 FMA peak measured
-  live, DRAM traffic from its committed ncu capture.  `roofline_m2l`: the
-  tile M2L (the stream's dominant M2L kernel) on a Laplace
-  order-14 level, against the FP32 FMA peak measured live on the GPU
-  (`wbfmm_b200_fp32_fma_peak`); `traffic` from the committed ncu capture of
-  the same launch.
+* `roofline`: the stream's dominant kernel, the FP32 Helmholtz tile M2L
+  (23% of the stream's device time in profiles/launches_serving_stream_48.md)
+  on an order-14 level (1e5 points, k = 10, level 4): algorithmic FLOPs of
+  the dense level's list-4 pairs / event time, against the FP32 FMA peak
+  measured live on the GPU (`wbfmm_b200_fp32_fma_peak`), `traffic` from the
+  committed ncu capture of the same launch.  `roofline_p2p`: the FP32 near
+  field (k_p2p, the next kernel, 18%) on a 2e5-point Helmholtz cube, exact
+  pair count; `roofline_m2l_laplace`: the Laplace tile M2L on an order-14
+  level (3e5 points, level 5).
 * `cpu_baseline` and `--impl reference`: the reference's own CPU FMM
   (oracle/_ref, the unmodified reference sources, M2L on up to 16 threads)
   run request by request on a bounded sample of the stream.
@@ -862,12 +863,16 @@ def tile_profile_traffic(path=None):
     return tot
 
 
-def tile_roofline(local):
-    """The stream's dominant M2L kernel (the offset-major tile kernel at the
-    stream's Laplace order 14) on a dense level: 3e5 points, depth 5, level
-    5, FP32; algorithmic FLOPs of the rotate / coaxial / rotate-back shifts
-    per launch / CUDA-event launch time (L2 flushed before each), against
-    the FP32 FMA peak measured here."""
+TILE_HELM_PROFILE = os.path.join(ROOT, "profiles", "k_m2l_tiles_helmholtz_1e5_p14_level4.md")
+
+
+def tile_roofline(local, helm: bool):
+    """The offset-major tile M2L on a dense level at the stream's order 14,
+    FP32: Helmholtz (the stream's dominant kernel) on level 4 of 1e5 points
+    (k = 10, depth 4), or Laplace on level 5 of 3e5 points (depth 5);
+    algorithmic FLOPs of the rotate / coaxial / rotate-back shifts per launch
+    / CUDA-event launch time (L2 flushed before each), against the FP32 FMA
+    peak measured here."""
     import torch
 
     from wbfmm_b200 import engine
@@ -875,7 +880,10 @@ def tile_roofline(local):
     dev = torch.device("cuda", local)
     stream = torch.cuda.Stream(dev)
     peak = engine.fp32_fma_peak()
-    p = _cube(engine.LAPLACE, 300_000, 5, 14)
+    if helm:
+        p, level, n = _cube(engine.HELMHOLTZ, 100_000, 4, 14, k=10.0), 4, 100_000
+    else:
+        p, level, n = _cube(engine.LAPLACE, 300_000, 5, 14), 5, 300_000
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     cfg = engine.SolverConfig.from_problem(p, engine.FP32)
     with engine.Solver(cfg, stream=stream.cuda_stream) as s:
@@ -887,29 +895,27 @@ def tile_roofline(local):
             with torch.cuda.stream(stream):
                 flush.zero_()
             a.record(stream)
-            s.m2l(5)
+            s.m2l(level)
             b.record(stream)
             torch.cuda.synchronize(dev)
             if i:
                 times.append(a.elapsed_time(b))
     ms = float(np.mean(times))
-    flops = list4_pairs(5)[5] * lap_flops_per_pair(14)
+    order = p.order_s[level]
+    fpp = helm_flops_per_pair if helm else lap_flops_per_pair
+    flops = list4_pairs(p.depth)[level] * fpp(order)
     achieved = flops / (ms * 1e-3) / 1e12
-    peaks = {}
-    try:
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-    except Exception:
-        pass
-    bf16 = peaks.get("bf16_tflops")
-    return {"bound": "simt", "kernel": "k_m2l_tiles<float, Laplace>: M2L of level 5, order 14, "
-                                       "300,000 points, depth 5",
+    prof = TILE_HELM_PROFILE if helm else TILE_PROFILE
+    name = "Helmholtz, k = 10" if helm else "Laplace"
+    return {"bound": "simt",
+            "kernel": f"k_m2l_tiles<float, {'Helmholtz' if helm else 'Laplace'}>: M2L of level "
+                      f"{level}, order {order}, {n:,} points ({name}), depth {p.depth}",
             "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
             "peak_source": "FP32 FMA throughput measured live (wbfmm_b200_fp32_fma_peak)",
-            "traffic": tile_profile_traffic(),
+            "traffic": tile_profile_traffic(prof),
             "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of the same launch, "
-                              "profiles/k_m2l_tiles_laplace_3e5_p14_level5.md",
-            "algorithmic_flops_per_launch": flops, "ms_per_launch": ms,
-            "frac_of_bf16_tensor_peak": (achieved / bf16) if bf16 else None}
+                              "profiles/" + os.path.basename(prof),
+            "algorithmic_flops_per_launch": flops, "ms_per_launch": ms}
 
 
 def p2p_pairs(s, depth):
@@ -935,11 +941,10 @@ def p2p_pairs(s, depth):
 
 
 def p2p_roofline(local):
-    """The served stream's dominant kernel (the FP32 near field, Helmholtz
-    potential and gradient, 44 flops per pair with each MUFU operation counted
-    once): 2e5 points, depth 4, k = 10; its time is the evaluation's minus the
-    L2P's (CUDA events, L2 flushed before each), against the FP32 FMA peak
-    measured here."""
+    """The FP32 near field (Helmholtz potential and gradient, 44 flops per
+    pair with each MUFU operation counted once): 2e5 points, depth 4,
+    k = 10; its time is the evaluation's minus the L2P's (CUDA events, L2
+    flushed before each), against the FP32 FMA peak measured here."""
     import torch
 
     from wbfmm_b200 import engine
@@ -974,8 +979,7 @@ def p2p_roofline(local):
     flops = pairs * 44
     achieved = flops / (ms * 1e-3) / 1e12
     return {"bound": "simt", "kernel": "k_p2p<float, Helmholtz> potential + gradient: near field "
-                                       "of 200,000 points, depth 4 (41% of the served stream's "
-                                       "device time)",
+                                       "of 200,000 points, depth 4",
             "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
             "peak_source": "FP32 FMA throughput measured live (wbfmm_b200_fp32_fma_peak)",
             "traffic": tile_profile_traffic(P2P_PROFILE),
@@ -1044,8 +1048,9 @@ def our_arm(args, ws, rank, local):
                                     label, min(args.steps, 5))
         for k in ("fp32", "fp64"):
             cube[k].pop("step_ms", None)
-    roofline = p2p_roofline(local)
-    roofline_m2l = tile_roofline(local)
+    roofline = tile_roofline(local, helm=True)
+    roofline_p2p = p2p_roofline(local)
+    roofline_m2l_laplace = tile_roofline(local, helm=False)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         from oracle.oracle_api import have_reference
@@ -1073,7 +1078,8 @@ def our_arm(args, ws, rank, local):
         "e2e": {"value": sh["points_per_s"], "unit": "points/s", "ms_per_step": sh["ms_per_step"],
                 "h2d_bytes_per_step": ws * served["bytes_per_step"]["h2d"],
                 "d2h_bytes_per_step": ws * served["bytes_per_step"]["d2h"]},
-        "roofline": roofline, "roofline_m2l": roofline_m2l, "cpu_baseline": cpu,
+        "roofline": roofline, "roofline_p2p": roofline_p2p,
+        "roofline_m2l_laplace": roofline_m2l_laplace, "cpu_baseline": cpu,
         "gpu_launches": sd["kernel_launches_per_step"], "clocks": sd["clocks"],
         "served": served, "cube_c2": cube,
     }
