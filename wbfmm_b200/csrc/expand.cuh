@@ -14,7 +14,10 @@
 // P2M routines generate their coefficient contributions in a fixed order
 // that depends only on the expansion order, through an `emit(index, re, im)`
 // callback; the warp kernels reduce each emission across lanes, so the
-// lanes of a warp must (and do) follow the same sequence.
+// lanes of a warp must (and do) follow the same sequence.  Two coefficients
+// computed together (Helmholtz orders +m and -m, Laplace's cos and sin
+// parts) go through the emitter's pair(...) where it has one (a warp
+// reduction of several values at once), else one by one (emit_two).
 #pragma once
 
 #include "fmm_math.cuh"
@@ -35,6 +38,28 @@ HD void zero_rows(const Scratch<T>& sc, int k) {
     Row<T> w = sc.row(r);
     for (int i = 0; i < sc.len; i++) w[i] = T(0);
   }
+}
+
+// two emissions: e.pair(...) when the emitter has it, else e(...) twice
+template <class E, typename T>
+HD auto emit_two(E& e, int i1, T r1, T m1, int i2, T r2, T m2, int)
+    -> decltype(e.pair(i1, r1, m1, i2, r2, m2), void()) {
+  e.pair(i1, r1, m1, i2, r2, m2);
+}
+template <class E, typename T>
+HD void emit_two(E& e, int i1, T r1, T m1, int i2, T r2, T m2, long) {
+  e(i1, r1, m1);
+  e(i2, r2, m2);
+}
+template <class E, typename T>
+HD auto emit_two(E& e, int i1, T v1, int i2, T v2, int)
+    -> decltype(e.pair(i1, v1, i2, v2), void()) {
+  e.pair(i1, v1, i2, v2);
+}
+template <class E, typename T>
+HD void emit_two(E& e, int i1, T v1, int i2, T v2, long) {
+  e(i1, v1);
+  e(i2, v2);
 }
 
 // (cos, sin) of (m+1) ph from those of m ph and ph
@@ -64,11 +89,16 @@ HD void p2m_helmholtz(int N, T k, const T* xc, const T* xs, T qr, T qi,
     emit(cidx(n, sgn * m), a * (qr * cm + sgn * qi * smm),
          a * (qi * cm - sgn * qr * smm));
   };
+  // orders +m and -m together
+  auto pair = [&](int n, int m, T jn, T P, T cm, T smm) {
+    const T a = jn * P;
+    emit_two(emit, cidx(n, m), a * (qr * cm + qi * smm), a * (qi * cm - qr * smm),
+             cidx(n, -m), a * (qr * cm - qi * smm), a * (qi * cm + qr * smm), 0);
+  };
   term(0, 0, 1, bj.jm, pm[0], T(1), T(0));
   if (N == 1) return;
   term(1, 0, 1, bj.j, pn[0], T(1), T(0));
-  term(1, 1, 1, bj.j, pn[1], c1, s1);
-  term(1, 1, -1, bj.j, pn[1], c1, s1);
+  pair(1, 1, bj.j, pn[1], c1, s1);
   for (int n = 2; n <= N; n++) {
     legendre_step(pm, pn, n - 1, C, S, leg);
     Row<T> t = pm; pm = pn; pn = t;
@@ -77,9 +107,7 @@ HD void p2m_helmholtz(int N, T k, const T* xc, const T* xs, T qr, T qi,
     T cm = T(1), smm = T(0);
     for (int m = 1; m <= n; m++) {
       rot_next(cm, smm, c1, s1, &cm, &smm);
-      const T P = pn[m];
-      term(n, m, 1, bj.j, P, cm, smm);
-      term(n, m, -1, bj.j, P, cm, smm);
+      pair(n, m, bj.j, pn[m], cm, smm);
     }
   }
 }
@@ -162,8 +190,8 @@ HD void p2m_laplace(int N, const T* xc, const T* xs, T q, Emit&& emit,
   emit(0, q * rn * pm[0] / T(1));
   rn = r;
   emit(1, q * rn * pn[0] / T(3));
-  emit(lidx(1, 1), q * rn * pn[1] * c1 / T(3));
-  emit(lidx(1, 1) + 1, -(q * rn * pn[1] * s1 / T(3)));
+  emit_two(emit, lidx(1, 1), q * rn * pn[1] * c1 / T(3), lidx(1, 1) + 1,
+           -(q * rn * pn[1] * s1 / T(3)), 0);
   for (int n = 2; n <= N; n++) {
     rn *= r;
     legendre_step(pm, pn, n - 1, C, S, leg);
@@ -175,8 +203,7 @@ HD void p2m_laplace(int N, const T* xc, const T* xs, T q, Emit&& emit,
       rot_next(cm, smm, c1, s1, &cm, &smm);
       const int id = lidx(n, m);
       const T P = pn[m];
-      emit(id, q * rn * P * cm * inv);
-      emit(id + 1, -(q * rn * P * smm * inv));
+      emit_two(emit, id, q * rn * P * cm * inv, id + 1, -(q * rn * P * smm * inv), 0);
     }
   }
 }

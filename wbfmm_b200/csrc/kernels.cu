@@ -35,6 +35,62 @@ __device__ __forceinline__ T warp_sum(T v) {
   return v;
 }
 
+// Sums over the warp of several values at once, by transposing while
+// reducing: after the exchanges across lanes 16 (and 8) apart, each half
+// (quarter) of the warp carries one value, whose sum the remaining steps
+// form.  Two values: lanes 0-15 hold the sum of a, 16-31 of b (5 shuffles
+// instead of 10); four: lanes 0-7, 8-15, 16-23, 24-31 hold those of a, b,
+// c, d (6 shuffles instead of 20).
+template <typename T>
+__device__ __forceinline__ T warp_sum2(T a, T b, int lane) {
+  const bool hi = lane & 16;
+  T w = (hi ? b : a) + __shfl_xor_sync(0xffffffffu, hi ? a : b, 16);
+#pragma unroll
+  for (int o = 8; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+  return w;
+}
+template <typename T>
+__device__ __forceinline__ T warp_sum4(T a, T b, T c, T d, int lane) {
+  const bool hi = lane & 16, q = lane & 8;
+  const T u = (hi ? c : a) + __shfl_xor_sync(0xffffffffu, hi ? a : c, 16);
+  const T v = (hi ? d : b) + __shfl_xor_sync(0xffffffffu, hi ? b : d, 16);
+  T w = (q ? v : u) + __shfl_xor_sync(0xffffffffu, q ? u : v, 8);
+#pragma unroll
+  for (int o = 4; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+  return w;
+}
+
+// the P2M kernel's emitters: each emission summed over the warp's points
+// (one per lane) into the warp's accumulator in shared memory; pairs of
+// emissions reduced together (warp_sum2 / warp_sum4), their sums added by
+// one lane of each half / quarter
+template <typename T>
+struct P2MEmitHelm {
+  T* acc;
+  int lane;
+  __device__ __forceinline__ void operator()(int idx, T re, T im) const {
+    re = warp_sum(re); im = warp_sum(im);
+    if (lane == 0) { acc[2 * idx] += re; acc[2 * idx + 1] += im; }
+  }
+  __device__ __forceinline__ void pair(int i1, T r1, T m1, int i2, T r2, T m2) const {
+    const T w = warp_sum4(r1, m1, r2, m2, lane);
+    if ((lane & 7) == 0) acc[2 * ((lane & 16) ? i2 : i1) + ((lane & 8) ? 1 : 0)] += w;
+  }
+};
+template <typename T>
+struct P2MEmitLap {
+  T* acc;
+  int lane;
+  __device__ __forceinline__ void operator()(int idx, T v) const {
+    v = warp_sum(v);
+    if (lane == 0) acc[idx] += v;
+  }
+  __device__ __forceinline__ void pair(int i1, T v1, int i2, T v2) const {
+    const T w = warp_sum2(v1, v2, lane);
+    if ((lane & 15) == 0) acc[(lane & 16) ? i2 : i1] += w;
+  }
+};
+
 // box centre exactly as wbfmm_tree_box_centre (src/util.c:290-330)
 __device__ __forceinline__ void box_centre(int64_t b, double x0, double y0,
                                            double z0, double wb, double* c) {
@@ -116,10 +172,7 @@ __global__ void k_p2m(P2MParams<T> p, int legt) {
                  act ? (T)(p.z[s] - cd[2]) : T(0)};
       auto expand = [&](const auto& leg) {
         if (HELM) {
-          auto emit = [&](int idx, T re, T im) {
-            re = warp_sum(re); im = warp_sum(im);
-            if (lane == 0) { acc[2 * idx] += re; acc[2 * idx + 1] += im; }
-          };
+          const P2MEmitHelm<T> emit{acc, lane};
           if (p.q) {
             T qr = act ? p.q[2 * s] : T(0), qi = act ? p.q[2 * s + 1] : T(0);
             p2m_helmholtz<T>(p.N, p.k, xc, xs, qr, qi, emit, leg, sc);
@@ -131,10 +184,7 @@ __global__ void k_p2m(P2MParams<T> p, int legt) {
             p2m_helmholtz_dipole<T>(p.N, p.k, xc, xs, nrm, dr, di, emit, leg, sc);
           }
         } else {
-          auto emit = [&](int idx, T v) {
-            v = warp_sum(v);
-            if (lane == 0) acc[idx] += v;
-          };
+          const P2MEmitLap<T> emit{acc, lane};
           if (p.q) {
             T qv = act ? p.q[s] : T(0);
             p2m_laplace<T>(p.N, xc, xs, qv, emit, leg, sc);
