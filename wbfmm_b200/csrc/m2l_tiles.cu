@@ -167,6 +167,14 @@ __device__ __forceinline__ void load_cols(const double2* p, double2 (&o)[4]) {
 #pragma unroll
   for (int k = 0; k < 4; k++) o[k] = p[k];
 }
+__device__ __forceinline__ void store_cols(float2* p, const float2 (&v)[4]) {
+  reinterpret_cast<float4*>(p)[0] = make_float4(v[0].x, v[0].y, v[1].x, v[1].y);
+  reinterpret_cast<float4*>(p)[1] = make_float4(v[2].x, v[2].y, v[3].x, v[3].y);
+}
+__device__ __forceinline__ void store_cols(double2* p, const double2 (&v)[4]) {
+#pragma unroll
+  for (int k = 0; k < 4; k++) p[k] = v[k];
+}
 
 template <typename T2, typename T>
 __device__ __forceinline__ T2 cmul(T2 a, T er, T ei) {
@@ -475,7 +483,10 @@ k_m2l_tiles(LanesParams<T> p, OpTables<T> t, int TC, bool dense) {
       }
     }
     __syncthreads();
-    // stage D: back rotation per degree, e^{-i nu ch}, accumulate
+    // stage D: back rotation per degree, e^{-i nu ch}, accumulate; when
+    // every target has a column (the map is the identity) a thread's four
+    // accumulator columns are updated with two 16-byte loads and stores
+    const bool full = cnt == TC;
     for (int w = tid; w < q.nB * TQ; w += kTileThreads) {
       const int d = dB[w / TQ], t0 = (w % TQ) * 4;
       const int n = d & 255, nu0 = (d >> 8) - 64;
@@ -519,6 +530,17 @@ k_m2l_tiles(LanesParams<T> p, OpTables<T> t, int TC, bool dense) {
           const int nu = nu0 + r, an = nu < 0 ? -nu : nu;
           const T er = sech[2 * an], ei = nu < 0 ? sech[2 * an + 1] : -sech[2 * an + 1];
           T2* ar = A + (size_t)cidx(n, nu) * TC;
+          if (full) {
+            T2 cur[4];
+            load_cols(ar + t0, cur);
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+              const T2 o = cmul(r ? a1[k] : a0[k], er, ei);
+              cur[k].x += o.x; cur[k].y += o.y;
+            }
+            store_cols(ar + t0, cur);
+            continue;
+          }
 #pragma unroll
           for (int k = 0; k < 4; k++) {
             if (t0 + k >= cnt) break;
@@ -551,6 +573,18 @@ k_m2l_tiles(LanesParams<T> p, OpTables<T> t, int TC, bool dense) {
           const int nu = nu0 + r;
           const T er = sech[2 * nu], ei = sech[2 * nu + 1];
           T2* ar = A + (size_t)hidx(n, nu) * TC;
+          if (full) {
+            T2 cur[4];
+            load_cols(ar + t0, cur);
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+              const T2 a = r ? a1[k] : a0[k];
+              cur[k].x += er * a.x + ei * a.y;
+              if (nu != 0) cur[k].y += er * a.y - ei * a.x;
+            }
+            store_cols(ar + t0, cur);
+            continue;
+          }
 #pragma unroll
           for (int k = 0; k < 4; k++) {
             if (t0 + k >= cnt) break;
