@@ -183,3 +183,21 @@ def test_sparse_repeated_geometry(gpu_lib):
     ref2 = solve(p2, engine.FP64, False)
     for x, y in zip(c, ref2):
         assert rel_l2(x, y) < 1e-13
+
+
+def test_sparse_deep_clusters(gpu_lib):
+    """A deep tree of clustered points (2e6 points, depth 8, the lane M2L at
+    order 6): sparse and dense storage give the same fields, and the sparse
+    arrays are a fraction of the dense ones."""
+    p = W.laplace_clusters(2_000_000, depth=8, order=6, seed=66)
+    dense = solve(p, engine.FP32, False, mode=1)
+    ss, sparse = solve(p, engine.FP32, True, keep=True, mode=1)
+    try:
+        g, b = ss.coefficient_storage(0)
+        dense_bytes = sum(8 ** lv * 2 * (p.order_s[lv] + 1) ** 2 * 4 for lv in range(1, p.depth + 1))
+        assert b < dense_bytes / 4, (b, dense_bytes)
+    finally:
+        ss.close()
+    for a, c in zip(sparse, dense):
+        assert np.all(np.isfinite(a))
+        assert rel_l2(a, c) < 1e-6, rel_l2(a, c)
