@@ -201,3 +201,27 @@ def test_sparse_deep_clusters(gpu_lib):
     for a, c in zip(sparse, dense):
         assert np.all(np.isfinite(a))
         assert rel_l2(a, c) < 1e-6, rel_l2(a, c)
+
+
+def test_sparse_graph_replay(gpu_lib):
+    """Repeated solves with new strengths through the captured graph (the
+    group maps are built by the first, uncaptured run): the same fields as
+    direct runs, bit for bit."""
+    p = separate_targets(67)
+    rng = np.random.default_rng(68)
+    qs = [rng.standard_normal(p.ns) for _ in range(3)]
+    cfg = engine.SolverConfig.from_problem(p, engine.FP32, sparse=True)
+    refs = []
+    with engine.Solver(cfg) as s:
+        s.set_sources(p.xs).set_targets(p.xt)
+        for q in qs:
+            s.set_strengths(q).run()
+            refs.append(s.field())
+    with engine.Solver(cfg) as s:
+        s.set_deferred_checks(True)
+        s.set_sources(p.xs).set_targets(p.xt)
+        for q, ref in zip(qs, refs):
+            s.set_strengths(q).run_graph()
+            s.wait()
+            for a, b in zip(s.field(), ref):
+                assert np.array_equal(a, b)
