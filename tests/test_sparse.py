@@ -13,7 +13,9 @@ src/boxes.c:518-583).
 * the stored groups of each level are the boxes of the level above that
   hold sources (the tree's box counts) or targets (the floor rule of
   src/boxes.c:585-634, counted on the host); the bytes follow from them;
-* the calls that need dense Layout L arrays refuse a sparse solver.
+* the calls that need dense Layout L arrays refuse a sparse solver;
+* against the reference's own outputs (the golden fixtures) at 1e-10, and
+  under graph replay bit for bit.
 """
 import numpy as np
 import pytest
@@ -225,3 +227,27 @@ def test_sparse_graph_replay(gpu_lib):
             s.wait()
             for a, b in zip(s.field(), ref):
                 assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("name", ["laplace_small", "helmholtz_small", "laplace_dipole_small",
+                                  "helmholtz_dipole_small"])
+def test_sparse_matches_reference_golden(gpu_lib, name):
+    """Sparse storage against the reference's own outputs (the golden
+    fixtures: the unmodified reference FMM at the same depth and orders,
+    monopoles and dipoles), 1e-10 as the dense plain form."""
+    import os
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", name + ".npz"))
+    p = W.Problem(name, int(z["problem"]), int(z["depth"]), list(z["order_s"]),
+                  list(z["order_r"]), float(z["k"]), z["xs"], z["q"] if z["q"].size else None,
+                  z["xt"], normals=z["normals"] if z["normals"].size else None,
+                  dipoles=z["dipoles"] if z["dipoles"].size else None)
+    p.x0, p.D = z["x0"], float(z["D"])
+    has_grad = z["grad"].size > 0
+    field = engine.POTENTIAL | (engine.GRADIENT if has_grad else 0)
+    cfg = engine.SolverConfig.from_problem(p, engine.FP64, field, sparse=True)
+    with engine.Solver(cfg) as s:
+        s.set_sources(p.xs, p.normals).set_strengths(p.q, p.dipoles).set_targets(p.xt).run()
+        pot, grad = s.field()
+    assert rel_l2(pot, z["pot"]) < 1e-10
+    if has_grad:
+        assert rel_l2(grad, z["grad"]) < 1e-10
