@@ -11,6 +11,11 @@
 // its arrays, so the same values); the spherical Bessel functions come
 // from BesselJSeq.
 //
+// The P2M loops are marked for unrolling: with a compile-time order (the
+// kernels' fixed-order instantiation, scratch rows in a per-thread array)
+// every index becomes a constant and the rows stay in registers; with a
+// run-time order the loops are left as they are.
+//
 // P2M routines generate their coefficient contributions in a fixed order
 // that depends only on the expansion order, through an `emit(index, re, im)`
 // callback; the warp kernels reduce each emission across lanes, so the
@@ -34,8 +39,10 @@ HD int l2p_rows(bool helm, bool grad) { return helm && grad ? 3 : 2; }
 // zero rows 0..k-1 (entries 0..len-1)
 template <typename T>
 HD void zero_rows(const Scratch<T>& sc, int k) {
+#pragma unroll
   for (int r = 0; r < k; r++) {
     Row<T> w = sc.row(r);
+#pragma unroll
     for (int i = 0; i < sc.len; i++) w[i] = T(0);
   }
 }
@@ -99,12 +106,14 @@ HD void p2m_helmholtz(int N, T k, const T* xc, const T* xs, T qr, T qi,
   if (N == 1) return;
   term(1, 0, 1, bj.j, pn[0], T(1), T(0));
   pair(1, 1, bj.j, pn[1], c1, s1);
+#pragma unroll
   for (int n = 2; n <= N; n++) {
     legendre_step(pm, pn, n - 1, C, S, leg);
     Row<T> t = pm; pm = pn; pn = t;
     bj.step();
     term(n, 0, 1, bj.j, pn[0], T(1), T(0));
     T cm = T(1), smm = T(0);
+#pragma unroll
     for (int m = 1; m <= n; m++) {
       rot_next(cm, smm, c1, s1, &cm, &smm);
       pair(n, m, bj.j, pn[m], cm, smm);
@@ -157,12 +166,14 @@ HD void p2m_helmholtz_dipole(int N, T k, const T* xc, const T* xs,
   inc(1, 0, 1, bj.j, pn[0], T(1), T(0));
   inc(1, 1, 1, bj.j, pn[1], c1, s1);
   inc(1, 1, -1, bj.j, pn[1], c1, s1);
+#pragma unroll
   for (int n = 2; n <= N; n++) {
     legendre_step(pm, pn, n - 1, C, S, leg);
     Row<T> t = pm; pm = pn; pn = t;
     bj.step();
     inc(n, 0, 1, bj.j, pn[0], T(1), T(0));
     T cm = T(1), smm = T(0);
+#pragma unroll
     for (int m = 1; m <= n; m++) {
       rot_next(cm, smm, c1, s1, &cm, &smm);
       const T P = pn[m];
@@ -192,6 +203,7 @@ HD void p2m_laplace(int N, const T* xc, const T* xs, T q, Emit&& emit,
   emit(1, q * rn * pn[0] / T(3));
   emit_two(emit, lidx(1, 1), q * rn * pn[1] * c1 / T(3), lidx(1, 1) + 1,
            -(q * rn * pn[1] * s1 / T(3)), 0);
+#pragma unroll
   for (int n = 2; n <= N; n++) {
     rn *= r;
     legendre_step(pm, pn, n - 1, C, S, leg);
@@ -199,6 +211,7 @@ HD void p2m_laplace(int N, const T* xc, const T* xs, T q, Emit&& emit,
     T inv = T(1) / (T)(2 * n + 1);
     emit(n * n, q * rn * pn[0] * inv);
     T cm = T(1), smm = T(0);
+#pragma unroll
     for (int m = 1; m <= n; m++) {
       rot_next(cm, smm, c1, s1, &cm, &smm);
       const int id = lidx(n, m);
@@ -268,6 +281,7 @@ HD void p2m_laplace_dipole(int N, const T* xc, const T* xs, const T* nrm,
   inc_m0(1, rn, pn[0]);
   inc_m1(1, rn, pn[1]);
   if (N == 2) return;
+#pragma unroll
   for (int n = 2; n < N; n++) {
     rn *= r;
     legendre_step(pm, pn, n - 1, C, S, leg);
@@ -275,6 +289,7 @@ HD void p2m_laplace_dipole(int N, const T* xc, const T* xs, const T* nrm,
     inc_m0(n, rn, pn[0]);
     inc_m1(n, rn, pn[1]);
     T cm = c1, smm = s1;
+#pragma unroll
     for (int m = 2; m <= n; m++) {
       rot_next(cm, smm, c1, s1, &cm, &smm);
       inc(n, m, rn, pn[m], cm, smm);

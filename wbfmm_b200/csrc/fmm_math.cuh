@@ -204,6 +204,7 @@ HD void legendre_step(R pnm1, R pn, int n, T C, T S, const Leg& L = Leg()) {
   pnm1[n + 1] = L.d(n) * S * pn[n];
   pn[n + 1] = T(0);
   const T sq = L.c(n);
+#pragma unroll
   for (int m = 0; m <= n; m++) {
     const T v = C * sq * pn[m] - L.a(n, m) * pnm1[m];
     pnm1[m] = v * L.b(n, m);

@@ -124,37 +124,42 @@ static size_t l2p_row_bytes(int N, bool helm, bool grad, int threads) {
 // is worth more than the shorter latency
 constexpr size_t kRowSmemMax = 48 * 1024;
 constexpr int kL2PBoxes = 4;     // leaf boxes whose expansions an L2P CTA stages
+constexpr int kP2MFixedOrder = 14;   // P2M order with a compile-time instantiation
 #define WBFMM_TRY_K(call)          \
   do {                             \
     const int rc_ = (call);        \
     if (rc_) return rc_;           \
   } while (0)
 
-// SROWS: recursion rows in shared memory (else per-thread local arrays)
-template <typename T, bool HELM, bool SROWS>
+// SROWS: recursion rows in shared memory (else per-thread local arrays);
+// NC > 0: the expansion order fixed at compile time (p.N == NC), the rows
+// in a per-thread array whose every index the unrolled recursion knows, so
+// that they stay in registers
+template <typename T, bool HELM, bool SROWS, int NC = 0>
 __global__ void k_p2m(P2MParams<T> p, int legt) {
   extern __shared__ __align__(16) unsigned char smraw[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int nw = blockDim.x >> 5;
   // Legendre recursion constants of degrees <= N + 2, once per CTA
-  const int LW = p.N + 3;
+  const int LW = (NC > 0 ? NC : p.N) + 3;
   T* lt = (T*)smraw;
   if (legt) {
-    leg_table_fill(lt, p.N + 2, threadIdx.x, blockDim.x);
+    leg_table_fill(lt, LW - 1, threadIdx.x, blockDim.x);
     __syncthreads();
   }
   // the box's storage index, and (sparse storage) its Morton index
   const int64_t cb = (int64_t)blockIdx.x * nw + warp;
   if (cb >= p.nbox) return;   // whole warp leaves; no block barriers below
   const int64_t b = p.glist ? (((int64_t)p.glist[cb >> 3] << 3) | (cb & 7)) : cb;
-  const int nc = ncoef(p.N);
+  const int N = NC > 0 ? NC : p.N;
+  const int nc = ncoef(N);
   const int w = HELM ? 2 : 1;
-  const int RL = p.N + kRowPad;
+  const int RL = N + kRowPad;
   T* rows = (T*)smraw + (legt ? 4 * LW * LW : 0);
-  T loc[SROWS ? 1 : 2 * kPtMax];
-  const Scratch<T> sc = SROWS ? Scratch<T>{rows + threadIdx.x, RL, (int)blockDim.x}
-                              : Scratch<T>{loc, RL, 1};
-  T* acc = rows + (SROWS ? p2m_rows() * RL * blockDim.x : 0) + (size_t)warp * nc * w;
+  T loc[NC > 0 ? 2 * (NC + kRowPad) : (SROWS ? 1 : 2 * kPtMax)];
+  const Scratch<T> sc = SROWS && NC == 0 ? Scratch<T>{rows + threadIdx.x, RL, (int)blockDim.x}
+                                         : Scratch<T>{loc, RL, 1};
+  T* acc = rows + (SROWS && NC == 0 ? p2m_rows() * RL * blockDim.x : 0) + (size_t)warp * nc * w;
   for (int c = lane; c < nc * w; c += 32) acc[c] = T(0);
   __syncwarp();
   const uint32_t cnt = p.box_n[b], start = p.box_i[b];
@@ -175,25 +180,25 @@ __global__ void k_p2m(P2MParams<T> p, int legt) {
           const P2MEmitHelm<T> emit{acc, lane};
           if (p.q) {
             T qr = act ? p.q[2 * s] : T(0), qi = act ? p.q[2 * s + 1] : T(0);
-            p2m_helmholtz<T>(p.N, p.k, xc, xs, qr, qi, emit, leg, sc);
+            p2m_helmholtz<T>(N, p.k, xc, xs, qr, qi, emit, leg, sc);
           }
           if (p.dip) {
             T dr = act ? p.dip[2 * s] : T(0), di = act ? p.dip[2 * s + 1] : T(0);
             T nrm[3] = {act ? p.nx[s] : T(0), act ? p.ny[s] : T(0),
                         act ? p.nz[s] : T(1)};
-            p2m_helmholtz_dipole<T>(p.N, p.k, xc, xs, nrm, dr, di, emit, leg, sc);
+            p2m_helmholtz_dipole<T>(N, p.k, xc, xs, nrm, dr, di, emit, leg, sc);
           }
         } else {
           const P2MEmitLap<T> emit{acc, lane};
           if (p.q) {
             T qv = act ? p.q[s] : T(0);
-            p2m_laplace<T>(p.N, xc, xs, qv, emit, leg, sc);
+            p2m_laplace<T>(N, xc, xs, qv, emit, leg, sc);
           }
           if (p.dip) {
             T dv = act ? p.dip[s] : T(0);
             T nrm[3] = {act ? p.nx[s] : T(0), act ? p.ny[s] : T(0),
                         act ? p.nz[s] : T(1)};
-            p2m_laplace_dipole<T>(p.N, xc, xs, nrm, dv, emit, leg, sc);
+            p2m_laplace_dipole<T>(N, xc, xs, nrm, dv, emit, leg, sc);
           }
         }
       };
@@ -227,7 +232,12 @@ int launch_p2m(const P2MParams<T>& p, cudaStream_t s) {
   const bool srows = rows <= kRowSmemMax;
   size_t smem = leg + (srows ? rows : 0) + sizeof(T) * (size_t)nw * ncoef(p.N) * (HELM ? 2 : 1);
   unsigned grid = (unsigned)((p.nbox + nw - 1) / nw);
-  if (srows) {
+  if (p.N == kP2MFixedOrder) {
+    // the serving orders' leaf expansions: rows in registers
+    const size_t sm = leg + sizeof(T) * (size_t)nw * ncoef(p.N) * (HELM ? 2 : 1);
+    if (sm > 48 * 1024) WBFMM_SMEM(sm, k_p2m<T, HELM, false, kP2MFixedOrder>);
+    k_p2m<T, HELM, false, kP2MFixedOrder><<<grid, nw * 32, sm, s>>>(p, leg ? 1 : 0);
+  } else if (srows) {
     if (smem > 48 * 1024) WBFMM_SMEM(smem, k_p2m<T, HELM, true>);
     k_p2m<T, HELM, true><<<grid, nw * 32, smem, s>>>(p, leg ? 1 : 0);
   } else {
