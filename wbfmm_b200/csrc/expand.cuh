@@ -11,10 +11,11 @@
 // its arrays, so the same values); the spherical Bessel functions come
 // from BesselJSeq.
 //
-// The P2M loops are marked for unrolling: with a compile-time order (the
-// kernels' fixed-order instantiation, scratch rows in a per-thread array)
-// every index becomes a constant and the rows stay in registers; with a
-// run-time order the loops are left as they are.
+// The P2M and Laplace L2P loops are marked for unrolling: with a
+// compile-time order (the kernels' fixed-order instantiations, scratch rows
+// in a per-thread array) every index becomes a constant and the rows stay
+// in registers.  The Helmholtz L2P is not: unrolled at order 14 it needed
+// 170-255 registers and ran slower.
 //
 // P2M routines generate their coefficient contributions in a fixed order
 // that depends only on the expansion order, through an `emit(index, re, im)`
@@ -446,12 +447,14 @@ HD T l2p_laplace(int N, const T* xc, const T* xf, Coef&& coef,
   rn *= r;
   f += coef(1) * rn * pn[0];
   f += T(2) * pn[1] * rn * (coef(lidx(1, 1)) * c1 - coef(lidx(1, 1) + 1) * s1);
+#pragma unroll
   for (int n = 2; n <= N; n++) {
     rn *= r;
     legendre_step(pm, pn, n - 1, C, S, leg);
     Row<T> t = pm; pm = pn; pn = t;
     f += coef(n * n) * rn * pn[0];
     T cm = T(1), smm = T(0);
+#pragma unroll
     for (int m = 1; m <= n; m++) {
       rot_next(cm, smm, c1, s1, &cm, &smm);
       int id = lidx(n, m);
@@ -517,12 +520,14 @@ HD void l2p_laplace_grad(int N, const T* xc, const T* xf, Coef&& coef, T* g,
     if (pot) f += coef(0) * pm[0] + coef(1) * r * pn[0];
   }
   d_m(1, 1, rnm1, pm, pn, T(1), T(0), c1, s1, c2, s2);
+#pragma unroll
   for (int n = 2; n <= N; n++) {
     rnm1 *= r;
     legendre_step(pm, pn, n - 1, C, S, leg);
     Row<T> t = pm; pm = pn; pn = t;       // pm now degree n-1, pn degree n
     d_m0(n, rnm1, pm, pn);
     T ca = T(1), sa = T(0), cb = c1, sb = s1, cc, scc;
+#pragma unroll
     for (int m = 1; m <= n; m++) {
       rot_next(cb, sb, c1, s1, &cc, &scc);
       d_m(n, m, rnm1, pm, pn, ca, sa, cb, sb, cc, scc);

@@ -124,7 +124,7 @@ static size_t l2p_row_bytes(int N, bool helm, bool grad, int threads) {
 // is worth more than the shorter latency
 constexpr size_t kRowSmemMax = 48 * 1024;
 constexpr int kL2PBoxes = 4;     // leaf boxes whose expansions an L2P CTA stages
-constexpr int kP2MFixedOrder = 14;   // P2M order with a compile-time instantiation
+constexpr int kFixedOrder = 14;   // P2M / L2P order with a compile-time instantiation
 #define WBFMM_TRY_K(call)          \
   do {                             \
     const int rc_ = (call);        \
@@ -232,11 +232,15 @@ int launch_p2m(const P2MParams<T>& p, cudaStream_t s) {
   const bool srows = rows <= kRowSmemMax;
   size_t smem = leg + (srows ? rows : 0) + sizeof(T) * (size_t)nw * ncoef(p.N) * (HELM ? 2 : 1);
   unsigned grid = (unsigned)((p.nbox + nw - 1) / nw);
-  if (p.N == kP2MFixedOrder) {
-    // the serving orders' leaf expansions: rows in registers
-    const size_t sm = leg + sizeof(T) * (size_t)nw * ncoef(p.N) * (HELM ? 2 : 1);
-    if (sm > 48 * 1024) WBFMM_SMEM(sm, k_p2m<T, HELM, false, kP2MFixedOrder>);
-    k_p2m<T, HELM, false, kP2MFixedOrder><<<grid, nw * 32, sm, s>>>(p, leg ? 1 : 0);
+  // the serving orders' leaf expansions: rows in registers (not for FP64
+  // Helmholtz, whose unrolled recursion exceeds the register file)
+  constexpr bool kFixedOk = !(HELM && sizeof(T) == 8);
+  if (kFixedOk && p.N == kFixedOrder) {
+    if constexpr (kFixedOk) {
+      const size_t sm = leg + sizeof(T) * (size_t)nw * ncoef(p.N) * (HELM ? 2 : 1);
+      if (sm > 48 * 1024) WBFMM_SMEM(sm, k_p2m<T, HELM, false, kFixedOrder>);
+      k_p2m<T, HELM, false, kFixedOrder><<<grid, nw * 32, sm, s>>>(p, leg ? 1 : 0);
+    }
   } else if (srows) {
     if (smem > 48 * 1024) WBFMM_SMEM(smem, k_p2m<T, HELM, true>);
     k_p2m<T, HELM, true><<<grid, nw * 32, smem, s>>>(p, leg ? 1 : 0);
@@ -637,23 +641,26 @@ __host__ __device__ inline size_t l2p_table_bytes(int N) {
 // per-thread local arrays)
 // stage: the CTA's leaf expansions copied to shared memory when its targets
 // fall in at most kL2PBoxes leaf boxes (targets are sorted by box)
-template <typename T, bool HELM, bool SROWS, bool STAGE>
+// NC > 0: the expansion order fixed at compile time (p.N == NC), the rows
+// in a per-thread array whose every index the unrolled recursion knows
+template <typename T, bool HELM, bool SROWS, bool STAGE, int NC = 0>
 __global__ void k_l2p(EvalParams<T> p, int tab, int legt) {
   const int stage = STAGE ? 1 : 0;
   extern __shared__ __align__(16) unsigned char l2p_sm[];
   __shared__ unsigned s_bal[32];
   __shared__ int64_t s_box[kL2PBoxes];
   T* st = (T*)l2p_sm;
-  const int N = p.N;
+  const int N = NC > 0 ? NC : p.N;
   const int W = 2 * N + 3, M0 = N + 1;
   // Legendre constants (degrees <= N + 2) after the recursion tables
   const int LW = N + 3;
   T* lt = st + (tab ? l2p_table_bytes<T, HELM>(N) / sizeof(T) : 0);
   T* rows = lt + (legt ? 4 * LW * LW : 0);
-  T* cst = rows + (SROWS ? (size_t)l2p_rows(HELM, p.grad != nullptr) * (N + kRowPad) * blockDim.x : 0);
-  T loc[SROWS ? 1 : 3 * kPtMax];
-  const Scratch<T> sc = SROWS ? Scratch<T>{rows + threadIdx.x, N + kRowPad, (int)blockDim.x}
-                              : Scratch<T>{loc, N + kRowPad, 1};
+  constexpr bool SR = SROWS && NC == 0;
+  T* cst = rows + (SR ? (size_t)l2p_rows(HELM, p.grad != nullptr) * (N + kRowPad) * blockDim.x : 0);
+  T loc[NC > 0 ? 3 * (NC + kRowPad) : (SROWS ? 1 : 3 * kPtMax)];
+  const Scratch<T> sc = SR ? Scratch<T>{rows + threadIdx.x, N + kRowPad, (int)blockDim.x}
+                           : Scratch<T>{loc, N + kRowPad, 1};
   if (legt) leg_table_fill(lt, N + 2, threadIdx.x, blockDim.x);
   if (tab) {
     if (HELM) {
@@ -784,7 +791,21 @@ int launch_l2p(const EvalParams<T>& p, cudaStream_t s) {
     k_l2p<T, HELM, SR, ST><<<grid, 128, bytes, s>>>(p, sm ? 1 : 0, lg ? 1 : 0);
     return 0;
   };
-  if (rows <= kRowSmemMax) {
+  // the serving orders' Laplace leaf evaluation: rows in registers (the
+  // Helmholtz one, unrolled, needs 170-255 registers and runs slower)
+  constexpr bool kFixedOk = !HELM;
+  if (kFixedOk && p.N == kFixedOrder) {
+    if constexpr (kFixedOk) {
+      auto fixed = [&](auto stg) -> int {
+        constexpr bool ST = decltype(stg)::value;
+        const size_t bytes = sm + lg + (ST ? cb : 0);
+        if (bytes > 48 * 1024) WBFMM_SMEM(bytes, k_l2p<T, HELM, false, ST, kFixedOrder>);
+        k_l2p<T, HELM, false, ST, kFixedOrder><<<grid, 128, bytes, s>>>(p, sm ? 1 : 0, lg ? 1 : 0);
+        return 0;
+      };
+      WBFMM_TRY_K(stage ? fixed(std::true_type()) : fixed(std::false_type()));
+    }
+  } else if (rows <= kRowSmemMax) {
     WBFMM_TRY_K(stage ? go(std::true_type(), std::true_type()) : go(std::true_type(), std::false_type()));
   } else {
     WBFMM_TRY_K(stage ? go(std::false_type(), std::true_type()) : go(std::false_type(), std::false_type()));
