@@ -27,7 +27,8 @@ dataset).  One step = one batch of SERVE_BATCH requests.
   empty-box savings.  `served_over_plain` is value / plain value.
 * latency: Poisson arrivals at 30/50/70/90% of each arm's own batch
   throughput (host arrays) to one warmed server per arm, the loads one
-  after another, p50 / p99 per load; the top-level
+  after another, p50 / p99 per load, and per load the p99 and maximum of
+  each request's queue wait, host issue and device completion; the top-level
   `served_p50_s` / `served_p99_s` / `plain_p50_s` / `plain_p99_s` are at 70%.
 * accuracy: the served fields of sampled requests against the FP64 GPU
   direct sum (itself pinned to the reference's direct sums).
@@ -620,21 +621,33 @@ def served_section(args, ws, rank, local):
         for t in tk:
             srv.forget(t)
         lat = T[:, 3] - T[:, 0]
+        # where the time went: waiting for a slot (arrival -> start), the
+        # slot issuing the solve (start -> queued: staging and launches on
+        # the host), and the device finishing it (queued -> end)
+        parts = {"queue_wait": T[:, 1] - T[:, 0], "host_issue": T[:, 2] - T[:, 1],
+                 "completion": T[:, 3] - T[:, 2]}
         return {"offered_requests_per_s": float(rate),
                 "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
                 "mean_s": float(lat.mean()),
+                "parts_p99_s": {k: float(np.percentile(v, 99)) for k, v in parts.items()},
+                "parts_max_s": {k: float(v.max()) for k, v in parts.items()},
                 "achieved_points_per_s": float(sum(p.points for p in lat_reqs) /
                                                (T[:, 3].max() - base))}
 
     # one long-running server per arm, warmed once (pools, tables, kernels),
-    # sees the loads one after another (each drained before the next)
+    # sees the loads one after another (each drained before the next).  The
+    # warm-up runs every warm-up batch: a slot builds its FP64 solver at the
+    # first FP64 request it meets (a few percent of the stream), and one
+    # batch over six slots leaves some without one, a first-use cost (tens
+    # of ms of host issue) that would otherwise land in the first timed load
     latency = {}
     for name, slots, precf, skip, thr in (
             ("served_fp32", SERVE_SLOTS, served_prec, True, served_host["points_per_s"]),
             ("plain_fp64", 1, plain_prec, False, plain_host["points_per_s"])):
         latency[name] = {}
         with engine.Server(slots=slots) as srv:
-            run_batch(srv, warm[0], None, precf, skip)     # steady state
+            for b in warm:                                 # steady state
+                run_batch(srv, b, None, precf, skip)
             for load in SERVE_LOADS:
                 rate = load * thr / ws / mean_pts
                 latency[name][f"{int(load * 100)}%"] = run_latency(srv, precf, skip, rate,
