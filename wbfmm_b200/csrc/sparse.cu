@@ -73,7 +73,8 @@ size_t sparse_scan_scratch(int64_t n) {
 int sparse_group_map(const uint32_t* box_n, const uint8_t* tmask, int64_t n, uint32_t* flag,
                      uint32_t* gmap, uint32_t* count, void* scratch, size_t scratch_bytes,
                      cudaStream_t s) {
-  if (n <= 0 || n > 0x7fffffffLL) return set_error(-1, "sparse storage: group count out of range");
+  if (n <= 0 || n > 0x7fffffffLL)
+    return set_error(WBFMM_B200_E_ARG, "sparse storage: group count out of range");
   const unsigned blocks = (unsigned)((n + 255) / 256);
   k_group_flags<<<blocks, 256, 0, s>>>(box_n, tmask, n, flag);
   WBFMM_CUDA(cudaGetLastError());
