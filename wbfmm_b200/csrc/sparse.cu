@@ -12,6 +12,7 @@
 // scatter per level.
 #include <cub/cub.cuh>
 
+#include "../../include/wbfmm_b200.h"
 #include "engine.h"
 #include "fmm_math.cuh"
 #include "kernels.h"
