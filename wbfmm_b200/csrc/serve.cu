@@ -405,11 +405,15 @@ int wbfmm_b200_server_times(wbfmm_b200_server_t* srv, int64_t ticket,
   std::lock_guard<std::mutex> lk(srv->mu);
   auto it = srv->reqs.find(ticket);
   if (it == srv->reqs.end()) return set_error(WBFMM_B200_E_ARG, "unknown ticket");
-  t4[0] = it->second->t_arrival;
-  t4[1] = it->second->t_start;
-  t4[2] = it->second->t_queued;
-  t4[3] = it->second->t_end;
-  return it->second->state == 2 ? 0 : set_error(WBFMM_B200_E_STATE, "request not complete");
+  // a running request's slot writes its times without the lock; they are
+  // read only once its completion (written under the lock) is seen
+  const Req* q = it->second;
+  if (q->state != 2) return set_error(WBFMM_B200_E_STATE, "request not complete");
+  t4[0] = q->t_arrival;
+  t4[1] = q->t_start;
+  t4[2] = q->t_queued;
+  t4[3] = q->t_end;
+  return 0;
 }
 
 int wbfmm_b200_server_forget(wbfmm_b200_server_t* srv, int64_t ticket) {
@@ -430,17 +434,16 @@ int wbfmm_b200_server_drain(wbfmm_b200_server_t* srv) {
   return 0;
 }
 
-int wbfmm_b200_server_stats(wbfmm_b200_server_t* srv, int64_t* out6) {
-  if (!srv || !out6) return set_error(WBFMM_B200_E_ARG, "null argument");
-  int64_t* out7 = out6;
+int wbfmm_b200_server_stats(wbfmm_b200_server_t* srv, int64_t* out7) {
+  if (!srv || !out7) return set_error(WBFMM_B200_E_ARG, "null argument");
   std::lock_guard<std::mutex> lk(srv->mu);
   std::lock_guard<std::mutex> lc(srv->cache.mu);
-  out6[0] = srv->completed;
-  out6[1] = srv->peak_inflight;
-  out6[2] = srv->peak_running;
-  out6[3] = srv->cache.hits;
-  out6[4] = srv->cache.misses;
-  out6[5] = (int64_t)srv->cache.bytes;
+  out7[0] = srv->completed;
+  out7[1] = srv->peak_inflight;
+  out7[2] = srv->peak_running;
+  out7[3] = srv->cache.hits;
+  out7[4] = srv->cache.misses;
+  out7[5] = (int64_t)srv->cache.bytes;
   out7[6] = srv->launches;
   return 0;
 }
