@@ -49,6 +49,18 @@ def test_fp32_range_rule():
     assert not E.fp32_range_ok(lo)
 
 
+def test_poisson_arrivals():
+    """The latency runs' arrival times: increasing, seeded, and at the
+    offered rate (mean gap 1/rate; exponential gaps, so the coefficient of
+    variation is near one)."""
+    a = W.poisson_arrivals(20_000, 500.0, seed=7)
+    assert np.all(np.diff(a) > 0) and a[0] > 0
+    assert np.array_equal(a, W.poisson_arrivals(20_000, 500.0, seed=7))
+    gaps = np.diff(np.concatenate([[0.0], a]))
+    assert abs(gaps.mean() * 500.0 - 1.0) < 0.03
+    assert abs(gaps.std() / gaps.mean() - 1.0) < 0.05
+
+
 def test_footprint_grows_with_size():
     p1 = W.serve_request(np.random.default_rng(0), 2000, True, 5.0, False)
     p2 = W.serve_request(np.random.default_rng(0), 200000, True, 5.0, False)
