@@ -4,7 +4,8 @@ GPU tests: a request's fields are the same alone and inside a mixed stream;
 served FP32 fields meet 1e-6 relative-L2 against the FP64 direct sum; served
 FP64 fields equal the plain solver's; admission against the memory budget;
 a failing request leaves the others intact.  CPU tests: the serving-stream
-generator and the host-side helpers (footprint, FP32 range rule).
+generator, the latency runs' arrivals and the host-side helpers (footprint,
+FP32 range rule).
 """
 import math
 
